@@ -1,0 +1,237 @@
+"""CPU oracle for the ray-tracing hot path -- TEST INFRASTRUCTURE ONLY.
+
+This package is the checker.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg import it; the product package
+``vitrum_b200`` never does, and its CUDA path fails loudly when its own
+extension is missing instead of falling back here.
+
+The C restatement (``bvh_oracle.c``) follows the reference's shared-bvh CPU
+code (file:line citations in that file's header).  ``liborc.so`` is built by
+``make -C oracle`` (``__graft_entry__.build()`` runs it).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+LEAF_FLAG = 0xFFFF0000
+
+
+def build_library() -> str:
+    """Compile liborc.so in place (gcc; no reference sources involved)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "liborc.so")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liborc.so")
+        src = os.path.join(_HERE, "bvh_oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            build_library()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_hw_threads.restype = ctypes.c_int
+        L.orc_build_array_bvh.restype = ctypes.c_long
+        L.orc_build_array_bvh.argtypes = [P, ctypes.c_long, ctypes.c_int, P, ctypes.c_long, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P]
+        L.orc_collapse_wide.restype = ctypes.c_long
+        L.orc_collapse_wide.argtypes = [P, ctypes.c_long, ctypes.c_long, ctypes.c_long, P, P, P, P, P, P]
+        L.orc_first_hit_batch.restype = ctypes.c_int
+        L.orc_first_hit_batch.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_int, P, ctypes.c_int, P,
+                                          ctypes.c_long, P, ctypes.c_long, P, P, P, P, ctypes.c_int]
+        L.orc_count_visits.restype = ctypes.c_int
+        L.orc_count_visits.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_int, P, ctypes.c_int, P,
+                                       ctypes.c_long, P, P, ctypes.c_int]
+        L.orc_brute_first_hit.restype = ctypes.c_int
+        L.orc_brute_first_hit.argtypes = [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_long, P, ctypes.c_long,
+                                          P, P, P, P]
+        L.orc_triangle_fp64.restype = ctypes.c_int
+        L.orc_triangle_fp64.argtypes = [P, P, P, P, P, ctypes.c_double, P, P]
+        L.orc_watertight_f32.restype = ctypes.c_int
+        L.orc_watertight_f32.argtypes = [P, P, P, P, P, ctypes.c_float, P, P, P, P]
+        L.orc_first_hit_wt_batch.restype = ctypes.c_int
+        L.orc_first_hit_wt_batch.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_int, P, ctypes.c_int, P,
+                                             ctypes.c_long, P, ctypes.c_long, P, P, P, ctypes.c_int]
+        L.orc_wide_stack_entries.restype = ctypes.c_long
+        L.orc_wide_stack_entries.argtypes = [P, P, ctypes.c_long]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def hw_threads() -> int:
+    return int(lib().orc_hw_threads())
+
+
+class BinaryBvh:
+    """Result of the binary build: packed nodes plus triangle permutation."""
+
+    def __init__(self, nodes, reordered_to_source, indices, idx_stride):
+        self.nodes = nodes                      # (n, 8) uint32, buildArrayBvh.ts:13-27 layout
+        self.reordered_to_source = reordered_to_source
+        tri = reordered_to_source.astype(np.int64)
+        idx = indices.reshape(-1, idx_stride)
+        ro = np.zeros_like(idx)
+        ro[:, :3] = idx[tri, :3]
+        self.reordered_indices = ro.reshape(-1)  # reorderedIndices, padding lanes zero
+        self.idx_stride = idx_stride
+
+    @property
+    def node_count(self):
+        return self.nodes.shape[0]
+
+
+def build_array_bvh(positions, indices, pos_stride=4, idx_stride=4, max_leaf=4, bins=16, max_depth=58):
+    """buildArrayBvh (buildArrayBvh.ts:342) on float32 positions / uint32 indices."""
+    positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    indices = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+    ntri = indices.size // idx_stride
+    cap = max(1, 2 * ntri)
+    nodes = np.zeros((cap, 8), dtype=np.uint32)
+    r2s = np.zeros(max(ntri, 1), dtype=np.uint32)
+    n = lib().orc_build_array_bvh(_p(positions), positions.size, pos_stride, _p(indices), ntri, idx_stride,
+                                  max_leaf, bins, max_depth, _p(nodes), _p(r2s))
+    if n < 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return BinaryBvh(nodes[:n].copy(), r2s[:ntri].copy(), indices, idx_stride)
+
+
+class WideBvh:
+    def __init__(self, binary, node_bounds, child_bounds, child_meta, child_count, wide_to_binary, status):
+        self.binary = binary
+        self.node_bounds = node_bounds      # (n, 6) float32
+        self.child_bounds = child_bounds    # (n, 8, 6) uint16
+        self.child_meta = child_meta        # (n, 8, 3) uint32
+        self.child_count = child_count      # (n,) uint32
+        self.wide_to_binary = wide_to_binary
+        self.status = status                # 'wide' | 'empty' | 'binary-fallback'
+
+    @property
+    def node_count(self):
+        return self.child_count.shape[0]
+
+
+def collapse_wide(binary: BinaryBvh) -> WideBvh:
+    """buildCompressedWideBvhFromArrayBvh (compressedWideBvh.ts:248)."""
+    nb = binary.node_count
+    ntri = binary.reordered_to_source.size
+    cap = max(nb, 1)
+    node_bounds = np.zeros((cap, 6), dtype=np.float32)
+    child_bounds = np.zeros((cap, 8, 6), dtype=np.uint16)
+    child_meta = np.zeros((cap, 8, 3), dtype=np.uint32)
+    child_count = np.zeros(cap, dtype=np.uint32)
+    w2b = np.zeros(cap, dtype=np.uint32)
+    st = ctypes.c_int(0)
+    n = lib().orc_collapse_wide(_p(binary.nodes), nb, ntri, cap, _p(node_bounds), _p(child_bounds),
+                                _p(child_meta), _p(child_count), _p(w2b), ctypes.byref(st))
+    if n < 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    status = {0: "wide", 1: "empty", 2: "binary-fallback"}[st.value]
+    return WideBvh(binary, node_bounds[:n].copy(), child_bounds[:n].copy(), child_meta[:n].copy(),
+                   child_count[:n].copy(), w2b[:n].copy(), status)
+
+
+def build_compressed_wide_bvh(positions, indices, **kw) -> WideBvh:
+    """buildCompressedWideBvh (compressedWideBvh.ts:420)."""
+    return collapse_wide(build_array_bvh(positions, indices, **kw))
+
+
+def first_hit(wide: WideBvh, positions, rays, pos_stride=4, nthreads=0):
+    """intersectCompressedWideBvhFirstHit (compressedWideBvh.ts:754) per ray.
+
+    rays: (n, 8) float32 rows (ox, oy, oz, tmin, dx, dy, dz, tmax).
+    Returns (prim int32 [-1 miss], t float64 [inf miss], bary float64 (n,2) = (u, v), bvh_tri int32).
+    """
+    positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    prim = np.empty(n, dtype=np.int32)
+    t = np.empty(n, dtype=np.float64)
+    bary = np.empty((n, 2), dtype=np.float64)
+    bt = np.empty(n, dtype=np.int32)
+    b = wide.binary
+    lib().orc_first_hit_batch(_p(wide.node_bounds), _p(wide.child_bounds), _p(wide.child_meta),
+                              _p(wide.child_count), wide.node_count, _p(positions), pos_stride,
+                              _p(b.reordered_indices), b.idx_stride, _p(b.reordered_to_source),
+                              b.reordered_to_source.size, _p(rays), n, _p(prim), _p(t), _p(bary), _p(bt), nthreads)
+    return prim, t, bary, bt
+
+
+def first_hit_watertight(wide: WideBvh, positions, rays, pos_stride=4, nthreads=0):
+    """First hit with the f32 watertight test (the device semantic), same tree.
+
+    Returns (prim int32, t float32, bary float32 (n, 3) = weights of a, b, c).
+    """
+    positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    prim = np.empty(n, dtype=np.int32)
+    t = np.empty(n, dtype=np.float32)
+    bary = np.empty((n, 3), dtype=np.float32)
+    b = wide.binary
+    lib().orc_first_hit_wt_batch(_p(wide.node_bounds), _p(wide.child_bounds), _p(wide.child_meta),
+                                 _p(wide.child_count), wide.node_count, _p(positions), pos_stride,
+                                 _p(b.reordered_indices), b.idx_stride, _p(b.reordered_to_source),
+                                 b.reordered_to_source.size, _p(rays), n, _p(prim), _p(t), _p(bary), nthreads)
+    return prim, t, bary
+
+
+def count_visits(wide: WideBvh, positions, rays, pos_stride=4, nthreads=0):
+    """Near-first wide-node visits and triangle tests summed over the rays."""
+    positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    nn = ctypes.c_long(0)
+    nt = ctypes.c_long(0)
+    b = wide.binary
+    lib().orc_count_visits(_p(wide.node_bounds), _p(wide.child_bounds), _p(wide.child_meta),
+                           _p(wide.child_count), wide.node_count, _p(positions), pos_stride,
+                           _p(b.reordered_indices), b.idx_stride, _p(rays), rays.shape[0],
+                           ctypes.byref(nn), ctypes.byref(nt), nthreads)
+    return nn.value, nt.value
+
+
+def brute_first_hit(positions, indices, rays, pos_stride=4, idx_stride=4):
+    """Every triangle with the FP64 test; also returns the second-nearest t."""
+    positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    indices = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    prim = np.empty(n, dtype=np.int32)
+    t = np.empty(n, dtype=np.float64)
+    bary = np.empty((n, 2), dtype=np.float64)
+    second = np.empty(n, dtype=np.float64)
+    lib().orc_brute_first_hit(_p(positions), pos_stride, _p(indices), idx_stride, indices.size // idx_stride,
+                              _p(rays), n, _p(prim), _p(t), _p(bary), _p(second))
+    return prim, t, bary, second
+
+
+def triangle_fp64(o, d, a, b, c, tmin=0.0):
+    f = lambda v: np.ascontiguousarray(v, dtype=np.float32)
+    t = ctypes.c_double(0)
+    bary = np.zeros(3, dtype=np.float64)
+    hit = lib().orc_triangle_fp64(_p(f(o)), _p(f(d)), _p(f(a)), _p(f(b)), _p(f(c)), tmin, ctypes.byref(t), _p(bary))
+    return bool(hit), t.value, bary
+
+
+def watertight_f32(o, d, a, b, c, exclusive_min_t=0.0):
+    """intersectOpticalTriangleWatertightF32 (opticalWatertightTriangle.ts:98)."""
+    f = lambda v: np.ascontiguousarray(v, dtype=np.float32)
+    t = ctypes.c_float(0)
+    bary = np.zeros(3, dtype=np.float32)
+    side = ctypes.c_int(0)
+    mask = ctypes.c_int(0)
+    hit = lib().orc_watertight_f32(_p(f(o)), _p(f(d)), _p(f(a)), _p(f(b)), _p(f(c)), exclusive_min_t,
+                                   ctypes.byref(t), _p(bary), ctypes.byref(side), ctypes.byref(mask))
+    return dict(hit=bool(hit), t=t.value, bary=bary, side=side.value, zero_edge_mask=mask.value)

@@ -1,0 +1,179 @@
+"""GPU parity of the BVH build and closest/any-hit traversal against the CPU oracle.
+
+Everything goes through the C ABI (libvitrum_pt.so).  Bars:
+  * binary build: bit-exact node words and triangle order vs the oracle
+    restatement of buildArrayBvh;
+  * hit ids: identical to the oracle's f32 watertight query (the device
+    semantic) on every ray, and to the FP64 reference query except rays whose
+    two nearest hits are within 1e-6 relative t ("tie") or that pass within
+    1e-3 barycentric of an edge ("edge", counted separately); "error" == 0;
+  * t within 1e-5 relative, barycentrics within 1e-5 absolute of FP64.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import parity
+from vitrum_b200 import bvh as vb
+from vitrum_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _build_both(soup, **opts):
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices, **opts)
+    kw = {}
+    if "maxLeafTriangles" in opts:
+        kw["max_leaf"] = opts["maxLeafTriangles"]
+    w = oracle.build_compressed_wide_bvh(soup.positions, soup.indices, **kw)
+    return g, w
+
+
+def _assert_parity(soup, rays, g, w, label):
+    hits = g.intersect_first_hit(rays)
+    wp, wt, _ = oracle.first_hit_watertight(w, soup.positions, rays)
+    # device decisions == watertight oracle decisions (f32 exact ties excepted)
+    diff = np.nonzero(hits["prim"] != wp)[0]
+    if diff.size:
+        r = parity.classify(soup.positions, soup.indices, rays[diff], hits[diff],
+                            tuple(x[diff] for x in oracle.first_hit(w, soup.positions, rays[diff])[:3]))
+        assert r["error"] == 0 and r["edge"] == 0, (label, "watertight mismatch", r)
+    ref = oracle.first_hit(w, soup.positions, rays)
+    rep = parity.classify(soup.positions, soup.indices, rays, hits, ref[:3])
+    assert rep["error"] == 0, (label, rep)
+    assert rep["t_bad"] == 0 and rep["bary_bad"] == 0, (label, rep)
+    occ = g.intersect_any_hit(rays)
+    assert np.array_equal(occ, hits["prim"] >= 0), label
+    return rep
+
+
+def test_build_bit_exact_config1_size(cuda):
+    soup = scenes.random_triangles(65536, seed=2024)
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices)
+    b = oracle.build_array_bvh(soup.positions, soup.indices)
+    nodes, r2s = g.export_binary()
+    assert np.array_equal(nodes, b.nodes)
+    assert np.array_equal(r2s, b.reordered_to_source)
+    info = g.info()
+    assert info["triangle_count"] == 65536 and info["binary_node_count"] == b.node_count
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 17, 100, 1000])
+def test_build_bit_exact_small(cuda, n):
+    soup = scenes.random_triangles(n, seed=n)
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices)
+    b = oracle.build_array_bvh(soup.positions, soup.indices)
+    nodes, r2s = g.export_binary()
+    assert np.array_equal(nodes, b.nodes) and np.array_equal(r2s, b.reordered_to_source)
+
+
+def test_closest_hit_parity_config1(cuda):
+    """65,536 triangles, 1,048,576 rays: the full closest-hit workload."""
+    soup, rays = scenes.config1()
+    g, w = _build_both(soup)
+    rep = _assert_parity(soup, rays, g, w, "config1")
+    assert rep["hits"] > 0.9 * rep["n"]
+    print("config1 parity:", rep)
+
+
+@pytest.mark.parametrize("leaf", [1, 2, 3])
+def test_closest_hit_parity_leaf_sizes(cuda, leaf):
+    soup = scenes.random_triangles(5000, seed=10 + leaf)
+    rays = scenes.sphere_rays(20000, seed=20 + leaf)
+    g, w = _build_both(soup, maxLeafTriangles=leaf)
+    _assert_parity(soup, rays, g, w, f"leaf{leaf}")
+
+
+def test_empty_mesh_misses(cuda):
+    g = vb.build_compressed_wide_bvh(np.zeros((0, 4), np.float32), np.zeros((0, 4), np.uint32))
+    rays = scenes.sphere_rays(1000, seed=3)
+    h = g.intersect_first_hit(rays)
+    assert (h["prim"] == -1).all()
+    assert not g.intersect_any_hit(rays).any()
+
+
+def test_single_triangle_and_tmin_tmax(cuda):
+    # cwbvhTMinParity.test.ts:31-67 through the device path
+    pos = np.array([-1, -1, 5, 0, 1, -1, 5, 0, 0, 1, 5, 0], np.float32)
+    idx = np.array([0, 1, 2, 0], np.uint32)
+    g = vb.build_compressed_wide_bvh(pos, idx)
+    rays = np.array([[0, 0, 0, 5, 0, 0, 1, np.inf],
+                     [0, 0, 0, 5 - 1e-4, 0, 0, 1, np.inf],
+                     [0, 0, 0, 1e-5, 0, 0, 1, 5],
+                     [0, 0, 0, 1e-5, 0, 0, 1, 5.0001]], np.float32)
+    h = g.intersect_first_hit(rays)
+    assert list(h["prim"]) == [-1, 0, -1, 0]
+    assert abs(h["t"][1] - 5) < 1e-6
+    assert list(g.intersect_any_hit(rays)) == [False, True, False, True]
+
+
+def test_degenerate_and_large_coordinates(cuda):
+    # compressedWideBvhDifferential.test.ts:289+: degenerate, skinny and large-coordinate geometry
+    base = 1.0e8
+    tris = np.array([
+        [[base, base, base], [base + 64, base, base], [base, base + 64, base]],
+        [[base, base, base + 32], [base + 64, base, base + 32], [base, base + 8, base + 32]],
+        [[base + 16, base + 16, base + 16]] * 3,                       # zero-area
+        [[0, 0, 0], [1e-6, 0, 0], [0, 1e-6, 0]],                        # nanometre
+        [[-5, -5, 1], [5, -5, 1], [5, 5, 1]],
+        [[-5, -5, 1], [5, 5, 1], [-5, 5, 1]],                           # shares the diagonal
+    ], np.float32)
+    pos = np.zeros((tris.shape[0] * 3, 4), np.float32)
+    pos[:, :3] = tris.reshape(-1, 3)
+    idx = np.zeros((tris.shape[0], 4), np.uint32)
+    idx[:, :3] = np.arange(tris.shape[0] * 3).reshape(-1, 3)
+    soup = scenes.TriangleSoup(pos, idx)
+    rng = np.random.default_rng(5)
+    rays = []
+    for _ in range(2000):
+        tgt = tris[rng.integers(0, tris.shape[0])].mean(0).astype(np.float64)
+        tgt += rng.normal(0, 2.0, 3) * (1.0 if abs(tgt[0]) < 1e6 else 20.0)
+        o = tgt + rng.normal(0, 50.0, 3)
+        d = tgt - o
+        rays.append([*o, 1e-4, *(d / np.linalg.norm(d)), np.inf])
+    rays = np.array(rays, np.float32)
+    g, w = _build_both(soup)
+    _assert_parity(soup, rays, g, w, "degenerate")
+    # the shared diagonal: exactly one of the two faces is reported, never a gap
+    diag = np.array([[0, 0, 0, 1e-4, 0, 0, 1, np.inf], [1, 1, 0, 1e-4, 0, 0, 1, np.inf],
+                     [-2, -2, 0, 1e-4, 0, 0, 1, np.inf]], np.float32)
+    h = g.intersect_first_hit(diag)
+    assert set(h["prim"]) <= {4, 5} and (h["prim"] >= 0).all()
+
+
+def test_watertight_kernel_bit_exact(cuda):
+    import torch
+    rng = np.random.default_rng(7)
+    cases = []
+    # the known-answer configurations of opticalWatertightTriangle.test.ts
+    cases.append([0, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, 1, 1, 1, 1, 0])
+    cases.append([0, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, 1, -1, 1, 1, 0])
+    cases.append([2, 2, 0, -1, -1, 0, 1, -1, -1, 1, 1, -1, 1, 1, 1, 0])
+    cases.append([2, 2, 0, -1, -1, 0, -1, 1, -1, 1, 1, 1, 1, 1, -1, 0])
+    cases.append([2, 2, 2, -1, -1, -1, 1, -1, -1, 1, 1, -1, 1, 1, 1, 0])
+    cases.append([2, 0, 0, -1, 1, 0, 1, -1, -1, 1, 1, -1, 1, 1, 1, 0])
+    cases.append([2, 0, 0, -1, 1, 0, -1, 1, -1, 1, 1, 1, 1, 1, -1, 0])
+    for _ in range(20000):
+        o = rng.uniform(-3, 3, 3)
+        tri = rng.uniform(-1, 1, (3, 3))
+        if rng.random() < 0.2:
+            tri = np.round(tri * 4) / 4       # grid-aligned: exact zero edge functions
+            o = np.round(o * 4) / 4
+        d = tri.mean(0) + rng.normal(0, 0.4, 3) - o
+        if rng.random() < 0.1:
+            d = np.round(d * 2) / 2
+        cases.append([*o, *d, *tri.reshape(-1), rng.choice([0.0, 1e-4, 0.5])])
+    cases = np.array(cases, np.float32)
+    dev = torch.from_numpy(cases).cuda()
+    out = torch.zeros((cases.shape[0], 7), dtype=torch.int32, device="cuda")  # vt_watertight_result
+    vb.watertight_eval_device(dev.data_ptr(), cases.shape[0], out.data_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    for i, c in enumerate(cases):
+        ref = oracle.watertight_f32(c[0:3], c[3:6], c[6:9], c[9:12], c[12:15], float(c[15]))
+        assert got[i, 0] == int(ref["hit"]), i
+        if ref["hit"]:
+            gf = got[i, 1:5].view(np.float32)
+            assert gf[0].tobytes() == np.float32(ref["t"]).tobytes(), i
+            assert np.array_equal(gf[1:4], ref["bary"]), i
+            assert got[i, 5] == ref["side"] and got[i, 6] == ref["zero_edge_mask"], i

@@ -1,0 +1,89 @@
+"""ctypes binding of libvitrum_pt.so (the C ABI declared in include/vitrum_pt.h).
+
+The library is required: importing a symbol from here raises if the shared
+object is missing or fails to load.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvitrum_pt.so")
+
+VT_OK = 0
+STATUS_NAMES = {
+    0: "VT_OK", 1: "VT_ERR_INVALID_ARGUMENT", 2: "VT_ERR_RANGE", 3: "VT_ERR_CUDA", 4: "VT_ERR_OUT_OF_MEMORY",
+    5: "VT_ERR_STATE", 6: "VT_ERR_BUILD", 7: "VT_ERR_TIMEOUT",
+}
+
+
+class VtError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class BuildOptions(ctypes.Structure):
+    _fields_ = [("position_stride", ctypes.c_int32), ("index_stride", ctypes.c_int32),
+                ("max_leaf_triangles", ctypes.c_int32), ("bin_count", ctypes.c_int32),
+                ("max_depth", ctypes.c_int32)]
+
+
+class BvhInfo(ctypes.Structure):
+    _fields_ = [("triangle_count", ctypes.c_int64), ("binary_node_count", ctypes.c_int64),
+                ("wide_node_count", ctypes.c_int64), ("wide_depth", ctypes.c_int32),
+                ("binary_depth", ctypes.c_int32), ("build_ms", ctypes.c_double)]
+
+
+class WatertightResult(ctypes.Structure):
+    _fields_ = [("hit", ctypes.c_int32), ("t", ctypes.c_float), ("bary", ctypes.c_float * 3),
+                ("side", ctypes.c_int32), ("zero_edge_mask", ctypes.c_int32)]
+
+
+_lib = None
+
+P = ctypes.c_void_p
+SZ = ctypes.c_size_t
+I32 = ctypes.c_int32
+
+# name -> argtypes; every entry returns vt_status unless listed in _RESTYPE
+SIGNATURES = {
+    "vt_last_error": [],
+    "vt_version": [],
+    "vt_bvh_build": [I32, P, SZ, P, SZ, P, P],
+    "vt_bvh_build_device": [I32, P, SZ, P, SZ, P, P, P],
+    "vt_bvh_get_info": [P, P],
+    "vt_bvh_export_binary": [P, P, SZ, P, SZ],
+    "vt_bvh_trace_closest_device": [P, P, SZ, P, P],
+    "vt_bvh_trace_any_device": [P, P, SZ, P, P],
+    "vt_bvh_trace_closest": [P, P, SZ, P],
+    "vt_bvh_trace_any": [P, P, SZ, P],
+    "vt_bvh_destroy": [P],
+    "vt_watertight_eval_device": [I32, P, SZ, P, P],
+}
+_RESTYPE = {"vt_last_error": ctypes.c_char_p, "vt_version": ctypes.c_char_p}
+
+
+def lib():
+    """Load libvitrum_pt.so (raises OSError when it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing; build it with `python -m vitrum_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, ctypes.c_int32)
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != VT_OK:
+        raise VtError(status, lib().vt_last_error().decode())
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args))

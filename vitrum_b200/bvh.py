@@ -1,0 +1,134 @@
+"""Mesh acceleration structure: the shared-bvh API surface on the B200 path.
+
+Mirrors the reference's shared-bvh entry points (packages/shared-bvh/src):
+
+    buildArrayBvh / buildCompressedWideBvh   -> build_compressed_wide_bvh()
+    intersectCompressedWideBvhFirstHit       -> Bvh.intersect_first_hit()
+    intersectCompressedWideBvhAnyHit         -> Bvh.intersect_any_hit()
+
+Options keep the reference names and defaults (BuildArrayBvhOpts,
+buildArrayBvh.ts:277-318).  Invalid options raise ValueError (RangeError /
+TypeError in the reference).  Everything runs through libvitrum_pt.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+
+_OPTION_KEYS = ("positionStride", "indexStride", "maxLeafTriangles", "binCount", "maxDepth")
+
+
+def _options(opts: dict) -> N.BuildOptions:
+    for k in opts:
+        if k not in _OPTION_KEYS:
+            raise ValueError(f"unknown option {k!r}")
+    return N.BuildOptions(int(opts.get("positionStride", 4)), int(opts.get("indexStride", 4)),
+                          int(opts.get("maxLeafTriangles", 4)), int(opts.get("binCount", 16)),
+                          int(opts.get("maxDepth", 58)))
+
+
+def _ptr(a) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Bvh:
+    """Owning handle of a vt_bvh (device-resident 8-wide BVH)."""
+
+    def __init__(self, handle: ctypes.c_void_p, device: int):
+        self._h = handle
+        self.device = device
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self) -> None:
+        if self._h:
+            N.call("vt_bvh_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise RuntimeError("Bvh is disposed")
+        return self._h
+
+    # ---------------------------------------------------------------- info
+    def info(self) -> dict:
+        i = N.BvhInfo()
+        N.call("vt_bvh_get_info", self.handle, ctypes.byref(i))
+        return {f: getattr(i, f) for f, _ in N.BvhInfo._fields_}
+
+    def export_binary(self):
+        """(nodes (n, 8) uint32 in the reference layout, reordered_to_source uint32)."""
+        inf = self.info()
+        nodes = np.zeros((inf["binary_node_count"], 8), dtype=np.uint32)
+        r2s = np.zeros(max(inf["triangle_count"], 1), dtype=np.uint32)
+        N.call("vt_bvh_export_binary", self.handle, _ptr(nodes), nodes.size, _ptr(r2s), r2s.size)
+        return nodes, r2s[: inf["triangle_count"]]
+
+    # ------------------------------------------------------------- queries
+    def intersect_first_hit(self, rays: np.ndarray) -> np.ndarray:
+        """Closest hit for host rays (n, 8) float32 -> structured (prim, t, u, v)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        out = np.empty(rays.shape[0], dtype=HIT_DTYPE)
+        N.call("vt_bvh_trace_closest", self.handle, _ptr(rays), rays.shape[0], _ptr(out))
+        return out
+
+    def intersect_any_hit(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        out = np.empty(rays.shape[0], dtype=np.uint8)
+        N.call("vt_bvh_trace_any", self.handle, _ptr(rays), rays.shape[0], _ptr(out))
+        return out.astype(bool)
+
+    def trace_closest_device(self, rays_ptr: int, n: int, hits_ptr: int, stream: int = 0) -> None:
+        """Enqueue closest hit on device buffers (32-byte rays, 16-byte hits)."""
+        N.call("vt_bvh_trace_closest_device", self.handle, ctypes.c_void_p(rays_ptr), n,
+               ctypes.c_void_p(hits_ptr), ctypes.c_void_p(stream))
+
+    def trace_any_device(self, rays_ptr: int, n: int, occluded_ptr: int, stream: int = 0) -> None:
+        N.call("vt_bvh_trace_any_device", self.handle, ctypes.c_void_p(rays_ptr), n,
+               ctypes.c_void_p(occluded_ptr), ctypes.c_void_p(stream))
+
+
+HIT_DTYPE = np.dtype([("prim", np.int32), ("t", np.float32), ("u", np.float32), ("v", np.float32)])
+
+
+def build_compressed_wide_bvh(positions, indices, device: int = 0, **opts) -> Bvh:
+    """buildCompressedWideBvh(positions, indices, triMaterialIds, opts) on the GPU path.
+
+    positions: float32 array (stride positionStride), indices: uint32 array
+    (stride indexStride).  Host arrays are copied; the caller keeps them.
+    """
+    o = _options(opts)
+    pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    idx = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+    h = ctypes.c_void_p()
+    N.call("vt_bvh_build", device, _ptr(pos), pos.size, _ptr(idx), idx.size, ctypes.byref(o), ctypes.byref(h))
+    return Bvh(h, device)
+
+
+def build_compressed_wide_bvh_device(positions_ptr: int, position_words: int, indices_ptr: int, index_words: int,
+                                     device: int = 0, stream: int = 0, **opts) -> Bvh:
+    o = _options(opts)
+    h = ctypes.c_void_p()
+    N.call("vt_bvh_build_device", device, ctypes.c_void_p(positions_ptr), position_words,
+           ctypes.c_void_p(indices_ptr), index_words, ctypes.byref(o), ctypes.c_void_p(stream), ctypes.byref(h))
+    return Bvh(h, device)
+
+
+def watertight_eval_device(cases_ptr: int, n: int, out_ptr: int, device: int = 0, stream: int = 0) -> None:
+    N.call("vt_watertight_eval_device", device, ctypes.c_void_p(cases_ptr), n, ctypes.c_void_p(out_ptr),
+           ctypes.c_void_p(stream))

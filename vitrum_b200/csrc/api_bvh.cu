@@ -1,0 +1,247 @@
+// api_bvh.cu -- C-ABI entry points for the mesh acceleration structure.
+//
+// vt_bvh_build*        replaces buildArrayBvh + buildCompressedWideBvh
+//                      (packages/shared-bvh/src/buildArrayBvh.ts:342,
+//                      compressedWideBvh.ts:420)
+// vt_bvh_trace_*       replaces intersectCompressedWideBvhFirstHit / AnyHit
+//                      (compressedWideBvh.ts:754, :862)
+// Errors follow the reference's conventions: invalid options or geometry
+// raise (here: return a status and a message), nothing throws across the ABI.
+#include <chrono>
+#include <memory>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bvh_host.h"
+#include "traverse.h"
+#include "vt_common.h"
+
+struct vt_bvh {
+  int device = 0;
+  vt::BuildOptions opts;
+  vt::BinaryBvhHost binary;              // binary tree in the reference layout (for export)
+  vt::DeviceBuffer<uint4> nodes;         // 8-wide nodes
+  vt::DeviceBuffer<float4> tris;         // triangle records
+  vt::DeviceBuffer<int> status;          // traversal status word
+  int64_t ntri = 0;
+  int64_t wide_count = 0;
+  int wide_depth = 0;
+  double build_ms = 0.0;
+  // staging for the host-buffer entry points
+  vt::DeviceBuffer<float4> rays_scratch;
+  vt::DeviceBuffer<int4> hits_scratch;
+  vt::DeviceBuffer<uint8_t> occ_scratch;
+};
+
+namespace vt {
+
+thread_local std::string t_last_error;
+void set_last_error(const std::string& msg) { t_last_error = msg; }
+void clear_last_error() { t_last_error.clear(); }
+
+static BuildOptions resolve(const vt_bvh_build_options* o) {
+  BuildOptions r;
+  if (!o) return r;
+  if (o->position_stride) r.position_stride = o->position_stride;
+  if (o->index_stride) r.index_stride = o->index_stride;
+  if (o->max_leaf_triangles) r.max_leaf = o->max_leaf_triangles;
+  if (o->bin_count) r.bins = o->bin_count;
+  if (o->max_depth) r.max_depth = o->max_depth;
+  return r;
+}
+
+static void upload(vt_bvh* b, const float* positions, const uint32_t* indices) {
+  WideBvhHost w = encode_wide(b->binary, positions, b->opts.position_stride, indices, b->opts.index_stride);
+  DeviceScope ds(b->device);
+  b->nodes.resize(w.nodes.size() / 4);
+  b->tris.resize(std::max<size_t>(w.tris.size() / 4, 1));
+  VT_CUDA(cudaMemcpy(b->nodes.ptr, w.nodes.data(), w.nodes.size() * 4, cudaMemcpyHostToDevice));
+  if (!w.tris.empty()) VT_CUDA(cudaMemcpy(b->tris.ptr, w.tris.data(), w.tris.size() * 4, cudaMemcpyHostToDevice));
+  b->status.resize(1);
+  VT_CUDA(cudaMemset(b->status.ptr, 0, sizeof(int)));
+  b->wide_count = (int64_t)(w.nodes.size() / 20);
+  b->wide_depth = w.depth;
+}
+
+static vt_bvh* build_host(int device, const float* positions, size_t pw, const uint32_t* indices, size_t iw,
+                          const vt_bvh_build_options* options) {
+  auto t0 = std::chrono::steady_clock::now();
+  auto b = std::make_unique<vt_bvh>();
+  b->device = device;
+  b->opts = resolve(options);
+  b->binary = build_binary_host(positions, pw, indices, iw, b->opts);
+  b->ntri = (int64_t)(iw / b->opts.index_stride);
+  upload(b.get(), positions, indices);
+  b->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return b.release();
+}
+
+static void check_trace_args(vt_bvh* b, const void* rays, size_t n, const void* out) {
+  if (!b) fail(VT_ERR_INVALID_ARGUMENT, "bvh is null");
+  if (n && (!rays || !out)) fail(VT_ERR_INVALID_ARGUMENT, "rays and output must be non-null");
+}
+
+static TraceArgs trace_args(vt_bvh* b, const vt_ray* rays, size_t n) {
+  TraceArgs a;
+  a.nodes = b->nodes.ptr;
+  a.tris = b->tris.ptr;
+  a.rays = reinterpret_cast<const float4*>(rays);
+  a.n = n;
+  a.status = b->status.ptr;
+  a.stack_depth = b->wide_depth + 1;
+  return a;
+}
+
+static void check_status(vt_bvh* b) {
+  int st = 0;
+  VT_CUDA(cudaMemcpy(&st, b->status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) {
+    cudaMemset(b->status.ptr, 0, sizeof(int));
+    fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+  }
+}
+
+}  // namespace vt
+
+using namespace vt;
+
+extern "C" {
+
+const char* vt_last_error(void) { return t_last_error.c_str(); }
+const char* vt_version(void) { return "vitrum_b200 0.1 (sm_100a)"; }
+
+vt_status vt_bvh_build(int32_t device, const float* positions, size_t position_words, const uint32_t* indices,
+                       size_t index_words, const vt_bvh_build_options* options, vt_bvh** out_bvh) {
+  return guard([&] {
+    if (!out_bvh) fail(VT_ERR_INVALID_ARGUMENT, "out_bvh is null");
+    *out_bvh = nullptr;
+    if (position_words && !positions) fail(VT_ERR_INVALID_ARGUMENT, "positions is null");
+    if (index_words && !indices) fail(VT_ERR_INVALID_ARGUMENT, "indices is null");
+    *out_bvh = build_host(device, positions, position_words, indices, index_words, options);
+  });
+}
+
+vt_status vt_bvh_build_device(int32_t device, const float* d_positions, size_t position_words,
+                              const uint32_t* d_indices, size_t index_words, const vt_bvh_build_options* options,
+                              void* cuda_stream, vt_bvh** out_bvh) {
+  return guard([&] {
+    if (!out_bvh) fail(VT_ERR_INVALID_ARGUMENT, "out_bvh is null");
+    *out_bvh = nullptr;
+    DeviceScope ds(device);
+    std::vector<float> p(position_words);
+    std::vector<uint32_t> i(index_words);
+    cudaStream_t s = (cudaStream_t)cuda_stream;
+    if (position_words)
+      VT_CUDA(cudaMemcpyAsync(p.data(), d_positions, position_words * 4, cudaMemcpyDeviceToHost, s));
+    if (index_words) VT_CUDA(cudaMemcpyAsync(i.data(), d_indices, index_words * 4, cudaMemcpyDeviceToHost, s));
+    VT_CUDA(cudaStreamSynchronize(s));
+    *out_bvh = build_host(device, p.data(), position_words, i.data(), index_words, options);
+  });
+}
+
+vt_status vt_bvh_get_info(const vt_bvh* b, vt_bvh_info* info) {
+  return guard([&] {
+    if (!b || !info) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    info->triangle_count = b->ntri;
+    info->binary_node_count = (int64_t)b->binary.nodes.size();
+    info->wide_node_count = b->wide_count;
+    info->wide_depth = b->wide_depth;
+    info->binary_depth = b->binary.depth;
+    info->build_ms = b->build_ms;
+  });
+}
+
+vt_status vt_bvh_export_binary(const vt_bvh* b, uint32_t* nodes, size_t node_word_capacity,
+                               uint32_t* reordered_to_source, size_t triangle_capacity) {
+  return guard([&] {
+    if (!b) fail(VT_ERR_INVALID_ARGUMENT, "bvh is null");
+    if (nodes) {
+      if (node_word_capacity < b->binary.nodes.size() * 8) fail(VT_ERR_RANGE, "node buffer too small");
+      std::memcpy(nodes, b->binary.nodes.data(), b->binary.nodes.size() * 32);
+    }
+    if (reordered_to_source) {
+      if (triangle_capacity < b->binary.reordered_to_source.size()) fail(VT_ERR_RANGE, "triangle buffer too small");
+      std::memcpy(reordered_to_source, b->binary.reordered_to_source.data(),
+                  b->binary.reordered_to_source.size() * 4);
+    }
+  });
+}
+
+vt_status vt_bvh_trace_closest_device(vt_bvh* b, const vt_ray* d_rays, size_t n, vt_hit* d_hits,
+                                      void* cuda_stream) {
+  return guard([&] {
+    check_trace_args(b, d_rays, n, d_hits);
+    DeviceScope ds(b->device);
+    TraceArgs a = trace_args(b, d_rays, n);
+    a.hits = reinterpret_cast<int4*>(d_hits);
+    launch_trace_closest(a, (cudaStream_t)cuda_stream);
+    VT_CUDA(cudaGetLastError());
+  });
+}
+
+vt_status vt_bvh_trace_any_device(vt_bvh* b, const vt_ray* d_rays, size_t n, uint8_t* d_occluded,
+                                  void* cuda_stream) {
+  return guard([&] {
+    check_trace_args(b, d_rays, n, d_occluded);
+    DeviceScope ds(b->device);
+    TraceArgs a = trace_args(b, d_rays, n);
+    a.occluded = d_occluded;
+    launch_trace_any(a, (cudaStream_t)cuda_stream);
+    VT_CUDA(cudaGetLastError());
+  });
+}
+
+vt_status vt_bvh_trace_closest(vt_bvh* b, const vt_ray* rays, size_t n, vt_hit* hits) {
+  return guard([&] {
+    check_trace_args(b, rays, n, hits);
+    if (!n) return;
+    DeviceScope ds(b->device);
+    b->rays_scratch.resize(2 * n);
+    b->hits_scratch.resize(n);
+    VT_CUDA(cudaMemcpy(b->rays_scratch.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice));
+    TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr), n);
+    a.hits = b->hits_scratch.ptr;
+    launch_trace_closest(a, 0);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaMemcpy(hits, b->hits_scratch.ptr, n * sizeof(vt_hit), cudaMemcpyDeviceToHost));
+    check_status(b);
+  });
+}
+
+vt_status vt_bvh_trace_any(vt_bvh* b, const vt_ray* rays, size_t n, uint8_t* occluded) {
+  return guard([&] {
+    check_trace_args(b, rays, n, occluded);
+    if (!n) return;
+    DeviceScope ds(b->device);
+    b->rays_scratch.resize(2 * n);
+    b->occ_scratch.resize(n);
+    VT_CUDA(cudaMemcpy(b->rays_scratch.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice));
+    TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr), n);
+    a.occluded = b->occ_scratch.ptr;
+    launch_trace_any(a, 0);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaMemcpy(occluded, b->occ_scratch.ptr, n, cudaMemcpyDeviceToHost));
+    check_status(b);
+  });
+}
+
+vt_status vt_bvh_destroy(vt_bvh* b) {
+  return guard([&] {
+    if (!b) return;
+    DeviceScope ds(b->device);
+    delete b;
+  });
+}
+
+vt_status vt_watertight_eval_device(int32_t device, const float* d_cases, size_t n, vt_watertight_result* d_out,
+                                    void* cuda_stream) {
+  return guard([&] {
+    if (n && (!d_cases || !d_out)) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceScope ds(device);
+    launch_watertight_eval(d_cases, n, d_out, (cudaStream_t)cuda_stream);
+    VT_CUDA(cudaGetLastError());
+  });
+}
+
+}  // extern "C"

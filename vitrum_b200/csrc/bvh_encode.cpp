@@ -1,0 +1,191 @@
+// bvh_encode.cpp -- 8-wide collapse and compressed-node encoding.
+//
+// Collapse: the reference's greedy rule (collectWideChildren,
+// packages/shared-bvh/src/compressedWideBvh.ts:215-242): starting from the
+// two children of a binary interior node, repeatedly replace the interior
+// child of largest surface area by its two children until 8 slots are used
+// or only leaves remain.  The resulting wide topology is the reference's.
+//
+// Encoding (ours, for the GPU): breadth-first node numbering so the hottest
+// nodes form a prefix, slot assignment for octant-ordered traversal, u8
+// child bounds on a power-of-two grid anchored at the parent minimum, and
+// each wide node's leaf triangles gathered contiguously as 48-byte records.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bvh_host.h"
+
+namespace vt {
+
+static double half_area(const BinaryNode& n) {
+  double dx = std::max(0.0, (double)n.mx[0] - n.mn[0]);
+  double dy = std::max(0.0, (double)n.mx[1] - n.mn[1]);
+  double dz = std::max(0.0, (double)n.mx[2] - n.mn[2]);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+int collect_wide_children(const BinaryNode* nodes, uint32_t root, uint32_t out[8]) {
+  const BinaryNode& r = nodes[root];
+  if (is_leaf_word(r.w7)) { out[0] = root; return 1; }
+  int n = 2;
+  out[0] = root + 1;
+  out[1] = root + r.w6;
+  while (n < 8) {
+    int at = -1;
+    double best = -1;
+    for (int i = 0; i < n; ++i) {
+      const BinaryNode& c = nodes[out[i]];
+      if (is_leaf_word(c.w7)) continue;
+      double a = half_area(c);
+      if (a > best) { best = a; at = i; }
+    }
+    if (at < 0) break;
+    uint32_t x = out[at];
+    std::memmove(out + at + 2, out + at + 1, sizeof(uint32_t) * (n - at - 1));
+    out[at] = x + 1;
+    out[at + 1] = x + nodes[x].w6;
+    ++n;
+  }
+  return n;
+}
+
+// Greedy slot assignment: slot s is visited first by rays whose direction
+// sign bits (x:4, y:2, z:1; bit set = negative) equal s, so it should hold
+// the child lying furthest against that direction.
+void assign_slots(const BinaryNode* nodes, const BinaryNode& parent, const uint32_t* ch, int n, int slot_of[8]) {
+  double pc[3];
+  for (int k = 0; k < 3; ++k) pc[k] = 0.5 * ((double)parent.mn[k] + parent.mx[k]);
+  double cost[8][8];
+  for (int i = 0; i < n; ++i) {
+    const BinaryNode& c = nodes[ch[i]];
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = 0.5 * ((double)c.mn[k] + c.mx[k]) - pc[k];
+    for (int s = 0; s < 8; ++s) {
+      double sx = (s & 4) ? -1.0 : 1.0, sy = (s & 2) ? -1.0 : 1.0, sz = (s & 1) ? -1.0 : 1.0;
+      cost[i][s] = d[0] * sx + d[1] * sy + d[2] * sz;
+    }
+  }
+  bool used_c[8] = {}, used_s[8] = {};
+  for (int i = 0; i < 8; ++i) slot_of[i] = -1;
+  for (int round = 0; round < n; ++round) {
+    int bi = -1, bs = -1;
+    double bc = INFINITY;
+    for (int i = 0; i < n; ++i) {
+      if (used_c[i]) continue;
+      for (int s = 0; s < 8; ++s) {
+        if (used_s[s]) continue;
+        if (bi < 0 || cost[i][s] < bc) { bc = cost[i][s]; bi = i; bs = s; }
+      }
+    }
+    used_c[bi] = true;
+    used_s[bs] = true;
+    slot_of[bi] = bs;
+  }
+}
+
+// Smallest e with 255 * 2^e >= extent (extent > 0), clamped to the normal range.
+static int grid_exponent(double extent) {
+  if (!(extent > 0)) return -126;
+  int e;
+  std::frexp(extent / 255.0, &e);  // extent/255 = m * 2^e, m in [0.5, 1)
+  while (e > -126 && std::ldexp(255.0, e - 1) >= extent) --e;
+  while (std::ldexp(255.0, e) < extent) ++e;
+  return std::min(127, std::max(-126, e));
+}
+
+WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
+                        int idx_stride) {
+  WideBvhHost out;
+  const BinaryNode* nodes = bin.nodes.data();
+  const size_t ntri = bin.reordered_to_source.size();
+  std::vector<uint32_t> wide_bin;   // binary node behind each wide node (BFS order)
+  std::vector<int> level;
+  wide_bin.push_back(0);
+  level.push_back(1);
+  out.depth = 1;
+  if (ntri == 0) {
+    uint32_t w[20] = {};
+    // All-empty slots: inverted boxes (qlo 255, qhi 0), no children.
+    std::memset(reinterpret_cast<uint8_t*>(w) + 32, 0xFF, 24);
+    out.nodes.assign(w, w + 20);
+    return out;
+  }
+  out.tris.reserve(ntri * 12);
+  for (size_t wi = 0; wi < wide_bin.size(); ++wi) {
+    const BinaryNode& parent = nodes[wide_bin[wi]];
+    uint32_t ch[8];
+    int n = collect_wide_children(nodes, wide_bin[wi], ch);
+    int slot_of[8];
+    assign_slots(nodes, parent, ch, n, slot_of);
+    int child_at_slot[8];
+    for (int s = 0; s < 8; ++s) child_at_slot[s] = -1;
+    for (int i = 0; i < n; ++i) child_at_slot[slot_of[i]] = i;
+
+    uint8_t bytes[80];
+    std::memset(bytes, 0, sizeof bytes);
+    float p[3] = {parent.mn[0], parent.mn[1], parent.mn[2]};
+    std::memcpy(bytes, p, 12);
+    int ex[3];
+    for (int k = 0; k < 3; ++k) {
+      ex[k] = grid_exponent((double)parent.mx[k] - (double)parent.mn[k]);
+      bytes[12 + k] = (uint8_t)(ex[k] + 127);
+    }
+    uint8_t imask = 0;
+    uint32_t child_base = (uint32_t)wide_bin.size();
+    uint32_t tri_base = (uint32_t)(out.tris.size() / 12);
+    uint32_t tri_off = 0;
+    for (int s = 0; s < 8; ++s) {
+      uint8_t* qlo = bytes + 32;  // qlo_x at +0, qlo_y at +8, qlo_z at +16
+      uint8_t* qhi = bytes + 56;  // qhi_x at +0, qhi_y at +8, qhi_z at +16
+      int ci = child_at_slot[s];
+      if (ci < 0) {
+        for (int k = 0; k < 3; ++k) { qlo[k * 8 + s] = 255; qhi[k * 8 + s] = 0; }
+        continue;
+      }
+      const BinaryNode& c = nodes[ch[ci]];
+      for (int k = 0; k < 3; ++k) {
+        double step = std::ldexp(1.0, ex[k]);
+        double lo = std::floor(((double)c.mn[k] - (double)p[k]) / step);
+        double hi = std::ceil(((double)c.mx[k] - (double)p[k]) / step);
+        lo = std::min(255.0, std::max(0.0, lo));
+        hi = std::min(255.0, std::max(0.0, hi));
+        qlo[k * 8 + s] = (uint8_t)lo;
+        qhi[k * 8 + s] = (uint8_t)hi;
+      }
+      if (is_leaf_word(c.w7)) {
+        uint32_t cnt = c.w7 & 0xFFFFu, first = c.w6;
+        bytes[24 + s] = (uint8_t)((cnt << 5) | tri_off);
+        for (uint32_t t = 0; t < cnt; ++t) {
+          uint32_t src = bin.reordered_to_source[first + t];
+          const uint32_t* iv = indices + (size_t)src * idx_stride;
+          for (int v = 0; v < 3; ++v) {
+            const float* q = positions + (size_t)iv[v] * pos_stride;
+            out.tris.push_back(q[0]);
+            out.tris.push_back(q[1]);
+            out.tris.push_back(q[2]);
+            uint32_t w = v == 0 ? src : 0u;
+            float wf;
+            std::memcpy(&wf, &w, 4);
+            out.tris.push_back(wf);
+          }
+        }
+        tri_off += cnt;
+      } else {
+        imask |= (uint8_t)(1u << s);
+        wide_bin.push_back(ch[ci]);
+        level.push_back(level[wi] + 1);
+        out.depth = std::max(out.depth, level[wi] + 1);
+      }
+    }
+    bytes[15] = imask;
+    std::memcpy(bytes + 16, &child_base, 4);
+    std::memcpy(bytes + 20, &tri_base, 4);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(bytes);
+    out.nodes.insert(out.nodes.end(), w, w + 20);
+  }
+  return out;
+}
+
+}  // namespace vt

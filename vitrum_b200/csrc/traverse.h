@@ -1,0 +1,28 @@
+// traverse.h -- launchers of the traversal kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/vitrum_pt.h"
+
+namespace vt {
+
+struct TraceArgs {
+  const uint4* nodes = nullptr;   // 8-wide nodes, 5 uint4 each
+  const float4* tris = nullptr;   // 3 float4 per triangle
+  const float4* rays = nullptr;   // 2 float4 per ray (vt_ray)
+  size_t n = 0;
+  int4* hits = nullptr;           // vt_hit per ray (closest)
+  uint8_t* occluded = nullptr;    // 1 byte per ray (any)
+  int* status = nullptr;          // device word, bit 0 = stack capacity exceeded
+  int stack_depth = 64;           // wide-tree depth bound
+};
+
+void launch_trace_closest(const TraceArgs& a, cudaStream_t s);
+void launch_trace_any(const TraceArgs& a, cudaStream_t s);
+void launch_watertight_eval(const float* cases, size_t n, vt_watertight_result* out, cudaStream_t s);
+
+}  // namespace vt
