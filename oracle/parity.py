@@ -107,3 +107,28 @@ def classify(positions, indices, rays, gpu, ref, tie_rel=TIE_REL, edge_eps=EDGE_
 def triangle_check(o, d, a, b, c, tmin=0.0):
     """FP64 reference test of one ray/triangle pair (compressedWideBvh.ts:551)."""
     return triangle_fp64(o, d, a, b, c, tmin)
+
+
+def watertight_disagreements(positions, indices, rays, gpu_prim, wt_prim):
+    """Rays where the device and the f32 watertight oracle chose different
+    triangles, split into exact f32 t ties (either order is correct) and
+    real disagreements.  Returns (ties, errors) as lists of ray indices."""
+    from . import watertight_f32
+    pos = np.asarray(positions, np.float32).reshape(-1, 4)
+    idx = np.asarray(indices, np.uint32).reshape(-1, 4)
+    rays = np.asarray(rays, np.float32).reshape(-1, 8)
+    ties, errors = [], []
+    for i in np.nonzero(gpu_prim != wt_prim)[0]:
+        r = rays[i]
+        res = []
+        for p in (int(gpu_prim[i]), int(wt_prim[i])):
+            if p < 0:
+                res.append(None)
+                continue
+            res.append(watertight_f32(r[0:3], r[4:7], *_tri(pos, idx, p), float(r[3])))
+        if all(x is not None and x["hit"] for x in res) and \
+                np.float32(res[0]["t"]).tobytes() == np.float32(res[1]["t"]).tobytes():
+            ties.append(int(i))
+        else:
+            errors.append(int(i))
+    return ties, errors

@@ -32,12 +32,9 @@ def _build_both(soup, **opts):
 def _assert_parity(soup, rays, g, w, label):
     hits = g.intersect_first_hit(rays)
     wp, wt, _ = oracle.first_hit_watertight(w, soup.positions, rays)
-    # device decisions == watertight oracle decisions (f32 exact ties excepted)
-    diff = np.nonzero(hits["prim"] != wp)[0]
-    if diff.size:
-        r = parity.classify(soup.positions, soup.indices, rays[diff], hits[diff],
-                            tuple(x[diff] for x in oracle.first_hit(w, soup.positions, rays[diff])[:3]))
-        assert r["error"] == 0 and r["edge"] == 0, (label, "watertight mismatch", r)
+    # device decisions == watertight oracle decisions (exact f32 t ties excepted)
+    ties, errors = parity.watertight_disagreements(soup.positions, soup.indices, rays, hits["prim"], wp)
+    assert not errors, (label, "watertight mismatch on rays", errors[:10], "ties", len(ties))
     ref = oracle.first_hit(w, soup.positions, rays)
     rep = parity.classify(soup.positions, soup.indices, rays, hits, ref[:3])
     assert rep["error"] == 0, (label, rep)

@@ -17,7 +17,10 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libvitrum_pt.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# host code: no FMA contraction (the BVH encoder restates single-precision
+# reference arithmetic that must round every operation)
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+         "-Xcompiler", "-ffp-contract=off",
          "-I" + os.path.join(HERE, "..", "include")]
 
 

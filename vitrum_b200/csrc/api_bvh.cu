@@ -24,6 +24,7 @@ struct vt_bvh {
   vt::DeviceBuffer<uint4> nodes;         // 8-wide nodes
   vt::DeviceBuffer<float4> tris;         // triangle records
   vt::DeviceBuffer<int> status;          // traversal status word
+  vt::DeviceBuffer<unsigned long long> counter;  // persistent-kernel ray counter (calls on one bvh are serialised)
   int64_t ntri = 0;
   int64_t wide_count = 0;
   int wide_depth = 0;
@@ -60,6 +61,7 @@ static void upload(vt_bvh* b, const float* positions, const uint32_t* indices) {
   if (!w.tris.empty()) VT_CUDA(cudaMemcpy(b->tris.ptr, w.tris.data(), w.tris.size() * 4, cudaMemcpyHostToDevice));
   b->status.resize(1);
   VT_CUDA(cudaMemset(b->status.ptr, 0, sizeof(int)));
+  b->counter.resize(1);
   b->wide_count = (int64_t)(w.nodes.size() / 20);
   b->wide_depth = w.depth;
 }
@@ -80,6 +82,7 @@ static vt_bvh* build_host(int device, const float* positions, size_t pw, const u
 static void check_trace_args(vt_bvh* b, const void* rays, size_t n, const void* out) {
   if (!b) fail(VT_ERR_INVALID_ARGUMENT, "bvh is null");
   if (n && (!rays || !out)) fail(VT_ERR_INVALID_ARGUMENT, "rays and output must be non-null");
+  if (n > 0xFFFFFFFFull) fail(VT_ERR_RANGE, "at most 2^32 - 1 rays per call");
 }
 
 static TraceArgs trace_args(vt_bvh* b, const vt_ray* rays, size_t n) {
@@ -89,7 +92,8 @@ static TraceArgs trace_args(vt_bvh* b, const vt_ray* rays, size_t n) {
   a.rays = reinterpret_cast<const float4*>(rays);
   a.n = n;
   a.status = b->status.ptr;
-  a.stack_depth = b->wide_depth + 1;
+  a.stack_depth = 2 * b->wide_depth + 2;  // one node group and one postponed triangle group per level
+  a.counter = b->counter.ptr;
   return a;
 }
 

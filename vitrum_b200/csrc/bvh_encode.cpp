@@ -9,10 +9,12 @@
 // Encoding (ours, for the GPU): breadth-first node numbering so the hottest
 // nodes form a prefix, slot assignment for octant-ordered traversal, u8
 // child bounds on a power-of-two grid anchored at the parent minimum, and
-// each wide node's leaf triangles gathered contiguously as 48-byte records.
+// each wide node's leaf triangles gathered as 64-byte records (vertices,
+// source id, precomputed reference normal) in per-slot blocks of four.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <stdexcept>
 #include <vector>
 
 #include "bvh_host.h"
@@ -85,6 +87,30 @@ void assign_slots(const BinaryNode* nodes, const BinaryNode& parent, const uint3
   }
 }
 
+// Unit normal exactly as the reference's watertight test derives it from the
+// triangle (opticalWatertightTriangle.ts:164-201): every operation single
+// precision, individually rounded (this file is compiled without FMA
+// contraction).  Returns false when that derivation rejects the triangle.
+static bool reference_normal(const float a[3], const float b[3], const float c[3], float nn[3]) {
+  float e1r[3], e2r[3];
+  for (int k = 0; k < 3; ++k) { e1r[k] = b[k] - a[k]; e2r[k] = c[k] - a[k]; }
+  float es = 0.0f;
+  for (int k = 0; k < 3; ++k) es = std::max(es, std::fabs(e1r[k]));
+  for (int k = 0; k < 3; ++k) es = std::max(es, std::fabs(e2r[k]));
+  if (!(es > 0.0f) || !std::isfinite(es)) return false;
+  float s1[3], s2[3];
+  for (int k = 0; k < 3; ++k) { s1[k] = e1r[k] / es; s2[k] = e2r[k] / es; }
+  float nr[3] = {s1[1] * s2[2] - s1[2] * s2[1], s1[2] * s2[0] - s1[0] * s2[2], s1[0] * s2[1] - s1[1] * s2[0]};
+  float ns = std::max(std::max(std::fabs(nr[0]), std::fabs(nr[1])), std::fabs(nr[2]));
+  if (!(ns > 0.0f) || !std::isfinite(ns)) return false;
+  float nd[3] = {nr[0] / ns, nr[1] / ns, nr[2] / ns};
+  float l2 = (nd[0] * nd[0] + nd[1] * nd[1]) + nd[2] * nd[2];
+  float nl = std::sqrt(l2);
+  if (!(nl > 0.0f) || !std::isfinite(nl)) return false;
+  for (int k = 0; k < 3; ++k) nn[k] = nd[k] / nl;
+  return true;
+}
+
 // Smallest e with 255 * 2^e >= extent (extent > 0), clamped to the normal range.
 static int grid_exponent(double extent) {
   if (!(extent > 0)) return -126;
@@ -112,7 +138,11 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
     out.nodes.assign(w, w + 20);
     return out;
   }
-  out.tris.reserve(ntri * 12);
+  out.tris.reserve(ntri * 24);
+  // 28 leading empty records: tri_base = block - 4 * first_leaf_slot then
+  // never wraps, and stays below 2^31 (bit 31 tags node groups on the
+  // traversal stack).
+  out.tris.assign(16 * 28, 0.0f);
   for (size_t wi = 0; wi < wide_bin.size(); ++wi) {
     const BinaryNode& parent = nodes[wide_bin[wi]];
     uint32_t ch[8];
@@ -134,8 +164,17 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
     }
     uint8_t imask = 0;
     uint32_t child_base = (uint32_t)wide_bin.size();
-    uint32_t tri_base = (uint32_t)(out.tris.size() / 12);
-    uint32_t tri_off = 0;
+    // leaf slot s uses records [block + 4*(s - first_leaf_slot), +count)
+    int first_leaf = 8, last_leaf = -1;
+    for (int s = 0; s < 8; ++s) {
+      int ci = child_at_slot[s];
+      if (ci >= 0 && is_leaf_word(nodes[ch[ci]].w7)) { first_leaf = std::min(first_leaf, s); last_leaf = s; }
+    }
+    const uint32_t block = (uint32_t)(out.tris.size() / 16);
+    const uint32_t tri_base = block - 4u * (uint32_t)(first_leaf < 8 ? first_leaf : 0);
+    if (block < 28 || tri_base >= 0x80000000u) throw std::length_error("triangle records exceed 2^31");
+    if (last_leaf >= 0) out.tris.resize(out.tris.size() + 16 * (size_t)(4 * (last_leaf - first_leaf) + 4), 0.0f);
+    uint32_t tri_valid = 0;
     for (int s = 0; s < 8; ++s) {
       uint8_t* qlo = bytes + 32;  // qlo_x at +0, qlo_y at +8, qlo_z at +16
       uint8_t* qhi = bytes + 56;  // qhi_x at +0, qhi_y at +8, qhi_z at +16
@@ -156,22 +195,22 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
       }
       if (is_leaf_word(c.w7)) {
         uint32_t cnt = c.w7 & 0xFFFFu, first = c.w6;
-        bytes[24 + s] = (uint8_t)((cnt << 5) | tri_off);
+        tri_valid |= ((1u << cnt) - 1u) << (4 * s);
         for (uint32_t t = 0; t < cnt; ++t) {
           uint32_t src = bin.reordered_to_source[first + t];
           const uint32_t* iv = indices + (size_t)src * idx_stride;
-          for (int v = 0; v < 3; ++v) {
-            const float* q = positions + (size_t)iv[v] * pos_stride;
-            out.tris.push_back(q[0]);
-            out.tris.push_back(q[1]);
-            out.tris.push_back(q[2]);
-            uint32_t w = v == 0 ? src : 0u;
-            float wf;
-            std::memcpy(&wf, &w, 4);
-            out.tris.push_back(wf);
-          }
+          float* rec = &out.tris[16 * ((size_t)block + 4 * (s - first_leaf) + t)];
+          float v[3][3];
+          for (int vi = 0; vi < 3; ++vi)
+            for (int k = 0; k < 3; ++k) v[vi][k] = positions[(size_t)iv[vi] * pos_stride + k];
+          for (int vi = 0; vi < 3; ++vi)
+            for (int k = 0; k < 3; ++k) rec[4 * vi + k] = v[vi][k];
+          std::memcpy(&rec[3], &src, 4);
+          float nn[3] = {0, 0, 0};
+          bool valid = reference_normal(v[0], v[1], v[2], nn);
+          rec[12] = nn[0]; rec[13] = nn[1]; rec[14] = nn[2];
+          rec[15] = valid ? 1.0f : 0.0f;
         }
-        tri_off += cnt;
       } else {
         imask |= (uint8_t)(1u << s);
         wide_bin.push_back(ch[ci]);
@@ -179,6 +218,7 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
         out.depth = std::max(out.depth, level[wi] + 1);
       }
     }
+    std::memcpy(bytes + 24, &tri_valid, 4);
     bytes[15] = imask;
     std::memcpy(bytes + 16, &child_base, 4);
     std::memcpy(bytes + 20, &tri_base, 4);

@@ -25,7 +25,7 @@ struct BinaryBvhHost {
 
 struct WideBvhHost {
   std::vector<uint32_t> nodes;  // 20 words per wide node
-  std::vector<float> tris;      // 12 floats per triangle
+  std::vector<float> tris;      // 16 floats per triangle record slot
   int depth = 0;
 };
 

@@ -16,6 +16,7 @@
 // outward quantisation this never culls a box the exact ray touches.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "bvh_types.h"
@@ -49,46 +50,108 @@ __device__ __forceinline__ Slab make_slab(float p, float e_bits, float inv, floa
   return r;
 }
 
+// Per-lane ray state of the persistent kernel.
+struct LaneRay {
+  float ox, oy, oz, tmin, dx, dy, dz, closest;
+  float ix, iy, iz;
+  uint32_t oct;
+  int best;  // triangle record index of the closest hit so far
+};
+
+// Reorders an 8-bit slot mask into key order: bit s moves to bit s ^ oct.
+__device__ __forceinline__ uint32_t xor_permute8(uint32_t m, uint32_t oct) {
+  if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+  if (oct & 2u) m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+  if (oct & 4u) m = ((m & 0x0Fu) << 4) | ((m >> 4) & 0x0Fu);
+  return m;
+}
+
+// Spreads bit s of an 8-bit mask to nibble s (0xF) of a 32-bit word.
+__device__ __forceinline__ uint32_t nibble_spread8(uint32_t m) {
+  m = (m | (m << 12)) & 0x000F000Fu;
+  m = (m | (m << 6)) & 0x03030303u;
+  m = (m | (m << 3)) & 0x11111111u;
+  return m * 15u;
+}
+
 template <bool ANY, int STK>
-__global__ void __launch_bounds__(kBlock) k_trace(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
+__global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                                   const float4* __restrict__ rays, size_t n,
                                                   int4* __restrict__ hits, uint8_t* __restrict__ occluded,
-                                                  int* __restrict__ status) {
+                                                  int* __restrict__ status,
+                                                  unsigned long long* __restrict__ ray_counter) {
+  // Persistent warps, one ray per lane.  Every iteration each live lane
+  // (1) expands at most one wide node, (2) runs at most two watertight
+  // triangle tests from a two-entry queue of triangle groups, and (3) picks
+  // its next node without waiting for its queued triangles.  Node work and
+  // triangle work therefore proceed in lock-step phases with most lanes
+  // busy in each, and a lane whose ray finished takes the next unclaimed
+  // ray from its warp's pool (one atomicAdd per 64 rays).
   extern __shared__ uint2 stack_mem[];  // [STK][kBlock], one column per thread
   uint2* const stack = stack_mem + threadIdx.x;
-  const size_t ray = (size_t)blockIdx.x * kBlock + threadIdx.x;
-  if (ray >= n) return;
-  const float4 r0 = __ldg(rays + 2 * ray);
-  const float4 r1 = __ldg(rays + 2 * ray + 1);
-  const float tmin = r0.w;
-  float closest = r1.w;
-  const WtRay wr = wt_setup(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+  const uint32_t lane = threadIdx.x & 31u;
+  constexpr uint32_t kFull = 0xFFFFFFFFu;
+  constexpr uint32_t kNodeGroup = 0x80000000u;  // stack x-bit: entry is a node group (else triangle group)
+  constexpr uint32_t kChunk = 64;
 
-  auto safe = [](float d) { return fabsf(d) > 1e-30f ? d : copysignf(1e-30f, d); };
-  const float ix = __frcp_rn(safe(r1.x)), iy = __frcp_rn(safe(r1.y)), iz = __frcp_rn(safe(r1.z));
-  const bool nx = ix < 0.0f, ny = iy < 0.0f, nz = iz < 0.0f;
-  const uint32_t oct = (nx ? 4u : 0u) | (ny ? 2u : 0u) | (nz ? 1u : 0u);
-
-  int best = -1;
-  float best_t = closest, best_u = 0.0f, best_v = 0.0f;
-  bool done = false;
-
-  // current internal-node group: base index, key-ordered hit bits (0..7), imask
-  uint32_t gbase = 0, ghits = 0, gimask = 0;
-  uint32_t tbase = 0, thits = 0;
+  bool live = false, exhausted = false;
+  uint32_t ray = 0, pool_next = 0, pool_end = 0;
+  const uint32_t n32 = (uint32_t)n;
+  LaneRay R;
+  WtRay wr;
+  uint32_t gbase = 0, ghits = 0, gimask = 0, node = 0;
+  uint32_t q0b = 0, q0m = 0, q1b = 0, q1m = 0;  // triangle-group queue (base, hit mask)
+  bool expand = false;
   int sp = 0;
-  uint32_t node = 0;
 
   while (true) {
-    // ---- expand `node`
-    {
+    // ---- refill idle lanes from the warp's ray pool
+    const uint32_t idle = __ballot_sync(kFull, !live);
+    if (idle) {
+      if (pool_next >= pool_end && !exhausted) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(ray_counter, (unsigned long long)kChunk);
+        base = __shfl_sync(kFull, base, 0);
+        pool_next = (uint32_t)(base < n32 ? base : n32);
+        pool_end = base + kChunk < n32 ? (uint32_t)(base + kChunk) : n32;
+        exhausted = base + kChunk >= n32;
+      }
+      const uint32_t avail = pool_end > pool_next ? pool_end - pool_next : 0u;
+      const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+      if (!live && rank < avail) {
+        ray = pool_next + rank;
+        const float4 r0 = __ldg(rays + 2 * (size_t)ray), r1 = __ldg(rays + 2 * (size_t)ray + 1);
+        R.ox = r0.x; R.oy = r0.y; R.oz = r0.z; R.tmin = r0.w;
+        R.dx = r1.x; R.dy = r1.y; R.dz = r1.z; R.closest = r1.w;
+        auto safe = [](float d) { return fabsf(d) > 1e-30f ? d : copysignf(1e-30f, d); };
+        R.ix = __frcp_rn(safe(R.dx)); R.iy = __frcp_rn(safe(R.dy)); R.iz = __frcp_rn(safe(R.dz));
+        R.oct = (R.ix < 0.0f ? 4u : 0u) | (R.iy < 0.0f ? 2u : 0u) | (R.iz < 0.0f ? 1u : 0u);
+        R.best = -1;
+        wr = wt_setup(R.ox, R.oy, R.oz, R.dx, R.dy, R.dz);
+        gbase = ghits = gimask = 0;
+        q0m = q1m = 0;
+        node = 0;
+        expand = true;
+        sp = 0;
+        live = true;
+      }
+      const uint32_t cnt = (uint32_t)__popc(idle);
+      pool_next += avail < cnt ? avail : cnt;
+      if (exhausted && pool_next >= pool_end && __ballot_sync(kFull, live) == 0) break;
+    }
+    if (!live) continue;
+
+    // ---- (1) expand one node
+    if (expand) {
+      expand = false;
       const uint4* np = nodes + (size_t)node * 5;
       const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
       const uint32_t e = w0.w;
-      const Slab sx = make_slab(__uint_as_float(w0.x), __uint_as_float((e & 0xFFu) << 23), ix, r0.x);
-      const Slab sy = make_slab(__uint_as_float(w0.y), __uint_as_float(((e >> 8) & 0xFFu) << 23), iy, r0.y);
-      const Slab sz = make_slab(__uint_as_float(w0.z), __uint_as_float(((e >> 16) & 0xFFu) << 23), iz, r0.z);
+      const Slab sx = make_slab(__uint_as_float(w0.x), __uint_as_float((e & 0xFFu) << 23), R.ix, R.ox);
+      const Slab sy = make_slab(__uint_as_float(w0.y), __uint_as_float(((e >> 8) & 0xFFu) << 23), R.iy, R.oy);
+      const Slab sz = make_slab(__uint_as_float(w0.z), __uint_as_float(((e >> 16) & 0xFFu) << 23), R.iz, R.oz);
       const uint32_t imask = e >> 24;
+      const bool nx = R.oct & 4u, ny = R.oct & 2u, nz = R.oct & 1u;
       // q words: lo_x = w2.xy, lo_y = w2.zw, lo_z = w3.xy, hi_x = w3.zw, hi_y = w4.xy, hi_z = w4.zw
       const uint32_t nx0 = nx ? w3.z : w2.x, nx1 = nx ? w3.w : w2.y;
       const uint32_t fx0 = nx ? w2.x : w3.z, fx1 = nx ? w2.y : w3.w;
@@ -96,7 +159,7 @@ __global__ void __launch_bounds__(kBlock) k_trace(const uint4* __restrict__ node
       const uint32_t fy0 = ny ? w2.z : w4.x, fy1 = ny ? w2.w : w4.y;
       const uint32_t nz0 = nz ? w4.z : w3.x, nz1 = nz ? w4.w : w3.y;
       const uint32_t fz0 = nz ? w3.x : w4.z, fz1 = nz ? w3.y : w4.w;
-      uint32_t nh = 0, th = 0;
+      uint32_t hm = 0;  // slot-indexed hit mask
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const uint32_t sel = (uint32_t)(j & 3);
@@ -104,88 +167,139 @@ __global__ void __launch_bounds__(kBlock) k_trace(const uint4* __restrict__ node
         const float qny = u8f(j < 4 ? ny0 : ny1, sel), qfy = u8f(j < 4 ? fy0 : fy1, sel);
         const float qnz = u8f(j < 4 ? nz0 : nz1, sel), qfz = u8f(j < 4 ? fz0 : fz1, sel);
         const float tn = fmaxf(fmaxf(fmaf(qnx, sx.adj, sx.on), fmaf(qny, sy.adj, sy.on)),
-                               fmaxf(fmaf(qnz, sz.adj, sz.on), tmin));
+                               fmaxf(fmaf(qnz, sz.adj, sz.on), R.tmin));
         const float tf = fminf(fminf(fmaf(qfx, sx.adj, sx.of), fmaf(qfy, sy.adj, sy.of)),
-                               fminf(fmaf(qfz, sz.adj, sz.of), closest));
-        if (tn <= tf) {
-          if ((imask >> j) & 1u) {
-            nh |= 1u << ((uint32_t)j ^ oct);
-          } else {
-            const uint32_t m = ((j < 4 ? w1.z : w1.w) >> (8 * (j & 3))) & 0xFFu;
-            th |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-          }
-        }
+                               fminf(fmaf(qfz, sz.adj, sz.of), R.closest));
+        hm |= (tn <= tf) ? (1u << j) : 0u;
       }
+      const uint32_t nh = xor_permute8(hm & imask, R.oct);
+      uint32_t th = nibble_spread8(hm & ~imask) & w1.z;
       gbase = w1.x;
       ghits = nh;
       gimask = imask;
-      tbase = w1.y;
-      thits = th;
+      if (th) {
+        if (q0m == 0) { q0b = w1.y; q0m = th; }
+        else if (q1m == 0) { q1b = w1.y; q1m = th; }
+        else if (sp < STK) { stack[sp * kBlock] = make_uint2(w1.y, th); ++sp; }
+        else {
+          // no room anywhere: test the group now (correct, only slower)
+          while (th) {
+            const uint32_t tri = w1.y + (uint32_t)(__ffs(th) - 1);
+            th &= th - 1;
+            const float4* rec = tris + 4 * (size_t)tri;
+            const float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
+            const float t = wt_candidate(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
+                                         make_float3(c.x, c.y, c.z), R.tmin, R.closest,
+                                         [rec] { return __ldg(rec + 3); });
+            if (t >= 0.0f) { R.closest = t; R.best = (int)tri; }
+          }
+        }
+      }
     }
-    // ---- triangles of the expanded node
-    while (thits) {
-      const uint32_t k = (uint32_t)(__ffs(thits) - 1);
-      thits &= thits - 1;
-      const uint32_t tri = tbase + k;
-      const float4 a = __ldg(tris + 3 * (size_t)tri), b = __ldg(tris + 3 * (size_t)tri + 1),
-                   c = __ldg(tris + 3 * (size_t)tri + 2);
-      WtHit h;
-      if (wt_intersect(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z),
-                       tmin, &h) &&
-          h.t < closest) {
-        closest = h.t;
-        best = (int)tri;
-        best_t = h.t;
-        best_u = h.bary[1];
-        best_v = h.bary[2];
+
+    // ---- (2) up to two triangle tests from the queue head
+    bool done = false;
+#pragma unroll 1
+    for (int rep = 0; rep < 2; ++rep) {
+      if (q0m == 0) break;
+      const uint32_t tri = q0b + (uint32_t)(__ffs(q0m) - 1);
+      q0m &= q0m - 1;
+      if (q0m == 0) { q0b = q1b; q0m = q1m; q1m = 0; }
+      const float4* rec = tris + 4 * (size_t)tri;
+      const float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
+      const float t = wt_candidate(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
+                                   make_float3(c.x, c.y, c.z), R.tmin, R.closest, [rec] { return __ldg(rec + 3); });
+      if (t >= 0.0f) {
+        R.closest = t;
+        R.best = (int)tri;
         if (ANY) { done = true; break; }
       }
     }
-    if (ANY && done) break;
-    // ---- next node: current group, else the stack
-    while (ghits == 0) {
-      if (sp == 0) break;
-      --sp;
-      const uint2 g = stack[sp * kBlock];
-      gbase = g.x;
-      ghits = g.y & 0xFFu;
-      gimask = g.y >> 8;
-    }
-    if (ghits == 0) break;
-    const uint32_t k = (uint32_t)(__ffs(ghits) - 1);
-    ghits &= ghits - 1;
-    const uint32_t slot = k ^ oct;
-    node = gbase + __popc(gimask & ((1u << slot) - 1u));
-    if (ghits) {
-      if (sp < STK) {
-        stack[sp * kBlock] = make_uint2(gbase, ghits | (gimask << 8));
-        ++sp;
-      } else {
-        atomicOr(status, 1);  // stack capacity exceeded: result incomplete, reported to the host
-      }
-    }
-  }
 
-  if (ANY) {
-    occluded[ray] = (uint8_t)(best >= 0 ? 1 : 0);
+    // ---- (3) next node: current group, else the stack (triangle groups join the queue)
+    if (!done && !expand) {
+      while (true) {
+        if (ghits) {
+          const uint32_t k = (uint32_t)(__ffs(ghits) - 1);
+          ghits &= ghits - 1;
+          const uint32_t slot = k ^ R.oct;
+          node = gbase + __popc(gimask & ((1u << slot) - 1u));
+          expand = true;
+          if (ghits) {
+            if (sp < STK) {
+              stack[sp * kBlock] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
+              ++sp;
+            } else {
+              atomicOr(status, 1);  // stack capacity exceeded: result incomplete, reported to the host
+            }
+            ghits = 0;
+          }
+          break;
+        }
+        if (sp == 0) break;
+        const uint2 g = stack[(sp - 1) * kBlock];
+        if (g.x & kNodeGroup) {
+          --sp;
+          gbase = g.x & ~kNodeGroup;
+          ghits = g.y & 0xFFu;
+          gimask = g.y >> 8;
+        } else if (q1m == 0) {
+          --sp;
+          if (q0m == 0) { q0b = g.x; q0m = g.y; } else { q1b = g.x; q1m = g.y; }
+        } else {
+          break;  // queue full: test triangles first
+        }
+      }
+      if (!expand && q0m == 0 && sp == 0) done = true;
+    }
+    if (!done) continue;
+
+    // ---- ray finished: write its record, the lane is refilled next iteration
+    live = false;
+    if (ANY) {
+      occluded[ray] = (uint8_t)(R.best >= 0 ? 1 : 0);
+      continue;
+    }
+    // closest: (triangle record, watertight t); k_refine_hits turns it into
+    // (source id, t, u, v) in a coalesced pass with every lane busy
+    hits[ray] = make_int4(R.best, __float_as_int(R.closest), 0, 0);
+  }
+}
+
+// Second pass of the closest-hit query: one thread per ray, float-float
+// re-evaluation of the chosen triangle for t and barycentrics, record index
+// replaced by the source triangle id (-1 and tmax for a miss).
+__global__ void __launch_bounds__(256) k_refine_hits(const float4* __restrict__ tris,
+                                                      const float4* __restrict__ rays, size_t n,
+                                                      int4* __restrict__ hits) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 h = hits[i];
+  if (h.x < 0) {
+    hits[i] = make_int4(-1, h.y, 0, 0);
     return;
   }
-  int4 out;
-  if (best >= 0) {
-    const float4 a = __ldg(tris + 3 * (size_t)best), b = __ldg(tris + 3 * (size_t)best + 1),
-                 c = __ldg(tris + 3 * (size_t)best + 2);
-    float t, u, v;
-    if (ff_refine(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), make_float3(a.x, a.y, a.z),
-                  make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z), &t, &u, &v)) {
-      best_t = t;
-      best_u = u;
-      best_v = v;
-    }
-    out = make_int4((int)__float_as_uint(a.w), __float_as_int(best_t), __float_as_int(best_u), __float_as_int(best_v));
+  const float4 r0 = __ldg(rays + 2 * i), r1 = __ldg(rays + 2 * i + 1);
+  const float4* rec = tris + 4 * (size_t)(uint32_t)h.x;
+  const float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
+  float t = __int_as_float(h.y), u = 0.0f, v = 0.0f;
+  float tr, ur, vr;
+  if (ff_refine(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), make_float3(a.x, a.y, a.z),
+                make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z), &tr, &ur, &vr)) {
+    t = tr;
+    u = ur;
+    v = vr;
   } else {
-    out = make_int4(-1, __float_as_int(r1.w), 0, 0);
+    // degenerate in float-float too: report the watertight barycentrics
+    WtRay wr = wt_setup(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+    WtHit wh;
+    if (wt_intersect(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z),
+                     r0.w, &wh)) {
+      u = wh.bary[1];
+      v = wh.bary[2];
+    }
   }
-  hits[ray] = out;
+  hits[i] = make_int4((int)__float_as_uint(a.w), __float_as_int(t), __float_as_int(u), __float_as_int(v));
 }
 
 __global__ void k_watertight_eval(const float* __restrict__ cases, size_t n, vt_watertight_result* out) {
@@ -209,25 +323,36 @@ __global__ void k_watertight_eval(const float* __restrict__ cases, size_t n, vt_
 }
 
 template <bool ANY, int STK>
-void launch_stk(const TraceArgs& a, unsigned grid, cudaStream_t s) {
+void launch_stk(const TraceArgs& a, cudaStream_t s) {
   const size_t smem = sizeof(uint2) * STK * kBlock;
   if (smem > 48 * 1024)  // opt-in above the default 48 KB dynamic limit
     cudaFuncSetAttribute(k_trace<ANY, STK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_trace<ANY, STK><<<grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded, a.status);
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ANY, STK>, kBlock, smem);
+  // persistent grid: every resident slot once, never more blocks than rays need
+  size_t grid = (size_t)std::max(1, sms) * (size_t)std::max(1, per_sm);
+  grid = std::min(grid, (a.n + kBlock - 1) / kBlock);
+  cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
+  k_trace<ANY, STK><<<(unsigned)grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded,
+                                                         a.status, a.counter);
 }
 
 template <bool ANY>
 void launch_trace_t(const TraceArgs& a, cudaStream_t s) {
-  const unsigned grid = (unsigned)((a.n + kBlock - 1) / kBlock);
-  if (grid == 0) return;
-  if (a.stack_depth <= 16) launch_stk<ANY, 16>(a, grid, s);
-  else if (a.stack_depth <= 32) launch_stk<ANY, 32>(a, grid, s);
-  else launch_stk<ANY, 64>(a, grid, s);
+  if (a.n == 0) return;
+  if (a.stack_depth <= 16) launch_stk<ANY, 16>(a, s);
+  else if (a.stack_depth <= 32) launch_stk<ANY, 32>(a, s);
+  else launch_stk<ANY, 64>(a, s);
 }
 
 }  // namespace
 
-void launch_trace_closest(const TraceArgs& a, cudaStream_t s) { launch_trace_t<false>(a, s); }
+void launch_trace_closest(const TraceArgs& a, cudaStream_t s) {
+  launch_trace_t<false>(a, s);
+  if (a.n) k_refine_hits<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a.tris, a.rays, a.n, a.hits);
+}
 void launch_trace_any(const TraceArgs& a, cudaStream_t s) { launch_trace_t<true>(a, s); }
 
 void launch_watertight_eval(const float* cases, size_t n, vt_watertight_result* out, cudaStream_t s) {

@@ -19,6 +19,7 @@ struct TraceArgs {
   uint8_t* occluded = nullptr;    // 1 byte per ray (any)
   int* status = nullptr;          // device word, bit 0 = stack capacity exceeded
   int stack_depth = 64;           // wide-tree depth bound
+  unsigned long long* counter = nullptr;  // device word: next unclaimed ray (reset per launch)
 };
 
 void launch_trace_closest(const TraceArgs& a, cudaStream_t s);

@@ -23,6 +23,7 @@ namespace vt {
 struct WtRay {
   float o[3];     // origin
   float d[3];     // direction as given
+  float dn[3];    // d / ds (each component correctly rounded)
   float ds;       // max |d|
   float sx, sy, sz;
   int kx, ky, kz;
@@ -43,7 +44,8 @@ __device__ __forceinline__ WtRay wt_setup(float ox, float oy, float oz, float dx
   r.d[0] = dx; r.d[1] = dy; r.d[2] = dz;
   r.ds = max3n(fabsf(dx), fabsf(dy), fabsf(dz));
   r.ok = (r.ds > 0.0f) && isfinite(r.ds);
-  float dn[3] = {__fdiv_rn(dx, r.ds), __fdiv_rn(dy, r.ds), __fdiv_rn(dz, r.ds)};
+  float* dn = r.dn;
+  dn[0] = __fdiv_rn(dx, r.ds); dn[1] = __fdiv_rn(dy, r.ds); dn[2] = __fdiv_rn(dz, r.ds);
   int kz = fabsf(dn[1]) > fabsf(dn[0]) ? 1 : 0;
   if (fabsf(dn[2]) > fabsf(fsel3(dn, kz))) kz = 2;
   int kx = kz == 2 ? 0 : kz + 1;
@@ -199,6 +201,74 @@ __device__ __forceinline__ bool wt_intersect(const WtRay& r, float3 a, float3 b,
   if (pos ? (e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) : (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return false;
   return wt_finish(r, a, b, c, e0, e1, e2, det, __fmul_rn(az, r.sz), __fmul_rn(bz, r.sz), __fmul_rn(cz, r.sz),
                    apx, apy, bpx, bpy, cpx, cpy, exclusive_min_t, out);
+}
+
+// Rare tail of the traversal test: t for a hit whose projected point lies
+// exactly on an edge or vertex (opticalWatertightTriangle.ts:151-162).
+__device__ __noinline__ float wt_zero_edge_t(const WtRay r, const float3 A, const float3 B, const float3 C, float n0,
+                                             float n1, float n2, float apx, float apy, float bpx, float bpy,
+                                             float cpx, float cpy) {
+  const float a[3] = {A.x, A.y, A.z}, b[3] = {B.x, B.y, B.z}, c[3] = {C.x, C.y, C.z};
+  const int zc = (n0 == 0.0f) + (n1 == 0.0f) + (n2 == 0.0f);
+  float t = -1.0f;
+  if (zc >= 2) {
+    if (n0 != 0.0f) t = wt_ray_param(r.o, r.d, a);
+    if (n1 != 0.0f) t = wt_ray_param(r.o, r.d, b);
+    if (n2 != 0.0f) t = wt_ray_param(r.o, r.d, c);
+  } else if (n0 == 0.0f) {
+    t = wt_edge_ray_param(r.o, r.d, b, c, bpx, bpy, cpx, cpy);
+  } else if (n1 == 0.0f) {
+    t = wt_edge_ray_param(r.o, r.d, c, a, cpx, cpy, apx, apy);
+  } else {
+    t = wt_edge_ray_param(r.o, r.d, a, b, apx, apy, bpx, bpy);
+  }
+  return t;
+}
+
+// Watertight test inside traversal.  Returns the exact f32 t when the
+// triangle is hit with max(exclusive_min_t, 0) < t < closest, else -1.  The
+// accept/reject decision is identical to wt_intersect followed by
+// `t < closest`: the interval check only moves ahead of the normal/side
+// checks (which can only reject), and the triangle-only part of those checks
+// -- the reference's normal derivation -- comes precomputed in the record
+// (`nrm` = (n.xyz, valid)), leaving the ray-dependent side determinant.
+template <class NormalFetch>
+__device__ __forceinline__ float wt_candidate(const WtRay& r, float3 a, float3 b, float3 c, float exclusive_min_t,
+                                              float closest, NormalFetch nrm_fetch) {
+  float apx, apy, az, bpx, bpy, bz, cpx, cpy, cz;
+  wt_project3(r, a, apx, apy, az);
+  wt_project3(r, b, bpx, bpy, bz);
+  wt_project3(r, c, cpx, cpy, cz);
+  const float e0 = wt_edge(bpx, bpy, cpx, cpy);
+  const float e1 = wt_edge(cpx, cpy, apx, apy);
+  const float e2 = wt_edge(apx, apy, bpx, bpy);
+  const float det = __fadd_rn(__fadd_rn(e0, e1), e2);
+  if (det == 0.0f || !isfinite(det)) return -1.0f;
+  const bool pos = det > 0.0f;
+  if (pos ? (e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) : (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return -1.0f;
+  const float lo = exclusive_min_t > 0.0f ? exclusive_min_t : 0.0f;
+  const float st = __fadd_rn(__fadd_rn(__fmul_rn(e0, __fmul_rn(az, r.sz)), __fmul_rn(e1, __fmul_rn(bz, r.sz))),
+                             __fmul_rn(e2, __fmul_rn(cz, r.sz)));
+  float t;
+  if (e0 != 0.0f && e1 != 0.0f && e2 != 0.0f) {
+    // Cheap reject before the exact divisions: the fast quotient is within a
+    // few ulp of the exact one while both operands stay below 2^126, so a
+    // 1e-5 relative margin decides most far candidates without changing any result.
+    if (fabsf(det) < 1e30f && r.ds < 1e30f) {
+      const float ta = __fdividef(__fdividef(st, det), r.ds);
+      if (ta > closest * 1.00001f + 1e-30f || ta < lo * 0.99999f - 1e-30f) return -1.0f;
+    }
+    t = __fdiv_rn(__fdiv_rn(st, det), r.ds);
+  } else {
+    t = wt_zero_edge_t(r, a, b, c, pos ? e0 : -e0, pos ? e1 : -e1, pos ? e2 : -e2, apx, apy, bpx, bpy, cpx, cpy);
+  }
+  if (!(t > lo) || !isfinite(t) || !(t < closest)) return -1.0f;
+  const float4 nrm = nrm_fetch();
+  if (!(nrm.w != 0.0f)) return -1.0f;
+  const float sd = -__fadd_rn(__fadd_rn(__fmul_rn(r.dn[0], nrm.x), __fmul_rn(r.dn[1], nrm.y)),
+                              __fmul_rn(r.dn[2], nrm.z));
+  if (sd == 0.0f || !isfinite(sd)) return -1.0f;
+  return t;
 }
 
 // ------------------------------------------------------------ float-float
