@@ -1,0 +1,27 @@
+// bvh_object.h -- the vt_bvh object behind the C ABI handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bvh_host.h"
+#include "vt_common.h"
+
+struct vt_bvh {
+  int device = 0;
+  vt::BuildOptions opts;
+  vt::BinaryBvhHost binary;              // binary tree in the reference layout (for export)
+  vt::DeviceBuffer<uint4> nodes;         // 8-wide nodes
+  vt::DeviceBuffer<float4> tris;         // triangle records
+  vt::DeviceBuffer<int> status;          // traversal status word
+  vt::DeviceBuffer<unsigned long long> counter;  // persistent-kernel ray counter (calls on one bvh are serialised)
+  int64_t ntri = 0;
+  int64_t wide_count = 0;
+  int wide_depth = 0;
+  double build_ms = 0.0;
+  // staging for the host-buffer entry points
+  vt::DeviceBuffer<float4> rays_scratch;
+  vt::DeviceBuffer<int4> hits_scratch;
+  vt::DeviceBuffer<uint8_t> occ_scratch;
+};
