@@ -127,6 +127,21 @@ vt_status vt_bvh_trace_any(vt_bvh* bvh, const vt_ray* rays, size_t n, uint8_t* o
 
 vt_status vt_bvh_destroy(vt_bvh* bvh);
 
+/*
+ * Closest hit for host rays without allocating any device memory.  No
+ * counterpart in the reference: its query is a CPU function.  For callers
+ * that cannot allocate -- hosts with a fixed, pre-reserved device memory
+ * budget, or host-array callers (the Node addon) on a path where no
+ * cudaMalloc may happen; vt_bvh_trace_closest grows per-object staging
+ * instead.  Scratch is a library-wide device array of 3 MiB + 256 B, held by
+ * every GPU that loads the library until exit; n is at most 65,536 rays per
+ * call (VT_ERR_RANGE beyond).  The first call on a device looks up that
+ * array's address and must precede any stream capture.  Calls that overlap
+ * on the GPU race on the shared array.  Synchronous; same results as
+ * vt_bvh_trace_closest.
+ */
+vt_status vt_bvh_trace_closest_noalloc(const vt_bvh* bvh, const vt_ray* rays, size_t n, vt_hit* hits);
+
 /* ------------------------------------------------------------------ */
 /* Triangle test (shared-bvh/src/opticalWatertightTriangle.ts:98)       */
 /* ------------------------------------------------------------------ */

@@ -60,6 +60,7 @@ SIGNATURES = {
     "vt_bvh_trace_closest": [P, P, SZ, P],
     "vt_bvh_trace_any": [P, P, SZ, P],
     "vt_bvh_destroy": [P],
+    "vt_bvh_trace_closest_noalloc": [P, P, SZ, P],
     "vt_watertight_eval_device": [I32, P, SZ, P, P],
 }
 _RESTYPE = {"vt_last_error": ctypes.c_char_p, "vt_version": ctypes.c_char_p}
