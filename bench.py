@@ -1,28 +1,36 @@
 """Benchmark of the B200 ray-tracing hot path (one JSON line on rank 0).
 
-Workload (N=1, per GPU): closest-hit query over 65,536 seeded float32
-triangles with 1,048,576 rays per step (tmin 1e-4, tmax +inf), the
-shared-bvh build + query configuration.  Metric: Mrays/s (whole job).
+Headline workload (per GPU, N=1): unidirectional path tracing of the
+procedural box room -- 262,146 triangles, 512 x 512, 64 spp, at most 5
+bounces, NEE + MIS, Russian roulette after bounce 3, FP32 accumulation.  One
+step = one frame rendered from a cleared accumulation.  Metric: Mrays/s
+(extension + shadow rays traced, whole job); samples/s and ms/frame beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-* value: device-resident rays, K launches timed with CUDA events on the
-  launching stream, barrier + synchronize on both sides, max over ranks.
-  Four ray batches (4 x 48 MB of rays + hits) rotate so the per-step I/O is
-  larger than the 126 MB L2 and never cached between steps; the BVH itself
-  (3.4 MB) stays L2-resident by design.
-* e2e: the same metric through the public host-buffer call
-  (vt_bvh_trace_closest): pinned host rays copied in, hits copied out, per step.
-* roofline: algorithmic bytes per launch (32 + 16 + 80 V_node + 48 V_tri per
-  ray, V counted by the CPU oracle) / average launch time, against the
-  measured HBM copy bandwidth.
-* --impl reference: the reference algorithm's CPU query (C restatement of
-  intersectCompressedWideBvhFirstHit) on all host cores, bounded sample per step.
-* N > 1: independent replicas (rays shard across GPUs, no collective): weak scaling.
+* value: device time of K frames (CUDA events on the engine's stream around
+  each frame's graph replays; barrier + synchronize around the loop; max
+  over ranks).  Each frame streams ~400 MB of wave state (> 126 MB L2).
+* e2e: the same frames through the public Engine calls with the image read
+  back to host memory each step (vt_render_frame + vt_capture).
+* roofline: the traversal kernel (extension + shadow launches) -- algorithmic
+  bytes 32 + 16 + 80 V_node + 48 V_tri per ray with V counted by the CPU
+  oracle on this scene's path-tracing rays (tests/golden/visit_counts.json),
+  divided by the traversal stages' device time from a profiled frame, against
+  the measured HBM copy bandwidth.
+* query: the closest-hit query workload (65,536 triangles, 1,048,576 rays)
+  with its own roofline, reported in the same line.
+* cpu_baseline / --impl reference: the C restatement (oracle) of the same
+  estimator on all host cores on a bounded crop (no reference CPU integrator
+  exists at this scale; the reference's own CPU tracer is a Lambert-only
+  brute-force test helper).
+* N > 1: independent replicas (pixels/frames are independent, the scene is
+  replicated, no data-path collective): weak scaling.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -35,16 +43,21 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_TRIS = 65536
-N_RAYS = 1 << 20
-SEED = 2024
-BATCHES = 4
-WORKLOAD = "closest-hit query: 65,536 float32 triangles, 1,048,576 rays/step (tmin 1e-4, tmax inf)"
-METRIC = "Mrays/s (closest-hit query, 65,536 tris / 1,048,576 rays per step)"
+W = H = 512
+SPP = 64
+BOUNCES = 5
+Q_TRIS = 65536
+Q_RAYS = 1 << 20
+Q_SEED = 2024
+Q_BATCHES = 4
+WORKLOAD = ("box-room path tracing: 262,146 triangles, 512x512, 64 spp, max 5 bounces, NEE+MIS on the area "
+            "light, RR after bounce 3, FP32 accumulation")
+METRIC = "Mrays/s (box-room path tracing 512x512, 64 spp, 5 bounces; extension + shadow rays)"
 
 
 def _env_rank():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
 def _peaks():
@@ -56,20 +69,19 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic():
-    """dram read+write bytes per launch of the traversal kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "traverse_closest_config1.txt")
+def _profile_value(name, key):
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             return float(line.split(":")[1].split()[0])
     return None
 
 
-def _visit_model():
+def _visits():
     with open(os.path.join(ROOT, "tests", "golden", "visit_counts.json")) as f:
-        return json.load(f)["closest_hit_65536_tris_1048576_rays_seed2024"]
+        return json.load(f)
 
 
 class Clocks:
@@ -119,55 +131,118 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_reference(rays: np.ndarray, soup, target_s: float = 8.0):
-    """The reference query restated in C (oracle), all host cores, bounded sample."""
+# ------------------------------------------------------------------ CPU baseline
+def cpu_pt_baseline(target_s=8.0):
+    """The path-tracing estimator restated in C (oracle) on all host cores, on a
+    bounded centre crop of the same frame: returns (Mrays/s, cores, sample text)."""
     import oracle
+    from vitrum_b200 import scenes
+    sc, cam = scenes.box_room()
     threads = oracle.hw_threads()
-    t0 = time.perf_counter()
-    w = oracle.build_compressed_wide_bvh(soup.positions, soup.indices)
-    build_ms = (time.perf_counter() - t0) * 1e3
-    probe = rays[:16384]
-    t0 = time.perf_counter()
-    oracle.first_hit(w, soup.positions, probe, nthreads=threads)
-    rate = probe.shape[0] / (time.perf_counter() - t0)
-    n = int(min(rays.shape[0], max(probe.shape[0], rate * target_s)))
-    return w, threads, build_ms, n
+    nc, ns, dt = oracle.pt_ray_totals(sc, cam, 64, 64, 1, BOUNCES, nthreads=threads)
+    rate = (nc + ns) / dt
+    spp = int(max(1, min(64, target_s * rate / ((nc + ns) / 1.0))))
+    nc, ns, dt = oracle.pt_ray_totals(sc, cam, 64, 64, spp, BOUNCES, nthreads=threads)
+    return (nc + ns) / dt / 1e6, threads, (f"64x64-pixel frame of the same scene and camera, {spp} spp, "
+                                           f"{BOUNCES} bounces ({nc + ns} rays); C restatement of the estimator")
 
 
 def run_reference(args, rank, world):
-    from vitrum_b200 import scenes
-    import oracle
     if rank != 0:
         return
-    soup, rays = scenes.config1(N_TRIS, N_RAYS, seed=SEED)
-    w, threads, build_ms, n = cpu_reference(rays, soup, target_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
-    sample = rays[:n]
+    import oracle
+    from vitrum_b200 import scenes
+    sc, cam = scenes.box_room()
+    threads = oracle.hw_threads()
+    spp = 4
     for _ in range(args.warmup):
-        oracle.first_hit(w, soup.positions, sample, nthreads=threads)
-    t0 = time.perf_counter()
+        oracle.pt_ray_totals(sc, cam, 64, 64, spp, BOUNCES, nthreads=threads)
+    rays, secs = 0, 0.0
     for _ in range(args.steps):
-        oracle.first_hit(w, soup.positions, sample, nthreads=threads)
-    dt = time.perf_counter() - t0
-    value = n * args.steps / dt / 1e6
+        nc, ns, dt = oracle.pt_ray_totals(sc, cam, 64, 64, spp, BOUNCES, nthreads=threads)
+        rays += nc + ns
+        secs += dt
+    value = rays / secs / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded splitmix64)",
-        "config": {"workload": WORKLOAD, "seed": SEED},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (procedural box room)", "config": {"workload": WORKLOAD},
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} of {N_RAYS} rays per step; C restatement of shared-bvh "
-                                   f"intersectCompressedWideBvhFirstHit (FP64), build {build_ms:.1f} ms"},
+                         "sample": f"each step a 64x64-pixel frame of the same scene and camera at {spp} spp; "
+                                   "C restatement of the path-tracing estimator (the reference ships no "
+                                   "production CPU integrator)"},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ query workload
+def run_query(args, dev, local, rank, world, barrier):
+    import torch
+    from vitrum_b200 import _native as N
+    from vitrum_b200 import bvh as vb
+    from vitrum_b200 import scenes
+    soup, _ = scenes.config1(Q_TRIS, 16, seed=Q_SEED)
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices, device=local)
+    host = [scenes.sphere_rays(Q_RAYS, seed=Q_SEED + 1 + 1000 * rank + b) for b in range(Q_BATCHES)]
+    d_rays = [torch.from_numpy(r).to(dev) for r in host]
+    d_hits = [torch.empty((Q_RAYS, 4), dtype=torch.int32, device=dev) for _ in range(Q_BATCHES)]
+    stream = torch.cuda.current_stream(dev)
+
+    def step(i):
+        b = i % Q_BATCHES
+        g.trace_closest_device(d_rays[b].data_ptr(), Q_RAYS, d_hits[b].data_ptr(), stream.cuda_stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for i in range(args.steps):
+        step(i)
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    pin = [torch.from_numpy(r).pin_memory() for r in host]
+    pin_hits = torch.empty((Q_RAYS, 4), dtype=torch.int32).pin_memory()
+    N.call("vt_bvh_trace_closest", g.handle, ctypes.c_void_p(pin[0].data_ptr()), Q_RAYS,
+           ctypes.c_void_p(pin_hits.data_ptr()))
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        N.call("vt_bvh_trace_closest", g.handle, ctypes.c_void_p(pin[i % Q_BATCHES].data_ptr()), Q_RAYS,
+               ctypes.c_void_p(pin_hits.data_ptr()))
+    e2e_s = time.perf_counter() - t0
+    model = _visits()["closest_hit_65536_tris_1048576_rays_seed2024"]
+    peak, peak_kind = _peaks()
+    avg_s = statistics.mean(per) / 1e3
+    achieved = model["bytes_per_ray"] * Q_RAYS / avg_s / 1e9
+    g.close()
+    return {
+        "workload": "closest-hit query: 65,536 float32 triangles, 1,048,576 rays/launch (tmin 1e-4, tmax inf); "
+                    "4 rotating ray batches (192 MB rays+hits) > 126 MB L2",
+        "value": Q_RAYS * args.steps / (total_ms / 1e3) / 1e6, "unit": "Mrays/s",
+        "ms_per_launch": total_ms / args.steps,
+        "e2e": {"value": Q_RAYS * args.steps / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": Q_RAYS * 32,
+                "d2h_bytes_per_step": Q_RAYS * 16},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": _profile_value("traverse_closest_config1.txt", "dram_bytes_per_launch"),
+                     "peak_kind": peak_kind,
+                     "model": f"{model['bytes_per_ray']:.1f} B/ray (48 + 80*{model['v_node']:.3f} + "
+                              f"48*{model['v_tri']:.3f})"},
+    }
+
+
+# ------------------------------------------------------------------ path tracing workload
 def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
-    from vitrum_b200 import bvh as vb
+    from vitrum_b200 import _native as N
     from vitrum_b200 import scenes
+    from vitrum_b200.engine import Engine
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -179,114 +254,100 @@ def run_ours(args, rank, world, local):
         if world > 1:
             dist.barrier()
 
-    soup, _ = scenes.config1(N_TRIS, 16, seed=SEED)
-    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices, device=local)
-    info = g.info()
-    # per-rank ray batches (distinct seeds per rank and batch)
-    host_batches = [scenes.sphere_rays(N_RAYS, seed=SEED + 1 + 1000 * rank + b) for b in range(BATCHES)]
-    d_rays = [torch.from_numpy(r).to(dev) for r in host_batches]
-    d_hits = [torch.empty((N_RAYS, 4), dtype=torch.int32, device=dev) for _ in range(BATCHES)]
-    stream = torch.cuda.current_stream(dev)
-    sptr = stream.cuda_stream
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
-    def step(i):
-        b = i % BATCHES
-        g.trace_closest_device(d_rays[b].data_ptr(), N_RAYS, d_hits[b].data_ptr(), sptr)
+    sc, cam = scenes.box_room()
+    e = Engine(device=local, max_bounces=BOUNCES)
+    t0 = time.perf_counter()
+    e.set_scene(sc)
+    build_s = time.perf_counter() - t0
+
+    def frame(seed):
+        e.reset()
+        e.render_frame(cam, W, H, samples=SPP, frame_seed=seed)
 
     for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize(dev)
-
+        frame(1000 + i)
+    # per-stage device times of one frame (profiling path: direct launches, not timed for `value`)
+    e.reset()
+    stages = e.profile_frame(cam, W, H, samples=SPP, frame_seed=999)
+    st_before = e.stats()
     clocks = Clocks(local)
     clocks.start()
     barrier()
     torch.cuda.synchronize(dev)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    ev[0].record(stream)
+    frame_ms = []
+    rays0 = e.stats()
     for i in range(args.steps):
-        step(i)
-        ev[i + 1].record(stream)
+        frame(rank * 100000 + i)
+        frame_ms.append(e.stats()["last_frame_ms"])
     torch.cuda.synchronize(dev)
     barrier()
     clk = clocks.stop()
-    per_launch = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * N_RAYS * args.steps / (total_ms / 1e3) / 1e6
+    rays1 = e.stats()
+    rays = (rays1["closest_rays"] - rays0["closest_rays"]) + (rays1["shadow_rays"] - rays0["shadow_rays"])
+    closest = rays1["closest_rays"] - rays0["closest_rays"]
+    shadow = rays1["shadow_rays"] - rays0["shadow_rays"]
+    dev_s = max_over_ranks(sum(frame_ms) / 1e3)
+    value = world * rays / dev_s / 1e6
+    samples_per_s = world * W * H * SPP * args.steps / dev_s
 
-    # ---- e2e through the public host-buffer call, pinned host memory
-    pin_rays = [torch.from_numpy(r).pin_memory() for r in host_batches]
-    pin_hits = torch.empty((N_RAYS, 4), dtype=torch.int32).pin_memory()
-    from vitrum_b200 import _native as N
-    import ctypes
-
-    def e2e_step(i):
-        N.call("vt_bvh_trace_closest", g.handle, ctypes.c_void_p(pin_rays[i % BATCHES].data_ptr()), N_RAYS,
-               ctypes.c_void_p(pin_hits.data_ptr()))
-
-    for i in range(max(1, args.warmup)):
-        e2e_step(i)
-    barrier()
-    torch.cuda.synchronize(dev)
+    # e2e: public Engine calls, image read back to host every step
     t0 = time.perf_counter()
     for i in range(args.steps):
-        e2e_step(i)
-    torch.cuda.synchronize(dev)
-    e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * N_RAYS * args.steps / float(t.item()) / 1e6
+        frame(rank * 100000 + i)
+        img = e.capture_frame()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * rays / e2e_s / 1e6
 
-    # check the last hits are sane (no timing)
-    hits = pin_hits.numpy()
-    hit_frac = float((hits[:, 0] >= 0).mean())
+    query = run_query(args, dev, local, rank, world, barrier) if not args.no_query else None
 
     if rank == 0:
-        model = _visit_model()
-        avg_launch_s = statistics.mean(per_launch) / 1e3
-        bytes_per_launch = model["bytes_per_ray"] * N_RAYS
-        achieved = bytes_per_launch / avg_launch_s / 1e9
+        vc = _visits()["box_room_pt_512_64spp_5b"]
+        per_frame_closest = closest / args.steps
+        per_frame_shadow = shadow / args.steps
+        alg_bytes = (per_frame_closest * vc["closest_bytes_per_ray"] + per_frame_shadow * vc["shadow_bytes_per_ray"])
+        trace_s = (stages["trace_closest_ms"] + stages["trace_shadow_ms"]) / 1e3
+        achieved = alg_bytes / trace_s / 1e9
         peak, peak_kind = _peaks()
-        traffic = _traffic()
+        launches = stages["trace_closest_launches"]  # one per bounce per wave
+        waves = launches // BOUNCES if launches else 0
+        kernels_per_frame = waves * (1 + BOUNCES * 7 + 2)
         cpu = None
         if not args.no_cpu_baseline:
-            import oracle
-            soup_c, rays_c = scenes.config1(N_TRIS, N_RAYS, seed=SEED)
-            w, threads, build_ms, n = cpu_reference(rays_c, soup_c, target_s=8.0)
-            sample = rays_c[:n]
-            t0 = time.perf_counter()
-            oracle.first_hit(w, soup_c.positions, sample, nthreads=threads)
-            dt = time.perf_counter() - t0
-            cpu = {"value": n / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                   "sample": f"{n} rays of the same workload; C restatement of shared-bvh "
-                             f"intersectCompressedWideBvhFirstHit (FP64); CPU build {build_ms:.1f} ms"}
+            v, cores, sample = cpu_pt_baseline()
+            cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "port", "sample": sample}
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded splitmix64)",
-            "config": {"workload": WORKLOAD, "seed": SEED, "parallelism": f"replicas{world}",
-                       "l2": "4 rotating ray batches (192 MB rays+hits) > 126 MB L2; BVH L2-resident",
-                       "bvh": {"wide_nodes": info["wide_node_count"], "binary_nodes": info["binary_node_count"],
-                               "wide_depth": info["wide_depth"], "build_ms_host": round(info["build_ms"], 2)}},
+            "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural box room)",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas{world}", "resolution": [W, H], "spp": SPP,
+                       "max_bounces": BOUNCES, "triangles": sc.triangle_count,
+                       "l2": "per-frame wave state ~400 MB > 126 MB L2; BVH L2-resident",
+                       "scene_build_s": round(build_s, 3)},
+            "samples_per_s": samples_per_s, "ms_per_frame": dev_s * 1e3 / args.steps,
+            "rays_per_frame": {"extension": per_frame_closest, "shadow": per_frame_shadow},
+            "stages_ms": {k: round(v, 3) for k, v in stages.items() if k.endswith("_ms")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": peak_kind,
-                         "model": f"{model['bytes_per_ray']:.1f} B/ray = 48 + 80*{model['v_node']:.3f} + "
-                                  f"48*{model['v_tri']:.3f} (oracle near-first counts)",
-                         "avg_launch_ms": avg_launch_s * 1e3},
-            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 32,
-                    "d2h_bytes_per_step": N_RAYS * 16},
-            "gpu_launches": args.steps,
+                         "frac": achieved / peak,
+                         "traffic": _profile_value("path_trace_box_room.txt", "dram_bytes_per_trace_launch"),
+                         "peak_kind": peak_kind, "kernel": "k_trace (extension + shadow launches)",
+                         "model": f"extension {vc['closest_bytes_per_ray']:.1f} B/ray, shadow "
+                                  f"{vc['shadow_bytes_per_ray']:.1f} B/ray (oracle visit counts)",
+                         "trace_ms_per_frame": trace_s * 1e3},
+            "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(ctypes.c_float) * 32 + 20,
+                    "d2h_bytes_per_step": W * H * 16},
+            "gpu_launches": kernels_per_frame * args.steps,
             "clocks": clk,
-            "hit_fraction": hit_frac,
             "cpu_baseline": cpu,
+            "query": query,
         }
         print(json.dumps(line), flush=True)
-    g.close()
+    e.dispose()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -295,10 +356,11 @@ def run_ours(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-query", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = _env_rank()

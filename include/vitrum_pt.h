@@ -143,6 +143,135 @@ vt_status vt_bvh_destroy(vt_bvh* bvh);
 vt_status vt_bvh_trace_closest_noalloc(const vt_bvh* bvh, const vt_ray* rays, size_t n, vt_hit* hits);
 
 /* ------------------------------------------------------------------ */
+/* Path-tracing engine (@vitrum/core Engine, backend pt-webgpu)         */
+/* ------------------------------------------------------------------ */
+
+typedef struct vt_engine vt_engine;
+
+/* Creation-time options (PTEngineWebGPUOptions, pt-webgpu/src/index.ts:219-345).
+ * Zero selects the default. */
+typedef struct vt_engine_options {
+  int32_t max_bounces;            /* default 8 (PT_WEBGPU_MAX_BOUNCES, ptWebgpuValidation.ts:181), at most 8 */
+  int32_t max_samples_per_pixel;  /* default 4096 (index.ts:370) */
+  int32_t debug;                  /* 1 enables vt_pick (EngineOptions.debug, engine/factory.ts) */
+  int32_t oracle_accumulation;    /* 1 keeps FP64 per-pixel sums and sums of squares */
+  int32_t sort_by_material;       /* 0 = on (default), -1 = off: shading in queue order */
+  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^21 */
+} vt_engine_options;
+
+/* Material (core Material subset, core/src/scene/material.ts): transmission > 0
+ * selects the smooth dielectric, metallic >= 0.5 the GGX conductor, otherwise
+ * Lambert.  emission is radiance leaving the front face (winding normal). */
+typedef struct vt_material_desc {
+  float base_color[3];
+  float roughness;
+  float metallic;
+  float transmission;
+  float ior;
+  float emission[3];
+} vt_material_desc;
+
+/* One triangle mesh in world space. */
+typedef struct vt_mesh_desc {
+  const float* positions;   /* 3 floats per vertex */
+  size_t vertex_count;
+  const uint32_t* indices;  /* 3 per triangle */
+  size_t triangle_count;
+  uint32_t material;        /* index into vt_scene_desc.materials */
+} vt_mesh_desc;
+
+typedef struct vt_point_light_desc {
+  float position[3];
+  float intensity[3];       /* radiant intensity; irradiance falls off as 1/d^2 */
+} vt_point_light_desc;
+
+/* Scene (core Scene, core/src/scene/index.ts:42-46): primitives, emitters,
+ * environment.  The environment is an equirectangular RGB image (row 0 at +y). */
+typedef struct vt_scene_desc {
+  const vt_mesh_desc* meshes;
+  size_t mesh_count;
+  const vt_material_desc* materials;
+  size_t material_count;
+  const vt_point_light_desc* point_lights;
+  size_t point_light_count;
+  const float* environment_rgb;  /* width * height * 3 floats, or NULL */
+  int32_t environment_width;
+  int32_t environment_height;
+  float environment_intensity;
+} vt_scene_desc;
+
+/* Per-frame input (core FrameInput, core/src/frame.ts:91): camera matrices
+ * column-major, viewport, sampling. */
+typedef struct vt_frame_input {
+  float view[16];
+  float projection[16];
+  int32_t width;
+  int32_t height;
+  uint32_t frame_seed;
+  int32_t samples;   /* samples per pixel to add in this call */
+  int32_t bounces;   /* 0 = the engine's max_bounces */
+} vt_frame_input;
+
+/* FrameOutput (core/src/frame.ts:376-421).  radiance_device is the engine's
+ * accumulation buffer (float4 per pixel: rgb sum, sample count), valid until
+ * the next render or reset. */
+typedef struct vt_frame_output {
+  int32_t kind;                 /* 0 rendered, 1 skipped (converged) */
+  int32_t samples_accumulated;
+  int32_t is_converged;
+  int32_t width;
+  int32_t height;
+  const void* radiance_device;
+} vt_frame_output;
+
+typedef struct vt_engine_stats {
+  uint64_t closest_rays;   /* extension rays traced since vt_create */
+  uint64_t shadow_rays;    /* shadow rays traced since vt_create */
+  double last_frame_ms;    /* device time of the last vt_render_frame */
+  int64_t triangle_count;
+  int64_t emitter_count;
+} vt_engine_stats;
+
+/* Device time per wavefront stage of one profiled frame. */
+typedef struct vt_stage_times {
+  double raygen_ms;
+  double trace_closest_ms;
+  double sort_ms;
+  double shade_ms;
+  double trace_shadow_ms;
+  double resolve_ms;
+  double accumulate_ms;
+  double frame_ms;
+  int32_t trace_closest_launches;
+  int32_t trace_shadow_launches;
+} vt_stage_times;
+
+/* createPTEngine_WebGPU (pt-webgpu/src/index.ts:2363) */
+vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine** out_engine);
+/* Engine.setScene (core/src/engine/index.ts:120; pt-webgpu index.ts:1120).  Copies the scene. */
+vt_status vt_set_scene(vt_engine* engine, const vt_scene_desc* scene);
+/* Engine.renderFrame (index.ts:251; pt-webgpu index.ts:1817): adds input->samples samples. */
+vt_status vt_render_frame(vt_engine* engine, const vt_frame_input* input, vt_frame_output* output);
+/* vt_render_frame issuing the wave stages directly (no graph replay) with
+ * events between them; the frame timings FrameStats.passTimings would carry
+ * (core/src/engine/telemetry.ts:15-40). */
+vt_status vt_profile_frame(vt_engine* engine, const vt_frame_input* input, vt_frame_output* output,
+                           vt_stage_times* out_times);
+/* Engine.captureFrame (index.ts:466): mean radiance, RGBA float32, row-major, top-left. */
+vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
+/* FP64 per-pixel mean and per-sample variance (requires oracle_accumulation);
+ * 3 doubles per pixel each. */
+vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
+/* Engine.debug.pickPrimitive (engine/debug.ts:33-35; pickPrimitiveCpu.ts:674):
+ * source triangle id under pixel (x, y) of the last frame's camera, or -1. */
+vt_status vt_pick(vt_engine* engine, float x, float y, int32_t* out_triangle);
+/* Engine.reset (pt-webgpu index.ts:2052): clears the accumulation. */
+vt_status vt_reset(vt_engine* engine);
+vt_status vt_engine_get_stats(const vt_engine* engine, vt_engine_stats* out_stats);
+/* Engine.dispose */
+vt_status vt_destroy(vt_engine* engine);
+
+/* ------------------------------------------------------------------ */
 /* Triangle test (shared-bvh/src/opticalWatertightTriangle.ts:98)       */
 /* ------------------------------------------------------------------ */
 

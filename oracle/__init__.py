@@ -50,7 +50,7 @@ def lib():
                                           ctypes.c_long, P, ctypes.c_long, P, P, P, P, ctypes.c_int]
         L.orc_count_visits.restype = ctypes.c_int
         L.orc_count_visits.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_int, P, ctypes.c_int, P,
-                                       ctypes.c_long, P, P, ctypes.c_int]
+                                       ctypes.c_long, P, P, ctypes.c_int, ctypes.c_int]
         L.orc_brute_first_hit.restype = ctypes.c_int
         L.orc_brute_first_hit.argtypes = [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_long, P, ctypes.c_long,
                                           P, P, P, P]
@@ -188,8 +188,9 @@ def first_hit_watertight(wide: WideBvh, positions, rays, pos_stride=4, nthreads=
     return prim, t, bary
 
 
-def count_visits(wide: WideBvh, positions, rays, pos_stride=4, nthreads=0):
-    """Near-first wide-node visits and triangle tests summed over the rays."""
+def count_visits(wide: WideBvh, positions, rays, pos_stride=4, nthreads=0, any_hit=False):
+    """Near-first wide-node visits and triangle tests summed over the rays
+    (any_hit: stop at the first accepted triangle, the shadow-ray query)."""
     positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
     rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
     nn = ctypes.c_long(0)
@@ -198,7 +199,7 @@ def count_visits(wide: WideBvh, positions, rays, pos_stride=4, nthreads=0):
     lib().orc_count_visits(_p(wide.node_bounds), _p(wide.child_bounds), _p(wide.child_meta),
                            _p(wide.child_count), wide.node_count, _p(positions), pos_stride,
                            _p(b.reordered_indices), b.idx_stride, _p(rays), rays.shape[0],
-                           ctypes.byref(nn), ctypes.byref(nt), nthreads)
+                           ctypes.byref(nn), ctypes.byref(nt), nthreads, 1 if any_hit else 0)
     return nn.value, nt.value
 
 
@@ -235,3 +236,88 @@ def watertight_f32(o, d, a, b, c, exclusive_min_t=0.0):
     hit = lib().orc_watertight_f32(_p(f(o)), _p(f(d)), _p(f(a)), _p(f(b)), _p(f(c)), exclusive_min_t,
                                    ctypes.byref(t), _p(bary), ctypes.byref(side), ctypes.byref(mask))
     return dict(hit=bool(hit), t=t.value, bary=bary, side=side.value, zero_edge_mask=mask.value)
+
+
+# ---------------------------------------------------------------- path tracer
+def _pt_lib():
+    L = lib()
+    if not getattr(L, "_pt_ready", False):
+        P = ctypes.c_void_p
+        L.orc_pt_render.restype = ctypes.c_int
+        L.orc_pt_render.argtypes = [P, ctypes.c_long, P, ctypes.c_long, P, P, ctypes.c_int, P, ctypes.c_long, P,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                    ctypes.c_int, P, P, P, P, ctypes.c_long, P]
+        L._pt_ready = True
+    return L
+
+
+def flatten_scene(scene):
+    """(positions (V,4) f32, indices (T,4) u32, tri_material u32, materials (M,12) f32,
+    points (P,6) f32, env (H,W,3) f32 or None, env_intensity) from an engine Scene."""
+    pos, idx, tm = [], [], []
+    base = 0
+    for m in scene.meshes:
+        p = np.asarray(m.positions, np.float32).reshape(-1, 3)
+        i = np.asarray(m.indices, np.uint32).reshape(-1, 3)
+        p4 = np.zeros((p.shape[0], 4), np.float32)
+        p4[:, :3] = p
+        i4 = np.zeros((i.shape[0], 4), np.uint32)
+        i4[:, :3] = i + base
+        pos.append(p4)
+        idx.append(i4)
+        tm.append(np.full(i.shape[0], m.material, np.uint32))
+        base += p.shape[0]
+    mats = np.zeros((len(scene.materials), 12), np.float32)
+    for k, m in enumerate(scene.materials):
+        mats[k, 0:3] = m.base_color
+        mats[k, 3:7] = (m.roughness, m.metallic, m.transmission, m.ior)
+        mats[k, 7:10] = m.emission
+    pts = np.array([[*l.position, *l.intensity] for l in scene.point_lights], np.float32).reshape(-1, 6)
+    env = None if scene.environment is None else np.ascontiguousarray(scene.environment.rgb, np.float32)
+    ei = 1.0 if scene.environment is None else float(scene.environment.intensity)
+    return np.concatenate(pos), np.concatenate(idx), np.concatenate(tm), mats, pts, env, ei
+
+
+def inverse_view_proj(camera, width, height):
+    """Row-major float32 inverse of projection * view, as the engine computes it."""
+    view, proj = camera.matrices(width / height)
+    V = np.asarray(view, np.float64).reshape(4, 4).T
+    Pm = np.asarray(proj, np.float64).reshape(4, 4).T
+    return np.linalg.inv(Pm @ V).astype(np.float32)
+
+
+def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_base=0, bias=2e-5, nthreads=0,
+              log_rays=0):
+    """CPU path tracer: (sum, sum_sq) FP64 per pixel, shapes (H, W, 3).
+
+    With log_rays > 0 also returns (closest_rays, shadow_rays, totals): the
+    first log_rays extension and shadow rays as (n, 8) float32 rows and the
+    total number of each traced."""
+    pos, idx, tm, mats, pts, env, ei = flatten_scene(scene)
+    ivp = np.ascontiguousarray(inverse_view_proj(camera, width, height))
+    s = np.zeros((height, width, 3), np.float64)
+    q = np.zeros_like(s)
+    ew, eh = (0, 0) if env is None else (env.shape[1], env.shape[0])
+    lc = np.zeros((max(log_rays, 0), 8), np.float32)
+    ls = np.zeros((max(log_rays, 0), 8), np.float32)
+    totals = np.zeros(2, np.int64)
+    r = _pt_lib().orc_pt_render(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
+                                _p(pts) if pts.size else None, pts.shape[0], _p(env) if env is not None else None,
+                                ew, eh, ei, _p(ivp), width, height, spp, max_bounces, seed, sample_base, bias,
+                                nthreads, _p(s), _p(q), _p(lc) if log_rays else None, _p(ls) if log_rays else None,
+                                max(log_rays, 0), _p(totals))
+    if r != 0:
+        raise RuntimeError("oracle path tracer failed")
+    if log_rays:
+        nc, ns = int(totals[0]), int(totals[1])
+        return s, q, lc[:min(nc, log_rays)], ls[:min(ns, log_rays)], (nc, ns)
+    return s, q
+
+
+def pt_ray_totals(scene, camera, width, height, spp, max_bounces, seed=0, nthreads=0):
+    """Rays traced by the CPU path tracer: (closest, shadow, seconds)."""
+    import time
+    t0 = time.perf_counter()
+    out = pt_render(scene, camera, width, height, spp, max_bounces, seed=seed, nthreads=nthreads, log_rays=1)
+    return out[4][0], out[4][1], time.perf_counter() - t0

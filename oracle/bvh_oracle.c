@@ -717,7 +717,7 @@ static void first_hit_one(const orc_wide_t* W, const double o[3], const double d
  * to first_hit_one up to exact t ties.
  */
 static void count_one(const orc_wide_t* W, const double o[3], const double d[3], double tmin, double tmax,
-                      long* n_nodes, long* n_tris) {
+                      long* n_nodes, long* n_tris, int any) {
   double closest = tmax;
   if (W->n_wide == 0) return;
   const float* rb = W->node_bounds;
@@ -756,7 +756,10 @@ static void count_one(const orc_wide_t* W, const double o[3], const double d[3],
         double a[3], b[3], c[3], t, bary[3];
         vtx(W, ib[0], a); vtx(W, ib[1], b); vtx(W, ib[2], c);
         *n_tris += 1;
-        if (tri_fp64(o, d, a, b, c, tmin, &t, bary) && t > tmin && t < closest) closest = t;
+        if (tri_fp64(o, d, a, b, c, tmin, &t, bary) && t > tmin && t < closest) {
+          closest = t;
+          if (any) return;
+        }
       }
     }
     /* internal children far-to-near so the nearest pops first */
@@ -775,6 +778,7 @@ typedef struct {
   double* t;
   double* bary_uv;
   int32_t* bvh_tri;
+  int any;
   long nodes[256], tris[256];
 } batch_ctx_t;
 
@@ -799,7 +803,7 @@ static void count_range(void* c, long b, long e, int worker) {
     const float* ry = x->rays + r * 8;
     double o[3] = {ry[0], ry[1], ry[2]}, d[3] = {ry[4], ry[5], ry[6]};
     long a = 0, q = 0;
-    count_one(&x->W, o, d, ry[3], ry[7], &a, &q);
+    count_one(&x->W, o, d, ry[3], ry[7], &a, &q, x->any);
     x->nodes[worker] += a;
     x->tris[worker] += q;
   }
@@ -828,11 +832,11 @@ int orc_first_hit_batch(const float* node_bounds, const uint16_t* child_bounds, 
 int orc_count_visits(const float* node_bounds, const uint16_t* child_bounds, const uint32_t* child_meta,
                      const uint32_t* child_count, long n_wide, const float* positions, int pos_stride,
                      const uint32_t* reordered_indices, int idx_stride, const float* rays, long nrays,
-                     long* out_nodes, long* out_tris, int nthreads) {
+                     long* out_nodes, long* out_tris, int nthreads, int any) {
   batch_ctx_t* x = (batch_ctx_t*)calloc(1, sizeof(batch_ctx_t));
   orc_wide_t W = {node_bounds, child_bounds, child_meta, child_count, n_wide, positions,
                   pos_stride, reordered_indices, idx_stride, NULL, 0};
-  x->W = W; x->rays = rays;
+  x->W = W; x->rays = rays; x->any = any;
   parallel_for(nrays, 512, nthreads, count_range, x);
   long sn = 0, st = 0;
   for (int i = 0; i < 256; ++i) { sn += x->nodes[i]; st += x->tris[i]; }
@@ -874,6 +878,13 @@ int orc_brute_first_hit(const float* positions, int pos_stride, const uint32_t* 
     if (second_t) second_t[r] = second;
   }
   return 0;
+}
+
+/* FP64 triangle test on double inputs (the path-tracer oracle uses it). */
+int orc_tri_hit_d(const double o[3], const double d[3], const double a[3], const double b[3], const double c[3],
+                  double tmin, double* t) {
+  double bary[3];
+  return tri_fp64(o, d, a, b, c, tmin, t, bary);
 }
 
 /* FP64 single triangle test exposed for unit tests. */

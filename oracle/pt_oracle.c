@@ -1,0 +1,655 @@
+/*
+ * pt_oracle.c -- CPU restatement of the unidirectional path tracer.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker of the device path tracer).
+ *
+ * Follows the reference integrator's estimator for the plain-PT subset
+ * (packages/pt-webgpu/src/wgsl/pathTrace/kernel.wgsl.ts:963-2030, CPU mirror
+ * packages/pt-webgpu/src/__tests__/cpuTracer.ts:411-518 generalised to the
+ * Lambert / GGX-conductor / smooth-dielectric set):
+ *   PCG32 and the frame key            shared-samplers/src/wgsl/pcg.wgsl.ts:5-24,
+ *                                      pt-webgpu/src/wgsl/common.wgsl.ts:194-196
+ *   primary ray from the inverse VP    kernelCore.wgsl.ts:22-26, common.wgsl.ts:431-470
+ *   one light entry, uniform pick      kernel.wgsl.ts:1149-1675 (cpuTracer.ts:411-452)
+ *   power-heuristic MIS                material.wgsl.ts:2808-2822
+ *   GGX VNDF, Fresnel, frDielectric    bsdf.wgsl.ts:1710-1737, material.wgsl.ts:2766-2806
+ *   RR for bounce > 2                  kernelCore.wgsl.ts:54-67
+ * with the same random-number consumption order as the device kernels, so
+ * most samples follow the same path on both sides.  Visibility is the FP64
+ * Moller-Trumbore test (compressedWideBvh.ts:551-614) over a binned-SAH BVH
+ * built by orc_build_array_bvh.  Accumulates FP64 per-pixel sums and sums
+ * of squares.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+long orc_build_array_bvh(const float* positions, long n_pos_words, int pos_stride, const uint32_t* indices,
+                         long ntri, int idx_stride, int max_leaf, int nbins, int max_depth, uint32_t* out_nodes,
+                         uint32_t* out_reordered_to_source);
+int orc_tri_hit_d(const double o[3], const double d[3], const double a[3], const double b[3], const double c[3],
+                  double tmin, double* t);
+int orc_hw_threads(void);
+
+#define PI_F 3.14159265358979323846f
+
+/* ---------------------------------------------------------------- RNG */
+static uint32_t pcg_init(uint32_t px, uint32_t py, uint32_t key) {
+  uint32_t s = px * 1664525u + py * 1013904223u + key * 22695477u;
+  s ^= s >> 17;
+  s ^= s << 31;
+  s ^= s >> 11;
+  return s;
+}
+static uint32_t pcg_next(uint32_t* s) {
+  *s = *s * 747796405u + 2891336453u;
+  uint32_t w = ((*s >> ((*s >> 28) + 4u)) ^ *s) * 277803737u;
+  return (w >> 22) ^ w;
+}
+static float rand01(uint32_t* s) { return (float)(pcg_next(s) >> 8) * (1.0f / 16777216.0f); }
+static float represented_bernoulli(float p) {
+  if (!(p > 0.0f)) return 0.0f;
+  if (p >= 1.0f) return 1.0f;
+  float b = floorf(p * 16777216.0f + 0.5f);
+  if (b < 1.0f) b = 1.0f;
+  if (b > 16777215.0f) b = 16777215.0f;
+  return b * (1.0f / 16777216.0f);
+}
+static uint32_t rand_bounded(uint32_t* s, uint32_t bound) {
+  if (bound <= 1u) return 0u;
+  uint32_t threshold = (0u - bound) % bound;
+  uint32_t v = pcg_next(s);
+  for (int k = 0; k < 64 && v < threshold; ++k) v = pcg_next(s);
+  return v % bound;
+}
+
+/* ---------------------------------------------------------------- vectors */
+typedef struct { float x, y, z; } v3;
+static v3 V(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static v3 add(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static v3 sub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static v3 mul(v3 a, v3 b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+static v3 scl(v3 a, float s) { return V(a.x * s, a.y * s, a.z * s); }
+static float dot3(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static v3 cross3(v3 a, v3 b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static float maxc(v3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
+static v3 nrm(v3 a) {
+  float l2 = dot3(a, a);
+  return l2 > 1e-30f ? scl(a, 1.0f / sqrtf(l2)) : V(0, 0, 1);
+}
+static void onb(v3 n, v3* t, v3* b) {
+  float l2 = n.x * n.x + n.y * n.y;
+  if (l2 > 1e-10f) {
+    float inv = 1.0f / sqrtf(l2);
+    *t = V(-n.y * inv, n.x * inv, 0.0f);
+  } else {
+    *t = V(1, 0, 0);
+  }
+  *b = cross3(n, *t);
+}
+
+/* ---------------------------------------------------------------- scene */
+typedef struct {
+  float base[3], roughness, emission[3], ior;
+  int kind; /* 0 lambert, 1 conductor, 2 dielectric */
+  float alpha;
+  int emissive;
+} orc_mat_t;
+
+typedef struct {
+  const float* pos;       /* stride 4 */
+  const uint32_t* idx;    /* stride 4 */
+  const uint32_t* tmat;   /* per triangle */
+  long ntri;
+  uint32_t* nodes;        /* binary BVH */
+  uint32_t* r2s;
+  const orc_mat_t* mats;
+  /* emitters */
+  const uint32_t* em_tri; /* emissive triangle ids */
+  const float* em_cdf;
+  long n_em;
+  float em_area;
+  const float* points;    /* 6 floats each: position, intensity */
+  long n_points;
+  const float* env;       /* W*H*3 */
+  const float* env_marg;  /* H+1 */
+  const float* env_cond;  /* H*(W+1) */
+  int env_w, env_h, env_sampleable;
+  float env_scale;
+  int n_entries;
+  float bias;
+  /* camera / frame */
+  const float* inv_vp;    /* row-major */
+  int width, height, max_bounces;
+  uint32_t seed, sample_base;
+  int spp;
+  double* sum;
+  double* sq;
+  /* optional ray log: first `log_cap` rays of each kind (8 floats each) and totals */
+  float* log_closest;
+  float* log_shadow;
+  long log_cap;
+  long n_closest, n_shadow;  /* totals, updated atomically */
+} orc_pt_t;
+
+static void log_ray(orc_pt_t* S, int shadow, const double o[3], const double d[3], double tmax) {
+  long k = __atomic_fetch_add(shadow ? &S->n_shadow : &S->n_closest, 1, __ATOMIC_RELAXED);
+  float* buf = shadow ? S->log_shadow : S->log_closest;
+  if (!buf || k >= S->log_cap) return;
+  float* r = buf + 8 * k;
+  r[0] = (float)o[0]; r[1] = (float)o[1]; r[2] = (float)o[2]; r[3] = 0.0f;
+  r[4] = (float)d[0]; r[5] = (float)d[1]; r[6] = (float)d[2]; r[7] = (float)tmax;
+}
+
+static void tri_vertices(const orc_pt_t* S, long t, double a[3], double b[3], double c[3]) {
+  const uint32_t* iv = S->idx + 4 * t;
+  for (int k = 0; k < 3; ++k) {
+    a[k] = S->pos[4 * iv[0] + k];
+    b[k] = S->pos[4 * iv[1] + k];
+    c[k] = S->pos[4 * iv[2] + k];
+  }
+}
+
+static int box_hit(const float* mn, const float* mx, const double o[3], const double inv[3], double tmax, double* tn) {
+  double t0 = 0.0, t1 = tmax;
+  for (int k = 0; k < 3; ++k) {
+    double a = (mn[k] - o[k]) * inv[k], b = (mx[k] - o[k]) * inv[k];
+    if (a > b) { double x = a; a = b; b = x; }
+    if (a > t0) t0 = a;
+    if (b < t1) t1 = b;
+    if (t1 < t0) return 0;
+  }
+  *tn = t0;
+  return 1;
+}
+
+/* closest (any=0) or any (any=1) hit with t in (0, tmax); returns triangle id or -1 */
+static long trace(const orc_pt_t* S, const double o[3], const double d[3], double tmax, int any, double* t_out) {
+  double inv[3];
+  for (int k = 0; k < 3; ++k) inv[k] = 1.0 / (fabs(d[k]) > 1e-30 ? d[k] : copysign(1e-30, d[k]));
+  uint32_t stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  long best = -1;
+  double closest = tmax;
+  while (sp > 0) {
+    uint32_t n = stack[--sp];
+    const uint32_t* nd = S->nodes + 8 * (size_t)n;
+    double tn;
+    if (!box_hit((const float*)nd, (const float*)nd + 3, o, inv, closest, &tn)) continue;
+    if ((nd[7] >> 16) == 0xFFFFu) {
+      uint32_t cnt = nd[7] & 0xFFFFu;
+      for (uint32_t i = 0; i < cnt; ++i) {
+        long tri = S->r2s[nd[6] + i];
+        double a[3], b[3], c[3], t;
+        tri_vertices(S, tri, a, b, c);
+        if (orc_tri_hit_d(o, d, a, b, c, 0.0, &t) && t > 0.0 && t < closest) {
+          closest = t;
+          best = tri;
+          if (any) { *t_out = t; return best; }
+        }
+      }
+      continue;
+    }
+    uint32_t l = n + 1, r = n + nd[6];
+    if (sp + 2 > 128) continue;
+    /* near child on top */
+    double tl = 0, tr = 0;
+    const uint32_t* ln = S->nodes + 8 * (size_t)l;
+    const uint32_t* rn = S->nodes + 8 * (size_t)r;
+    int hl = box_hit((const float*)ln, (const float*)ln + 3, o, inv, closest, &tl);
+    int hr = box_hit((const float*)rn, (const float*)rn + 3, o, inv, closest, &tr);
+    if (hl && hr) {
+      if (tl < tr) { stack[sp++] = r; stack[sp++] = l; } else { stack[sp++] = l; stack[sp++] = r; }
+    } else if (hl) {
+      stack[sp++] = l;
+    } else if (hr) {
+      stack[sp++] = r;
+    }
+  }
+  *t_out = closest;
+  return best;
+}
+
+/* ---------------------------------------------------------------- BSDF */
+static v3 schlick(v3 f0, float c) {
+  float m = fminf(fmaxf(1.0f - c, 0.0f), 1.0f), m2 = m * m, m5 = m2 * m2 * m;
+  return add(f0, scl(sub(V(1, 1, 1), f0), m5));
+}
+static float fr_dielectric(float cos_i, float eta) {
+  float ct = fminf(fmaxf(cos_i, -1.0f), 1.0f), e = eta;
+  if (ct < 0.0f) { e = 1.0f / e; ct = -ct; }
+  float s2i = fmaxf(0.0f, 1.0f - ct * ct), s2t = s2i / (e * e);
+  if (s2t >= 1.0f) return 1.0f;
+  float cost = sqrtf(fmaxf(0.0f, 1.0f - s2t));
+  float rp = (e * ct - cost) / (e * ct + cost), rs = (ct - e * cost) / (ct + e * cost);
+  return 0.5f * (rp * rp + rs * rs);
+}
+static float ggx_d(float nh, float a) {
+  float a2 = a * a, d = nh * nh * (a2 - 1.0f) + 1.0f;
+  return a2 / (PI_F * d * d);
+}
+static float ggx_g1(float nv, float a) {
+  float a2 = a * a;
+  return 2.0f * nv / (nv + sqrtf(a2 + (1.0f - a2) * nv * nv));
+}
+static v3 ggx_vndf(v3 wo, float a, float u1, float u2) {
+  v3 vh = nrm(V(a * wo.x, a * wo.y, wo.z)), t1, t2;
+  onb(vh, &t1, &t2);
+  float r = sqrtf(u1), phi = 2.0f * PI_F * u2;
+  float p1 = r * cosf(phi), p2 = r * sinf(phi), s = 0.5f * (1.0f + vh.z);
+  p2 = (1.0f - s) * sqrtf(fmaxf(0.0f, 1.0f - p1 * p1)) + s * p2;
+  float z = sqrtf(fmaxf(0.0f, 1.0f - p1 * p1 - p2 * p2));
+  v3 nh = add(add(scl(t1, p1), scl(t2, p2)), scl(vh, z));
+  return nrm(V(a * nh.x, a * nh.y, fmaxf(1e-6f, nh.z)));
+}
+static float power_h(float a, float b) {
+  if (!(a >= 0.0f) || !(b >= 0.0f) || a > 3.402823466e38f || b > 3.402823466e38f) return 0.0f;
+  float m = fmaxf(a, b);
+  if (!(m > 0.0f)) return 0.0f;
+  float x = a / m, y = b / m;
+  return (x * x) / (x * x + y * y);
+}
+static void bsdf_eval(const orc_mat_t* m, v3 wo, v3 wi, v3* fc, float* pdf) {
+  *fc = V(0, 0, 0);
+  *pdf = 0.0f;
+  if (wi.z <= 0.0f || wo.z <= 0.0f) return;
+  if (m->kind == 0) {
+    *fc = scl(V(m->base[0], m->base[1], m->base[2]), wi.z / PI_F);
+    *pdf = wi.z / PI_F;
+  } else if (m->kind == 1) {
+    v3 h = nrm(add(wo, wi));
+    float d = ggx_d(h.z, m->alpha), go = ggx_g1(wo.z, m->alpha), gi = ggx_g1(wi.z, m->alpha);
+    v3 F = schlick(V(m->base[0], m->base[1], m->base[2]), fmaxf(0.0f, dot3(wo, h)));
+    *fc = scl(F, d * go * gi / (4.0f * wo.z));
+    *pdf = d * go / (4.0f * wo.z);
+  }
+}
+
+/* ---------------------------------------------------------------- lights */
+static int cdf_search(const float* cdf, int n, float u) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (cdf[mid] > u) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+static void env_texel(const orc_pt_t* S, v3 d, int* col, int* row, float* st) {
+  float y = fminf(fmaxf(d.y, -1.0f), 1.0f), theta = acosf(y), phi = atan2f(d.z, d.x);
+  if (phi < 0.0f) phi += 2.0f * PI_F;
+  *col = (int)(phi * (0.5f / PI_F) * S->env_w);
+  if (*col > S->env_w - 1) *col = S->env_w - 1;
+  *row = (int)(theta * (1.0f / PI_F) * S->env_h);
+  if (*row > S->env_h - 1) *row = S->env_h - 1;
+  *st = sinf(theta);
+}
+static float env_pdf(const orc_pt_t* S, int col, int row, float st) {
+  if (!(st > 0.0f)) return 0.0f;
+  float pm = S->env_marg[row + 1] - S->env_marg[row];
+  const float* cc = S->env_cond + (size_t)row * (S->env_w + 1);
+  float pc = cc[col + 1] - cc[col];
+  return pm * pc * (float)S->env_w * (float)S->env_h / (2.0f * PI_F * PI_F * st);
+}
+static v3 env_le(const orc_pt_t* S, int col, int row) {
+  const float* e = S->env + 3 * ((size_t)row * S->env_w + col);
+  return scl(V(e[0], e[1], e[2]), S->env_scale);
+}
+
+typedef struct { v3 wi, Le; float dist, pdf; int delta, valid; } lsample_t;
+
+static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
+  lsample_t ls;
+  memset(&ls, 0, sizeof ls);
+  float psel = 1.0f / (float)S->n_entries;
+  uint32_t e = rand_bounded(rng, (uint32_t)S->n_entries);
+  if (S->n_em > 0) {
+    if (e == 0) {
+      float u = rand01(rng);
+      int k = cdf_search(S->em_cdf, (int)S->n_em, u);
+      double A[3], B[3], C[3];
+      tri_vertices(S, S->em_tri[k], A, B, C);
+      float u1 = rand01(rng), u2 = rand01(rng), su = sqrtf(u1);
+      float wa = 1.0f - su, wb = su * (1.0f - u2), wc = su * u2;
+      v3 a = V((float)A[0], (float)A[1], (float)A[2]), b = V((float)B[0], (float)B[1], (float)B[2]),
+         c = V((float)C[0], (float)C[1], (float)C[2]);
+      v3 X = add(add(scl(a, wa), scl(b, wb)), scl(c, wc));
+      v3 nl = nrm(cross3(sub(b, a), sub(c, a)));
+      v3 d = sub(X, P);
+      float d2 = dot3(d, d), dist = sqrtf(d2);
+      ls.wi = scl(d, 1.0f / dist);
+      float cosl = -dot3(ls.wi, nl);
+      if (!(cosl > 0.0f) || !(dist > 0.0f)) return ls;
+      const orc_mat_t* m = &S->mats[S->tmat[S->em_tri[k]]];
+      ls.Le = V(m->emission[0], m->emission[1], m->emission[2]);
+      ls.dist = dist;
+      ls.pdf = psel * d2 / (S->em_area * cosl);
+      ls.valid = 1;
+      return ls;
+    }
+    e -= 1;
+  }
+  if ((long)e < S->n_points) {
+    const float* p = S->points + 6 * e;
+    v3 d = sub(V(p[0], p[1], p[2]), P);
+    float d2 = dot3(d, d);
+    if (!(d2 > 0.0f)) return ls;
+    float dist = sqrtf(d2);
+    ls.wi = scl(d, 1.0f / dist);
+    ls.dist = dist;
+    ls.Le = scl(V(p[3], p[4], p[5]), 1.0f / d2);
+    ls.pdf = psel;
+    ls.delta = 1;
+    ls.valid = 1;
+    return ls;
+  }
+  float u1 = rand01(rng), u2 = rand01(rng);
+  int row = cdf_search(S->env_marg + 1, S->env_h, u1);
+  const float* cc = S->env_cond + (size_t)row * (S->env_w + 1);
+  int col = cdf_search(cc + 1, S->env_w, u2);
+  float m0 = S->env_marg[row], m1 = S->env_marg[row + 1], c0 = cc[col], c1 = cc[col + 1];
+  float fv = m1 > m0 ? (u1 - m0) / (m1 - m0) : 0.5f, fu = c1 > c0 ? (u2 - c0) / (c1 - c0) : 0.5f;
+  float v = ((float)row + fminf(fmaxf(fv, 0.0f), 0.999999f)) / (float)S->env_h;
+  float u = ((float)col + fminf(fmaxf(fu, 0.0f), 0.999999f)) / (float)S->env_w;
+  float theta = v * PI_F, phi = u * 2.0f * PI_F, st = sinf(theta);
+  ls.wi = V(st * cosf(phi), cosf(theta), st * sinf(phi));
+  ls.dist = INFINITY;
+  ls.Le = env_le(S, col, row);
+  ls.pdf = psel * env_pdf(S, col, row, st);
+  ls.valid = ls.pdf > 0.0f;
+  return ls;
+}
+
+/* ---------------------------------------------------------------- integrator */
+static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
+  uint32_t rng = pcg_init((uint32_t)x, (uint32_t)y, S->seed ^ sample);
+  float jx = rand01(&rng), jy = rand01(&rng);
+  float u = ((float)x + jx) / (float)S->width, vv = ((float)y + jy) / (float)S->height;
+  float nx = u * 2.0f - 1.0f, ny = 1.0f - vv * 2.0f;
+  const float* M = S->inv_vp;
+  float nf[4], fr[4];
+  for (int r = 0; r < 4; ++r) {
+    nf[r] = M[4 * r] * nx + M[4 * r + 1] * ny - M[4 * r + 2] + M[4 * r + 3];
+    fr[r] = M[4 * r] * nx + M[4 * r + 1] * ny + M[4 * r + 2] + M[4 * r + 3];
+  }
+  v3 o = V(nf[0] / nf[3], nf[1] / nf[3], nf[2] / nf[3]);
+  v3 d = nrm(sub(V(fr[0] / fr[3], fr[1] / fr[3], fr[2] / fr[3]), o));
+  v3 T = V(1, 1, 1), L = V(0, 0, 0);
+  int prev_delta = 1;
+  float prev_pdf = 0.0f;
+  for (int bounce = 0; bounce < S->max_bounces; ++bounce) {
+    int last = bounce + 1 >= S->max_bounces;
+    double od[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z}, t;
+    log_ray(S, 0, od, dd, INFINITY);
+    long tri = trace(S, od, dd, INFINITY, 0, &t);
+    if (tri < 0) {
+      if (S->env) {
+        int col, row;
+        float st;
+        env_texel(S, d, &col, &row, &st);
+        float w = 1.0f;
+        if (!prev_delta && S->env_sampleable) w = power_h(prev_pdf, env_pdf(S, col, row, st) / (float)S->n_entries);
+        L = add(L, scl(mul(T, env_le(S, col, row)), w));
+      }
+      break;
+    }
+    double A[3], B[3], C[3];
+    tri_vertices(S, tri, A, B, C);
+    v3 a = V((float)A[0], (float)A[1], (float)A[2]), b = V((float)B[0], (float)B[1], (float)B[2]),
+       c = V((float)C[0], (float)C[1], (float)C[2]);
+    v3 ng = nrm(cross3(sub(b, a), sub(c, a)));
+    const orc_mat_t* m = &S->mats[S->tmat[tri]];
+    float tf = (float)t;
+    v3 P = add(o, scl(d, tf));
+    float dn = dot3(d, ng);
+    int front = dn < 0.0f;
+    if (m->emissive && front) {
+      float w = 1.0f;
+      if (!prev_delta) {
+        float cosl = -dn;
+        float pl = cosl > 0.0f ? (1.0f / (float)S->n_entries) * tf * tf / (S->em_area * cosl) : 0.0f;
+        w = power_h(prev_pdf, pl);
+      }
+      L = add(L, scl(mul(T, V(m->emission[0], m->emission[1], m->emission[2])), w));
+    }
+    v3 n = front ? ng : scl(ng, -1.0f);
+    float off = S->bias * fmaxf(1.0f, fmaxf(fabsf(P.x), fmaxf(fabsf(P.y), fabsf(P.z))));
+    v3 wo = scl(d, -1.0f), tb, bb;
+    onb(n, &tb, &bb);
+    v3 wol = V(dot3(wo, tb), dot3(wo, bb), dot3(wo, n));
+    int alive = 0;
+    if (m->kind != 2) {
+      if (S->n_entries > 0) {
+        lsample_t ls = sample_light(S, P, &rng);
+        if (ls.valid) {
+          v3 wil = V(dot3(ls.wi, tb), dot3(ls.wi, bb), dot3(ls.wi, n)), fc;
+          float pb;
+          bsdf_eval(m, wol, wil, &fc, &pb);
+          if (maxc(fc) > 0.0f) {
+            float w = (ls.delta || last) ? 1.0f : power_h(ls.pdf, pb);
+            v3 cc = scl(mul(mul(T, fc), ls.Le), w / ls.pdf);
+            if (maxc(cc) > 0.0f) {
+              v3 so = add(P, scl(n, off));
+              double sod[3] = {so.x, so.y, so.z}, sdd[3] = {ls.wi.x, ls.wi.y, ls.wi.z}, st2;
+              double tmax = isinf(ls.dist) ? INFINITY : (double)(ls.dist * (1.0f - 1e-4f));
+              log_ray(S, 1, sod, sdd, tmax);
+              if (trace(S, sod, sdd, tmax, 1, &st2) < 0) L = add(L, cc);
+            }
+          }
+        }
+      }
+      if (!last) {
+        float u1 = rand01(&rng), u2 = rand01(&rng), pdf = 0.0f;
+        v3 wil = V(0, 0, 0), wgt = V(0, 0, 0);
+        if (m->kind == 0) {
+          float r = sqrtf(u1), phi = 2.0f * PI_F * u2;
+          wil = V(r * cosf(phi), r * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
+          pdf = wil.z / PI_F;
+          wgt = V(m->base[0], m->base[1], m->base[2]);
+        } else {
+          v3 hl = ggx_vndf(wol, m->alpha, u1, u2);
+          float oh = dot3(wol, hl);
+          wil = sub(scl(hl, 2.0f * oh), wol);
+          if (wil.z > 0.0f && oh > 0.0f) {
+            pdf = ggx_d(hl.z, m->alpha) * ggx_g1(wol.z, m->alpha) / (4.0f * wol.z);
+            wgt = scl(schlick(V(m->base[0], m->base[1], m->base[2]), oh), ggx_g1(wil.z, m->alpha));
+          }
+        }
+        if (pdf > 0.0f && maxc(wgt) > 0.0f) {
+          v3 wi = add(add(scl(tb, wil.x), scl(bb, wil.y)), scl(n, wil.z));
+          T = mul(T, wgt);
+          alive = 1;
+          o = add(P, scl(n, off));
+          d = wi;
+          prev_delta = 0;
+          prev_pdf = pdf;
+        }
+      }
+    } else if (!last) {
+      float eta = front ? m->ior : 1.0f / m->ior, cosi = wol.z;
+      float F = represented_bernoulli(fr_dielectric(cosi, eta));
+      v3 wi = V(0, 0, 0), wgt = V(1, 1, 1);
+      int refl = rand01(&rng) < F;
+      if (!refl) {
+        float s2t = fmaxf(0.0f, 1.0f - cosi * cosi) / (eta * eta);
+        if (s2t >= 1.0f) {
+          refl = 1;
+        } else {
+          float cost = sqrtf(1.0f - s2t);
+          wi = nrm(add(scl(d, 1.0f / eta), scl(n, cosi / eta - cost)));
+          wgt = scl(V(1, 1, 1), 1.0f / (eta * eta));
+        }
+      }
+      if (refl) wi = add(d, scl(n, 2.0f * cosi));
+      T = mul(T, wgt);
+      o = add(P, scl(n, off * (refl ? 1.0f : -1.0f)));
+      d = wi;
+      alive = 1;
+      prev_delta = 1;
+      prev_pdf = 0.0f;
+    }
+    if (alive && bounce > 2) {
+      float q = represented_bernoulli(fminf(fmaxf(maxc(T), 0.1f), 0.95f));
+      if (!(rand01(&rng) < q)) alive = 0;
+      else T = scl(T, 1.0f / q);
+    }
+    if (!alive) break;
+  }
+  return L;
+}
+
+typedef struct { orc_pt_t* S; long next; pthread_mutex_t mu; } pt_job_t;
+
+static void* pt_worker(void* arg) {
+  pt_job_t* j = (pt_job_t*)arg;
+  orc_pt_t* S = j->S;
+  long npx = (long)S->width * S->height;
+  for (;;) {
+    pthread_mutex_lock(&j->mu);
+    long p = j->next++;
+    pthread_mutex_unlock(&j->mu);
+    if (p >= npx) break;
+    int x = (int)(p % S->width), y = (int)(p / S->width);
+    double s[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+    for (int k = 0; k < S->spp; ++k) {
+      v3 L = radiance_sample(S, x, y, S->sample_base + (uint32_t)k);
+      double v[3] = {L.x, L.y, L.z};
+      for (int c = 0; c < 3; ++c) { s[c] += v[c]; q[c] += v[c] * v[c]; }
+    }
+    for (int c = 0; c < 3; ++c) { S->sum[3 * p + c] = s[c]; S->sq[3 * p + c] = q[c]; }
+  }
+  return NULL;
+}
+
+/*
+ * Render width x height pixels x spp samples.  materials: 12 floats each
+ * (base rgb 0-2, roughness 3, metallic 4, transmission 5, ior 6, emission rgb 7-9, pad);
+ * env: W*H*3 floats (NULL for none); points: 6 floats each.  Writes FP64
+ * sum and sum of squares (3 per pixel).  Returns 0, or -1 on a build error.
+ */
+int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
+                  const float* materials, int n_mat, const float* points, long n_points, const float* env,
+                  int env_w, int env_h, float env_scale, const float* inv_vp, int width, int height, int spp,
+                  int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
+                  double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals) {
+  orc_pt_t S;
+  memset(&S, 0, sizeof S);
+  S.pos = pos;
+  S.idx = idx;
+  S.tmat = tri_mat;
+  S.ntri = ntri;
+  S.nodes = (uint32_t*)malloc(sizeof(uint32_t) * 8 * (size_t)(2 * ntri + 1));
+  S.r2s = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));
+  long nn = orc_build_array_bvh(pos, nvert * 4, 4, idx, ntri, 4, 4, 16, 58, S.nodes, S.r2s);
+  if (nn < 0) { free(S.nodes); free(S.r2s); return -1; }
+  orc_mat_t* mats = (orc_mat_t*)calloc((size_t)n_mat, sizeof(orc_mat_t));
+  for (int i = 0; i < n_mat; ++i) {
+    const float* m = materials + 12 * i;
+    for (int k = 0; k < 3; ++k) { mats[i].base[k] = m[k]; mats[i].emission[k] = m[7 + k]; }
+    mats[i].roughness = m[3];
+    mats[i].ior = m[6] > 0 ? m[6] : 1.5f;
+    mats[i].kind = m[5] > 0 ? 2 : (m[4] >= 0.5f ? 1 : 0);
+    mats[i].alpha = fmaxf(m[3] * m[3], 1e-3f);
+    mats[i].emissive = m[7] > 0 || m[8] > 0 || m[9] > 0;
+  }
+  S.mats = mats;
+  uint32_t* em = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));
+  float* cdf = (float*)malloc(sizeof(float) * (size_t)(ntri + 1));
+  double total = 0.0;
+  long ne = 0;
+  for (long t = 0; t < ntri; ++t) {
+    if (!mats[tri_mat[t]].emissive) continue;
+    double a[3], b[3], c[3];
+    tri_vertices(&S, t, a, b, c);
+    double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+    double area = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+    if (!(area > 0.0)) continue;
+    em[ne] = (uint32_t)t;
+    total += area;
+    cdf[ne] = (float)total;
+    ++ne;
+  }
+  for (long i = 0; i < ne; ++i) cdf[i] = (float)(cdf[i] / total);
+  if (ne) cdf[ne - 1] = 1.0f;
+  S.em_tri = em;
+  S.em_cdf = cdf;
+  S.n_em = ne;
+  S.em_area = (float)total;
+  S.points = points;
+  S.n_points = n_points;
+  float *marg = NULL, *cond = NULL;
+  if (env) {
+    S.env = env;
+    S.env_w = env_w;
+    S.env_h = env_h;
+    S.env_scale = env_scale > 0 ? env_scale : 1.0f;
+    marg = (float*)malloc(sizeof(float) * (size_t)(env_h + 1));
+    cond = (float*)malloc(sizeof(float) * (size_t)env_h * (env_w + 1));
+    double tot = 0.0;
+    double* rows = (double*)malloc(sizeof(double) * (size_t)env_h);
+    double* cum = (double*)malloc(sizeof(double) * (size_t)env_w);
+    for (int r = 0; r < env_h; ++r) {
+      double st = sin(M_PI * (r + 0.5) / env_h), acc = 0.0;
+      cond[(size_t)r * (env_w + 1)] = 0.0f;
+      for (int c = 0; c < env_w; ++c) {
+        const float* px = env + 3 * ((size_t)r * env_w + c);
+        double lum = 0.2126 * px[0] + 0.7152 * px[1] + 0.0722 * px[2];
+        acc += fmax(0.0, lum * S.env_scale) * st;
+        cum[c] = acc;
+      }
+      for (int c = 0; c < env_w; ++c)
+        cond[(size_t)r * (env_w + 1) + c + 1] = acc > 0 ? (float)(cum[c] / acc) : (float)(c + 1) / env_w;
+      cond[(size_t)r * (env_w + 1) + env_w] = 1.0f;
+      rows[r] = acc;
+      tot += acc;
+    }
+    marg[0] = 0.0f;
+    double run = 0.0;
+    for (int r = 0; r < env_h; ++r) {
+      run += rows[r];
+      marg[r + 1] = tot > 0 ? (float)(run / tot) : (float)(r + 1) / env_h;
+    }
+    marg[env_h] = 1.0f;
+    S.env_marg = marg;
+    S.env_cond = cond;
+    S.env_sampleable = tot > 0.0;
+    free(rows);
+    free(cum);
+  }
+  S.n_entries = (ne ? 1 : 0) + (int)n_points + (S.env_sampleable ? 1 : 0);
+  S.bias = bias;
+  S.inv_vp = inv_vp;
+  S.width = width;
+  S.height = height;
+  S.max_bounces = max_bounces;
+  S.seed = seed;
+  S.sample_base = sample_base;
+  S.spp = spp;
+  S.sum = sum;
+  S.sq = sq;
+  S.log_closest = log_closest;
+  S.log_shadow = log_shadow;
+  S.log_cap = log_cap;
+  pt_job_t job;
+  job.S = &S;
+  job.next = 0;
+  pthread_mutex_init(&job.mu, NULL);
+  if (nthreads <= 0) nthreads = orc_hw_threads();
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  for (int i = 0; i < nthreads; ++i) pthread_create(&th[i], NULL, pt_worker, &job);
+  for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
+  pthread_mutex_destroy(&job.mu);
+  if (ray_totals) { ray_totals[0] = S.n_closest; ray_totals[1] = S.n_shadow; }
+  free(S.nodes);
+  free(S.r2s);
+  free(mats);
+  free(em);
+  free(cdf);
+  free(marg);
+  free(cond);
+  return 0;
+}

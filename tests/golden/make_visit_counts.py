@@ -30,6 +30,23 @@ def main():
         "v_node": nn / n, "v_tri": nt / n,
         "bytes_per_ray": 32 + 16 + 80 * nn / n + 48 * nt / n,
     }
+    # path-tracing rays of the box room (512^2 / 64 spp / 5 bounces workload):
+    # rays logged by the CPU path tracer at 128 x 128, 4 spp, same camera
+    sc, cam = scenes.box_room()
+    _, _, lc, ls, (nc, ns) = oracle.pt_render(sc, cam, 128, 128, 4, 5, log_rays=1 << 20)
+    pos, idx, _, _, _, _, _ = oracle.flatten_scene(sc)
+    wb = oracle.build_compressed_wide_bvh(pos, idx)
+    cn, ct = oracle.count_visits(wb, pos, lc)
+    sn, st = oracle.count_visits(wb, pos, ls, any_hit=True)
+    out["box_room_pt_512_64spp_5b"] = {
+        "sample": "128x128 pixels, 4 spp, 5 bounces (CPU path tracer, same estimator and camera)",
+        "paths": 128 * 128 * 4, "closest_rays": nc, "shadow_rays": ns,
+        "closest_per_path": nc / (128 * 128 * 4), "shadow_per_path": ns / (128 * 128 * 4),
+        "closest_v_node": cn / len(lc), "closest_v_tri": ct / len(lc),
+        "shadow_v_node": sn / len(ls), "shadow_v_tri": st / len(ls),
+        "closest_bytes_per_ray": 32 + 16 + 80 * cn / len(lc) + 48 * ct / len(lc),
+        "shadow_bytes_per_ray": 32 + 16 + 80 * sn / len(ls) + 48 * st / len(ls),
+    }
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "visit_counts.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)

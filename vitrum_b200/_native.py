@@ -62,6 +62,16 @@ SIGNATURES = {
     "vt_bvh_destroy": [P],
     "vt_bvh_trace_closest_noalloc": [P, P, SZ, P],
     "vt_watertight_eval_device": [I32, P, SZ, P, P],
+    "vt_create": [I32, P, P],
+    "vt_set_scene": [P, P],
+    "vt_render_frame": [P, P, P],
+    "vt_profile_frame": [P, P, P, P],
+    "vt_capture": [P, P, SZ],
+    "vt_capture_moments": [P, P, P, SZ],
+    "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
+    "vt_reset": [P],
+    "vt_engine_get_stats": [P, P],
+    "vt_destroy": [P],
 }
 _RESTYPE = {"vt_last_error": ctypes.c_char_p, "vt_version": ctypes.c_char_p}
 

@@ -1,0 +1,748 @@
+// api_engine.cu -- the path-tracing engine behind the vitrum Engine contract.
+//
+// vt_create / vt_set_scene / vt_render_frame / vt_capture / vt_pick /
+// vt_reset / vt_destroy mirror createPTEngine_WebGPU and the @vitrum/core
+// Engine methods (packages/core/src/engine/index.ts:109-466,
+// packages/pt-webgpu/src/index.ts:418-2363).  A frame is rendered as waves
+// of width*height*spp_wave paths; each wave's launches (raygen, per bounce:
+// extend, material sort, shade, shadow, resolve; accumulate) are captured
+// once into a CUDA graph and replayed, the wave's sample offset living in
+// device memory so replays need no parameter updates.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "bvh_host.h"
+#include "pt_kernels.h"
+#include "traverse.h"
+#include "vt_common.h"
+
+using vt::DeviceBuffer;
+using vt::fail;
+
+struct vt_engine {
+  int device = 0;
+  vt_engine_options opts{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // scene
+  bool has_scene = false;
+  vt::BinaryBvhHost binary;
+  DeviceBuffer<uint4> nodes;
+  DeviceBuffer<float4> tris;
+  int wide_depth = 1;
+  DeviceBuffer<vt::pt::Material> materials;
+  DeviceBuffer<float4> emitters;
+  DeviceBuffer<float> emitter_cdf;
+  DeviceBuffer<float4> points;
+  DeviceBuffer<float4> env;
+  DeviceBuffer<float> env_marginal, env_conditional;
+  vt::pt::SceneView view;
+  int64_t ntri = 0, n_emitters = 0;
+  // accumulation
+  int width = 0, height = 0;
+  DeviceBuffer<float4> accum;
+  DeviceBuffer<double> sum64, sq64;
+  int samples = 0;
+  float inv_vp[16] = {};
+  float view_m[16] = {}, proj_m[16] = {};
+  bool have_camera = false;
+  uint32_t frame_seed = 0;
+  // wave buffers
+  uint32_t capacity = 0;
+  DeviceBuffer<float4> rays[2], through[2];
+  DeviceBuffer<uint4> state[2];
+  DeviceBuffer<int4> hits;
+  DeviceBuffer<uint32_t> order, keys, counters;
+  DeviceBuffer<float4> shadow_rays, shadow_contrib, radiance;
+  DeviceBuffer<uint8_t> occluded;
+  DeviceBuffer<unsigned long long> trace_counter, totals;
+  DeviceBuffer<int> trace_status;
+  // graph cache: one executable per spp_wave value
+  struct Graph {
+    uint32_t spp_wave = 0, bounces = 0;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<Graph> graphs;
+  double last_ms = 0.0;
+  // pick
+  DeviceBuffer<float4> pick_ray;
+  DeviceBuffer<int4> pick_hit;
+  DeviceBuffer<int> pick_status;
+  DeviceBuffer<unsigned long long> pick_counter;
+
+  void drop_graphs() {
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
+  ~vt_engine() {
+    drop_graphs();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// ---------------------------------------------------------------- matrices
+void mat_mul_cm(const double* a, const double* b, double* out) {  // column-major 4x4: out = a * b
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += a[k * 4 + r] * b[c * 4 + k];
+      out[c * 4 + r] = s;
+    }
+}
+
+bool invert4(const double* m, double* inv) {  // any layout, Gauss-Jordan with partial pivoting
+  double a[4][8];
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      a[r][c] = m[r * 4 + c];
+      a[r][c + 4] = r == c ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < 4; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 4; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+    if (!(std::fabs(a[piv][c]) > 1e-300)) return false;
+    if (piv != c)
+      for (int k = 0; k < 8; ++k) std::swap(a[c][k], a[piv][k]);
+    const double d = a[c][c];
+    for (int k = 0; k < 8; ++k) a[c][k] /= d;
+    for (int r = 0; r < 4; ++r) {
+      if (r == c) continue;
+      const double f = a[r][c];
+      for (int k = 0; k < 8; ++k) a[r][k] -= f * a[c][k];
+    }
+  }
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) inv[r * 4 + c] = a[r][c + 4];
+  return true;
+}
+
+// inverse(P * V) as a row-major float matrix
+void inverse_view_proj(const float* view, const float* proj, float* out_rm) {
+  double v[16], p[16], vp[16], rm[16], inv[16];
+  for (int i = 0; i < 16; ++i) { v[i] = view[i]; p[i] = proj[i]; }
+  mat_mul_cm(p, v, vp);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) rm[r * 4 + c] = vp[c * 4 + r];
+  if (!invert4(rm, inv)) fail(VT_ERR_INVALID_ARGUMENT, "camera view-projection matrix is singular");
+  for (int i = 0; i < 16; ++i) out_rm[i] = (float)inv[i];
+}
+
+double luminance(const float* c) { return 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]; }
+
+template <class T>
+void upload(DeviceBuffer<T>& dst, const std::vector<T>& src, cudaStream_t s) {
+  dst.resize(std::max<size_t>(src.size(), 1));
+  if (!src.empty()) VT_CUDA(cudaMemcpyAsync(dst.ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+// ---------------------------------------------------------------- scene
+void set_scene(vt_engine* e, const vt_scene_desc* sc) {
+  if (!sc) fail(VT_ERR_INVALID_ARGUMENT, "scene is null");
+  if (sc->mesh_count && !sc->meshes) fail(VT_ERR_INVALID_ARGUMENT, "meshes is null");
+  if (sc->material_count && !sc->materials) fail(VT_ERR_INVALID_ARGUMENT, "materials is null");
+  if (sc->point_light_count && !sc->point_lights) fail(VT_ERR_INVALID_ARGUMENT, "point_lights is null");
+  std::vector<float> pos;
+  std::vector<uint32_t> idx, tri_mat;
+  for (size_t m = 0; m < sc->mesh_count; ++m) {
+    const vt_mesh_desc& md = sc->meshes[m];
+    if (md.material >= sc->material_count)
+      fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " references material " + std::to_string(md.material));
+    if ((md.vertex_count && !md.positions) || (md.triangle_count && !md.indices))
+      fail(VT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(m) + " has null arrays");
+    const uint32_t base = (uint32_t)(pos.size() / 4);
+    for (size_t v = 0; v < md.vertex_count; ++v) {
+      for (int k = 0; k < 3; ++k) {
+        const float x = md.positions[3 * v + k];
+        if (!std::isfinite(x)) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " has a non-finite position");
+        pos.push_back(x);
+      }
+      pos.push_back(0.0f);
+    }
+    for (size_t t = 0; t < md.triangle_count; ++t) {
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t i = md.indices[3 * t + k];
+        if (i >= md.vertex_count) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " index out of range");
+        idx.push_back(base + i);
+      }
+      idx.push_back(0u);
+      tri_mat.push_back(md.material);
+    }
+  }
+  // materials
+  std::vector<vt::pt::Material> mats(sc->material_count);
+  for (size_t i = 0; i < sc->material_count; ++i) {
+    const vt_material_desc& d = sc->materials[i];
+    vt::pt::Material& m = mats[i];
+    m.base_color = make_float3(d.base_color[0], d.base_color[1], d.base_color[2]);
+    m.roughness = d.roughness;
+    m.emission = make_float3(d.emission[0], d.emission[1], d.emission[2]);
+    m.ior = d.ior > 0.0f ? d.ior : 1.5f;
+    m.kind = d.transmission > 0.0f ? vt::pt::kDielectric
+                                   : (d.metallic >= 0.5f ? vt::pt::kConductor : vt::pt::kLambert);
+    m.alpha = std::max(d.roughness * d.roughness, 1e-3f);
+    m.emissive = (d.emission[0] > 0.0f || d.emission[1] > 0.0f || d.emission[2] > 0.0f) ? 1u : 0u;
+    m.pad = 0;
+  }
+  // geometry
+  vt::BuildOptions bo;
+  e->binary = vt::build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
+  vt::WideBvhHost w = vt::encode_wide(e->binary, pos.data(), 4, idx.data(), 4, tri_mat.data());
+  const size_t ntri = tri_mat.size();
+  // emissive triangles, sampled uniformly over their total area
+  std::vector<float4> em;
+  std::vector<float> cdf;
+  double total = 0.0;
+  for (size_t t = 0; t < ntri; ++t) {
+    if (!mats[tri_mat[t]].emissive) continue;
+    const float* a = &pos[4 * idx[4 * t]];
+    const float* b = &pos[4 * idx[4 * t + 1]];
+    const float* c = &pos[4 * idx[4 * t + 2]];
+    const double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+    const double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+    const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                 cz = e1[0] * e2[1] - e1[1] * e2[0];
+    const double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+    if (!(area > 0.0)) continue;
+    uint32_t mb = tri_mat[t];
+    float mf;
+    std::memcpy(&mf, &mb, 4);
+    em.push_back(make_float4(a[0], a[1], a[2], mf));
+    em.push_back(make_float4(b[0], b[1], b[2], (float)area));
+    em.push_back(make_float4(c[0], c[1], c[2], 0.0f));
+    total += area;
+    cdf.push_back((float)total);
+  }
+  for (float& x : cdf) x = (float)(x / total);
+  if (!cdf.empty()) cdf.back() = 1.0f;
+  // point lights
+  std::vector<float4> pts;
+  for (size_t i = 0; i < sc->point_light_count; ++i) {
+    const vt_point_light_desc& p = sc->point_lights[i];
+    pts.push_back(make_float4(p.position[0], p.position[1], p.position[2], 0.0f));
+    pts.push_back(make_float4(p.intensity[0], p.intensity[1], p.intensity[2], 0.0f));
+  }
+  // environment: equirectangular, importance by luminance * sin(theta)
+  std::vector<float4> envt;
+  std::vector<float> marg, cond;
+  const bool has_env = sc->environment_rgb && sc->environment_width > 0 && sc->environment_height > 0;
+  bool env_sampleable = false;
+  if (has_env) {
+    const int W = sc->environment_width, H = sc->environment_height;
+    const float scale = sc->environment_intensity > 0.0f ? sc->environment_intensity : 1.0f;
+    envt.resize((size_t)W * H);
+    cond.resize((size_t)H * (W + 1));
+    marg.resize(H + 1);
+    std::vector<double> rows(H);
+    double tot = 0.0;
+    for (int r = 0; r < H; ++r) {
+      const double st = std::sin(M_PI * (r + 0.5) / H);
+      double acc = 0.0;
+      cond[(size_t)r * (W + 1)] = 0.0f;
+      std::vector<double> cum(W);
+      for (int c = 0; c < W; ++c) {
+        const float* px = sc->environment_rgb + 3 * ((size_t)r * W + c);
+        envt[(size_t)r * W + c] = make_float4(px[0], px[1], px[2], 0.0f);
+        acc += std::max(0.0, luminance(px) * scale) * st;
+        cum[c] = acc;
+      }
+      for (int c = 0; c < W; ++c) cond[(size_t)r * (W + 1) + c + 1] = acc > 0 ? (float)(cum[c] / acc) : (float)(c + 1) / W;
+      cond[(size_t)r * (W + 1) + W] = 1.0f;
+      rows[r] = acc;
+      tot += acc;
+    }
+    marg[0] = 0.0f;
+    double run = 0.0;
+    for (int r = 0; r < H; ++r) {
+      run += rows[r];
+      marg[r + 1] = tot > 0 ? (float)(run / tot) : (float)(r + 1) / H;
+    }
+    marg[H] = 1.0f;
+    env_sampleable = tot > 0.0;
+  }
+  cudaStream_t s = e->stream;
+  VT_CUDA(cudaStreamSynchronize(s));
+  e->drop_graphs();
+  e->nodes.resize(w.nodes.size() / 4);
+  VT_CUDA(cudaMemcpyAsync(e->nodes.ptr, w.nodes.data(), w.nodes.size() * 4, cudaMemcpyHostToDevice, s));
+  e->tris.resize(std::max<size_t>(w.tris.size() / 4, 1));
+  if (!w.tris.empty()) VT_CUDA(cudaMemcpyAsync(e->tris.ptr, w.tris.data(), w.tris.size() * 4, cudaMemcpyHostToDevice, s));
+  e->wide_depth = w.depth;
+  upload(e->materials, mats, s);
+  upload(e->emitters, em, s);
+  upload(e->emitter_cdf, cdf, s);
+  upload(e->points, pts, s);
+  upload(e->env, envt, s);
+  upload(e->env_marginal, marg, s);
+  upload(e->env_conditional, cond, s);
+  VT_CUDA(cudaStreamSynchronize(s));
+  vt::pt::SceneView v;
+  v.nodes = e->nodes.ptr;
+  v.tris = e->tris.ptr;
+  v.stack_depth = 2 * w.depth + 2;
+  v.materials = e->materials.ptr;
+  v.material_count = (uint32_t)mats.size();
+  v.emitters = e->emitters.ptr;
+  v.emitter_cdf = e->emitter_cdf.ptr;
+  v.n_emitters = (uint32_t)cdf.size();
+  v.emit_area_total = (float)total;
+  v.points = e->points.ptr;
+  v.n_points = (uint32_t)(pts.size() / 2);
+  v.env = has_env ? e->env.ptr : nullptr;
+  v.env_marginal = env_sampleable ? e->env_marginal.ptr : nullptr;
+  v.env_conditional = env_sampleable ? e->env_conditional.ptr : nullptr;
+  v.env_w = has_env ? sc->environment_width : 0;
+  v.env_h = has_env ? sc->environment_height : 0;
+  v.env_scale = sc->environment_intensity > 0.0f ? sc->environment_intensity : 1.0f;
+  v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + (env_sampleable ? 1u : 0u);
+  e->view = v;
+  e->ntri = (int64_t)ntri;
+  e->n_emitters = (int64_t)v.n_emitters;
+  e->has_scene = true;
+  e->samples = 0;
+  if (e->accum.ptr) VT_CUDA(cudaMemset(e->accum.ptr, 0, e->accum.bytes()));
+  if (e->sum64.ptr) VT_CUDA(cudaMemset(e->sum64.ptr, 0, e->sum64.bytes()));
+  if (e->sq64.ptr) VT_CUDA(cudaMemset(e->sq64.ptr, 0, e->sq64.bytes()));
+}
+
+// ---------------------------------------------------------------- waves
+void ensure_capacity(vt_engine* e, uint32_t cap) {
+  if (e->capacity >= cap) return;
+  e->drop_graphs();
+  for (int q = 0; q < 2; ++q) {
+    e->rays[q].resize(2 * (size_t)cap);
+    e->through[q].resize(cap);
+    e->state[q].resize(cap);
+  }
+  e->hits.resize(cap);
+  e->order.resize(cap);
+  e->keys.resize(cap);
+  e->shadow_rays.resize(2 * (size_t)cap);
+  e->shadow_contrib.resize(cap);
+  e->occluded.resize(cap);
+  e->radiance.resize(cap);
+  e->capacity = cap;
+}
+
+vt::pt::WaveBuffers wave_buffers(vt_engine* e) {
+  vt::pt::WaveBuffers w;
+  for (int q = 0; q < 2; ++q) {
+    w.rays[q] = e->rays[q].ptr;
+    w.state[q] = e->state[q].ptr;
+    w.through[q] = e->through[q].ptr;
+  }
+  w.hits = e->hits.ptr;
+  w.order = e->order.ptr;
+  w.keys = e->keys.ptr;
+  w.shadow_rays = e->shadow_rays.ptr;
+  w.shadow_contrib = e->shadow_contrib.ptr;
+  w.occluded = e->occluded.ptr;
+  w.radiance = e->radiance.ptr;
+  w.counters = e->counters.ptr;
+  w.trace_counter = e->trace_counter.ptr;
+  w.trace_status = e->trace_status.ptr;
+  return w;
+}
+
+// Optional per-stage event pairs (profiling; never used while capturing a graph).
+struct StageTimer {
+  enum Stage { kRaygen, kTraceClosest, kSort, kShade, kTraceShadow, kResolve, kAccumulate, kStages };
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  int open_stage = -1;
+  cudaEvent_t open_ev = nullptr;
+  int launches[kStages] = {};
+  void begin(int st, cudaStream_t s) {
+    cudaEventCreate(&open_ev);
+    cudaEventRecord(open_ev, s);
+    open_stage = st;
+  }
+  void end(cudaStream_t s) {
+    cudaEvent_t e1;
+    cudaEventCreate(&e1);
+    cudaEventRecord(e1, s);
+    marks.push_back({open_stage, {open_ev, e1}});
+    launches[open_stage] += 1;
+  }
+  void collect(double* ms) {
+    for (auto& m : marks) {
+      float x = 0.0f;
+      cudaEventElapsedTime(&x, m.second.first, m.second.second);
+      ms[m.first] += x;
+      cudaEventDestroy(m.second.first);
+      cudaEventDestroy(m.second.second);
+    }
+    marks.clear();
+  }
+};
+
+void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t s, StageTimer* tm = nullptr) {
+  auto B = [&](int st) { if (tm) tm->begin(st, s); };
+  auto E = [&]() { if (tm) tm->end(s); };
+  vt::pt::FrameView f;
+  std::memcpy(f.inv_vp, e->inv_vp, sizeof f.inv_vp);
+  f.width = (uint32_t)e->width;
+  f.height = (uint32_t)e->height;
+  f.frame_seed = e->frame_seed;
+  f.spp_wave = spp_wave;
+  f.max_bounces = bounces;
+  f.paths = f.width * f.height * spp_wave;
+  f.sort_by_material = e->opts.sort_by_material >= 0 ? 1u : 0u;
+  const vt::pt::WaveBuffers w = wave_buffers(e);
+  vt::pt::AccumView a;
+  a.accum = e->accum.ptr;
+  a.sum64 = e->sum64.ptr;
+  a.sq64 = e->sq64.ptr;
+  const uint32_t cap = f.paths;
+  B(StageTimer::kRaygen);
+  vt::pt::launch_raygen(f, w, s);
+  E();
+  int cur = 0;
+  for (uint32_t b = 0; b < bounces; ++b) {
+    vt::TraceArgs t;
+    t.nodes = e->nodes.ptr;
+    t.tris = e->tris.ptr;
+    t.rays = w.rays[cur];
+    t.n = cap;
+    t.hits = w.hits;
+    t.status = e->trace_status.ptr;
+    t.counter = e->trace_counter.ptr;
+    t.stack_depth = 2 * e->wide_depth + 2;
+    t.n_dev = w.counters + cur;
+    B(StageTimer::kTraceClosest);
+    vt::launch_trace_closest_records(t, s);
+    E();
+    if (f.sort_by_material) {
+      B(StageTimer::kSort);
+      vt::pt::launch_sort_by_material(e->view, w, cur, cap, s);
+      E();
+    }
+    B(StageTimer::kShade);
+    vt::pt::launch_shade(e->view, f, w, cur, b, cap, s);
+    E();
+    vt::TraceArgs sh = t;
+    sh.rays = w.shadow_rays;
+    sh.hits = nullptr;
+    sh.occluded = w.occluded;
+    sh.n_dev = w.counters + vt::pt::kCntShadow;
+    B(StageTimer::kTraceShadow);
+    vt::launch_trace_any(sh, s);
+    E();
+    B(StageTimer::kResolve);
+    vt::pt::launch_shadow_resolve(w, cap, s);
+    vt::pt::launch_count_rays(w, cur, e->totals.ptr, s);
+    E();
+    cur ^= 1;
+  }
+  B(StageTimer::kAccumulate);
+  vt::pt::launch_accumulate(f, w, a, s);
+  E();
+}
+
+cudaGraphExec_t wave_graph(vt_engine* e, uint32_t spp_wave, uint32_t bounces) {
+  for (auto& g : e->graphs)
+    if (g.spp_wave == spp_wave && g.bounces == bounces) return g.exec;
+  cudaGraph_t graph = nullptr;
+  VT_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  record_wave(e, spp_wave, bounces, e->stream);
+  VT_CUDA(cudaStreamEndCapture(e->stream, &graph));
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  VT_CUDA(err);
+  e->graphs.push_back({spp_wave, bounces, exec});
+  return exec;
+}
+
+void reset_accumulation(vt_engine* e) {
+  e->samples = 0;
+  if (e->accum.ptr) VT_CUDA(cudaMemsetAsync(e->accum.ptr, 0, e->accum.bytes(), e->stream));
+  if (e->sum64.ptr) VT_CUDA(cudaMemsetAsync(e->sum64.ptr, 0, e->sum64.bytes(), e->stream));
+  if (e->sq64.ptr) VT_CUDA(cudaMemsetAsync(e->sq64.ptr, 0, e->sq64.bytes(), e->stream));
+  VT_CUDA(cudaMemsetAsync(e->counters.ptr, 0, e->counters.bytes(), e->stream));
+}
+
+void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, double* stage_ms = nullptr,
+                  int* stage_launches = nullptr) {
+  if (!in || !out) fail(VT_ERR_INVALID_ARGUMENT, "input and output must be non-null");
+  if (!e->has_scene) fail(VT_ERR_STATE, "renderFrame before setScene");
+  if (in->width <= 0 || in->height <= 0 || in->width > 16384 || in->height > 16384)
+    fail(VT_ERR_RANGE, "viewport must be 1..16384 pixels per side");
+  if (in->samples < 0) fail(VT_ERR_RANGE, "samples must be >= 0");
+  const int maxb = e->opts.max_bounces;
+  const uint32_t bounces = (uint32_t)std::min(in->bounces > 0 ? in->bounces : maxb, maxb);
+  float ivp[16];
+  inverse_view_proj(in->view, in->projection, ivp);
+  const bool size_changed = in->width != e->width || in->height != e->height;
+  const bool cam_changed = !e->have_camera || std::memcmp(ivp, e->inv_vp, sizeof ivp) != 0 ||
+                           in->frame_seed != e->frame_seed;
+  if (size_changed) {
+    e->width = in->width;
+    e->height = in->height;
+    const size_t px = (size_t)in->width * in->height;
+    e->accum.resize(px);
+    if (e->opts.oracle_accumulation) {
+      e->sum64.resize(3 * px);
+      e->sq64.resize(3 * px);
+    }
+  }
+  if (size_changed || cam_changed) {
+    std::memcpy(e->inv_vp, ivp, sizeof ivp);
+    std::memcpy(e->view_m, in->view, sizeof e->view_m);
+    std::memcpy(e->proj_m, in->projection, sizeof e->proj_m);
+    e->frame_seed = in->frame_seed;
+    e->have_camera = true;
+    e->drop_graphs();
+    reset_accumulation(e);
+  }
+  const int room = e->opts.max_samples_per_pixel - e->samples;
+  out->width = e->width;
+  out->height = e->height;
+  out->radiance_device = e->accum.ptr;
+  if (room <= 0 || in->samples == 0) {
+    out->kind = room <= 0 ? 1 : 0;
+    out->samples_accumulated = e->samples;
+    out->is_converged = room <= 0 ? 1 : 0;
+    return;
+  }
+  const uint32_t spp = (uint32_t)std::min(in->samples, room);
+  const uint32_t wh = (uint32_t)(e->width * e->height);
+  const uint32_t wave_paths = e->opts.wave_paths > 0 ? (uint32_t)e->opts.wave_paths : (1u << 21);
+  uint32_t spp_wave = std::max<uint32_t>(1u, wave_paths / wh);
+  spp_wave = std::min(spp_wave, spp);
+  while (spp % spp_wave) --spp_wave;  // equal waves: one graph per frame shape
+  ensure_capacity(e, wh * spp_wave);
+  if (stage_ms) {
+    // profiling: the same launches, issued directly with events between stages
+    StageTimer tm;
+    VT_CUDA(cudaEventRecord(e->ev0, e->stream));
+    for (uint32_t done = 0; done < spp; done += spp_wave) record_wave(e, spp_wave, bounces, e->stream, &tm);
+    VT_CUDA(cudaEventRecord(e->ev1, e->stream));
+    VT_CUDA(cudaEventSynchronize(e->ev1));
+    VT_CUDA(cudaGetLastError());
+    tm.collect(stage_ms);
+    for (int k = 0; k < StageTimer::kStages; ++k) stage_launches[k] += tm.launches[k];
+  } else {
+    cudaGraphExec_t g = wave_graph(e, spp_wave, bounces);
+    VT_CUDA(cudaEventRecord(e->ev0, e->stream));
+    for (uint32_t done = 0; done < spp; done += spp_wave) VT_CUDA(cudaGraphLaunch(g, e->stream));
+    VT_CUDA(cudaEventRecord(e->ev1, e->stream));
+    VT_CUDA(cudaEventSynchronize(e->ev1));
+  }
+  float ms = 0.0f;
+  VT_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+  e->last_ms = ms;
+  int st = 0;
+  VT_CUDA(cudaMemcpy(&st, e->trace_status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+  e->samples += (int)spp;
+  out->kind = 0;
+  out->samples_accumulated = e->samples;
+  out->is_converged = e->samples >= e->opts.max_samples_per_pixel ? 1 : 0;
+}
+
+void camera_ray(const vt_engine* e, float x, float y, float* ray8) {
+  const float nx = (x / e->width) * 2.0f - 1.0f, ny = 1.0f - (y / e->height) * 2.0f;
+  const float* M = e->inv_vp;
+  double nf[4], fr[4];
+  for (int r = 0; r < 4; ++r) {
+    nf[r] = (double)M[4 * r] * nx + (double)M[4 * r + 1] * ny - M[4 * r + 2] + M[4 * r + 3];
+    fr[r] = (double)M[4 * r] * nx + (double)M[4 * r + 1] * ny + M[4 * r + 2] + M[4 * r + 3];
+  }
+  double o[3], d[3], l = 0;
+  for (int k = 0; k < 3; ++k) {
+    o[k] = nf[k] / nf[3];
+    d[k] = fr[k] / fr[3] - o[k];
+    l += d[k] * d[k];
+  }
+  l = std::sqrt(l);
+  for (int k = 0; k < 3; ++k) { ray8[k] = (float)o[k]; ray8[4 + k] = (float)(d[k] / l); }
+  ray8[3] = 0.0f;
+  ray8[7] = INFINITY;
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine** out_engine) {
+  return vt::guard([&] {
+    if (!out_engine) fail(VT_ERR_INVALID_ARGUMENT, "out_engine is null");
+    *out_engine = nullptr;
+    auto e = std::make_unique<vt_engine>();
+    e->device = device;
+    if (options) e->opts = *options;
+    if (e->opts.max_bounces == 0) e->opts.max_bounces = 8;
+    if (e->opts.max_bounces < 1 || e->opts.max_bounces > 8) fail(VT_ERR_RANGE, "max_bounces must be in [1, 8]");
+    if (e->opts.max_samples_per_pixel == 0) e->opts.max_samples_per_pixel = 4096;
+    if (e->opts.max_samples_per_pixel < 1) fail(VT_ERR_RANGE, "max_samples_per_pixel must be >= 1");
+    if (e->opts.wave_paths < 0) fail(VT_ERR_RANGE, "wave_paths must be >= 0");
+    vt::DeviceScope ds(device);
+    VT_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    VT_CUDA(cudaEventCreate(&e->ev0));
+    VT_CUDA(cudaEventCreate(&e->ev1));
+    e->counters.resize(vt::pt::kCntWords);
+    VT_CUDA(cudaMemset(e->counters.ptr, 0, e->counters.bytes()));
+    e->trace_counter.resize(1);
+    e->trace_status.resize(1);
+    VT_CUDA(cudaMemset(e->trace_status.ptr, 0, sizeof(int)));
+    e->totals.resize(2);
+    VT_CUDA(cudaMemset(e->totals.ptr, 0, e->totals.bytes()));
+    *out_engine = e.release();
+  });
+}
+
+vt_status vt_set_scene(vt_engine* e, const vt_scene_desc* scene) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    vt::DeviceScope ds(e->device);
+    set_scene(e, scene);
+  });
+}
+
+vt_status vt_render_frame(vt_engine* e, const vt_frame_input* input, vt_frame_output* output) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    vt::DeviceScope ds(e->device);
+    render_frame(e, input, output);
+  });
+}
+
+vt_status vt_profile_frame(vt_engine* e, const vt_frame_input* input, vt_frame_output* output,
+                           vt_stage_times* times) {
+  return vt::guard([&] {
+    if (!e || !times) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    vt::DeviceScope ds(e->device);
+    double ms[StageTimer::kStages] = {};
+    int launches[StageTimer::kStages] = {};
+    render_frame(e, input, output, ms, launches);
+    times->raygen_ms = ms[StageTimer::kRaygen];
+    times->trace_closest_ms = ms[StageTimer::kTraceClosest];
+    times->sort_ms = ms[StageTimer::kSort];
+    times->shade_ms = ms[StageTimer::kShade];
+    times->trace_shadow_ms = ms[StageTimer::kTraceShadow];
+    times->resolve_ms = ms[StageTimer::kResolve];
+    times->accumulate_ms = ms[StageTimer::kAccumulate];
+    times->trace_closest_launches = launches[StageTimer::kTraceClosest];
+    times->trace_shadow_launches = launches[StageTimer::kTraceShadow];
+    times->frame_ms = e->last_ms;
+  });
+}
+
+vt_status vt_capture(vt_engine* e, float* rgba, size_t cap) {
+  return vt::guard([&] {
+    if (!e || !rgba) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->accum.ptr) fail(VT_ERR_STATE, "captureFrame before renderFrame");
+    const size_t px = (size_t)e->width * e->height;
+    if (cap < 4 * px) fail(VT_ERR_RANGE, "capture buffer too small");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    VT_CUDA(cudaMemcpy(rgba, e->accum.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < px; ++i) {
+      const float n = rgba[4 * i + 3];
+      const float inv = n > 0.0f ? 1.0f / n : 0.0f;
+      rgba[4 * i] *= inv;
+      rgba[4 * i + 1] *= inv;
+      rgba[4 * i + 2] *= inv;
+      rgba[4 * i + 3] = 1.0f;
+    }
+  });
+}
+
+vt_status vt_capture_moments(vt_engine* e, double* mean_rgb, double* var_rgb, size_t cap) {
+  return vt::guard([&] {
+    if (!e || !mean_rgb || !var_rgb) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->opts.oracle_accumulation || !e->sum64.ptr) fail(VT_ERR_STATE, "engine has no FP64 accumulation");
+    const size_t px = (size_t)e->width * e->height;
+    if (cap < 3 * px) fail(VT_ERR_RANGE, "moment buffers too small");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    VT_CUDA(cudaMemcpy(mean_rgb, e->sum64.ptr, 3 * px * sizeof(double), cudaMemcpyDeviceToHost));
+    VT_CUDA(cudaMemcpy(var_rgb, e->sq64.ptr, 3 * px * sizeof(double), cudaMemcpyDeviceToHost));
+    const double n = (double)e->samples;
+    for (size_t i = 0; i < 3 * px; ++i) {
+      const double m = n > 0 ? mean_rgb[i] / n : 0.0;
+      const double q = n > 0 ? var_rgb[i] / n : 0.0;
+      mean_rgb[i] = m;
+      var_rgb[i] = n > 1 ? std::max(0.0, (q - m * m) * n / (n - 1)) : 0.0;
+    }
+  });
+}
+
+vt_status vt_pick(vt_engine* e, float x, float y, int32_t* out_triangle) {
+  return vt::guard([&] {
+    if (!e || !out_triangle) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->opts.debug) fail(VT_ERR_STATE, "pickPrimitive requires the debug option");
+    if (!e->has_scene || !e->have_camera) fail(VT_ERR_STATE, "pickPrimitive before setScene/renderFrame");
+    vt::DeviceScope ds(e->device);
+    float ray[8];
+    camera_ray(e, x, y, ray);
+    e->pick_ray.resize(2);
+    e->pick_hit.resize(1);
+    e->pick_status.resize(1);
+    e->pick_counter.resize(1);
+    VT_CUDA(cudaMemcpyAsync(e->pick_ray.ptr, ray, sizeof ray, cudaMemcpyHostToDevice, e->stream));
+    VT_CUDA(cudaMemsetAsync(e->pick_status.ptr, 0, sizeof(int), e->stream));
+    vt::TraceArgs t;
+    t.nodes = e->nodes.ptr;
+    t.tris = e->tris.ptr;
+    t.rays = e->pick_ray.ptr;
+    t.n = 1;
+    t.hits = e->pick_hit.ptr;
+    t.status = e->pick_status.ptr;
+    t.counter = e->pick_counter.ptr;
+    t.stack_depth = 2 * e->wide_depth + 2;
+    vt::launch_trace_closest(t, e->stream);
+    VT_CUDA(cudaGetLastError());
+    int4 h;
+    VT_CUDA(cudaMemcpyAsync(&h, e->pick_hit.ptr, sizeof h, cudaMemcpyDeviceToHost, e->stream));
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    *out_triangle = h.x;
+  });
+}
+
+vt_status vt_reset(vt_engine* e) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    vt::DeviceScope ds(e->device);
+    reset_accumulation(e);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+  });
+}
+
+vt_status vt_engine_get_stats(const vt_engine* e, vt_engine_stats* out) {
+  return vt::guard([&] {
+    if (!e || !out) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    vt::DeviceScope ds(e->device);
+    unsigned long long t[2] = {0, 0};
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    VT_CUDA(cudaMemcpy(t, e->totals.ptr, sizeof t, cudaMemcpyDeviceToHost));
+    out->closest_rays = t[0];
+    out->shadow_rays = t[1];
+    out->last_frame_ms = e->last_ms;
+    out->triangle_count = e->ntri;
+    out->emitter_count = e->n_emitters;
+  });
+}
+
+vt_status vt_destroy(vt_engine* e) {
+  return vt::guard([&] {
+    if (!e) return;
+    vt::DeviceScope ds(e->device);
+    cudaStreamSynchronize(e->stream);
+    delete e;
+  });
+}
+
+}  // extern "C"

@@ -122,7 +122,7 @@ static int grid_exponent(double extent) {
 }
 
 WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
-                        int idx_stride) {
+                        int idx_stride, const uint32_t* tri_materials) {
   WideBvhHost out;
   const BinaryNode* nodes = bin.nodes.data();
   const size_t ntri = bin.reordered_to_source.size();
@@ -206,6 +206,7 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
           for (int vi = 0; vi < 3; ++vi)
             for (int k = 0; k < 3; ++k) rec[4 * vi + k] = v[vi][k];
           std::memcpy(&rec[3], &src, 4);
+          if (tri_materials) std::memcpy(&rec[7], &tri_materials[src], 4);
           float nn[3] = {0, 0, 0};
           bool valid = reference_normal(v[0], v[1], v[2], nn);
           rec[12] = nn[0]; rec[13] = nn[1]; rec[14] = nn[2];

@@ -38,7 +38,8 @@ BinaryBvhHost build_binary_host(const float* positions, size_t position_words, c
 // 8-wide collapse of one binary interior node (reference greedy rule).
 int collect_wide_children(const BinaryNode* nodes, uint32_t root, uint32_t out[8]);
 
+// tri_materials (optional, one per source triangle) is stored in each record's v1.w.
 WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
-                        int idx_stride);
+                        int idx_stride, const uint32_t* tri_materials = nullptr);
 
 }  // namespace vt

@@ -1,0 +1,507 @@
+// pt_kernels.cu -- wavefront stages of the unidirectional path tracer.
+//
+// One wave = width*height*spp_wave paths.  Stages per bounce:
+//   extend   closest hit of the live queue (k_trace, traverse.cu)
+//   sort     counting sort of the queue by the hit's BSDF family (miss,
+//            Lambert, conductor, dielectric) so shading warps run one family
+//   shade    emission (MIS), next-event estimation on the area-light group,
+//            point lights and the environment (one light entry chosen
+//            uniformly, power-heuristic MIS against the BSDF pdf), BSDF
+//            sampling, Russian roulette, warp-ballot compaction of survivors
+//            and shadow rays into the next queues
+//   shadow   any hit of the shadow queue (k_trace)
+//   resolve  unoccluded shadow contributions added to the path's radiance
+// and after the last bounce `accumulate` folds each pixel's samples into the
+// FP32 accumulation (and, for the oracle, FP64 sums and sums of squares).
+//
+// Estimator (restated from pt-webgpu/src/wgsl/pathTrace/kernel.wgsl.ts:963-2030
+// for the Lambert / GGX-conductor / smooth-dielectric subset):
+//  - camera emission and emission after a delta event: weight 1;
+//  - emission reached by a BSDF sample: power(pdf_bsdf, pdf_light);
+//  - NEE: power(pdf_light, pdf_bsdf) for area / environment, 1 for points;
+//    at the last vertex (no continuation is traced) NEE takes weight 1 so the
+//    two strategies still sum to one for every path length;
+//  - RR for bounce index > 2: survival clamp(max T, 0.1, 0.95), 2^-24 buckets.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pt_common.cuh"
+#include "pt_kernels.h"
+
+namespace vt {
+namespace pt {
+
+namespace {
+
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t rand_bounded(uint32_t& s, uint32_t bound) {
+  if (bound <= 1u) return 0u;
+  const uint32_t threshold = (0u - bound) % bound;
+  uint32_t v = pcg_next(s);
+  for (int k = 0; k < 64 && v < threshold; ++k) v = pcg_next(s);  // P(retry) < bound / 2^32
+  return v % bound;
+}
+
+
+// first index with cdf[i] > u (cdf inclusive, last entry 1)
+__device__ __forceinline__ uint32_t cdf_search(const float* cdf, uint32_t n, float u) {
+  uint32_t lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (cdf[mid] > u) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------- environment
+__device__ __forceinline__ void env_texel(const SceneView& sc, float3 d, int& col, int& row, float& sin_t) {
+  const float y = fminf(fmaxf(d.y, -1.0f), 1.0f);
+  const float theta = acosf(y);
+  float phi = atan2f(d.z, d.x);
+  if (phi < 0.0f) phi += 2.0f * CUDART_PI_F;
+  col = min(sc.env_w - 1, (int)(phi * (0.5f / CUDART_PI_F) * sc.env_w));
+  row = min(sc.env_h - 1, (int)(theta * (1.0f / CUDART_PI_F) * sc.env_h));
+  sin_t = sinf(theta);
+}
+
+__device__ __forceinline__ float env_pdf_texel(const SceneView& sc, int col, int row, float sin_t) {
+  if (!(sin_t > 0.0f)) return 0.0f;
+  const float pm = sc.env_marginal[row + 1] - sc.env_marginal[row];
+  const float* cc = sc.env_conditional + (size_t)row * (sc.env_w + 1);
+  const float pc = cc[col + 1] - cc[col];
+  return pm * pc * (float)sc.env_w * (float)sc.env_h / (2.0f * CUDART_PI_F * CUDART_PI_F * sin_t);
+}
+
+__device__ __forceinline__ float3 env_radiance(const SceneView& sc, int col, int row) {
+  const float4 e = __ldg(sc.env + (size_t)row * sc.env_w + col);
+  return f3(e.x, e.y, e.z) * sc.env_scale;
+}
+
+// ---------------------------------------------------------------- light sample
+struct LightSample {
+  float3 wi;
+  float dist;       // distance to the light point (inf for the environment)
+  float3 Le;        // emitted radiance (area/env) or intensity / dist^2 (point)
+  float pdf;        // solid-angle pdf including the entry selection (delta: selection only)
+  bool delta;
+  bool valid;
+};
+
+__device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng) {
+  LightSample ls;
+  ls.valid = false;
+  ls.delta = false;
+  const uint32_t n = sc.n_light_entries;
+  const float psel = 1.0f / (float)n;
+  uint32_t e = rand_bounded(rng, n);
+  const bool has_area = sc.n_emitters > 0;
+  if (has_area) {
+    if (e == 0) {
+      const float u = rand01(rng);
+      const uint32_t k = cdf_search(sc.emitter_cdf, sc.n_emitters, u);
+      const float4 a = __ldg(sc.emitters + 3 * k), b = __ldg(sc.emitters + 3 * k + 1), c = __ldg(sc.emitters + 3 * k + 2);
+      float u1 = rand01(rng), u2 = rand01(rng);
+      const float su = sqrtf(u1);
+      const float wa = 1.0f - su, wb = su * (1.0f - u2), wc = su * u2;
+      const float3 A = f3(a.x, a.y, a.z), B = f3(b.x, b.y, b.z), C = f3(c.x, c.y, c.z);
+      const float3 X = A * wa + B * wb + C * wc;
+      const float3 nl = normalize(cross(B - A, C - A));
+      const float3 d = X - P;
+      const float d2 = dot(d, d);
+      const float dist = sqrtf(d2);
+      ls.wi = d * (1.0f / dist);
+      const float cosl = -dot(ls.wi, nl);
+      if (!(cosl > 0.0f) || !(dist > 0.0f)) return ls;
+      const Material m = sc.materials[__float_as_uint(a.w)];
+      ls.Le = m.emission;
+      ls.dist = dist;
+      ls.pdf = psel * d2 / (sc.emit_area_total * cosl);
+      ls.valid = true;
+      return ls;
+    }
+    e -= 1;
+  }
+  if (e < sc.n_points) {
+    const float4 p = __ldg(sc.points + 2 * e), I = __ldg(sc.points + 2 * e + 1);
+    const float3 d = f3(p.x, p.y, p.z) - P;
+    const float d2 = dot(d, d);
+    if (!(d2 > 0.0f)) return ls;
+    const float dist = sqrtf(d2);
+    ls.wi = d * (1.0f / dist);
+    ls.dist = dist;
+    ls.Le = f3(I.x, I.y, I.z) * (1.0f / d2);
+    ls.pdf = psel;
+    ls.delta = true;
+    ls.valid = true;
+    return ls;
+  }
+  // environment
+  const float u1 = rand01(rng), u2 = rand01(rng);
+  const uint32_t row = cdf_search(sc.env_marginal + 1, (uint32_t)sc.env_h, u1);
+  const float* cc = sc.env_conditional + (size_t)row * (sc.env_w + 1);
+  const uint32_t col = cdf_search(cc + 1, (uint32_t)sc.env_w, u2);
+  const float m0 = sc.env_marginal[row], m1 = sc.env_marginal[row + 1];
+  const float c0 = cc[col], c1 = cc[col + 1];
+  const float fv = m1 > m0 ? (u1 - m0) / (m1 - m0) : 0.5f;
+  const float fu = c1 > c0 ? (u2 - c0) / (c1 - c0) : 0.5f;
+  const float v = ((float)row + fminf(fmaxf(fv, 0.0f), 0.999999f)) / (float)sc.env_h;
+  const float u = ((float)col + fminf(fmaxf(fu, 0.0f), 0.999999f)) / (float)sc.env_w;
+  const float theta = v * CUDART_PI_F, phi = u * 2.0f * CUDART_PI_F;
+  const float st = sinf(theta);
+  ls.wi = f3(st * cosf(phi), cosf(theta), st * sinf(phi));
+  ls.dist = CUDART_INF_F;
+  ls.Le = env_radiance(sc, (int)col, (int)row);
+  ls.pdf = psel * env_pdf_texel(sc, (int)col, (int)row, st);
+  ls.valid = ls.pdf > 0.0f;
+  return ls;
+}
+
+// pdf (solid angle, with selection) of reaching an emissive triangle point by light sampling
+__device__ __forceinline__ float area_light_pdf(const SceneView& sc, float dist, float cosl) {
+  if (!(cosl > 0.0f)) return 0.0f;
+  return (1.0f / (float)sc.n_light_entries) * dist * dist / (sc.emit_area_total * cosl);
+}
+
+// ---------------------------------------------------------------- raygen
+__global__ void k_raygen(FrameView f, WaveBuffers w) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) w.counters[0] = f.paths;
+  if (i >= f.paths) return;
+  const uint32_t wh = f.width * f.height;
+  const uint32_t pix = i % wh, s = i / wh;
+  const uint32_t x = pix % f.width, y = pix / f.width;
+  const uint32_t sample = w.counters[kCntWaveSample] + s;
+  uint32_t rng = pcg_init(x, y, f.frame_seed ^ sample);
+  const float jx = rand01(rng), jy = rand01(rng);
+  const float u = ((float)x + jx) / (float)f.width, v = ((float)y + jy) / (float)f.height;
+  const float nx = u * 2.0f - 1.0f, ny = 1.0f - v * 2.0f;
+  const float* M = f.inv_vp;
+  float nf[4], fr[4];
+  for (int r = 0; r < 4; ++r) {
+    nf[r] = M[4 * r] * nx + M[4 * r + 1] * ny - M[4 * r + 2] + M[4 * r + 3];
+    fr[r] = M[4 * r] * nx + M[4 * r + 1] * ny + M[4 * r + 2] + M[4 * r + 3];
+  }
+  const float3 o = f3(nf[0] / nf[3], nf[1] / nf[3], nf[2] / nf[3]);
+  const float3 far = f3(fr[0] / fr[3], fr[1] / fr[3], fr[2] / fr[3]);
+  const float3 d = normalize(far - o);
+  w.rays[0][2 * i] = make_float4(o.x, o.y, o.z, 0.0f);
+  w.rays[0][2 * i + 1] = make_float4(d.x, d.y, d.z, CUDART_INF_F);
+  w.state[0][i] = make_uint4(i, rng, 1u /* previous event delta: camera */, 0u);
+  w.through[0][i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  w.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// ---------------------------------------------------------------- material sort
+__device__ __forceinline__ uint32_t hit_key(const SceneView& sc, int4 h) {
+  if (h.x < 0) return 0u;
+  const float4 v1 = __ldg(sc.tris + 4 * (size_t)(uint32_t)h.x + 1);
+  return 1u + sc.materials[__float_as_uint(v1.w)].kind;
+}
+
+__global__ void k_classify(SceneView sc, WaveBuffers w, int cur) {
+  const uint32_t n = w.counters[cur];
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    const uint32_t key = valid ? hit_key(sc, w.hits[i]) : 0xFFu;
+    if (valid) w.keys[i] = key;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      const uint32_t m = __ballot_sync(kFull, key == k);
+      if (m && lane == (uint32_t)(__ffs(m) - 1)) atomicAdd(&w.counters[kCntHist + k], (uint32_t)__popc(m));
+    }
+  }
+}
+
+__global__ void k_scatter(WaveBuffers w, int cur) {
+  const uint32_t n = w.counters[cur];
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t off[4];
+  off[0] = 0;
+  for (int k = 1; k < 4; ++k) off[k] = off[k - 1] + w.counters[kCntHist + k - 1];
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    const uint32_t key = valid ? w.keys[i] : 0xFFu;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      const uint32_t m = __ballot_sync(kFull, key == k);
+      if (!m) continue;
+      const int leader = __ffs(m) - 1;
+      uint32_t b = 0;
+      if ((int)lane == leader) b = atomicAdd(&w.counters[kCntCursor + k], (uint32_t)__popc(m));
+      b = __shfl_sync(kFull, b, leader);
+      if (key == k) w.order[off[k] + b + __popc(m & ((1u << lane) - 1u))] = i;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- shade
+__global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
+  const int nxt = cur ^ 1;
+  const uint32_t n = w.counters[cur];
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool last = bounce + 1 >= f.max_bounces;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    bool alive = false, shadow = false;
+    float4 next_o, next_d, sh_o, sh_d, sh_c;
+    uint4 next_state;
+    float3 T = f3(0.0f, 0.0f, 0.0f);
+    if (valid) {
+      const uint32_t p = f.sort_by_material ? w.order[i] : i;
+      const float4 r0 = w.rays[cur][2 * p], r1 = w.rays[cur][2 * p + 1];
+      const uint4 st = w.state[cur][p];
+      const float4 tp = w.through[cur][p];
+      const int4 h = w.hits[p];
+      T = f3(tp.x, tp.y, tp.z);
+      const uint32_t path = st.x;
+      uint32_t rng = st.y;
+      const bool prev_delta = st.z & 1u;
+      const float prev_pdf = __uint_as_float(st.w);
+      const float3 o = f3(r0.x, r0.y, r0.z), d = f3(r1.x, r1.y, r1.z);
+      float3 rad = f3(0.0f, 0.0f, 0.0f);
+      if (h.x < 0) {
+        if (sc.env) {
+          int col, row;
+          float sin_t;
+          env_texel(sc, d, col, row, sin_t);
+          float wgt = 1.0f;
+          if (!prev_delta && sc.env_marginal)
+            wgt = power_heuristic(prev_pdf, env_pdf_texel(sc, col, row, sin_t) / (float)sc.n_light_entries);
+          rad = rad + T * env_radiance(sc, col, row) * wgt;
+        }
+      } else {
+        const float4* rec = sc.tris + 4 * (size_t)(uint32_t)h.x;
+        const float4 v1 = __ldg(rec + 1), nr = __ldg(rec + 3);
+        const float t = __int_as_float(h.y);
+        const Material m = sc.materials[__float_as_uint(v1.w)];
+        const float3 P = o + d * t;
+        const float3 ng = f3(nr.x, nr.y, nr.z);
+        const float dn = dot(d, ng);
+        const bool front = dn < 0.0f;
+        if (m.emissive && front) {
+          float wgt = 1.0f;
+          if (!prev_delta) wgt = power_heuristic(prev_pdf, area_light_pdf(sc, t, -dn));
+          rad = rad + T * m.emission * wgt;
+        }
+        const float3 n = front ? ng : -ng;  // facing the incoming ray
+        const float off = sc.bias * fmaxf(1.0f, fmaxf(fabsf(P.x), fmaxf(fabsf(P.y), fabsf(P.z))));
+        const float3 wo = -d;
+        float3 tb, bb;
+        onb(n, tb, bb);
+        const float3 wol = to_local(wo, tb, bb, n);
+        if (m.kind != kDielectric) {
+          // ---- next-event estimation
+          if (sc.n_light_entries > 0) {
+            const LightSample ls = sample_light(sc, P, rng);
+            if (ls.valid) {
+              float3 fc;
+              float pb;
+              bsdf_eval(m, wol, to_local(ls.wi, tb, bb, n), fc, pb);
+              if (maxc(fc) > 0.0f) {
+                const float wgt = (ls.delta || last) ? 1.0f : power_heuristic(ls.pdf, pb);
+                const float3 c = T * fc * ls.Le * (wgt / ls.pdf);
+                if (maxc(c) > 0.0f) {
+                  const float3 so = P + n * off;
+                  const float tmax = isinf(ls.dist) ? CUDART_INF_F : ls.dist * (1.0f - 1e-4f);
+                  sh_o = make_float4(so.x, so.y, so.z, 0.0f);
+                  sh_d = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, tmax);
+                  sh_c = make_float4(c.x, c.y, c.z, __uint_as_float(path));
+                  shadow = true;
+                }
+              }
+            }
+          }
+          // ---- BSDF sample
+          if (!last) {
+            float3 wil = f3(0.0f, 0.0f, 0.0f), wgt = f3(0.0f, 0.0f, 0.0f);
+            float pdf = 0.0f;
+            const float u1 = rand01(rng), u2 = rand01(rng);
+            if (m.kind == kLambert) {
+              const float r = sqrtf(u1), phi = 2.0f * CUDART_PI_F * u2;
+              wil = f3(r * cosf(phi), r * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
+              pdf = wil.z / CUDART_PI_F;
+              wgt = m.base_color;
+            } else {
+              const float3 hl = ggx_vndf(wol, m.alpha, u1, u2);
+              const float oh = dot(wol, hl);
+              wil = hl * (2.0f * oh) - wol;
+              if (wil.z > 0.0f && oh > 0.0f) {
+                pdf = ggx_d(hl.z, m.alpha) * ggx_g1(wol.z, m.alpha) / (4.0f * wol.z);
+                wgt = schlick(m.base_color, oh) * ggx_g1(wil.z, m.alpha);
+              }
+            }
+            if (pdf > 0.0f && maxc(wgt) > 0.0f) {
+              const float3 wi = to_world(wil, tb, bb, n);
+              T = T * wgt;
+              alive = true;
+              const float3 no = P + n * off;
+              next_o = make_float4(no.x, no.y, no.z, 0.0f);
+              next_d = make_float4(wi.x, wi.y, wi.z, CUDART_INF_F);
+              next_state = make_uint4(path, 0u, 0u, __float_as_uint(pdf));
+            }
+          }
+        } else if (!last) {
+          // ---- smooth dielectric: Fresnel-partitioned reflection / refraction
+          const float eta = front ? m.ior : 1.0f / m.ior;  // n_t / n_i
+          const float cosi = wol.z;
+          const float F = represented_bernoulli(fr_dielectric(cosi, eta));
+          float3 wi;
+          float3 wgt = f3(1.0f, 1.0f, 1.0f);
+          bool reflect = rand01(rng) < F;
+          if (!reflect) {
+            const float sin2t = fmaxf(0.0f, 1.0f - cosi * cosi) / (eta * eta);
+            if (sin2t >= 1.0f) {
+              reflect = true;  // unreachable when F == 1 (total internal reflection)
+            } else {
+              const float cost = sqrtf(1.0f - sin2t);
+              wi = d * (1.0f / eta) + n * (cosi / eta - cost);
+              wi = normalize(wi);
+              wgt = f3(1.0f, 1.0f, 1.0f) * (1.0f / (eta * eta));  // radiance scales by (n_i / n_t)^2
+            }
+          }
+          if (reflect) wi = d + n * (2.0f * cosi);
+          T = T * wgt;
+          const float side = reflect ? 1.0f : -1.0f;
+          const float3 no = P + n * (off * side);
+          alive = true;
+          next_o = make_float4(no.x, no.y, no.z, 0.0f);
+          next_d = make_float4(wi.x, wi.y, wi.z, CUDART_INF_F);
+          next_state = make_uint4(path, 0u, 1u, 0u);
+        }
+        // ---- Russian roulette
+        if (alive && bounce > 2) {
+          const float q = represented_bernoulli(fminf(fmaxf(maxc(T), 0.1f), 0.95f));
+          if (!(rand01(rng) < q)) alive = false;
+          else T = T * (1.0f / q);
+        }
+      }
+      next_state.y = rng;
+      if (maxc(rad) > 0.0f) {
+        float4 acc = w.radiance[path];
+        w.radiance[path] = make_float4(acc.x + rad.x, acc.y + rad.y, acc.z + rad.z, 0.0f);
+      }
+    }
+    // ---- warp-ballot compaction of survivors and shadow rays
+    const uint32_t am = __ballot_sync(kFull, alive);
+    if (am) {
+      uint32_t b = 0;
+      if (lane == (uint32_t)(__ffs(am) - 1)) b = atomicAdd(&w.counters[nxt], (uint32_t)__popc(am));
+      b = __shfl_sync(kFull, b, __ffs(am) - 1);
+      if (alive) {
+        const uint32_t q = b + __popc(am & ((1u << lane) - 1u));
+        w.rays[nxt][2 * q] = next_o;
+        w.rays[nxt][2 * q + 1] = next_d;
+        w.state[nxt][q] = next_state;
+        w.through[nxt][q] = make_float4(T.x, T.y, T.z, 0.0f);
+      }
+    }
+    const uint32_t sm = __ballot_sync(kFull, shadow);
+    if (sm) {
+      uint32_t b = 0;
+      if (lane == (uint32_t)(__ffs(sm) - 1)) b = atomicAdd(&w.counters[kCntShadow], (uint32_t)__popc(sm));
+      b = __shfl_sync(kFull, b, __ffs(sm) - 1);
+      if (shadow) {
+        const uint32_t q = b + __popc(sm & ((1u << lane) - 1u));
+        w.shadow_rays[2 * q] = sh_o;
+        w.shadow_rays[2 * q + 1] = sh_d;
+        w.shadow_contrib[q] = sh_c;
+      }
+    }
+  }
+}
+
+__global__ void k_shadow_resolve(WaveBuffers w) {
+  const uint32_t n = w.counters[kCntShadow];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (w.occluded[i]) continue;
+    const float4 c = w.shadow_contrib[i];
+    const uint32_t path = __float_as_uint(c.w);
+    float4 acc = w.radiance[path];
+    w.radiance[path] = make_float4(acc.x + c.x, acc.y + c.y, acc.z + c.z, 0.0f);
+  }
+}
+
+__global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
+  const uint32_t wh = f.width * f.height;
+  const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= wh) return;
+  float3 s = f3(0.0f, 0.0f, 0.0f);
+  double s64[3] = {0, 0, 0}, q64[3] = {0, 0, 0};
+  for (uint32_t k = 0; k < f.spp_wave; ++k) {
+    const float4 r = w.radiance[(size_t)k * wh + pix];
+    s = s + f3(r.x, r.y, r.z);
+    if (a.sum64) {
+      const double v[3] = {r.x, r.y, r.z};
+      for (int c = 0; c < 3; ++c) { s64[c] += v[c]; q64[c] += v[c] * v[c]; }
+    }
+  }
+  float4 acc = a.accum[pix];
+  a.accum[pix] = make_float4(acc.x + s.x, acc.y + s.y, acc.z + s.z, acc.w + (float)f.spp_wave);
+  if (a.sum64) {
+    for (int c = 0; c < 3; ++c) {
+      a.sum64[3 * (size_t)pix + c] += s64[c];
+      a.sq64[3 * (size_t)pix + c] += q64[c];
+    }
+  }
+}
+
+// next wave's samples start after this wave's (read by k_raygen)
+__global__ void k_advance_wave(FrameView f, WaveBuffers w) { w.counters[kCntWaveSample] += f.spp_wave; }
+
+__global__ void k_count_rays(WaveBuffers w, int cur, unsigned long long* totals) {
+  totals[0] += w.counters[cur];
+  totals[1] += w.counters[kCntShadow];
+}
+
+unsigned grid_for(uint32_t n, unsigned block) {
+  unsigned g = (unsigned)((n + block - 1) / block);
+  return g ? g : 1;
+}
+
+}  // namespace
+
+void launch_count_rays(const WaveBuffers& w, int cur, unsigned long long* totals, cudaStream_t s) {
+  k_count_rays<<<1, 1, 0, s>>>(w, cur, totals);
+}
+
+void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s) {
+  k_raygen<<<grid_for(f.paths, 256), 256, 0, s>>>(f, w);
+}
+
+void launch_sort_by_material(const SceneView& sc, const WaveBuffers& w, int cur, uint32_t capacity,
+                             cudaStream_t s) {
+  cudaMemsetAsync(w.counters + kCntHist, 0, sizeof(uint32_t) * 16, s);
+  const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
+  k_classify<<<g, 256, 0, s>>>(sc, w, cur);
+  k_scatter<<<g, 256, 0, s>>>(w, cur);
+}
+
+void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur, uint32_t bounce,
+                  uint32_t capacity, cudaStream_t s) {
+  cudaMemsetAsync(w.counters + (cur ^ 1), 0, sizeof(uint32_t), s);
+  cudaMemsetAsync(w.counters + kCntShadow, 0, sizeof(uint32_t), s);
+  const unsigned g = grid_for(capacity, 128) < 148 * 16 ? grid_for(capacity, 128) : 148 * 16;
+  k_shade<<<g, 128, 0, s>>>(sc, f, w, cur, bounce);
+}
+
+void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t s) {
+  const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
+  k_shadow_resolve<<<g, 256, 0, s>>>(w);
+}
+
+void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s) {
+  k_accumulate<<<grid_for(f.width * f.height, 256), 256, 0, s>>>(f, w, a);
+  k_advance_wave<<<1, 1, 0, s>>>(f, w);
+}
+
+}  // namespace pt
+}  // namespace vt

@@ -1,0 +1,87 @@
+// pt_kernels.h -- device views and launchers of the wavefront path tracer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pt_common.cuh"
+
+namespace vt {
+namespace pt {
+
+// Scene as the shading kernels see it.  Geometry lives in the BVH's triangle
+// records (vertices, source id in v0.w, material id in v1.w, reference
+// normal + validity in the fourth float4).
+struct SceneView {
+  const uint4* nodes = nullptr;
+  const float4* tris = nullptr;
+  int stack_depth = 16;
+  const Material* materials = nullptr;
+  uint32_t material_count = 0;
+  // emissive triangles: 3 float4 each = (v0, emitter material bits), (v1, area), (v2, 0)
+  const float4* emitters = nullptr;
+  const float* emitter_cdf = nullptr;  // inclusive cumulative area / total, one per emitter
+  uint32_t n_emitters = 0;
+  float emit_area_total = 0.0f;
+  // point lights: 2 float4 each = (position, 0), (intensity rgb, 0)
+  const float4* points = nullptr;
+  uint32_t n_points = 0;
+  // equirectangular environment (rgb as float4), with marginal/conditional CDFs
+  const float4* env = nullptr;
+  const float* env_marginal = nullptr;  // env_h + 1 entries
+  const float* env_conditional = nullptr;  // env_h rows of env_w + 1 entries
+  int env_w = 0, env_h = 0;
+  float env_scale = 1.0f;
+  uint32_t n_light_entries = 0;  // area group (if any) + point lights + environment (if any)
+  float bias = 2e-5f;            // origin offset along the geometric normal, relative to max(1, |P|_inf)
+};
+
+struct FrameView {
+  float inv_vp[16];         // row-major inverse view-projection
+  uint32_t width = 0, height = 0;
+  uint32_t frame_seed = 0;
+  uint32_t spp_wave = 1;    // samples per pixel in one wave
+  uint32_t max_bounces = 5;
+  uint32_t paths = 0;       // width * height * spp_wave
+  uint32_t sort_by_material = 1;
+};
+
+// Path queues (double-buffered), hit records, shadow queue and per-path radiance.
+struct WaveBuffers {
+  float4* rays[2] = {nullptr, nullptr};    // 2 float4 per path (vt_ray)
+  uint4* state[2] = {nullptr, nullptr};    // (path id, rng, flags, prev pdf bits)
+  float4* through[2] = {nullptr, nullptr}; // throughput rgb
+  int4* hits = nullptr;
+  uint32_t* order = nullptr;               // material-sorted permutation of the current queue
+  uint32_t* keys = nullptr;
+  float4* shadow_rays = nullptr;           // 2 float4 per shadow ray
+  float4* shadow_contrib = nullptr;        // rgb, path id bits
+  uint8_t* occluded = nullptr;
+  float4* radiance = nullptr;              // per path id
+  uint32_t* counters = nullptr;            // [queue0, queue1, shadow, hist[8], cursor[8], wave_sample]
+  unsigned long long* trace_counter = nullptr;
+  int* trace_status = nullptr;
+};
+
+enum : int { kCntShadow = 2, kCntHist = 3, kCntCursor = 11, kCntWaveSample = 19, kCntWords = 20 };
+
+// Accumulation targets.
+struct AccumView {
+  float4* accum = nullptr;    // rgb sum, sample count (FP32, the displayed estimate)
+  double* sum64 = nullptr;    // 3 per pixel, FP64 sum (oracle accumulation)
+  double* sq64 = nullptr;     // 3 per pixel, FP64 sum of squares
+};
+
+void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s);
+void launch_sort_by_material(const SceneView& sc, const WaveBuffers& w, int cur, uint32_t capacity,
+                             cudaStream_t s);
+void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur, uint32_t bounce,
+                  uint32_t capacity, cudaStream_t s);
+void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t s);
+void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s);
+// totals[0] += queue count traced this bounce, totals[1] += shadow rays traced
+void launch_count_rays(const WaveBuffers& w, int cur, unsigned long long* totals, cudaStream_t s);
+
+}  // namespace pt
+}  // namespace vt

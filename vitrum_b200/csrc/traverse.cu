@@ -79,7 +79,8 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
                                                   const float4* __restrict__ rays, size_t n,
                                                   int4* __restrict__ hits, uint8_t* __restrict__ occluded,
                                                   int* __restrict__ status,
-                                                  unsigned long long* __restrict__ ray_counter) {
+                                                  unsigned long long* __restrict__ ray_counter,
+                                                  const uint32_t* __restrict__ n_dev) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
 
   bool live = false, exhausted = false;
   uint32_t ray = 0, pool_next = 0, pool_end = 0;
-  const uint32_t n32 = (uint32_t)n;
+  const uint32_t n32 = n_dev ? *n_dev : (uint32_t)n;
   LaneRay R;
   WtRay wr;
   uint32_t gbase = 0, ghits = 0, gimask = 0, node = 0;
@@ -336,7 +337,7 @@ void launch_stk(const TraceArgs& a, cudaStream_t s) {
   grid = std::min(grid, (a.n + kBlock - 1) / kBlock);
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
   k_trace<ANY, STK><<<(unsigned)grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded,
-                                                         a.status, a.counter);
+                                                         a.status, a.counter, a.n_dev);
 }
 
 template <bool ANY>
@@ -354,6 +355,7 @@ void launch_trace_closest(const TraceArgs& a, cudaStream_t s) {
   if (a.n) k_refine_hits<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a.tris, a.rays, a.n, a.hits);
 }
 void launch_trace_any(const TraceArgs& a, cudaStream_t s) { launch_trace_t<true>(a, s); }
+void launch_trace_closest_records(const TraceArgs& a, cudaStream_t s) { launch_trace_t<false>(a, s); }
 
 void launch_watertight_eval(const float* cases, size_t n, vt_watertight_result* out, cudaStream_t s) {
   if (n == 0) return;

@@ -20,9 +20,12 @@ struct TraceArgs {
   int* status = nullptr;          // device word, bit 0 = stack capacity exceeded
   int stack_depth = 64;           // wide-tree depth bound
   unsigned long long* counter = nullptr;  // device word: next unclaimed ray (reset per launch)
+  const uint32_t* n_dev = nullptr;  // when set, the ray count is read from this device word (n = capacity)
 };
 
 void launch_trace_closest(const TraceArgs& a, cudaStream_t s);
+// Closest hit without the refinement pass: hits hold (triangle record, watertight t bits, 0, 0).
+void launch_trace_closest_records(const TraceArgs& a, cudaStream_t s);
 void launch_trace_any(const TraceArgs& a, cudaStream_t s);
 void launch_watertight_eval(const float* cases, size_t n, vt_watertight_result* out, cudaStream_t s);
 

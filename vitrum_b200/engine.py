@@ -1,0 +1,273 @@
+"""The vitrum Engine contract on the B200 path tracer.
+
+Mirrors @vitrum/core's Engine (packages/core/src/engine/index.ts:109-466) as
+implemented by pt-webgpu (packages/pt-webgpu/src/index.ts): a Scene goes in
+through set_scene(), render_frame() adds samples to a progressive
+accumulation, capture_frame() returns the running mean as RGBA float32
+(row-major, top-left), debug.pick_primitive(x, y) returns the triangle under a
+pixel, reset() clears the accumulation, dispose() releases the device state.
+All work happens in libvitrum_pt.so (vt_create ... vt_destroy).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+
+
+# ---------------------------------------------------------------- C structs
+class _EngineOptions(ctypes.Structure):
+    _fields_ = [("max_bounces", ctypes.c_int32), ("max_samples_per_pixel", ctypes.c_int32),
+                ("debug", ctypes.c_int32), ("oracle_accumulation", ctypes.c_int32),
+                ("sort_by_material", ctypes.c_int32), ("wave_paths", ctypes.c_int32)]
+
+
+class _MaterialDesc(ctypes.Structure):
+    _fields_ = [("base_color", ctypes.c_float * 3), ("roughness", ctypes.c_float), ("metallic", ctypes.c_float),
+                ("transmission", ctypes.c_float), ("ior", ctypes.c_float), ("emission", ctypes.c_float * 3)]
+
+
+class _MeshDesc(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("vertex_count", ctypes.c_size_t), ("indices", ctypes.c_void_p),
+                ("triangle_count", ctypes.c_size_t), ("material", ctypes.c_uint32)]
+
+
+class _PointLightDesc(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float * 3), ("intensity", ctypes.c_float * 3)]
+
+
+class _SceneDesc(ctypes.Structure):
+    _fields_ = [("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_size_t), ("materials", ctypes.c_void_p),
+                ("material_count", ctypes.c_size_t), ("point_lights", ctypes.c_void_p),
+                ("point_light_count", ctypes.c_size_t), ("environment_rgb", ctypes.c_void_p),
+                ("environment_width", ctypes.c_int32), ("environment_height", ctypes.c_int32),
+                ("environment_intensity", ctypes.c_float)]
+
+
+class _FrameInput(ctypes.Structure):
+    _fields_ = [("view", ctypes.c_float * 16), ("projection", ctypes.c_float * 16), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("frame_seed", ctypes.c_uint32), ("samples", ctypes.c_int32),
+                ("bounces", ctypes.c_int32)]
+
+
+class _FrameOutput(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("samples_accumulated", ctypes.c_int32), ("is_converged", ctypes.c_int32),
+                ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("radiance_device", ctypes.c_void_p)]
+
+
+class _StageTimes(ctypes.Structure):
+    _fields_ = [("raygen_ms", ctypes.c_double), ("trace_closest_ms", ctypes.c_double), ("sort_ms", ctypes.c_double),
+                ("shade_ms", ctypes.c_double), ("trace_shadow_ms", ctypes.c_double), ("resolve_ms", ctypes.c_double),
+                ("accumulate_ms", ctypes.c_double), ("frame_ms", ctypes.c_double),
+                ("trace_closest_launches", ctypes.c_int32), ("trace_shadow_launches", ctypes.c_int32)]
+
+
+class _EngineStats(ctypes.Structure):
+    _fields_ = [("closest_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("last_frame_ms", ctypes.c_double), ("triangle_count", ctypes.c_int64),
+                ("emitter_count", ctypes.c_int64)]
+
+
+# ---------------------------------------------------------------- scene types
+@dataclass
+class Material:
+    """core Material subset: transmission > 0 -> smooth dielectric, metallic >= 0.5 ->
+    GGX conductor, otherwise Lambert.  emission is front-face radiance."""
+    base_color: Sequence[float] = (0.8, 0.8, 0.8)
+    roughness: float = 1.0
+    metallic: float = 0.0
+    transmission: float = 0.0
+    ior: float = 1.5
+    emission: Sequence[float] = (0.0, 0.0, 0.0)
+
+
+@dataclass
+class Mesh:
+    positions: np.ndarray  # (V, 3) float32 world space
+    indices: np.ndarray    # (T, 3) uint32
+    material: int = 0
+
+
+@dataclass
+class PointLight:
+    position: Sequence[float]
+    intensity: Sequence[float]
+
+
+@dataclass
+class Environment:
+    rgb: np.ndarray        # (H, W, 3) float32 equirectangular, row 0 at +y
+    intensity: float = 1.0
+
+
+@dataclass
+class Scene:
+    meshes: List[Mesh] = field(default_factory=list)
+    materials: List[Material] = field(default_factory=list)
+    point_lights: List[PointLight] = field(default_factory=list)
+    environment: Optional[Environment] = None
+
+    @property
+    def triangle_count(self) -> int:
+        return int(sum(m.indices.shape[0] for m in self.meshes))
+
+
+@dataclass
+class Camera:
+    eye: Sequence[float]
+    target: Sequence[float]
+    up: Sequence[float] = (0.0, 1.0, 0.0)
+    fov_y_deg: float = 40.0
+    near: float = 0.01
+    far: float = 1000.0
+
+    def matrices(self, aspect: float):
+        """(view, projection) column-major float32[16], OpenGL conventions."""
+        e = np.asarray(self.eye, np.float64)
+        t = np.asarray(self.target, np.float64)
+        u = np.asarray(self.up, np.float64)
+        f = t - e
+        f /= np.linalg.norm(f)
+        s = np.cross(f, u)
+        s /= np.linalg.norm(s)
+        uu = np.cross(s, f)
+        view = np.eye(4)
+        view[0, :3], view[1, :3], view[2, :3] = s, uu, -f
+        view[0, 3], view[1, 3], view[2, 3] = -s @ e, -uu @ e, f @ e
+        k = 1.0 / math.tan(math.radians(self.fov_y_deg) / 2)
+        n, fa = self.near, self.far
+        proj = np.zeros((4, 4))
+        proj[0, 0] = k / aspect
+        proj[1, 1] = k
+        proj[2, 2] = (fa + n) / (n - fa)
+        proj[2, 3] = 2 * fa * n / (n - fa)
+        proj[3, 2] = -1.0
+        return view.T.reshape(-1).astype(np.float32), proj.T.reshape(-1).astype(np.float32)
+
+
+# ---------------------------------------------------------------- engine
+class _Debug:
+    def __init__(self, engine: "Engine"):
+        self._e = engine
+
+    def pick_primitive(self, x: float, y: float) -> Optional[int]:
+        """Engine.debug.pickPrimitive: source triangle index under pixel (x, y), or None."""
+        out = ctypes.c_int32(-1)
+        N.call("vt_pick", self._e.handle, float(x), float(y), ctypes.byref(out))
+        return None if out.value < 0 else int(out.value)
+
+
+class Engine:
+    """createPTEngine (pt-webgpu factory, index.ts:2363) on the CUDA backend."""
+
+    def __init__(self, device: int = 0, max_bounces: int = 8, max_samples_per_pixel: int = 4096,
+                 debug: bool = False, oracle_accumulation: bool = False, sort_by_material: bool = True,
+                 wave_paths: int = 0):
+        opts = _EngineOptions(max_bounces, max_samples_per_pixel, 1 if debug else 0, 1 if oracle_accumulation else 0,
+                              0 if sort_by_material else -1, wave_paths)
+        h = ctypes.c_void_p()
+        N.call("vt_create", device, ctypes.byref(opts), ctypes.byref(h))
+        self._h = h
+        self.device = device
+        self.debug = _Debug(self) if debug else None
+        self._keep = []
+        self.width = self.height = 0
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise RuntimeError("engine is disposed")
+        return self._h
+
+    def set_scene(self, scene: Scene) -> None:
+        keep = []
+        meshes = (_MeshDesc * max(1, len(scene.meshes)))()
+        for i, m in enumerate(scene.meshes):
+            p = np.ascontiguousarray(m.positions, np.float32).reshape(-1, 3)
+            ix = np.ascontiguousarray(m.indices, np.uint32).reshape(-1, 3)
+            keep += [p, ix]
+            meshes[i] = _MeshDesc(p.ctypes.data, p.shape[0], ix.ctypes.data, ix.shape[0], int(m.material))
+        mats = (_MaterialDesc * max(1, len(scene.materials)))()
+        for i, m in enumerate(scene.materials):
+            mats[i] = _MaterialDesc((ctypes.c_float * 3)(*m.base_color), m.roughness, m.metallic, m.transmission,
+                                    m.ior, (ctypes.c_float * 3)(*m.emission))
+        pls = (_PointLightDesc * max(1, len(scene.point_lights)))()
+        for i, l in enumerate(scene.point_lights):
+            pls[i] = _PointLightDesc((ctypes.c_float * 3)(*l.position), (ctypes.c_float * 3)(*l.intensity))
+        env_ptr, ew, eh, ei = None, 0, 0, 1.0
+        if scene.environment is not None:
+            env = np.ascontiguousarray(scene.environment.rgb, np.float32)
+            keep.append(env)
+            env_ptr, eh, ew, ei = env.ctypes.data, env.shape[0], env.shape[1], scene.environment.intensity
+        desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes), ctypes.cast(mats, ctypes.c_void_p),
+                          len(scene.materials), ctypes.cast(pls, ctypes.c_void_p), len(scene.point_lights), env_ptr,
+                          ew, eh, ei)
+        N.call("vt_set_scene", self.handle, ctypes.byref(desc))
+
+    def render_frame(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,
+                     frame_seed: int = 0) -> dict:
+        view, proj = camera.matrices(width / height)
+        fin = _FrameInput((ctypes.c_float * 16)(*view), (ctypes.c_float * 16)(*proj), width, height, frame_seed,
+                          samples, bounces)
+        out = _FrameOutput()
+        N.call("vt_render_frame", self.handle, ctypes.byref(fin), ctypes.byref(out))
+        self.width, self.height = out.width, out.height
+        return {"kind": "rendered" if out.kind == 0 else "skipped", "samplesAccumulated": out.samples_accumulated,
+                "isConverged": bool(out.is_converged),
+                "primaryRadiance": {"devicePtr": out.radiance_device, "width": out.width, "height": out.height,
+                                    "format": "rgba32f-sum-count"}}
+
+    def profile_frame(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,
+                      frame_seed: int = 0) -> dict:
+        """render_frame with per-stage device timings (no graph replay)."""
+        view, proj = camera.matrices(width / height)
+        fin = _FrameInput((ctypes.c_float * 16)(*view), (ctypes.c_float * 16)(*proj), width, height, frame_seed,
+                          samples, bounces)
+        out = _FrameOutput()
+        tm = _StageTimes()
+        N.call("vt_profile_frame", self.handle, ctypes.byref(fin), ctypes.byref(out), ctypes.byref(tm))
+        self.width, self.height = out.width, out.height
+        return {f: getattr(tm, f) for f, _ in _StageTimes._fields_}
+
+    def capture_frame(self) -> np.ndarray:
+        """Mean radiance (H, W, 4) float32, alpha 1 (Engine.captureFrame)."""
+        out = np.empty((self.height, self.width, 4), np.float32)
+        N.call("vt_capture", self.handle, ctypes.c_void_p(out.ctypes.data), out.size)
+        return out
+
+    def capture_moments(self):
+        """FP64 per-pixel mean and per-sample variance, each (H, W, 3)."""
+        m = np.empty((self.height, self.width, 3), np.float64)
+        v = np.empty_like(m)
+        N.call("vt_capture_moments", self.handle, ctypes.c_void_p(m.ctypes.data), ctypes.c_void_p(v.ctypes.data),
+               m.size)
+        return m, v
+
+    def stats(self) -> dict:
+        s = _EngineStats()
+        N.call("vt_engine_get_stats", self.handle, ctypes.byref(s))
+        return {f: getattr(s, f) for f, _ in _EngineStats._fields_}
+
+    def reset(self) -> None:
+        N.call("vt_reset", self.handle)
+
+    def dispose(self) -> None:
+        if self._h:
+            N.call("vt_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+
+def create_engine(**options) -> Engine:
+    """createPTEngine_CUDA(options) -> Engine (options: max_bounces, max_samples_per_pixel, debug, ...)."""
+    return Engine(**options)

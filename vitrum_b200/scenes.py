@@ -91,3 +91,85 @@ def config1(n_tris: int = 65536, n_rays: int = 1 << 20, seed: int = 2024):
     """Plain BVH build + closest-hit query workload: 65,536 float32 triangles,
     1,048,576 rays, tmin 1e-4, tmax +inf."""
     return random_triangles(n_tris, seed=seed), sphere_rays(n_rays, seed=seed + 1)
+
+
+# ---------------------------------------------------------------- box room
+def grid_quad(origin, edge_u, edge_v, n: int):
+    """n x n cells over the parallelogram origin + [0,1] edge_u + [0,1] edge_v, two
+    triangles per cell, winding so the normal is edge_u x edge_v."""
+    o = np.asarray(origin, np.float64)
+    eu = np.asarray(edge_u, np.float64)
+    ev = np.asarray(edge_v, np.float64)
+    s = np.linspace(0.0, 1.0, n + 1)
+    uu, vv = np.meshgrid(s, s, indexing="ij")
+    pos = o + uu[..., None] * eu + vv[..., None] * ev
+    pos = pos.reshape(-1, 3).astype(np.float32)
+    i = np.arange(n)
+    a = (i[:, None] * (n + 1) + i[None, :]).reshape(-1)
+    b = a + (n + 1)
+    c = b + 1
+    d = a + 1
+    tris = np.stack([np.stack([a, b, c], 1), np.stack([a, c, d], 1)], 1).reshape(-1, 3).astype(np.uint32)
+    return pos, tris
+
+
+def box_mesh(lo, hi, n: int):
+    """Axis-aligned box [lo, hi], each face n x n cells, outward winding."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    dx, dy, dz = hi - lo
+    X, Y, Z = np.array([dx, 0, 0]), np.array([0, dy, 0]), np.array([0, 0, dz])
+    faces = [
+        (lo, Y, X),                     # z = lo.z, normal -z
+        (lo + Z, X, Y),                 # z = hi.z, normal +z
+        (lo, Z, Y),                     # x = lo.x, normal -x
+        (lo + X, Y, Z),                 # x = hi.x, normal +x
+        (lo, X, Z),                     # y = lo.y, normal -y
+        (lo + Y, Z, X),                 # y = hi.y, normal +y
+    ]
+    ps, ts, off = [], [], 0
+    for o, eu, ev in faces:
+        p, t = grid_quad(o, eu, ev, n)
+        ps.append(p)
+        ts.append(t + off)
+        off += p.shape[0]
+    return np.concatenate(ps), np.concatenate(ts)
+
+
+def box_room(wall_cells: int = 128, box_cells: int = 64):
+    """Procedural box room: five unit walls (open at z = 1), a 0.3 box
+    (smooth dielectric, IOR 1.5) and a 0.3 x 0.6 x 0.3 box (GGX conductor,
+    roughness 0.2), a 0.25 x 0.25 emitter under the ceiling (radiance 15).
+
+    With the defaults: 5 x 128^2 x 2 + 2 x 6 x 64^2 x 2 + 2 = 262,146 triangles.
+    Returns (engine.Scene, engine.Camera) for a 40 degree pinhole camera."""
+    from .engine import Camera, Material, Mesh, Scene
+    mats = [
+        Material(base_color=(0.75, 0.75, 0.75)),                       # 0 grey walls
+        Material(base_color=(0.63, 0.06, 0.05)),                       # 1 left wall
+        Material(base_color=(0.14, 0.45, 0.09)),                       # 2 right wall
+        Material(base_color=(0.9, 0.85, 0.6), roughness=0.2, metallic=1.0),  # 3 GGX conductor
+        Material(base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.5),    # 4 dielectric
+        Material(base_color=(0.0, 0.0, 0.0), emission=(15.0, 15.0, 15.0)),  # 5 emitter
+    ]
+    n = wall_cells
+    meshes = []
+    walls = [
+        ((0, 0, 0), (0, 0, 1), (1, 0, 0), 0),   # floor y=0, normal +y
+        ((0, 1, 0), (1, 0, 0), (0, 0, 1), 0),   # ceiling y=1, normal -y
+        ((0, 0, 0), (1, 0, 0), (0, 1, 0), 0),   # back z=0, normal +z
+        ((0, 0, 0), (0, 1, 0), (0, 0, 1), 1),   # left x=0, normal +x
+        ((1, 0, 0), (0, 0, 1), (0, 1, 0), 2),   # right x=1, normal -x
+    ]
+    for o, eu, ev, m in walls:
+        p, t = grid_quad(o, eu, ev, n)
+        meshes.append(Mesh(p, t, m))
+    p, t = box_mesh((0.55, 0.001, 0.15), (0.85, 0.601, 0.45), box_cells)  # lifted: no face coplanar with the floor
+    meshes.append(Mesh(p, t, 3))
+    p, t = box_mesh((0.15, 0.001, 0.5), (0.45, 0.301, 0.8), box_cells)
+    meshes.append(Mesh(p, t, 4))
+    h = 0.125
+    p, t = grid_quad((0.5 - h, 0.999, 0.5 - h), (2 * h, 0, 0), (0, 0, 2 * h), 1)  # normal -y (down)
+    meshes.append(Mesh(p, t, 5))
+    cam = Camera(eye=(0.5, 0.5, 1.94), target=(0.5, 0.5, 0.0), fov_y_deg=40.0)
+    return Scene(meshes=meshes, materials=mats), cam
