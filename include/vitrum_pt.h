@@ -185,11 +185,23 @@ typedef struct vt_point_light_desc {
   float intensity[3];       /* radiant intensity; irradiance falls off as 1/d^2 */
 } vt_point_light_desc;
 
+/* One placement of a mesh (core instanced-mesh / transform; the TLAS instance
+ * of shared-bvh/src/tlas.ts:859).  With instances present every mesh is a
+ * bottom-level prototype in its local space and is drawn only through
+ * instances; emissive materials are not allowed on instances. */
+typedef struct vt_instance_desc {
+  uint32_t mesh;              /* index into vt_scene_desc.meshes */
+  uint32_t material;          /* material of this placement */
+  float local_to_world[16];   /* column-major, invertible */
+} vt_instance_desc;
+
 /* Scene (core Scene, core/src/scene/index.ts:42-46): primitives, emitters,
  * environment.  The environment is an equirectangular RGB image (row 0 at +y). */
 typedef struct vt_scene_desc {
   const vt_mesh_desc* meshes;
   size_t mesh_count;
+  const vt_instance_desc* instances;  /* NULL / 0: the meshes are world-space geometry */
+  size_t instance_count;
   const vt_material_desc* materials;
   size_t material_count;
   const vt_point_light_desc* point_lights;
@@ -263,8 +275,16 @@ vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
  * 3 doubles per pixel each. */
 vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
 /* Engine.debug.pickPrimitive (engine/debug.ts:33-35; pickPrimitiveCpu.ts:674):
- * source triangle id under pixel (x, y) of the last frame's camera, or -1. */
+ * under pixel (x, y) of the last frame's camera: the instance index in a
+ * scene with instances, else the source triangle index; -1 on a miss. */
 vt_status vt_pick(vt_engine* engine, float x, float y, int32_t* out_triangle);
+/* Closest hit of host rays against the engine's scene (vt_bvh_trace_closest
+ * on a whole scene, two-level when it has instances).  hits[i].prim is the
+ * triangle index within its mesh in a scene with instances, else the index over
+ * all meshes in order (-1 on a miss); t and (u, v) as vt_hit.  instances[i]
+ * receives the instance index, or -1 on a miss or without instances (may be NULL).
+ * No reference counterpart: the WebGPU engine exposes no ray query. */
+vt_status vt_trace_rays(vt_engine* engine, const vt_ray* rays, size_t n, vt_hit* hits, int32_t* instances);
 /* Engine.reset (pt-webgpu index.ts:2052): clears the accumulation. */
 vt_status vt_reset(vt_engine* engine);
 vt_status vt_engine_get_stats(const vt_engine* engine, vt_engine_stats* out_stats);

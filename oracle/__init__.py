@@ -61,6 +61,8 @@ def lib():
         L.orc_first_hit_wt_batch.restype = ctypes.c_int
         L.orc_first_hit_wt_batch.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_int, P, ctypes.c_int, P,
                                              ctypes.c_long, P, ctypes.c_long, P, P, P, ctypes.c_int]
+        L.orc_build_tlas.restype = ctypes.c_long
+        L.orc_build_tlas.argtypes = [P, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P]
         L.orc_wide_stack_entries.restype = ctypes.c_long
         L.orc_wide_stack_entries.argtypes = [P, P, ctypes.c_long]
         _LIB = L
@@ -141,6 +143,20 @@ def collapse_wide(binary: BinaryBvh) -> WideBvh:
     status = {0: "wide", 1: "empty", 2: "binary-fallback"}[st.value]
     return WideBvh(binary, node_bounds[:n].copy(), child_bounds[:n].copy(), child_meta[:n].copy(),
                    child_count[:n].copy(), w2b[:n].copy(), status)
+
+
+def build_tlas(aabbs, max_leaf=1, bins=16, max_depth=58):
+    """buildTlas (tlas.ts:859) over (n, 6) instance AABBs (min xyz, max xyz) in double.
+
+    Returns (nodes (m, 8) uint32, instanceIndices uint32)."""
+    a = np.ascontiguousarray(aabbs, dtype=np.float64).reshape(-1, 6)
+    n = a.shape[0]
+    nodes = np.zeros((max(2 * n, 1), 8), np.uint32)
+    perm = np.zeros(max(n, 1), np.uint32)
+    m = lib().orc_build_tlas(_p(a), n, max_leaf, bins, max_depth, _p(nodes), _p(perm))
+    if m < 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return nodes[:m].copy(), perm[:n].copy()
 
 
 def build_compressed_wide_bvh(positions, indices, **kw) -> WideBvh:

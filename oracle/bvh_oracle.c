@@ -1117,3 +1117,246 @@ int orc_first_hit_wt_batch(const float* node_bounds, const uint16_t* child_bound
   free(x);
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* TLAS build over instance AABBs (tlas.ts:257-989)                    */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  uint32_t orig;
+  double cen[3], mn[3], mx[3];
+} trec_t;
+
+typedef struct {
+  double mn[3], mx[3];
+  uint32_t w6, w7;
+} tnode_t;
+
+typedef struct {
+  tnode_t* nodes;
+  long n, cap;
+  uint32_t* perm;
+  long np;
+  int max_leaf, nbins, max_depth, err;
+} tstate_t;
+
+static double tsa(const double mn[3], const double mx[3]) { /* aabbSurfaceArea :265-273 */
+  double dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+  dx = jsmax(0, dx); dy = jsmax(0, dy); dz = jsmax(0, dz);
+  return 2 * (dx * dy + dy * dz + dz * dx);
+}
+
+static int min_balanced_depth(long count, int max_leaf) { /* :423-426 */
+  long leaves = (count + max_leaf - 1) / max_leaf;
+  if (leaves <= 1) return 0;
+  return (int)ceil(log2((double)leaves));
+}
+
+static const trec_t* g_tsort;
+static int g_taxis;
+static int cmp_tbal(const void* pa, const void* pb) {
+  const trec_t* a = &g_tsort[*(const uint32_t*)pa];
+  const trec_t* b = &g_tsort[*(const uint32_t*)pb];
+  double d = a->cen[g_taxis] - b->cen[g_taxis];
+  if (d != 0) return d < 0 ? -1 : 1;
+  return a->orig < b->orig ? -1 : (a->orig > b->orig ? 1 : 0);
+}
+
+static long tpush(tstate_t* s) {
+  if (s->n == s->cap) {
+    s->cap = s->cap ? 2 * s->cap : 64;
+    s->nodes = (tnode_t*)realloc(s->nodes, (size_t)s->cap * sizeof(tnode_t));
+  }
+  return s->n++;
+}
+
+static int tbin(double c, double cmin, double ext, int K) { /* Math.floor((c - cMin) / ext * K) clamped */
+  double t = floor((c - cmin) / ext * K);
+  if (t < 0) t = 0;
+  if (t > K - 1) t = K - 1;
+  return (int)t;
+}
+
+/* buildRecursive :467-579; sub holds record indices into R */
+static long tbuild(tstate_t* s, const trec_t* R, uint32_t* sub, long cnt, int depth) {
+  long me = s->n;
+  if (cnt <= s->max_leaf) { /* buildLeaf :289-309 */
+    long ni = tpush(s);
+    tnode_t nd;
+    for (int k = 0; k < 3; ++k) { nd.mn[k] = INFINITY; nd.mx[k] = -INFINITY; }
+    for (long i = 0; i < cnt; ++i)
+      for (int k = 0; k < 3; ++k) {
+        if (R[sub[i]].mn[k] < nd.mn[k]) nd.mn[k] = R[sub[i]].mn[k];
+        if (R[sub[i]].mx[k] > nd.mx[k]) nd.mx[k] = R[sub[i]].mx[k];
+      }
+    nd.w6 = (uint32_t)s->np;
+    nd.w7 = ORC_LEAF_FLAG | (uint32_t)cnt;
+    s->nodes[ni] = nd;
+    for (long i = 0; i < cnt; ++i) s->perm[s->np++] = R[sub[i]].orig;
+    return me;
+  }
+  if (depth >= s->max_depth || min_balanced_depth(cnt, s->max_leaf) > s->max_depth - depth) {
+    s->err = 1;
+    return me;
+  }
+  double cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (long i = 0; i < cnt; ++i) /* computeCentroidBounds :316-328 */
+    for (int k = 0; k < 3; ++k) {
+      if (R[sub[i]].cen[k] < cmn[k]) cmn[k] = R[sub[i]].cen[k];
+      if (R[sub[i]].cen[k] > cmx[k]) cmx[k] = R[sub[i]].cen[k];
+    }
+  const int K = s->nbins;
+  double ext[3] = {cmx[0] - cmn[0], cmx[1] - cmn[1], cmx[2] - cmn[2]};
+  int have = 0, baxis = 0, bbin = 0;
+  double bcost = 0;
+  if (!(ext[0] <= 0 && ext[1] <= 0 && ext[2] <= 0)) { /* pickSplit :330-393 */
+    double (*bmn)[3] = malloc(sizeof(double[3]) * K), (*bmx)[3] = malloc(sizeof(double[3]) * K);
+    long* bc = malloc(sizeof(long) * K);
+    double *lsa = malloc(sizeof(double) * K), *rsa = malloc(sizeof(double) * K);
+    long *lc = malloc(sizeof(long) * K), *rc = malloc(sizeof(long) * K);
+    for (int axis = 0; axis < 3; ++axis) {
+      if (ext[axis] <= 0) continue;
+      for (int b = 0; b < K; ++b) {
+        for (int k = 0; k < 3; ++k) { bmn[b][k] = INFINITY; bmx[b][k] = -INFINITY; }
+        bc[b] = 0;
+      }
+      for (long i = 0; i < cnt; ++i) {
+        const trec_t* r = &R[sub[i]];
+        int b = tbin(r->cen[axis], cmn[axis], ext[axis], K);
+        for (int k = 0; k < 3; ++k) {
+          if (r->mn[k] < bmn[b][k]) bmn[b][k] = r->mn[k];
+          if (r->mx[k] > bmx[b][k]) bmx[b][k] = r->mx[k];
+        }
+        bc[b] += 1;
+      }
+      double lmn[3] = {INFINITY, INFINITY, INFINITY}, lmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      long lcount = 0;
+      for (int b = 0; b < K; ++b) { /* unionBinInto skips empty bins :279-288 */
+        if (bc[b]) {
+          for (int k = 0; k < 3; ++k) {
+            if (bmn[b][k] < lmn[k]) lmn[k] = bmn[b][k];
+            if (bmx[b][k] > lmx[k]) lmx[k] = bmx[b][k];
+          }
+          lcount += bc[b];
+        }
+        lsa[b] = tsa(lmn, lmx);
+        lc[b] = lcount;
+      }
+      double rmn[3] = {INFINITY, INFINITY, INFINITY}, rmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      long rcount = 0;
+      for (int b = K - 1; b >= 0; --b) {
+        if (bc[b]) {
+          for (int k = 0; k < 3; ++k) {
+            if (bmn[b][k] < rmn[k]) rmn[k] = bmn[b][k];
+            if (bmx[b][k] > rmx[k]) rmx[k] = bmx[b][k];
+          }
+          rcount += bc[b];
+        }
+        rsa[b] = tsa(rmn, rmx);
+        rc[b] = rcount;
+      }
+      double total = lsa[K - 1];
+      if (total <= 0) continue;
+      for (int b = 0; b < K - 1; ++b) {
+        if (lc[b] == 0 || rc[b + 1] == 0) continue;
+        double sah = ((double)lc[b] * lsa[b] + (double)rc[b + 1] * rsa[b + 1]) / total;
+        if (!have || sah < bcost) { have = 1; baxis = axis; bbin = b; bcost = sah; }
+      }
+    }
+    free(bmn); free(bmx); free(bc); free(lsa); free(rsa); free(lc); free(rc);
+  }
+  int axis = have ? baxis : 0;
+  uint32_t* left = malloc(sizeof(uint32_t) * (size_t)cnt);
+  uint32_t* right = malloc(sizeof(uint32_t) * (size_t)cnt);
+  long nl = 0, nr = 0;
+  int fallback = 0;
+  if (!have) fallback = 1;
+  else if (bcost >= (double)cnt) fallback = 1;
+  else {
+    for (long i = 0; i < cnt; ++i) { /* partitionByBin :395-413 */
+      int b = tbin(R[sub[i]].cen[baxis], cmn[baxis], ext[baxis], K);
+      if (b <= bbin) left[nl++] = sub[i]; else right[nr++] = sub[i];
+    }
+    if (nl == 0 || nr == 0) fallback = 1;
+    else if (min_balanced_depth(nl, s->max_leaf) > s->max_depth - (depth + 1) ||
+             min_balanced_depth(nr, s->max_leaf) > s->max_depth - (depth + 1))
+      fallback = 1;
+  }
+  if (fallback) { /* balancedPartition :429-451 */
+    axis = 0;
+    if (ext[1] > ext[axis]) axis = 1;
+    if (ext[2] > ext[axis]) axis = 2;
+    uint32_t* ord = malloc(sizeof(uint32_t) * (size_t)cnt);
+    memcpy(ord, sub, sizeof(uint32_t) * (size_t)cnt);
+    g_tsort = R;
+    g_taxis = axis;
+    qsort(ord, (size_t)cnt, sizeof(uint32_t), cmp_tbal);
+    long mid = cnt / 2;
+    nl = mid; nr = cnt - mid;
+    memcpy(left, ord, sizeof(uint32_t) * (size_t)nl);
+    memcpy(right, ord + mid, sizeof(uint32_t) * (size_t)nr);
+    free(ord);
+  }
+  long ni = tpush(s);
+  s->nodes[ni].w7 = (uint32_t)axis;
+  tbuild(s, R, left, nl, depth + 1);
+  long ri = tbuild(s, R, right, nr, depth + 1);
+  free(left);
+  free(right);
+  tnode_t* me_n = &s->nodes[ni];
+  const tnode_t* L = &s->nodes[ni + 1];
+  const tnode_t* Rn = &s->nodes[ri];
+  me_n->w6 = (uint32_t)(ri - ni);
+  for (int k = 0; k < 3; ++k) {
+    me_n->mn[k] = jsmin(L->mn[k], Rn->mn[k]);
+    me_n->mx[k] = jsmax(L->mx[k], Rn->mx[k]);
+  }
+  return me;
+}
+
+/*
+ * buildTlas (tlas.ts:859).  aabb: 6 doubles per instance (min xyz, max xyz).
+ * Outputs packed nodes (8 u32 each, f32 bounds) and instanceIndices.
+ * Returns node count or -1.
+ */
+long orc_build_tlas(const double* aabb, long n, int max_leaf, int nbins, int max_depth, uint32_t* out_nodes,
+                    uint32_t* out_perm) {
+  if (n <= 0) return fail("buildTlas: instances list is empty");
+  trec_t* R = (trec_t*)malloc(sizeof(trec_t) * (size_t)n);
+  for (long i = 0; i < n; ++i) {
+    R[i].orig = (uint32_t)i;
+    for (int k = 0; k < 3; ++k) {
+      R[i].mn[k] = aabb[6 * i + k];
+      R[i].mx[k] = aabb[6 * i + 3 + k];
+      R[i].cen[k] = (R[i].mn[k] + R[i].mx[k]) * 0.5; /* aabbCentroid :187-193 */
+    }
+  }
+  tstate_t s;
+  memset(&s, 0, sizeof s);
+  s.perm = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
+  s.max_leaf = max_leaf;
+  s.nbins = nbins;
+  s.max_depth = max_depth;
+  uint32_t* all = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
+  for (long i = 0; i < n; ++i) all[i] = (uint32_t)i;
+  long result = -1;
+  if (min_balanced_depth(n, max_leaf) <= max_depth) {
+    tbuild(&s, R, all, n, 0);
+    if (!s.err) {
+      for (long i = 0; i < s.n; ++i) { /* flattenNodes :581-598 */
+        float f[6];
+        for (int k = 0; k < 3; ++k) { f[k] = (float)s.nodes[i].mn[k]; f[3 + k] = (float)s.nodes[i].mx[k]; }
+        memcpy(out_nodes + 8 * i, f, 24);
+        out_nodes[8 * i + 6] = s.nodes[i].w6;
+        out_nodes[8 * i + 7] = s.nodes[i].w7;
+      }
+      memcpy(out_perm, s.perm, sizeof(uint32_t) * (size_t)n);
+      result = s.n;
+    }
+  }
+  if (result < 0) fail("buildTlas: cannot encode the instances within the traversal-safe depth");
+  free(all);
+  free(R);
+  free(s.nodes);
+  free(s.perm);
+  return result;
+}

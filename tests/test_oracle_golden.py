@@ -70,6 +70,47 @@ def test_build_matches_reference_golden_bytes(case):
     assert np.array_equal(b.reordered_indices.reshape(-1, 4), gold_idx)
 
 
+def golden_tlas():
+    g = json.load(open(GOLDEN))
+    for name in SCENES:
+        pk = g[name]
+        by_root = {}
+        for bd in pk["primitiveTlasBindings"]:
+            by_root.setdefault(bd["blasRoot"], bd)
+        l2w = np.array(pk["tlasInstanceLocalToWorld"], np.float32).reshape(-1, 4, 4)
+        aabbs = []
+        for i, root in enumerate(pk["tlasBlasRoots"]):
+            bd = by_root[root]
+            lo, hi = np.array(bd["localAabbMin"], np.float64), np.array(bd["localAabbMax"], np.float64)
+            M = l2w[i].astype(np.float64).T  # column-major storage
+            corners = np.array([[(hi if c & 1 else lo)[0], (hi if c & 2 else lo)[1], (hi if c & 4 else lo)[2]]
+                                for c in range(8)])
+            w = corners @ M[:3, :3].T + M[:3, 3]  # transformAabb (scenePack.ts:197-223)
+            aabbs.append(np.r_[w.min(0), w.max(0)])
+        yield name, np.array(aabbs), np.array(pk["tlasNodes"], np.uint32).reshape(-1, 8), \
+            np.array(pk["tlasInstanceIndices"], np.uint32), pk["tlasNodeCount"]
+
+
+@pytest.mark.parametrize("case", list(golden_tlas()), ids=lambda c: c[0])
+def test_tlas_matches_reference_golden_bytes(case):
+    """buildTlas (tlas.ts:859) over the instances' world AABBs: node words and instance order."""
+    _, aabbs, gold_nodes, gold_perm, count = case
+    nodes, perm = oracle.build_tlas(aabbs)
+    assert nodes.shape[0] == count
+    assert np.array_equal(nodes, gold_nodes)
+    assert np.array_equal(perm, gold_perm)
+
+
+def test_tlas_balanced_fallback_on_coincident_instances():
+    # every instance on the same AABB: SAH finds no split, the balanced median
+    # fallback still gives one instance per leaf (maxLeafSize 1)
+    aabbs = np.tile([0.0, 0.0, 0.0, 1.0, 1.0, 1.0], (37, 1))
+    nodes, perm = oracle.build_tlas(aabbs)
+    leaf = (nodes[:, 7] >> 16) == 0xFFFF
+    assert (nodes[leaf, 7] & 0xFFFF).max() == 1 and leaf.sum() == 37
+    assert sorted(perm.tolist()) == list(range(37))
+
+
 def test_empty_and_single():
     # buildArrayBvh.test.ts:44-72
     b = oracle.build_array_bvh(np.zeros((0, 4), np.float32), np.zeros((0, 4), np.uint32))

@@ -69,6 +69,7 @@ SIGNATURES = {
     "vt_capture": [P, P, SZ],
     "vt_capture_moments": [P, P, P, SZ],
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
+    "vt_trace_rays": [P, P, SZ, P, P],
     "vt_reset": [P],
     "vt_engine_get_stats": [P, P],
     "vt_destroy": [P],

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -37,6 +38,16 @@ struct vt_engine {
   DeviceBuffer<uint4> nodes;
   DeviceBuffer<float4> tris;
   int wide_depth = 1;
+  int stack_depth = 16;            // traversal stack entries the scene needs
+  DeviceBuffer<float4> insts;      // instance records in top-level leaf order
+  DeviceBuffer<float4> inst_table; // instance records by instance index
+  DeviceBuffer<float4> inst_l2w;   // local-to-world rows by instance index (hit refinement)
+  int64_t n_instances = 0;
+  // vt_trace_rays staging
+  DeviceBuffer<float4> q_rays;
+  DeviceBuffer<int4> q_hits;
+  DeviceBuffer<int> q_inst, q_status;
+  DeviceBuffer<unsigned long long> q_counter;
   DeviceBuffer<vt::pt::Material> materials;
   DeviceBuffer<float4> emitters;
   DeviceBuffer<float> emitter_cdf;
@@ -196,16 +207,102 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
     m.emissive = (d.emission[0] > 0.0f || d.emission[1] > 0.0f || d.emission[2] > 0.0f) ? 1u : 0u;
     m.pad = 0;
   }
+  const size_t ntri = tri_mat.size();
   // geometry
   vt::BuildOptions bo;
-  e->binary = vt::build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
-  vt::WideBvhHost w = vt::encode_wide(e->binary, pos.data(), 4, idx.data(), 4, tri_mat.data());
-  const size_t ntri = tri_mat.size();
+  const bool two_level = sc->instance_count > 0;
+  if (two_level && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
+  std::vector<uint32_t> node_words;
+  std::vector<float> rec_floats, inst_lanes, inst_tab, inst_rows;
+  int depth = 1;
+  uint32_t root = 0;
+  if (!two_level) {
+    e->binary = vt::build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
+    vt::WideBvhHost w = vt::encode_wide(e->binary, pos.data(), 4, idx.data(), 4, tri_mat.data());
+    node_words = std::move(w.nodes);
+    rec_floats = std::move(w.tris);
+    depth = w.depth;
+  } else {
+    // one bottom-level tree per mesh, in the mesh's own space, concatenated
+    std::vector<uint32_t> blas_root(sc->mesh_count);
+    std::vector<std::array<double, 6>> local_box(sc->mesh_count);
+    int blas_depth = 1;
+    size_t vbase = 0, tbase = 0;
+    for (size_t m = 0; m < sc->mesh_count; ++m) {
+      const vt_mesh_desc& md = sc->meshes[m];
+      std::vector<float> mp(pos.begin() + 4 * vbase, pos.begin() + 4 * (vbase + md.vertex_count));
+      std::vector<uint32_t> mi(idx.begin() + 4 * tbase, idx.begin() + 4 * (tbase + md.triangle_count));
+      for (size_t t = 0; t < md.triangle_count; ++t)
+        for (int k = 0; k < 3; ++k) mi[4 * t + k] -= (uint32_t)vbase;
+      std::vector<uint32_t> mm(md.triangle_count, md.material);
+      vt::BinaryBvhHost b = vt::build_binary_host(mp.data(), mp.size(), mi.data(), mi.size(), bo);
+      vt::WideBvhHost w = vt::encode_wide(b, mp.data(), 4, mi.data(), 4, mm.data(),
+                                          (uint32_t)(node_words.size() / 20), (uint32_t)(rec_floats.size() / 16));
+      blas_root[m] = (uint32_t)(node_words.size() / 20);
+      node_words.insert(node_words.end(), w.nodes.begin(), w.nodes.end());
+      rec_floats.insert(rec_floats.end(), w.tris.begin(), w.tris.end());
+      blas_depth = std::max(blas_depth, w.depth);
+      const vt::BinaryNode& rn = b.nodes[0];
+      local_box[m] = {rn.mn[0], rn.mn[1], rn.mn[2], rn.mx[0], rn.mx[1], rn.mx[2]};
+      if (md.triangle_count == 0) local_box[m] = {0, 0, 0, 0, 0, 0};
+      vbase += md.vertex_count;
+      tbase += md.triangle_count;
+    }
+    // instances: world-to-local rows and world AABBs (transformAabb, scenePack.ts:197-223)
+    const size_t ni = sc->instance_count;
+    std::vector<vt::InstanceRecord> recs(ni);
+    std::vector<double> aabbs(6 * ni);
+    for (size_t i = 0; i < ni; ++i) {
+      const vt_instance_desc& id = sc->instances[i];
+      if (id.mesh >= sc->mesh_count) fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references mesh " +
+                                                            std::to_string(id.mesh));
+      if (id.material >= sc->material_count)
+        fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references material " + std::to_string(id.material));
+      if (mats[id.material].emissive) fail(VT_ERR_INVALID_ARGUMENT, "emissive materials are not supported on instances");
+      double rm[16], inv[16];
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) rm[r * 4 + c] = id.local_to_world[c * 4 + r];
+      if (!invert4(rm, inv)) fail(VT_ERR_INVALID_ARGUMENT, "instance " + std::to_string(i) + " is not invertible");
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) inst_rows.push_back(id.local_to_world[c * 4 + r]);
+      vt::InstanceRecord& rec = recs[i];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) rec.w2l[4 * r + c] = (float)inv[r * 4 + c];
+      rec.blas_root = blas_root[id.mesh];
+      rec.instance_id = (uint32_t)i;
+      rec.material = id.material;
+      rec.pad = 0;
+      const auto& lb = local_box[id.mesh];
+      double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (int c = 0; c < 8; ++c) {
+        const double q[3] = {(c & 1) ? lb[3] : lb[0], (c & 2) ? lb[4] : lb[1], (c & 4) ? lb[5] : lb[2]};
+        for (int k = 0; k < 3; ++k) {
+          const double v = rm[k * 4] * q[0] + rm[k * 4 + 1] * q[1] + rm[k * 4 + 2] * q[2] + rm[k * 4 + 3];
+          mn[k] = std::min(mn[k], v);
+          mx[k] = std::max(mx[k], v);
+        }
+      }
+      for (int k = 0; k < 3; ++k) { aabbs[6 * i + k] = mn[k]; aabbs[6 * i + 3 + k] = mx[k]; }
+    }
+    vt::BinaryBvhHost tl = vt::build_tlas_host(aabbs.data(), ni);
+    root = (uint32_t)(node_words.size() / 20);
+    vt::WideBvhHost tw = vt::encode_wide_tlas(tl, recs.data(), root);
+    node_words.insert(node_words.end(), tw.nodes.begin(), tw.nodes.end());
+    inst_lanes = std::move(tw.tris);
+    inst_tab.resize(16 * ni);
+    std::memcpy(inst_tab.data(), recs.data(), ni * sizeof(vt::InstanceRecord));
+    depth = tw.depth + blas_depth;
+    e->binary = std::move(tl);
+  }
+  vt::WideBvhHost w;
+  w.nodes = std::move(node_words);
+  w.tris = std::move(rec_floats);
+  w.depth = depth;
   // emissive triangles, sampled uniformly over their total area
   std::vector<float4> em;
   std::vector<float> cdf;
   double total = 0.0;
-  for (size_t t = 0; t < ntri; ++t) {
+  for (size_t t = 0; t < ntri && !two_level; ++t) {
     if (!mats[tri_mat[t]].emissive) continue;
     const float* a = &pos[4 * idx[4 * t]];
     const float* b = &pos[4 * idx[4 * t + 1]];
@@ -280,6 +377,17 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   e->tris.resize(std::max<size_t>(w.tris.size() / 4, 1));
   if (!w.tris.empty()) VT_CUDA(cudaMemcpyAsync(e->tris.ptr, w.tris.data(), w.tris.size() * 4, cudaMemcpyHostToDevice, s));
   e->wide_depth = w.depth;
+  e->stack_depth = two_level ? 2 * w.depth + 6 : 2 * w.depth + 2;
+  {
+    std::vector<float4> il(inst_lanes.size() / 4), it(inst_tab.size() / 4), ir(inst_rows.size() / 4);
+    if (!il.empty()) std::memcpy(il.data(), inst_lanes.data(), inst_lanes.size() * 4);
+    if (!it.empty()) std::memcpy(it.data(), inst_tab.data(), inst_tab.size() * 4);
+    if (!ir.empty()) std::memcpy(ir.data(), inst_rows.data(), inst_rows.size() * 4);
+    upload(e->insts, il, s);
+    upload(e->inst_table, it, s);
+    upload(e->inst_l2w, ir, s);
+  }
+  e->n_instances = (int64_t)sc->instance_count;
   upload(e->materials, mats, s);
   upload(e->emitters, em, s);
   upload(e->emitter_cdf, cdf, s);
@@ -291,7 +399,10 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   vt::pt::SceneView v;
   v.nodes = e->nodes.ptr;
   v.tris = e->tris.ptr;
-  v.stack_depth = 2 * w.depth + 2;
+  v.stack_depth = e->stack_depth;
+  v.insts = two_level ? e->insts.ptr : nullptr;
+  v.inst_table = two_level ? e->inst_table.ptr : nullptr;
+  v.root = root;
   v.materials = e->materials.ptr;
   v.material_count = (uint32_t)mats.size();
   v.emitters = e->emitters.ptr;
@@ -418,7 +529,9 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.hits = w.hits;
     t.status = e->trace_status.ptr;
     t.counter = e->trace_counter.ptr;
-    t.stack_depth = 2 * e->wide_depth + 2;
+    t.stack_depth = e->stack_depth;
+    t.insts = e->view.insts;
+    t.root = e->view.root;
     t.n_dev = w.counters + cur;
     B(StageTimer::kTraceClosest);
     vt::launch_trace_closest_records(t, s);
@@ -702,13 +815,67 @@ vt_status vt_pick(vt_engine* e, float x, float y, int32_t* out_triangle) {
     t.hits = e->pick_hit.ptr;
     t.status = e->pick_status.ptr;
     t.counter = e->pick_counter.ptr;
-    t.stack_depth = 2 * e->wide_depth + 2;
-    vt::launch_trace_closest(t, e->stream);
+    t.stack_depth = e->stack_depth;
+    t.insts = e->view.insts;
+    t.root = e->view.root;
+    t.inst_table = e->view.inst_table;
+    vt::launch_trace_closest_records(t, e->stream);
     VT_CUDA(cudaGetLastError());
     int4 h;
     VT_CUDA(cudaMemcpyAsync(&h, e->pick_hit.ptr, sizeof h, cudaMemcpyDeviceToHost, e->stream));
     VT_CUDA(cudaStreamSynchronize(e->stream));
-    *out_triangle = h.x;
+    if (h.x < 0) {
+      *out_triangle = -1;
+    } else if (h.z >= 0) {
+      *out_triangle = h.z;
+    } else {
+      float4 v0;
+      VT_CUDA(cudaMemcpy(&v0, e->tris.ptr + 4 * (size_t)h.x, sizeof v0, cudaMemcpyDeviceToHost));
+      uint32_t id;
+      std::memcpy(&id, &v0.w, 4);
+      *out_triangle = (int32_t)id;
+    }
+  });
+}
+
+vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits, int32_t* instances) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    if (n && (!rays || !hits)) fail(VT_ERR_INVALID_ARGUMENT, "rays and hits must be non-null");
+    if (n > 0xFFFFFFFFull) fail(VT_ERR_RANGE, "at most 2^32 - 1 rays per call");
+    if (!e->has_scene) fail(VT_ERR_STATE, "trace before setScene");
+    if (!n) return;
+    vt::DeviceScope ds(e->device);
+    e->q_rays.resize(2 * n);
+    e->q_hits.resize(n);
+    e->q_inst.resize(n);
+    e->q_status.resize(1);
+    e->q_counter.resize(1);
+    VT_CUDA(cudaMemcpyAsync(e->q_rays.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice, e->stream));
+    VT_CUDA(cudaMemsetAsync(e->q_status.ptr, 0, sizeof(int), e->stream));
+    vt::TraceArgs t;
+    t.nodes = e->nodes.ptr;
+    t.tris = e->tris.ptr;
+    t.rays = e->q_rays.ptr;
+    t.n = n;
+    t.hits = e->q_hits.ptr;
+    t.status = e->q_status.ptr;
+    t.counter = e->q_counter.ptr;
+    t.stack_depth = e->stack_depth;
+    t.insts = e->view.insts;
+    t.root = e->view.root;
+    t.inst_table = e->view.inst_table;
+    t.inst_l2w = e->view.inst_table ? e->inst_l2w.ptr : nullptr;
+    t.inst_out = e->q_inst.ptr;
+    vt::launch_trace_closest(t, e->stream);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaMemcpyAsync(hits, e->q_hits.ptr, n * sizeof(vt_hit), cudaMemcpyDeviceToHost, e->stream));
+    if (instances)
+      VT_CUDA(cudaMemcpyAsync(instances, e->q_inst.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
+    int st = 0;
+    VT_CUDA(cudaMemcpyAsync(&st, e->q_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    if (st) fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
   });
 }
 

@@ -242,4 +242,193 @@ BinaryBvhHost build_binary_host(const float* positions, size_t position_words, c
   return out;
 }
 
+// ---------------------------------------------------------------- TLAS
+// The reference's buildTlas (shared-bvh/src/tlas.ts:330-579): per node the
+// centroid AABB, 16 bins on every axis with a positive centroid extent,
+// prefix/suffix unions of non-empty bins, cost (N_L*SA_L + N_R*SA_R)/SA_total
+// with full surface area, leaf of <= max_leaf instances, and the balanced
+// median split (widest centroid axis, ties by input index) when the SAH is
+// degenerate, not improving, empty-sided or would exceed the depth budget.
+// Interior bounds are the union of the two children (:562-575).
+namespace {
+
+struct TRec {
+  uint32_t orig;
+  double cen[3], mn[3], mx[3];
+};
+
+struct TlasBuilder {
+  std::vector<TRec> recs;
+  std::vector<BinaryNode> nodes;
+  std::vector<double> nmn, nmx;  // exact (double) node bounds, 3 per node
+  std::vector<uint32_t> perm;
+  int max_leaf, bins, max_depth;
+
+  static int min_balanced_depth(size_t count, int max_leaf) {
+    const size_t leaves = (count + max_leaf - 1) / max_leaf;
+    return leaves <= 1 ? 0 : (int)std::ceil(std::log2((double)leaves));
+  }
+  static double area(const double* mn, const double* mx) {
+    double dx = std::max(0.0, mx[0] - mn[0]), dy = std::max(0.0, mx[1] - mn[1]), dz = std::max(0.0, mx[2] - mn[2]);
+    return 2 * (dx * dy + dy * dz + dz * dx);
+  }
+  int bin_of(double c, double cmin, double ext) const {
+    double t = std::floor((c - cmin) / ext * bins);
+    return (int)std::min<double>(bins - 1, std::max(0.0, t));
+  }
+
+  uint32_t push() {
+    nodes.push_back(BinaryNode{});
+    nmn.resize(3 * nodes.size());
+    nmx.resize(3 * nodes.size());
+    return (uint32_t)nodes.size() - 1;
+  }
+
+  uint32_t build(std::vector<uint32_t>& sub, int depth) {
+    const uint32_t me = (uint32_t)nodes.size();
+    if ((int)sub.size() <= max_leaf) {
+      const uint32_t ni = push();
+      double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (uint32_t r : sub)
+        for (int k = 0; k < 3; ++k) {
+          mn[k] = std::min(mn[k], recs[r].mn[k]);
+          mx[k] = std::max(mx[k], recs[r].mx[k]);
+        }
+      for (int k = 0; k < 3; ++k) { nmn[3 * ni + k] = mn[k]; nmx[3 * ni + k] = mx[k]; }
+      nodes[ni].w6 = (uint32_t)perm.size();
+      nodes[ni].w7 = kLeafFlag | (uint32_t)sub.size();
+      for (uint32_t r : sub) perm.push_back(recs[r].orig);
+      return me;
+    }
+    if (depth >= max_depth || min_balanced_depth(sub.size(), max_leaf) > max_depth - depth)
+      fail(VT_ERR_BUILD, "cannot encode " + std::to_string(sub.size()) + " instances within the traversal-safe depth");
+    double cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t r : sub)
+      for (int k = 0; k < 3; ++k) {
+        cmn[k] = std::min(cmn[k], recs[r].cen[k]);
+        cmx[k] = std::max(cmx[k], recs[r].cen[k]);
+      }
+    const double ext[3] = {cmx[0] - cmn[0], cmx[1] - cmn[1], cmx[2] - cmn[2]};
+    bool have = false;
+    int baxis = 0, bbin = 0;
+    double bcost = 0.0;
+    if (!(ext[0] <= 0 && ext[1] <= 0 && ext[2] <= 0)) {
+      std::vector<double> bmn(3 * bins), bmx(3 * bins), lsa(bins), rsa(bins);
+      std::vector<size_t> bc(bins), lc(bins), rc(bins);
+      for (int axis = 0; axis < 3; ++axis) {
+        if (ext[axis] <= 0) continue;
+        std::fill(bmn.begin(), bmn.end(), INFINITY);
+        std::fill(bmx.begin(), bmx.end(), -INFINITY);
+        std::fill(bc.begin(), bc.end(), 0);
+        for (uint32_t r : sub) {
+          const int b = bin_of(recs[r].cen[axis], cmn[axis], ext[axis]);
+          for (int k = 0; k < 3; ++k) {
+            bmn[3 * b + k] = std::min(bmn[3 * b + k], recs[r].mn[k]);
+            bmx[3 * b + k] = std::max(bmx[3 * b + k], recs[r].mx[k]);
+          }
+          bc[b] += 1;
+        }
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        size_t c = 0;
+        for (int b = 0; b < bins; ++b) {
+          if (bc[b]) {
+            for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], bmn[3 * b + k]); hi[k] = std::max(hi[k], bmx[3 * b + k]); }
+            c += bc[b];
+          }
+          lsa[b] = area(lo, hi);
+          lc[b] = c;
+        }
+        for (int k = 0; k < 3; ++k) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+        c = 0;
+        for (int b = bins - 1; b >= 0; --b) {
+          if (bc[b]) {
+            for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], bmn[3 * b + k]); hi[k] = std::max(hi[k], bmx[3 * b + k]); }
+            c += bc[b];
+          }
+          rsa[b] = area(lo, hi);
+          rc[b] = c;
+        }
+        const double total = lsa[bins - 1];
+        if (total <= 0) continue;
+        for (int b = 0; b < bins - 1; ++b) {
+          if (lc[b] == 0 || rc[b + 1] == 0) continue;
+          const double sah = ((double)lc[b] * lsa[b] + (double)rc[b + 1] * rsa[b + 1]) / total;
+          if (!have || sah < bcost) { have = true; baxis = axis; bbin = b; bcost = sah; }
+        }
+      }
+    }
+    int axis = have ? baxis : 0;
+    std::vector<uint32_t> left, right;
+    bool fallback = !have || bcost >= (double)sub.size();
+    if (!fallback) {
+      for (uint32_t r : sub) (bin_of(recs[r].cen[baxis], cmn[baxis], ext[baxis]) <= bbin ? left : right).push_back(r);
+      fallback = left.empty() || right.empty() ||
+                 min_balanced_depth(left.size(), max_leaf) > max_depth - (depth + 1) ||
+                 min_balanced_depth(right.size(), max_leaf) > max_depth - (depth + 1);
+    }
+    if (fallback) {
+      axis = 0;
+      if (ext[1] > ext[axis]) axis = 1;
+      if (ext[2] > ext[axis]) axis = 2;
+      std::vector<uint32_t> ord = sub;
+      const int ax = axis;
+      std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+        const double d = recs[a].cen[ax] - recs[b].cen[ax];
+        return d != 0 ? d < 0 : recs[a].orig < recs[b].orig;
+      });
+      const size_t mid = ord.size() / 2;
+      left.assign(ord.begin(), ord.begin() + mid);
+      right.assign(ord.begin() + mid, ord.end());
+    }
+    const uint32_t ni = push();
+    nodes[ni].w7 = (uint32_t)axis;
+    sub.clear();
+    sub.shrink_to_fit();
+    build(left, depth + 1);
+    const uint32_t ri = build(right, depth + 1);
+    nodes[ni].w6 = ri - ni;
+    for (int k = 0; k < 3; ++k) {
+      nmn[3 * ni + k] = std::min(nmn[3 * (ni + 1) + k], nmn[3 * ri + k]);
+      nmx[3 * ni + k] = std::max(nmx[3 * (ni + 1) + k], nmx[3 * ri + k]);
+    }
+    return me;
+  }
+};
+
+}  // namespace
+
+BinaryBvhHost build_tlas_host(const double* aabbs, size_t n, int max_leaf, int bins, int max_depth) {
+  if (n == 0) fail(VT_ERR_INVALID_ARGUMENT, "buildTlas: instances list is empty");
+  TlasBuilder b;
+  b.max_leaf = max_leaf;
+  b.bins = bins;
+  b.max_depth = max_depth;
+  b.recs.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    TRec& r = b.recs[i];
+    r.orig = (uint32_t)i;
+    for (int k = 0; k < 3; ++k) {
+      r.mn[k] = aabbs[6 * i + k];
+      r.mx[k] = aabbs[6 * i + 3 + k];
+      if (!std::isfinite(r.mn[k]) || !std::isfinite(r.mx[k])) fail(VT_ERR_RANGE, "instance AABB is not finite");
+      if (r.mx[k] < r.mn[k]) fail(VT_ERR_RANGE, "instance AABB is inverted");
+      r.cen[k] = (r.mn[k] + r.mx[k]) * 0.5;
+    }
+  }
+  if (TlasBuilder::min_balanced_depth(n, max_leaf) > max_depth)
+    fail(VT_ERR_RANGE, "instances cannot fit the traversal-safe depth");
+  std::vector<uint32_t> all(n);
+  std::iota(all.begin(), all.end(), 0u);
+  b.build(all, 0);
+  BinaryBvhHost out;
+  out.nodes = std::move(b.nodes);
+  for (size_t i = 0; i < out.nodes.size(); ++i)
+    for (int k = 0; k < 3; ++k) {
+      out.nodes[i].mn[k] = (float)b.nmn[3 * i + k];
+      out.nodes[i].mx[k] = (float)b.nmx[3 * i + k];
+    }
+  out.reordered_to_source = std::move(b.perm);
+  return out;
+}
+
 }  // namespace vt

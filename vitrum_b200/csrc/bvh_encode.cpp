@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
+#include <cstdint>
 #include <vector>
 
 #include "bvh_host.h"
@@ -121,27 +122,30 @@ static int grid_exponent(double extent) {
   return std::min(127, std::max(-126, e));
 }
 
-WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
-                        int idx_stride, const uint32_t* tri_materials) {
+// Encodes the binary tree as 8-wide nodes.  Node indices are offset by
+// node_base and record indices by rec_base (trees concatenated into shared
+// arrays); emit(leaf, slot_records) writes a leaf's payload records (16
+// floats each) for the leaf's binary node.
+template <class EmitLeaf>
+static WideBvhHost encode_core(const BinaryBvhHost& bin, uint32_t node_base, uint32_t rec_base, EmitLeaf emit) {
   WideBvhHost out;
   const BinaryNode* nodes = bin.nodes.data();
-  const size_t ntri = bin.reordered_to_source.size();
+  const size_t nleaf_items = bin.reordered_to_source.size();
   std::vector<uint32_t> wide_bin;   // binary node behind each wide node (BFS order)
   std::vector<int> level;
   wide_bin.push_back(0);
   level.push_back(1);
   out.depth = 1;
-  if (ntri == 0) {
+  if (nleaf_items == 0) {
     uint32_t w[20] = {};
     // All-empty slots: inverted boxes (qlo 255, qhi 0), no children.
     std::memset(reinterpret_cast<uint8_t*>(w) + 32, 0xFF, 24);
     out.nodes.assign(w, w + 20);
     return out;
   }
-  out.tris.reserve(ntri * 24);
   // 28 leading empty records: tri_base = block - 4 * first_leaf_slot then
-  // never wraps, and stays below 2^31 (bit 31 tags node groups on the
-  // traversal stack).
+  // never wraps, and stays below 2^30 (bits 30-31 tag stack entries).
+  out.tris.reserve((nleaf_items + 28) * 24);
   out.tris.assign(16 * 28, 0.0f);
   for (size_t wi = 0; wi < wide_bin.size(); ++wi) {
     const BinaryNode& parent = nodes[wide_bin[wi]];
@@ -163,7 +167,7 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
       bytes[12 + k] = (uint8_t)(ex[k] + 127);
     }
     uint8_t imask = 0;
-    uint32_t child_base = (uint32_t)wide_bin.size();
+    const uint32_t child_base = node_base + (uint32_t)wide_bin.size();
     // leaf slot s uses records [block + 4*(s - first_leaf_slot), +count)
     int first_leaf = 8, last_leaf = -1;
     for (int s = 0; s < 8; ++s) {
@@ -171,8 +175,8 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
       if (ci >= 0 && is_leaf_word(nodes[ch[ci]].w7)) { first_leaf = std::min(first_leaf, s); last_leaf = s; }
     }
     const uint32_t block = (uint32_t)(out.tris.size() / 16);
-    const uint32_t tri_base = block - 4u * (uint32_t)(first_leaf < 8 ? first_leaf : 0);
-    if (block < 28 || tri_base >= 0x80000000u) throw std::length_error("triangle records exceed 2^31");
+    const uint32_t tri_base = rec_base + block - 4u * (uint32_t)(first_leaf < 8 ? first_leaf : 0);
+    if ((uint64_t)rec_base + block + 32 >= 0x40000000ull) throw std::length_error("leaf records exceed 2^30");
     if (last_leaf >= 0) out.tris.resize(out.tris.size() + 16 * (size_t)(4 * (last_leaf - first_leaf) + 4), 0.0f);
     uint32_t tri_valid = 0;
     for (int s = 0; s < 8; ++s) {
@@ -194,24 +198,9 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
         qhi[k * 8 + s] = (uint8_t)hi;
       }
       if (is_leaf_word(c.w7)) {
-        uint32_t cnt = c.w7 & 0xFFFFu, first = c.w6;
+        const uint32_t cnt = c.w7 & 0xFFFFu;
         tri_valid |= ((1u << cnt) - 1u) << (4 * s);
-        for (uint32_t t = 0; t < cnt; ++t) {
-          uint32_t src = bin.reordered_to_source[first + t];
-          const uint32_t* iv = indices + (size_t)src * idx_stride;
-          float* rec = &out.tris[16 * ((size_t)block + 4 * (s - first_leaf) + t)];
-          float v[3][3];
-          for (int vi = 0; vi < 3; ++vi)
-            for (int k = 0; k < 3; ++k) v[vi][k] = positions[(size_t)iv[vi] * pos_stride + k];
-          for (int vi = 0; vi < 3; ++vi)
-            for (int k = 0; k < 3; ++k) rec[4 * vi + k] = v[vi][k];
-          std::memcpy(&rec[3], &src, 4);
-          if (tri_materials) std::memcpy(&rec[7], &tri_materials[src], 4);
-          float nn[3] = {0, 0, 0};
-          bool valid = reference_normal(v[0], v[1], v[2], nn);
-          rec[12] = nn[0]; rec[13] = nn[1]; rec[14] = nn[2];
-          rec[15] = valid ? 1.0f : 0.0f;
-        }
+        emit(c, &out.tris[16 * ((size_t)block + 4 * (s - first_leaf))]);
       } else {
         imask |= (uint8_t)(1u << s);
         wide_bin.push_back(ch[ci]);
@@ -227,6 +216,41 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
     out.nodes.insert(out.nodes.end(), w, w + 20);
   }
   return out;
+}
+
+WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
+                        int idx_stride, const uint32_t* tri_materials, uint32_t node_base, uint32_t rec_base) {
+  return encode_core(bin, node_base, rec_base, [&](const BinaryNode& leaf, float* recs) {
+    const uint32_t cnt = leaf.w7 & 0xFFFFu, first = leaf.w6;
+    for (uint32_t t = 0; t < cnt; ++t) {
+      const uint32_t src = bin.reordered_to_source[first + t];
+      const uint32_t* iv = indices + (size_t)src * idx_stride;
+      float* rec = recs + 16 * t;
+      float v[3][3];
+      for (int vi = 0; vi < 3; ++vi)
+        for (int k = 0; k < 3; ++k) v[vi][k] = positions[(size_t)iv[vi] * pos_stride + k];
+      for (int vi = 0; vi < 3; ++vi)
+        for (int k = 0; k < 3; ++k) rec[4 * vi + k] = v[vi][k];
+      std::memcpy(&rec[3], &src, 4);
+      if (tri_materials) std::memcpy(&rec[7], &tri_materials[src], 4);
+      float nn[3] = {0, 0, 0};
+      const bool valid = reference_normal(v[0], v[1], v[2], nn);
+      rec[12] = nn[0];
+      rec[13] = nn[1];
+      rec[14] = nn[2];
+      rec[15] = valid ? 1.0f : 0.0f;
+    }
+  });
+}
+
+WideBvhHost encode_wide_tlas(const BinaryBvhHost& tlas, const InstanceRecord* instances, uint32_t node_base) {
+  return encode_core(tlas, node_base, 0, [&](const BinaryNode& leaf, float* recs) {
+    const uint32_t cnt = leaf.w7 & 0xFFFFu, first = leaf.w6;
+    for (uint32_t i = 0; i < cnt; ++i) {
+      const uint32_t inst = tlas.reordered_to_source[first + i];
+      std::memcpy(recs + 16 * i, &instances[inst], sizeof(InstanceRecord));
+    }
+  });
 }
 
 }  // namespace vt

@@ -39,7 +39,28 @@ BinaryBvhHost build_binary_host(const float* positions, size_t position_words, c
 int collect_wide_children(const BinaryNode* nodes, uint32_t root, uint32_t out[8]);
 
 // tri_materials (optional, one per source triangle) is stored in each record's v1.w.
+// node_base / rec_base offset the encoded indices for trees concatenated into shared arrays.
 WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
-                        int idx_stride, const uint32_t* tri_materials = nullptr);
+                        int idx_stride, const uint32_t* tri_materials = nullptr, uint32_t node_base = 0,
+                        uint32_t rec_base = 0);
+
+// Top-level instance record (64 bytes): world-to-local affine rows, then
+// (BLAS root node, instance id, material, 0) as u32 bits.
+struct InstanceRecord {
+  float w2l[12];
+  uint32_t blas_root;
+  uint32_t instance_id;
+  uint32_t material;
+  uint32_t pad;
+};
+static_assert(sizeof(InstanceRecord) == 64, "instance record is 64 bytes");
+
+// Binned-SAH TLAS over instance AABBs, the reference's buildTlas
+// (shared-bvh/src/tlas.ts:859-989): aabbs = 6 doubles per instance.
+BinaryBvhHost build_tlas_host(const double* aabbs, size_t n, int max_leaf = 1, int bins = 16,
+                              int max_depth = kMaxBinaryDepth);
+
+// Wide encoding of a TLAS: leaf payload records are InstanceRecords.
+WideBvhHost encode_wide_tlas(const BinaryBvhHost& tlas, const InstanceRecord* instances, uint32_t node_base);
 
 }  // namespace vt

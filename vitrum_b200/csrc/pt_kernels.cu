@@ -194,10 +194,14 @@ __global__ void k_raygen(FrameView f, WaveBuffers w) {
 }
 
 // ---------------------------------------------------------------- material sort
+__device__ __forceinline__ uint32_t hit_material(const SceneView& sc, int4 h) {
+  if (h.z >= 0) return __float_as_uint(__ldg(sc.inst_table + 4 * (size_t)h.z + 3).z);
+  return __float_as_uint(__ldg(sc.tris + 4 * (size_t)(uint32_t)h.x + 1).w);
+}
+
 __device__ __forceinline__ uint32_t hit_key(const SceneView& sc, int4 h) {
   if (h.x < 0) return 0u;
-  const float4 v1 = __ldg(sc.tris + 4 * (size_t)(uint32_t)h.x + 1);
-  return 1u + sc.materials[__float_as_uint(v1.w)].kind;
+  return 1u + sc.materials[hit_material(sc, h)].kind;
 }
 
 __global__ void k_classify(SceneView sc, WaveBuffers w, int cur) {
@@ -280,11 +284,18 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
         }
       } else {
         const float4* rec = sc.tris + 4 * (size_t)(uint32_t)h.x;
-        const float4 v1 = __ldg(rec + 1), nr = __ldg(rec + 3);
+        const float4 nr = __ldg(rec + 3);
         const float t = __int_as_float(h.y);
-        const Material m = sc.materials[__float_as_uint(v1.w)];
+        const Material m = sc.materials[hit_material(sc, h)];
         const float3 P = o + d * t;
-        const float3 ng = f3(nr.x, nr.y, nr.z);
+        float3 ng = f3(nr.x, nr.y, nr.z);
+        if (h.z >= 0) {
+          // instance: world normal = (world-to-local)^T * local normal
+          const float4* ir = sc.inst_table + 4 * (size_t)h.z;
+          const float4 m0 = __ldg(ir), m1 = __ldg(ir + 1), m2 = __ldg(ir + 2);
+          ng = normalize(f3(m0.x * ng.x + m1.x * ng.y + m2.x * ng.z, m0.y * ng.x + m1.y * ng.y + m2.y * ng.z,
+                            m0.z * ng.x + m1.z * ng.y + m2.z * ng.z));
+        }
         const float dn = dot(d, ng);
         const bool front = dn < 0.0f;
         if (m.emissive && front) {

@@ -34,6 +34,10 @@ struct SceneView {
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
   uint32_t n_light_entries = 0;  // area group (if any) + point lights + environment (if any)
+  // two-level scenes: instance records (4 float4: world-to-local rows, (blas root, id, material, 0))
+  const float4* insts = nullptr;       // in top-level leaf order (traversal)
+  const float4* inst_table = nullptr;  // by instance index (shading)
+  uint32_t root = 0;                   // first node of the traversal
   float bias = 2e-5f;            // origin offset along the geometric normal, relative to max(1, |P|_inf)
 };
 

@@ -58,6 +58,18 @@ struct LaneRay {
   int best;  // triangle record index of the closest hit so far
 };
 
+// Per-ray traversal constants for origin o and direction d (world ray, or an
+// instance's local ray: d is not renormalised, so t is the same in both).
+__device__ __forceinline__ void set_ray(LaneRay& R, WtRay& wr, float ox, float oy, float oz, float dx, float dy,
+                                        float dz) {
+  R.ox = ox; R.oy = oy; R.oz = oz;
+  R.dx = dx; R.dy = dy; R.dz = dz;
+  auto safe = [](float d) { return fabsf(d) > 1e-30f ? d : copysignf(1e-30f, d); };
+  R.ix = __frcp_rn(safe(dx)); R.iy = __frcp_rn(safe(dy)); R.iz = __frcp_rn(safe(dz));
+  R.oct = (R.ix < 0.0f ? 4u : 0u) | (R.iy < 0.0f ? 2u : 0u) | (R.iz < 0.0f ? 1u : 0u);
+  wr = wt_setup(ox, oy, oz, dx, dy, dz);
+}
+
 // Reorders an 8-bit slot mask into key order: bit s moves to bit s ^ oct.
 __device__ __forceinline__ uint32_t xor_permute8(uint32_t m, uint32_t oct) {
   if (oct & 1u) m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
@@ -74,13 +86,14 @@ __device__ __forceinline__ uint32_t nibble_spread8(uint32_t m) {
   return m * 15u;
 }
 
-template <bool ANY, int STK>
+template <bool ANY, int STK, bool TWO>
 __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                                   const float4* __restrict__ rays, size_t n,
                                                   int4* __restrict__ hits, uint8_t* __restrict__ occluded,
                                                   int* __restrict__ status,
                                                   unsigned long long* __restrict__ ray_counter,
-                                                  const uint32_t* __restrict__ n_dev) {
+                                                  const uint32_t* __restrict__ n_dev,
+                                                  const float4* __restrict__ insts, uint32_t root) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -92,7 +105,11 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   uint2* const stack = stack_mem + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31u;
   constexpr uint32_t kFull = 0xFFFFFFFFu;
-  constexpr uint32_t kNodeGroup = 0x80000000u;  // stack x-bit: entry is a node group (else triangle group)
+  // stack entry tags in x: bit 31 node group, bit 30 instance group, both: return
+  // marker of an instance (two-level only); neither: triangle group
+  constexpr uint32_t kNodeGroup = 0x80000000u;
+  constexpr uint32_t kInstGroup = 0x40000000u;
+  constexpr uint32_t kTagMask = 0xC0000000u;
   constexpr uint32_t kChunk = 64;
 
   bool live = false, exhausted = false;
@@ -100,6 +117,8 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   const uint32_t n32 = n_dev ? *n_dev : (uint32_t)n;
   LaneRay R;
   WtRay wr;
+  float wox = 0.f, woy = 0.f, woz = 0.f, wdx = 0.f, wdy = 0.f, wdz = 0.f;  // world ray (two-level)
+  int cur_inst = -1, best_inst = -1;
   uint32_t gbase = 0, ghits = 0, gimask = 0, node = 0;
   uint32_t q0b = 0, q0m = 0, q1b = 0, q1m = 0;  // triangle-group queue (base, hit mask)
   bool expand = false;
@@ -122,16 +141,15 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       if (!live && rank < avail) {
         ray = pool_next + rank;
         const float4 r0 = __ldg(rays + 2 * (size_t)ray), r1 = __ldg(rays + 2 * (size_t)ray + 1);
-        R.ox = r0.x; R.oy = r0.y; R.oz = r0.z; R.tmin = r0.w;
-        R.dx = r1.x; R.dy = r1.y; R.dz = r1.z; R.closest = r1.w;
-        auto safe = [](float d) { return fabsf(d) > 1e-30f ? d : copysignf(1e-30f, d); };
-        R.ix = __frcp_rn(safe(R.dx)); R.iy = __frcp_rn(safe(R.dy)); R.iz = __frcp_rn(safe(R.dz));
-        R.oct = (R.ix < 0.0f ? 4u : 0u) | (R.iy < 0.0f ? 2u : 0u) | (R.iz < 0.0f ? 1u : 0u);
+        R.tmin = r0.w;
+        R.closest = r1.w;
+        set_ray(R, wr, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+        if (TWO) { wox = r0.x; woy = r0.y; woz = r0.z; wdx = r1.x; wdy = r1.y; wdz = r1.z; }
+        cur_inst = best_inst = -1;
         R.best = -1;
-        wr = wt_setup(R.ox, R.oy, R.oz, R.dx, R.dy, R.dz);
         gbase = ghits = gimask = 0;
         q0m = q1m = 0;
-        node = 0;
+        node = root;
         expand = true;
         sp = 0;
         live = true;
@@ -178,6 +196,16 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       gbase = w1.x;
       ghits = nh;
       gimask = imask;
+      if (TWO && cur_inst < 0 && th) {
+        // top level: the leaf records are instances, entered through the stack
+        if (sp < STK) {
+          stack[sp * kBlock] = make_uint2(w1.y | kInstGroup, th);
+          ++sp;
+        } else {
+          atomicOr(status, 1);
+        }
+        th = 0;
+      }
       if (th) {
         if (q0m == 0) { q0b = w1.y; q0m = th; }
         else if (q1m == 0) { q1b = w1.y; q1m = th; }
@@ -192,7 +220,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
             const float t = wt_candidate(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
                                          make_float3(c.x, c.y, c.z), R.tmin, R.closest,
                                          [rec] { return __ldg(rec + 3); });
-            if (t >= 0.0f) { R.closest = t; R.best = (int)tri; }
+            if (t >= 0.0f) { R.closest = t; R.best = (int)tri; best_inst = cur_inst; }
           }
         }
       }
@@ -213,6 +241,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       if (t >= 0.0f) {
         R.closest = t;
         R.best = (int)tri;
+        best_inst = cur_inst;
         if (ANY) { done = true; break; }
       }
     }
@@ -239,7 +268,40 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
         }
         if (sp == 0) break;
         const uint2 g = stack[(sp - 1) * kBlock];
-        if (g.x & kNodeGroup) {
+        const uint32_t tag = g.x & kTagMask;
+        if (TWO && tag == kTagMask) {
+          // return marker: leave the instance once its queued triangles are tested
+          if (q0m != 0) break;
+          --sp;
+          set_ray(R, wr, wox, woy, woz, wdx, wdy, wdz);
+          cur_inst = -1;
+        } else if (TWO && tag == kInstGroup) {
+          // enter the next instance of the group
+          --sp;
+          const uint32_t k = (uint32_t)(__ffs(g.y) - 1);
+          const uint32_t rest = g.y & (g.y - 1);
+          if (rest) { stack[sp * kBlock] = make_uint2(g.x, rest); ++sp; }
+          if (sp < STK) {
+            stack[sp * kBlock] = make_uint2(kTagMask, 0u);
+            ++sp;
+            const float4* ir = insts + 4 * (size_t)((g.x & ~kTagMask) + k);
+            const float4 m0 = __ldg(ir), m1 = __ldg(ir + 1), m2 = __ldg(ir + 2);
+            const uint4 meta = __ldg(reinterpret_cast<const uint4*>(ir + 3));
+            const float lox = fmaf(m0.x, wox, fmaf(m0.y, woy, fmaf(m0.z, woz, m0.w)));
+            const float loy = fmaf(m1.x, wox, fmaf(m1.y, woy, fmaf(m1.z, woz, m1.w)));
+            const float loz = fmaf(m2.x, wox, fmaf(m2.y, woy, fmaf(m2.z, woz, m2.w)));
+            const float ldx = fmaf(m0.x, wdx, fmaf(m0.y, wdy, m0.z * wdz));
+            const float ldy = fmaf(m1.x, wdx, fmaf(m1.y, wdy, m1.z * wdz));
+            const float ldz = fmaf(m2.x, wdx, fmaf(m2.y, wdy, m2.z * wdz));
+            set_ray(R, wr, lox, loy, loz, ldx, ldy, ldz);
+            cur_inst = (int)meta.y;
+            node = meta.x;
+            expand = true;
+            break;
+          } else {
+            atomicOr(status, 1);
+          }
+        } else if (tag == kNodeGroup) {
           --sp;
           gbase = g.x & ~kNodeGroup;
           ghits = g.y & 0xFFu;
@@ -263,39 +325,63 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
     }
     // closest: (triangle record, watertight t); k_refine_hits turns it into
     // (source id, t, u, v) in a coalesced pass with every lane busy
-    hits[ray] = make_int4(R.best, __float_as_int(R.closest), 0, 0);
+    hits[ray] = make_int4(R.best, __float_as_int(R.closest), best_inst, 0);
   }
 }
 
 // Second pass of the closest-hit query: one thread per ray, float-float
 // re-evaluation of the chosen triangle for t and barycentrics, record index
-// replaced by the source triangle id (-1 and tmax for a miss).
+// replaced by the source triangle id (-1 and tmax for a miss).  Instance hits
+// are re-evaluated in world space (the placed triangle against the world ray).
 __global__ void __launch_bounds__(256) k_refine_hits(const float4* __restrict__ tris,
                                                       const float4* __restrict__ rays, size_t n,
-                                                      int4* __restrict__ hits) {
+                                                      int4* __restrict__ hits, const float4* __restrict__ inst_table,
+                                                      const float4* __restrict__ inst_l2w,
+                                                      int* __restrict__ inst_out) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int4 h = hits[i];
+  if (inst_out) inst_out[i] = h.x < 0 ? -1 : h.z;
   if (h.x < 0) {
     hits[i] = make_int4(-1, h.y, 0, 0);
     return;
   }
-  const float4 r0 = __ldg(rays + 2 * i), r1 = __ldg(rays + 2 * i + 1);
+  float4 r0 = __ldg(rays + 2 * i), r1 = __ldg(rays + 2 * i + 1);
   const float4* rec = tris + 4 * (size_t)(uint32_t)h.x;
   const float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
+  const float3 A = make_float3(a.x, a.y, a.z), B = make_float3(b.x, b.y, b.z), C = make_float3(c.x, c.y, c.z);
   float t = __int_as_float(h.y), u = 0.0f, v = 0.0f;
   float tr, ur, vr;
-  if (ff_refine(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), make_float3(a.x, a.y, a.z),
-                make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z), &tr, &ur, &vr)) {
+  const bool placed = inst_table && h.z >= 0;
+  bool ok;
+  if (placed && inst_l2w) {
+    const float4* lr = inst_l2w + 3 * (size_t)h.z;
+    ok = ff_refine_placed(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), __ldg(lr), __ldg(lr + 1),
+                          __ldg(lr + 2), A, B, C, &tr, &ur, &vr);
+  } else {
+    if (placed) {
+      // the instance's local ray, computed as the traversal computed it
+      const float4* ir = inst_table + 4 * (size_t)h.z;
+      const float4 m0 = __ldg(ir), m1 = __ldg(ir + 1), m2 = __ldg(ir + 2);
+      const float ox = r0.x, oy = r0.y, oz = r0.z, dx = r1.x, dy = r1.y, dz = r1.z;
+      r0.x = fmaf(m0.x, ox, fmaf(m0.y, oy, fmaf(m0.z, oz, m0.w)));
+      r0.y = fmaf(m1.x, ox, fmaf(m1.y, oy, fmaf(m1.z, oz, m1.w)));
+      r0.z = fmaf(m2.x, ox, fmaf(m2.y, oy, fmaf(m2.z, oz, m2.w)));
+      r1.x = fmaf(m0.x, dx, fmaf(m0.y, dy, m0.z * dz));
+      r1.y = fmaf(m1.x, dx, fmaf(m1.y, dy, m1.z * dz));
+      r1.z = fmaf(m2.x, dx, fmaf(m2.y, dy, m2.z * dz));
+    }
+    ok = ff_refine(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), A, B, C, &tr, &ur, &vr);
+  }
+  if (ok) {
     t = tr;
     u = ur;
     v = vr;
-  } else {
+  } else if (!placed) {
     // degenerate in float-float too: report the watertight barycentrics
     WtRay wr = wt_setup(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
     WtHit wh;
-    if (wt_intersect(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z),
-                     r0.w, &wh)) {
+    if (wt_intersect(wr, A, B, C, r0.w, &wh)) {
       u = wh.bary[1];
       v = wh.bary[2];
     }
@@ -323,36 +409,44 @@ __global__ void k_watertight_eval(const float* __restrict__ cases, size_t n, vt_
   out[i] = res;
 }
 
-template <bool ANY, int STK>
+template <bool ANY, int STK, bool TWO>
 void launch_stk(const TraceArgs& a, cudaStream_t s) {
   const size_t smem = sizeof(uint2) * STK * kBlock;
   if (smem > 48 * 1024)  // opt-in above the default 48 KB dynamic limit
-    cudaFuncSetAttribute(k_trace<ANY, STK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_trace<ANY, STK, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ANY, STK>, kBlock, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ANY, STK, TWO>, kBlock, smem);
   // persistent grid: every resident slot once, never more blocks than rays need
   size_t grid = (size_t)std::max(1, sms) * (size_t)std::max(1, per_sm);
   grid = std::min(grid, (a.n + kBlock - 1) / kBlock);
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
-  k_trace<ANY, STK><<<(unsigned)grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded,
-                                                         a.status, a.counter, a.n_dev);
+  k_trace<ANY, STK, TWO><<<(unsigned)grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded,
+                                                              a.status, a.counter, a.n_dev, a.insts, a.root);
+}
+
+template <bool ANY, bool TWO>
+void launch_depth(const TraceArgs& a, cudaStream_t s) {
+  if (a.stack_depth <= 16) launch_stk<ANY, 16, TWO>(a, s);
+  else if (a.stack_depth <= 32) launch_stk<ANY, 32, TWO>(a, s);
+  else launch_stk<ANY, 64, TWO>(a, s);
 }
 
 template <bool ANY>
 void launch_trace_t(const TraceArgs& a, cudaStream_t s) {
   if (a.n == 0) return;
-  if (a.stack_depth <= 16) launch_stk<ANY, 16>(a, s);
-  else if (a.stack_depth <= 32) launch_stk<ANY, 32>(a, s);
-  else launch_stk<ANY, 64>(a, s);
+  if (a.insts) launch_depth<ANY, true>(a, s);
+  else launch_depth<ANY, false>(a, s);
 }
 
 }  // namespace
 
 void launch_trace_closest(const TraceArgs& a, cudaStream_t s) {
   launch_trace_t<false>(a, s);
-  if (a.n) k_refine_hits<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a.tris, a.rays, a.n, a.hits);
+  if (a.n)
+    k_refine_hits<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a.tris, a.rays, a.n, a.hits, a.inst_table,
+                                                                a.inst_l2w, a.inst_out);
 }
 void launch_trace_any(const TraceArgs& a, cudaStream_t s) { launch_trace_t<true>(a, s); }
 void launch_trace_closest_records(const TraceArgs& a, cudaStream_t s) { launch_trace_t<false>(a, s); }

@@ -310,20 +310,11 @@ __device__ __forceinline__ ff ff_div(ff a, ff b) {
 }
 __device__ __forceinline__ ff ff_from(float a) { return {a, 0.0f}; }
 
-// Moller-Trumbore in float-float arithmetic: exact edge/offset vectors
-// (two_sum), products with fma error terms.  Writes t, u (weight of b), v
-// (weight of c) rounded to f32.  Returns false when det is zero.
-__device__ __noinline__ bool ff_refine(const float3 O, const float3 D, const float3 A, const float3 B,
-                                       const float3 C, float* t_out, float* u_out, float* v_out) {
-  const float o[3] = {O.x, O.y, O.z}, d[3] = {D.x, D.y, D.z};
-  const float a[3] = {A.x, A.y, A.z}, b[3] = {B.x, B.y, B.z}, c[3] = {C.x, C.y, C.z};
-  ff e1[3], e2[3], ao[3], dd[3];
-  for (int k = 0; k < 3; ++k) {
-    e1[k] = ff_two_sum(b[k], -a[k]);
-    e2[k] = ff_two_sum(c[k], -a[k]);
-    ao[k] = ff_two_sum(o[k], -a[k]);
-    dd[k] = ff_from(d[k]);
-  }
+// Moller-Trumbore in float-float arithmetic: edge/offset vectors and
+// products with fma error terms.  Writes t, u (weight of b), v (weight of c)
+// rounded to f32.  Returns false when det is zero.
+__device__ __forceinline__ bool ff_refine_core(const ff e1[3], const ff e2[3], const ff ao[3], const ff dd[3],
+                                               float* t_out, float* u_out, float* v_out) {
   ff n[3] = {ff_sub(ff_mul(e1[1], e2[2]), ff_mul(e1[2], e2[1])),
              ff_sub(ff_mul(e1[2], e2[0]), ff_mul(e1[0], e2[2])),
              ff_sub(ff_mul(e1[0], e2[1]), ff_mul(e1[1], e2[0]))};
@@ -340,6 +331,53 @@ __device__ __noinline__ bool ff_refine(const float3 O, const float3 D, const flo
   *u_out = __fadd_rn(u.hi, u.lo);
   *v_out = __fadd_rn(v.hi, v.lo);
   return true;
+}
+
+// f32 ray and vertices: the edge and offset vectors are exact (two_sum).
+__device__ __noinline__ bool ff_refine(const float3 O, const float3 D, const float3 A, const float3 B,
+                                       const float3 C, float* t_out, float* u_out, float* v_out) {
+  const float o[3] = {O.x, O.y, O.z}, d[3] = {D.x, D.y, D.z};
+  const float a[3] = {A.x, A.y, A.z}, b[3] = {B.x, B.y, B.z}, c[3] = {C.x, C.y, C.z};
+  ff e1[3], e2[3], ao[3], dd[3];
+  for (int k = 0; k < 3; ++k) {
+    e1[k] = ff_two_sum(b[k], -a[k]);
+    e2[k] = ff_two_sum(c[k], -a[k]);
+    ao[k] = ff_two_sum(o[k], -a[k]);
+    dd[k] = ff_from(d[k]);
+  }
+  return ff_refine_core(e1, e2, ao, dd, t_out, u_out, v_out);
+}
+
+// rows of an affine 3x4 map applied to an f32 point in float-float: exact
+// products (fma error terms) summed with two_sum.
+__device__ __forceinline__ ff ff_affine_row(float4 m, float x, float y, float z) {
+  return ff_add(ff_add(ff_mul(ff_from(m.x), ff_from(x)), ff_mul(ff_from(m.y), ff_from(y))),
+                ff_add(ff_mul(ff_from(m.z), ff_from(z)), ff_from(m.w)));
+}
+
+// World-space refinement of a hit on an instanced triangle: the local
+// vertices are carried to world space through the instance's local-to-world
+// rows in float-float, so t, u, v are those of the placed triangle against the
+// f32 world ray, free of the rounding of the f32 world-to-local transform.
+__device__ __noinline__ bool ff_refine_placed(const float3 O, const float3 D, const float4 l0, const float4 l1,
+                                              const float4 l2, const float3 A, const float3 B, const float3 C,
+                                              float* t_out, float* u_out, float* v_out) {
+  const float3 v[3] = {A, B, C};
+  ff w[3][3];
+  for (int i = 0; i < 3; ++i) {
+    w[i][0] = ff_affine_row(l0, v[i].x, v[i].y, v[i].z);
+    w[i][1] = ff_affine_row(l1, v[i].x, v[i].y, v[i].z);
+    w[i][2] = ff_affine_row(l2, v[i].x, v[i].y, v[i].z);
+  }
+  const float o[3] = {O.x, O.y, O.z}, d[3] = {D.x, D.y, D.z};
+  ff e1[3], e2[3], ao[3], dd[3];
+  for (int k = 0; k < 3; ++k) {
+    e1[k] = ff_sub(w[1][k], w[0][k]);
+    e2[k] = ff_sub(w[2][k], w[0][k]);
+    ao[k] = ff_sub(ff_from(o[k]), w[0][k]);
+    dd[k] = ff_from(d[k]);
+  }
+  return ff_refine_core(e1, e2, ao, dd, t_out, u_out, v_out);
 }
 
 }  // namespace vt

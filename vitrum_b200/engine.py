@@ -41,8 +41,13 @@ class _PointLightDesc(ctypes.Structure):
     _fields_ = [("position", ctypes.c_float * 3), ("intensity", ctypes.c_float * 3)]
 
 
+class _InstanceDesc(ctypes.Structure):
+    _fields_ = [("mesh", ctypes.c_uint32), ("material", ctypes.c_uint32), ("local_to_world", ctypes.c_float * 16)]
+
+
 class _SceneDesc(ctypes.Structure):
-    _fields_ = [("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_size_t), ("materials", ctypes.c_void_p),
+    _fields_ = [("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_size_t), ("instances", ctypes.c_void_p),
+                ("instance_count", ctypes.c_size_t), ("materials", ctypes.c_void_p),
                 ("material_count", ctypes.c_size_t), ("point_lights", ctypes.c_void_p),
                 ("point_light_count", ctypes.c_size_t), ("environment_rgb", ctypes.c_void_p),
                 ("environment_width", ctypes.c_int32), ("environment_height", ctypes.c_int32),
@@ -94,6 +99,16 @@ class Mesh:
 
 
 @dataclass
+class Instance:
+    """A placement of meshes[mesh] (core instanced mesh; TLAS instance, shared-bvh/src/tlas.ts:859).
+
+    local_to_world is a 4x4 row-major matrix (affine, invertible)."""
+    mesh: int
+    local_to_world: np.ndarray
+    material: int = 0
+
+
+@dataclass
 class PointLight:
     position: Sequence[float]
     intensity: Sequence[float]
@@ -109,12 +124,33 @@ class Environment:
 class Scene:
     meshes: List[Mesh] = field(default_factory=list)
     materials: List[Material] = field(default_factory=list)
+    instances: List[Instance] = field(default_factory=list)
     point_lights: List[PointLight] = field(default_factory=list)
     environment: Optional[Environment] = None
 
     @property
     def triangle_count(self) -> int:
+        """Distinct triangles (prototype meshes count once however often they are placed)."""
         return int(sum(m.indices.shape[0] for m in self.meshes))
+
+    @property
+    def instanced_triangle_count(self) -> int:
+        if not self.instances:
+            return self.triangle_count
+        return int(sum(self.meshes[i.mesh].indices.shape[0] for i in self.instances))
+
+    def flattened(self) -> "Scene":
+        """The same scene with every instance baked into a world-space mesh."""
+        if not self.instances:
+            return self
+        out = []
+        for inst in self.instances:
+            m = self.meshes[inst.mesh]
+            M = np.asarray(inst.local_to_world, np.float64).reshape(4, 4)
+            p = np.asarray(m.positions, np.float64).reshape(-1, 3) @ M[:3, :3].T + M[:3, 3]
+            out.append(Mesh(p.astype(np.float32), np.asarray(m.indices, np.uint32).reshape(-1, 3), inst.material))
+        return Scene(meshes=out, materials=self.materials, point_lights=self.point_lights,
+                     environment=self.environment)
 
 
 @dataclass
@@ -204,7 +240,13 @@ class Engine:
             env = np.ascontiguousarray(scene.environment.rgb, np.float32)
             keep.append(env)
             env_ptr, eh, ew, ei = env.ctypes.data, env.shape[0], env.shape[1], scene.environment.intensity
-        desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes), ctypes.cast(mats, ctypes.c_void_p),
+        insts = (_InstanceDesc * max(1, len(scene.instances)))()
+        for i, inst in enumerate(scene.instances):
+            M = np.asarray(inst.local_to_world, np.float32).reshape(4, 4)
+            insts[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
+        desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes),
+                          ctypes.cast(insts, ctypes.c_void_p) if scene.instances else None, len(scene.instances),
+                          ctypes.cast(mats, ctypes.c_void_p),
                           len(scene.materials), ctypes.cast(pls, ctypes.c_void_p), len(scene.point_lights), env_ptr,
                           ew, eh, ei)
         N.call("vt_set_scene", self.handle, ctypes.byref(desc))
@@ -247,6 +289,19 @@ class Engine:
         N.call("vt_capture_moments", self.handle, ctypes.c_void_p(m.ctypes.data), ctypes.c_void_p(v.ctypes.data),
                m.size)
         return m, v
+
+    def trace_rays(self, rays: np.ndarray):
+        """Closest hits of (n, 8) float32 rays [ox oy oz tmin dx dy dz tmax] against the scene.
+
+        Returns (hits, instances): a HIT_DTYPE array (prim, t, u, v) and an
+        int32 array of instance indices (-1 on a miss or without instances)."""
+        from .bvh import HIT_DTYPE
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        hits = np.empty(r.shape[0], HIT_DTYPE)
+        inst = np.empty(r.shape[0], np.int32)
+        N.call("vt_trace_rays", self.handle, ctypes.c_void_p(r.ctypes.data), r.shape[0],
+               ctypes.c_void_p(hits.ctypes.data), ctypes.c_void_p(inst.ctypes.data))
+        return hits, inst
 
     def stats(self) -> dict:
         s = _EngineStats()

@@ -173,3 +173,118 @@ def box_room(wall_cells: int = 128, box_cells: int = 64):
     meshes.append(Mesh(p, t, 5))
     cam = Camera(eye=(0.5, 0.5, 1.94), target=(0.5, 0.5, 0.0), fov_y_deg=40.0)
     return Scene(meshes=meshes, materials=mats), cam
+
+
+# ---------------------------------------------------------------- instanced cloud
+def icosphere(level: int):
+    """Unit icosphere: the icosahedron with each face split into 4, `level`
+    times, new vertices projected to the sphere.  20 * 4**level triangles,
+    outward winding; shared edges produce bit-identical midpoints."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                  [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4],
+                  [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8],
+                  [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    for _ in range(level):
+        a, b, c = f[:, 0], f[:, 1], f[:, 2]
+        edges = np.concatenate([np.stack([a, b], 1), np.stack([b, c], 1), np.stack([c, a], 1)])
+        key = np.sort(edges, axis=1)
+        uniq, inv = np.unique(key, axis=0, return_inverse=True)
+        mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        m = inv.reshape(3, -1) + v.shape[0]
+        ab, bc, ca = m[0], m[1], m[2]
+        v = np.concatenate([v, mid])
+        f = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1), np.stack([c, ca, bc], 1),
+                            np.stack([ab, bc, ca], 1)])
+    return v.astype(np.float32), f.astype(np.uint32)
+
+
+def torus(major: int = 256, minor: int = 64, R: float = 0.7, r: float = 0.3):
+    """Torus around +y with `major` x `minor` segments (2 triangles each), outward winding."""
+    u = 2 * np.pi * np.arange(major) / major
+    w = 2 * np.pi * np.arange(minor) / minor
+    U, W = np.meshgrid(u, w, indexing="ij")
+    ring = R + r * np.cos(W)
+    pos = np.stack([ring * np.cos(U), r * np.sin(W), ring * np.sin(U)], -1).reshape(-1, 3).astype(np.float32)
+    i = np.arange(major)[:, None]
+    j = np.arange(minor)[None, :]
+    a = i * minor + j
+    b = ((i + 1) % major) * minor + j
+    c = ((i + 1) % major) * minor + (j + 1) % minor
+    d = i * minor + (j + 1) % minor
+    tris = np.stack([np.stack([a, d, c], -1), np.stack([a, c, b], -1)], -2).reshape(-1, 3).astype(np.uint32)
+    return pos, tris
+
+
+def random_rotations(u: np.ndarray) -> np.ndarray:
+    """Uniform rotations from (n, 3) uniforms (Shoemake's unit-quaternion method)."""
+    u1, u2, u3 = u[:, 0], u[:, 1], u[:, 2]
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], 1)
+    x, y, z, w = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+def gradient_sky(width: int = 256, height: int = 128, horizon=(0.9, 0.9, 1.0), zenith=(0.25, 0.45, 0.9),
+                 ground=(0.18, 0.16, 0.14)):
+    """Analytic gradient sky baked to an equirectangular image (row 0 at +y):
+    zenith-to-horizon blend by elevation above the horizon, flat ground below."""
+    theta = np.pi * (np.arange(height) + 0.5) / height
+    el = np.cos(theta)  # +1 at the zenith
+    t = np.clip(el, 0.0, 1.0) ** 0.5
+    sky = (1 - t)[:, None] * np.asarray(horizon) + t[:, None] * np.asarray(zenith)
+    rows = np.where(el[:, None] >= 0, sky, np.asarray(ground))
+    return np.ascontiguousarray(np.broadcast_to(rows[:, None, :], (height, width, 3)), np.float32)
+
+
+def instanced_cloud(n_instances: int = 1024, seed: int = 3, n_points: int = 32, sphere_levels=(3, 4, 5, 6),
+                    torus_segments=(256, 64), cube_cells=(32, 64, 128), extent: float = 20.0):
+    """Two-level instanced workload: 8 prototype meshes (icospheres at levels
+    3-6, a 256 x 64 torus, cubes with 32/64/128 cells per edge), `n_instances`
+    placements with a uniform random rotation, scale U[0.2, 1] and translation
+    U[-extent, extent]^3; one material per instance (50% Lambert albedo
+    U[0.1, 0.9]^3, 30% GGX conductor roughness U[0.05, 0.6], 20% dielectric IOR
+    U[1.3, 1.7]); a gradient sky and `n_points` point lights of intensity
+    U[5, 50].  Returns (engine.Scene, engine.Camera)."""
+    from .engine import Camera, Environment, Instance, Material, Mesh, PointLight, Scene
+    meshes = []
+    for lv in sphere_levels:
+        p, t = icosphere(lv)
+        meshes.append(Mesh(p, t, 0))
+    p, t = torus(*torus_segments)
+    meshes.append(Mesh(p, t, 0))
+    for n in cube_cells:
+        p, t = box_mesh((-0.6, -0.6, -0.6), (0.6, 0.6, 0.6), n)
+        meshes.append(Mesh(p, t, 0))
+    n = n_instances
+    u = uniform(seed, 10, 16 * n).reshape(n, 16)
+    rot = random_rotations(u[:, 0:3])
+    scale = 0.2 + 0.8 * u[:, 3]
+    trans = (u[:, 4:7] * 2 - 1) * extent
+    which = np.minimum((u[:, 7] * len(meshes)).astype(np.int64), len(meshes) - 1)
+    kind = u[:, 8]
+    mats, insts = [], []
+    for i in range(n):
+        if kind[i] < 0.5:
+            mats.append(Material(base_color=tuple(0.1 + 0.8 * u[i, 9:12])))
+        elif kind[i] < 0.8:
+            mats.append(Material(base_color=tuple(0.5 + 0.45 * u[i, 9:12]), roughness=0.05 + 0.55 * u[i, 12],
+                                 metallic=1.0))
+        else:
+            mats.append(Material(base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.3 + 0.4 * u[i, 12]))
+        M = np.eye(4)
+        M[:3, :3] = rot[i] * scale[i]
+        M[:3, 3] = trans[i]
+        insts.append(Instance(mesh=int(which[i]), local_to_world=M.astype(np.float32), material=i))
+    lp = uniform(seed, 11, 4 * n_points).reshape(n_points, 4)
+    lights = [PointLight(tuple((lp[k, :3] * 2 - 1) * extent), (5 + 45 * lp[k, 3],) * 3) for k in range(n_points)]
+    env = Environment(gradient_sky(), 1.0)
+    cam = Camera(eye=(0.0, 6.0, 3.2 * extent), target=(0.0, 0.0, 0.0), fov_y_deg=45.0, near=0.01,
+                 far=20.0 * extent)
+    return Scene(meshes=meshes, materials=mats, instances=insts, point_lights=lights, environment=env), cam
