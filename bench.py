@@ -20,6 +20,8 @@ step = one frame rendered from a cleared accumulation.  Metric: Mrays/s
   the measured HBM copy bandwidth.
 * query: the closest-hit query workload (65,536 triangles, 1,048,576 rays)
   with its own roofline, reported in the same line.
+* instanced: the two-level workload (1024 instances, 1920x1080, 16 spp, 8
+  bounces) in the same line: Mrays/s, ms/frame, stage times.
 * cpu_baseline / --impl reference: the C restatement (oracle) of the same
   estimator on all host cores on a bounded crop (no reference CPU integrator
   exists at this scale; the reference's own CPU tracer is a Lambert-only
@@ -77,6 +79,14 @@ def _profile_value(name, key):
         if line.startswith(key + ":"):
             return float(line.split(":")[1].split()[0])
     return None
+
+
+def _scaled_traffic(rays_per_frame):
+    """DRAM bytes of the traversal launches per frame: the ncu-measured bytes per
+    extension ray of a bounce-0 launch (profiles/path_trace_box_room.txt) times
+    the frame's traced rays (an estimate: shadow rays are assumed to cost the same)."""
+    b = _profile_value("path_trace_box_room.txt", "dram_bytes_per_extension_ray")
+    return None if b is None else b * rays_per_frame
 
 
 def _visits():
@@ -236,6 +246,56 @@ def run_query(args, dev, local, rank, world, barrier):
     }
 
 
+# ------------------------------------------------------------------ instanced workload
+I_W, I_H, I_SPP, I_BOUNCES = 1920, 1080, 16, 8
+
+
+def run_instanced(args, dev, local, barrier):
+    """1024-instance two-level scene (8 prototypes, 399,616 distinct / 50,961,408
+    instanced triangles), gradient sky + 32 point lights, 1920x1080, 16 spp, 8 bounces."""
+    import torch
+    from vitrum_b200 import scenes
+    from vitrum_b200.engine import Engine
+    sc, cam = scenes.instanced_cloud()
+    e = Engine(device=local, max_bounces=I_BOUNCES)
+    t0 = time.perf_counter()
+    e.set_scene(sc)
+    build_s = time.perf_counter() - t0
+    steps = max(1, min(args.steps, 3))
+
+    def frame(seed):
+        e.reset()
+        e.render_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=seed)
+
+    frame(7)
+    e.reset()
+    stages = e.profile_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=8)
+    torch.cuda.synchronize(dev)
+    barrier()
+    r0 = e.stats()
+    ms = []
+    for i in range(steps):
+        frame(100 + i)
+        ms.append(e.stats()["last_frame_ms"])
+    torch.cuda.synchronize(dev)
+    barrier()
+    r1 = e.stats()
+    rays = (r1["closest_rays"] - r0["closest_rays"]) + (r1["shadow_rays"] - r0["shadow_rays"])
+    dev_s = sum(ms) / 1e3
+    e.dispose()
+    return {
+        "workload": "two-level instanced cloud: 1024 instances of 8 prototype meshes (icospheres levels 3-6, "
+                    "256x64 torus, cubes 32/64/128 cells per edge), 399,616 distinct / 50,961,408 instanced "
+                    "triangles, gradient sky + 32 point lights, 1920x1080, 16 spp, max 8 bounces",
+        "value": rays / dev_s / 1e6, "unit": "Mrays/s", "ms_per_frame": dev_s * 1e3 / steps,
+        "samples_per_s": I_W * I_H * I_SPP * steps / dev_s, "frames": steps,
+        "rays_per_frame": {"extension": (r1["closest_rays"] - r0["closest_rays"]) / steps,
+                           "shadow": (r1["shadow_rays"] - r0["shadow_rays"]) / steps},
+        "stages_ms": {k: round(v, 3) for k, v in stages.items() if k.endswith("_ms")},
+        "scene_build_s": round(build_s, 3),
+    }
+
+
 # ------------------------------------------------------------------ path tracing workload
 def run_ours(args, rank, world, local):
     import torch
@@ -305,6 +365,7 @@ def run_ours(args, rank, world, local):
     e2e = world * rays / e2e_s / 1e6
 
     query = run_query(args, dev, local, rank, world, barrier) if not args.no_query else None
+    instanced = run_instanced(args, dev, local, barrier) if not args.no_instanced else None
 
     if rank == 0:
         vc = _visits()["box_room_pt_512_64spp_5b"]
@@ -334,17 +395,19 @@ def run_ours(args, rank, world, local):
             "stages_ms": {k: round(v, 3) for k, v in stages.items() if k.endswith("_ms")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": _profile_value("path_trace_box_room.txt", "dram_bytes_per_trace_launch"),
+                         "traffic": _scaled_traffic(per_frame_closest + per_frame_shadow),
                          "peak_kind": peak_kind, "kernel": "k_trace (extension + shadow launches)",
                          "model": f"extension {vc['closest_bytes_per_ray']:.1f} B/ray, shadow "
                                   f"{vc['shadow_bytes_per_ray']:.1f} B/ray (oracle visit counts)",
-                         "trace_ms_per_frame": trace_s * 1e3},
+                         "trace_ms_per_frame": trace_s * 1e3,
+                         "per": "frame (all k_trace launches of one frame)"},
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(ctypes.c_float) * 32 + 20,
                     "d2h_bytes_per_step": W * H * 16},
             "gpu_launches": kernels_per_frame * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
             "query": query,
+            "instanced": instanced,
         }
         print(json.dumps(line), flush=True)
     e.dispose()
@@ -361,6 +424,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-query", action="store_true")
+    ap.add_argument("--no-instanced", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = _env_rank()
