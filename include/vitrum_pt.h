@@ -312,6 +312,55 @@ typedef struct vt_watertight_result {
 vt_status vt_watertight_eval_device(int32_t device, const float* d_cases, size_t n, vt_watertight_result* d_out,
                                     void* cuda_stream);
 
+/* ------------------------------------------------------------------ */
+/* Neural radiance cache (walkaround-hybrid/src/neural/nrc/)            */
+/* ------------------------------------------------------------------ */
+
+typedef struct vt_nrc vt_nrc;
+
+/* NrcConfig (nrcSubsystem.ts:116-132) with the hash grid and optimiser
+ * settings that matter here.  Fixed: 2 features per entry, 64-wide MLP with
+ * 5 hidden ReLU layers and 3 linear outputs, fp16 weights and activations with
+ * fp32 accumulation, Adam beta 0.9 / 0.999, eps 1e-8. */
+typedef struct vt_nrc_config {
+  int32_t levels;            /* hash-grid levels, 1..16 */
+  int32_t log2_table_size;   /* entries per level = 2^log2_table_size, 4..24 */
+  float base_resolution;     /* level l resolution = floor(base * growth^l) */
+  float growth;
+  float learning_rate;       /* MLP */
+  float table_learning_rate; /* hash grid */
+  float aabb_min[3];         /* positions are normalised into this box */
+  float aabb_max[3];
+  uint32_t seed;             /* weight / table initialisation */
+} vt_nrc_config;
+
+/* Features of one cache query or training sample, 16 floats:
+ * position xyz, outgoing direction xyz (unit), normal xyz, roughness,
+ * diffuse albedo rgb, specular albedo rgb.  A training sample appends the
+ * target radiance rgb and one unused float (20 floats). */
+#define VT_NRC_RECORD_FLOATS 16
+#define VT_NRC_SAMPLE_FLOATS 20
+#define VT_NRC_WEIGHT_COUNT (6 * 64 * 64) /* [layer][out][in]; layer 5 uses rows 0..2 */
+
+/* NrcSubsystem construction (nrcSubsystem.ts resolveNrcConfig + allocation). */
+vt_status vt_nrc_create(int32_t device, const vt_nrc_config* config, vt_nrc** out);
+vt_status vt_nrc_destroy(vt_nrc* nrc);
+/* Cache query (nrcQuery.wgsl.ts): rgb[3 i..] = network(records[16 i..]), host arrays. */
+vt_status vt_nrc_query(vt_nrc* nrc, const float* records, size_t n, float* rgb);
+/* One optimiser step on n samples (fusedMlpTrainer.ts train step + the table
+ * Adam of hashGridTableTrainer.ts); *loss receives the mean relative-L2 loss
+ * before the step (may be NULL). */
+vt_status vt_nrc_train(vt_nrc* nrc, const float* samples, size_t n, float* loss);
+/* Gradients of the mean loss over n samples without an update (the
+ * nrcEncodeBackwardHarness.ts / fusedMlpHarness.ts check path).  grad_table
+ * receives levels * 2^log2 * 2 floats (may be NULL). */
+vt_status vt_nrc_gradients(vt_nrc* nrc, const float* samples, size_t n, float* grad_weights, float* grad_table,
+                           float* loss);
+/* NrcStateSnapshot (nrcStateSnapshot.ts): f32 master weights and table. */
+vt_status vt_nrc_get_params(vt_nrc* nrc, float* weights, float* table);
+/* Replaces the parameters and clears the optimiser state. */
+vt_status vt_nrc_set_params(vt_nrc* nrc, const float* weights, const float* table);
+
 #ifdef __cplusplus
 }
 #endif

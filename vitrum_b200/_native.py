@@ -70,6 +70,13 @@ SIGNATURES = {
     "vt_capture_moments": [P, P, P, SZ],
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
     "vt_trace_rays": [P, P, SZ, P, P],
+    "vt_nrc_create": [I32, P, P],
+    "vt_nrc_destroy": [P],
+    "vt_nrc_query": [P, P, SZ, P],
+    "vt_nrc_train": [P, P, SZ, P],
+    "vt_nrc_gradients": [P, P, SZ, P, P, P],
+    "vt_nrc_get_params": [P, P, P],
+    "vt_nrc_set_params": [P, P, P],
     "vt_reset": [P],
     "vt_engine_get_stats": [P, P],
     "vt_destroy": [P],
