@@ -22,6 +22,9 @@ step = one frame rendered from a cleared accumulation.  Metric: Mrays/s
   with its own roofline, reported in the same line.
 * instanced: the two-level workload (1024 instances, 1920x1080, 16 spp, 8
   bounces) in the same line: Mrays/s, ms/frame, stage times.
+* nrc: equal-time relMSE of the neural-radiance-cache path tracer against
+  plain path tracing on the instanced scene (480x270, 65,536-spp FP64 oracle),
+  and both frame costs at 1920x1080 x 16 spp.
 * cpu_baseline / --impl reference: the C restatement (oracle) of the same
   estimator on all host cores on a bounded crop (no reference CPU integrator
   exists at this scale; the reference's own CPU tracer is a Lambert-only
@@ -296,6 +299,86 @@ def run_instanced(args, dev, local, barrier):
     }
 
 
+# ------------------------------------------------------------------ radiance cache workload
+NRC_W, NRC_H, NRC_SPP, NRC_WARM, NRC_FRAMES = 480, 270, 16, 32, 8
+
+
+def _relmse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def run_nrc(args, dev, local, barrier):
+    """Equal-time relMSE, neural radiance cache vs plain path tracing, on the
+    1024-instance scene at 480x270 (a quarter of 1920x1080 per side, so that
+    the 65,536-spp FP64-accumulated oracle fits the run), 8 bounces, 16 spp per
+    frame, cache warmed by NRC_WARM frames of online training first; plus the
+    per-frame costs of both at 1920x1080 x 16 spp."""
+    import torch
+    from vitrum_b200 import scenes
+    from vitrum_b200.engine import Engine
+    sc, cam = scenes.instanced_cloud()
+    B = I_BOUNCES
+    t0 = time.perf_counter()
+    o = Engine(device=local, max_bounces=B, oracle_accumulation=True, max_samples_per_pixel=1 << 20)
+    o.set_scene(sc)
+    done = 0
+    while done < args.oracle_spp:
+        k = min(2048, args.oracle_spp - done)
+        o.render_frame(cam, NRC_W, NRC_H, samples=k, frame_seed=4242)
+        done += k
+    ref, _ = o.capture_moments()
+    o.dispose()
+    oracle_s = time.perf_counter() - t0
+
+    def curve(nrc):
+        e = Engine(device=local, max_bounces=B, max_samples_per_pixel=1 << 20)
+        e.set_scene(sc)
+        if nrc:
+            e.set_nrc(prefix_bounces=1, train_steps=4, train_batch=65536)
+            for _ in range(NRC_WARM):
+                e.render_frame(cam, NRC_W, NRC_H, samples=NRC_SPP, frame_seed=7)
+            e.reset()
+        t, pts = 0.0, []
+        for f in range(NRC_FRAMES):
+            e.render_frame(cam, NRC_W, NRC_H, samples=NRC_SPP, frame_seed=7)
+            t += e.stats()["last_frame_ms"]
+            pts.append((t, _relmse(e.capture_frame()[..., :3].astype(np.float64), ref)))
+        e.reset()
+        full = e.profile_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=8)
+        e.dispose()
+        return pts, full
+
+    plain, plain_full = curve(False)
+    nrc, nrc_full = curve(True)
+
+    def at(pts, t):  # relMSE of the accumulated image at device time t (log-linear interpolation)
+        ts = [p[0] for p in pts]
+        if t <= ts[0]:
+            return pts[0][1] * ts[0] / t  # fewer samples than one frame: variance ~ 1/time
+        for (ta, ra), (tb, rb) in zip(pts, pts[1:]):
+            if t <= tb:
+                w = (t - ta) / (tb - ta)
+                return float(np.exp((1 - w) * np.log(ra) + w * np.log(rb)))
+        return pts[-1][1] * ts[-1] / t
+    budgets = [nrc[k][0] for k in (0, 1, 3, 7)]
+    table = [{"ms": round(b, 2), "nrc": round(at(nrc, b), 5), "plain": round(at(plain, b), 5),
+              "ratio": round(at(plain, b) / at(nrc, b), 2)} for b in budgets]
+    return {
+        "workload": "1024-instance cloud, 480x270, 8 bounces, 16 spp per frame; NRC: hash grid 16 x 2^19 x 2 fp16 "
+                    "(base 16, growth 1.5), 64-input MLP 5 x 64 ReLU + 3, fp16/fp32-accumulate on tcgen05, 4 Adam "
+                    "steps x 65,536 samples per frame, 1-bounce prefix; cache warmed by %d frames" % NRC_WARM,
+        "oracle": {"spp": args.oracle_spp, "accumulation": "fp64", "seconds": round(oracle_s, 1)},
+        "metric": "relMSE = mean((x - ref)^2 / (ref^2 + 1e-2)) at equal device time",
+        "equal_time": table,
+        "nrc_curve": [(round(t, 2), round(r, 5)) for t, r in nrc],
+        "plain_curve": [(round(t, 2), round(r, 5)) for t, r in plain],
+        "full_frame_1920x1080_16spp_ms": {"plain": round(plain_full["frame_ms"], 2),
+                                          "nrc": round(nrc_full["frame_ms"], 2),
+                                          "nrc_train_ms": round(nrc_full["nrc_train_ms"], 2),
+                                          "nrc_query_ms": round(nrc_full["nrc_query_ms"], 2)},
+    }
+
+
 # ------------------------------------------------------------------ path tracing workload
 def run_ours(args, rank, world, local):
     import torch
@@ -366,6 +449,7 @@ def run_ours(args, rank, world, local):
 
     query = run_query(args, dev, local, rank, world, barrier) if not args.no_query else None
     instanced = run_instanced(args, dev, local, barrier) if not args.no_instanced else None
+    nrc = run_nrc(args, dev, local, barrier) if not args.no_nrc else None
 
     if rank == 0:
         vc = _visits()["box_room_pt_512_64spp_5b"]
@@ -408,6 +492,7 @@ def run_ours(args, rank, world, local):
             "cpu_baseline": cpu,
             "query": query,
             "instanced": instanced,
+            "nrc": nrc,
         }
         print(json.dumps(line), flush=True)
     e.dispose()
@@ -425,6 +510,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-query", action="store_true")
     ap.add_argument("--no-instanced", action="store_true")
+    ap.add_argument("--no-nrc", action="store_true")
+    ap.add_argument("--oracle-spp", type=int, default=65536)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = _env_rank()

@@ -256,6 +256,8 @@ typedef struct vt_stage_times {
   double frame_ms;
   int32_t trace_closest_launches;
   int32_t trace_shadow_launches;
+  double nrc_train_ms;     /* training wave, targets and optimiser steps (0 without the cache) */
+  double nrc_query_ms;     /* cache inference of the render waves */
 } vt_stage_times;
 
 /* createPTEngine_WebGPU (pt-webgpu/src/index.ts:2363) */
@@ -360,6 +362,25 @@ vt_status vt_nrc_gradients(vt_nrc* nrc, const float* samples, size_t n, float* g
 vt_status vt_nrc_get_params(vt_nrc* nrc, float* weights, float* table);
 /* Replaces the parameters and clears the optimiser state. */
 vt_status vt_nrc_set_params(vt_nrc* nrc, const float* weights, const float* table);
+
+/* Path tracing with the cache (NrcSubsystem driven by the engine; Mueller et
+ * al. 2021 as the reference runs it): every frame a training wave of plain
+ * paths from random pixels records each vertex's features and the radiance
+ * gathered after it (targets), `train_steps` Adam steps of `train_batch`
+ * samples follow, then the render waves trace `prefix_bounces` bounces and end
+ * each path in a cache query at the next vertex.  For the first
+ * `warmup_frames` frames the render waves are plain path tracing. */
+typedef struct vt_nrc_render_options {
+  int32_t enabled;          /* 0: plain path tracing */
+  int32_t prefix_bounces;   /* bounces before the query (>= 1; 1 queries the second vertex) */
+  int32_t train_steps;      /* optimiser steps per frame (4) */
+  int32_t train_batch;      /* samples per step (65536) */
+  int32_t train_paths;      /* training paths per frame (0: train_steps * train_batch / 2) */
+  int32_t warmup_frames;    /* plain frames while the cache warms up */
+  vt_nrc_config cache;      /* aabb is replaced by the scene's bounds */
+} vt_nrc_render_options;
+
+vt_status vt_set_nrc(vt_engine* engine, const vt_nrc_render_options* options);
 
 #ifdef __cplusplus
 }

@@ -70,6 +70,7 @@ SIGNATURES = {
     "vt_capture_moments": [P, P, P, SZ],
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
     "vt_trace_rays": [P, P, SZ, P, P],
+    "vt_set_nrc": [P, P],
     "vt_nrc_create": [I32, P, P],
     "vt_nrc_destroy": [P],
     "vt_nrc_query": [P, P, SZ, P],

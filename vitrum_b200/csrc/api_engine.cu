@@ -20,12 +20,23 @@
 #include <vector>
 
 #include "bvh_host.h"
+#include "nrc_cache.h"
 #include "pt_kernels.h"
 #include "traverse.h"
 #include "vt_common.h"
 
 using vt::DeviceBuffer;
 using vt::fail;
+
+// Radiance-cache state of an engine.
+struct NrcEngine {
+  vt_nrc_render_options opts{};
+  std::unique_ptr<vt::nrc::Cache> cache;
+  vt::DeviceBuffer<float4> records, queries, samples;
+  vt::DeviceBuffer<uint32_t> seed;
+  uint32_t train_paths = 0;
+  int frames = 0;  // frames rendered since the cache was created
+};
 
 struct vt_engine {
   int device = 0;
@@ -75,9 +86,11 @@ struct vt_engine {
   DeviceBuffer<uint8_t> occluded;
   DeviceBuffer<unsigned long long> trace_counter, totals;
   DeviceBuffer<int> trace_status;
-  // graph cache: one executable per spp_wave value
+  std::unique_ptr<NrcEngine> nrc;
+  // graph cache: one executable per wave shape and mode
   struct Graph {
     uint32_t spp_wave = 0, bounces = 0;
+    int mode = 0;
     cudaGraphExec_t exec = nullptr;
   };
   std::vector<Graph> graphs;
@@ -102,6 +115,8 @@ struct vt_engine {
 };
 
 namespace {
+
+void nrc_rebuild(vt_engine* e);
 
 // ---------------------------------------------------------------- matrices
 void mat_mul_cm(const double* a, const double* b, double* out) {  // column-major 4x4: out = a * b
@@ -422,6 +437,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   e->ntri = (int64_t)ntri;
   e->n_emitters = (int64_t)v.n_emitters;
   e->has_scene = true;
+  if (e->nrc) nrc_rebuild(e);
   e->samples = 0;
   if (e->accum.ptr) VT_CUDA(cudaMemset(e->accum.ptr, 0, e->accum.bytes()));
   if (e->sum64.ptr) VT_CUDA(cudaMemset(e->sum64.ptr, 0, e->sum64.bytes()));
@@ -464,12 +480,18 @@ vt::pt::WaveBuffers wave_buffers(vt_engine* e) {
   w.counters = e->counters.ptr;
   w.trace_counter = e->trace_counter.ptr;
   w.trace_status = e->trace_status.ptr;
+  if (e->nrc) {
+    w.nrc_records = e->nrc->records.ptr;
+    w.nrc_queries = e->nrc->queries.ptr;
+    w.nrc_seed = e->nrc->seed.ptr;
+  }
   return w;
 }
 
 // Optional per-stage event pairs (profiling; never used while capturing a graph).
 struct StageTimer {
-  enum Stage { kRaygen, kTraceClosest, kSort, kShade, kTraceShadow, kResolve, kAccumulate, kStages };
+  enum Stage { kRaygen, kTraceClosest, kSort, kShade, kTraceShadow, kResolve, kAccumulate, kNrcTrain, kNrcQuery,
+               kStages };
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
   int open_stage = -1;
   cudaEvent_t open_ev = nullptr;
@@ -498,7 +520,53 @@ struct StageTimer {
   }
 };
 
-void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t s, StageTimer* tm = nullptr) {
+// (Re)creates the cache over the scene's bounds (training starts over).
+void nrc_rebuild(vt_engine* e) {
+  NrcEngine& n = *e->nrc;
+  vt::nrc::Config c;
+  const vt_nrc_config& k = n.opts.cache;
+  c.levels = k.levels;
+  c.log2_table = k.log2_table_size;
+  c.base_resolution = k.base_resolution;
+  c.growth = k.growth;
+  c.lr = k.learning_rate;
+  c.table_lr = k.table_learning_rate;
+  float mn[3] = {0, 0, 0}, mx[3] = {1, 1, 1};
+  if (e->has_scene && !e->binary.nodes.empty()) {
+    const vt::BinaryNode& r = e->binary.nodes[0];
+    for (int i = 0; i < 3; ++i) {
+      const float pad = 1e-3f * std::max(1e-3f, r.mx[i] - r.mn[i]);
+      if (r.mx[i] >= r.mn[i]) { mn[i] = r.mn[i] - pad; mx[i] = r.mx[i] + pad; }
+    }
+  }
+  for (int i = 0; i < 3; ++i) { c.aabb_min[i] = mn[i]; c.aabb_max[i] = mx[i]; }
+  n.cache = std::make_unique<vt::nrc::Cache>(c, k.seed);
+  n.frames = 0;
+  e->drop_graphs();
+}
+
+void ensure_nrc_buffers(vt_engine* e, uint32_t render_paths) {
+  NrcEngine& n = *e->nrc;
+  const size_t rec = (size_t)n.train_paths * (size_t)e->opts.max_bounces * 6;
+  const size_t smp = (size_t)n.opts.train_steps * (size_t)n.opts.train_batch * 5;
+  const size_t qry = (size_t)std::max(render_paths, e->capacity) * 5;
+  if (n.records.count < rec || n.samples.count < smp || n.queries.count < qry || !n.seed.ptr) {
+    e->drop_graphs();
+    if (n.records.count < rec) n.records.resize(rec);
+    if (n.samples.count < smp) n.samples.resize(smp);
+    if (n.queries.count < qry) n.queries.resize(qry);
+    if (!n.seed.ptr) {
+      n.seed.resize(1);
+      VT_CUDA(cudaMemset(n.seed.ptr, 0, sizeof(uint32_t)));
+    }
+  }
+}
+
+// Wave modes: plain path tracing, render with cache queries, cache training.
+enum WaveMode : int { kPlain = 0, kNrcRender = 1, kNrcTrain = 2 };
+
+void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t s, StageTimer* tm = nullptr,
+                 int mode = kPlain) {
   auto B = [&](int st) { if (tm) tm->begin(st, s); };
   auto E = [&]() { if (tm) tm->end(s); };
   vt::pt::FrameView f;
@@ -510,6 +578,15 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
   f.max_bounces = bounces;
   f.paths = f.width * f.height * spp_wave;
   f.sort_by_material = e->opts.sort_by_material >= 0 ? 1u : 0u;
+  if (mode == kNrcTrain) {
+    f.train = 1;
+    f.paths = e->nrc->train_paths;
+    f.record_bounces = bounces;
+    VT_CUDA(cudaMemsetAsync(e->nrc->records.ptr, 0, e->nrc->records.bytes(), s));
+  } else if (mode == kNrcRender) {
+    f.nrc_prefix = bounces - 1;
+  }
+  VT_CUDA(cudaMemsetAsync(e->counters.ptr + vt::pt::kCntQuery, 0, 2 * sizeof(uint32_t), s));
   const vt::pt::WaveBuffers w = wave_buffers(e);
   vt::pt::AccumView a;
   a.accum = e->accum.ptr;
@@ -558,24 +635,54 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     E();
     cur ^= 1;
   }
+  if (mode == kNrcTrain) {
+    B(StageTimer::kNrcTrain);
+    const NrcEngine& n = *e->nrc;
+    vt::pt::launch_nrc_targets(w, f.paths, bounces, n.samples.ptr,
+                               (uint32_t)(n.opts.train_steps * n.opts.train_batch), s);
+    E();
+    return;
+  }
+  if (mode == kNrcRender) {
+    B(StageTimer::kNrcQuery);
+    e->nrc->cache->query(w.nrc_queries, 5, w.counters + vt::pt::kCntQuery, cap, nullptr, w.radiance, s);
+    E();
+  }
   B(StageTimer::kAccumulate);
   vt::pt::launch_accumulate(f, w, a, s);
   E();
 }
 
-cudaGraphExec_t wave_graph(vt_engine* e, uint32_t spp_wave, uint32_t bounces) {
+cudaGraphExec_t wave_graph(vt_engine* e, uint32_t spp_wave, uint32_t bounces, int mode = kPlain) {
   for (auto& g : e->graphs)
-    if (g.spp_wave == spp_wave && g.bounces == bounces) return g.exec;
+    if (g.spp_wave == spp_wave && g.bounces == bounces && g.mode == mode) return g.exec;
   cudaGraph_t graph = nullptr;
   VT_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-  record_wave(e, spp_wave, bounces, e->stream);
+  record_wave(e, spp_wave, bounces, e->stream, nullptr, mode);
   VT_CUDA(cudaStreamEndCapture(e->stream, &graph));
   cudaGraphExec_t exec = nullptr;
   cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
   VT_CUDA(err);
-  e->graphs.push_back({spp_wave, bounces, exec});
+  e->graphs.push_back({spp_wave, bounces, mode, exec});
   return exec;
+}
+
+// Training part of a frame: one training wave (graph), then the optimiser
+// steps (direct launches: the bias corrections change every step).
+void nrc_train(vt_engine* e, uint32_t bounces, StageTimer* tm) {
+  NrcEngine& n = *e->nrc;
+  cudaStream_t s = e->stream;
+  if (tm) {
+    record_wave(e, 1, bounces, s, tm, kNrcTrain);
+    tm->begin(StageTimer::kNrcTrain, s);
+  } else {
+    VT_CUDA(cudaGraphLaunch(wave_graph(e, 1, bounces, kNrcTrain), s));
+  }
+  const size_t stride = 5 * (size_t)n.opts.train_batch;
+  for (int k = 0; k < n.opts.train_steps; ++k)
+    n.cache->train_step(n.samples.ptr + stride * k, (uint32_t)n.opts.train_batch, s);
+  if (tm) tm->end(s);
 }
 
 void reset_accumulation(vt_engine* e) {
@@ -636,22 +743,47 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   spp_wave = std::min(spp_wave, spp);
   while (spp % spp_wave) --spp_wave;  // equal waves: one graph per frame shape
   ensure_capacity(e, wh * spp_wave);
+  // with the cache: train, then render waves that end in cache queries
+  int mode = kPlain;
+  uint32_t wave_bounces = bounces;
+  if (e->nrc) {
+    NrcEngine& n = *e->nrc;
+    ensure_capacity(e, n.train_paths);
+    ensure_nrc_buffers(e, wh * spp_wave);
+    if (n.frames >= n.opts.warmup_frames) {
+      mode = kNrcRender;
+      wave_bounces = std::min<uint32_t>(bounces, (uint32_t)n.opts.prefix_bounces + 1u);
+    }
+  }
   if (stage_ms) {
     // profiling: the same launches, issued directly with events between stages
     StageTimer tm;
     VT_CUDA(cudaEventRecord(e->ev0, e->stream));
-    for (uint32_t done = 0; done < spp; done += spp_wave) record_wave(e, spp_wave, bounces, e->stream, &tm);
+    if (e->nrc) nrc_train(e, bounces, &tm);
+    for (uint32_t done = 0; done < spp; done += spp_wave)
+      record_wave(e, spp_wave, wave_bounces, e->stream, &tm, mode);
     VT_CUDA(cudaEventRecord(e->ev1, e->stream));
     VT_CUDA(cudaEventSynchronize(e->ev1));
     VT_CUDA(cudaGetLastError());
     tm.collect(stage_ms);
     for (int k = 0; k < StageTimer::kStages; ++k) stage_launches[k] += tm.launches[k];
   } else {
-    cudaGraphExec_t g = wave_graph(e, spp_wave, bounces);
+    if (e->nrc) wave_graph(e, 1, bounces, kNrcTrain);  // capture outside the timed region
+    cudaGraphExec_t g = wave_graph(e, spp_wave, wave_bounces, mode);
     VT_CUDA(cudaEventRecord(e->ev0, e->stream));
+    if (e->nrc) nrc_train(e, bounces, nullptr);
     for (uint32_t done = 0; done < spp; done += spp_wave) VT_CUDA(cudaGraphLaunch(g, e->stream));
     VT_CUDA(cudaEventRecord(e->ev1, e->stream));
     VT_CUDA(cudaEventSynchronize(e->ev1));
+  }
+  if (e->nrc) {
+    e->nrc->frames += 1;
+    int d[2] = {0, 0};
+    VT_CUDA(cudaMemcpy(d, e->nrc->cache->d_diag(), sizeof d, cudaMemcpyDeviceToHost));
+    if (d[0]) {
+      VT_CUDA(cudaMemset(e->nrc->cache->d_diag(), 0, sizeof(int)));
+      fail(VT_ERR_TIMEOUT, "tensor-core wait expired in an NRC kernel");
+    }
   }
   float ms = 0.0f;
   VT_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
@@ -749,6 +881,8 @@ vt_status vt_profile_frame(vt_engine* e, const vt_frame_input* input, vt_frame_o
     times->accumulate_ms = ms[StageTimer::kAccumulate];
     times->trace_closest_launches = launches[StageTimer::kTraceClosest];
     times->trace_shadow_launches = launches[StageTimer::kTraceShadow];
+    times->nrc_train_ms = ms[StageTimer::kNrcTrain];
+    times->nrc_query_ms = ms[StageTimer::kNrcQuery];
     times->frame_ms = e->last_ms;
   });
 }
@@ -876,6 +1010,36 @@ vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits
     VT_CUDA(cudaMemcpyAsync(&st, e->q_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     VT_CUDA(cudaStreamSynchronize(e->stream));
     if (st) fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+  });
+}
+
+vt_status vt_set_nrc(vt_engine* e, const vt_nrc_render_options* o) {
+  return vt::guard([&] {
+    if (!e || !o) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    e->drop_graphs();
+    if (!o->enabled) {
+      e->nrc.reset();
+      return;
+    }
+    if (o->prefix_bounces < 1 || o->prefix_bounces >= e->opts.max_bounces)
+      fail(VT_ERR_RANGE, "prefix_bounces must be in [1, max_bounces - 1]");
+    if (o->train_steps < 0 || o->train_steps > 64) fail(VT_ERR_RANGE, "train_steps must be in [0, 64]");
+    if (o->train_batch < 128 || o->train_batch > (1 << 20) || o->train_batch % 128)
+      fail(VT_ERR_RANGE, "train_batch must be a multiple of 128 in [128, 2^20]");
+    if (o->train_paths < 0 || o->warmup_frames < 0) fail(VT_ERR_RANGE, "train_paths and warmup_frames must be >= 0");
+    auto n = std::make_unique<NrcEngine>();
+    n->opts = *o;
+    n->train_paths = o->train_paths > 0 ? (uint32_t)o->train_paths
+                                        : (uint32_t)std::max(1024, o->train_steps * o->train_batch / 2);
+    e->nrc = std::move(n);
+    try {
+      nrc_rebuild(e);
+    } catch (...) {
+      e->nrc.reset();
+      throw;
+    }
   });
 }
 

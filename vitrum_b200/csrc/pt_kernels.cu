@@ -170,10 +170,18 @@ __global__ void k_raygen(FrameView f, WaveBuffers w) {
   if (i == 0) w.counters[0] = f.paths;
   if (i >= f.paths) return;
   const uint32_t wh = f.width * f.height;
-  const uint32_t pix = i % wh, s = i / wh;
+  uint32_t pix = i % wh, s = i / wh;
+  uint32_t key;
+  if (f.train) {
+    // training paths: uniformly random pixels, a key stream of their own
+    uint32_t h = pcg_init(i, *w.nrc_seed, 0x7A3D9E1Bu ^ f.frame_seed);
+    pix = pcg_next(h) % wh;
+    key = pcg_next(h) | 1u;
+  } else {
+    key = f.frame_seed ^ (w.counters[kCntWaveSample] + s);
+  }
   const uint32_t x = pix % f.width, y = pix / f.width;
-  const uint32_t sample = w.counters[kCntWaveSample] + s;
-  uint32_t rng = pcg_init(x, y, f.frame_seed ^ sample);
+  uint32_t rng = pcg_init(x, y, key);
   const float jx = rand01(rng), jy = rand01(rng);
   const float u = ((float)x + jx) / (float)f.width, v = ((float)y + jy) / (float)f.height;
   const float nx = u * 2.0f - 1.0f, ny = 1.0f - v * 2.0f;
@@ -245,6 +253,19 @@ __global__ void k_scatter(WaveBuffers w, int cur) {
   }
 }
 
+// ---------------------------------------------------------------- cache features
+// (position, outgoing direction, normal facing it, roughness, diffuse albedo,
+// specular albedo) as the radiance cache's 16-float record.
+__device__ __forceinline__ void nrc_features(const Material& m, float3 P, float3 wo, float3 n, float4 (&q)[4]) {
+  const float3 zero = f3(0.0f, 0.0f, 0.0f);
+  const float3 dif = m.kind == kLambert ? m.base_color : zero;
+  const float3 spe = m.kind == kConductor ? m.base_color : (m.kind == kDielectric ? f3(1.0f, 1.0f, 1.0f) : zero);
+  q[0] = make_float4(P.x, P.y, P.z, wo.x);
+  q[1] = make_float4(wo.y, wo.z, n.x, n.y);
+  q[2] = make_float4(n.z, m.roughness, dif.x, dif.y);
+  q[3] = make_float4(dif.z, spe.x, spe.y, spe.z);
+}
+
 // ---------------------------------------------------------------- shade
 __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
   const int nxt = cur ^ 1;
@@ -255,8 +276,10 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
        base += gridDim.x * blockDim.x) {
     const uint32_t i = base + lane;
     const bool valid = i < n;
-    bool alive = false, shadow = false;
+    bool alive = false, shadow = false, query = false;
     float4 next_o, next_d, sh_o, sh_d, sh_c;
+    float4 qf[4];
+    float4 qt;
     uint4 next_state;
     float3 T = f3(0.0f, 0.0f, 0.0f);
     if (valid) {
@@ -309,7 +332,24 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
         float3 tb, bb;
         onb(n, tb, bb);
         const float3 wol = to_local(wo, tb, bb, n);
-        if (m.kind != kDielectric) {
+        query = bounce == f.nrc_prefix;
+        if (f.train || query) nrc_features(m, P, wo, n, qf);
+        if (f.train) {
+          // training record: features, radiance gathered so far (incl. this
+          // vertex's emission), throughput on arrival
+          float4* rec = w.nrc_records + 6 * ((size_t)path * f.record_bounces + bounce);
+          const float4 acc = w.radiance[path];
+          rec[0] = qf[0];
+          rec[1] = qf[1];
+          rec[2] = qf[2];
+          rec[3] = qf[3];
+          rec[4] = make_float4(acc.x + rad.x, acc.y + rad.y, acc.z + rad.z, 1.0f);
+          rec[5] = make_float4(T.x, T.y, T.z, 0.0f);
+        }
+        if (query) {
+          // the path ends in the cache: its scattered radiance is predicted here
+          qt = make_float4(__uint_as_float(path), T.x, T.y, T.z);
+        } else if (m.kind != kDielectric) {
           // ---- next-event estimation
           if (sc.n_light_entries > 0) {
             const LightSample ls = sample_light(sc, P, rng);
@@ -427,6 +467,20 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
         w.shadow_contrib[q] = sh_c;
       }
     }
+    const uint32_t qm = __ballot_sync(kFull, query);
+    if (qm) {
+      uint32_t b = 0;
+      if (lane == (uint32_t)(__ffs(qm) - 1)) b = atomicAdd(&w.counters[kCntQuery], (uint32_t)__popc(qm));
+      b = __shfl_sync(kFull, b, __ffs(qm) - 1);
+      if (query) {
+        float4* o = w.nrc_queries + 5 * (size_t)(b + __popc(qm & ((1u << lane) - 1u)));
+        o[0] = qf[0];
+        o[1] = qf[1];
+        o[2] = qf[2];
+        o[3] = qf[3];
+        o[4] = qt;
+      }
+    }
   }
 }
 
@@ -473,6 +527,62 @@ __global__ void k_count_rays(WaveBuffers w, int cur, unsigned long long* totals)
   totals[1] += w.counters[kCntShadow];
 }
 
+__global__ void k_nrc_targets(WaveBuffers w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t total = paths * bounces;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *w.nrc_seed += 1u;  // next training wave draws new paths
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < total;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t sl = base + lane;
+    bool keep = false;
+    float4 tg = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (sl < total) {
+      const float4* rec = w.nrc_records + 6 * (size_t)sl;
+      const float4 A = rec[4];
+      if (A.w != 0.0f) {
+        const float4 T = rec[5];
+        const float4 L = w.radiance[sl / bounces];
+        auto tgt = [](float l, float a, float t) {
+          const float v = t > 0.0f ? (l - a) / t : 0.0f;
+          return fminf(1024.0f, fmaxf(0.0f, v));
+        };
+        tg = make_float4(tgt(L.x, A.x, T.x), tgt(L.y, A.y, T.y), tgt(L.z, A.z, T.z), 0.0f);
+        keep = isfinite(tg.x) && isfinite(tg.y) && isfinite(tg.z);
+      }
+    }
+    const uint32_t km = __ballot_sync(kFull, keep);
+    if (!km) continue;
+    uint32_t b = 0;
+    if (lane == (uint32_t)(__ffs(km) - 1)) b = atomicAdd(&w.counters[kCntSamples], (uint32_t)__popc(km));
+    b = __shfl_sync(kFull, b, __ffs(km) - 1);
+    if (keep) {
+      const uint32_t q = b + __popc(km & ((1u << lane) - 1u));
+      if (q < capacity) {
+        const float4* rec = w.nrc_records + 6 * (size_t)sl;
+        float4* o = samples + 5 * (size_t)q;
+        o[0] = rec[0];
+        o[1] = rec[1];
+        o[2] = rec[2];
+        o[3] = rec[3];
+        o[4] = tg;
+      }
+    }
+  }
+}
+
+__global__ void k_nrc_fill(WaveBuffers w, float4* samples, uint32_t capacity) {
+  const uint32_t got = min(w.counters[kCntSamples], capacity);
+  for (uint32_t i = got + blockIdx.x * blockDim.x + threadIdx.x; i < capacity; i += gridDim.x * blockDim.x) {
+    float4* o = samples + 5 * (size_t)i;
+    if (got == 0) {
+      for (int k = 0; k < 5; ++k) o[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else {
+      const float4* src = samples + 5 * (size_t)(i % got);
+      for (int k = 0; k < 5; ++k) o[k] = src[k];
+    }
+  }
+}
+
 unsigned grid_for(uint32_t n, unsigned block) {
   unsigned g = (unsigned)((n + block - 1) / block);
   return g ? g : 1;
@@ -507,6 +617,15 @@ void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w,
 void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t s) {
   const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
   k_shadow_resolve<<<g, 256, 0, s>>>(w);
+}
+
+void launch_nrc_targets(const WaveBuffers& w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity,
+                        cudaStream_t s) {
+  const uint32_t total = paths * bounces;
+  const unsigned g = grid_for(total, 256) < 148 * 8 ? grid_for(total, 256) : 148 * 8;
+  k_nrc_targets<<<g, 256, 0, s>>>(w, paths, bounces, samples, capacity);
+  const unsigned gf = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
+  k_nrc_fill<<<gf, 256, 0, s>>>(w, samples, capacity);
 }
 
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s) {

@@ -49,6 +49,10 @@ struct FrameView {
   uint32_t max_bounces = 5;
   uint32_t paths = 0;       // width * height * spp_wave
   uint32_t sort_by_material = 1;
+  // neural radiance cache
+  uint32_t train = 0;                  // training wave: random pixels, one record per vertex, no accumulation
+  uint32_t record_bounces = 0;         // record slots per training path
+  uint32_t nrc_prefix = 0xFFFFFFFFu;   // render waves: hits of this bounce become cache queries
 };
 
 // Path queues (double-buffered), hit records, shadow queue and per-path radiance.
@@ -66,9 +70,16 @@ struct WaveBuffers {
   uint32_t* counters = nullptr;            // [queue0, queue1, shadow, hist[8], cursor[8], wave_sample]
   unsigned long long* trace_counter = nullptr;
   int* trace_status = nullptr;
+  // neural radiance cache
+  float4* nrc_records = nullptr;   // training: 6 float4 per (path, bounce) = features, (A rgb, valid), (T rgb, 0)
+  float4* nrc_queries = nullptr;   // render: 5 float4 per query = features, (path bits, T rgb)
+  uint32_t* nrc_seed = nullptr;    // training-wave counter (pixel choice and RNG key)
 };
 
-enum : int { kCntShadow = 2, kCntHist = 3, kCntCursor = 11, kCntWaveSample = 19, kCntWords = 20 };
+enum : int {
+  kCntShadow = 2, kCntHist = 3, kCntCursor = 11, kCntWaveSample = 19, kCntQuery = 20, kCntSamples = 21,
+  kCntWords = 22
+};
 
 // Accumulation targets.
 struct AccumView {
@@ -86,6 +97,14 @@ void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s);
 // totals[0] += queue count traced this bounce, totals[1] += shadow rays traced
 void launch_count_rays(const WaveBuffers& w, int cur, unsigned long long* totals, cudaStream_t s);
+
+// Training samples from a finished training wave: target = (L_final - A) / T
+// per recorded vertex (the radiance the path gathered after the vertex, per
+// unit throughput), clamped to [0, 1024] (recordUnpack.ts NRC_MAX_TRAINING_TARGET);
+// appended to `samples` (5 float4 each) up to `capacity`, then the remaining
+// slots are filled cyclically from the collected ones.
+void launch_nrc_targets(const WaveBuffers& w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity,
+                        cudaStream_t s);
 
 }  // namespace pt
 }  // namespace vt

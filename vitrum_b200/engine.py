@@ -69,7 +69,15 @@ class _StageTimes(ctypes.Structure):
     _fields_ = [("raygen_ms", ctypes.c_double), ("trace_closest_ms", ctypes.c_double), ("sort_ms", ctypes.c_double),
                 ("shade_ms", ctypes.c_double), ("trace_shadow_ms", ctypes.c_double), ("resolve_ms", ctypes.c_double),
                 ("accumulate_ms", ctypes.c_double), ("frame_ms", ctypes.c_double),
-                ("trace_closest_launches", ctypes.c_int32), ("trace_shadow_launches", ctypes.c_int32)]
+                ("trace_closest_launches", ctypes.c_int32), ("trace_shadow_launches", ctypes.c_int32),
+                ("nrc_train_ms", ctypes.c_double), ("nrc_query_ms", ctypes.c_double)]
+
+
+class _NrcRenderOptions(ctypes.Structure):
+    from .nrc import _Config as _NrcConfig
+    _fields_ = [("enabled", ctypes.c_int32), ("prefix_bounces", ctypes.c_int32), ("train_steps", ctypes.c_int32),
+                ("train_batch", ctypes.c_int32), ("train_paths", ctypes.c_int32), ("warmup_frames", ctypes.c_int32),
+                ("cache", _NrcConfig)]
 
 
 class _EngineStats(ctypes.Structure):
@@ -302,6 +310,17 @@ class Engine:
         N.call("vt_trace_rays", self.handle, ctypes.c_void_p(r.ctypes.data), r.shape[0],
                ctypes.c_void_p(hits.ctypes.data), ctypes.c_void_p(inst.ctypes.data))
         return hits, inst
+
+    def set_nrc(self, enabled: bool = True, prefix_bounces: int = 1, train_steps: int = 4, train_batch: int = 65536,
+                train_paths: int = 0, warmup_frames: int = 0, cache=None) -> None:
+        """Path tracing with the neural radiance cache (vt_set_nrc): each frame
+        trains the cache on its own training paths, then ends the render paths
+        in a cache query after `prefix_bounces` bounces."""
+        from .nrc import NrcConfig
+        cfg = (cache or NrcConfig()).to_c()
+        o = _NrcRenderOptions(1 if enabled else 0, prefix_bounces, train_steps, train_batch, train_paths,
+                              warmup_frames, cfg)
+        N.call("vt_set_nrc", self.handle, ctypes.byref(o))
 
     def stats(self) -> dict:
         s = _EngineStats()
