@@ -362,6 +362,11 @@ vt_status vt_nrc_gradients(vt_nrc* nrc, const float* samples, size_t n, float* g
 vt_status vt_nrc_get_params(vt_nrc* nrc, float* weights, float* table);
 /* Replaces the parameters and clears the optimiser state. */
 vt_status vt_nrc_set_params(vt_nrc* nrc, const float* weights, const float* table);
+/* Device-pointer forms, enqueued on `cuda_stream` (NULL: the legacy default
+ * stream); records / samples / rgb are device arrays with the layouts above.
+ * No reference counterpart (the WebGPU subsystem binds its own buffers). */
+vt_status vt_nrc_query_device(vt_nrc* nrc, const float* d_records, size_t n, float* d_rgb, void* cuda_stream);
+vt_status vt_nrc_train_device(vt_nrc* nrc, const float* d_samples, size_t n, void* cuda_stream);
 
 /* Path tracing with the cache (NrcSubsystem driven by the engine; Mueller et
  * al. 2021 as the reference runs it): every frame a training wave of plain

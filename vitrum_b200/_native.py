@@ -78,6 +78,8 @@ SIGNATURES = {
     "vt_nrc_gradients": [P, P, SZ, P, P, P],
     "vt_nrc_get_params": [P, P, P],
     "vt_nrc_set_params": [P, P, P],
+    "vt_nrc_query_device": [P, P, SZ, P, P],
+    "vt_nrc_train_device": [P, P, SZ, P],
     "vt_reset": [P],
     "vt_engine_get_stats": [P, P],
     "vt_destroy": [P],

@@ -309,6 +309,31 @@ vt_status vt_nrc_gradients(vt_nrc* h, const float* samples, size_t n, float* gra
   });
 }
 
+vt_status vt_nrc_query_device(vt_nrc* h, const float* d_records, size_t n, float* d_rgb, void* cuda_stream) {
+  return vt::guard([&] {
+    if (!h) vt::fail(VT_ERR_INVALID_ARGUMENT, "nrc is null");
+    if (n && (!d_records || !d_rgb)) vt::fail(VT_ERR_INVALID_ARGUMENT, "records and rgb must be non-null");
+    if (n > 0x7FFFFFFFull) vt::fail(VT_ERR_RANGE, "at most 2^31 - 1 queries per call");
+    if (reinterpret_cast<uintptr_t>(d_records) % 16) vt::fail(VT_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
+    vt::DeviceScope ds(h->device);
+    h->cache->query(reinterpret_cast<const float4*>(d_records), 4, nullptr, (uint32_t)n, d_rgb, nullptr,
+                    static_cast<cudaStream_t>(cuda_stream));
+    VT_CUDA(cudaGetLastError());
+  });
+}
+
+vt_status vt_nrc_train_device(vt_nrc* h, const float* d_samples, size_t n, void* cuda_stream) {
+  return vt::guard([&] {
+    if (!h) vt::fail(VT_ERR_INVALID_ARGUMENT, "nrc is null");
+    if (!d_samples || !n) vt::fail(VT_ERR_INVALID_ARGUMENT, "samples must be non-empty");
+    if (n > 0x7FFFFFFFull) vt::fail(VT_ERR_RANGE, "at most 2^31 - 1 samples per step");
+    if (reinterpret_cast<uintptr_t>(d_samples) % 16) vt::fail(VT_ERR_INVALID_ARGUMENT, "samples must be 16-byte aligned");
+    vt::DeviceScope ds(h->device);
+    h->cache->train_step(reinterpret_cast<const float4*>(d_samples), (uint32_t)n, static_cast<cudaStream_t>(cuda_stream));
+    VT_CUDA(cudaGetLastError());
+  });
+}
+
 vt_status vt_nrc_get_params(vt_nrc* h, float* weights, float* table) {
   return vt::guard([&] {
     if (!h) vt::fail(VT_ERR_INVALID_ARGUMENT, "nrc is null");

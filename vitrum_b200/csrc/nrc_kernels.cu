@@ -1,7 +1,7 @@
 // nrc_kernels.cu -- neural radiance cache kernels for sm_100a.
 //
-// k_nrc_infer   persistent; per tile of 128 queries: encode (hash grid + SH4 +
-//               surface features) into a swizzled fp16 tile, then six
+// k_nrc_infer   persistent, three CTAs per SM; per tile of 128 queries: encode
+//               (hash grid + SH4 + surface features) into a swizzled fp16 tile, then six
 //               tcgen05.mma layers (M=128, N=64, K=64 as four K=16 steps) with
 //               the fp32 accumulator in TMEM, ReLU + fp16 repack in the epilogue
 //               between layers, prediction read from TMEM.
@@ -98,7 +98,8 @@ __device__ __forceinline__ void sh4(float x, float y, float z, float (&s)[16]) {
 __device__ __forceinline__ void encode(const View& v, float4 a, float4 b, float4 c, float4 d, uint32_t (&p)[32],
                                        float3& n01) {
   n01 = normalise(v, a.x, a.y, a.z);
-#pragma unroll 1
+  // all levels unrolled: the 8 x levels table gathers are independent and in flight together
+#pragma unroll
   for (int l = 0; l < kMaxLevels; ++l) {
     float f0 = 0.0f, f1 = 0.0f;
     if (l < v.levels) {
@@ -138,10 +139,10 @@ __device__ __forceinline__ void encode(const View& v, float4 a, float4 b, float4
 // Scatter of the hash-feature input gradient g[0..31] (already scaled) into
 // the f32 table gradient with the trilinear weights.
 __device__ __forceinline__ void scatter_table(const View& v, float3 n01, const float (&g)[kEncWidth]) {
-#pragma unroll 1
-  for (int l = 0; l < v.levels; ++l) {
+#pragma unroll
+  for (int l = 0; l < kMaxLevels; ++l) {
     const float g0 = g[2 * l], g1 = g[2 * l + 1];
-    if (g0 == 0.0f && g1 == 0.0f) continue;
+    if (l >= v.levels || (g0 == 0.0f && g1 == 0.0f)) continue;
     const float N = v.res[l];
     const float px = n01.x * N, py = n01.y * N, pz = n01.z * N;
     const float x0 = floorf(px), y0 = floorf(py), z0 = floorf(pz);
@@ -224,8 +225,9 @@ __global__ void __launch_bounds__(128, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
   uint8_t* wt = base;
-  uint8_t* act = base + kLayers * kWBytes;  // two ping-pong tiles
-  uint64_t* bar = reinterpret_cast<uint64_t*>(act + 2 * kTileBytes);
+  uint8_t* act = base + kLayers * kWBytes;  // one tile: each layer's MMA has finished reading it before the
+                                            // epilogue writes the next layer's input over it
+  uint64_t* bar = reinterpret_cast<uint64_t*>(act + kTileBytes);
   uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
   const uint32_t n = n_dev ? *n_dev : n_host;
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(128, 1)
   tc::fence_after_sync();
   const uint32_t tmem = *slot;
   const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
-  const uint32_t w_s = tc::smem_u32(wt), a_s[2] = {tc::smem_u32(act), tc::smem_u32(act + kTileBytes)};
+  const uint32_t w_s = tc::smem_u32(wt), a_s = tc::smem_u32(act);
   uint32_t phase = 0;
   bool failed = false;
   for (uint32_t tile = blockIdx.x; tile * kTile < n && !failed; tile += gridDim.x) {
@@ -259,10 +261,9 @@ __global__ void __launch_bounds__(128, 1)
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    int cur = 0;
     for (int l = 0; l < kLayers; ++l) {
       if (tid == 0) {
-        issue_fwd(tmem, a_s[cur], w_s + l * kWBytes);
+        issue_fwd(tmem, a_s, w_s + l * kWBytes);
         tc::mma_commit(bar);
       }
       if (!wait_all(bar, phase)) { failed = true; break; }
@@ -273,11 +274,10 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
         for (int k = 0; k < 32; ++k)
           p[k] = pack_h2(fmaxf(__uint_as_float(acc[2 * k]), 0.0f), fmaxf(__uint_as_float(acc[2 * k + 1]), 0.0f));
-        store_row(act + (cur ^ 1) * kTileBytes, tid, p);
+        store_row(act, tid, p);
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
-        cur ^= 1;
       } else {
         uint32_t o[16];
         tc::tmem_ld16(lane_addr, o);
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(128, 1)
       uint32_t acc[64];
       load_acc64(lane_addr + 64u + 64u * (uint32_t)l, acc);
       float* gw = v.grad_w + (size_t)l * kWidth * kWidth + (size_t)tid * kWidth;
-#pragma unroll 8
+#pragma unroll
       for (int k = 0; k < 64; ++k) atomicAdd(gw + k, __uint_as_float(acc[k]) * inv_n);
     }
   }
@@ -542,7 +542,7 @@ __global__ void k_nrc_adam_table(float2* __restrict__ master, float2* __restrict
   }
 }
 
-constexpr size_t kInferSmem = kLayers * kWBytes + 2 * kTileBytes + 64 + 1024;
+constexpr size_t kInferSmem = kLayers * kWBytes + kTileBytes + 64 + 1024;
 constexpr size_t kTrainSmem = kLayers * kWBytes + (1 + kLayers) * kTileBytes + 64 + 1024;
 
 int sm_count() {
@@ -566,9 +566,9 @@ void launch_infer(const View& v, const float4* records, uint32_t rec_stride_f4, 
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem);
     attr = true;
   }
-  // two CTAs per SM (80 KB shared memory and 64 TMEM columns each)
+  // three CTAs per SM (65 KB shared memory and 64 TMEM columns each)
   const uint32_t tiles = (n + kTile - 1) / kTile;
-  const uint32_t grid = tiles < (uint32_t)(2 * sm_count()) ? tiles : (uint32_t)(2 * sm_count());
+  const uint32_t grid = tiles < (uint32_t)(3 * sm_count()) ? tiles : (uint32_t)(3 * sm_count());
   k_nrc_infer<<<grid, 128, kInferSmem, s>>>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance);
 }
 

@@ -88,6 +88,15 @@ class RadianceCache:
         N.call("vt_nrc_query", self.handle, _p(r), r.shape[0], _p(out))
         return out
 
+    def query_device(self, records_ptr: int, n: int, rgb_ptr: int, stream: int = 0) -> None:
+        """Enqueue a query on device arrays (16 floats per record in, 3 floats out)."""
+        N.call("vt_nrc_query_device", self.handle, ctypes.c_void_p(records_ptr), n, ctypes.c_void_p(rgb_ptr),
+               ctypes.c_void_p(stream))
+
+    def train_step_device(self, samples_ptr: int, n: int, stream: int = 0) -> None:
+        """Enqueue one optimiser step on a device array of n samples (20 floats each)."""
+        N.call("vt_nrc_train_device", self.handle, ctypes.c_void_p(samples_ptr), n, ctypes.c_void_p(stream))
+
     def train_step(self, samples: np.ndarray) -> float:
         s = np.ascontiguousarray(samples, np.float32).reshape(-1, SAMPLE_FLOATS)
         loss = ctypes.c_float()
