@@ -387,6 +387,52 @@ typedef struct vt_nrc_render_options {
 
 vt_status vt_set_nrc(vt_engine* engine, const vt_nrc_render_options* options);
 
+/* ------------------------------------------------------------------ */
+/* Batch: many scenes in one launch sequence                            */
+/* ------------------------------------------------------------------ */
+/* No reference counterpart (the WebGPU engine renders one scene per engine):
+ * scenes of uneven size and resolution share every wave, so small frames do
+ * not leave the GPU idle.  Paths of all scenes form one index space consumed
+ * wave by wave through a device cursor; traversal takes a per-ray root; the
+ * whole frame (all waves) is one CUDA graph.  Scenes must be single-level. */
+
+typedef struct vt_batch vt_batch;
+
+typedef struct vt_batch_stats {
+  double frame_ms;            /* device time of the batch frame (all scenes) */
+  uint64_t closest_rays;      /* extension rays traced by the frame */
+  uint64_t shadow_rays;
+  int32_t waves;
+  int32_t kernel_launches;    /* kernels in the frame's graph */
+} vt_batch_stats;
+
+/* Launch-shape knobs, chosen by vt_batch_autotune or set directly. */
+typedef struct vt_tuning {
+  int32_t wave_paths;         /* paths per wave */
+  int32_t sort_by_material;   /* 1 sort shading work by BSDF family, 0 not */
+  int32_t trace_blocks_per_sm;/* persistent traversal CTAs per SM (0: occupancy limit) */
+} vt_tuning;
+
+vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_batch** out);
+/* One frame per scene: frames[i].samples samples at frames[i].width x height with
+ * frames[i].bounces (0: options.max_bounces) through the camera of frames[i]. */
+vt_status vt_batch_set_scenes(vt_batch* batch, const vt_scene_desc* scenes, const vt_frame_input* frames,
+                              size_t count);
+/* Renders every scene's frame from a cleared accumulation. */
+vt_status vt_batch_render(vt_batch* batch, vt_batch_stats* stats);
+vt_status vt_batch_capture(vt_batch* batch, size_t index, float* rgba, size_t float_capacity);
+vt_status vt_batch_set_tuning(vt_batch* batch, const vt_tuning* tuning);
+vt_status vt_batch_get_tuning(const vt_batch* batch, vt_tuning* tuning);
+/* The project's autotuner: times candidate launch shapes on this batch (each
+ * candidate renders the batch once) and keeps the fastest; `report` receives
+ * up to `report_capacity` (tuning, frame_ms) pairs tried. */
+typedef struct vt_tuning_trial {
+  vt_tuning tuning;
+  double frame_ms;
+} vt_tuning_trial;
+vt_status vt_batch_autotune(vt_batch* batch, vt_tuning_trial* report, size_t report_capacity, size_t* report_count);
+vt_status vt_batch_destroy(vt_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,14 @@ SIGNATURES = {
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
     "vt_trace_rays": [P, P, SZ, P, P],
     "vt_set_nrc": [P, P],
+    "vt_batch_create": [I32, P, P],
+    "vt_batch_set_scenes": [P, P, P, SZ],
+    "vt_batch_render": [P, P],
+    "vt_batch_capture": [P, SZ, P, SZ],
+    "vt_batch_set_tuning": [P, P],
+    "vt_batch_get_tuning": [P, P],
+    "vt_batch_autotune": [P, P, SZ, P],
+    "vt_batch_destroy": [P],
     "vt_nrc_create": [I32, P, P],
     "vt_nrc_destroy": [P],
     "vt_nrc_query": [P, P, SZ, P],

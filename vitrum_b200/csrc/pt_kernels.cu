@@ -212,14 +212,18 @@ __device__ __forceinline__ uint32_t hit_key(const SceneView& sc, int4 h) {
   return 1u + sc.materials[hit_material(sc, h)].kind;
 }
 
-__global__ void k_classify(SceneView sc, WaveBuffers w, int cur) {
+__global__ void k_classify(SceneView sc0, FrameView f, WaveBuffers w, int cur) {
   const uint32_t n = w.counters[cur];
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
        base += gridDim.x * blockDim.x) {
     const uint32_t i = base + lane;
     const bool valid = i < n;
-    const uint32_t key = valid ? hit_key(sc, w.hits[i]) : 0xFFu;
+    uint32_t key = 0xFFu;
+    if (valid) {
+      const SceneView& sc = f.batch ? f.batch[(w.state[cur][i].z >> 8) & 0xFFu].view : sc0;
+      key = hit_key(sc, w.hits[i]);
+    }
     if (valid) w.keys[i] = key;
 #pragma unroll
     for (uint32_t k = 0; k < 4; ++k) {
@@ -267,11 +271,10 @@ __device__ __forceinline__ void nrc_features(const Material& m, float3 P, float3
 }
 
 // ---------------------------------------------------------------- shade
-__global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
+__global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
   const int nxt = cur ^ 1;
   const uint32_t n = w.counters[cur];
   const uint32_t lane = threadIdx.x & 31u;
-  const bool last = bounce + 1 >= f.max_bounces;
   for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
        base += gridDim.x * blockDim.x) {
     const uint32_t i = base + lane;
@@ -282,10 +285,15 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
     float4 qt;
     uint4 next_state;
     float3 T = f3(0.0f, 0.0f, 0.0f);
+    uint32_t root_of_path = 0;
     if (valid) {
       const uint32_t p = f.sort_by_material ? w.order[i] : i;
       const float4 r0 = w.rays[cur][2 * p], r1 = w.rays[cur][2 * p + 1];
       const uint4 st = w.state[cur][p];
+      const uint32_t sid = (st.z >> 8) & 0xFFu;
+      const SceneView& sc = f.batch ? f.batch[sid].view : sc0;
+      const bool last = bounce + 1 >= (f.batch ? f.batch[sid].max_bounces : f.max_bounces);
+      root_of_path = sc.root;
       const float4 tp = w.through[cur][p];
       const int4 h = w.hits[p];
       T = f3(tp.x, tp.y, tp.z);
@@ -436,6 +444,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
         }
       }
       next_state.y = rng;
+      next_state.z |= sid << 8;
       if (maxc(rad) > 0.0f) {
         float4 acc = w.radiance[path];
         w.radiance[path] = make_float4(acc.x + rad.x, acc.y + rad.y, acc.z + rad.z, 0.0f);
@@ -453,6 +462,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
         w.rays[nxt][2 * q + 1] = next_d;
         w.state[nxt][q] = next_state;
         w.through[nxt][q] = make_float4(T.x, T.y, T.z, 0.0f);
+        if (w.ray_root[nxt]) w.ray_root[nxt][q] = root_of_path;
       }
     }
     const uint32_t sm = __ballot_sync(kFull, shadow);
@@ -465,6 +475,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc, FrameView f, WaveBu
         w.shadow_rays[2 * q] = sh_o;
         w.shadow_rays[2 * q + 1] = sh_d;
         w.shadow_contrib[q] = sh_c;
+        if (w.shadow_root) w.shadow_root[q] = root_of_path;
       }
     }
     const uint32_t qm = __ballot_sync(kFull, query);
@@ -583,6 +594,67 @@ __global__ void k_nrc_fill(WaveBuffers w, float4* samples, uint32_t capacity) {
   }
 }
 
+// ---------------------------------------------------------------- batch
+// Paths of the whole batch form one index space: scene s owns
+// [path_begin_s, path_begin_s + W_s H_s spp_s), pixel-major within a sample.
+// Each wave takes the next `capacity` paths at the device cursor.
+__global__ void k_raygen_batch(FrameView f, WaveBuffers w, uint32_t capacity) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long base = *w.batch_cursor;
+  const unsigned long long left = base < f.batch_paths ? f.batch_paths - base : 0ull;
+  const uint32_t cnt = left < capacity ? (uint32_t)left : capacity;
+  if (i == 0) {
+    w.counters[0] = cnt;
+    w.counters[kCntBatchPaths] = cnt;
+  }
+  if (i >= cnt) return;
+  const unsigned long long g = base + i;
+  uint32_t lo = 0, hi = f.n_scenes - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (f.batch[mid].path_begin <= g) lo = mid; else hi = mid - 1;
+  }
+  const BatchScene& B = f.batch[lo];
+  const unsigned long long local = g - B.path_begin;
+  const uint32_t wh = B.width * B.height;
+  const uint32_t pix = (uint32_t)(local % wh), sample = (uint32_t)(local / wh);
+  const uint32_t x = pix % B.width, y = pix / B.width;
+  uint32_t rng = pcg_init(x, y, B.frame_seed ^ sample);
+  const float jx = rand01(rng), jy = rand01(rng);
+  const float u = ((float)x + jx) / (float)B.width, v = ((float)y + jy) / (float)B.height;
+  const float nx = u * 2.0f - 1.0f, ny = 1.0f - v * 2.0f;
+  const float* M = B.inv_vp;
+  float nf[4], fr[4];
+  for (int r = 0; r < 4; ++r) {
+    nf[r] = M[4 * r] * nx + M[4 * r + 1] * ny - M[4 * r + 2] + M[4 * r + 3];
+    fr[r] = M[4 * r] * nx + M[4 * r + 1] * ny + M[4 * r + 2] + M[4 * r + 3];
+  }
+  const float3 o = f3(nf[0] / nf[3], nf[1] / nf[3], nf[2] / nf[3]);
+  const float3 far = f3(fr[0] / fr[3], fr[1] / fr[3], fr[2] / fr[3]);
+  const float3 d = normalize(far - o);
+  w.rays[0][2 * i] = make_float4(o.x, o.y, o.z, 0.0f);
+  w.rays[0][2 * i + 1] = make_float4(d.x, d.y, d.z, CUDART_INF_F);
+  w.state[0][i] = make_uint4(i, rng, 1u | (lo << 8), 0u);
+  w.through[0][i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  w.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  w.ray_root[0][i] = B.view.root;
+  w.path_pixel[i] = B.accum_offset + pix;
+}
+
+__global__ void k_accumulate_batch(WaveBuffers w, float4* accum) {
+  const uint32_t cnt = w.counters[kCntBatchPaths];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const float4 r = w.radiance[i];
+    float* a = reinterpret_cast<float*>(accum + w.path_pixel[i]);
+    atomicAdd(a, r.x);
+    atomicAdd(a + 1, r.y);
+    atomicAdd(a + 2, r.z);
+    atomicAdd(a + 3, 1.0f);
+  }
+}
+
+__global__ void k_advance_batch(WaveBuffers w) { *w.batch_cursor += w.counters[kCntBatchPaths]; }
+
 unsigned grid_for(uint32_t n, unsigned block) {
   unsigned g = (unsigned)((n + block - 1) / block);
   return g ? g : 1;
@@ -598,11 +670,11 @@ void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s) {
   k_raygen<<<grid_for(f.paths, 256), 256, 0, s>>>(f, w);
 }
 
-void launch_sort_by_material(const SceneView& sc, const WaveBuffers& w, int cur, uint32_t capacity,
-                             cudaStream_t s) {
+void launch_sort_by_material(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur,
+                             uint32_t capacity, cudaStream_t s) {
   cudaMemsetAsync(w.counters + kCntHist, 0, sizeof(uint32_t) * 16, s);
   const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
-  k_classify<<<g, 256, 0, s>>>(sc, w, cur);
+  k_classify<<<g, 256, 0, s>>>(sc, f, w, cur);
   k_scatter<<<g, 256, 0, s>>>(w, cur);
 }
 
@@ -626,6 +698,16 @@ void launch_nrc_targets(const WaveBuffers& w, uint32_t paths, uint32_t bounces, 
   k_nrc_targets<<<g, 256, 0, s>>>(w, paths, bounces, samples, capacity);
   const unsigned gf = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
   k_nrc_fill<<<gf, 256, 0, s>>>(w, samples, capacity);
+}
+
+void launch_raygen_batch(const FrameView& f, const WaveBuffers& w, uint32_t capacity, cudaStream_t s) {
+  k_raygen_batch<<<grid_for(capacity, 256), 256, 0, s>>>(f, w, capacity);
+}
+
+void launch_accumulate_batch(const WaveBuffers& w, float4* accum, uint32_t capacity, cudaStream_t s) {
+  const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
+  k_accumulate_batch<<<g, 256, 0, s>>>(w, accum);
+  k_advance_batch<<<1, 1, 0, s>>>(w);
 }
 
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s) {

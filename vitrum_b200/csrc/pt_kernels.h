@@ -41,6 +41,17 @@ struct SceneView {
   float bias = 2e-5f;            // origin offset along the geometric normal, relative to max(1, |P|_inf)
 };
 
+// One scene of a batch (the batched persistent launch): its scene view,
+// camera and sampling, and where its paths and pixels sit in the batch.
+struct BatchScene {
+  SceneView view;
+  float inv_vp[16];
+  uint32_t width = 0, height = 0, spp = 0, max_bounces = 0;
+  uint32_t frame_seed = 0;
+  uint32_t accum_offset = 0;            // first pixel of this scene in the batch accumulation
+  unsigned long long path_begin = 0;    // first path of this scene in the batch's path space
+};
+
 struct FrameView {
   float inv_vp[16];         // row-major inverse view-projection
   uint32_t width = 0, height = 0;
@@ -53,6 +64,10 @@ struct FrameView {
   uint32_t train = 0;                  // training wave: random pixels, one record per vertex, no accumulation
   uint32_t record_bounces = 0;         // record slots per training path
   uint32_t nrc_prefix = 0xFFFFFFFFu;   // render waves: hits of this bounce become cache queries
+  // batch: paths of many scenes in one wave (scene id in bits 8-15 of the path flags)
+  const BatchScene* batch = nullptr;
+  uint32_t n_scenes = 0;
+  unsigned long long batch_paths = 0;  // total paths of the batch
 };
 
 // Path queues (double-buffered), hit records, shadow queue and per-path radiance.
@@ -74,11 +89,16 @@ struct WaveBuffers {
   float4* nrc_records = nullptr;   // training: 6 float4 per (path, bounce) = features, (A rgb, valid), (T rgb, 0)
   float4* nrc_queries = nullptr;   // render: 5 float4 per query = features, (path bits, T rgb)
   uint32_t* nrc_seed = nullptr;    // training-wave counter (pixel choice and RNG key)
+  // batch
+  uint32_t* ray_root[2] = {nullptr, nullptr};  // traversal root node per queued ray
+  uint32_t* shadow_root = nullptr;
+  uint32_t* path_pixel = nullptr;              // batch accumulation pixel per path
+  unsigned long long* batch_cursor = nullptr;  // first path of the next wave
 };
 
 enum : int {
   kCntShadow = 2, kCntHist = 3, kCntCursor = 11, kCntWaveSample = 19, kCntQuery = 20, kCntSamples = 21,
-  kCntWords = 22
+  kCntBatchPaths = 22, kCntWords = 23
 };
 
 // Accumulation targets.
@@ -89,12 +109,16 @@ struct AccumView {
 };
 
 void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s);
-void launch_sort_by_material(const SceneView& sc, const WaveBuffers& w, int cur, uint32_t capacity,
-                             cudaStream_t s);
+void launch_sort_by_material(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur,
+                             uint32_t capacity, cudaStream_t s);
 void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur, uint32_t bounce,
                   uint32_t capacity, cudaStream_t s);
 void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t s);
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s);
+// Batch: the next `capacity` paths of the batch's path space (device cursor),
+// and their accumulation (atomic per pixel) followed by the cursor advance.
+void launch_raygen_batch(const FrameView& f, const WaveBuffers& w, uint32_t capacity, cudaStream_t s);
+void launch_accumulate_batch(const WaveBuffers& w, float4* accum, uint32_t capacity, cudaStream_t s);
 // totals[0] += queue count traced this bounce, totals[1] += shadow rays traced
 void launch_count_rays(const WaveBuffers& w, int cur, unsigned long long* totals, cudaStream_t s);
 

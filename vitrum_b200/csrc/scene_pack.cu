@@ -1,0 +1,314 @@
+// scene_pack.cu -- host-side packing of a vt_scene_desc into the device
+// layouts (scenePack.ts packSceneFromCore:1104-1310 restated for the wide
+// BVH): per-triangle records and 8-wide nodes (one tree, or per-mesh bottom
+// levels under a top level over the instances), materials, the area-light
+// CDF, point lights and the environment with its importance CDFs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "scene_pack.h"
+
+namespace vt {
+
+namespace {
+double luminance(const float* c) { return 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]; }
+}  // namespace
+
+bool invert4(const double* m, double* inv) {  // any layout, Gauss-Jordan with partial pivoting
+  double a[4][8];
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      a[r][c] = m[r * 4 + c];
+      a[r][c + 4] = r == c ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < 4; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 4; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+    if (!(std::fabs(a[piv][c]) > 1e-300)) return false;
+    if (piv != c)
+      for (int k = 0; k < 8; ++k) std::swap(a[c][k], a[piv][k]);
+    const double d = a[c][c];
+    for (int k = 0; k < 8; ++k) a[c][k] /= d;
+    for (int r = 0; r < 4; ++r) {
+      if (r == c) continue;
+      const double f = a[r][c];
+      for (int k = 0; k < 8; ++k) a[r][k] -= f * a[c][k];
+    }
+  }
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) inv[r * 4 + c] = a[r][c + 4];
+  return true;
+}
+
+namespace {
+void mat_mul_cm(const double* a, const double* b, double* out) {  // column-major 4x4: out = a * b
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += a[k * 4 + r] * b[c * 4 + k];
+      out[c * 4 + r] = s;
+    }
+}
+
+
+}  // namespace
+
+// inverse(P * V) as a row-major float matrix
+void inverse_view_proj(const float* view, const float* proj, float* out_rm) {
+  double v[16], p[16], vp[16], rm[16], inv[16];
+  for (int i = 0; i < 16; ++i) { v[i] = view[i]; p[i] = proj[i]; }
+  mat_mul_cm(p, v, vp);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) rm[r * 4 + c] = vp[c * 4 + r];
+  if (!invert4(rm, inv)) fail(VT_ERR_INVALID_ARGUMENT, "camera view-projection matrix is singular");
+  for (int i = 0; i < 16; ++i) out_rm[i] = (float)inv[i];
+}
+
+
+
+PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base) {
+  if (!sc) fail(VT_ERR_INVALID_ARGUMENT, "scene is null");
+  if (sc->mesh_count && !sc->meshes) fail(VT_ERR_INVALID_ARGUMENT, "meshes is null");
+  if (sc->material_count && !sc->materials) fail(VT_ERR_INVALID_ARGUMENT, "materials is null");
+  if (sc->point_light_count && !sc->point_lights) fail(VT_ERR_INVALID_ARGUMENT, "point_lights is null");
+  PackedScene p;
+  std::vector<float> pos;
+  std::vector<uint32_t> idx, tri_mat;
+  for (size_t m = 0; m < sc->mesh_count; ++m) {
+    const vt_mesh_desc& md = sc->meshes[m];
+    if (md.material >= sc->material_count)
+      fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " references material " + std::to_string(md.material));
+    if ((md.vertex_count && !md.positions) || (md.triangle_count && !md.indices))
+      fail(VT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(m) + " has null arrays");
+    const uint32_t base = (uint32_t)(pos.size() / 4);
+    for (size_t v = 0; v < md.vertex_count; ++v) {
+      for (int k = 0; k < 3; ++k) {
+        const float x = md.positions[3 * v + k];
+        if (!std::isfinite(x)) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " has a non-finite position");
+        pos.push_back(x);
+      }
+      pos.push_back(0.0f);
+    }
+    for (size_t t = 0; t < md.triangle_count; ++t) {
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t i = md.indices[3 * t + k];
+        if (i >= md.vertex_count) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " index out of range");
+        idx.push_back(base + i);
+      }
+      idx.push_back(0u);
+      tri_mat.push_back(md.material);
+    }
+  }
+  // materials
+  std::vector<pt::Material> mats(sc->material_count);
+  for (size_t i = 0; i < sc->material_count; ++i) {
+    const vt_material_desc& d = sc->materials[i];
+    pt::Material& m = mats[i];
+    m.base_color = make_float3(d.base_color[0], d.base_color[1], d.base_color[2]);
+    m.roughness = d.roughness;
+    m.emission = make_float3(d.emission[0], d.emission[1], d.emission[2]);
+    m.ior = d.ior > 0.0f ? d.ior : 1.5f;
+    m.kind = d.transmission > 0.0f ? pt::kDielectric
+                                   : (d.metallic >= 0.5f ? pt::kConductor : pt::kLambert);
+    m.alpha = std::max(d.roughness * d.roughness, 1e-3f);
+    m.emissive = (d.emission[0] > 0.0f || d.emission[1] > 0.0f || d.emission[2] > 0.0f) ? 1u : 0u;
+    m.pad = 0;
+  }
+  const size_t ntri = tri_mat.size();
+  // geometry
+  BuildOptions bo;
+  const bool two_level = sc->instance_count > 0;
+  if (two_level && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
+  std::vector<uint32_t> node_words;
+  std::vector<float> rec_floats, inst_lanes, inst_tab, inst_rows;
+  int depth = 1;
+  uint32_t root = 0;
+  if (!two_level) {
+    p.binary = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
+    WideBvhHost w = encode_wide(p.binary, pos.data(), 4, idx.data(), 4, tri_mat.data(), node_base, rec_base);
+    node_words = std::move(w.nodes);
+    rec_floats = std::move(w.tris);
+    depth = w.depth;
+  } else {
+    // one bottom-level tree per mesh, in the mesh's own space, concatenated
+    std::vector<uint32_t> blas_root(sc->mesh_count);
+    std::vector<std::array<double, 6>> local_box(sc->mesh_count);
+    int blas_depth = 1;
+    size_t vbase = 0, tbase = 0;
+    for (size_t m = 0; m < sc->mesh_count; ++m) {
+      const vt_mesh_desc& md = sc->meshes[m];
+      std::vector<float> mp(pos.begin() + 4 * vbase, pos.begin() + 4 * (vbase + md.vertex_count));
+      std::vector<uint32_t> mi(idx.begin() + 4 * tbase, idx.begin() + 4 * (tbase + md.triangle_count));
+      for (size_t t = 0; t < md.triangle_count; ++t)
+        for (int k = 0; k < 3; ++k) mi[4 * t + k] -= (uint32_t)vbase;
+      std::vector<uint32_t> mm(md.triangle_count, md.material);
+      BinaryBvhHost b = build_binary_host(mp.data(), mp.size(), mi.data(), mi.size(), bo);
+      WideBvhHost w = encode_wide(b, mp.data(), 4, mi.data(), 4, mm.data(),
+                                          (uint32_t)(node_words.size() / 20), (uint32_t)(rec_floats.size() / 16));
+      blas_root[m] = (uint32_t)(node_words.size() / 20);
+      node_words.insert(node_words.end(), w.nodes.begin(), w.nodes.end());
+      rec_floats.insert(rec_floats.end(), w.tris.begin(), w.tris.end());
+      blas_depth = std::max(blas_depth, w.depth);
+      const BinaryNode& rn = b.nodes[0];
+      local_box[m] = {rn.mn[0], rn.mn[1], rn.mn[2], rn.mx[0], rn.mx[1], rn.mx[2]};
+      if (md.triangle_count == 0) local_box[m] = {0, 0, 0, 0, 0, 0};
+      vbase += md.vertex_count;
+      tbase += md.triangle_count;
+    }
+    // instances: world-to-local rows and world AABBs (transformAabb, scenePack.ts:197-223)
+    const size_t ni = sc->instance_count;
+    std::vector<InstanceRecord> recs(ni);
+    std::vector<double> aabbs(6 * ni);
+    for (size_t i = 0; i < ni; ++i) {
+      const vt_instance_desc& id = sc->instances[i];
+      if (id.mesh >= sc->mesh_count) fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references mesh " +
+                                                            std::to_string(id.mesh));
+      if (id.material >= sc->material_count)
+        fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references material " + std::to_string(id.material));
+      if (mats[id.material].emissive) fail(VT_ERR_INVALID_ARGUMENT, "emissive materials are not supported on instances");
+      double rm[16], inv[16];
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) rm[r * 4 + c] = id.local_to_world[c * 4 + r];
+      if (!invert4(rm, inv)) fail(VT_ERR_INVALID_ARGUMENT, "instance " + std::to_string(i) + " is not invertible");
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) inst_rows.push_back(id.local_to_world[c * 4 + r]);
+      InstanceRecord& rec = recs[i];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) rec.w2l[4 * r + c] = (float)inv[r * 4 + c];
+      rec.blas_root = blas_root[id.mesh];
+      rec.instance_id = (uint32_t)i;
+      rec.material = id.material;
+      rec.pad = 0;
+      const auto& lb = local_box[id.mesh];
+      double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (int c = 0; c < 8; ++c) {
+        const double q[3] = {(c & 1) ? lb[3] : lb[0], (c & 2) ? lb[4] : lb[1], (c & 4) ? lb[5] : lb[2]};
+        for (int k = 0; k < 3; ++k) {
+          const double v = rm[k * 4] * q[0] + rm[k * 4 + 1] * q[1] + rm[k * 4 + 2] * q[2] + rm[k * 4 + 3];
+          mn[k] = std::min(mn[k], v);
+          mx[k] = std::max(mx[k], v);
+        }
+      }
+      for (int k = 0; k < 3; ++k) { aabbs[6 * i + k] = mn[k]; aabbs[6 * i + 3 + k] = mx[k]; }
+    }
+    BinaryBvhHost tl = build_tlas_host(aabbs.data(), ni);
+    root = (uint32_t)(node_words.size() / 20);
+    WideBvhHost tw = encode_wide_tlas(tl, recs.data(), root);
+    node_words.insert(node_words.end(), tw.nodes.begin(), tw.nodes.end());
+    inst_lanes = std::move(tw.tris);
+    inst_tab.resize(16 * ni);
+    std::memcpy(inst_tab.data(), recs.data(), ni * sizeof(InstanceRecord));
+    depth = tw.depth + blas_depth;
+    p.binary = std::move(tl);
+  }
+  WideBvhHost w;
+  w.nodes = std::move(node_words);
+  w.tris = std::move(rec_floats);
+  w.depth = depth;
+  // emissive triangles, sampled uniformly over their total area
+  std::vector<float4> em;
+  std::vector<float> cdf;
+  double total = 0.0;
+  for (size_t t = 0; t < ntri && !two_level; ++t) {
+    if (!mats[tri_mat[t]].emissive) continue;
+    const float* a = &pos[4 * idx[4 * t]];
+    const float* b = &pos[4 * idx[4 * t + 1]];
+    const float* c = &pos[4 * idx[4 * t + 2]];
+    const double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+    const double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+    const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                 cz = e1[0] * e2[1] - e1[1] * e2[0];
+    const double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+    if (!(area > 0.0)) continue;
+    uint32_t mb = tri_mat[t];
+    float mf;
+    std::memcpy(&mf, &mb, 4);
+    em.push_back(make_float4(a[0], a[1], a[2], mf));
+    em.push_back(make_float4(b[0], b[1], b[2], (float)area));
+    em.push_back(make_float4(c[0], c[1], c[2], 0.0f));
+    total += area;
+    cdf.push_back((float)total);
+  }
+  for (float& x : cdf) x = (float)(x / total);
+  if (!cdf.empty()) cdf.back() = 1.0f;
+  // point lights
+  std::vector<float4> pts;
+  for (size_t i = 0; i < sc->point_light_count; ++i) {
+    const vt_point_light_desc& p = sc->point_lights[i];
+    pts.push_back(make_float4(p.position[0], p.position[1], p.position[2], 0.0f));
+    pts.push_back(make_float4(p.intensity[0], p.intensity[1], p.intensity[2], 0.0f));
+  }
+  // environment: equirectangular, importance by luminance * sin(theta)
+  std::vector<float4> envt;
+  std::vector<float> marg, cond;
+  const bool has_env = sc->environment_rgb && sc->environment_width > 0 && sc->environment_height > 0;
+  bool env_sampleable = false;
+  if (has_env) {
+    const int W = sc->environment_width, H = sc->environment_height;
+    const float scale = sc->environment_intensity > 0.0f ? sc->environment_intensity : 1.0f;
+    envt.resize((size_t)W * H);
+    cond.resize((size_t)H * (W + 1));
+    marg.resize(H + 1);
+    std::vector<double> rows(H);
+    double tot = 0.0;
+    for (int r = 0; r < H; ++r) {
+      const double st = std::sin(M_PI * (r + 0.5) / H);
+      double acc = 0.0;
+      cond[(size_t)r * (W + 1)] = 0.0f;
+      std::vector<double> cum(W);
+      for (int c = 0; c < W; ++c) {
+        const float* px = sc->environment_rgb + 3 * ((size_t)r * W + c);
+        envt[(size_t)r * W + c] = make_float4(px[0], px[1], px[2], 0.0f);
+        acc += std::max(0.0, luminance(px) * scale) * st;
+        cum[c] = acc;
+      }
+      for (int c = 0; c < W; ++c) cond[(size_t)r * (W + 1) + c + 1] = acc > 0 ? (float)(cum[c] / acc) : (float)(c + 1) / W;
+      cond[(size_t)r * (W + 1) + W] = 1.0f;
+      rows[r] = acc;
+      tot += acc;
+    }
+    marg[0] = 0.0f;
+    double run = 0.0;
+    for (int r = 0; r < H; ++r) {
+      run += rows[r];
+      marg[r + 1] = tot > 0 ? (float)(run / tot) : (float)(r + 1) / H;
+    }
+    marg[H] = 1.0f;
+    env_sampleable = tot > 0.0;
+  }
+  if (two_level && (node_base || rec_base)) fail(VT_ERR_INVALID_ARGUMENT, "instanced scenes cannot be offset");
+  p.two_level = two_level;
+  p.node_words = std::move(w.nodes);
+  p.rec_floats = std::move(w.tris);
+  p.depth = w.depth;
+  p.stack_depth = two_level ? 2 * w.depth + 6 : 2 * w.depth + 2;
+  p.root = two_level ? root : node_base;
+  p.inst_lanes = std::move(inst_lanes);
+  p.inst_tab = std::move(inst_tab);
+  p.inst_rows = std::move(inst_rows);
+  p.n_instances = sc->instance_count;
+  p.mats = std::move(mats);
+  p.emitters = std::move(em);
+  p.cdf = std::move(cdf);
+  p.emit_total = total;
+  p.points = std::move(pts);
+  p.env = std::move(envt);
+  p.marg = std::move(marg);
+  p.cond = std::move(cond);
+  p.has_env = has_env;
+  p.env_sampleable = env_sampleable;
+  p.env_w = has_env ? sc->environment_width : 0;
+  p.env_h = has_env ? sc->environment_height : 0;
+  p.env_scale = sc->environment_intensity > 0.0f ? sc->environment_intensity : 1.0f;
+  p.ntri = ntri;
+  return p;
+}
+
+}  // namespace vt

@@ -1,0 +1,47 @@
+// scene_pack.h -- a vt_scene_desc packed into the device layouts (host arrays).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/vitrum_pt.h"
+#include "bvh_host.h"
+#include "pt_common.cuh"
+#include "vt_common.h"
+
+namespace vt {
+
+struct PackedScene {
+  BinaryBvhHost binary;              // the tree (single level) or the top level over the instances
+  bool two_level = false;
+  std::vector<uint32_t> node_words;  // 20 words per wide node, indices offset by node_base
+  std::vector<float> rec_floats;     // 16 floats per triangle record, offset by rec_base
+  int depth = 1, stack_depth = 4;
+  uint32_t root = 0;                 // first node of the traversal
+  std::vector<float> inst_lanes, inst_tab, inst_rows;  // two-level: leaf-order records, by id, local-to-world rows
+  size_t n_instances = 0;
+  std::vector<pt::Material> mats;
+  std::vector<float4> emitters;      // 3 float4 per emissive triangle (world space)
+  std::vector<float> cdf;            // inclusive area CDF
+  double emit_total = 0.0;
+  std::vector<float4> points;        // 2 float4 per point light
+  std::vector<float4> env;
+  std::vector<float> marg, cond;
+  bool has_env = false, env_sampleable = false;
+  int env_w = 0, env_h = 0;
+  float env_scale = 1.0f;
+  size_t ntri = 0;
+};
+
+// Validates and packs; single-level trees are offset by node_base / rec_base
+// (scenes concatenated into shared arrays); instanced scenes need both zero.
+PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base);
+
+// 4x4 inverse (Gauss-Jordan, partial pivoting); false when singular.
+bool invert4(const double* m, double* inv);
+// inverse(P * V) of column-major view / projection as a row-major float matrix.
+void inverse_view_proj(const float* view, const float* proj, float* out_rm);
+
+}  // namespace vt

@@ -93,7 +93,8 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
                                                   int* __restrict__ status,
                                                   unsigned long long* __restrict__ ray_counter,
                                                   const uint32_t* __restrict__ n_dev,
-                                                  const float4* __restrict__ insts, uint32_t root) {
+                                                  const float4* __restrict__ insts, uint32_t root,
+                                                  const uint32_t* __restrict__ roots) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
         R.best = -1;
         gbase = ghits = gimask = 0;
         q0m = q1m = 0;
-        node = root;
+        node = roots ? __ldg(roots + ray) : root;
         expand = true;
         sp = 0;
         live = true;
@@ -419,11 +420,13 @@ void launch_stk(const TraceArgs& a, cudaStream_t s) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ANY, STK, TWO>, kBlock, smem);
   // persistent grid: every resident slot once, never more blocks than rays need
+  if (a.blocks_per_sm > 0) per_sm = std::min(per_sm, a.blocks_per_sm);
   size_t grid = (size_t)std::max(1, sms) * (size_t)std::max(1, per_sm);
   grid = std::min(grid, (a.n + kBlock - 1) / kBlock);
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
   k_trace<ANY, STK, TWO><<<(unsigned)grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded,
-                                                              a.status, a.counter, a.n_dev, a.insts, a.root);
+                                                              a.status, a.counter, a.n_dev, a.insts, a.root,
+                                                              a.roots);
 }
 
 template <bool ANY, bool TWO>

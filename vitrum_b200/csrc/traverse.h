@@ -24,8 +24,10 @@ struct TraceArgs {
   const float4* insts = nullptr;    // two-level: instance records (4 float4 each); nodes[root] is the TLAS root
   uint32_t root = 0;                // first node to expand
   const float4* inst_table = nullptr;  // refinement of instance hits: records by instance index
+  const uint32_t* roots = nullptr;    // optional per-ray root node (rays of several scenes in one launch)
   const float4* inst_l2w = nullptr;   // refinement of instance hits: local-to-world rows (3 per instance)
   int* inst_out = nullptr;          // optional: instance index per ray (-1 miss / single level)
+  int blocks_per_sm = 0;            // persistent CTAs per SM (0: the occupancy limit)
 };
 
 void launch_trace_closest(const TraceArgs& a, cudaStream_t s);

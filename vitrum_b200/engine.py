@@ -194,6 +194,39 @@ class Camera:
         return view.T.reshape(-1).astype(np.float32), proj.T.reshape(-1).astype(np.float32)
 
 
+def _marshal_scene(scene: "Scene"):
+    """(vt_scene_desc, list of arrays that must outlive the call)."""
+    keep = []
+    meshes = (_MeshDesc * max(1, len(scene.meshes)))()
+    for i, m in enumerate(scene.meshes):
+        p = np.ascontiguousarray(m.positions, np.float32).reshape(-1, 3)
+        ix = np.ascontiguousarray(m.indices, np.uint32).reshape(-1, 3)
+        keep += [p, ix]
+        meshes[i] = _MeshDesc(p.ctypes.data, p.shape[0], ix.ctypes.data, ix.shape[0], int(m.material))
+    mats = (_MaterialDesc * max(1, len(scene.materials)))()
+    for i, m in enumerate(scene.materials):
+        mats[i] = _MaterialDesc((ctypes.c_float * 3)(*m.base_color), m.roughness, m.metallic, m.transmission,
+                                m.ior, (ctypes.c_float * 3)(*m.emission))
+    pls = (_PointLightDesc * max(1, len(scene.point_lights)))()
+    for i, l in enumerate(scene.point_lights):
+        pls[i] = _PointLightDesc((ctypes.c_float * 3)(*l.position), (ctypes.c_float * 3)(*l.intensity))
+    env_ptr, ew, eh, ei = None, 0, 0, 1.0
+    if scene.environment is not None:
+        env = np.ascontiguousarray(scene.environment.rgb, np.float32)
+        keep.append(env)
+        env_ptr, eh, ew, ei = env.ctypes.data, env.shape[0], env.shape[1], scene.environment.intensity
+    insts = (_InstanceDesc * max(1, len(scene.instances)))()
+    for i, inst in enumerate(scene.instances):
+        M = np.asarray(inst.local_to_world, np.float32).reshape(4, 4)
+        insts[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
+    desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes),
+                      ctypes.cast(insts, ctypes.c_void_p) if scene.instances else None, len(scene.instances),
+                      ctypes.cast(mats, ctypes.c_void_p),
+                      len(scene.materials), ctypes.cast(pls, ctypes.c_void_p), len(scene.point_lights), env_ptr,
+                      ew, eh, ei)
+    return desc, (keep, meshes, insts, mats, pls)
+
+
 # ---------------------------------------------------------------- engine
 class _Debug:
     def __init__(self, engine: "Engine"):
@@ -229,34 +262,7 @@ class Engine:
         return self._h
 
     def set_scene(self, scene: Scene) -> None:
-        keep = []
-        meshes = (_MeshDesc * max(1, len(scene.meshes)))()
-        for i, m in enumerate(scene.meshes):
-            p = np.ascontiguousarray(m.positions, np.float32).reshape(-1, 3)
-            ix = np.ascontiguousarray(m.indices, np.uint32).reshape(-1, 3)
-            keep += [p, ix]
-            meshes[i] = _MeshDesc(p.ctypes.data, p.shape[0], ix.ctypes.data, ix.shape[0], int(m.material))
-        mats = (_MaterialDesc * max(1, len(scene.materials)))()
-        for i, m in enumerate(scene.materials):
-            mats[i] = _MaterialDesc((ctypes.c_float * 3)(*m.base_color), m.roughness, m.metallic, m.transmission,
-                                    m.ior, (ctypes.c_float * 3)(*m.emission))
-        pls = (_PointLightDesc * max(1, len(scene.point_lights)))()
-        for i, l in enumerate(scene.point_lights):
-            pls[i] = _PointLightDesc((ctypes.c_float * 3)(*l.position), (ctypes.c_float * 3)(*l.intensity))
-        env_ptr, ew, eh, ei = None, 0, 0, 1.0
-        if scene.environment is not None:
-            env = np.ascontiguousarray(scene.environment.rgb, np.float32)
-            keep.append(env)
-            env_ptr, eh, ew, ei = env.ctypes.data, env.shape[0], env.shape[1], scene.environment.intensity
-        insts = (_InstanceDesc * max(1, len(scene.instances)))()
-        for i, inst in enumerate(scene.instances):
-            M = np.asarray(inst.local_to_world, np.float32).reshape(4, 4)
-            insts[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
-        desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes),
-                          ctypes.cast(insts, ctypes.c_void_p) if scene.instances else None, len(scene.instances),
-                          ctypes.cast(mats, ctypes.c_void_p),
-                          len(scene.materials), ctypes.cast(pls, ctypes.c_void_p), len(scene.point_lights), env_ptr,
-                          ew, eh, ei)
+        desc, keep = _marshal_scene(scene)
         N.call("vt_set_scene", self.handle, ctypes.byref(desc))
 
     def render_frame(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,

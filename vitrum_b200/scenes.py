@@ -288,3 +288,27 @@ def instanced_cloud(n_instances: int = 1024, seed: int = 3, n_points: int = 32, 
     cam = Camera(eye=(0.0, 6.0, 3.2 * extent), target=(0.0, 0.0, 0.0), fov_y_deg=45.0, near=0.01,
                  far=20.0 * extent)
     return Scene(meshes=meshes, materials=mats, instances=insts, point_lights=lights, environment=env), cam
+
+
+# ---------------------------------------------------------------- batch of box rooms
+def box_room_sized(triangles: int):
+    """Box room with wall and box subdivisions chosen so that its triangle
+    count (10 w^2 + 24 b^2 + 2 with b = w / 2) is close to `triangles`."""
+    w = max(2, int(round((max(triangles, 64) / 16.0) ** 0.5)))
+    return box_room(wall_cells=w, box_cells=max(1, w // 2))
+
+
+def box_room_batch(n: int = 64, seed: int = 4):
+    """Batched-launch workload: n box rooms with triangle counts log-uniform in
+    [2^12, 2^21], resolution from {256^2, 512^2, 768^2, 1024^2}, 2-8 bounces,
+    4-32 spp.  Returns a list of (scene, camera, width, height, bounces, spp)."""
+    u = uniform(seed, 30, 4 * n).reshape(n, 4)
+    out = []
+    for i in range(n):
+        tris = int(round(2 ** (12 + 9 * u[i, 0])))
+        res = (256, 512, 768, 1024)[min(3, int(u[i, 1] * 4))]
+        bounces = 2 + min(6, int(u[i, 2] * 7))
+        spp = 4 + min(28, int(u[i, 3] * 29))
+        sc, cam = box_room_sized(tris)
+        out.append((sc, cam, res, res, bounces, spp))
+    return out
