@@ -25,6 +25,9 @@ step = one frame rendered from a cleared accumulation.  Metric: Mrays/s
 * nrc: equal-time relMSE of the neural-radiance-cache path tracer against
   plain path tracing on the instanced scene (480x270, 65,536-spp FP64 oracle),
   and both frame costs at 1920x1080 x 16 spp.
+* batch: 64 box rooms of uneven size rendered as one batch (autotuned launch
+  shape, one CUDA graph per batch frame) against the same frames one scene at
+  a time: aggregate Mrays/s of both.
 * cpu_baseline / --impl reference: the C restatement (oracle) of the same
   estimator on all host cores on a bounded crop (no reference CPU integrator
   exists at this scale; the reference's own CPU tracer is a Lambert-only
@@ -299,6 +302,65 @@ def run_instanced(args, dev, local, barrier):
     }
 
 
+# ------------------------------------------------------------------ batched workload
+def run_batch(args, dev, local, barrier):
+    """64 box rooms (triangles log-uniform in [2^12, 2^21], 256^2..1024^2,
+    2-8 bounces, 4-32 spp) rendered as one batch (one CUDA graph per batch
+    frame, launch shape from the autotuner) against the same frames rendered
+    one scene after another through the single-scene engine."""
+    from vitrum_b200 import scenes
+    from vitrum_b200.batch import Batch, BatchItem
+    from vitrum_b200.engine import Engine
+    work = scenes.box_room_batch(64)
+    items = [BatchItem(sc, cam, w, h, spp, b, frame_seed=100 + i) for i, (sc, cam, w, h, b, spp) in enumerate(work)]
+    t0 = time.perf_counter()
+    probe = Batch([BatchItem(it.scene, it.camera, it.width, it.height, 4, it.bounces, it.frame_seed) for it in items],
+                  device=local)
+    trials = probe.autotune()
+    tuned = probe.tuning
+    probe.close()
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b = Batch(items, device=local)
+    build_s = time.perf_counter() - t0
+    b.set_tuning(tuned["wave_paths"], bool(tuned["sort_by_material"]), tuned["trace_blocks_per_sm"])
+    b.render()  # warm-up (graph capture)
+    steps = max(1, min(args.steps, 3))
+    ms, rays = 0.0, 0
+    for _ in range(steps):
+        st = b.render()
+        ms += st["frame_ms"]
+        rays += st["closest_rays"] + st["shadow_rays"]
+    waves, launches = st["waves"], st["kernel_launches"]
+    b.close()
+    # the same frames, one scene at a time, through the engine (set_scene untimed)
+    e = Engine(device=local, max_bounces=8)
+    seq_ms, seq_rays, seq_launches = 0.0, 0, 0
+    for it in items:
+        e.set_scene(it.scene)
+        e.reset()
+        r0 = e.stats()
+        e.render_frame(it.camera, it.width, it.height, samples=it.samples, bounces=it.bounces,
+                       frame_seed=it.frame_seed)
+        r1 = e.stats()
+        seq_ms += r1["last_frame_ms"]
+        seq_rays += (r1["closest_rays"] - r0["closest_rays"]) + (r1["shadow_rays"] - r0["shadow_rays"])
+    e.dispose()
+    return {
+        "workload": "64 box rooms: triangles log-uniform in [2^12, 2^21] (%d total), resolution from "
+                    "{256^2, 512^2, 768^2, 1024^2}, 2-8 bounces, 4-32 spp; %d paths per batch frame"
+                    % (sum(it.scene.triangle_count for it in items),
+                       sum(it.width * it.height * it.samples for it in items)),
+        "value": rays / (ms / 1e3) / 1e6, "unit": "Mrays/s", "ms_per_batch_frame": ms / steps,
+        "waves": waves, "kernels_per_batch_frame": launches,
+        "sequential": {"value": seq_rays / (seq_ms / 1e3) / 1e6, "unit": "Mrays/s", "ms": seq_ms,
+                       "note": "same frames through the single-scene engine, one scene after another"},
+        "speedup_vs_sequential": (rays / ms) / (seq_rays / seq_ms) if seq_ms > 0 else None,
+        "tuning": tuned, "autotune_trials": trials, "autotune_s": round(tune_s, 1),
+        "scene_build_s": round(build_s, 2),
+    }
+
+
 # ------------------------------------------------------------------ radiance cache workload
 NRC_W, NRC_H, NRC_SPP, NRC_WARM, NRC_FRAMES = 480, 270, 16, 32, 8
 
@@ -413,6 +475,9 @@ def run_ours(args, rank, world, local):
         e.reset()
         e.render_frame(cam, W, H, samples=SPP, frame_seed=seed)
 
+    # launch shape from the project's autotuner (outside the timed region)
+    trials = e.autotune(cam, W, H, samples=SPP, frame_seed=555) if not args.no_autotune else []
+    tuning = e.tuning
     for i in range(args.warmup):
         frame(1000 + i)
     # per-stage device times of one frame (profiling path: direct launches, not timed for `value`)
@@ -450,6 +515,7 @@ def run_ours(args, rank, world, local):
     query = run_query(args, dev, local, rank, world, barrier) if not args.no_query else None
     instanced = run_instanced(args, dev, local, barrier) if not args.no_instanced else None
     nrc = run_nrc(args, dev, local, barrier) if not args.no_nrc else None
+    batch = run_batch(args, dev, local, barrier) if not args.no_batch else None
 
     if rank == 0:
         vc = _visits()["box_room_pt_512_64spp_5b"]
@@ -461,7 +527,7 @@ def run_ours(args, rank, world, local):
         peak, peak_kind = _peaks()
         launches = stages["trace_closest_launches"]  # one per bounce per wave
         waves = launches // BOUNCES if launches else 0
-        kernels_per_frame = waves * (1 + BOUNCES * 7 + 2)
+        kernels_per_frame = waves * (1 + BOUNCES * (5 + (2 if tuning["sort_by_material"] else 0)) + 2)
         cpu = None
         if not args.no_cpu_baseline:
             v, cores, sample = cpu_pt_baseline()
@@ -473,6 +539,7 @@ def run_ours(args, rank, world, local):
             "config": {"workload": WORKLOAD, "parallelism": f"replicas{world}", "resolution": [W, H], "spp": SPP,
                        "max_bounces": BOUNCES, "triangles": sc.triangle_count,
                        "l2": "per-frame wave state ~400 MB > 126 MB L2; BVH L2-resident",
+                       "tuning": tuning, "autotune_trials": trials,
                        "scene_build_s": round(build_s, 3)},
             "samples_per_s": samples_per_s, "ms_per_frame": dev_s * 1e3 / args.steps,
             "rays_per_frame": {"extension": per_frame_closest, "shadow": per_frame_shadow},
@@ -493,6 +560,7 @@ def run_ours(args, rank, world, local):
             "query": query,
             "instanced": instanced,
             "nrc": nrc,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
     e.dispose()
@@ -511,6 +579,8 @@ def main():
     ap.add_argument("--no-query", action="store_true")
     ap.add_argument("--no-instanced", action="store_true")
     ap.add_argument("--no-nrc", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--oracle-spp", type=int, default=65536)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -433,6 +433,13 @@ typedef struct vt_tuning_trial {
 vt_status vt_batch_autotune(vt_batch* batch, vt_tuning_trial* report, size_t report_capacity, size_t* report_count);
 vt_status vt_batch_destroy(vt_batch* batch);
 
+/* The autotuner for a single-scene engine: renders `frame` (from a cleared
+ * accumulation) once per candidate launch shape after a warm-up and keeps the
+ * fastest; later frames use it.  No reference counterpart. */
+vt_status vt_engine_autotune(vt_engine* engine, const vt_frame_input* frame, vt_tuning_trial* report,
+                             size_t report_capacity, size_t* report_count);
+vt_status vt_engine_get_tuning(const vt_engine* engine, vt_tuning* tuning);
+
 #ifdef __cplusplus
 }
 #endif

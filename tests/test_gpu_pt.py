@@ -208,3 +208,19 @@ def test_pick_primitive(cuda):
         N.call("vt_pick", plain.handle, 1.0, 1.0, N.ctypes.byref(N.ctypes.c_int32()))
     e.dispose()
     plain.dispose()
+
+
+def test_autotune_keeps_the_image(cuda):
+    sc, cam = small_room()
+    e = Engine(max_bounces=5)
+    e.set_scene(sc)
+    e.render_frame(cam, 32, 32, samples=8, frame_seed=4)
+    before = e.capture_frame()
+    trials = e.autotune(cam, 32, 32, samples=8, frame_seed=4)
+    assert len(trials) >= 4 and all(t["frame_ms"] > 0 for t in trials)
+    best = min(trials, key=lambda t: t["frame_ms"])
+    assert e.tuning["wave_paths"] == best["wave_paths"]
+    e.reset()
+    e.render_frame(cam, 32, 32, samples=8, frame_seed=4)
+    assert np.allclose(e.capture_frame(), before, rtol=1e-5, atol=1e-6)
+    e.dispose()

@@ -88,6 +88,7 @@ struct vt_engine {
   DeviceBuffer<unsigned long long> trace_counter, totals;
   DeviceBuffer<int> trace_status;
   std::unique_ptr<NrcEngine> nrc;
+  int trace_blocks_per_sm = 0;      // traversal CTAs per SM (0: occupancy limit), from the autotuner
   // graph cache: one executable per wave shape and mode
   struct Graph {
     uint32_t spp_wave = 0, bounces = 0;
@@ -357,6 +358,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.n_dev = w.counters + cur;
+    t.blocks_per_sm = e->trace_blocks_per_sm;
     B(StageTimer::kTraceClosest);
     vt::launch_trace_closest_records(t, s);
     E();
@@ -787,6 +789,72 @@ vt_status vt_set_nrc(vt_engine* e, const vt_nrc_render_options* o) {
       e->nrc.reset();
       throw;
     }
+  });
+}
+
+vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tuning_trial* report, size_t cap,
+                             size_t* count) {
+  return vt::guard([&] {
+    if (!e || !frame) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->has_scene) fail(VT_ERR_STATE, "autotune before setScene");
+    if (frame->samples < 1) fail(VT_ERR_RANGE, "autotune needs a frame with samples >= 1");
+    vt::DeviceScope ds(e->device);
+    std::vector<vt_tuning_trial> trials;
+    auto apply = [&](const vt_tuning& t) {
+      e->opts.wave_paths = t.wave_paths;
+      e->opts.sort_by_material = t.sort_by_material ? 0 : -1;
+      e->trace_blocks_per_sm = t.trace_blocks_per_sm;
+      e->drop_graphs();
+    };
+    auto time_it = [&](const vt_tuning& t) {
+      apply(t);
+      vt_frame_output out{};
+      double best = 1e30;
+      for (int rep = 0; rep < 3; ++rep) {  // first render captures the graph
+        reset_accumulation(e);
+        render_frame(e, frame, &out);
+        if (rep) best = std::min(best, e->last_ms);
+      }
+      trials.push_back({t, best});
+      return best;
+    };
+    vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 21), e->opts.sort_by_material >= 0 ? 1 : 0,
+                   e->trace_blocks_per_sm};
+    double best_ms = time_it(best);
+    for (int wp : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
+      if (wp == best.wave_paths) continue;
+      vt_tuning t = best;
+      t.wave_paths = wp;
+      const double ms = time_it(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    {
+      vt_tuning t = best;
+      t.sort_by_material = best.sort_by_material ? 0 : 1;
+      const double ms = time_it(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    for (int bp : {4, 6}) {
+      if (bp == best.trace_blocks_per_sm) continue;
+      vt_tuning t = best;
+      t.trace_blocks_per_sm = bp;
+      const double ms = time_it(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    apply(best);
+    reset_accumulation(e);
+    if (count) *count = trials.size();
+    if (report)
+      for (size_t i = 0; i < trials.size() && i < cap; ++i) report[i] = trials[i];
+  });
+}
+
+vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
+  return vt::guard([&] {
+    if (!e || !t) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 21);
+    t->sort_by_material = e->opts.sort_by_material >= 0 ? 1 : 0;
+    t->trace_blocks_per_sm = e->trace_blocks_per_sm;
   });
 }
 

@@ -328,6 +328,30 @@ class Engine:
                               warmup_frames, cfg)
         N.call("vt_set_nrc", self.handle, ctypes.byref(o))
 
+    def autotune(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,
+                 frame_seed: int = 0):
+        """The project's autotuner (vt_engine_autotune): times candidate launch
+        shapes (wave size, material sort, traversal CTAs per SM) on this frame
+        and keeps the fastest.  Returns the trials [(tuning dict, ms)]."""
+        from .batch import _Trial, _Tuning
+        view, proj = camera.matrices(width / height)
+        fin = _FrameInput((ctypes.c_float * 16)(*view), (ctypes.c_float * 16)(*proj), width, height, frame_seed,
+                          samples, bounces)
+        trials = (_Trial * 32)()
+        n = ctypes.c_size_t()
+        N.call("vt_engine_autotune", self.handle, ctypes.byref(fin), ctypes.cast(trials, ctypes.c_void_p), 32,
+               ctypes.byref(n))
+        self.width, self.height = width, height
+        return [dict({f: getattr(trials[i].tuning, f) for f, _ in _Tuning._fields_}, frame_ms=trials[i].frame_ms)
+                for i in range(min(n.value, 32))]
+
+    @property
+    def tuning(self) -> dict:
+        from .batch import _Tuning
+        t = _Tuning()
+        N.call("vt_engine_get_tuning", self.handle, ctypes.byref(t))
+        return {f: getattr(t, f) for f, _ in _Tuning._fields_}
+
     def stats(self) -> dict:
         s = _EngineStats()
         N.call("vt_engine_get_stats", self.handle, ctypes.byref(s))
