@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   // its next node without waiting for its queued triangles.  Node work and
   // triangle work therefore proceed in lock-step phases with most lanes
   // busy in each, and a lane whose ray finished takes the next unclaimed
-  // ray from its warp's pool (one atomicAdd per 64 rays).
+  // ray from its warp's pool (one atomicAdd per 16 rays).
   extern __shared__ uint2 stack_mem[];  // [STK][kBlock], one column per thread
   uint2* const stack = stack_mem + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31u;
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   constexpr uint32_t kNodeGroup = 0x80000000u;
   constexpr uint32_t kInstGroup = 0x40000000u;
   constexpr uint32_t kTagMask = 0xC0000000u;
-  constexpr uint32_t kChunk = 64;
+  constexpr uint32_t kChunk = 16;  // rays per pool refill: small enough to spread short launches over all warps
 
   bool live = false, exhausted = false;
   uint32_t ray = 0, pool_next = 0, pool_end = 0;
