@@ -64,8 +64,8 @@ METRIC = "Mrays/s (box-room path tracing 512x512, 64 spp, 5 bounces; extension +
 
 
 def _env_rank():
-    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
-            int(os.environ.get("LOCAL_RANK", "0")))
+    from vitrum_b200.replicas import env_rank
+    return env_rank()
 
 
 def _peaks():
@@ -444,26 +444,16 @@ def run_nrc(args, dev, local, barrier):
 # ------------------------------------------------------------------ path tracing workload
 def run_ours(args, rank, world, local):
     import torch
-    import torch.distributed as dist
     from vitrum_b200 import _native as N
     from vitrum_b200 import scenes
     from vitrum_b200.engine import Engine
 
+    from vitrum_b200.replicas import Group, replica_seed, whole_job_rate
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    group = Group(world, "nccl", dev)
+    barrier = group.barrier
+    max_over_ranks = group.max
 
     sc, cam = scenes.box_room()
     e = Engine(device=local, max_bounces=BOUNCES)
@@ -491,7 +481,7 @@ def run_ours(args, rank, world, local):
     frame_ms = []
     rays0 = e.stats()
     for i in range(args.steps):
-        frame(rank * 100000 + i)
+        frame(replica_seed(rank, i))
         frame_ms.append(e.stats()["last_frame_ms"])
     torch.cuda.synchronize(dev)
     barrier()
@@ -501,21 +491,23 @@ def run_ours(args, rank, world, local):
     closest = rays1["closest_rays"] - rays0["closest_rays"]
     shadow = rays1["shadow_rays"] - rays0["shadow_rays"]
     dev_s = max_over_ranks(sum(frame_ms) / 1e3)
-    value = world * rays / dev_s / 1e6
+    value = whole_job_rate(rays, world, dev_s) / 1e6
     samples_per_s = world * W * H * SPP * args.steps / dev_s
 
     # e2e: public Engine calls, image read back to host every step
     t0 = time.perf_counter()
     for i in range(args.steps):
-        frame(rank * 100000 + i)
+        frame(replica_seed(rank, i))
         img = e.capture_frame()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * rays / e2e_s / 1e6
 
-    query = run_query(args, dev, local, rank, world, barrier) if not args.no_query else None
-    instanced = run_instanced(args, dev, local, barrier) if not args.no_instanced else None
-    nrc = run_nrc(args, dev, local, barrier) if not args.no_nrc else None
-    batch = run_batch(args, dev, local, barrier) if not args.no_batch else None
+    # the sub-workloads are reported from single-GPU runs (replicas would repeat them)
+    solo = world == 1
+    query = run_query(args, dev, local, rank, world, barrier) if solo and not args.no_query else None
+    instanced = run_instanced(args, dev, local, barrier) if solo and not args.no_instanced else None
+    nrc = run_nrc(args, dev, local, barrier) if solo and not args.no_nrc else None
+    batch = run_batch(args, dev, local, barrier) if solo and not args.no_batch else None
 
     if rank == 0:
         vc = _visits()["box_room_pt_512_64spp_5b"]
@@ -564,9 +556,7 @@ def run_ours(args, rank, world, local):
         }
         print(json.dumps(line), flush=True)
     e.dispose()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.close()
 
 
 def main():
