@@ -169,7 +169,13 @@ typedef struct vt_material_desc {
   float transmission;
   float ior;
   float emission[3];
+  uint32_t flags;           /* VT_MATERIAL_* bits */
 } vt_material_desc;
+
+/* Material flags (the hits traceClosest / traceAny skip and retrace past,
+ * pt-webgpu/src/wgsl/pathTrace/intersection.wgsl.ts:462-528). */
+#define VT_MATERIAL_SINGLE_SIDED 1u  /* back-face hits are ignored by every ray */
+#define VT_MATERIAL_NO_SHADOW 2u     /* castShadow: false -- ignored by shadow (any-hit) rays */
 
 /* One triangle mesh in world space. */
 typedef struct vt_mesh_desc {

@@ -289,6 +289,7 @@ def flatten_scene(scene):
         mats[k, 0:3] = m.base_color
         mats[k, 3:7] = (m.roughness, m.metallic, m.transmission, m.ior)
         mats[k, 7:10] = m.emission
+        mats[k, 10] = (0 if getattr(m, "double_sided", True) else 1) | (0 if getattr(m, "cast_shadow", True) else 2)
     pts = np.array([[*l.position, *l.intensity] for l in scene.point_lights], np.float32).reshape(-1, 6)
     env = None if scene.environment is None else np.ascontiguousarray(scene.environment.rgb, np.float32)
     ei = 1.0 if scene.environment is None else float(scene.environment.intensity)

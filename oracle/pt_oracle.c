@@ -96,6 +96,7 @@ typedef struct {
   int kind; /* 0 lambert, 1 conductor, 2 dielectric */
   float alpha;
   int emissive;
+  unsigned flags; /* 1 single-sided (back faces ignored), 2 ignored by shadow rays */
 } orc_mat_t;
 
 typedef struct {
@@ -185,7 +186,14 @@ static long trace(const orc_pt_t* S, const double o[3], const double d[3], doubl
         long tri = S->r2s[nd[6] + i];
         double a[3], b[3], c[3], t;
         tri_vertices(S, tri, a, b, c);
+        const unsigned fl = S->mats[S->tmat[tri]].flags;
+        if (any && (fl & 2u)) continue; /* castShadow: false */
         if (orc_tri_hit_d(o, d, a, b, c, 0.0, &t) && t > 0.0 && t < closest) {
+          if (fl & 1u) { /* single-sided: skip hits on the back face */
+            const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+            const double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            if (d[0] * n[0] + d[1] * n[1] + d[2] * n[2] > 0.0) continue;
+          }
           closest = t;
           best = tri;
           if (any) { *t_out = t; return best; }
@@ -553,6 +561,7 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
     mats[i].kind = m[5] > 0 ? 2 : (m[4] >= 0.5f ? 1 : 0);
     mats[i].alpha = fmaxf(m[3] * m[3], 1e-3f);
     mats[i].emissive = m[7] > 0 || m[8] > 0 || m[9] > 0;
+    mats[i].flags = (unsigned)m[10];
   }
   S.mats = mats;
   uint32_t* em = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));

@@ -99,7 +99,7 @@ struct Material {
   uint32_t kind;
   float alpha;       // GGX alpha = max(roughness^2, 1e-3)
   uint32_t emissive; // emission > 0
-  uint32_t pad;
+  uint32_t flags;    // VT_MATERIAL_* bits
 };
 
 __device__ __forceinline__ float3 schlick(float3 f0, float c) {

@@ -119,7 +119,8 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
                                    : (d.metallic >= 0.5f ? pt::kConductor : pt::kLambert);
     m.alpha = std::max(d.roughness * d.roughness, 1e-3f);
     m.emissive = (d.emission[0] > 0.0f || d.emission[1] > 0.0f || d.emission[2] > 0.0f) ? 1u : 0u;
-    m.pad = 0;
+    if (d.flags & ~3u) fail(VT_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has unknown flags");
+    m.flags = d.flags;
   }
   const size_t ntri = tri_mat.size();
   // geometry
@@ -136,6 +137,14 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     node_words = std::move(w.nodes);
     rec_floats = std::move(w.tris);
     depth = w.depth;
+    // material flags of each triangle record in its free word (v2.w); padding records stay 0
+    for (size_t r = 0; r + 16 <= rec_floats.size(); r += 16) {
+      if (rec_floats[r + 15] == 0.0f) continue;
+      uint32_t mat;
+      std::memcpy(&mat, &rec_floats[r + 7], 4);
+      const uint32_t fl = mat < mats.size() ? mats[mat].flags : 0u;
+      std::memcpy(&rec_floats[r + 11], &fl, 4);
+    }
   } else {
     // one bottom-level tree per mesh, in the mesh's own space, concatenated
     std::vector<uint32_t> blas_root(sc->mesh_count);
@@ -185,7 +194,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
       rec.blas_root = blas_root[id.mesh];
       rec.instance_id = (uint32_t)i;
       rec.material = id.material;
-      rec.pad = 0;
+      rec.pad = mats[id.material].flags;
       const auto& lb = local_box[id.mesh];
       double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
       for (int c = 0; c < 8; ++c) {

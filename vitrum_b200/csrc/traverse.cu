@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   WtRay wr;
   float wox = 0.f, woy = 0.f, woz = 0.f, wdx = 0.f, wdy = 0.f, wdz = 0.f;  // world ray (two-level)
   int cur_inst = -1, best_inst = -1;
+  uint32_t cur_flags = 0;  // material flags of the instance being traversed (two-level)
   uint32_t gbase = 0, ghits = 0, gimask = 0, node = 0;
   uint32_t q0b = 0, q0m = 0, q1b = 0, q1m = 0;  // triangle-group queue (base, hit mask)
   bool expand = false;
@@ -147,6 +148,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
         set_ray(R, wr, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
         if (TWO) { wox = r0.x; woy = r0.y; woz = r0.z; wdx = r1.x; wdy = r1.y; wdz = r1.z; }
         cur_inst = best_inst = -1;
+        cur_flags = 0;
         R.best = -1;
         gbase = ghits = gimask = 0;
         q0m = q1m = 0;
@@ -218,9 +220,11 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
             th &= th - 1;
             const float4* rec = tris + 4 * (size_t)tri;
             const float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
+            const uint32_t fl = __float_as_uint(c.w) | cur_flags;
+            if (ANY && (fl & VT_MATERIAL_NO_SHADOW)) continue;
             const float t = wt_candidate(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
                                          make_float3(c.x, c.y, c.z), R.tmin, R.closest,
-                                         [rec] { return __ldg(rec + 3); });
+                                         [rec] { return __ldg(rec + 3); }, (fl & VT_MATERIAL_SINGLE_SIDED) != 0);
             if (t >= 0.0f) { R.closest = t; R.best = (int)tri; best_inst = cur_inst; }
           }
         }
@@ -237,8 +241,11 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       if (q0m == 0) { q0b = q1b; q0m = q1m; q1m = 0; }
       const float4* rec = tris + 4 * (size_t)tri;
       const float4 a = __ldg(rec), b = __ldg(rec + 1), c = __ldg(rec + 2);
+      const uint32_t fl = __float_as_uint(c.w) | cur_flags;
+      if (ANY && (fl & VT_MATERIAL_NO_SHADOW)) continue;
       const float t = wt_candidate(wr, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
-                                   make_float3(c.x, c.y, c.z), R.tmin, R.closest, [rec] { return __ldg(rec + 3); });
+                                   make_float3(c.x, c.y, c.z), R.tmin, R.closest, [rec] { return __ldg(rec + 3); },
+                                   (fl & VT_MATERIAL_SINGLE_SIDED) != 0);
       if (t >= 0.0f) {
         R.closest = t;
         R.best = (int)tri;
@@ -276,6 +283,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
           --sp;
           set_ray(R, wr, wox, woy, woz, wdx, wdy, wdz);
           cur_inst = -1;
+          cur_flags = 0;
         } else if (TWO && tag == kInstGroup) {
           // enter the next instance of the group
           --sp;
@@ -296,6 +304,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
             const float ldz = fmaf(m2.x, wdx, fmaf(m2.y, wdy, m2.z * wdz));
             set_ray(R, wr, lox, loy, loz, ldx, ldy, ldz);
             cur_inst = (int)meta.y;
+            cur_flags = meta.w;
             node = meta.x;
             expand = true;
             break;

@@ -234,7 +234,7 @@ __device__ __noinline__ float wt_zero_edge_t(const WtRay r, const float3 A, cons
 // (`nrm` = (n.xyz, valid)), leaving the ray-dependent side determinant.
 template <class NormalFetch>
 __device__ __forceinline__ float wt_candidate(const WtRay& r, float3 a, float3 b, float3 c, float exclusive_min_t,
-                                              float closest, NormalFetch nrm_fetch) {
+                                              float closest, NormalFetch nrm_fetch, bool cull_back = false) {
   float apx, apy, az, bpx, bpy, bz, cpx, cpy, cz;
   wt_project3(r, a, apx, apy, az);
   wt_project3(r, b, bpx, bpy, bz);
@@ -268,6 +268,7 @@ __device__ __forceinline__ float wt_candidate(const WtRay& r, float3 a, float3 b
   const float sd = -__fadd_rn(__fadd_rn(__fmul_rn(r.dn[0], nrm.x), __fmul_rn(r.dn[1], nrm.y)),
                               __fmul_rn(r.dn[2], nrm.z));
   if (sd == 0.0f || !isfinite(sd)) return -1.0f;
+  if (cull_back && sd < 0.0f) return -1.0f;  // single-sided surface seen from behind: traversal continues past it
   return t;
 }
 

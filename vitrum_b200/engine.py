@@ -29,7 +29,8 @@ class _EngineOptions(ctypes.Structure):
 
 class _MaterialDesc(ctypes.Structure):
     _fields_ = [("base_color", ctypes.c_float * 3), ("roughness", ctypes.c_float), ("metallic", ctypes.c_float),
-                ("transmission", ctypes.c_float), ("ior", ctypes.c_float), ("emission", ctypes.c_float * 3)]
+                ("transmission", ctypes.c_float), ("ior", ctypes.c_float), ("emission", ctypes.c_float * 3),
+                ("flags", ctypes.c_uint32)]
 
 
 class _MeshDesc(ctypes.Structure):
@@ -97,6 +98,12 @@ class Material:
     transmission: float = 0.0
     ior: float = 1.5
     emission: Sequence[float] = (0.0, 0.0, 0.0)
+    double_sided: bool = True   # False: back-face hits are skipped by every ray
+    cast_shadow: bool = True    # False: shadow rays pass through (castShadow: false)
+
+    @property
+    def flags(self) -> int:
+        return (0 if self.double_sided else 1) | (0 if self.cast_shadow else 2)
 
 
 @dataclass
@@ -206,7 +213,7 @@ def _marshal_scene(scene: "Scene"):
     mats = (_MaterialDesc * max(1, len(scene.materials)))()
     for i, m in enumerate(scene.materials):
         mats[i] = _MaterialDesc((ctypes.c_float * 3)(*m.base_color), m.roughness, m.metallic, m.transmission,
-                                m.ior, (ctypes.c_float * 3)(*m.emission))
+                                m.ior, (ctypes.c_float * 3)(*m.emission), m.flags)
     pls = (_PointLightDesc * max(1, len(scene.point_lights)))()
     for i, l in enumerate(scene.point_lights):
         pls[i] = _PointLightDesc((ctypes.c_float * 3)(*l.position), (ctypes.c_float * 3)(*l.intensity))
