@@ -155,8 +155,8 @@ typedef struct vt_engine_options {
   int32_t max_samples_per_pixel;  /* default 4096 (index.ts:370) */
   int32_t debug;                  /* 1 enables vt_pick (EngineOptions.debug, engine/factory.ts) */
   int32_t oracle_accumulation;    /* 1 keeps FP64 per-pixel sums and sums of squares */
-  int32_t sort_by_material;       /* 0 = on (default), -1 = off: shading in queue order */
-  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^21 */
+  int32_t sort_by_material;       /* 1 = sort shading work by BSDF family; 0 (default) = queue order */
+  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^22 */
 } vt_engine_options;
 
 /* Material (core Material subset, core/src/scene/material.ts): transmission > 0

@@ -87,7 +87,7 @@ class Batch:
         N.call("vt_batch_get_tuning", self.handle, ctypes.byref(t))
         return {f: getattr(t, f) for f, _ in _Tuning._fields_}
 
-    def set_tuning(self, wave_paths: int, sort_by_material: bool = True, trace_blocks_per_sm: int = 0) -> None:
+    def set_tuning(self, wave_paths: int, sort_by_material: bool = False, trace_blocks_per_sm: int = 0) -> None:
         t = _Tuning(wave_paths, 1 if sort_by_material else 0, trace_blocks_per_sm)
         N.call("vt_batch_set_tuning", self.handle, ctypes.byref(t))
 

@@ -24,7 +24,7 @@ using vt::fail;
 struct vt_batch {
   int device = 0;
   vt_engine_options opts{};
-  vt_tuning tuning{1 << 21, 1, 0};
+  vt_tuning tuning{1 << 22, 0, 0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // scenes
@@ -242,7 +242,7 @@ vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_b
     if (b->opts.max_bounces == 0) b->opts.max_bounces = 8;
     if (b->opts.max_bounces < 1 || b->opts.max_bounces > 8) fail(VT_ERR_RANGE, "max_bounces must be in [1, 8]");
     if (b->opts.wave_paths > 0) b->tuning.wave_paths = b->opts.wave_paths;
-    if (b->opts.sort_by_material < 0) b->tuning.sort_by_material = 0;
+    if (b->opts.sort_by_material > 0) b->tuning.sort_by_material = 1;
     int n = 0;
     VT_CUDA(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) fail(VT_ERR_INVALID_ARGUMENT, "no such CUDA device");

@@ -325,7 +325,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
   f.spp_wave = spp_wave;
   f.max_bounces = bounces;
   f.paths = f.width * f.height * spp_wave;
-  f.sort_by_material = e->opts.sort_by_material >= 0 ? 1u : 0u;
+  f.sort_by_material = e->opts.sort_by_material > 0 ? 1u : 0u;
   if (mode == kNrcTrain) {
     f.train = 1;
     f.paths = e->nrc->train_paths;
@@ -487,7 +487,7 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   }
   const uint32_t spp = (uint32_t)std::min(in->samples, room);
   const uint32_t wh = (uint32_t)(e->width * e->height);
-  const uint32_t wave_paths = e->opts.wave_paths > 0 ? (uint32_t)e->opts.wave_paths : (1u << 21);
+  const uint32_t wave_paths = e->opts.wave_paths > 0 ? (uint32_t)e->opts.wave_paths : (1u << 22);
   uint32_t spp_wave = std::max<uint32_t>(1u, wave_paths / wh);
   spp_wave = std::min(spp_wave, spp);
   while (spp % spp_wave) --spp_wave;  // equal waves: one graph per frame shape
@@ -802,7 +802,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
     std::vector<vt_tuning_trial> trials;
     auto apply = [&](const vt_tuning& t) {
       e->opts.wave_paths = t.wave_paths;
-      e->opts.sort_by_material = t.sort_by_material ? 0 : -1;
+      e->opts.sort_by_material = t.sort_by_material ? 1 : 0;
       e->trace_blocks_per_sm = t.trace_blocks_per_sm;
       e->drop_graphs();
     };
@@ -818,7 +818,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       trials.push_back({t, best});
       return best;
     };
-    vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 21), e->opts.sort_by_material >= 0 ? 1 : 0,
+    vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 22), e->opts.sort_by_material > 0 ? 1 : 0,
                    e->trace_blocks_per_sm};
     double best_ms = time_it(best);
     for (int wp : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
@@ -852,8 +852,8 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
 vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
   return vt::guard([&] {
     if (!e || !t) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
-    t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 21);
-    t->sort_by_material = e->opts.sort_by_material >= 0 ? 1 : 0;
+    t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 22);
+    t->sort_by_material = e->opts.sort_by_material > 0 ? 1 : 0;
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
   });
 }

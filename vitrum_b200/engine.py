@@ -250,10 +250,10 @@ class Engine:
     """createPTEngine (pt-webgpu factory, index.ts:2363) on the CUDA backend."""
 
     def __init__(self, device: int = 0, max_bounces: int = 8, max_samples_per_pixel: int = 4096,
-                 debug: bool = False, oracle_accumulation: bool = False, sort_by_material: bool = True,
+                 debug: bool = False, oracle_accumulation: bool = False, sort_by_material: bool = False,
                  wave_paths: int = 0):
         opts = _EngineOptions(max_bounces, max_samples_per_pixel, 1 if debug else 0, 1 if oracle_accumulation else 0,
-                              0 if sort_by_material else -1, wave_paths)
+                              1 if sort_by_material else 0, wave_paths)
         h = ctypes.c_void_p()
         N.call("vt_create", device, ctypes.byref(opts), ctypes.byref(h))
         self._h = h
