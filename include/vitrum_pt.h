@@ -191,6 +191,26 @@ typedef struct vt_point_light_desc {
   float intensity[3];       /* radiant intensity; irradiance falls off as 1/d^2 */
 } vt_point_light_desc;
 
+/* Directional light (sun): light travelling along `direction`.  With
+ * angular_radius 0 a delta light of irradiance `irradiance` at normal
+ * incidence; otherwise a disc of that angular radius and that irradiance,
+ * sampled by cone and reachable by BSDF rays that escape the scene (MIS). */
+typedef struct vt_directional_light_desc {
+  float direction[3];
+  float irradiance[3];
+  float angular_radius;     /* radians, < pi/2 */
+} vt_directional_light_desc;
+
+/* Rectangle light: corner + [0,1] edge_u + [0,1] edge_v, emitting `radiance`
+ * from the side edge_u x edge_v faces; seen from behind and by shadow rays it
+ * is transparent.  Packed as two emissive triangles (single-level scenes). */
+typedef struct vt_rect_light_desc {
+  float corner[3];
+  float edge_u[3];
+  float edge_v[3];
+  float radiance[3];
+} vt_rect_light_desc;
+
 /* One placement of a mesh (core instanced-mesh / transform; the TLAS instance
  * of shared-bvh/src/tlas.ts:859).  With instances present every mesh is a
  * bottom-level prototype in its local space and is drawn only through
@@ -216,6 +236,10 @@ typedef struct vt_scene_desc {
   int32_t environment_width;
   int32_t environment_height;
   float environment_intensity;
+  const vt_directional_light_desc* directional_lights;
+  size_t directional_light_count;
+  const vt_rect_light_desc* rect_lights;
+  size_t rect_light_count;
 } vt_scene_desc;
 
 /* Per-frame input (core FrameInput, core/src/frame.ts:91): camera matrices

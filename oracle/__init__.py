@@ -261,6 +261,7 @@ def _pt_lib():
         P = ctypes.c_void_p
         L.orc_pt_render.restype = ctypes.c_int
         L.orc_pt_render.argtypes = [P, ctypes.c_long, P, ctypes.c_long, P, P, ctypes.c_int, P, ctypes.c_long, P,
+                                    ctypes.c_long, P,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                     ctypes.c_int, P, P, P, P, ctypes.c_long, P]
@@ -284,16 +285,49 @@ def flatten_scene(scene):
         idx.append(i4)
         tm.append(np.full(i.shape[0], m.material, np.uint32))
         base += p.shape[0]
-    mats = np.zeros((len(scene.materials), 12), np.float32)
+    rects = list(getattr(scene, "rect_lights", []))
+    mats = np.zeros((len(scene.materials) + len(rects), 12), np.float32)
     for k, m in enumerate(scene.materials):
         mats[k, 0:3] = m.base_color
         mats[k, 3:7] = (m.roughness, m.metallic, m.transmission, m.ior)
         mats[k, 7:10] = m.emission
         mats[k, 10] = (0 if getattr(m, "double_sided", True) else 1) | (0 if getattr(m, "cast_shadow", True) else 2)
+    # rectangle lights: two one-sided emissive triangles each, transparent to shadow rays
+    for j, r in enumerate(rects):
+        k = len(scene.materials) + j
+        mats[k, 3:7] = (1.0, 0.0, 0.0, 1.5)
+        mats[k, 7:10] = r.radiance
+        mats[k, 10] = 3
+        c, u, v = (np.asarray(x, np.float32) for x in (r.corner, r.edge_u, r.edge_v))
+        p4 = np.zeros((4, 4), np.float32)
+        for q, (a, b) in enumerate(((0, 0), (1, 0), (1, 1), (0, 1))):
+            p4[q, :3] = (c + np.float32(a) * u) + np.float32(b) * v
+        i4 = np.array([[0, 1, 2, 0], [0, 2, 3, 0]], np.uint32)
+        i4[:, :3] += base
+        pos.append(p4)
+        idx.append(i4)
+        tm.append(np.full(2, k, np.uint32))
+        base += 4
     pts = np.array([[*l.position, *l.intensity] for l in scene.point_lights], np.float32).reshape(-1, 6)
     env = None if scene.environment is None else np.ascontiguousarray(scene.environment.rgb, np.float32)
     ei = 1.0 if scene.environment is None else float(scene.environment.intensity)
     return np.concatenate(pos), np.concatenate(idx), np.concatenate(tm), mats, pts, env, ei
+
+
+def directional_lights(scene):
+    """(n, 8) float32: direction towards the light, cos(angular radius) (1 for a
+    delta light), rgb (irradiance of a delta light, disc radiance otherwise), delta flag."""
+    out = []
+    for l in getattr(scene, "directional_lights", []):
+        d = np.asarray(l.direction, np.float32).astype(np.float64)
+        n = float(np.sqrt(d @ d))
+        delta = float(l.angular_radius) == 0.0
+        st = np.sin(np.float64(np.float32(l.angular_radius)))
+        to_l = 1.0 if delta else 1.0 / (np.pi * st * st)
+        E = np.asarray(l.irradiance, np.float32).astype(np.float64)
+        out.append([*(-d / n), 1.0 if delta else np.cos(np.float64(np.float32(l.angular_radius))),
+                    *(E * to_l), 1.0 if delta else 0.0])
+    return np.array(out, np.float32).reshape(-1, 8)
 
 
 def inverse_view_proj(camera, width, height):
@@ -319,8 +353,10 @@ def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_bas
     lc = np.zeros((max(log_rays, 0), 8), np.float32)
     ls = np.zeros((max(log_rays, 0), 8), np.float32)
     totals = np.zeros(2, np.int64)
+    dls = directional_lights(scene)
     r = _pt_lib().orc_pt_render(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
-                                _p(pts) if pts.size else None, pts.shape[0], _p(env) if env is not None else None,
+                                _p(pts) if pts.size else None, pts.shape[0], _p(dls) if dls.size else None,
+                                dls.shape[0], _p(env) if env is not None else None,
                                 ew, eh, ei, _p(ivp), width, height, spp, max_bounces, seed, sample_base, bias,
                                 nthreads, _p(s), _p(q), _p(lc) if log_rays else None, _p(ls) if log_rays else None,
                                 max(log_rays, 0), _p(totals))

@@ -114,6 +114,8 @@ typedef struct {
   float em_area;
   const float* points;    /* 6 floats each: position, intensity */
   long n_points;
+  const float* dirs; /* 8 floats: direction towards the light, cos(angular radius), rgb, delta */
+  long n_dirs;
   const float* env;       /* W*H*3 */
   const float* env_marg;  /* H+1 */
   const float* env_cond;  /* H*(W+1) */
@@ -353,6 +355,27 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
     ls.valid = 1;
     return ls;
   }
+  e -= (uint32_t)S->n_points;
+  if ((long)e < S->n_dirs) {
+    const float* q = S->dirs + 8 * e;
+    v3 w = V(q[0], q[1], q[2]);
+    ls.dist = INFINITY;
+    ls.Le = V(q[4], q[5], q[6]);
+    if (q[7] != 0.0f) {
+      ls.wi = w;
+      ls.pdf = psel;
+      ls.delta = 1;
+    } else {
+      float u1 = rand01(rng), u2 = rand01(rng);
+      float ct = 1.0f - u1 * (1.0f - q[3]), st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct)), ph = 2.0f * PI_F * u2;
+      v3 tu, tv;
+      onb(w, &tu, &tv);
+      ls.wi = add(add(scl(tu, st * cosf(ph)), scl(tv, st * sinf(ph))), scl(w, ct));
+      ls.pdf = psel / (2.0f * PI_F * (1.0f - q[3]));
+    }
+    ls.valid = 1;
+    return ls;
+  }
   float u1 = rand01(rng), u2 = rand01(rng);
   int row = cdf_search(S->env_marg + 1, S->env_h, u1);
   const float* cc = S->env_cond + (size_t)row * (S->env_w + 1);
@@ -393,6 +416,13 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
     log_ray(S, 0, od, dd, INFINITY);
     long tri = trace(S, od, dd, INFINITY, 0, &t);
     if (tri < 0) {
+      for (long k = 0; k < S->n_dirs; ++k) {
+        const float* q = S->dirs + 8 * k;
+        if (q[7] != 0.0f || dot3(d, V(q[0], q[1], q[2])) < q[3]) continue;
+        float w = 1.0f;
+        if (!prev_delta) w = power_h(prev_pdf, 1.0f / ((float)S->n_entries * 2.0f * PI_F * (1.0f - q[3])));
+        L = add(L, scl(mul(T, V(q[4], q[5], q[6])), w));
+      }
       if (S->env) {
         int col, row;
         float st;
@@ -538,7 +568,8 @@ static void* pt_worker(void* arg) {
  * sum and sum of squares (3 per pixel).  Returns 0, or -1 on a build error.
  */
 int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
-                  const float* materials, int n_mat, const float* points, long n_points, const float* env,
+                  const float* materials, int n_mat, const float* points, long n_points, const float* dirs,
+                  long n_dirs, const float* env,
                   int env_w, int env_h, float env_scale, const float* inv_vp, int width, int height, int spp,
                   int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
                   double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals) {
@@ -589,6 +620,8 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
   S.em_area = (float)total;
   S.points = points;
   S.n_points = n_points;
+  S.dirs = dirs;
+  S.n_dirs = n_dirs;
   float *marg = NULL, *cond = NULL;
   if (env) {
     S.env = env;
@@ -628,7 +661,7 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
     free(rows);
     free(cum);
   }
-  S.n_entries = (ne ? 1 : 0) + (int)n_points + (S.env_sampleable ? 1 : 0);
+  S.n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_dirs + (S.env_sampleable ? 1 : 0);
   S.bias = bias;
   S.inv_vp = inv_vp;
   S.width = width;

@@ -63,7 +63,7 @@ struct vt_engine {
   DeviceBuffer<vt::pt::Material> materials;
   DeviceBuffer<float4> emitters;
   DeviceBuffer<float> emitter_cdf;
-  DeviceBuffer<float4> points;
+  DeviceBuffer<float4> points, dirs;
   DeviceBuffer<float4> env;
   DeviceBuffer<float> env_marginal, env_conditional;
   vt::pt::SceneView view;
@@ -154,6 +154,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   upload(e->emitters, p.emitters, s);
   upload(e->emitter_cdf, p.cdf, s);
   upload(e->points, p.points, s);
+  upload(e->dirs, p.dirs, s);
   upload(e->env, p.env, s);
   upload(e->env_marginal, p.marg, s);
   upload(e->env_conditional, p.cond, s);
@@ -173,13 +174,15 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.emit_area_total = (float)p.emit_total;
   v.points = e->points.ptr;
   v.n_points = (uint32_t)(p.points.size() / 2);
+  v.dirs = e->dirs.ptr;
+  v.n_dirs = (uint32_t)(p.dirs.size() / 2);
   v.env = p.has_env ? e->env.ptr : nullptr;
   v.env_marginal = p.env_sampleable ? e->env_marginal.ptr : nullptr;
   v.env_conditional = p.env_sampleable ? e->env_conditional.ptr : nullptr;
   v.env_w = p.env_w;
   v.env_h = p.env_h;
   v.env_scale = p.env_scale;
-  v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + (p.env_sampleable ? 1u : 0u);
+  v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_dirs + (p.env_sampleable ? 1u : 0u);
   e->view = v;
   e->binary = std::move(p.binary);
   e->ntri = (int64_t)p.ntri;

@@ -137,6 +137,28 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
     ls.valid = true;
     return ls;
   }
+  e -= sc.n_points;
+  if (e < sc.n_dirs) {
+    const float4 dw = __ldg(sc.dirs + 2 * e), dl = __ldg(sc.dirs + 2 * e + 1);
+    const float3 w = f3(dw.x, dw.y, dw.z);
+    ls.dist = CUDART_INF_F;
+    ls.Le = f3(dl.x, dl.y, dl.z);
+    if (dl.w != 0.0f) {  // delta: irradiance along w
+      ls.wi = w;
+      ls.pdf = psel;
+      ls.delta = true;
+    } else {  // disc of angular radius acos(dw.w): uniform in the cone
+      const float u1 = rand01(rng), u2 = rand01(rng);
+      const float ct = 1.0f - u1 * (1.0f - dw.w), st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+      const float ph = 2.0f * CUDART_PI_F * u2;
+      float3 tu, tv;
+      onb(w, tu, tv);
+      ls.wi = tu * (st * cosf(ph)) + tv * (st * sinf(ph)) + w * ct;
+      ls.pdf = psel / (2.0f * CUDART_PI_F * (1.0f - dw.w));
+    }
+    ls.valid = true;
+    return ls;
+  }
   // environment
   const float u1 = rand01(rng), u2 = rand01(rng);
   const uint32_t row = cdf_search(sc.env_marginal + 1, (uint32_t)sc.env_h, u1);
@@ -304,6 +326,15 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
       const float3 o = f3(r0.x, r0.y, r0.z), d = f3(r1.x, r1.y, r1.z);
       float3 rad = f3(0.0f, 0.0f, 0.0f);
       if (h.x < 0) {
+        // escaped: discs of directional lights it points into (MIS against their cone sampling)
+        for (uint32_t k = 0; k < sc.n_dirs; ++k) {
+          const float4 dw = __ldg(sc.dirs + 2 * k), dl = __ldg(sc.dirs + 2 * k + 1);
+          if (dl.w != 0.0f || dot(d, f3(dw.x, dw.y, dw.z)) < dw.w) continue;
+          float wgt = 1.0f;
+          if (!prev_delta)
+            wgt = power_heuristic(prev_pdf, 1.0f / ((float)sc.n_light_entries * 2.0f * CUDART_PI_F * (1.0f - dw.w)));
+          rad = rad + T * f3(dl.x, dl.y, dl.z) * wgt;
+        }
         if (sc.env) {
           int col, row;
           float sin_t;

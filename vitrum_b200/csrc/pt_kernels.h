@@ -27,13 +27,17 @@ struct SceneView {
   // point lights: 2 float4 each = (position, 0), (intensity rgb, 0)
   const float4* points = nullptr;
   uint32_t n_points = 0;
+  // directional lights: 2 float4 each = (direction towards the light, cos of the angular radius),
+  // (rgb: irradiance of a delta light or radiance of a disc, 1 for delta)
+  const float4* dirs = nullptr;
+  uint32_t n_dirs = 0;
   // equirectangular environment (rgb as float4), with marginal/conditional CDFs
   const float4* env = nullptr;
   const float* env_marginal = nullptr;  // env_h + 1 entries
   const float* env_conditional = nullptr;  // env_h rows of env_w + 1 entries
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
-  uint32_t n_light_entries = 0;  // area group (if any) + point lights + environment (if any)
+  uint32_t n_light_entries = 0;  // area group (if any) + point lights + directional lights + environment (if any)
   // two-level scenes: instance records (4 float4: world-to-local rows, (blas root, id, material, 0))
   const float4* insts = nullptr;       // in top-level leaf order (traversal)
   const float4* inst_table = nullptr;  // by instance index (shading)

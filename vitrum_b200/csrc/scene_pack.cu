@@ -122,6 +122,41 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     if (d.flags & ~3u) fail(VT_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has unknown flags");
     m.flags = d.flags;
   }
+  // rectangle lights: two emissive triangles each, one-sided, transparent to shadow rays
+  if (sc->rect_light_count) {
+    if (!sc->rect_lights) fail(VT_ERR_INVALID_ARGUMENT, "rect_lights is null");
+    if (sc->instance_count) fail(VT_ERR_INVALID_ARGUMENT, "rect lights need a single-level scene");
+    for (size_t i = 0; i < sc->rect_light_count; ++i) {
+      const vt_rect_light_desc& r = sc->rect_lights[i];
+      pt::Material m{};
+      m.base_color = make_float3(0.0f, 0.0f, 0.0f);
+      m.roughness = 1.0f;
+      m.emission = make_float3(r.radiance[0], r.radiance[1], r.radiance[2]);
+      m.ior = 1.5f;
+      m.kind = pt::kLambert;
+      m.alpha = 1.0f;
+      m.emissive = (r.radiance[0] > 0.0f || r.radiance[1] > 0.0f || r.radiance[2] > 0.0f) ? 1u : 0u;
+      m.flags = VT_MATERIAL_SINGLE_SIDED | VT_MATERIAL_NO_SHADOW;
+      const uint32_t mi = (uint32_t)mats.size();
+      mats.push_back(m);
+      const uint32_t base = (uint32_t)(pos.size() / 4);
+      for (int c = 0; c < 4; ++c) {
+        const float a = (c == 1 || c == 2) ? 1.0f : 0.0f, b = (c >= 2) ? 1.0f : 0.0f;
+        for (int k = 0; k < 3; ++k) {
+          const float x = r.corner[k] + a * r.edge_u[k] + b * r.edge_v[k];
+          if (!std::isfinite(x)) fail(VT_ERR_RANGE, "rect light " + std::to_string(i) + " is not finite");
+          pos.push_back(x);
+        }
+        pos.push_back(0.0f);
+      }
+      const uint32_t tri[6] = {0, 1, 2, 0, 2, 3};
+      for (int t = 0; t < 2; ++t) {
+        for (int k = 0; k < 3; ++k) idx.push_back(base + tri[3 * t + k]);
+        idx.push_back(0u);
+        tri_mat.push_back(mi);
+      }
+    }
+  }
   const size_t ntri = tri_mat.size();
   // geometry
   BuildOptions bo;
@@ -254,6 +289,24 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     pts.push_back(make_float4(p.position[0], p.position[1], p.position[2], 0.0f));
     pts.push_back(make_float4(p.intensity[0], p.intensity[1], p.intensity[2], 0.0f));
   }
+  // directional lights
+  std::vector<float4> dirs;
+  if (sc->directional_light_count && !sc->directional_lights) fail(VT_ERR_INVALID_ARGUMENT, "directional_lights is null");
+  for (size_t i = 0; i < sc->directional_light_count; ++i) {
+    const vt_directional_light_desc& dl = sc->directional_lights[i];
+    const double dx = dl.direction[0], dy = dl.direction[1], dz = dl.direction[2];
+    const double len = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(len > 0.0) || !std::isfinite(len)) fail(VT_ERR_INVALID_ARGUMENT, "directional light direction is zero");
+    if (!(dl.angular_radius >= 0.0f) || !(dl.angular_radius < 1.5f))
+      fail(VT_ERR_RANGE, "directional light angular_radius must be in [0, 1.5)");
+    const bool delta = dl.angular_radius == 0.0f;
+    const double st = std::sin((double)dl.angular_radius);
+    const double to_l = delta ? 1.0 : 1.0 / (M_PI * st * st);  // disc radiance from its irradiance
+    dirs.push_back(make_float4((float)(-dx / len), (float)(-dy / len), (float)(-dz / len),
+                               delta ? 1.0f : (float)std::cos((double)dl.angular_radius)));
+    dirs.push_back(make_float4((float)(dl.irradiance[0] * to_l), (float)(dl.irradiance[1] * to_l),
+                               (float)(dl.irradiance[2] * to_l), delta ? 1.0f : 0.0f));
+  }
   // environment: equirectangular, importance by luminance * sin(theta)
   std::vector<float4> envt;
   std::vector<float> marg, cond;
@@ -308,6 +361,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   p.cdf = std::move(cdf);
   p.emit_total = total;
   p.points = std::move(pts);
+  p.dirs = std::move(dirs);
   p.env = std::move(envt);
   p.marg = std::move(marg);
   p.cond = std::move(cond);

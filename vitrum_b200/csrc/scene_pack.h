@@ -27,6 +27,7 @@ struct PackedScene {
   std::vector<float> cdf;            // inclusive area CDF
   double emit_total = 0.0;
   std::vector<float4> points;        // 2 float4 per point light
+  std::vector<float4> dirs;          // 2 float4 per directional light
   std::vector<float4> env;
   std::vector<float> marg, cond;
   bool has_env = false, env_sampleable = false;

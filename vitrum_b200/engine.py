@@ -46,13 +46,24 @@ class _InstanceDesc(ctypes.Structure):
     _fields_ = [("mesh", ctypes.c_uint32), ("material", ctypes.c_uint32), ("local_to_world", ctypes.c_float * 16)]
 
 
+class _DirectionalDesc(ctypes.Structure):
+    _fields_ = [("direction", ctypes.c_float * 3), ("irradiance", ctypes.c_float * 3), ("angular_radius", ctypes.c_float)]
+
+
+class _RectDesc(ctypes.Structure):
+    _fields_ = [("corner", ctypes.c_float * 3), ("edge_u", ctypes.c_float * 3), ("edge_v", ctypes.c_float * 3),
+                ("radiance", ctypes.c_float * 3)]
+
+
 class _SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_size_t), ("instances", ctypes.c_void_p),
                 ("instance_count", ctypes.c_size_t), ("materials", ctypes.c_void_p),
                 ("material_count", ctypes.c_size_t), ("point_lights", ctypes.c_void_p),
                 ("point_light_count", ctypes.c_size_t), ("environment_rgb", ctypes.c_void_p),
                 ("environment_width", ctypes.c_int32), ("environment_height", ctypes.c_int32),
-                ("environment_intensity", ctypes.c_float)]
+                ("environment_intensity", ctypes.c_float), ("directional_lights", ctypes.c_void_p),
+                ("directional_light_count", ctypes.c_size_t), ("rect_lights", ctypes.c_void_p),
+                ("rect_light_count", ctypes.c_size_t)]
 
 
 class _FrameInput(ctypes.Structure):
@@ -130,6 +141,24 @@ class PointLight:
 
 
 @dataclass
+class DirectionalLight:
+    """Light travelling along `direction`; angular_radius 0: delta light of that
+    irradiance, else a disc of that angular radius and irradiance."""
+    direction: Sequence[float]
+    irradiance: Sequence[float]
+    angular_radius: float = 0.0
+
+
+@dataclass
+class RectLight:
+    """corner + [0,1] edge_u + [0,1] edge_v emitting `radiance` towards edge_u x edge_v."""
+    corner: Sequence[float]
+    edge_u: Sequence[float]
+    edge_v: Sequence[float]
+    radiance: Sequence[float]
+
+
+@dataclass
 class Environment:
     rgb: np.ndarray        # (H, W, 3) float32 equirectangular, row 0 at +y
     intensity: float = 1.0
@@ -142,6 +171,8 @@ class Scene:
     instances: List[Instance] = field(default_factory=list)
     point_lights: List[PointLight] = field(default_factory=list)
     environment: Optional[Environment] = None
+    directional_lights: List[DirectionalLight] = field(default_factory=list)
+    rect_lights: List[RectLight] = field(default_factory=list)
 
     @property
     def triangle_count(self) -> int:
@@ -165,7 +196,7 @@ class Scene:
             p = np.asarray(m.positions, np.float64).reshape(-1, 3) @ M[:3, :3].T + M[:3, 3]
             out.append(Mesh(p.astype(np.float32), np.asarray(m.indices, np.uint32).reshape(-1, 3), inst.material))
         return Scene(meshes=out, materials=self.materials, point_lights=self.point_lights,
-                     environment=self.environment)
+                     environment=self.environment, directional_lights=self.directional_lights)
 
 
 @dataclass
@@ -226,12 +257,21 @@ def _marshal_scene(scene: "Scene"):
     for i, inst in enumerate(scene.instances):
         M = np.asarray(inst.local_to_world, np.float32).reshape(4, 4)
         insts[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
+    dls = (_DirectionalDesc * max(1, len(scene.directional_lights)))()
+    for i, l in enumerate(scene.directional_lights):
+        dls[i] = _DirectionalDesc((ctypes.c_float * 3)(*l.direction), (ctypes.c_float * 3)(*l.irradiance),
+                                  l.angular_radius)
+    rls = (_RectDesc * max(1, len(scene.rect_lights)))()
+    for i, r in enumerate(scene.rect_lights):
+        rls[i] = _RectDesc((ctypes.c_float * 3)(*r.corner), (ctypes.c_float * 3)(*r.edge_u),
+                           (ctypes.c_float * 3)(*r.edge_v), (ctypes.c_float * 3)(*r.radiance))
     desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes),
                       ctypes.cast(insts, ctypes.c_void_p) if scene.instances else None, len(scene.instances),
                       ctypes.cast(mats, ctypes.c_void_p),
                       len(scene.materials), ctypes.cast(pls, ctypes.c_void_p), len(scene.point_lights), env_ptr,
-                      ew, eh, ei)
-    return desc, (keep, meshes, insts, mats, pls)
+                      ew, eh, ei, ctypes.cast(dls, ctypes.c_void_p), len(scene.directional_lights),
+                      ctypes.cast(rls, ctypes.c_void_p), len(scene.rect_lights))
+    return desc, (keep, meshes, insts, mats, pls, dls, rls)
 
 
 # ---------------------------------------------------------------- engine
