@@ -201,6 +201,16 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       gimask = imask;
       if (TWO && cur_inst < 0 && th) {
         // top level: the leaf records are instances, entered through the stack
+        // before this node's internal children (which wait below them)
+        if (ghits) {
+          if (sp < STK) {
+            stack[sp * kBlock] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
+            ++sp;
+          } else {
+            atomicOr(status, 1);
+          }
+          ghits = 0;
+        }
         if (sp < STK) {
           stack[sp * kBlock] = make_uint2(w1.y | kInstGroup, th);
           ++sp;
