@@ -413,6 +413,9 @@ typedef struct vt_nrc_render_options {
   int32_t train_paths;      /* training paths per frame (0: train_steps * train_batch / 2) */
   int32_t warmup_frames;    /* plain frames while the cache warms up */
   vt_nrc_config cache;      /* aabb is replaced by the scene's bounds */
+  float fallback_error;     /* > 0: screen tiles whose cache error estimate (EMA of the relative
+                               luminance bias at the query vertex) exceeds this keep path tracing */
+  int32_t fallback_tile;    /* tile edge in pixels (0: 16) */
 } vt_nrc_render_options;
 
 vt_status vt_set_nrc(vt_engine* engine, const vt_nrc_render_options* options);

@@ -95,3 +95,23 @@ def test_trained_cache_lowers_equal_time_error(cuda):
     print(f"equal time ({t_nrc:.2f} ms): NRC 4 x 16 spp relMSE {e_nrc:.4f} vs plain {spp} spp {e_plain:.4f} "
           f"({e_plain / e_nrc:.2f}x)")
     assert e_nrc < 0.5 * e_plain
+
+
+def test_error_fallback_tiles_keep_path_tracing(cuda):
+    """With a threshold below every tile's cache error estimate the render paths
+    never end in the cache: the frame is plain path tracing, sample for sample."""
+    sc, cam = scenes.box_room(wall_cells=8, box_cells=4)
+    W = H = 32
+    plain = Engine(max_bounces=5)
+    plain.set_scene(sc)
+    plain.render_frame(cam, W, H, samples=8, frame_seed=21)
+    want = plain.capture_frame()
+    plain.dispose()
+    for thr, same in ((1e-9, True), (1e9, False)):
+        e = Engine(max_bounces=5)
+        e.set_scene(sc)
+        e.set_nrc(prefix_bounces=1, fallback_error=thr, cache=NrcConfig(levels=8, log2_table_size=12), **SMALL)
+        e.render_frame(cam, W, H, samples=8, frame_seed=21)
+        got = e.capture_frame()
+        assert np.array_equal(got, want) == same, thr
+        e.dispose()

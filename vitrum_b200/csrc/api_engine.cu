@@ -35,6 +35,8 @@ struct NrcEngine {
   std::unique_ptr<vt::nrc::Cache> cache;
   vt::DeviceBuffer<float4> records, queries, samples;
   vt::DeviceBuffer<uint32_t> seed;
+  vt::DeviceBuffer<float> tile_stats, tile_error;  // fallback: per screen tile (sums; error EMA)
+  uint32_t tiles_x = 0, tiles_y = 0, tile_width = 0;
   uint32_t train_paths = 0;
   int frames = 0;  // frames rendered since the cache was created
 };
@@ -84,6 +86,7 @@ struct vt_engine {
   DeviceBuffer<int4> hits;
   DeviceBuffer<uint32_t> order, keys, counters;
   DeviceBuffer<float4> shadow_rays, shadow_contrib, radiance;
+  DeviceBuffer<uint32_t> path_pixel;  // training paths: their pixel
   DeviceBuffer<uint8_t> occluded;
   DeviceBuffer<unsigned long long> trace_counter, totals;
   DeviceBuffer<int> trace_status;
@@ -211,6 +214,7 @@ void ensure_capacity(vt_engine* e, uint32_t cap) {
   e->shadow_contrib.resize(cap);
   e->occluded.resize(cap);
   e->radiance.resize(cap);
+  e->path_pixel.resize(cap);
   e->capacity = cap;
 }
 
@@ -231,6 +235,7 @@ vt::pt::WaveBuffers wave_buffers(vt_engine* e) {
   w.counters = e->counters.ptr;
   w.trace_counter = e->trace_counter.ptr;
   w.trace_status = e->trace_status.ptr;
+  w.path_pixel = e->path_pixel.ptr;
   if (e->nrc) {
     w.nrc_records = e->nrc->records.ptr;
     w.nrc_queries = e->nrc->queries.ptr;
@@ -298,6 +303,23 @@ void nrc_rebuild(vt_engine* e) {
 
 void ensure_nrc_buffers(vt_engine* e, uint32_t render_paths) {
   NrcEngine& n = *e->nrc;
+  if (n.opts.fallback_error > 0.0f) {
+    const uint32_t t = n.opts.fallback_tile > 0 ? (uint32_t)n.opts.fallback_tile : 16u;
+    const uint32_t tx = ((uint32_t)e->width + t - 1) / t, ty = ((uint32_t)e->height + t - 1) / t;
+    if (tx != n.tiles_x || ty != n.tiles_y || n.tile_width != (uint32_t)e->width) {
+      e->drop_graphs();
+      n.tiles_x = tx;
+      n.tiles_y = ty;
+      n.tile_width = (uint32_t)e->width;
+      n.tile_stats.resize(3 * (size_t)tx * ty);
+      n.tile_error.resize((size_t)tx * ty);
+      VT_CUDA(cudaMemset(n.tile_stats.ptr, 0, n.tile_stats.bytes()));
+      VT_CUDA(cudaMemset(n.tile_error.ptr, 0, n.tile_error.bytes()));  // no evidence yet: use the cache
+    }
+    n.cache->set_error_tiles(n.tile_stats.ptr, n.tile_width, t, tx);
+  } else {
+    n.cache->set_error_tiles(nullptr, 0, 16, 0);
+  }
   const size_t rec = (size_t)n.train_paths * (size_t)e->opts.max_bounces * 6;
   const size_t smp = (size_t)n.opts.train_steps * (size_t)n.opts.train_batch * 5;
   const size_t qry = (size_t)std::max(render_paths, e->capacity) * 5;
@@ -335,7 +357,14 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     f.record_bounces = bounces;
     VT_CUDA(cudaMemsetAsync(e->nrc->records.ptr, 0, e->nrc->records.bytes(), s));
   } else if (mode == kNrcRender) {
-    f.nrc_prefix = bounces - 1;
+    const NrcEngine& n = *e->nrc;
+    f.nrc_prefix = (uint32_t)std::min<int>(n.opts.prefix_bounces, (int)bounces - 1);
+    if (n.opts.fallback_error > 0.0f && n.tile_error.ptr) {
+      f.nrc_tile_error = n.tile_error.ptr;
+      f.nrc_fallback = n.opts.fallback_error;
+      f.nrc_tile = n.opts.fallback_tile > 0 ? (uint32_t)n.opts.fallback_tile : 16u;
+      f.nrc_tiles_x = n.tiles_x;
+    }
   }
   VT_CUDA(cudaMemsetAsync(e->counters.ptr + vt::pt::kCntQuery, 0, 2 * sizeof(uint32_t), s));
   const vt::pt::WaveBuffers w = wave_buffers(e);
@@ -391,7 +420,8 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     B(StageTimer::kNrcTrain);
     const NrcEngine& n = *e->nrc;
     vt::pt::launch_nrc_targets(w, f.paths, bounces, n.samples.ptr,
-                               (uint32_t)(n.opts.train_steps * n.opts.train_batch), s);
+                               (uint32_t)(n.opts.train_steps * n.opts.train_batch), (uint32_t)n.opts.prefix_bounces,
+                               s);
     E();
     return;
   }
@@ -434,6 +464,8 @@ void nrc_train(vt_engine* e, uint32_t bounces, StageTimer* tm) {
   const size_t stride = 5 * (size_t)n.opts.train_batch;
   for (int k = 0; k < n.opts.train_steps; ++k)
     n.cache->train_step(n.samples.ptr + stride * k, (uint32_t)n.opts.train_batch, s);
+  if (n.opts.fallback_error > 0.0f && n.tile_error.ptr)
+    vt::pt::launch_nrc_tile_update(n.tile_stats.ptr, n.tile_error.ptr, n.tiles_x * n.tiles_y, 0.25f, s);
   if (tm) tm->end(s);
 }
 
@@ -504,7 +536,9 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     ensure_nrc_buffers(e, wh * spp_wave);
     if (n.frames >= n.opts.warmup_frames) {
       mode = kNrcRender;
-      wave_bounces = std::min<uint32_t>(bounces, (uint32_t)n.opts.prefix_bounces + 1u);
+      // with the fallback, paths of high-error tiles continue past the query vertex
+      wave_bounces = n.opts.fallback_error > 0.0f ? bounces
+                                                  : std::min<uint32_t>(bounces, (uint32_t)n.opts.prefix_bounces + 1u);
     }
   }
   if (stage_ms) {
@@ -781,6 +815,8 @@ vt_status vt_set_nrc(vt_engine* e, const vt_nrc_render_options* o) {
     if (o->train_batch < 128 || o->train_batch > (1 << 20) || o->train_batch % 128)
       fail(VT_ERR_RANGE, "train_batch must be a multiple of 128 in [128, 2^20]");
     if (o->train_paths < 0 || o->warmup_frames < 0) fail(VT_ERR_RANGE, "train_paths and warmup_frames must be >= 0");
+    if (!(o->fallback_error >= 0.0f) || o->fallback_tile < 0 || o->fallback_tile > 4096)
+      fail(VT_ERR_RANGE, "fallback_error must be >= 0 and fallback_tile in [0, 4096]");
     auto n = std::make_unique<NrcEngine>();
     n->opts = *o;
     n->train_paths = o->train_paths > 0 ? (uint32_t)o->train_paths

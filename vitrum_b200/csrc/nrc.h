@@ -60,6 +60,12 @@ struct View {
   float aabb_inv[3] = {1, 1, 1};     // 1 / extent (0 for a flat axis)
   int* error = nullptr;              // non-zero: a bounded wait expired (kernel returned early)
   float* loss = nullptr;             // sum of per-sample losses of a training step
+  // error estimate per screen tile: samples whose target.w holds (pixel + 1) add
+  // (prediction luminance, target luminance, 1) to tile_stats[3 * tile]
+  float* tile_stats = nullptr;
+  uint32_t tile_width = 0;           // image width in pixels
+  uint32_t tile_size = 16;           // tile edge in pixels
+  uint32_t tiles_x = 0;
 };
 
 // Features of one cache query / training sample: 4 float4

@@ -89,6 +89,10 @@ View Cache::view() const {
   }
   v.error = diag_.ptr;
   v.loss = loss_.ptr;
+  v.tile_stats = tile_stats_;
+  v.tile_width = tile_width_;
+  v.tile_size = tile_size_;
+  v.tiles_x = tiles_x_;
   return v;
 }
 

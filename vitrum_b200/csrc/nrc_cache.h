@@ -34,6 +34,13 @@ class Cache {
   void get_params(float* weights, float* table) const;  // host arrays
   void set_params(const float* weights, const float* table);
   void set_aabb(const float* mn, const float* mx);
+  // Screen-tile error statistics gathered by later training steps (nullptr: none).
+  void set_error_tiles(float* stats, uint32_t width, uint32_t tile, uint32_t tiles_x) {
+    tile_stats_ = stats;
+    tile_width_ = width;
+    tile_size_ = tile;
+    tiles_x_ = tiles_x;
+  }
   void clear_gradients(cudaStream_t s);
 
   const Config& config() const { return cfg_; }
@@ -55,6 +62,8 @@ class Cache {
   DeviceBuffer<__half2> t16_;
   DeviceBuffer<int> diag_;    // [0] wait expired, [1] non-finite optimiser events
   DeviceBuffer<float> loss_;
+  float* tile_stats_ = nullptr;
+  uint32_t tile_width_ = 0, tile_size_ = 16, tiles_x_ = 0;
 };
 
 }  // namespace nrc

@@ -413,6 +413,16 @@ __global__ void __launch_bounds__(128, 1)
         }
       }
     }
+    if (valid && v.tile_stats && __float_as_uint(tgt.w) != 0u && isfinite(pr[0]) && isfinite(pr[1]) &&
+        isfinite(pr[2])) {
+      // cache error estimate of the sample's screen tile (prediction vs target luminance)
+      const uint32_t pix = __float_as_uint(tgt.w) - 1u;
+      const uint32_t tile = (pix / v.tile_width / v.tile_size) * v.tiles_x + (pix % v.tile_width) / v.tile_size;
+      float* ts = v.tile_stats + 3 * (size_t)tile;
+      atomicAdd(ts, 0.2126f * fmaxf(pr[0], 0.0f) + 0.7152f * fmaxf(pr[1], 0.0f) + 0.0722f * fmaxf(pr[2], 0.0f));
+      atomicAdd(ts + 1, 0.2126f * tgt.x + 0.7152f * tgt.y + 0.0722f * tgt.z);
+      atomicAdd(ts + 2, 1.0f);
+    }
 #pragma unroll
     for (int k = 0; k < 32; ++k) p[k] = 0u;
     p[0] = pack_h2(g[0], g[1]);

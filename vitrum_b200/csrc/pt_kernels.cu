@@ -219,6 +219,7 @@ __global__ void k_raygen(FrameView f, WaveBuffers w) {
   w.rays[0][2 * i] = make_float4(o.x, o.y, o.z, 0.0f);
   w.rays[0][2 * i + 1] = make_float4(d.x, d.y, d.z, CUDART_INF_F);
   w.state[0][i] = make_uint4(i, rng, 1u /* previous event delta: camera */, 0u);
+  if (f.train && w.path_pixel) w.path_pixel[i] = pix;
   w.through[0][i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
   w.radiance[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
@@ -372,6 +373,12 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
         onb(n, tb, bb);
         const float3 wol = to_local(wo, tb, bb, n);
         query = bounce == f.nrc_prefix;
+        if (query && f.nrc_tile_error) {
+          // tiles whose cache error estimate is above the threshold keep path tracing
+          const uint32_t pix = path % (f.width * f.height);
+          const uint32_t tile = (pix / f.width / f.nrc_tile) * f.nrc_tiles_x + (pix % f.width) / f.nrc_tile;
+          if (f.nrc_tile_error[tile] > f.nrc_fallback) query = false;
+        }
         if (f.train || query) nrc_features(m, P, wo, n, qf);
         if (f.train) {
           // training record: features, radiance gathered so far (incl. this
@@ -569,7 +576,8 @@ __global__ void k_count_rays(WaveBuffers w, int cur, unsigned long long* totals)
   totals[1] += w.counters[kCntShadow];
 }
 
-__global__ void k_nrc_targets(WaveBuffers w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity) {
+__global__ void k_nrc_targets(WaveBuffers w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity,
+                              uint32_t query_bounce) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t total = paths * bounces;
   if (blockIdx.x == 0 && threadIdx.x == 0) *w.nrc_seed += 1u;  // next training wave draws new paths
@@ -589,6 +597,7 @@ __global__ void k_nrc_targets(WaveBuffers w, uint32_t paths, uint32_t bounces, f
           return fminf(1024.0f, fmaxf(0.0f, v));
         };
         tg = make_float4(tgt(L.x, A.x, T.x), tgt(L.y, A.y, T.y), tgt(L.z, A.z, T.z), 0.0f);
+        if (w.path_pixel && sl % bounces == query_bounce) tg.w = __uint_as_float(w.path_pixel[sl / bounces] + 1u);
         keep = isfinite(tg.x) && isfinite(tg.y) && isfinite(tg.z);
       }
     }
@@ -686,6 +695,17 @@ __global__ void k_accumulate_batch(WaveBuffers w, float4* accum) {
 
 __global__ void k_advance_batch(WaveBuffers w) { *w.batch_cursor += w.counters[kCntBatchPaths]; }
 
+__global__ void k_nrc_tile_update(float* stats, float* err, uint32_t tiles, float alpha) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += gridDim.x * blockDim.x) {
+    float* s = stats + 3 * (size_t)t;
+    if (s[2] > 0.0f) {
+      const float e = fabsf(s[0] - s[1]) / (s[1] + 1e-3f * s[2]);
+      err[t] = isfinite(e) ? (1.0f - alpha) * err[t] + alpha * e : err[t];
+    }
+    s[0] = s[1] = s[2] = 0.0f;
+  }
+}
+
 unsigned grid_for(uint32_t n, unsigned block) {
   unsigned g = (unsigned)((n + block - 1) / block);
   return g ? g : 1;
@@ -723,10 +743,10 @@ void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t
 }
 
 void launch_nrc_targets(const WaveBuffers& w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity,
-                        cudaStream_t s) {
+                        uint32_t query_bounce, cudaStream_t s) {
   const uint32_t total = paths * bounces;
   const unsigned g = grid_for(total, 256) < 148 * 8 ? grid_for(total, 256) : 148 * 8;
-  k_nrc_targets<<<g, 256, 0, s>>>(w, paths, bounces, samples, capacity);
+  k_nrc_targets<<<g, 256, 0, s>>>(w, paths, bounces, samples, capacity, query_bounce);
   const unsigned gf = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
   k_nrc_fill<<<gf, 256, 0, s>>>(w, samples, capacity);
 }
@@ -739,6 +759,10 @@ void launch_accumulate_batch(const WaveBuffers& w, float4* accum, uint32_t capac
   const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
   k_accumulate_batch<<<g, 256, 0, s>>>(w, accum);
   k_advance_batch<<<1, 1, 0, s>>>(w);
+}
+
+void launch_nrc_tile_update(float* tile_stats, float* tile_error, uint32_t tiles, float alpha, cudaStream_t s) {
+  k_nrc_tile_update<<<grid_for(tiles, 256), 256, 0, s>>>(tile_stats, tile_error, tiles, alpha);
 }
 
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s) {

@@ -68,6 +68,9 @@ struct FrameView {
   uint32_t train = 0;                  // training wave: random pixels, one record per vertex, no accumulation
   uint32_t record_bounces = 0;         // record slots per training path
   uint32_t nrc_prefix = 0xFFFFFFFFu;   // render waves: hits of this bounce become cache queries
+  const float* nrc_tile_error = nullptr;  // per screen tile: cache error estimate (render waves)
+  float nrc_fallback = 0.0f;           // tiles above this error continue as plain path tracing
+  uint32_t nrc_tile = 16, nrc_tiles_x = 0;
   // batch: paths of many scenes in one wave (scene id in bits 8-15 of the path flags)
   const BatchScene* batch = nullptr;
   uint32_t n_scenes = 0;
@@ -132,7 +135,10 @@ void launch_count_rays(const WaveBuffers& w, int cur, unsigned long long* totals
 // appended to `samples` (5 float4 each) up to `capacity`, then the remaining
 // slots are filled cyclically from the collected ones.
 void launch_nrc_targets(const WaveBuffers& w, uint32_t paths, uint32_t bounces, float4* samples, uint32_t capacity,
-                        cudaStream_t s);
+                        uint32_t query_bounce, cudaStream_t s);
+// Error map update after a frame's training: err = EMA of |sum pred - sum target| / (sum target + 1e-3)
+// over the tile's query-vertex samples; clears the sums.
+void launch_nrc_tile_update(float* tile_stats, float* tile_error, uint32_t tiles, float alpha, cudaStream_t s);
 
 }  // namespace pt
 }  // namespace vt
