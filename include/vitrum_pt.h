@@ -407,7 +407,9 @@ vt_status vt_nrc_train_device(vt_nrc* nrc, const float* d_samples, size_t n, voi
  * `warmup_frames` frames the render waves are plain path tracing. */
 typedef struct vt_nrc_render_options {
   int32_t enabled;          /* 0: plain path tracing */
-  int32_t prefix_bounces;   /* bounces before the query (>= 1; 1 queries the second vertex) */
+  int32_t prefix_bounces;   /* bounces before the query (1 queries the second vertex); 0: spread
+                               termination (spreadTermination.ts): query at the first vertex k >= 2
+                               whose accumulated spread a(x_k) exceeds spread_c * a0 */
   int32_t train_steps;      /* optimiser steps per frame (4) */
   int32_t train_batch;      /* samples per step (65536) */
   int32_t train_paths;      /* training paths per frame (0: train_steps * train_batch / 2) */
@@ -416,6 +418,7 @@ typedef struct vt_nrc_render_options {
   float fallback_error;     /* > 0: screen tiles whose cache error estimate (EMA of the relative
                                luminance bias at the query vertex) exceeds this keep path tracing */
   int32_t fallback_tile;    /* tile edge in pixels (0: 16) */
+  float spread_c;           /* spread termination constant (0: 0.01, the paper's c) */
 } vt_nrc_render_options;
 
 vt_status vt_set_nrc(vt_engine* engine, const vt_nrc_render_options* options);

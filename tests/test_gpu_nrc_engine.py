@@ -46,7 +46,8 @@ def test_nrc_options_validation(cuda):
     sc, cam = cloud()
     e = Engine(max_bounces=4)
     e.set_scene(sc)
-    for bad in (dict(prefix_bounces=0), dict(prefix_bounces=4), dict(train_batch=100), dict(train_steps=-1)):
+    for bad in (dict(prefix_bounces=-1), dict(prefix_bounces=4), dict(train_batch=100), dict(train_steps=-1),
+                dict(spread_c=-1.0), dict(fallback_error=-1.0)):
         kw = dict(SMALL)
         kw.update(bad)
         with pytest.raises(N.VtError):
@@ -115,3 +116,33 @@ def test_error_fallback_tiles_keep_path_tracing(cuda):
         got = e.capture_frame()
         assert np.array_equal(got, want) == same, thr
         e.dispose()
+
+
+def test_spread_termination(cuda):
+    """prefix_bounces 0: paths end in the cache where their accumulated spread
+    exceeds c * a0 (spreadTermination.ts).  A huge c never triggers (the frame is
+    plain path tracing, sample for sample); the default c queries the cache and
+    keeps the image close to the oracle."""
+    sc, cam = scenes.box_room(wall_cells=8, box_cells=4)
+    W = H = 32
+    plain = Engine(max_bounces=5)
+    plain.set_scene(sc)
+    plain.render_frame(cam, W, H, samples=8, frame_seed=31)
+    want = plain.capture_frame()
+    plain.dispose()
+    e = Engine(max_bounces=5)
+    e.set_scene(sc)
+    e.set_nrc(prefix_bounces=0, spread_c=1e30, cache=NrcConfig(levels=8, log2_table_size=12), **SMALL)
+    e.render_frame(cam, W, H, samples=8, frame_seed=31)
+    assert np.array_equal(e.capture_frame(), want)
+    e.dispose()
+    e = Engine(max_bounces=5)
+    e.set_scene(sc)
+    e.set_nrc(prefix_bounces=0, cache=NrcConfig(levels=8, log2_table_size=12), **SMALL)
+    for _ in range(24):
+        e.render_frame(cam, W, H, samples=8, frame_seed=31)
+    st = e.profile_frame(cam, W, H, samples=8, frame_seed=31)
+    img = e.capture_frame()[..., :3]
+    assert st["nrc_query_ms"] > 0 and np.isfinite(img).all()
+    assert abs(img.mean() / want[..., :3].mean() - 1) < 0.1
+    e.dispose()

@@ -358,7 +358,11 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     VT_CUDA(cudaMemsetAsync(e->nrc->records.ptr, 0, e->nrc->records.bytes(), s));
   } else if (mode == kNrcRender) {
     const NrcEngine& n = *e->nrc;
-    f.nrc_prefix = (uint32_t)std::min<int>(n.opts.prefix_bounces, (int)bounces - 1);
+    if (n.opts.prefix_bounces == 0) {
+      f.nrc_spread_c = n.opts.spread_c > 0.0f ? n.opts.spread_c : 0.01f;
+    } else {
+      f.nrc_prefix = (uint32_t)std::min<int>(n.opts.prefix_bounces, (int)bounces - 1);
+    }
     if (n.opts.fallback_error > 0.0f && n.tile_error.ptr) {
       f.nrc_tile_error = n.tile_error.ptr;
       f.nrc_fallback = n.opts.fallback_error;
@@ -420,8 +424,8 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     B(StageTimer::kNrcTrain);
     const NrcEngine& n = *e->nrc;
     vt::pt::launch_nrc_targets(w, f.paths, bounces, n.samples.ptr,
-                               (uint32_t)(n.opts.train_steps * n.opts.train_batch), (uint32_t)n.opts.prefix_bounces,
-                               s);
+                               (uint32_t)(n.opts.train_steps * n.opts.train_batch),
+                               (uint32_t)std::max(1, n.opts.prefix_bounces), s);
     E();
     return;
   }
@@ -537,8 +541,9 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     if (n.frames >= n.opts.warmup_frames) {
       mode = kNrcRender;
       // with the fallback, paths of high-error tiles continue past the query vertex
-      wave_bounces = n.opts.fallback_error > 0.0f ? bounces
-                                                  : std::min<uint32_t>(bounces, (uint32_t)n.opts.prefix_bounces + 1u);
+      wave_bounces = (n.opts.fallback_error > 0.0f || n.opts.prefix_bounces == 0)
+                         ? bounces
+                         : std::min<uint32_t>(bounces, (uint32_t)n.opts.prefix_bounces + 1u);
     }
   }
   if (stage_ms) {
@@ -809,8 +814,9 @@ vt_status vt_set_nrc(vt_engine* e, const vt_nrc_render_options* o) {
       e->nrc.reset();
       return;
     }
-    if (o->prefix_bounces < 1 || o->prefix_bounces >= e->opts.max_bounces)
-      fail(VT_ERR_RANGE, "prefix_bounces must be in [1, max_bounces - 1]");
+    if (o->prefix_bounces < 0 || o->prefix_bounces >= e->opts.max_bounces)
+      fail(VT_ERR_RANGE, "prefix_bounces must be in [0, max_bounces - 1]");
+    if (!(o->spread_c >= 0.0f)) fail(VT_ERR_RANGE, "spread_c must be >= 0");
     if (o->train_steps < 0 || o->train_steps > 64) fail(VT_ERR_RANGE, "train_steps must be in [0, 64]");
     if (o->train_batch < 128 || o->train_batch > (1 << 20) || o->train_batch % 128)
       fail(VT_ERR_RANGE, "train_batch must be a multiple of 128 in [128, 2^20]");

@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
     uint4 next_state;
     float3 T = f3(0.0f, 0.0f, 0.0f);
     uint32_t root_of_path = 0;
+    float spread = 0.0f;  // running sum of spread terms (spread termination)
     if (valid) {
       const uint32_t p = f.sort_by_material ? w.order[i] : i;
       const float4 r0 = w.rays[cur][2 * p], r1 = w.rays[cur][2 * p + 1];
@@ -372,7 +373,24 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
         float3 tb, bb;
         onb(n, tb, bb);
         const float3 wol = to_local(wo, tb, bb, n);
-        query = bounce == f.nrc_prefix;
+        if (f.nrc_spread_c > 0.0f) {
+          // a0 = t^2 / (4 pi |cos|) at the primary vertex (kept as sqrt in radiance.w); later
+          // vertices add sqrt(t^2 / (p |cos|)) of the segment that reached them (delta segments add 0)
+          const float ac = fabsf(dn) + 1e-7f;
+          spread = tp.w;
+          if (bounce == 0) {
+            const float a0 = sqrtf(t * t / (4.0f * CUDART_PI_F * ac));
+            float4 r = w.radiance[path];
+            r.w = a0;
+            w.radiance[path] = r;
+          } else {
+            if (!prev_delta) spread += prev_pdf > 0.0f ? sqrtf(t * t / (prev_pdf * ac)) : 3.0e19f;
+            const float a0 = w.radiance[path].w;
+            query = spread * spread > f.nrc_spread_c * a0 * a0;
+          }
+        } else {
+          query = bounce == f.nrc_prefix;
+        }
         if (query && f.nrc_tile_error) {
           // tiles whose cache error estimate is above the threshold keep path tracing
           const uint32_t pix = path % (f.width * f.height);
@@ -485,7 +503,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
       next_state.z |= sid << 8;
       if (maxc(rad) > 0.0f) {
         float4 acc = w.radiance[path];
-        w.radiance[path] = make_float4(acc.x + rad.x, acc.y + rad.y, acc.z + rad.z, 0.0f);
+        w.radiance[path] = make_float4(acc.x + rad.x, acc.y + rad.y, acc.z + rad.z, acc.w);
       }
     }
     // ---- warp-ballot compaction of survivors and shadow rays
@@ -499,7 +517,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
         w.rays[nxt][2 * q] = next_o;
         w.rays[nxt][2 * q + 1] = next_d;
         w.state[nxt][q] = next_state;
-        w.through[nxt][q] = make_float4(T.x, T.y, T.z, 0.0f);
+        w.through[nxt][q] = make_float4(T.x, T.y, T.z, spread);
         if (w.ray_root[nxt]) w.ray_root[nxt][q] = root_of_path;
       }
     }
@@ -540,7 +558,7 @@ __global__ void k_shadow_resolve(WaveBuffers w) {
     const float4 c = w.shadow_contrib[i];
     const uint32_t path = __float_as_uint(c.w);
     float4 acc = w.radiance[path];
-    w.radiance[path] = make_float4(acc.x + c.x, acc.y + c.y, acc.z + c.z, 0.0f);
+    w.radiance[path] = make_float4(acc.x + c.x, acc.y + c.y, acc.z + c.z, acc.w);
   }
 }
 

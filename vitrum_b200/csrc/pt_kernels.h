@@ -71,6 +71,8 @@ struct FrameView {
   const float* nrc_tile_error = nullptr;  // per screen tile: cache error estimate (render waves)
   float nrc_fallback = 0.0f;           // tiles above this error continue as plain path tracing
   uint32_t nrc_tile = 16, nrc_tiles_x = 0;
+  float nrc_spread_c = 0.0f;           // > 0: spread termination (nrc_prefix unused): query at the first
+                                       // vertex k >= 2 with a(x_k) > c * a0 (spreadTermination.ts:70-184)
   // batch: paths of many scenes in one wave (scene id in bits 8-15 of the path flags)
   const BatchScene* batch = nullptr;
   uint32_t n_scenes = 0;

@@ -89,7 +89,8 @@ class _NrcRenderOptions(ctypes.Structure):
     from .nrc import _Config as _NrcConfig
     _fields_ = [("enabled", ctypes.c_int32), ("prefix_bounces", ctypes.c_int32), ("train_steps", ctypes.c_int32),
                 ("train_batch", ctypes.c_int32), ("train_paths", ctypes.c_int32), ("warmup_frames", ctypes.c_int32),
-                ("cache", _NrcConfig), ("fallback_error", ctypes.c_float), ("fallback_tile", ctypes.c_int32)]
+                ("cache", _NrcConfig), ("fallback_error", ctypes.c_float), ("fallback_tile", ctypes.c_int32),
+                ("spread_c", ctypes.c_float)]
 
 
 class _EngineStats(ctypes.Structure):
@@ -366,15 +367,16 @@ class Engine:
 
     def set_nrc(self, enabled: bool = True, prefix_bounces: int = 1, train_steps: int = 4, train_batch: int = 65536,
                 train_paths: int = 0, warmup_frames: int = 0, cache=None, fallback_error: float = 0.0,
-                fallback_tile: int = 16) -> None:
+                fallback_tile: int = 16, spread_c: float = 0.0) -> None:
         """Path tracing with the neural radiance cache (vt_set_nrc): each frame
         trains the cache on its own training paths, then ends the render paths
-        in a cache query after `prefix_bounces` bounces.  fallback_error > 0:
+        in a cache query after `prefix_bounces` bounces (0: at the first vertex
+        whose path spread exceeds spread_c * a0, default c 0.01).  fallback_error > 0:
         screen tiles whose cache error estimate exceeds it keep path tracing."""
         from .nrc import NrcConfig
         cfg = (cache or NrcConfig()).to_c()
         o = _NrcRenderOptions(1 if enabled else 0, prefix_bounces, train_steps, train_batch, train_paths,
-                              warmup_frames, cfg, fallback_error, fallback_tile)
+                              warmup_frames, cfg, fallback_error, fallback_tile, spread_c)
         N.call("vt_set_nrc", self.handle, ctypes.byref(o))
 
     def autotune(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,
