@@ -117,14 +117,28 @@ vt_status vt_bvh_build_device(int32_t device, const float* d_positions, size_t p
     if (!out_bvh) fail(VT_ERR_INVALID_ARGUMENT, "out_bvh is null");
     *out_bvh = nullptr;
     DeviceScope ds(device);
+    if (position_words && !d_positions) fail(VT_ERR_INVALID_ARGUMENT, "positions is null");
+    if (index_words && !d_indices) fail(VT_ERR_INVALID_ARGUMENT, "indices is null");
+    auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t s = (cudaStream_t)cuda_stream;
+    auto b = std::make_unique<vt_bvh>();
+    b->device = device;
+    b->opts = resolve(options);
+    // the binary tree is built on the GPU (binCount <= 16), the wide encoding on the host
+    if (b->opts.bins <= 16) {
+      b->binary = build_binary_gpu(d_positions, position_words, d_indices, index_words, b->opts, s);
+    }
     std::vector<float> p(position_words);
     std::vector<uint32_t> i(index_words);
-    cudaStream_t s = (cudaStream_t)cuda_stream;
     if (position_words)
       VT_CUDA(cudaMemcpyAsync(p.data(), d_positions, position_words * 4, cudaMemcpyDeviceToHost, s));
     if (index_words) VT_CUDA(cudaMemcpyAsync(i.data(), d_indices, index_words * 4, cudaMemcpyDeviceToHost, s));
     VT_CUDA(cudaStreamSynchronize(s));
-    *out_bvh = build_host(device, p.data(), position_words, i.data(), index_words, options);
+    if (b->opts.bins > 16) b->binary = build_binary_host(p.data(), position_words, i.data(), index_words, b->opts);
+    b->ntri = (int64_t)(index_words / b->opts.index_stride);
+    upload(b.get(), p.data(), i.data());
+    b->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    *out_bvh = b.release();
   });
 }
 

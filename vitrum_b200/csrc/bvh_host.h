@@ -1,6 +1,8 @@
 // bvh_host.h -- host-side containers of the BVH build pipeline.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -30,6 +32,9 @@ struct WideBvhHost {
 };
 
 void validate_options(const BuildOptions& o);
+// The same tree built on the GPU from device positions / indices (binCount <= 16).
+BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const uint32_t* d_idx, size_t index_words,
+                               const BuildOptions& o, cudaStream_t s);
 
 // Binned-SAH binary build on host arrays (throws vt::Error).
 BinaryBvhHost build_binary_host(const float* positions, size_t position_words, const uint32_t* indices,
