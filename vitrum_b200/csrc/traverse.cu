@@ -34,6 +34,25 @@ __device__ __forceinline__ float u8f(uint32_t word, uint32_t sel) {
   return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | sel)) - 8388608.0f;
 }
 
+__device__ __forceinline__ uint64_t pack2(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float lo32(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float hi32(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
+// (near, far) t of one axis: bytes `sel` of the near / far words as floats (2^23
+// mantissa trick, packed subtraction), then one packed FMA with (adj, adj) and (on, of)
+__device__ __forceinline__ uint64_t slab2(uint32_t nw, uint32_t fw, uint32_t sel, uint64_t adj2, uint64_t off2) {
+  const uint32_t a = __byte_perm(nw, 0x4B000000u, 0x7540u | sel), b = __byte_perm(fw, 0x4B000000u, 0x7540u | sel);
+  uint64_t q, t;
+  const uint64_t m = 0x4B0000004B000000ull;  // 2^23, 2^23
+  asm("mov.b64 %0, {%1, %2};" : "=l"(q) : "r"(a), "r"(b));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(q) : "l"(q), "l"(m));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(t) : "l"(q), "l"(adj2), "l"(off2));
+  return t;
+}
+
 struct Slab {
   float adj, on, of;  // q scale, near offset, far offset
 };
@@ -181,17 +200,18 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       const uint32_t fy0 = ny ? w2.z : w4.x, fy1 = ny ? w2.w : w4.y;
       const uint32_t nz0 = nz ? w4.z : w3.x, nz1 = nz ? w4.w : w3.y;
       const uint32_t fz0 = nz ? w3.x : w4.z, fz1 = nz ? w3.y : w4.w;
+      const uint64_t ax2 = pack2(sx.adj, sx.adj), ay2 = pack2(sy.adj, sy.adj), az2 = pack2(sz.adj, sz.adj);
+      const uint64_t ox2 = pack2(sx.on, sx.of), oy2 = pack2(sy.on, sy.of), oz2 = pack2(sz.on, sz.of);
       uint32_t hm = 0;  // slot-indexed hit mask
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const uint32_t sel = (uint32_t)(j & 3);
-        const float qnx = u8f(j < 4 ? nx0 : nx1, sel), qfx = u8f(j < 4 ? fx0 : fx1, sel);
-        const float qny = u8f(j < 4 ? ny0 : ny1, sel), qfy = u8f(j < 4 ? fy0 : fy1, sel);
-        const float qnz = u8f(j < 4 ? nz0 : nz1, sel), qfz = u8f(j < 4 ? fz0 : fz1, sel);
-        const float tn = fmaxf(fmaxf(fmaf(qnx, sx.adj, sx.on), fmaf(qny, sy.adj, sy.on)),
-                               fmaxf(fmaf(qnz, sz.adj, sz.on), R.tmin));
-        const float tf = fminf(fminf(fmaf(qfx, sx.adj, sx.of), fmaf(qfy, sy.adj, sy.of)),
-                               fminf(fmaf(qfz, sz.adj, sz.of), R.closest));
+        // near and far plane of one axis as one packed f32x2 conversion and FMA
+        const uint64_t tx = slab2(j < 4 ? nx0 : nx1, j < 4 ? fx0 : fx1, sel, ax2, ox2);
+        const uint64_t ty = slab2(j < 4 ? ny0 : ny1, j < 4 ? fy0 : fy1, sel, ay2, oy2);
+        const uint64_t tz = slab2(j < 4 ? nz0 : nz1, j < 4 ? fz0 : fz1, sel, az2, oz2);
+        const float tn = fmaxf(fmaxf(lo32(tx), lo32(ty)), fmaxf(lo32(tz), R.tmin));
+        const float tf = fminf(fminf(hi32(tx), hi32(ty)), fminf(hi32(tz), R.closest));
         hm |= (tn <= tf) ? (1u << j) : 0u;
       }
       const uint32_t nh = xor_permute8(hm & imask, R.oct);
