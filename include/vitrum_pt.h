@@ -447,6 +447,10 @@ typedef struct vt_tuning {
   int32_t wave_paths;         /* paths per wave */
   int32_t sort_by_material;   /* 1 sort shading work by BSDF family, 0 not */
   int32_t trace_blocks_per_sm;/* persistent traversal CTAs per SM (0: occupancy limit) */
+  int32_t stage_hot_nodes;    /* 1: each traversal CTA first copies the top of the tree (root,
+                                 children, grandchildren) into shared memory with one bulk copy;
+                                 0: every node read goes through L1/L2.  A batch takes 0 only
+                                 (its launches carry one root per ray). */
 } vt_tuning;
 
 vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_batch** out);
@@ -475,6 +479,8 @@ vt_status vt_batch_destroy(vt_batch* batch);
 vt_status vt_engine_autotune(vt_engine* engine, const vt_frame_input* frame, vt_tuning_trial* report,
                              size_t report_capacity, size_t* report_count);
 vt_status vt_engine_get_tuning(const vt_engine* engine, vt_tuning* tuning);
+/* Sets the launch shape directly (e.g. one found by an earlier autotune). */
+vt_status vt_engine_set_tuning(vt_engine* engine, const vt_tuning* tuning);
 
 #ifdef __cplusplus
 }

@@ -65,3 +65,9 @@ def test_batch_validation(cuda):
     inst, icam = scenes.instanced_cloud(n_instances=4, sphere_levels=(1,), torus_segments=(8, 4), cube_cells=(2,))
     with pytest.raises(N.VtError):
         Batch([BatchItem(inst, icam, 16, 16, 1)])
+    b = Batch([BatchItem(sc, cam, 16, 16, 1)])
+    with pytest.raises(N.VtError):  # one root per ray: nothing to stage
+        b.set_tuning(1 << 20, stage_hot_nodes=True)
+    b.set_tuning(1 << 20)
+    assert b.tuning["stage_hot_nodes"] == 0
+    b.close()

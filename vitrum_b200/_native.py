@@ -81,6 +81,7 @@ SIGNATURES = {
     "vt_batch_destroy": [P],
     "vt_engine_autotune": [P, P, P, SZ, P],
     "vt_engine_get_tuning": [P, P],
+    "vt_engine_set_tuning": [P, P],
     "vt_nrc_create": [I32, P, P],
     "vt_nrc_destroy": [P],
     "vt_nrc_query": [P, P, SZ, P],

@@ -24,7 +24,7 @@ using vt::fail;
 struct vt_batch {
   int device = 0;
   vt_engine_options opts{};
-  vt_tuning tuning{1 << 22, 0, 0};
+  vt_tuning tuning{1 << 22, 0, 0, 0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // scenes
@@ -210,7 +210,7 @@ void render(vt_batch* b, vt_batch_stats* st) {
   VT_CUDA(cudaStreamSynchronize(s));
   int status = 0;
   VT_CUDA(cudaMemcpy(&status, b->trace_status.ptr, sizeof status, cudaMemcpyDeviceToHost));
-  if (status) fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+  if (status) fail(VT_ERR_BUILD, vt::trace_status_message(status));
   float ms = 0.0f;
   VT_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
   if (st) {
@@ -226,6 +226,8 @@ void validate_tuning(const vt_tuning& t) {
   if (t.wave_paths < 1024 || t.wave_paths > (1 << 26)) fail(VT_ERR_RANGE, "wave_paths must be in [1024, 2^26]");
   if (t.sort_by_material != 0 && t.sort_by_material != 1) fail(VT_ERR_RANGE, "sort_by_material must be 0 or 1");
   if (t.trace_blocks_per_sm < 0 || t.trace_blocks_per_sm > 16) fail(VT_ERR_RANGE, "trace_blocks_per_sm in [0, 16]");
+  if (t.stage_hot_nodes != 0)
+    fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 for a batch (its launches carry one root node per ray)");
 }
 
 }  // namespace

@@ -78,6 +78,7 @@ static TraceArgs trace_args(vt_bvh* b, const vt_ray* rays, size_t n) {
   a.status = b->status.ptr;
   a.stack_depth = 2 * b->wide_depth + 2;  // one node group and one postponed triangle group per level
   a.counter = b->counter.ptr;
+  a.node_count = b->nodes.count / 5;
   return a;
 }
 
@@ -86,7 +87,7 @@ static void check_status(vt_bvh* b) {
   VT_CUDA(cudaMemcpy(&st, b->status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
   if (st) {
     cudaMemset(b->status.ptr, 0, sizeof(int));
-    fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+    fail(VT_ERR_BUILD, trace_status_message(st));
   }
 }
 

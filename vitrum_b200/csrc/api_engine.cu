@@ -92,6 +92,7 @@ struct vt_engine {
   DeviceBuffer<int> trace_status;
   std::unique_ptr<NrcEngine> nrc;
   int trace_blocks_per_sm = 0;      // traversal CTAs per SM (0: occupancy limit), from the autotuner
+  bool trace_stage_nodes = false;   // traversal CTAs stage the top of the tree in shared memory
   // graph cache: one executable per wave shape and mode
   struct Graph {
     uint32_t spp_wave = 0, bounces = 0;
@@ -391,6 +392,8 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.status = e->trace_status.ptr;
     t.counter = e->trace_counter.ptr;
     t.stack_depth = e->stack_depth;
+    t.node_count = e->nodes.count / 5;
+    t.stage_nodes = e->trace_stage_nodes;
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.n_dev = w.counters + cur;
@@ -581,7 +584,7 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   e->last_ms = ms;
   int st = 0;
   VT_CUDA(cudaMemcpy(&st, e->trace_status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+  if (st) fail(VT_ERR_BUILD, vt::trace_status_message(st));
   e->samples += (int)spp;
   out->kind = 0;
   out->samples_accumulated = e->samples;
@@ -741,6 +744,8 @@ vt_status vt_pick(vt_engine* e, float x, float y, int32_t* out_triangle) {
     t.status = e->pick_status.ptr;
     t.counter = e->pick_counter.ptr;
     t.stack_depth = e->stack_depth;
+    t.node_count = e->nodes.count / 5;
+    t.stage_nodes = e->trace_stage_nodes;
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.inst_table = e->view.inst_table;
@@ -787,6 +792,8 @@ vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits
     t.status = e->q_status.ptr;
     t.counter = e->q_counter.ptr;
     t.stack_depth = e->stack_depth;
+    t.node_count = e->nodes.count / 5;
+    t.stage_nodes = e->trace_stage_nodes;
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.inst_table = e->view.inst_table;
@@ -800,7 +807,7 @@ vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits
     int st = 0;
     VT_CUDA(cudaMemcpyAsync(&st, e->q_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     VT_CUDA(cudaStreamSynchronize(e->stream));
-    if (st) fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+    if (st) fail(VT_ERR_BUILD, vt::trace_status_message(st));
   });
 }
 
@@ -849,6 +856,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       e->opts.wave_paths = t.wave_paths;
       e->opts.sort_by_material = t.sort_by_material ? 1 : 0;
       e->trace_blocks_per_sm = t.trace_blocks_per_sm;
+      e->trace_stage_nodes = t.stage_hot_nodes != 0;
       e->drop_graphs();
     };
     auto time_it = [&](const vt_tuning& t) {
@@ -864,7 +872,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       return best;
     };
     vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 22), e->opts.sort_by_material > 0 ? 1 : 0,
-                   e->trace_blocks_per_sm};
+                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0};
     double best_ms = time_it(best);
     for (int wp : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
       if (wp == best.wave_paths) continue;
@@ -886,6 +894,12 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       const double ms = time_it(t);
       if (ms < best_ms) { best_ms = ms; best = t; }
     }
+    {
+      vt_tuning t = best;
+      t.stage_hot_nodes = best.stage_hot_nodes ? 0 : 1;
+      const double ms = time_it(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
     apply(best);
     reset_accumulation(e);
     if (count) *count = trials.size();
@@ -900,6 +914,25 @@ vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
     t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 22);
     t->sort_by_material = e->opts.sort_by_material > 0 ? 1 : 0;
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
+    t->stage_hot_nodes = e->trace_stage_nodes ? 1 : 0;
+  });
+}
+
+vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
+  return vt::guard([&] {
+    if (!e || !t) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->wave_paths < 1024 || t->wave_paths > (1 << 26)) fail(VT_ERR_RANGE, "wave_paths must be in [1024, 2^26]");
+    if (t->sort_by_material != 0 && t->sort_by_material != 1) fail(VT_ERR_RANGE, "sort_by_material must be 0 or 1");
+    if (t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 16)
+      fail(VT_ERR_RANGE, "trace_blocks_per_sm must be in [0, 16]");
+    if (t->stage_hot_nodes != 0 && t->stage_hot_nodes != 1) fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 or 1");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    e->opts.wave_paths = t->wave_paths;
+    e->opts.sort_by_material = t->sort_by_material;
+    e->trace_blocks_per_sm = t->trace_blocks_per_sm;
+    e->trace_stage_nodes = t->stage_hot_nodes != 0;
+    e->drop_graphs();
   });
 }
 

@@ -81,11 +81,12 @@ extern "C" vt_status vt_bvh_trace_closest_noalloc(const vt_bvh* bvh, const vt_ra
     a.status = status;
     a.counter = counter;
     a.stack_depth = 2 * bvh->wide_depth + 2;
+    a.node_count = bvh->nodes.count / 5;
     vt::launch_trace_closest(a, 0);
     VT_CUDA(cudaGetLastError());
     VT_CUDA(cudaMemcpy(hits, d_hits, n * sizeof(vt_hit), cudaMemcpyDeviceToHost));
     int st = 0;
     VT_CUDA(cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (st) vt::fail(VT_ERR_BUILD, "traversal stack capacity exceeded");
+    if (st) vt::fail(VT_ERR_BUILD, vt::trace_status_message(st));
   });
 }

@@ -21,6 +21,7 @@
 
 #include "bvh_types.h"
 #include "traverse.h"
+#include "tc_sm100.cuh"
 #include "tri_intersect.cuh"
 
 namespace vt {
@@ -28,6 +29,11 @@ namespace vt {
 namespace {
 
 constexpr int kBlock = 128;
+// Breadth-first prefix of the tree below `root` that every CTA copies into
+// shared memory at start when staging is on: the root and its children and
+// grandchildren of a full 8-wide tree (1 + 8 + 64), 5840 bytes.
+constexpr uint32_t kHotNodes = 73;
+constexpr long long kStagingWaitCycles = 2000000000LL;  // about a second
 
 __device__ __forceinline__ float u8f(uint32_t word, uint32_t sel) {
   // byte `sel` of `word` as a float, via the 2^23 mantissa trick
@@ -105,7 +111,7 @@ __device__ __forceinline__ uint32_t nibble_spread8(uint32_t m) {
   return m * 15u;
 }
 
-template <bool ANY, int STK, bool TWO>
+template <bool ANY, int STK, bool TWO, bool HOT>
 __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                                   const float4* __restrict__ rays, size_t n,
                                                   int4* __restrict__ hits, uint8_t* __restrict__ occluded,
@@ -113,7 +119,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
                                                   unsigned long long* __restrict__ ray_counter,
                                                   const uint32_t* __restrict__ n_dev,
                                                   const float4* __restrict__ insts, uint32_t root,
-                                                  const uint32_t* __restrict__ roots) {
+                                                  const uint32_t* __restrict__ roots, uint32_t hot_count) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -121,8 +127,33 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   // triangle work therefore proceed in lock-step phases with most lanes
   // busy in each, and a lane whose ray finished takes the next unclaimed
   // ray from its warp's pool (one atomicAdd per 16 rays).
-  extern __shared__ uint2 stack_mem[];  // [STK][kBlock], one column per thread
+  // dynamic shared memory: the stack [STK][kBlock] (one column per thread),
+  // then hot_count staged nodes (80 bytes each) starting at nodes[root]
+  extern __shared__ __align__(16) uint2 stack_mem[];
+  __shared__ uint64_t hot_bar;
   uint2* const stack = stack_mem + threadIdx.x;
+  const uint4* const hot = reinterpret_cast<const uint4*>(stack_mem + STK * kBlock);
+  if (HOT && hot_count) {
+    // one bulk copy (TMA engine, no multicast) into shared memory, completed
+    // on an mbarrier by transaction bytes
+    if (threadIdx.x == 0) {
+      const uint32_t bar = tc::smem_u32(&hot_bar), bytes = hot_count * 80u;
+      tc::mbar_init(&hot_bar, 1);
+      tc::fence_mbar_init();
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                   ::"r"(tc::smem_u32(hot)), "l"(nodes + (size_t)root * 5), "r"(bytes), "r"(bar)
+                   : "memory");
+    }
+    __syncthreads();
+    if (!tc::mbar_wait(&hot_bar, 0, kStagingWaitCycles)) {
+      // report, let a late copy land before the shared memory is released,
+      // and leave the rays to the other CTAs
+      atomicOr(status, kTraceStagingWait);
+      tc::mbar_wait(&hot_bar, 0, kStagingWaitCycles);
+      return;
+    }
+  }
   const uint32_t lane = threadIdx.x & 31u;
   constexpr uint32_t kFull = 0xFFFFFFFFu;
   // stack entry tags in x: bit 31 node group, bit 30 instance group, both: return
@@ -186,7 +217,15 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
     if (expand) {
       expand = false;
       const uint4* np = nodes + (size_t)node * 5;
-      const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+      uint4 w0, w1, w2, w3, w4;
+      if (HOT) {
+        // staged prefix from shared memory, the rest from global (one generic load path)
+        const uint32_t hrel = node - root;
+        if (hrel < hot_count) np = hot + hrel * 5;
+        w0 = np[0]; w1 = np[1]; w2 = np[2]; w3 = np[3]; w4 = np[4];
+      } else {
+        w0 = __ldg(np); w1 = __ldg(np + 1); w2 = __ldg(np + 2); w3 = __ldg(np + 3); w4 = __ldg(np + 4);
+      }
       const uint32_t e = w0.w;
       const Slab sx = make_slab(__uint_as_float(w0.x), __uint_as_float((e & 0xFFu) << 23), R.ix, R.ox);
       const Slab sy = make_slab(__uint_as_float(w0.y), __uint_as_float(((e >> 8) & 0xFFu) << 23), R.iy, R.oy);
@@ -227,7 +266,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
             stack[sp * kBlock] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
             ++sp;
           } else {
-            atomicOr(status, 1);
+            atomicOr(status, kTraceStackOverflow);
           }
           ghits = 0;
         }
@@ -235,7 +274,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
           stack[sp * kBlock] = make_uint2(w1.y | kInstGroup, th);
           ++sp;
         } else {
-          atomicOr(status, 1);
+          atomicOr(status, kTraceStackOverflow);
         }
         th = 0;
       }
@@ -298,7 +337,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
               stack[sp * kBlock] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
               ++sp;
             } else {
-              atomicOr(status, 1);  // stack capacity exceeded: result incomplete, reported to the host
+              atomicOr(status, kTraceStackOverflow);  // stack capacity exceeded: result incomplete, reported to the host
             }
             ghits = 0;
           }
@@ -339,7 +378,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
             expand = true;
             break;
           } else {
-            atomicOr(status, 1);
+            atomicOr(status, kTraceStackOverflow);
           }
         } else if (tag == kNodeGroup) {
           --sp;
@@ -449,23 +488,40 @@ __global__ void k_watertight_eval(const float* __restrict__ cases, size_t n, vt_
   out[i] = res;
 }
 
+// Resident CTAs per SM of one instantiation with `smem` dynamic bytes (the
+// opt-in above 48 KB is set first).
+template <class K>
+int resident_per_sm(K kern, size_t smem) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
+  return per_sm;
+}
+
 template <bool ANY, int STK, bool TWO>
 void launch_stk(const TraceArgs& a, cudaStream_t s) {
-  const size_t smem = sizeof(uint2) * STK * kBlock;
-  if (smem > 48 * 1024)  // opt-in above the default 48 KB dynamic limit
-    cudaFuncSetAttribute(k_trace<ANY, STK, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int dev = 0, sms = 0, per_sm = 0;
+  auto plain = k_trace<ANY, STK, TWO, false>;
+  auto staged = k_trace<ANY, STK, TWO, true>;
+  const size_t stack_bytes = sizeof(uint2) * STK * kBlock;
+  int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ANY, STK, TWO>, kBlock, smem);
-  // persistent grid: every resident slot once, never more blocks than rays need
+  int per_sm = resident_per_sm(plain, stack_bytes);
   if (a.blocks_per_sm > 0) per_sm = std::min(per_sm, a.blocks_per_sm);
+  // staged prefix: the nodes from nodes[root] on, for launches with one root,
+  // a 16-aligned start (bulk copies), and no loss of resident CTAs
+  uint32_t hot = 0;
+  if (a.stage_nodes && !a.roots && a.node_count > a.root &&
+      reinterpret_cast<uintptr_t>(a.nodes + (size_t)a.root * 5) % 16 == 0) {
+    hot = (uint32_t)std::min<size_t>(kHotNodes, a.node_count - a.root);
+    if (resident_per_sm(staged, stack_bytes + 80 * (size_t)hot) < per_sm) hot = 0;
+  }
+  // persistent grid: every resident slot once, never more blocks than rays need
   size_t grid = (size_t)std::max(1, sms) * (size_t)std::max(1, per_sm);
   grid = std::min(grid, (a.n + kBlock - 1) / kBlock);
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
-  k_trace<ANY, STK, TWO><<<(unsigned)grid, kBlock, smem, s>>>(a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded,
-                                                              a.status, a.counter, a.n_dev, a.insts, a.root,
-                                                              a.roots);
+  (hot ? staged : plain)<<<(unsigned)grid, kBlock, stack_bytes + 80 * (size_t)hot, s>>>(
+      a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded, a.status, a.counter, a.n_dev, a.insts, a.root, a.roots, hot);
 }
 
 template <bool ANY, bool TWO>
@@ -492,6 +548,12 @@ void launch_trace_closest(const TraceArgs& a, cudaStream_t s) {
 }
 void launch_trace_any(const TraceArgs& a, cudaStream_t s) { launch_trace_t<true>(a, s); }
 void launch_trace_closest_records(const TraceArgs& a, cudaStream_t s) { launch_trace_t<false>(a, s); }
+
+const char* trace_status_message(int status) {
+  if (status & kTraceStackOverflow) return "traversal stack capacity exceeded";
+  if (status & kTraceStagingWait) return "traversal node staging did not complete in time";
+  return "traversal failed";
+}
 
 void launch_watertight_eval(const float* cases, size_t n, vt_watertight_result* out, cudaStream_t s) {
   if (n == 0) return;

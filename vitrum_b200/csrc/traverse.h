@@ -28,7 +28,16 @@ struct TraceArgs {
   const float4* inst_l2w = nullptr;   // refinement of instance hits: local-to-world rows (3 per instance)
   int* inst_out = nullptr;          // optional: instance index per ray (-1 miss / single level)
   int blocks_per_sm = 0;            // persistent CTAs per SM (0: the occupancy limit)
+  size_t node_count = 0;            // nodes in `nodes` (0: unknown, no shared-memory staging)
+  bool stage_nodes = false;         // each CTA copies the top of the tree below `root` into shared memory
 };
+
+// Bits of the device status word a traversal launch sets.
+enum : int {
+  kTraceStackOverflow = 1,  // a group did not fit the stack (the ray was finished without it)
+  kTraceStagingWait = 2,    // the shared-memory node staging did not complete in time (global reads used)
+};
+const char* trace_status_message(int status);
 
 void launch_trace_closest(const TraceArgs& a, cudaStream_t s);
 // Closest hit without the refinement pass: hits hold (triangle record, watertight t bits, 0, 0).
