@@ -159,17 +159,23 @@ typedef struct vt_engine_options {
   int32_t wave_paths;             /* paths in flight per wave; 0 = 2^22 */
 } vt_engine_options;
 
-/* Material (core Material subset, core/src/scene/material.ts): transmission > 0
- * selects the smooth dielectric, metallic >= 0.5 the GGX conductor, otherwise
- * Lambert.  emission is radiance leaving the front face (winding normal). */
+/* Material (core MaterialSpec subset, core/src/scene/material.ts), the
+ * reference's base BSDF: transmission > 0 with metallic 0 is a dielectric
+ * interface (delta at roughness 0, rough GGX otherwise; 1 - transmission of the
+ * refracted share scatters diffusely); anything else is opaque: Lambert
+ * diffuse under a GGX specular layer with F0 = mix(specular_intensity *
+ * ((ior-1)/(ior+1))^2, base_color, metallic) and Kulla-Conty multiple
+ * scattering.  specular_intensity 0 with metallic 0 is a pure Lambertian.
+ * emission is radiance leaving the front face (winding normal). */
 typedef struct vt_material_desc {
   float base_color[3];
-  float roughness;
-  float metallic;
-  float transmission;
-  float ior;
+  float roughness;          /* [0, 1]; GGX alpha = max(roughness^2, 1e-3) */
+  float metallic;           /* [0, 1] */
+  float transmission;       /* [0, 1] */
+  float ior;                /* 0: 1.5 */
   float emission[3];
   uint32_t flags;           /* VT_MATERIAL_* bits */
+  float specular_intensity; /* KHR_materials_specular factor in [0, 1] (MaterialSpec.specularIntensity, default 1) */
 } vt_material_desc;
 
 /* Material flags (the hits traceClosest / traceAny skip and retrace past,

@@ -292,6 +292,7 @@ def flatten_scene(scene):
         mats[k, 3:7] = (m.roughness, m.metallic, m.transmission, m.ior)
         mats[k, 7:10] = m.emission
         mats[k, 10] = (0 if getattr(m, "double_sided", True) else 1) | (0 if getattr(m, "cast_shadow", True) else 2)
+        mats[k, 11] = getattr(m, "specular_intensity", 1.0)
     # rectangle lights: two one-sided emissive triangles each, transparent to shadow rays
     for j, r in enumerate(rects):
         k = len(scene.materials) + j

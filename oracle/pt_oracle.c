@@ -6,13 +6,13 @@
  * Follows the reference integrator's estimator for the plain-PT subset
  * (packages/pt-webgpu/src/wgsl/pathTrace/kernel.wgsl.ts:963-2030, CPU mirror
  * packages/pt-webgpu/src/__tests__/cpuTracer.ts:411-518 generalised to the
- * Lambert / GGX-conductor / smooth-dielectric set):
+ * reference's base BSDF, listed at the BSDF section below):
  *   PCG32 and the frame key            shared-samplers/src/wgsl/pcg.wgsl.ts:5-24,
  *                                      pt-webgpu/src/wgsl/common.wgsl.ts:194-196
  *   primary ray from the inverse VP    kernelCore.wgsl.ts:22-26, common.wgsl.ts:431-470
  *   one light entry, uniform pick      kernel.wgsl.ts:1149-1675 (cpuTracer.ts:411-452)
  *   power-heuristic MIS                material.wgsl.ts:2808-2822
- *   GGX VNDF, Fresnel, frDielectric    bsdf.wgsl.ts:1710-1737, material.wgsl.ts:2766-2806
+ *   GGX VNDF                           bsdf.wgsl.ts:1710-1737
  *   RR for bounce > 2                  kernelCore.wgsl.ts:54-67
  * with the same random-number consumption order as the device kernels, so
  * most samples follow the same path on both sides.  Visibility is the FP64
@@ -25,6 +25,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include "../vitrum_b200/csrc/ggx_albedo_lut.h"
 
 long orc_build_array_bvh(const float* positions, long n_pos_words, int pos_stride, const uint32_t* indices,
                          long ntri, int idx_stride, int max_leaf, int nbins, int max_depth, uint32_t* out_nodes,
@@ -93,10 +95,11 @@ static void onb(v3 n, v3* t, v3* b) {
 /* ---------------------------------------------------------------- scene */
 typedef struct {
   float base[3], roughness, emission[3], ior;
-  int kind; /* 0 lambert, 1 conductor, 2 dielectric */
+  int kind; /* 0 opaque, 1 opaque metallic, 2 dielectric (transmission > 0, metallic 0) */
   float alpha;
   int emissive;
   unsigned flags; /* 1 single-sided (back faces ignored), 2 ignored by shadow rays */
+  float metallic, transmission, specular, f0_ior;
 } orc_mat_t;
 
 typedef struct {
@@ -223,27 +226,65 @@ static long trace(const orc_pt_t* S, const double o[3], const double d[3], doubl
   return best;
 }
 
-/* ---------------------------------------------------------------- BSDF */
-static v3 schlick(v3 f0, float c) {
-  float m = fminf(fmaxf(1.0f - c, 0.0f), 1.0f), m2 = m * m, m5 = m2 * m2 * m;
-  return add(f0, scl(sub(V(1, 1, 1), f0), m5));
+/* ---------------------------------------------------------------- BSDF
+ * The reference's base BSDF for the parameters the scene carries (base colour,
+ * roughness, metallic, transmission, IOR, specular factor):
+ *   opaque      evaluateBrdfFullWithClearcoatNormal  bsdf.wgsl.ts:809-916
+ *               F0 / F90 (KHR specular)              bsdf.wgsl.ts:192-222
+ *               lobe choice, marginal pdf            bsdf.wgsl.ts:1172-1211, 1555-1630
+ *               sampling + finite finalizer          bsdf.wgsl.ts:2919-2998, 1863-1924
+ *               Kulla-Conty lobe, E tables           material.wgsl.ts:2840-2931
+ *   dielectric  Fresnel (Schlick, exact TIR)         bsdf.wgsl.ts:227-256
+ *               events (represented Bernoulli)       bsdf.wgsl.ts:1036-1170
+ *               rough reflection / transmission      bsdf.wgsl.ts:941-1033, 1996-2140
+ *               sampling                             bsdf.wgsl.ts:2618-2812
+ *   GGX D, Smith G1 (tangent form)                   material.wgsl.ts:2797-2804, math/roughDielectric.ts:52-60
+ */
+static const float ggx_e_tab[VT_GGX_ALBEDO_DIM * VT_GGX_ALBEDO_DIM] = {VT_GGX_E_VALUES};
+static const float ggx_eavg_tab[VT_GGX_ALBEDO_DIM] = {VT_GGX_EAVG_VALUES};
+
+static float clamp01f(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+static v3 clamp01v(v3 v) { return V(clamp01f(v.x), clamp01f(v.y), clamp01f(v.z)); }
+static float lum(v3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+static float pow5f(float x) { float x2 = x * x; return x2 * x2 * x; }
+static v3 mbase(const orc_mat_t* m) { return V(m->base[0], m->base[1], m->base[2]); }
+
+static float ggx_albedo(float mu, float r) {
+  const int D = VT_GGX_ALBEDO_DIM;
+  float fr = clamp01f(r) * (float)(D - 1), fm = clamp01f(mu) * (float)(D - 1);
+  int r0 = (int)floorf(fr), m0 = (int)floorf(fm);
+  int r1 = r0 + 1 < D ? r0 + 1 : D - 1, m1 = m0 + 1 < D ? m0 + 1 : D - 1;
+  float tr = fr - (float)r0, tm = fm - (float)m0;
+  float e0 = ggx_e_tab[r0 * D + m0] + (ggx_e_tab[r0 * D + m1] - ggx_e_tab[r0 * D + m0]) * tm;
+  float e1 = ggx_e_tab[r1 * D + m0] + (ggx_e_tab[r1 * D + m1] - ggx_e_tab[r1 * D + m0]) * tm;
+  return fminf(fmaxf(e0 + (e1 - e0) * tr, 0.02f), 1.0f);
 }
-static float fr_dielectric(float cos_i, float eta) {
-  float ct = fminf(fmaxf(cos_i, -1.0f), 1.0f), e = eta;
-  if (ct < 0.0f) { e = 1.0f / e; ct = -ct; }
-  float s2i = fmaxf(0.0f, 1.0f - ct * ct), s2t = s2i / (e * e);
-  if (s2t >= 1.0f) return 1.0f;
-  float cost = sqrtf(fmaxf(0.0f, 1.0f - s2t));
-  float rp = (e * ct - cost) / (e * ct + cost), rs = (ct - e * cost) / (ct + e * cost);
-  return 0.5f * (rp * rp + rs * rs);
+static float ggx_albedo_avg(float r) {
+  const int D = VT_GGX_ALBEDO_DIM;
+  float fr = clamp01f(r) * (float)(D - 1);
+  int r0 = (int)floorf(fr), r1 = r0 + 1 < D ? r0 + 1 : D - 1;
+  float tr = fr - (float)r0;
+  return fminf(fmaxf(ggx_eavg_tab[r0] + (ggx_eavg_tab[r1] - ggx_eavg_tab[r0]) * tr, 0.3f), 1.0f);
+}
+static v3 ggx_multiscatter(v3 f0, float r, float nv, float nl) {
+  float eavg = ggx_albedo_avg(r), miss = 1.0f - eavg;
+  if (miss < 1e-4f) return V(0, 0, 0);
+  float eo = ggx_albedo(nv, r), ei = ggx_albedo(nl, r);
+  v3 favg = add(f0, scl(sub(V(1, 1, 1), f0), 1.0f / 21.0f));
+  v3 fms = scl(mul(favg, favg), eavg);
+  float shape = (1.0f - eo) * (1.0f - ei) / fmaxf(PI_F * miss, 1e-6f);
+  return V(fms.x / fmaxf(1.0f - favg.x * miss, 1e-4f) * shape, fms.y / fmaxf(1.0f - favg.y * miss, 1e-4f) * shape,
+           fms.z / fmaxf(1.0f - favg.z * miss, 1e-4f) * shape);
 }
 static float ggx_d(float nh, float a) {
-  float a2 = a * a, d = nh * nh * (a2 - 1.0f) + 1.0f;
+  float a2 = a * a, n2 = clamp01f(nh * nh), d = (1.0f - n2) + n2 * a2;
   return a2 / (PI_F * d * d);
 }
-static float ggx_g1(float nv, float a) {
-  float a2 = a * a;
-  return 2.0f * nv / (nv + sqrtf(a2 + (1.0f - a2) * nv * nv));
+static float smith_g1(float c, float a) {
+  c = fmaxf(c, 0.0f);
+  if (c <= 1e-6f) return 0.0f;
+  float c2 = c * c, t2 = fmaxf(0.0f, 1.0f - c2) / fmaxf(c2, 1e-10f);
+  return 2.0f / (1.0f + sqrtf(1.0f + a * a * t2));
 }
 static v3 ggx_vndf(v3 wo, float a, float u1, float u2) {
   v3 vh = nrm(V(a * wo.x, a * wo.y, wo.z)), t1, t2;
@@ -255,6 +296,10 @@ static v3 ggx_vndf(v3 wo, float a, float u1, float u2) {
   v3 nh = add(add(scl(t1, p1), scl(t2, p2)), scl(vh, z));
   return nrm(V(a * nh.x, a * nh.y, fmaxf(1e-6f, nh.z)));
 }
+static v3 cosine_sample(float u1, float u2) {
+  float r = sqrtf(u1), phi = 2.0f * PI_F * u2;
+  return V(r * cosf(phi), r * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
+}
 static float power_h(float a, float b) {
   if (!(a >= 0.0f) || !(b >= 0.0f) || a > 3.402823466e38f || b > 3.402823466e38f) return 0.0f;
   float m = fmaxf(a, b);
@@ -262,20 +307,188 @@ static float power_h(float a, float b) {
   float x = a / m, y = b / m;
   return (x * x) / (x * x + y * y);
 }
-static void bsdf_eval(const orc_mat_t* m, v3 wo, v3 wi, v3* fc, float* pdf) {
+
+/* opaque family */
+static v3 opaque_f0(const orc_mat_t* m) {
+  v3 d = V(m->f0_ior, m->f0_ior, m->f0_ior);
+  return add(d, scl(sub(mbase(m), d), m->metallic));
+}
+static v3 opaque_fresnel(const orc_mat_t* m, v3 f0, float c) {
+  float f90 = m->specular + (1.0f - m->specular) * m->metallic;
+  return add(f0, scl(sub(V(f90, f90, f90), f0), pow5f(clamp01f(1.0f - c))));
+}
+static float opaque_spec_prob(const orc_mat_t* m, v3 f0, float nv) {
+  float fl = lum(clamp01v(opaque_fresnel(m, f0, nv)));
+  return represented_bernoulli(fminf(fmaxf(0.04f + 0.92f * fmaxf(fl, m->metallic), 0.04f), 0.96f));
+}
+static void opaque_eval(const orc_mat_t* m, v3 wo, v3 wi, v3* fc, float* pdf) {
   *fc = V(0, 0, 0);
   *pdf = 0.0f;
-  if (wi.z <= 0.0f || wo.z <= 0.0f) return;
-  if (m->kind == 0) {
-    *fc = scl(V(m->base[0], m->base[1], m->base[2]), wi.z / PI_F);
-    *pdf = wi.z / PI_F;
-  } else if (m->kind == 1) {
-    v3 h = nrm(add(wo, wi));
-    float d = ggx_d(h.z, m->alpha), go = ggx_g1(wo.z, m->alpha), gi = ggx_g1(wi.z, m->alpha);
-    v3 F = schlick(V(m->base[0], m->base[1], m->base[2]), fmaxf(0.0f, dot3(wo, h)));
-    *fc = scl(F, d * go * gi / (4.0f * wo.z));
-    *pdf = d * go / (4.0f * wo.z);
+  float nv = fmaxf(wo.z, 0.0f), nl = fmaxf(wi.z, 0.0f);
+  if (nv <= 1e-5f || nl <= 1e-5f) return;
+  v3 h = nrm(add(wi, wo));
+  float nh = fmaxf(h.z, 0.0f), vh = fmaxf(dot3(wo, h), 0.0f);
+  v3 f0 = opaque_f0(m);
+  v3 F = clamp01v(opaque_fresnel(m, f0, vh));
+  v3 kd = scl(sub(V(1, 1, 1), F), 1.0f - m->metallic);
+  float d = ggx_d(nh, m->alpha), g1o = smith_g1(nv, m->alpha);
+  v3 spec = scl(F, d * g1o * smith_g1(nl, m->alpha) / fmaxf(4.0f * nv * nl, 1e-6f));
+  v3 ms = ggx_multiscatter(clamp01v(f0), m->roughness, nv, nl);
+  *fc = scl(add(add(scl(mul(kd, mbase(m)), 1.0f / PI_F), spec), ms), nl);
+  float sp = opaque_spec_prob(m, f0, nv);
+  *pdf = (1.0f - sp) * nl * (1.0f / PI_F) + sp * d * g1o / fmaxf(4.0f * nv, 1e-6f);
+}
+
+/* dielectric family; eta = n_t / n_i for light arriving along wo, wo on +z */
+static float diel_fresnel(const orc_mat_t* m, float c, float eta) {
+  c = clamp01f(fabsf(c));
+  eta = fmaxf(fabsf(eta), 1e-8f);
+  if (eta < 1.0f && 1.0f - c * c >= eta * eta) return 1.0f;
+  return clamp01f(m->f0_ior + (m->specular - m->f0_ior) * pow5f(1.0f - c));
+}
+/* (joint reflection, joint diffuse, joint transmission, P(reflection | not diffuse)) */
+static void diel_events(float d, float r, float t, float out[4]) {
+  d = fmaxf(d, 0.0f);
+  r = fmaxf(r, 0.0f);
+  t = fmaxf(t, 0.0f);
+  float total = d + r + t, dt = r + t;
+  out[0] = out[1] = out[2] = out[3] = 0.0f;
+  if (!(total > 0.0f)) return;
+  if (!(dt > 0.0f)) { out[1] = 1.0f; return; }
+  if (!(d > 0.0f)) {
+    float rc = t > 0.0f ? represented_bernoulli(r / dt) : 1.0f;
+    out[0] = rc; out[2] = 1.0f - rc; out[3] = rc;
+    return;
   }
+  float pd, pdi, rc;
+  if (d <= dt) { pd = represented_bernoulli(d / total); pdi = 1.0f - pd; }
+  else { pdi = represented_bernoulli(dt / total); pd = 1.0f - pdi; }
+  if (!(r > 0.0f)) rc = 0.0f;
+  else if (!(t > 0.0f)) rc = 1.0f;
+  else if (r <= t) rc = represented_bernoulli(r / dt);
+  else rc = 1.0f - represented_bernoulli(t / dt);
+  out[0] = pdi * rc; out[1] = pd; out[2] = pdi - pdi * rc; out[3] = rc;
+}
+static void diel_event_probs(const orc_mat_t* m, float eta, float cos_o, float wo_wm, float out[4]) {
+  float macro_t = 1.0f - diel_fresnel(m, cos_o, eta), fm = diel_fresnel(m, wo_wm, eta);
+  diel_events(clamp01f(macro_t * (1.0f - m->transmission)), fm, m->transmission * clamp01f(1.0f - fm), out);
+}
+static float vndf_pdf(const orc_mat_t* m, v3 wo, v3 wm) {
+  float no = fmaxf(wo.z, 1e-6f), om = dot3(wo, wm);
+  if (no <= 1e-5f || om <= 1e-6f || wm.z <= 0.0f) return 0.0f;
+  return ggx_d(fmaxf(wm.z, 0.0f), m->alpha) * smith_g1(no, m->alpha) * om / no;
+}
+static void diel_eval(const orc_mat_t* m, float eta, v3 wo, v3 wi, v3* fc, float* pdf) {
+  *fc = V(0, 0, 0);
+  *pdf = 0.0f;
+  int smooth = m->roughness <= 0.0f;
+  float co = wo.z, ci = wi.z, ev[4];
+  if (co <= 1e-5f) return;
+  if (wi.z > 0.0f) {
+    if (ci <= 1e-5f) return;
+    v3 wm = nrm(add(wo, wi));
+    diel_event_probs(m, eta, co, fabsf(dot3(wo, wm)), ev);
+    float macro_t = 1.0f - diel_fresnel(m, co, eta);
+    v3 f = scl(mbase(m), macro_t * (1.0f - m->transmission) * (1.0f / PI_F));
+    float ps = 0.0f;
+    if (!smooth) {
+      float d = ggx_d(fmaxf(wm.z, 0.0f), m->alpha), g1o = smith_g1(co, m->alpha);
+      float fm = diel_fresnel(m, fabsf(dot3(wo, wm)), eta);
+      float r = d * g1o * smith_g1(ci, m->alpha) * fm / fmaxf(4.0f * co * ci, 1e-10f);
+      f = add(f, V(r, r, r));
+      ps = d * g1o / fmaxf(4.0f * co, 1e-6f);
+    }
+    *fc = scl(f, ci);
+    *pdf = ev[1] * ci * (1.0f / PI_F) + ev[0] * ps;
+  } else {
+    if (smooth || ci >= -1e-5f) return;
+    v3 wm = nrm(add(wo, scl(wi, eta)));
+    if (wm.z < 0.0f) wm = scl(wm, -1.0f);
+    float im = dot3(wi, wm), om = dot3(wo, wm);
+    if (im * ci < 0.0f || om * co < 0.0f) return;
+    float den = im + om / eta;
+    float d = ggx_d(fmaxf(wm.z, 0.0f), m->alpha);
+    float g = smith_g1(co, m->alpha) * smith_g1(fabsf(ci), m->alpha);
+    float tr = 1.0f - diel_fresnel(m, fabsf(om), eta);
+    float ft = d * tr * g * fabsf(im * om / fmaxf(fabsf(den * den * ci * co), 1e-10f)) / (eta * eta);
+    *fc = scl(mbase(m), m->transmission * ft * fabsf(ci));
+    diel_event_probs(m, eta, co, fabsf(om), ev);
+    *pdf = ev[2] * vndf_pdf(m, wo, wm) * fabsf(im) / fmaxf(den * den, 1e-10f);
+  }
+}
+static void bsdf_eval(const orc_mat_t* m, float eta, v3 wo, v3 wi, v3* fc, float* pdf) {
+  if (m->kind == 2) diel_eval(m, eta, wo, wi, fc, pdf);
+  else opaque_eval(m, wo, wi, fc, pdf);
+}
+static int has_finite_support(const orc_mat_t* m) {
+  return m->kind != 2 || m->roughness > 0.0f || m->transmission < 1.0f;
+}
+typedef struct { v3 wi, weight; float pdf; int delta, valid; } bsample_t;
+static bsample_t sample_bsdf(const orc_mat_t* m, float eta, v3 wo, uint32_t* rng) {
+  bsample_t s;
+  s.wi = V(0, 0, 1);
+  s.weight = V(0, 0, 0);
+  s.pdf = 0.0f;
+  s.delta = 0;
+  s.valid = 0;
+  if (m->kind != 2) {
+    float sp = opaque_spec_prob(m, opaque_f0(m), fmaxf(wo.z, 0.0f));
+    int spec = rand01(rng) < sp;
+    float u1 = rand01(rng), u2 = rand01(rng);
+    if (spec) {
+      v3 h = ggx_vndf(wo, m->alpha, u1, u2);
+      s.wi = sub(scl(h, 2.0f * dot3(wo, h)), wo);
+    } else {
+      s.wi = cosine_sample(u1, u2);
+    }
+  } else {
+    int smooth = m->roughness <= 0.0f;
+    v3 wm = V(0, 0, 1);
+    if (!smooth) {
+      float u1 = rand01(rng), u2 = rand01(rng);
+      wm = ggx_vndf(wo, m->alpha, u1, u2);
+    }
+    float ci = dot3(wo, wm), k = 1.0f - (1.0f - ci * ci) / (eta * eta);
+    int can_refract = k >= 0.0f;
+    float fm = can_refract ? diel_fresnel(m, fabsf(ci), eta) : 1.0f;
+    float macro_t = 1.0f - diel_fresnel(m, wo.z, eta), ev[4];
+    diel_events(clamp01f(macro_t * (1.0f - m->transmission)), fm, m->transmission * clamp01f(1.0f - fm), ev);
+    int diffuse = rand01(rng) < ev[1], refl = 0;
+    if (!diffuse) refl = rand01(rng) < ev[3];
+    if (diffuse) {
+      float u1 = rand01(rng), u2 = rand01(rng);
+      s.wi = cosine_sample(u1, u2);
+    } else if (refl) {
+      s.wi = sub(scl(wm, 2.0f * ci), wo);
+      if (smooth) {
+        s.pdf = ev[0];
+        s.weight = scl(V(fm, fm, fm), 1.0f / fmaxf(ev[0], 1e-10f));
+        s.delta = 1;
+        s.valid = ev[0] > 0.0f;
+        return s;
+      }
+      if (s.wi.z <= 1e-5f) return s;
+    } else {
+      if (!can_refract) return s;
+      s.wi = nrm(add(scl(wo, -1.0f / eta), scl(wm, ci / eta - sqrtf(k))));
+      if (smooth) {
+        s.pdf = ev[2];
+        s.weight = scl(mbase(m), m->transmission * (1.0f - fm) / (eta * eta) / fmaxf(ev[2], 1e-10f));
+        s.delta = 1;
+        s.valid = ev[2] > 0.0f;
+        return s;
+      }
+      if (s.wi.z >= -1e-5f) return s;
+    }
+  }
+  v3 fc;
+  float pdf;
+  bsdf_eval(m, eta, wo, s.wi, &fc, &pdf);
+  if (!(pdf > 0.0f) || fabsf(s.wi.z) <= 1e-8f) return s;
+  s.pdf = pdf;
+  s.weight = scl(fc, 1.0f / pdf);
+  s.valid = maxc(s.weight) > 0.0f;
+  return s;
 }
 
 /* ---------------------------------------------------------------- lights */
@@ -458,75 +671,37 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
     onb(n, &tb, &bb);
     v3 wol = V(dot3(wo, tb), dot3(wo, bb), dot3(wo, n));
     int alive = 0;
-    if (m->kind != 2) {
-      if (S->n_entries > 0) {
-        lsample_t ls = sample_light(S, P, &rng);
-        if (ls.valid) {
-          v3 wil = V(dot3(ls.wi, tb), dot3(ls.wi, bb), dot3(ls.wi, n)), fc;
-          float pb;
-          bsdf_eval(m, wol, wil, &fc, &pb);
-          if (maxc(fc) > 0.0f) {
-            float w = (ls.delta || last) ? 1.0f : power_h(ls.pdf, pb);
-            v3 cc = scl(mul(mul(T, fc), ls.Le), w / ls.pdf);
-            if (maxc(cc) > 0.0f) {
-              v3 so = add(P, scl(n, off));
-              double sod[3] = {so.x, so.y, so.z}, sdd[3] = {ls.wi.x, ls.wi.y, ls.wi.z}, st2;
-              double tmax = isinf(ls.dist) ? INFINITY : (double)(ls.dist * (1.0f - 1e-4f));
-              log_ray(S, 1, sod, sdd, tmax);
-              if (trace(S, sod, sdd, tmax, 1, &st2) < 0) L = add(L, cc);
-            }
+    float eta = front ? m->ior : 1.0f / m->ior;
+    if (S->n_entries > 0 && has_finite_support(m)) {
+      lsample_t ls = sample_light(S, P, &rng);
+      if (ls.valid) {
+        v3 wil = V(dot3(ls.wi, tb), dot3(ls.wi, bb), dot3(ls.wi, n)), fc;
+        float pb;
+        bsdf_eval(m, eta, wol, wil, &fc, &pb);
+        if (maxc(fc) > 0.0f) {
+          float w = (ls.delta || last) ? 1.0f : power_h(ls.pdf, pb);
+          v3 cc = scl(mul(mul(T, fc), ls.Le), w / ls.pdf);
+          if (maxc(cc) > 0.0f) {
+            v3 so = add(P, scl(n, wil.z > 0.0f ? off : -off));
+            double sod[3] = {so.x, so.y, so.z}, sdd[3] = {ls.wi.x, ls.wi.y, ls.wi.z}, st2;
+            double tmax = isinf(ls.dist) ? INFINITY : (double)(ls.dist * (1.0f - 1e-4f));
+            log_ray(S, 1, sod, sdd, tmax);
+            if (trace(S, sod, sdd, tmax, 1, &st2) < 0) L = add(L, cc);
           }
         }
       }
-      if (!last) {
-        float u1 = rand01(&rng), u2 = rand01(&rng), pdf = 0.0f;
-        v3 wil = V(0, 0, 0), wgt = V(0, 0, 0);
-        if (m->kind == 0) {
-          float r = sqrtf(u1), phi = 2.0f * PI_F * u2;
-          wil = V(r * cosf(phi), r * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
-          pdf = wil.z / PI_F;
-          wgt = V(m->base[0], m->base[1], m->base[2]);
-        } else {
-          v3 hl = ggx_vndf(wol, m->alpha, u1, u2);
-          float oh = dot3(wol, hl);
-          wil = sub(scl(hl, 2.0f * oh), wol);
-          if (wil.z > 0.0f && oh > 0.0f) {
-            pdf = ggx_d(hl.z, m->alpha) * ggx_g1(wol.z, m->alpha) / (4.0f * wol.z);
-            wgt = scl(schlick(V(m->base[0], m->base[1], m->base[2]), oh), ggx_g1(wil.z, m->alpha));
-          }
-        }
-        if (pdf > 0.0f && maxc(wgt) > 0.0f) {
-          v3 wi = add(add(scl(tb, wil.x), scl(bb, wil.y)), scl(n, wil.z));
-          T = mul(T, wgt);
-          alive = 1;
-          o = add(P, scl(n, off));
-          d = wi;
-          prev_delta = 0;
-          prev_pdf = pdf;
-        }
+    }
+    if (!last) {
+      bsample_t bs = sample_bsdf(m, eta, wol, &rng);
+      if (bs.valid) {
+        v3 wi = add(add(scl(tb, bs.wi.x), scl(bb, bs.wi.y)), scl(n, bs.wi.z));
+        T = mul(T, bs.weight);
+        alive = 1;
+        o = add(P, scl(n, bs.wi.z > 0.0f ? off : -off));
+        d = wi;
+        prev_delta = bs.delta;
+        prev_pdf = bs.pdf;
       }
-    } else if (!last) {
-      float eta = front ? m->ior : 1.0f / m->ior, cosi = wol.z;
-      float F = represented_bernoulli(fr_dielectric(cosi, eta));
-      v3 wi = V(0, 0, 0), wgt = V(1, 1, 1);
-      int refl = rand01(&rng) < F;
-      if (!refl) {
-        float s2t = fmaxf(0.0f, 1.0f - cosi * cosi) / (eta * eta);
-        if (s2t >= 1.0f) {
-          refl = 1;
-        } else {
-          float cost = sqrtf(1.0f - s2t);
-          wi = nrm(add(scl(d, 1.0f / eta), scl(n, cosi / eta - cost)));
-          wgt = scl(V(1, 1, 1), 1.0f / (eta * eta));
-        }
-      }
-      if (refl) wi = add(d, scl(n, 2.0f * cosi));
-      T = mul(T, wgt);
-      o = add(P, scl(n, off * (refl ? 1.0f : -1.0f)));
-      d = wi;
-      alive = 1;
-      prev_delta = 1;
-      prev_pdf = 0.0f;
     }
     if (alive && bounce > 2) {
       float q = represented_bernoulli(fminf(fmaxf(maxc(T), 0.1f), 0.95f));
@@ -563,7 +738,8 @@ static void* pt_worker(void* arg) {
 
 /*
  * Render width x height pixels x spp samples.  materials: 12 floats each
- * (base rgb 0-2, roughness 3, metallic 4, transmission 5, ior 6, emission rgb 7-9, pad);
+ * (base rgb 0-2, roughness 3, metallic 4, transmission 5, ior 6, emission rgb 7-9, flags 10,
+ * specular intensity 11);
  * env: W*H*3 floats (NULL for none); points: 6 floats each.  Writes FP64
  * sum and sum of squares (3 per pixel).  Returns 0, or -1 on a build error.
  */
@@ -588,8 +764,13 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
     const float* m = materials + 12 * i;
     for (int k = 0; k < 3; ++k) { mats[i].base[k] = m[k]; mats[i].emission[k] = m[7 + k]; }
     mats[i].roughness = m[3];
-    mats[i].ior = m[6] > 0 ? m[6] : 1.5f;
-    mats[i].kind = m[5] > 0 ? 2 : (m[4] >= 0.5f ? 1 : 0);
+    mats[i].ior = m[6] > 0 ? fmaxf(m[6], 1.0f) : 1.5f;
+    mats[i].metallic = m[4];
+    mats[i].transmission = clamp01f(m[5]);
+    mats[i].specular = m[11];
+    float ratio = (mats[i].ior - 1.0f) / (mats[i].ior + 1.0f);
+    mats[i].f0_ior = ratio * ratio * mats[i].specular;
+    mats[i].kind = (m[5] > 0 && m[4] == 0.0f) ? 2 : (m[4] > 0.0f ? 1 : 0);
     mats[i].alpha = fmaxf(m[3] * m[3], 1e-3f);
     mats[i].emissive = m[7] > 0 || m[8] > 0 || m[9] > 0;
     mats[i].flags = (unsigned)m[10];

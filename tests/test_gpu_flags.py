@@ -48,7 +48,8 @@ def test_cast_shadow_false_is_ignored_by_shadow_rays(cuda, cast):
     floor, tf = scenes.grid_quad((-5, 0, -5), (0, 0, 10), (10, 0, 0), 4)
     occ, to = scenes.grid_quad((-4.9, 0.5, -4.9), (0, 0, 9.8), (9.8, 0, 0), 1)  # covers the floor below the light
     sc = Scene(meshes=[Mesh(floor, tf, 0), Mesh(occ, to, 1)],
-               materials=[Material(base_color=(rho,) * 3), Material(base_color=(0.0,) * 3, cast_shadow=cast)],
+               materials=[Material(base_color=(rho,) * 3, specular_intensity=0.0),
+                          Material(base_color=(0.0,) * 3, cast_shadow=cast, specular_intensity=0.0)],
                point_lights=[PointLight((0.0, h, 0.0), (I, I, I))])
     # camera between the floor and the occluder, looking at the floor under the occluder
     cam = Camera(eye=(0.0, 0.25, 3.0), target=(0.0, 0.0, 0.0), fov_y_deg=30.0, near=0.01, far=100.0)

@@ -16,7 +16,10 @@ pytestmark = pytest.mark.gpu
 
 def plane_scene(**lights):
     p, t = scenes.grid_quad((-5, 0, -5), (0, 0, 10), (10, 0, 0), 4)   # normal +y
-    return Scene(meshes=[Mesh(p, t, 0)], materials=[Material(base_color=(0.8, 0.8, 0.8))], **lights)
+    # a pure Lambertian (specular factor 0; roughness 0 keeps the multiple-scattering
+    # lobe that the F0 = 0 layer still carries below 1e-4 of the diffuse term)
+    mat = Material(base_color=(0.8, 0.8, 0.8), specular_intensity=0.0, roughness=0.0)
+    return Scene(meshes=[Mesh(p, t, 0)], materials=[mat], **lights)
 
 
 CAM = Camera(eye=(0.0, 3.0, 0.01), target=(0.0, 0.0, 0.0), fov_y_deg=50.0, near=0.01, far=100.0)

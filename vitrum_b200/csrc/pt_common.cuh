@@ -9,14 +9,15 @@
 //   Russian roulette clamp(max T, .1, .95) kernelCore.wgsl.ts:54-67
 //   cosine hemisphere + ONB                bsdf.wgsl.ts:1632-1663 (cpuTracer.ts:236-272)
 //   GGX VNDF (Heitz 2018)                  bsdf.wgsl.ts:1710-1737 (cpuTracer.ts:280-306)
-//   frDielectric                           material.wgsl.ts:2780 (cpuTracer.ts:313-324)
-//   Schlick Fresnel                        material.wgsl.ts:2766
+//   BSDF families                          see the materials section below
 //   power heuristic (beta = 2)             material.wgsl.ts:2808-2822 (cpuTracer.ts:343-354)
 #pragma once
 
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
+
+#include "ggx_albedo_lut.h"
 
 namespace vt {
 namespace pt {
@@ -89,47 +90,101 @@ __device__ __forceinline__ float power_heuristic(float a, float b) {
 }
 
 // ------------------------------------------------------------------ materials
-enum MaterialKind : uint32_t { kLambert = 0, kConductor = 1, kDielectric = 2 };
+// The reference's base BSDF restricted to the parameters the scene ABI carries
+// (base colour, roughness, metallic, transmission, IOR, specular factor; no
+// clearcoat / sheen / iridescence / anisotropy / thin film):
+//   opaque    transmission 0 or metallic > 0: Lambert diffuse under a GGX
+//             specular layer, F0 = mix(specular * ((ior-1)/(ior+1))^2, base,
+//             metallic), Kulla-Conty multiple scattering
+//             (evaluateBrdfFullWithClearcoatNormal, bsdf.wgsl.ts:809-916);
+//             sampling picks GGX visible normals with probability
+//             clamp(mix(.04, .96, max(lum F(N.V), metallic)), .04, .96), else
+//             the cosine lobe, and weights by the full BSDF over the marginal
+//             density (bsdf.wgsl.ts:2919-2998, 1863-1924, 1172-1211, 1555-1630)
+//   dielectric transmission > 0 and metallic 0: a Schlick-Fresnel interface
+//             (materialDielectricFresnel, bsdf.wgsl.ts:227-256, exact TIR)
+//             that reflects, transmits (tinted by base * transmission) or, with
+//             weight 1 - transmission, scatters diffusely; delta at roughness
+//             0, else the Walter 2007 rough model on sampled visible normals
+//             (bsdf.wgsl.ts:941-1033, 1099-1170, 1996-2160, 2618-2918)
+// The kinds are sort buckets: opaque with metallic 0 / > 0, dielectric.
+enum MaterialKind : uint32_t { kOpaque = 0, kMetal = 1, kDielectric = 2 };
 
 struct Material {
   float3 base_color;
   float roughness;
   float3 emission;   // radiance emitted from the front face
-  float ior;
+  float ior;         // of the material side (the other side is 1)
   uint32_t kind;
   float alpha;       // GGX alpha = max(roughness^2, 1e-3)
   uint32_t emissive; // emission > 0
   uint32_t flags;    // VT_MATERIAL_* bits
+  float metallic;
+  float transmission;  // clamped to [0, 1]
+  float specular;      // KHR_materials_specular factor: dielectric F0 scale and F90
+  float f0_ior;        // specular * ((ior - 1) / (ior + 1))^2
 };
 
-__device__ __forceinline__ float3 schlick(float3 f0, float c) {
-  const float m = fminf(fmaxf(1.0f - c, 0.0f), 1.0f);
-  const float m2 = m * m, m5 = m2 * m2 * m;
-  return f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * m5;
+__host__ __device__ __forceinline__ float clamp01(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+__host__ __device__ __forceinline__ float3 clamp01(float3 v) { return f3(clamp01(v.x), clamp01(v.y), clamp01(v.z)); }
+// BT.709 luminance (shared-samplers/src/wgsl/luminance.wgsl.ts:28-30)
+__host__ __device__ __forceinline__ float luminance(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+__device__ __forceinline__ float pow5(float x) {
+  const float x2 = x * x;
+  return x2 * x2 * x;
 }
 
-__device__ __forceinline__ float fr_dielectric(float cos_i, float eta) {
-  float ct = fminf(fmaxf(cos_i, -1.0f), 1.0f);
-  float e = eta;
-  if (ct < 0.0f) { e = 1.0f / e; ct = -ct; }
-  const float sin2i = fmaxf(0.0f, 1.0f - ct * ct);
-  const float sin2t = sin2i / (e * e);
-  if (sin2t >= 1.0f) return 1.0f;
-  const float cost = sqrtf(fmaxf(0.0f, 1.0f - sin2t));
-  const float rpar = (e * ct - cost) / (e * ct + cost);
-  const float rperp = (ct - e * cost) / (ct + e * cost);
-  return 0.5f * (rpar * rpar + rperp * rperp);
+static __constant__ float kGgxE[VT_GGX_ALBEDO_DIM * VT_GGX_ALBEDO_DIM] = {VT_GGX_E_VALUES};
+static __constant__ float kGgxEavg[VT_GGX_ALBEDO_DIM] = {VT_GGX_EAVG_VALUES};
+
+// Bilinear E_ss(mu, roughness), clamped to [0.02, 1] (ggxDirectionalAlbedo, material.wgsl.ts:2873-2891)
+__device__ __forceinline__ float ggx_albedo(float mu, float r) {
+  constexpr int kD = VT_GGX_ALBEDO_DIM;
+  const float fr = clamp01(r) * (float)(kD - 1), fm = clamp01(mu) * (float)(kD - 1);
+  const int r0 = (int)floorf(fr), m0 = (int)floorf(fm);
+  const int r1 = min(r0 + 1, kD - 1), m1 = min(m0 + 1, kD - 1);
+  const float tr = fr - (float)r0, tm = fm - (float)m0;
+  const float e0 = kGgxE[r0 * kD + m0] + (kGgxE[r0 * kD + m1] - kGgxE[r0 * kD + m0]) * tm;
+  const float e1 = kGgxE[r1 * kD + m0] + (kGgxE[r1 * kD + m1] - kGgxE[r1 * kD + m0]) * tm;
+  return fminf(fmaxf(e0 + (e1 - e0) * tr, 0.02f), 1.0f);
+}
+// Linear E_avg(roughness), clamped to [0.3, 1] (ggxAverageAlbedo, material.wgsl.ts:2894-2901)
+__device__ __forceinline__ float ggx_albedo_avg(float r) {
+  constexpr int kD = VT_GGX_ALBEDO_DIM;
+  const float fr = clamp01(r) * (float)(kD - 1);
+  const int r0 = (int)floorf(fr), r1 = min(r0 + 1, kD - 1);
+  const float tr = fr - (float)r0;
+  return fminf(fmaxf(kGgxEavg[r0] + (kGgxEavg[r1] - kGgxEavg[r0]) * tr, 0.3f), 1.0f);
+}
+// Kulla-Conty multiple-scattering BRDF (no cosine), f0 tinting the extra
+// bounces through F_avg = f0 + (1 - f0) / 21 (material.wgsl.ts:2903-2931)
+__device__ __forceinline__ float3 ggx_multiscatter(float3 f0, float r, float nv, float nl) {
+  const float eavg = ggx_albedo_avg(r);
+  const float miss = 1.0f - eavg;
+  if (miss < 1e-4f) return f3(0.0f, 0.0f, 0.0f);
+  const float eo = ggx_albedo(nv, r), ei = ggx_albedo(nl, r);
+  const float3 favg = f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * (1.0f / 21.0f);
+  const float3 den = f3(fmaxf(1.0f - favg.x * miss, 1e-4f), fmaxf(1.0f - favg.y * miss, 1e-4f),
+                        fmaxf(1.0f - favg.z * miss, 1e-4f));
+  const float3 fms = favg * favg * eavg;
+  const float shape = (1.0f - eo) * (1.0f - ei) / fmaxf(CUDART_PI_F * miss, 1e-6f);
+  return f3(fms.x / den.x, fms.y / den.y, fms.z / den.z) * shape;
 }
 
-// GGX distribution and Smith G1 in the local frame (n = +z)
+// GGX distribution in the cancellation-free form (ggxD, material.wgsl.ts:2797-2804)
 __device__ __forceinline__ float ggx_d(float nh, float a) {
   const float a2 = a * a;
-  const float d = nh * nh * (a2 - 1.0f) + 1.0f;
+  const float n2 = clamp01(nh * nh);
+  const float d = (1.0f - n2) + n2 * a2;
   return a2 / (CUDART_PI_F * d * d);
 }
-__device__ __forceinline__ float ggx_g1(float nv, float a) {
-  const float a2 = a * a;
-  return 2.0f * nv / (nv + sqrtf(a2 + (1.0f - a2) * nv * nv));
+// Smith G1 in the tangent form (roughDielectricSmithG1Wgsl, math/roughDielectric.ts:52-60)
+__device__ __forceinline__ float smith_g1(float c, float a) {
+  c = fmaxf(c, 0.0f);
+  if (c <= 1e-6f) return 0.0f;
+  const float c2 = c * c;
+  const float t2 = fmaxf(0.0f, 1.0f - c2) / fmaxf(c2, 1e-10f);
+  return 2.0f / (1.0f + sqrtf(1.0f + a * a * t2));
 }
 // Heitz 2018 visible-normal sample, wo and result in the local frame
 __device__ __forceinline__ float3 ggx_vndf(float3 wo, float a, float u1, float u2) {
@@ -146,24 +201,231 @@ __device__ __forceinline__ float3 ggx_vndf(float3 wo, float a, float u1, float u
   const float3 nh = t1 * p1 + t2 * p2 + vh * z;
   return normalize(f3(a * nh.x, a * nh.y, fmaxf(1e-6f, nh.z)));
 }
+__device__ __forceinline__ float3 cosine_sample(float u1, float u2) {
+  const float r = sqrtf(u1), phi = 2.0f * CUDART_PI_F * u2;
+  return f3(r * cosf(phi), r * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
+}
 
-// BSDF value * |cos(wi)| and solid-angle pdf for non-delta families.
-// wo, wi in the local frame with the shading normal at +z (wo.z > 0).
-__device__ __forceinline__ void bsdf_eval(const Material& m, float3 wo, float3 wi, float3& f_cos, float& pdf) {
+// ---- opaque family
+__device__ __forceinline__ float3 opaque_f0(const Material& m) {
+  const float3 d = f3(m.f0_ior, m.f0_ior, m.f0_ior);
+  return d + (m.base_color - d) * m.metallic;
+}
+__device__ __forceinline__ float3 opaque_fresnel(const Material& m, float3 f0, float c) {
+  const float f90 = m.specular + (1.0f - m.specular) * m.metallic;
+  return f0 + (f3(f90, f90, f90) - f0) * pow5(clamp01(1.0f - c));
+}
+// probability of sampling the specular lobe (brdfFiniteBaseLobeWeights)
+__device__ __forceinline__ float opaque_spec_prob(const Material& m, float3 f0, float nv) {
+  const float fl = luminance(clamp01(opaque_fresnel(m, f0, nv)));
+  return represented_bernoulli(fminf(fmaxf(0.04f + 0.92f * fmaxf(fl, m.metallic), 0.04f), 0.96f));
+}
+// BSDF * cos(wi) and the marginal sampling density; wo, wi in the local frame (n = +z)
+__device__ __forceinline__ void opaque_eval(const Material& m, float3 wo, float3 wi, float3& f_cos, float& pdf) {
   f_cos = f3(0.0f, 0.0f, 0.0f);
   pdf = 0.0f;
-  if (wi.z <= 0.0f || wo.z <= 0.0f) return;
-  if (m.kind == kLambert) {
-    f_cos = m.base_color * (wi.z / CUDART_PI_F);
-    pdf = wi.z / CUDART_PI_F;
-  } else if (m.kind == kConductor) {
-    const float3 h = normalize(wo + wi);
-    const float d = ggx_d(h.z, m.alpha);
-    const float g1o = ggx_g1(wo.z, m.alpha), g1i = ggx_g1(wi.z, m.alpha);
-    const float3 F = schlick(m.base_color, fmaxf(0.0f, dot(wo, h)));
-    f_cos = F * (d * g1o * g1i / (4.0f * wo.z));
-    pdf = d * g1o / (4.0f * wo.z);
+  const float nv = fmaxf(wo.z, 0.0f), nl = fmaxf(wi.z, 0.0f);
+  if (nv <= 1e-5f || nl <= 1e-5f) return;
+  const float3 h = normalize(wi + wo);
+  const float nh = fmaxf(h.z, 0.0f), vh = fmaxf(dot(wo, h), 0.0f);
+  const float3 f0 = opaque_f0(m);
+  const float3 F = clamp01(opaque_fresnel(m, f0, vh));
+  const float3 kd = (f3(1.0f, 1.0f, 1.0f) - F) * (1.0f - m.metallic);
+  const float d = ggx_d(nh, m.alpha);
+  const float g1o = smith_g1(nv, m.alpha);
+  const float3 spec = F * (d * g1o * smith_g1(nl, m.alpha) / fmaxf(4.0f * nv * nl, 1e-6f));
+  const float3 ms = ggx_multiscatter(clamp01(f0), m.roughness, nv, nl);
+  f_cos = (kd * m.base_color * (1.0f / CUDART_PI_F) + spec + ms) * nl;
+  const float sp = opaque_spec_prob(m, f0, nv);
+  pdf = (1.0f - sp) * nl * (1.0f / CUDART_PI_F) + sp * d * g1o / fmaxf(4.0f * nv, 1e-6f);
+}
+
+// ---- dielectric family
+__device__ __forceinline__ float diel_fresnel(const Material& m, float c, float eta) {
+  c = clamp01(fabsf(c));
+  eta = fmaxf(fabsf(eta), 1e-8f);
+  if (eta < 1.0f && 1.0f - c * c >= eta * eta) return 1.0f;  // total internal reflection
+  return clamp01(m.f0_ior + (m.specular - m.f0_ior) * pow5(1.0f - c));
+}
+// (joint reflection, joint diffuse, joint transmission, P(reflection | not diffuse))
+// as realised by rand01 thresholds (bsdfRepresentedDielectricEventProbabilities, bsdf.wgsl.ts:1036-1097)
+__device__ __forceinline__ float4 diel_events(float d, float r, float t) {
+  d = fmaxf(d, 0.0f);
+  r = fmaxf(r, 0.0f);
+  t = fmaxf(t, 0.0f);
+  const float total = d + r + t;
+  if (!(total > 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float dt = r + t;
+  if (!(dt > 0.0f)) return make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+  if (!(d > 0.0f)) {
+    const float rc = t > 0.0f ? represented_bernoulli(r / dt) : 1.0f;
+    return make_float4(rc, 0.0f, 1.0f - rc, rc);
   }
+  float pd, pdi;
+  if (d <= dt) {
+    pd = represented_bernoulli(d / total);
+    pdi = 1.0f - pd;
+  } else {
+    pdi = represented_bernoulli(dt / total);
+    pd = 1.0f - pdi;
+  }
+  float rc;
+  if (!(r > 0.0f)) rc = 0.0f;
+  else if (!(t > 0.0f)) rc = 1.0f;
+  else if (r <= t) rc = represented_bernoulli(r / dt);
+  else rc = 1.0f - represented_bernoulli(t / dt);
+  const float pr = pdi * rc;
+  return make_float4(pr, pd, pdi - pr, rc);
+}
+// event probabilities for the microfacet normal wm (bsdfDielectricFiniteEventProbabilities)
+__device__ __forceinline__ float4 diel_event_probs(const Material& m, float eta, float cos_o, float wo_wm) {
+  const float macro_t = 1.0f - diel_fresnel(m, cos_o, eta);
+  const float fm = diel_fresnel(m, wo_wm, eta);
+  return diel_events(clamp01(macro_t * (1.0f - m.transmission)), fm, m.transmission * clamp01(1.0f - fm));
+}
+// half vector of a transmission pair, on the side of n (bsdfRoughTransmissionHalfVector)
+__device__ __forceinline__ float3 diel_half_t(float3 wo, float3 wi, float eta) {
+  float3 wm = normalize(wo + wi * eta);
+  if (wm.z < 0.0f) wm = -wm;
+  return wm;
+}
+// visible-normal density of wm (bsdfGgxVisibleNormalPdf)
+__device__ __forceinline__ float vndf_pdf(const Material& m, float3 wo, float3 wm) {
+  const float no = fmaxf(wo.z, 1e-6f), om = dot(wo, wm);
+  if (no <= 1e-5f || om <= 1e-6f || wm.z <= 0.0f) return 0.0f;
+  return ggx_d(fmaxf(wm.z, 0.0f), m.alpha) * smith_g1(no, m.alpha) * om / no;
+}
+// BSDF * |cos(wi)| and marginal density; wo on the +z side, eta = n_t / n_i
+// for light arriving from wo's side
+__device__ __forceinline__ void diel_eval(const Material& m, float eta, float3 wo, float3 wi, float3& f_cos,
+                                          float& pdf) {
+  f_cos = f3(0.0f, 0.0f, 0.0f);
+  pdf = 0.0f;
+  const bool smooth = m.roughness <= 0.0f;
+  const float co = wo.z, ci = wi.z;
+  if (co <= 1e-5f) return;
+  if (wi.z > 0.0f) {
+    // same side: diffuse lobe plus rough reflection
+    if (ci <= 1e-5f) return;
+    const float3 wm = normalize(wo + wi);
+    const float4 ev = diel_event_probs(m, eta, co, fabsf(dot(wo, wm)));
+    const float macro_t = 1.0f - diel_fresnel(m, co, eta);
+    float3 f = m.base_color * (macro_t * (1.0f - m.transmission) * (1.0f / CUDART_PI_F));
+    float ps = 0.0f;
+    if (!smooth) {
+      const float d = ggx_d(fmaxf(wm.z, 0.0f), m.alpha);
+      const float g1o = smith_g1(co, m.alpha);
+      const float fm = diel_fresnel(m, fabsf(dot(wo, wm)), eta);
+      const float r = d * g1o * smith_g1(ci, m.alpha) * fm / fmaxf(4.0f * co * ci, 1e-10f);
+      f = f + f3(r, r, r);
+      ps = d * g1o / fmaxf(4.0f * co, 1e-6f);
+    }
+    f_cos = f * ci;
+    pdf = ev.y * ci * (1.0f / CUDART_PI_F) + ev.x * ps;
+  } else {
+    // opposite side: rough transmission only
+    if (smooth || ci >= -1e-5f) return;
+    const float3 wm = diel_half_t(wo, wi, eta);
+    const float im = dot(wi, wm), om = dot(wo, wm);
+    if (im * ci < 0.0f || om * co < 0.0f) return;
+    const float den = im + om / eta;
+    const float d = ggx_d(fmaxf(wm.z, 0.0f), m.alpha);
+    const float g = smith_g1(co, m.alpha) * smith_g1(fabsf(ci), m.alpha);
+    const float tr = 1.0f - diel_fresnel(m, fabsf(om), eta);
+    const float ft = d * tr * g * fabsf(im * om / fmaxf(fabsf(den * den * ci * co), 1e-10f)) / (eta * eta);
+    f_cos = m.base_color * (m.transmission * ft * fabsf(ci));
+    const float4 ev = diel_event_probs(m, eta, co, fabsf(om));
+    pdf = ev.z * vndf_pdf(m, wo, wm) * fabsf(im) / fmaxf(den * den, 1e-10f);
+  }
+}
+// Finite-support BSDF of either family (0 for delta-only surfaces).
+__device__ __forceinline__ void bsdf_eval(const Material& m, float eta, float3 wo, float3 wi, float3& f_cos,
+                                          float& pdf) {
+  if (m.kind == kDielectric) diel_eval(m, eta, wo, wi, f_cos, pdf);
+  else opaque_eval(m, wo, wi, f_cos, pdf);
+}
+__device__ __forceinline__ bool has_finite_support(const Material& m) {
+  return m.kind != kDielectric || m.roughness > 0.0f || m.transmission < 1.0f;
+}
+
+// One BSDF sample.  wo in the local frame (+z side), eta = n_t / n_i.
+struct BsdfSample {
+  float3 wi;       // local frame
+  float3 weight;   // f * |cos| / pdf
+  float pdf;       // event density (for delta events the discrete probability)
+  bool delta;
+  bool valid;
+};
+__device__ __forceinline__ BsdfSample sample_bsdf(const Material& m, float eta, float3 wo, uint32_t& rng) {
+  BsdfSample s;
+  s.wi = f3(0.0f, 0.0f, 1.0f);
+  s.weight = f3(0.0f, 0.0f, 0.0f);
+  s.pdf = 0.0f;
+  s.delta = false;
+  s.valid = false;
+  if (m.kind != kDielectric) {
+    const float sp = opaque_spec_prob(m, opaque_f0(m), fmaxf(wo.z, 0.0f));
+    const bool spec = rand01(rng) < sp;
+    const float u1 = rand01(rng), u2 = rand01(rng);
+    if (spec) {
+      const float3 h = ggx_vndf(wo, m.alpha, u1, u2);
+      s.wi = h * (2.0f * dot(wo, h)) - wo;
+    } else {
+      s.wi = cosine_sample(u1, u2);
+    }
+  } else {
+    const bool smooth = m.roughness <= 0.0f;
+    float3 wm = f3(0.0f, 0.0f, 1.0f);
+    if (!smooth) {
+      const float u1 = rand01(rng), u2 = rand01(rng);
+      wm = ggx_vndf(wo, m.alpha, u1, u2);
+    }
+    // refraction about wm (transmitted direction of the incoming ray -wo)
+    const float ci = dot(wo, wm);
+    const float k = 1.0f - (1.0f - ci * ci) / (eta * eta);
+    const bool can_refract = k >= 0.0f;
+    const float fm = can_refract ? diel_fresnel(m, fabsf(ci), eta) : 1.0f;
+    const float macro_t = 1.0f - diel_fresnel(m, wo.z, eta);
+    const float4 ev = diel_events(clamp01(macro_t * (1.0f - m.transmission)), fm,
+                                  m.transmission * clamp01(1.0f - fm));
+    const bool diffuse = rand01(rng) < ev.y;
+    bool refl = false;
+    if (!diffuse) refl = rand01(rng) < ev.w;
+    if (diffuse) {
+      const float u1 = rand01(rng), u2 = rand01(rng);
+      s.wi = cosine_sample(u1, u2);
+    } else if (refl) {
+      s.wi = wm * (2.0f * ci) - wo;
+      if (smooth) {
+        s.pdf = ev.x;
+        s.weight = f3(fm, fm, fm) * (1.0f / fmaxf(ev.x, 1e-10f));
+        s.delta = true;
+        s.valid = ev.x > 0.0f;
+        return s;
+      }
+      if (s.wi.z <= 1e-5f) return s;
+    } else {
+      if (!can_refract) return s;
+      s.wi = normalize(wo * (-1.0f / eta) + wm * (ci / eta - sqrtf(k)));
+      if (smooth) {
+        s.pdf = ev.z;
+        s.weight = m.base_color * (m.transmission * (1.0f - fm) / (eta * eta) / fmaxf(ev.z, 1e-10f));
+        s.delta = true;
+        s.valid = ev.z > 0.0f;
+        return s;
+      }
+      if (s.wi.z >= -1e-5f) return s;
+    }
+  }
+  // continuous events: the full BSDF over the marginal density
+  float3 fc;
+  float pdf;
+  bsdf_eval(m, eta, wo, s.wi, fc, pdf);
+  if (!(pdf > 0.0f) || fabsf(s.wi.z) <= 1e-8f) return s;
+  s.pdf = pdf;
+  s.weight = fc * (1.0f / pdf);
+  s.valid = maxc(s.weight) > 0.0f;
+  return s;
 }
 
 }  // namespace pt

@@ -284,9 +284,9 @@ __global__ void k_scatter(WaveBuffers w, int cur) {
 // (position, outgoing direction, normal facing it, roughness, diffuse albedo,
 // specular albedo) as the radiance cache's 16-float record.
 __device__ __forceinline__ void nrc_features(const Material& m, float3 P, float3 wo, float3 n, float4 (&q)[4]) {
-  const float3 zero = f3(0.0f, 0.0f, 0.0f);
-  const float3 dif = m.kind == kLambert ? m.base_color : zero;
-  const float3 spe = m.kind == kConductor ? m.base_color : (m.kind == kDielectric ? f3(1.0f, 1.0f, 1.0f) : zero);
+  const bool diel = m.kind == kDielectric;
+  const float3 dif = m.base_color * (diel ? 1.0f - m.transmission : 1.0f - m.metallic);
+  const float3 spe = diel ? f3(1.0f, 1.0f, 1.0f) : opaque_f0(m);
   q[0] = make_float4(P.x, P.y, P.z, wo.x);
   q[1] = make_float4(wo.y, wo.z, n.x, n.y);
   q[2] = make_float4(n.z, m.roughness, dif.x, dif.y);
@@ -413,19 +413,21 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
         if (query) {
           // the path ends in the cache: its scattered radiance is predicted here
           qt = make_float4(__uint_as_float(path), T.x, T.y, T.z);
-        } else if (m.kind != kDielectric) {
-          // ---- next-event estimation
-          if (sc.n_light_entries > 0) {
+        } else {
+          const float eta = front ? m.ior : 1.0f / m.ior;  // n_t / n_i for light arriving along wo
+          // ---- next-event estimation (surfaces with a finite BSDF lobe)
+          if (sc.n_light_entries > 0 && has_finite_support(m)) {
             const LightSample ls = sample_light(sc, P, rng);
             if (ls.valid) {
               float3 fc;
               float pb;
-              bsdf_eval(m, wol, to_local(ls.wi, tb, bb, n), fc, pb);
+              const float3 wil = to_local(ls.wi, tb, bb, n);
+              bsdf_eval(m, eta, wol, wil, fc, pb);
               if (maxc(fc) > 0.0f) {
                 const float wgt = (ls.delta || last) ? 1.0f : power_heuristic(ls.pdf, pb);
                 const float3 c = T * fc * ls.Le * (wgt / ls.pdf);
                 if (maxc(c) > 0.0f) {
-                  const float3 so = P + n * off;
+                  const float3 so = P + n * (wil.z > 0.0f ? off : -off);
                   const float tmax = isinf(ls.dist) ? CUDART_INF_F : ls.dist * (1.0f - 1e-4f);
                   sh_o = make_float4(so.x, so.y, so.z, 0.0f);
                   sh_d = make_float4(ls.wi.x, ls.wi.y, ls.wi.z, tmax);
@@ -437,60 +439,17 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
           }
           // ---- BSDF sample
           if (!last) {
-            float3 wil = f3(0.0f, 0.0f, 0.0f), wgt = f3(0.0f, 0.0f, 0.0f);
-            float pdf = 0.0f;
-            const float u1 = rand01(rng), u2 = rand01(rng);
-            if (m.kind == kLambert) {
-              const float r = sqrtf(u1), phi = 2.0f * CUDART_PI_F * u2;
-              wil = f3(r * cosf(phi), r * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - u1)));
-              pdf = wil.z / CUDART_PI_F;
-              wgt = m.base_color;
-            } else {
-              const float3 hl = ggx_vndf(wol, m.alpha, u1, u2);
-              const float oh = dot(wol, hl);
-              wil = hl * (2.0f * oh) - wol;
-              if (wil.z > 0.0f && oh > 0.0f) {
-                pdf = ggx_d(hl.z, m.alpha) * ggx_g1(wol.z, m.alpha) / (4.0f * wol.z);
-                wgt = schlick(m.base_color, oh) * ggx_g1(wil.z, m.alpha);
-              }
-            }
-            if (pdf > 0.0f && maxc(wgt) > 0.0f) {
-              const float3 wi = to_world(wil, tb, bb, n);
-              T = T * wgt;
+            const BsdfSample bs = sample_bsdf(m, eta, wol, rng);
+            if (bs.valid) {
+              const float3 wi = to_world(bs.wi, tb, bb, n);
+              T = T * bs.weight;
               alive = true;
-              const float3 no = P + n * off;
+              const float3 no = P + n * (bs.wi.z > 0.0f ? off : -off);
               next_o = make_float4(no.x, no.y, no.z, 0.0f);
               next_d = make_float4(wi.x, wi.y, wi.z, CUDART_INF_F);
-              next_state = make_uint4(path, 0u, 0u, __float_as_uint(pdf));
+              next_state = make_uint4(path, 0u, bs.delta ? 1u : 0u, __float_as_uint(bs.pdf));
             }
           }
-        } else if (!last) {
-          // ---- smooth dielectric: Fresnel-partitioned reflection / refraction
-          const float eta = front ? m.ior : 1.0f / m.ior;  // n_t / n_i
-          const float cosi = wol.z;
-          const float F = represented_bernoulli(fr_dielectric(cosi, eta));
-          float3 wi;
-          float3 wgt = f3(1.0f, 1.0f, 1.0f);
-          bool reflect = rand01(rng) < F;
-          if (!reflect) {
-            const float sin2t = fmaxf(0.0f, 1.0f - cosi * cosi) / (eta * eta);
-            if (sin2t >= 1.0f) {
-              reflect = true;  // unreachable when F == 1 (total internal reflection)
-            } else {
-              const float cost = sqrtf(1.0f - sin2t);
-              wi = d * (1.0f / eta) + n * (cosi / eta - cost);
-              wi = normalize(wi);
-              wgt = f3(1.0f, 1.0f, 1.0f) * (1.0f / (eta * eta));  // radiance scales by (n_i / n_t)^2
-            }
-          }
-          if (reflect) wi = d + n * (2.0f * cosi);
-          T = T * wgt;
-          const float side = reflect ? 1.0f : -1.0f;
-          const float3 no = P + n * (off * side);
-          alive = true;
-          next_o = make_float4(no.x, no.y, no.z, 0.0f);
-          next_d = make_float4(wi.x, wi.y, wi.z, CUDART_INF_F);
-          next_state = make_uint4(path, 0u, 1u, 0u);
         }
         // ---- Russian roulette
         if (alive && bounce > 2) {

@@ -114,9 +114,21 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     m.base_color = make_float3(d.base_color[0], d.base_color[1], d.base_color[2]);
     m.roughness = d.roughness;
     m.emission = make_float3(d.emission[0], d.emission[1], d.emission[2]);
-    m.ior = d.ior > 0.0f ? d.ior : 1.5f;
-    m.kind = d.transmission > 0.0f ? pt::kDielectric
-                                   : (d.metallic >= 0.5f ? pt::kConductor : pt::kLambert);
+    auto unit = [&](float v, const char* what) {
+      if (!(v >= 0.0f && v <= 1.0f))
+        fail(VT_ERR_RANGE, "material " + std::to_string(i) + ": " + what + " must be in [0, 1]");
+      return v;
+    };
+    unit(d.roughness, "roughness");
+    m.metallic = unit(d.metallic, "metallic");
+    m.transmission = unit(d.transmission, "transmission");
+    m.specular = unit(d.specular_intensity, "specular_intensity");
+    if (!(d.ior >= 0.0f) || !std::isfinite(d.ior)) fail(VT_ERR_RANGE, "material " + std::to_string(i) + ": ior must be >= 0");
+    m.ior = d.ior > 0.0f ? std::max(d.ior, 1.0f) : 1.5f;  // materialPacking.ts:130-131 (0 here: the 1.5 default)
+    const float ratio = (m.ior - 1.0f) / (m.ior + 1.0f);
+    m.f0_ior = ratio * ratio * m.specular;
+    m.kind = (d.transmission > 0.0f && d.metallic == 0.0f) ? pt::kDielectric
+                                                           : (d.metallic > 0.0f ? pt::kMetal : pt::kOpaque);
     m.alpha = std::max(d.roughness * d.roughness, 1e-3f);
     m.emissive = (d.emission[0] > 0.0f || d.emission[1] > 0.0f || d.emission[2] > 0.0f) ? 1u : 0u;
     if (d.flags & ~3u) fail(VT_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has unknown flags");
@@ -133,8 +145,12 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
       m.roughness = 1.0f;
       m.emission = make_float3(r.radiance[0], r.radiance[1], r.radiance[2]);
       m.ior = 1.5f;
-      m.kind = pt::kLambert;
+      m.kind = pt::kOpaque;
       m.alpha = 1.0f;
+      m.metallic = 0.0f;
+      m.transmission = 0.0f;
+      m.specular = 0.0f;  // a light, not a surface: nothing is reflected
+      m.f0_ior = 0.0f;
       m.emissive = (r.radiance[0] > 0.0f || r.radiance[1] > 0.0f || r.radiance[2] > 0.0f) ? 1u : 0u;
       m.flags = VT_MATERIAL_SINGLE_SIDED | VT_MATERIAL_NO_SHADOW;
       const uint32_t mi = (uint32_t)mats.size();

@@ -30,7 +30,7 @@ class _EngineOptions(ctypes.Structure):
 class _MaterialDesc(ctypes.Structure):
     _fields_ = [("base_color", ctypes.c_float * 3), ("roughness", ctypes.c_float), ("metallic", ctypes.c_float),
                 ("transmission", ctypes.c_float), ("ior", ctypes.c_float), ("emission", ctypes.c_float * 3),
-                ("flags", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32), ("specular_intensity", ctypes.c_float)]
 
 
 class _MeshDesc(ctypes.Structure):
@@ -102,8 +102,12 @@ class _EngineStats(ctypes.Structure):
 # ---------------------------------------------------------------- scene types
 @dataclass
 class Material:
-    """core Material subset: transmission > 0 -> smooth dielectric, metallic >= 0.5 ->
-    GGX conductor, otherwise Lambert.  emission is front-face radiance."""
+    """core MaterialSpec subset with the reference's base BSDF.  transmission > 0
+    with metallic 0: dielectric interface (delta at roughness 0, rough GGX
+    otherwise); anything else opaque: Lambert diffuse under a GGX specular layer
+    (F0 = mix(specular_intensity * ((ior-1)/(ior+1))^2, base_color, metallic),
+    Kulla-Conty multiple scattering).  specular_intensity=0 with metallic 0 is a
+    pure Lambertian.  emission is front-face radiance."""
     base_color: Sequence[float] = (0.8, 0.8, 0.8)
     roughness: float = 1.0
     metallic: float = 0.0
@@ -112,6 +116,7 @@ class Material:
     emission: Sequence[float] = (0.0, 0.0, 0.0)
     double_sided: bool = True   # False: back-face hits are skipped by every ray
     cast_shadow: bool = True    # False: shadow rays pass through (castShadow: false)
+    specular_intensity: float = 1.0  # KHR_materials_specular factor (MaterialSpec.specularIntensity)
 
     @property
     def flags(self) -> int:
@@ -245,7 +250,7 @@ def _marshal_scene(scene: "Scene"):
     mats = (_MaterialDesc * max(1, len(scene.materials)))()
     for i, m in enumerate(scene.materials):
         mats[i] = _MaterialDesc((ctypes.c_float * 3)(*m.base_color), m.roughness, m.metallic, m.transmission,
-                                m.ior, (ctypes.c_float * 3)(*m.emission), m.flags)
+                                m.ior, (ctypes.c_float * 3)(*m.emission), m.flags, m.specular_intensity)
     pls = (_PointLightDesc * max(1, len(scene.point_lights)))()
     for i, l in enumerate(scene.point_lights):
         pls[i] = _PointLightDesc((ctypes.c_float * 3)(*l.position), (ctypes.c_float * 3)(*l.intensity))

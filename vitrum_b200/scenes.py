@@ -145,12 +145,12 @@ def box_room(wall_cells: int = 128, box_cells: int = 64):
     Returns (engine.Scene, engine.Camera) for a 40 degree pinhole camera."""
     from .engine import Camera, Material, Mesh, Scene
     mats = [
-        Material(base_color=(0.75, 0.75, 0.75)),                       # 0 grey walls
-        Material(base_color=(0.63, 0.06, 0.05)),                       # 1 left wall
-        Material(base_color=(0.14, 0.45, 0.09)),                       # 2 right wall
-        Material(base_color=(0.9, 0.85, 0.6), roughness=0.2, metallic=1.0),  # 3 GGX conductor
-        Material(base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.5),    # 4 dielectric
-        Material(base_color=(0.0, 0.0, 0.0), emission=(15.0, 15.0, 15.0)),  # 5 emitter
+        Material(base_color=(0.75, 0.75, 0.75), specular_intensity=0.0),        # 0 grey walls (Lambertian)
+        Material(base_color=(0.63, 0.06, 0.05), specular_intensity=0.0),        # 1 left wall
+        Material(base_color=(0.14, 0.45, 0.09), specular_intensity=0.0),        # 2 right wall
+        Material(base_color=(0.9, 0.85, 0.6), roughness=0.2, metallic=1.0),    # 3 GGX conductor
+        Material(base_color=(1.0, 1.0, 1.0), roughness=0.0, transmission=1.0, ior=1.5),  # 4 smooth dielectric
+        Material(base_color=(0.0, 0.0, 0.0), emission=(15.0, 15.0, 15.0), specular_intensity=0.0),  # 5 emitter
     ]
     n = wall_cells
     meshes = []
@@ -272,12 +272,12 @@ def instanced_cloud(n_instances: int = 1024, seed: int = 3, n_points: int = 32, 
     mats, insts = [], []
     for i in range(n):
         if kind[i] < 0.5:
-            mats.append(Material(base_color=tuple(0.1 + 0.8 * u[i, 9:12])))
+            mats.append(Material(base_color=tuple(0.1 + 0.8 * u[i, 9:12]), specular_intensity=0.0))
         elif kind[i] < 0.8:
             mats.append(Material(base_color=tuple(0.5 + 0.45 * u[i, 9:12]), roughness=0.05 + 0.55 * u[i, 12],
                                  metallic=1.0))
         else:
-            mats.append(Material(base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.3 + 0.4 * u[i, 12]))
+            mats.append(Material(base_color=(1.0, 1.0, 1.0), roughness=0.0, transmission=1.0, ior=1.3 + 0.4 * u[i, 12]))
         M = np.eye(4)
         M[:3, :3] = rot[i] * scale[i]
         M[:3, 3] = trans[i]
