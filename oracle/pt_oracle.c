@@ -266,15 +266,17 @@ static float ggx_albedo_avg(float r) {
   float tr = fr - (float)r0;
   return fminf(fmaxf(ggx_eavg_tab[r0] + (ggx_eavg_tab[r1] - ggx_eavg_tab[r0]) * tr, 0.3f), 1.0f);
 }
+/* F_avg^2 E_avg / (1 - F_avg (1 - E_avg)) * (1 - E(mu_o)) (1 - E(mu_i)) / (pi (1 - E_avg)) */
 static v3 ggx_multiscatter(v3 f0, float r, float nv, float nl) {
   float eavg = ggx_albedo_avg(r), miss = 1.0f - eavg;
   if (miss < 1e-4f) return V(0, 0, 0);
   float eo = ggx_albedo(nv, r), ei = ggx_albedo(nl, r);
   v3 favg = add(f0, scl(sub(V(1, 1, 1), f0), 1.0f / 21.0f));
   v3 fms = scl(mul(favg, favg), eavg);
-  float shape = (1.0f - eo) * (1.0f - ei) / fmaxf(PI_F * miss, 1e-6f);
-  return V(fms.x / fmaxf(1.0f - favg.x * miss, 1e-4f) * shape, fms.y / fmaxf(1.0f - favg.y * miss, 1e-4f) * shape,
-           fms.z / fmaxf(1.0f - favg.z * miss, 1e-4f) * shape);
+  float shape_o = (1.0f - eo) / fmaxf(PI_F * miss, 1e-6f);
+  v3 mso = V(fms.x / fmaxf(1.0f - favg.x * miss, 1e-4f) * shape_o, fms.y / fmaxf(1.0f - favg.y * miss, 1e-4f) * shape_o,
+             fms.z / fmaxf(1.0f - favg.z * miss, 1e-4f) * shape_o);
+  return scl(mso, 1.0f - ei);
 }
 static float ggx_d(float nh, float a) {
   float a2 = a * a, n2 = clamp01f(nh * nh), d = (1.0f - n2) + n2 * a2;

@@ -134,8 +134,10 @@ __device__ __forceinline__ float pow5(float x) {
   return x2 * x2 * x;
 }
 
-static __constant__ float kGgxE[VT_GGX_ALBEDO_DIM * VT_GGX_ALBEDO_DIM] = {VT_GGX_E_VALUES};
-static __constant__ float kGgxEavg[VT_GGX_ALBEDO_DIM] = {VT_GGX_EAVG_VALUES};
+// global memory read through L1 (lanes index the tables divergently, which the
+// constant cache would serialise)
+static __device__ const float kGgxE[VT_GGX_ALBEDO_DIM * VT_GGX_ALBEDO_DIM] = {VT_GGX_E_VALUES};
+static __device__ const float kGgxEavg[VT_GGX_ALBEDO_DIM] = {VT_GGX_EAVG_VALUES};
 
 // Bilinear E_ss(mu, roughness), clamped to [0.02, 1] (ggxDirectionalAlbedo, material.wgsl.ts:2873-2891)
 __device__ __forceinline__ float ggx_albedo(float mu, float r) {
@@ -144,8 +146,10 @@ __device__ __forceinline__ float ggx_albedo(float mu, float r) {
   const int r0 = (int)floorf(fr), m0 = (int)floorf(fm);
   const int r1 = min(r0 + 1, kD - 1), m1 = min(m0 + 1, kD - 1);
   const float tr = fr - (float)r0, tm = fm - (float)m0;
-  const float e0 = kGgxE[r0 * kD + m0] + (kGgxE[r0 * kD + m1] - kGgxE[r0 * kD + m0]) * tm;
-  const float e1 = kGgxE[r1 * kD + m0] + (kGgxE[r1 * kD + m1] - kGgxE[r1 * kD + m0]) * tm;
+  const float e00 = __ldg(kGgxE + r0 * kD + m0), e01 = __ldg(kGgxE + r0 * kD + m1);
+  const float e10 = __ldg(kGgxE + r1 * kD + m0), e11 = __ldg(kGgxE + r1 * kD + m1);
+  const float e0 = e00 + (e01 - e00) * tm;
+  const float e1 = e10 + (e11 - e10) * tm;
   return fminf(fmaxf(e0 + (e1 - e0) * tr, 0.02f), 1.0f);
 }
 // Linear E_avg(roughness), clamped to [0.3, 1] (ggxAverageAlbedo, material.wgsl.ts:2894-2901)
@@ -154,21 +158,24 @@ __device__ __forceinline__ float ggx_albedo_avg(float r) {
   const float fr = clamp01(r) * (float)(kD - 1);
   const int r0 = (int)floorf(fr), r1 = min(r0 + 1, kD - 1);
   const float tr = fr - (float)r0;
-  return fminf(fmaxf(kGgxEavg[r0] + (kGgxEavg[r1] - kGgxEavg[r0]) * tr, 0.3f), 1.0f);
+  const float a0 = __ldg(kGgxEavg + r0), a1 = __ldg(kGgxEavg + r1);
+  return fminf(fmaxf(a0 + (a1 - a0) * tr, 0.3f), 1.0f);
 }
 // Kulla-Conty multiple-scattering BRDF (no cosine), f0 tinting the extra
-// bounces through F_avg = f0 + (1 - f0) / 21 (material.wgsl.ts:2903-2931)
-__device__ __forceinline__ float3 ggx_multiscatter(float3 f0, float r, float nv, float nl) {
+// bounces through F_avg = f0 + (1 - f0) / 21 (material.wgsl.ts:2903-2931):
+//   f_ms = F_avg^2 E_avg / (1 - F_avg (1 - E_avg)) * (1 - E(mu_o)) (1 - E(mu_i)) / (pi (1 - E_avg)).
+// Everything but the (1 - E(mu_i)) factor depends on the outgoing side only.
+__device__ __forceinline__ float3 ggx_multiscatter_o(float3 f0, float r, float nv) {
   const float eavg = ggx_albedo_avg(r);
   const float miss = 1.0f - eavg;
   if (miss < 1e-4f) return f3(0.0f, 0.0f, 0.0f);
-  const float eo = ggx_albedo(nv, r), ei = ggx_albedo(nl, r);
+  const float eo = ggx_albedo(nv, r);
   const float3 favg = f0 + (f3(1.0f, 1.0f, 1.0f) - f0) * (1.0f / 21.0f);
   const float3 den = f3(fmaxf(1.0f - favg.x * miss, 1e-4f), fmaxf(1.0f - favg.y * miss, 1e-4f),
                         fmaxf(1.0f - favg.z * miss, 1e-4f));
   const float3 fms = favg * favg * eavg;
-  const float shape = (1.0f - eo) * (1.0f - ei) / fmaxf(CUDART_PI_F * miss, 1e-6f);
-  return f3(fms.x / den.x, fms.y / den.y, fms.z / den.z) * shape;
+  const float shape_o = (1.0f - eo) / fmaxf(CUDART_PI_F * miss, 1e-6f);
+  return f3(fms.x / den.x, fms.y / den.y, fms.z / den.z) * shape_o;
 }
 
 // GGX distribution in the cancellation-free form (ggxD, material.wgsl.ts:2797-2804)
@@ -215,29 +222,41 @@ __device__ __forceinline__ float3 opaque_fresnel(const Material& m, float3 f0, f
   const float f90 = m.specular + (1.0f - m.specular) * m.metallic;
   return f0 + (f3(f90, f90, f90) - f0) * pow5(clamp01(1.0f - c));
 }
-// probability of sampling the specular lobe (brdfFiniteBaseLobeWeights)
-__device__ __forceinline__ float opaque_spec_prob(const Material& m, float3 f0, float nv) {
-  const float fl = luminance(clamp01(opaque_fresnel(m, f0, nv)));
-  return represented_bernoulli(fminf(fmaxf(0.04f + 0.92f * fmaxf(fl, m.metallic), 0.04f), 0.96f));
+// Per-vertex terms of the opaque BSDF that depend on the material and wo
+// only, shared by the NEE evaluation and the BSDF sample of one vertex.
+struct OpaqueSide {
+  float3 f0;
+  float nv;    // max(wo.z, 0)
+  float sp;    // probability of the specular lobe (brdfFiniteBaseLobeWeights)
+  float g1o;   // Smith G1 of wo
+  float3 mso;  // multiple-scattering lobe without its (1 - E(mu_i)) factor
+};
+__device__ __forceinline__ OpaqueSide opaque_side(const Material& m, float3 wo) {
+  OpaqueSide o;
+  o.f0 = opaque_f0(m);
+  o.nv = fmaxf(wo.z, 0.0f);
+  const float fl = luminance(clamp01(opaque_fresnel(m, o.f0, o.nv)));
+  o.sp = represented_bernoulli(fminf(fmaxf(0.04f + 0.92f * fmaxf(fl, m.metallic), 0.04f), 0.96f));
+  o.g1o = smith_g1(o.nv, m.alpha);
+  o.mso = ggx_multiscatter_o(clamp01(o.f0), m.roughness, o.nv);
+  return o;
 }
 // BSDF * cos(wi) and the marginal sampling density; wo, wi in the local frame (n = +z)
-__device__ __forceinline__ void opaque_eval(const Material& m, float3 wo, float3 wi, float3& f_cos, float& pdf) {
+__device__ __forceinline__ void opaque_eval(const Material& m, const OpaqueSide& o, float3 wo, float3 wi,
+                                            float3& f_cos, float& pdf) {
   f_cos = f3(0.0f, 0.0f, 0.0f);
   pdf = 0.0f;
-  const float nv = fmaxf(wo.z, 0.0f), nl = fmaxf(wi.z, 0.0f);
+  const float nv = o.nv, nl = fmaxf(wi.z, 0.0f);
   if (nv <= 1e-5f || nl <= 1e-5f) return;
   const float3 h = normalize(wi + wo);
   const float nh = fmaxf(h.z, 0.0f), vh = fmaxf(dot(wo, h), 0.0f);
-  const float3 f0 = opaque_f0(m);
-  const float3 F = clamp01(opaque_fresnel(m, f0, vh));
+  const float3 F = clamp01(opaque_fresnel(m, o.f0, vh));
   const float3 kd = (f3(1.0f, 1.0f, 1.0f) - F) * (1.0f - m.metallic);
   const float d = ggx_d(nh, m.alpha);
-  const float g1o = smith_g1(nv, m.alpha);
-  const float3 spec = F * (d * g1o * smith_g1(nl, m.alpha) / fmaxf(4.0f * nv * nl, 1e-6f));
-  const float3 ms = ggx_multiscatter(clamp01(f0), m.roughness, nv, nl);
+  const float3 spec = F * (d * o.g1o * smith_g1(nl, m.alpha) / fmaxf(4.0f * nv * nl, 1e-6f));
+  const float3 ms = o.mso * (1.0f - ggx_albedo(nl, m.roughness));
   f_cos = (kd * m.base_color * (1.0f / CUDART_PI_F) + spec + ms) * nl;
-  const float sp = opaque_spec_prob(m, f0, nv);
-  pdf = (1.0f - sp) * nl * (1.0f / CUDART_PI_F) + sp * d * g1o / fmaxf(4.0f * nv, 1e-6f);
+  pdf = (1.0f - o.sp) * nl * (1.0f / CUDART_PI_F) + o.sp * d * o.g1o / fmaxf(4.0f * nv, 1e-6f);
 }
 
 // ---- dielectric family
@@ -339,10 +358,21 @@ __device__ __forceinline__ void diel_eval(const Material& m, float eta, float3 w
   }
 }
 // Finite-support BSDF of either family (0 for delta-only surfaces).
-__device__ __forceinline__ void bsdf_eval(const Material& m, float eta, float3 wo, float3 wi, float3& f_cos,
-                                          float& pdf) {
+// `o` is opaque_side(m, wo) for the opaque family (unused for dielectrics).
+__device__ __forceinline__ void bsdf_eval(const Material& m, const OpaqueSide& o, float eta, float3 wo, float3 wi,
+                                          float3& f_cos, float& pdf) {
   if (m.kind == kDielectric) diel_eval(m, eta, wo, wi, f_cos, pdf);
-  else opaque_eval(m, wo, wi, f_cos, pdf);
+  else opaque_eval(m, o, wo, wi, f_cos, pdf);
+}
+__device__ __forceinline__ OpaqueSide surface_side(const Material& m, float3 wo) {
+  if (m.kind != kDielectric) return opaque_side(m, wo);
+  OpaqueSide o;
+  o.f0 = f3(0.0f, 0.0f, 0.0f);
+  o.nv = fmaxf(wo.z, 0.0f);
+  o.sp = 0.0f;
+  o.g1o = 0.0f;
+  o.mso = f3(0.0f, 0.0f, 0.0f);
+  return o;
 }
 __device__ __forceinline__ bool has_finite_support(const Material& m) {
   return m.kind != kDielectric || m.roughness > 0.0f || m.transmission < 1.0f;
@@ -356,7 +386,8 @@ struct BsdfSample {
   bool delta;
   bool valid;
 };
-__device__ __forceinline__ BsdfSample sample_bsdf(const Material& m, float eta, float3 wo, uint32_t& rng) {
+__device__ __forceinline__ BsdfSample sample_bsdf(const Material& m, const OpaqueSide& o, float eta, float3 wo,
+                                                  uint32_t& rng) {
   BsdfSample s;
   s.wi = f3(0.0f, 0.0f, 1.0f);
   s.weight = f3(0.0f, 0.0f, 0.0f);
@@ -364,8 +395,7 @@ __device__ __forceinline__ BsdfSample sample_bsdf(const Material& m, float eta, 
   s.delta = false;
   s.valid = false;
   if (m.kind != kDielectric) {
-    const float sp = opaque_spec_prob(m, opaque_f0(m), fmaxf(wo.z, 0.0f));
-    const bool spec = rand01(rng) < sp;
+    const bool spec = rand01(rng) < o.sp;
     const float u1 = rand01(rng), u2 = rand01(rng);
     if (spec) {
       const float3 h = ggx_vndf(wo, m.alpha, u1, u2);
@@ -420,7 +450,7 @@ __device__ __forceinline__ BsdfSample sample_bsdf(const Material& m, float eta, 
   // continuous events: the full BSDF over the marginal density
   float3 fc;
   float pdf;
-  bsdf_eval(m, eta, wo, s.wi, fc, pdf);
+  bsdf_eval(m, o, eta, wo, s.wi, fc, pdf);
   if (!(pdf > 0.0f) || fabsf(s.wi.z) <= 1e-8f) return s;
   s.pdf = pdf;
   s.weight = fc * (1.0f / pdf);

@@ -294,7 +294,9 @@ __device__ __forceinline__ void nrc_features(const Material& m, float3 P, float3
 }
 
 // ---------------------------------------------------------------- shade
-__global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
+// 8 resident blocks per SM (64 registers, some spilled to L1): the kernel is
+// load-latency bound, and occupancy beats spill-free code here.
+__global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
   const int nxt = cur ^ 1;
   const uint32_t n = w.counters[cur];
   const uint32_t lane = threadIdx.x & 31u;
@@ -415,6 +417,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
           qt = make_float4(__uint_as_float(path), T.x, T.y, T.z);
         } else {
           const float eta = front ? m.ior : 1.0f / m.ior;  // n_t / n_i for light arriving along wo
+          const OpaqueSide os = surface_side(m, wol);
           // ---- next-event estimation (surfaces with a finite BSDF lobe)
           if (sc.n_light_entries > 0 && has_finite_support(m)) {
             const LightSample ls = sample_light(sc, P, rng);
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
               float3 fc;
               float pb;
               const float3 wil = to_local(ls.wi, tb, bb, n);
-              bsdf_eval(m, eta, wol, wil, fc, pb);
+              bsdf_eval(m, os, eta, wol, wil, fc, pb);
               if (maxc(fc) > 0.0f) {
                 const float wgt = (ls.delta || last) ? 1.0f : power_heuristic(ls.pdf, pb);
                 const float3 c = T * fc * ls.Le * (wgt / ls.pdf);
@@ -439,7 +442,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sc0, FrameView f, WaveB
           }
           // ---- BSDF sample
           if (!last) {
-            const BsdfSample bs = sample_bsdf(m, eta, wol, rng);
+            const BsdfSample bs = sample_bsdf(m, os, eta, wol, rng);
             if (bs.valid) {
               const float3 wi = to_world(bs.wi, tb, bb, n);
               T = T * bs.weight;
