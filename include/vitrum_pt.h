@@ -192,10 +192,42 @@ typedef struct vt_mesh_desc {
   uint32_t material;        /* index into vt_scene_desc.materials */
 } vt_mesh_desc;
 
+/* Point light (core PointEmitter, core/src/scene/emitters.ts:67-72) with the
+ * reference's defaults: inverse-square falloff, no range cutoff.  A point light
+ * with another falloff or a range is a vt_spot_light_desc with angle pi. */
 typedef struct vt_point_light_desc {
   float position[3];
   float intensity[3];       /* radiant intensity; irradiance falls off as 1/d^2 */
 } vt_point_light_desc;
+
+/* Spot light (core SpotEmitter, core/src/scene/emitters.ts:74-85; NEE as
+ * pt-webgpu/src/wgsl/pathTrace/kernel.wgsl.ts:1344-1397): a delta light at
+ * `position` emitting `intensity` into the cone of half-angle `angle` around
+ * `direction`, smoothly from the inner cone angle * (1 - penumbra) to the outer
+ * edge, scaled by 1/d^decay (decay 0: none) and, with distance > 0, by
+ * clamp(1 - (d / distance)^4, 0, 1) (pointSpotDistanceAttenuation,
+ * material.wgsl.ts:2176-2204).  The reference's default decay is 2. */
+typedef struct vt_spot_light_desc {
+  float position[3];
+  float direction[3];       /* beam axis (normalised on input) */
+  float intensity[3];
+  float angle;              /* outer half-angle, radians, in (0, pi] */
+  float penumbra;           /* [0, 1] */
+  float distance;           /* range cutoff; 0 = none */
+  float decay;              /* falloff exponent >= 0 */
+} vt_spot_light_desc;
+
+/* Disc area light (core DiscAreaEmitter, emitters.ts:53-58): emits `radiance`
+ * from the side `normal` faces; sampled by the concentric map, hit
+ * analytically by BSDF rays (MIS), invisible to shadow rays and from behind,
+ * and not an occluder (pt-webgpu/src/scene/emitterPacking.ts:78-93,
+ * connect.wgsl.ts:390-450). */
+typedef struct vt_disc_light_desc {
+  float center[3];
+  float normal[3];
+  float radius;
+  float radiance[3];
+} vt_disc_light_desc;
 
 /* Directional light (sun): light travelling along `direction`.  With
  * angular_radius 0 a delta light of irradiance `irradiance` at normal
@@ -207,9 +239,10 @@ typedef struct vt_directional_light_desc {
   float angular_radius;     /* radians, < pi/2 */
 } vt_directional_light_desc;
 
-/* Rectangle light: corner + [0,1] edge_u + [0,1] edge_v, emitting `radiance`
- * from the side edge_u x edge_v faces; seen from behind and by shadow rays it
- * is transparent.  Packed as two emissive triangles (single-level scenes). */
+/* Rectangle light (core RectAreaEmitter, emitters.ts:60-65): corner + [0,1]
+ * edge_u + [0,1] edge_v, emitting `radiance` from the side edge_u x edge_v
+ * faces; an analytic emitter like vt_disc_light_desc (uniform area sampling,
+ * analytic BSDF-ray hits, never an occluder). */
 typedef struct vt_rect_light_desc {
   float corner[3];
   float edge_u[3];
@@ -246,6 +279,10 @@ typedef struct vt_scene_desc {
   size_t directional_light_count;
   const vt_rect_light_desc* rect_lights;
   size_t rect_light_count;
+  const vt_spot_light_desc* spot_lights;
+  size_t spot_light_count;
+  const vt_disc_light_desc* disc_lights;
+  size_t disc_light_count;
 } vt_scene_desc;
 
 /* Per-frame input (core FrameInput, core/src/frame.ts:91): camera matrices

@@ -12,6 +12,7 @@ code (file:line citations in that file's header).  ``liborc.so`` is built by
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -261,7 +262,7 @@ def _pt_lib():
         P = ctypes.c_void_p
         L.orc_pt_render.restype = ctypes.c_int
         L.orc_pt_render.argtypes = [P, ctypes.c_long, P, ctypes.c_long, P, P, ctypes.c_int, P, ctypes.c_long, P,
-                                    ctypes.c_long, P,
+                                    ctypes.c_long, P, ctypes.c_long, P,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                     ctypes.c_int, P, P, P, P, ctypes.c_long, P]
@@ -271,7 +272,7 @@ def _pt_lib():
 
 def flatten_scene(scene):
     """(positions (V,4) f32, indices (T,4) u32, tri_material u32, materials (M,12) f32,
-    points (P,6) f32, env (H,W,3) f32 or None, env_intensity) from an engine Scene."""
+    positional lights (P,16) f32, env (H,W,3) f32 or None, env_intensity) from an engine Scene."""
     pos, idx, tm = [], [], []
     base = 0
     for m in scene.meshes:
@@ -285,34 +286,53 @@ def flatten_scene(scene):
         idx.append(i4)
         tm.append(np.full(i.shape[0], m.material, np.uint32))
         base += p.shape[0]
-    rects = list(getattr(scene, "rect_lights", []))
-    mats = np.zeros((len(scene.materials) + len(rects), 12), np.float32)
+    mats = np.zeros((len(scene.materials), 12), np.float32)
     for k, m in enumerate(scene.materials):
         mats[k, 0:3] = m.base_color
         mats[k, 3:7] = (m.roughness, m.metallic, m.transmission, m.ior)
         mats[k, 7:10] = m.emission
         mats[k, 10] = (0 if getattr(m, "double_sided", True) else 1) | (0 if getattr(m, "cast_shadow", True) else 2)
         mats[k, 11] = getattr(m, "specular_intensity", 1.0)
-    # rectangle lights: two one-sided emissive triangles each, transparent to shadow rays
-    for j, r in enumerate(rects):
-        k = len(scene.materials) + j
-        mats[k, 3:7] = (1.0, 0.0, 0.0, 1.5)
-        mats[k, 7:10] = r.radiance
-        mats[k, 10] = 3
-        c, u, v = (np.asarray(x, np.float32) for x in (r.corner, r.edge_u, r.edge_v))
-        p4 = np.zeros((4, 4), np.float32)
-        for q, (a, b) in enumerate(((0, 0), (1, 0), (1, 1), (0, 1))):
-            p4[q, :3] = (c + np.float32(a) * u) + np.float32(b) * v
-        i4 = np.array([[0, 1, 2, 0], [0, 2, 3, 0]], np.uint32)
-        i4[:, :3] += base
-        pos.append(p4)
-        idx.append(i4)
-        tm.append(np.full(2, k, np.uint32))
-        base += 4
-    pts = np.array([[*l.position, *l.intensity] for l in scene.point_lights], np.float32).reshape(-1, 6)
+    pts = positional_lights(scene)
     env = None if scene.environment is None else np.ascontiguousarray(scene.environment.rgb, np.float32)
     ei = 1.0 if scene.environment is None else float(scene.environment.intensity)
     return np.concatenate(pos), np.concatenate(idx), np.concatenate(tm), mats, pts, env, ei
+
+
+def positional_lights(scene):
+    """(n, 16) float32, points then spots: position, 0, intensity, 0, axis, cos outer,
+    cos inner, range, decay, spot flag (points: no cone, no range, decay 2)."""
+    rows = []
+    for l in scene.point_lights:
+        rows.append([*l.position, 0, *l.intensity, 0, 0, 0, 0, -2, -1, 0, 2, 0])
+    for l in getattr(scene, "spot_lights", []):
+        d = np.asarray(l.direction, np.float32).astype(np.float64)
+        d = d / np.sqrt((d * d).sum())
+        outer = float(np.float32(l.angle))
+        inner = outer * (1.0 - float(np.float32(l.penumbra)))
+        rows.append([*l.position, 0, *l.intensity, 0, *d, math.cos(outer), math.cos(inner), l.distance, l.decay, 1])
+    return np.array(rows, np.float32).reshape(-1, 16)
+
+
+def area_lights(scene):
+    """(n, 16) float32, rectangles then discs: centre, shape (0 / 1), u half axis,
+    area, v half axis, 0, radiance, 0 (the emitting side is u x v)."""
+    rows = []
+    for r in getattr(scene, "rect_lights", []):
+        u = np.float32(0.5) * np.asarray(r.edge_u, np.float32)
+        v = np.float32(0.5) * np.asarray(r.edge_v, np.float32)
+        c = (np.asarray(r.corner, np.float32) + u) + v
+        cr = np.cross(u.astype(np.float64), v.astype(np.float64))
+        rows.append([*c, 0, *u, 4.0 * math.sqrt((cr * cr).sum()), *v, 0, *r.radiance, 0])
+    for dl in getattr(scene, "disc_lights", []):
+        n = np.asarray(dl.normal, np.float32).astype(np.float64)
+        n = n / math.sqrt((n * n).sum())
+        t = np.array([-n[2], 0.0, n[0]]) if abs(n[0]) > 0.9 else np.array([0.0, n[2], -n[1]])
+        t = t / math.sqrt((t * t).sum())
+        b = np.array([n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]])
+        rr = float(np.float32(dl.radius))
+        rows.append([*dl.center, 1, *(t * rr), math.pi * rr * rr, *(b * rr), 0, *dl.radiance, 0])
+    return np.array(rows, np.float32).reshape(-1, 16)
 
 
 def directional_lights(scene):
@@ -355,8 +375,10 @@ def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_bas
     ls = np.zeros((max(log_rays, 0), 8), np.float32)
     totals = np.zeros(2, np.int64)
     dls = directional_lights(scene)
+    als = area_lights(scene)
     r = _pt_lib().orc_pt_render(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
-                                _p(pts) if pts.size else None, pts.shape[0], _p(dls) if dls.size else None,
+                                _p(pts) if pts.size else None, pts.shape[0], _p(als) if als.size else None,
+                                als.shape[0], _p(dls) if dls.size else None,
                                 dls.shape[0], _p(env) if env is not None else None,
                                 ew, eh, ei, _p(ivp), width, height, spp, max_bounces, seed, sample_base, bias,
                                 nthreads, _p(s), _p(q), _p(lc) if log_rays else None, _p(ls) if log_rays else None,

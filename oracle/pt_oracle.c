@@ -115,8 +115,10 @@ typedef struct {
   const float* em_cdf;
   long n_em;
   float em_area;
-  const float* points;    /* 6 floats each: position, intensity */
+  const float* points;    /* 16 floats each: position, 0, intensity, 0, axis, cos outer, cos inner, range, decay, spot */
   long n_points;
+  const float* areas;     /* 16 floats each: centre, shape (0 rect / 1 disc), u, area, v, 0, radiance, 0 */
+  long n_areas;
   const float* dirs; /* 8 floats: direction towards the light, cos(angular radius), rgb, delta */
   long n_dirs;
   const float* env;       /* W*H*3 */
@@ -525,6 +527,62 @@ static v3 env_le(const orc_pt_t* S, int col, int row) {
 
 typedef struct { v3 wi, Le; float dist, pdf; int delta, valid; } lsample_t;
 
+/* point / spot falloff: 1 / d^decay and the range window (material.wgsl.ts:2176-2204) */
+static float positional_falloff(float dist, float d2, float range, float decay) {
+  if (!(dist > 0.0f) || dist > 3.402823466e38f) return 0.0f;
+  float a = 1.0f;
+  if (decay > 0.01f) {
+    float den = decay == 2.0f ? d2 : powf(dist, decay);
+    if (!(den > 0.0f)) a = 3.402823466e38f;
+    else if (den > 3.402823466e38f) return 0.0f;
+    else a = fminf(1.0f / den, 3.402823466e38f);
+  }
+  if (range > 0.0f) {
+    float q = dist / range, q2 = q * q;
+    a *= clamp01f(1.0f - q2 * q2);
+  }
+  return a;
+}
+static float smoothstep_f(float e0, float e1, float x) {
+  float t = clamp01f((x - e0) / (e1 - e0));
+  return t * t * (3.0f - 2.0f * t);
+}
+/* Shirley-Chiu concentric map (kernel.wgsl.ts:1422-1426) */
+static void concentric_disc(float a, float b, float* x, float* y) {
+  if (a == 0.0f && b == 0.0f) { *x = 0.0f; *y = 0.0f; return; }
+  float r, phi;
+  if (fabsf(a) > fabsf(b)) { r = a; phi = (0.25f * PI_F) * (b / a); }
+  else { r = b; phi = 0.5f * PI_F - (0.25f * PI_F) * (a / b); }
+  *x = r * cosf(phi);
+  *y = r * sinf(phi);
+}
+/* nearest analytic area light crossed by (o, d) from its emitting side before t_max
+ * (connect.wgsl.ts:390-450) */
+static int area_light_hit(const orc_pt_t* S, v3 o, v3 d, float t_max, v3* Le, float* pdf_sa) {
+  int found = 0;
+  float best = t_max;
+  for (long k = 0; k < S->n_areas; ++k) {
+    const float* q = S->areas + 16 * k;
+    v3 U = V(q[4], q[5], q[6]), Vv = V(q[8], q[9], q[10]), nl = nrm(cross3(U, Vv));
+    float den = dot3(nl, d);
+    if (!(den < 0.0f)) continue;
+    v3 c = V(q[0], q[1], q[2]);
+    float t = dot3(nl, sub(c, o)) / den;
+    if (!(t > 0.0f && t < best)) continue;
+    v3 rel = sub(add(o, scl(d, t)), c);
+    float uu = dot3(U, U), uv = dot3(U, Vv), vv = dot3(Vv, Vv), ru = dot3(rel, U), rv = dot3(rel, Vv);
+    float det = uu * vv - uv * uv;
+    float x = (ru * vv - rv * uv) / det, y = (rv * uu - ru * uv) / det;
+    int inside = q[3] != 0.0f ? x * x + y * y <= 1.0f : (fabsf(x) <= 1.0f && fabsf(y) <= 1.0f);
+    if (!inside) continue;
+    best = t;
+    found = 1;
+    *Le = V(q[12], q[13], q[14]);
+    *pdf_sa = t * t / (q[7] * -den);
+  }
+  return found;
+}
+
 static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
   lsample_t ls;
   memset(&ls, 0, sizeof ls);
@@ -557,20 +615,49 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
     e -= 1;
   }
   if ((long)e < S->n_points) {
-    const float* p = S->points + 6 * e;
+    /* point or spot light (kernel.wgsl.ts:1285-1397) */
+    const float* p = S->points + 16 * e;
     v3 d = sub(V(p[0], p[1], p[2]), P);
     float d2 = dot3(d, d);
     if (!(d2 > 0.0f)) return ls;
     float dist = sqrtf(d2);
+    if (p[13] > 0.0f && dist > p[13]) return ls;
     ls.wi = scl(d, 1.0f / dist);
+    float cone = 1.0f;
+    if (p[15] != 0.0f) {
+      float c = -dot3(ls.wi, V(p[8], p[9], p[10]));
+      if (!(c >= p[11])) return ls;
+      cone = smoothstep_f(p[11], fmaxf(p[12], p[11] + 1e-6f), c);
+    }
     ls.dist = dist;
-    ls.Le = scl(V(p[3], p[4], p[5]), 1.0f / d2);
+    ls.Le = scl(V(p[4], p[5], p[6]), cone * positional_falloff(dist, d2, p[13], p[14]));
     ls.pdf = psel;
     ls.delta = 1;
     ls.valid = 1;
     return ls;
   }
   e -= (uint32_t)S->n_points;
+  if ((long)e < S->n_areas) {
+    /* rectangle or disc, one-sided (kernel.wgsl.ts:1398-1493) */
+    const float* q = S->areas + 16 * e;
+    float xi1 = rand01(rng), xi2 = rand01(rng);
+    float x = xi1 * 2.0f - 1.0f, y = xi2 * 2.0f - 1.0f;
+    if (q[3] != 0.0f) concentric_disc(x, y, &x, &y);
+    v3 U = V(q[4], q[5], q[6]), Vv = V(q[8], q[9], q[10]);
+    v3 X = add(add(V(q[0], q[1], q[2]), scl(U, x)), scl(Vv, y));
+    v3 d = sub(X, P);
+    float d2 = dot3(d, d), dist = sqrtf(d2);
+    if (!(dist > 0.0f)) return ls;
+    ls.wi = scl(d, 1.0f / dist);
+    float cosl = -dot3(ls.wi, nrm(cross3(U, Vv)));
+    if (!(cosl > 0.0f)) return ls;
+    ls.Le = V(q[12], q[13], q[14]);
+    ls.dist = dist;
+    ls.pdf = psel * d2 / (q[7] * cosl);
+    ls.valid = 1;
+    return ls;
+  }
+  e -= (uint32_t)S->n_areas;
   if ((long)e < S->n_dirs) {
     const float* q = S->dirs + 8 * e;
     v3 w = V(q[0], q[1], q[2]);
@@ -630,6 +717,14 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
     double od[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z}, t;
     log_ray(S, 0, od, dd, INFINITY);
     long tri = trace(S, od, dd, INFINITY, 0, &t);
+    if (S->n_areas) {
+      v3 le = V(0, 0, 0);
+      float pa;
+      if (area_light_hit(S, o, d, tri < 0 ? INFINITY : (float)t, &le, &pa)) {
+        float w = prev_delta ? 1.0f : power_h(prev_pdf, pa / (float)S->n_entries);
+        L = add(L, scl(mul(T, le), w));
+      }
+    }
     if (tri < 0) {
       for (long k = 0; k < S->n_dirs; ++k) {
         const float* q = S->dirs + 8 * k;
@@ -742,11 +837,13 @@ static void* pt_worker(void* arg) {
  * Render width x height pixels x spp samples.  materials: 12 floats each
  * (base rgb 0-2, roughness 3, metallic 4, transmission 5, ior 6, emission rgb 7-9, flags 10,
  * specular intensity 11);
- * env: W*H*3 floats (NULL for none); points: 6 floats each.  Writes FP64
+ * env: W*H*3 floats (NULL for none); points: 16 floats each (points then spots);
+ * areas: 16 floats each (rectangles then discs).  Writes FP64
  * sum and sum of squares (3 per pixel).  Returns 0, or -1 on a build error.
  */
 int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
-                  const float* materials, int n_mat, const float* points, long n_points, const float* dirs,
+                  const float* materials, int n_mat, const float* points, long n_points, const float* areas,
+                  long n_areas, const float* dirs,
                   long n_dirs, const float* env,
                   int env_w, int env_h, float env_scale, const float* inv_vp, int width, int height, int spp,
                   int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
@@ -803,6 +900,8 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
   S.em_area = (float)total;
   S.points = points;
   S.n_points = n_points;
+  S.areas = areas;
+  S.n_areas = n_areas;
   S.dirs = dirs;
   S.n_dirs = n_dirs;
   float *marg = NULL, *cond = NULL;
@@ -844,7 +943,7 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
     free(rows);
     free(cum);
   }
-  S.n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_dirs + (S.env_sampleable ? 1 : 0);
+  S.n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_areas + (int)n_dirs + (S.env_sampleable ? 1 : 0);
   S.bias = bias;
   S.inv_vp = inv_vp;
   S.width = width;

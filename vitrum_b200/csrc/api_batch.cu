@@ -32,7 +32,7 @@ struct vt_batch {
   DeviceBuffer<uint4> nodes;
   DeviceBuffer<float4> tris;
   DeviceBuffer<vt::pt::Material> mats;
-  DeviceBuffer<float4> emitters, points, dirs, env;
+  DeviceBuffer<float4> emitters, points, dirs, env, areas;
   DeviceBuffer<float> cdf, marg, cond;
   DeviceBuffer<vt::pt::BatchScene> scenes;
   std::vector<vt::pt::BatchScene> host;
@@ -306,9 +306,9 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
     std::vector<uint32_t> nodes;
     std::vector<float> recs;
     std::vector<vt::pt::Material> mats;
-    std::vector<float4> ems, pts, dls, env;
+    std::vector<float4> ems, pts, dls, env, arl;
     std::vector<float> cdf, marg, cond;
-    struct Off { size_t mat, em, cdf, pt, dl, env, marg, cond; };
+    struct Off { size_t mat, em, cdf, pt, dl, env, marg, cond, arl; };
     std::vector<Off> off(count);
     b->host.assign(count, vt::pt::BatchScene{});
     unsigned long long path = 0;
@@ -325,13 +325,15 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
         if (imask) w[4] += nb;
         if (w[6]) w[5] += rb;
       }
-      off[i] = {mats.size(), ems.size(), cdf.size(), pts.size(), dls.size(), env.size(), marg.size(), cond.size()};
+      off[i] = {mats.size(), ems.size(), cdf.size(), pts.size(), dls.size(), env.size(), marg.size(), cond.size(),
+                arl.size()};
       nodes.insert(nodes.end(), p.node_words.begin(), p.node_words.end());
       recs.insert(recs.end(), p.rec_floats.begin(), p.rec_floats.end());
       mats.insert(mats.end(), p.mats.begin(), p.mats.end());
       ems.insert(ems.end(), p.emitters.begin(), p.emitters.end());
       cdf.insert(cdf.end(), p.cdf.begin(), p.cdf.end());
       pts.insert(pts.end(), p.points.begin(), p.points.end());
+      arl.insert(arl.end(), p.area_lights.begin(), p.area_lights.end());
       dls.insert(dls.end(), p.dirs.begin(), p.dirs.end());
       env.insert(env.end(), p.env.begin(), p.env.end());
       marg.insert(marg.end(), p.marg.begin(), p.marg.end());
@@ -354,13 +356,14 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       B.view.material_count = (uint32_t)p.mats.size();
       B.view.n_emitters = (uint32_t)p.cdf.size();
       B.view.emit_area_total = (float)p.emit_total;
-      B.view.n_points = (uint32_t)(p.points.size() / 2);
+      B.view.n_points = (uint32_t)(p.points.size() / vt::pt::kPositionalF4);
+      B.view.n_area = (uint32_t)(p.area_lights.size() / vt::pt::kAreaLightF4);
       B.view.n_dirs = (uint32_t)(p.dirs.size() / 2);
       B.view.env_w = p.env_w;
       B.view.env_h = p.env_h;
       B.view.env_scale = p.env_scale;
       B.view.n_light_entries =
-          (B.view.n_emitters ? 1u : 0u) + B.view.n_points + B.view.n_dirs + (p.env_sampleable ? 1u : 0u);
+          (B.view.n_emitters ? 1u : 0u) + B.view.n_points + B.view.n_area + B.view.n_dirs + (p.env_sampleable ? 1u : 0u);
     }
     if (pixels > 0xFFFFFFFFull) fail(VT_ERR_RANGE, "batch holds more than 2^32 pixels");
     if (recs.size() / 16 >= (1u << 30) || nodes.size() / 20 >= (1u << 30))
@@ -379,6 +382,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
     upload(b->emitters, ems, s);
     upload(b->cdf, cdf, s);
     upload(b->points, pts, s);
+    upload(b->areas, arl, s);
     upload(b->dirs, dls, s);
     upload(b->env, env, s);
     upload(b->marg, marg, s);
@@ -393,6 +397,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       v.emitters = b->emitters.ptr + off[i].em;
       v.emitter_cdf = b->cdf.ptr + off[i].cdf;
       v.points = b->points.ptr + off[i].pt;
+      v.area_lights = b->areas.ptr + off[i].arl;
       v.dirs = b->dirs.ptr + off[i].dl;
       v.env = p.has_env ? b->env.ptr + off[i].env : nullptr;
       v.env_marginal = p.env_sampleable ? b->marg.ptr + off[i].marg : nullptr;

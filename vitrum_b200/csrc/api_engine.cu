@@ -65,7 +65,7 @@ struct vt_engine {
   DeviceBuffer<vt::pt::Material> materials;
   DeviceBuffer<float4> emitters;
   DeviceBuffer<float> emitter_cdf;
-  DeviceBuffer<float4> points, dirs;
+  DeviceBuffer<float4> points, dirs, area_lights;
   DeviceBuffer<float4> env;
   DeviceBuffer<float> env_marginal, env_conditional;
   vt::pt::SceneView view;
@@ -158,6 +158,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   upload(e->emitters, p.emitters, s);
   upload(e->emitter_cdf, p.cdf, s);
   upload(e->points, p.points, s);
+  upload(e->area_lights, p.area_lights, s);
   upload(e->dirs, p.dirs, s);
   upload(e->env, p.env, s);
   upload(e->env_marginal, p.marg, s);
@@ -177,7 +178,9 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.n_emitters = (uint32_t)p.cdf.size();
   v.emit_area_total = (float)p.emit_total;
   v.points = e->points.ptr;
-  v.n_points = (uint32_t)(p.points.size() / 2);
+  v.n_points = (uint32_t)(p.points.size() / vt::pt::kPositionalF4);
+  v.area_lights = e->area_lights.ptr;
+  v.n_area = (uint32_t)(p.area_lights.size() / vt::pt::kAreaLightF4);
   v.dirs = e->dirs.ptr;
   v.n_dirs = (uint32_t)(p.dirs.size() / 2);
   v.env = p.has_env ? e->env.ptr : nullptr;
@@ -186,7 +189,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.env_w = p.env_w;
   v.env_h = p.env_h;
   v.env_scale = p.env_scale;
-  v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_dirs + (p.env_sampleable ? 1u : 0u);
+  v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_area + v.n_dirs + (p.env_sampleable ? 1u : 0u);
   e->view = v;
   e->binary = std::move(p.binary);
   e->ntri = (int64_t)p.ntri;

@@ -89,6 +89,74 @@ struct LightSample {
   bool valid;
 };
 
+// Distance falloff of point and spot lights: 1 / d^decay (none for decay <= 0.01;
+// exactly 1 / d^2 for decay 2) times the range window clamp(1 - (d / range)^4, 0, 1)
+// for range > 0 (pointSpotDistanceAttenuation, material.wgsl.ts:2176-2204).
+__device__ __forceinline__ float positional_falloff(float dist, float d2, float range, float decay) {
+  if (!(dist > 0.0f) || dist > 3.402823466e38f) return 0.0f;
+  float a = 1.0f;
+  if (decay > 0.01f) {
+    const float den = decay == 2.0f ? d2 : powf(dist, decay);
+    if (!(den > 0.0f)) a = 3.402823466e38f;
+    else if (den > 3.402823466e38f) return 0.0f;
+    else a = fminf(1.0f / den, 3.402823466e38f);
+  }
+  if (range > 0.0f) {
+    const float q = dist / range, q2 = q * q;
+    a *= clamp01(1.0f - q2 * q2);
+  }
+  return a;
+}
+// smoothstep(e0, e1, x) (kernel.wgsl.ts:1382, spot penumbra)
+__device__ __forceinline__ float smoothstep_f(float e0, float e1, float x) {
+  const float t = clamp01((x - e0) / (e1 - e0));
+  return t * t * (3.0f - 2.0f * t);
+}
+// Shirley-Chiu concentric map of (a, b) in [-1,1]^2 to the unit disc
+__device__ __forceinline__ float2 concentric_disc(float a, float b) {
+  if (a == 0.0f && b == 0.0f) return make_float2(0.0f, 0.0f);
+  float r, phi;
+  if (fabsf(a) > fabsf(b)) {
+    r = a;
+    phi = (0.25f * CUDART_PI_F) * (b / a);
+  } else {
+    r = b;
+    phi = 0.5f * CUDART_PI_F - (0.25f * CUDART_PI_F) * (a / b);
+  }
+  return make_float2(r * cosf(phi), r * sinf(phi));
+}
+// Nearest analytic area light that the ray (o, d) crosses from its emitting
+// side before t_max: its radiance and the solid-angle density of reaching that
+// point by sampling the light (connect.wgsl.ts:390-450; the lights are no occluders).
+__device__ __forceinline__ bool area_light_hit(const SceneView& sc, float3 o, float3 d, float t_max, float3& Le,
+                                               float& pdf_sa) {
+  bool found = false;
+  float best = t_max;
+  for (uint32_t k = 0; k < sc.n_area; ++k) {
+    const float4* q = sc.area_lights + kAreaLightF4 * (size_t)k;
+    const float4 a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + 2);
+    const float3 U = f3(a1.x, a1.y, a1.z), V = f3(a2.x, a2.y, a2.z);
+    const float3 nl = normalize(cross(U, V));
+    const float den = dot(nl, d);
+    if (!(den < 0.0f)) continue;  // behind or edge-on
+    const float3 c = f3(a0.x, a0.y, a0.z);
+    const float t = dot(nl, c - o) / den;
+    if (!(t > 0.0f && t < best)) continue;
+    const float3 rel = o + d * t - c;
+    const float uu = dot(U, U), uv = dot(U, V), vv = dot(V, V), ru = dot(rel, U), rv = dot(rel, V);
+    const float det = uu * vv - uv * uv;
+    const float x = (ru * vv - rv * uv) / det, y = (rv * uu - ru * uv) / det;
+    const bool inside = a0.w != 0.0f ? x * x + y * y <= 1.0f : (fabsf(x) <= 1.0f && fabsf(y) <= 1.0f);
+    if (!inside) continue;
+    best = t;
+    found = true;
+    const float4 a3 = __ldg(q + 3);
+    Le = f3(a3.x, a3.y, a3.z);
+    pdf_sa = t * t / (a1.w * -den);
+  }
+  return found;
+}
+
 __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng) {
   LightSample ls;
   ls.valid = false;
@@ -124,20 +192,57 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
     e -= 1;
   }
   if (e < sc.n_points) {
-    const float4 p = __ldg(sc.points + 2 * e), I = __ldg(sc.points + 2 * e + 1);
+    // point or spot light (kernel.wgsl.ts:1285-1397)
+    const float4* q = sc.points + kPositionalF4 * (size_t)e;
+    const float4 p = __ldg(q), I = __ldg(q + 1), ax = __ldg(q + 2), ex = __ldg(q + 3);
     const float3 d = f3(p.x, p.y, p.z) - P;
     const float d2 = dot(d, d);
     if (!(d2 > 0.0f)) return ls;
     const float dist = sqrtf(d2);
+    if (ex.y > 0.0f && dist > ex.y) return ls;  // beyond the range
     ls.wi = d * (1.0f / dist);
+    float cone = 1.0f;
+    if (ex.w != 0.0f) {
+      const float c = -dot(ls.wi, f3(ax.x, ax.y, ax.z));
+      if (!(c >= ax.w)) return ls;
+      cone = smoothstep_f(ax.w, fmaxf(ex.x, ax.w + 1e-6f), c);
+    }
     ls.dist = dist;
-    ls.Le = f3(I.x, I.y, I.z) * (1.0f / d2);
+    ls.Le = f3(I.x, I.y, I.z) * (cone * positional_falloff(dist, d2, ex.y, ex.z));
     ls.pdf = psel;
     ls.delta = true;
     ls.valid = true;
     return ls;
   }
   e -= sc.n_points;
+  if (e < sc.n_area) {
+    // rectangle (uniform in [-1,1]^2) or disc (concentric map), one-sided
+    // (kernel.wgsl.ts:1398-1493)
+    const float4* q = sc.area_lights + kAreaLightF4 * (size_t)e;
+    const float4 a0 = __ldg(q), a1 = __ldg(q + 1), a2 = __ldg(q + 2), a3 = __ldg(q + 3);
+    const float xi1 = rand01(rng), xi2 = rand01(rng);
+    float x = xi1 * 2.0f - 1.0f, y = xi2 * 2.0f - 1.0f;
+    if (a0.w != 0.0f) {
+      const float2 cd = concentric_disc(x, y);
+      x = cd.x;
+      y = cd.y;
+    }
+    const float3 U = f3(a1.x, a1.y, a1.z), V = f3(a2.x, a2.y, a2.z);
+    const float3 X = f3(a0.x, a0.y, a0.z) + U * x + V * y;
+    const float3 d = X - P;
+    const float d2 = dot(d, d);
+    const float dist = sqrtf(d2);
+    if (!(dist > 0.0f)) return ls;
+    ls.wi = d * (1.0f / dist);
+    const float cosl = -dot(ls.wi, normalize(cross(U, V)));
+    if (!(cosl > 0.0f)) return ls;
+    ls.Le = f3(a3.x, a3.y, a3.z);
+    ls.dist = dist;
+    ls.pdf = psel * d2 / (a1.w * cosl);
+    ls.valid = true;
+    return ls;
+  }
+  e -= sc.n_area;
   if (e < sc.n_dirs) {
     const float4 dw = __ldg(sc.dirs + 2 * e), dl = __ldg(sc.dirs + 2 * e + 1);
     const float3 w = f3(dw.x, dw.y, dw.z);
@@ -329,6 +434,15 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
       const float prev_pdf = __uint_as_float(st.w);
       const float3 o = f3(r0.x, r0.y, r0.z), d = f3(r1.x, r1.y, r1.z);
       float3 rad = f3(0.0f, 0.0f, 0.0f);
+      if (sc.n_area) {
+        // analytic area lights the incoming segment crossed (MIS against their sampling)
+        float3 Le;
+        float pa;
+        if (area_light_hit(sc, o, d, h.x < 0 ? CUDART_INF_F : __int_as_float(h.y), Le, pa)) {
+          const float wgt = prev_delta ? 1.0f : power_heuristic(prev_pdf, pa / (float)sc.n_light_entries);
+          rad = rad + T * Le * wgt;
+        }
+      }
       if (h.x < 0) {
         // escaped: discs of directional lights it points into (MIS against their cone sampling)
         for (uint32_t k = 0; k < sc.n_dirs; ++k) {

@@ -13,6 +13,15 @@ namespace pt {
 // Scene as the shading kernels see it.  Geometry lives in the BVH's triangle
 // records (vertices, source id in v0.w, material id in v1.w, reference
 // normal + validity in the fourth float4).
+// Positional delta lights (points, then spots), kPositionalF4 float4 each:
+//   (position, 0), (intensity rgb, 0), (axis, cos outer), (cos inner, range, decay, 1 for a spot)
+// Analytic area lights (rectangles, then discs), kAreaLightF4 float4 each:
+//   (centre, 0 rectangle / 1 disc), (u half axis, area), (v half axis, 0), (radiance rgb, 0)
+// a rectangle spans centre + [-1,1] u + [-1,1] v, a disc centre + u x + v y with
+// x^2 + y^2 <= 1; the emitting side is u x v.
+constexpr int kPositionalF4 = 4;
+constexpr int kAreaLightF4 = 4;
+
 struct SceneView {
   const uint4* nodes = nullptr;
   const float4* tris = nullptr;
@@ -24,9 +33,10 @@ struct SceneView {
   const float* emitter_cdf = nullptr;  // inclusive cumulative area / total, one per emitter
   uint32_t n_emitters = 0;
   float emit_area_total = 0.0f;
-  // point lights: 2 float4 each = (position, 0), (intensity rgb, 0)
-  const float4* points = nullptr;
+  const float4* points = nullptr;       // positional delta lights (layout above)
   uint32_t n_points = 0;
+  const float4* area_lights = nullptr;  // analytic rectangle / disc lights (layout above)
+  uint32_t n_area = 0;
   // directional lights: 2 float4 each = (direction towards the light, cos of the angular radius),
   // (rgb: irradiance of a delta light or radiance of a disc, 1 for delta)
   const float4* dirs = nullptr;
@@ -37,7 +47,9 @@ struct SceneView {
   const float* env_conditional = nullptr;  // env_h rows of env_w + 1 entries
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
-  uint32_t n_light_entries = 0;  // area group (if any) + point lights + directional lights + environment (if any)
+  // light entries, chosen uniformly by NEE: the emissive-mesh group (if any),
+  // positional lights, analytic area lights, directional lights, environment (if any)
+  uint32_t n_light_entries = 0;
   // two-level scenes: instance records (4 float4: world-to-local rows, (blas root, id, material, 0))
   const float4* insts = nullptr;       // in top-level leaf order (traversal)
   const float4* inst_table = nullptr;  // by instance index (shading)

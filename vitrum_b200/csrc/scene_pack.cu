@@ -134,45 +134,6 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     if (d.flags & ~3u) fail(VT_ERR_INVALID_ARGUMENT, "material " + std::to_string(i) + " has unknown flags");
     m.flags = d.flags;
   }
-  // rectangle lights: two emissive triangles each, one-sided, transparent to shadow rays
-  if (sc->rect_light_count) {
-    if (!sc->rect_lights) fail(VT_ERR_INVALID_ARGUMENT, "rect_lights is null");
-    if (sc->instance_count) fail(VT_ERR_INVALID_ARGUMENT, "rect lights need a single-level scene");
-    for (size_t i = 0; i < sc->rect_light_count; ++i) {
-      const vt_rect_light_desc& r = sc->rect_lights[i];
-      pt::Material m{};
-      m.base_color = make_float3(0.0f, 0.0f, 0.0f);
-      m.roughness = 1.0f;
-      m.emission = make_float3(r.radiance[0], r.radiance[1], r.radiance[2]);
-      m.ior = 1.5f;
-      m.kind = pt::kOpaque;
-      m.alpha = 1.0f;
-      m.metallic = 0.0f;
-      m.transmission = 0.0f;
-      m.specular = 0.0f;  // a light, not a surface: nothing is reflected
-      m.f0_ior = 0.0f;
-      m.emissive = (r.radiance[0] > 0.0f || r.radiance[1] > 0.0f || r.radiance[2] > 0.0f) ? 1u : 0u;
-      m.flags = VT_MATERIAL_SINGLE_SIDED | VT_MATERIAL_NO_SHADOW;
-      const uint32_t mi = (uint32_t)mats.size();
-      mats.push_back(m);
-      const uint32_t base = (uint32_t)(pos.size() / 4);
-      for (int c = 0; c < 4; ++c) {
-        const float a = (c == 1 || c == 2) ? 1.0f : 0.0f, b = (c >= 2) ? 1.0f : 0.0f;
-        for (int k = 0; k < 3; ++k) {
-          const float x = r.corner[k] + a * r.edge_u[k] + b * r.edge_v[k];
-          if (!std::isfinite(x)) fail(VT_ERR_RANGE, "rect light " + std::to_string(i) + " is not finite");
-          pos.push_back(x);
-        }
-        pos.push_back(0.0f);
-      }
-      const uint32_t tri[6] = {0, 1, 2, 0, 2, 3};
-      for (int t = 0; t < 2; ++t) {
-        for (int k = 0; k < 3; ++k) idx.push_back(base + tri[3 * t + k]);
-        idx.push_back(0u);
-        tri_mat.push_back(mi);
-      }
-    }
-  }
   const size_t ntri = tri_mat.size();
   // geometry
   BuildOptions bo;
@@ -298,12 +259,84 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   }
   for (float& x : cdf) x = (float)(x / total);
   if (!cdf.empty()) cdf.back() = 1.0f;
-  // point lights
+  // positional delta lights: points (inverse square, no range), then spots
+  // (emitterPacking.ts:652-705: cos outer, cos inner = cos(angle (1 - penumbra)), range, decay)
   std::vector<float4> pts;
+  auto finite3 = [](const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); };
+  if (sc->point_light_count && !sc->point_lights) fail(VT_ERR_INVALID_ARGUMENT, "point_lights is null");
   for (size_t i = 0; i < sc->point_light_count; ++i) {
     const vt_point_light_desc& p = sc->point_lights[i];
+    if (!finite3(p.position) || !finite3(p.intensity)) fail(VT_ERR_RANGE, "point light " + std::to_string(i) + " is not finite");
     pts.push_back(make_float4(p.position[0], p.position[1], p.position[2], 0.0f));
     pts.push_back(make_float4(p.intensity[0], p.intensity[1], p.intensity[2], 0.0f));
+    pts.push_back(make_float4(0.0f, 0.0f, 0.0f, -2.0f));
+    pts.push_back(make_float4(-1.0f, 0.0f, 2.0f, 0.0f));
+  }
+  if (sc->spot_light_count && !sc->spot_lights) fail(VT_ERR_INVALID_ARGUMENT, "spot_lights is null");
+  for (size_t i = 0; i < sc->spot_light_count; ++i) {
+    const vt_spot_light_desc& p = sc->spot_lights[i];
+    const std::string who = "spot light " + std::to_string(i);
+    if (!finite3(p.position) || !finite3(p.intensity) || !finite3(p.direction)) fail(VT_ERR_RANGE, who + " is not finite");
+    const double dl = std::sqrt((double)p.direction[0] * p.direction[0] + (double)p.direction[1] * p.direction[1] +
+                                (double)p.direction[2] * p.direction[2]);
+    if (!(dl > 0.0)) fail(VT_ERR_INVALID_ARGUMENT, who + ": direction is zero");
+    if (!(p.angle > 0.0f) || !(p.angle <= (float)M_PI)) fail(VT_ERR_RANGE, who + ": angle must be in (0, pi]");
+    if (!(p.penumbra >= 0.0f && p.penumbra <= 1.0f)) fail(VT_ERR_RANGE, who + ": penumbra must be in [0, 1]");
+    if (!(p.distance >= 0.0f) || !std::isfinite(p.distance)) fail(VT_ERR_RANGE, who + ": distance must be >= 0");
+    if (!(p.decay >= 0.0f) || !std::isfinite(p.decay)) fail(VT_ERR_RANGE, who + ": decay must be >= 0");
+    const double outer = p.angle, inner = outer * (1.0 - p.penumbra);
+    pts.push_back(make_float4(p.position[0], p.position[1], p.position[2], 0.0f));
+    pts.push_back(make_float4(p.intensity[0], p.intensity[1], p.intensity[2], 0.0f));
+    pts.push_back(make_float4((float)(p.direction[0] / dl), (float)(p.direction[1] / dl), (float)(p.direction[2] / dl),
+                              (float)std::cos(outer)));
+    pts.push_back(make_float4((float)std::cos(inner), p.distance, p.decay, 1.0f));
+  }
+  // analytic area lights: rectangles, then discs (emitterPacking.ts:78-93: centre, half axes, radiance, shape)
+  std::vector<float4> areas;
+  if (sc->rect_light_count && !sc->rect_lights) fail(VT_ERR_INVALID_ARGUMENT, "rect_lights is null");
+  for (size_t i = 0; i < sc->rect_light_count; ++i) {
+    const vt_rect_light_desc& r = sc->rect_lights[i];
+    const std::string who = "rect light " + std::to_string(i);
+    if (!finite3(r.corner) || !finite3(r.edge_u) || !finite3(r.edge_v) || !finite3(r.radiance))
+      fail(VT_ERR_RANGE, who + " is not finite");
+    float c[3], u[3], v[3];
+    for (int k = 0; k < 3; ++k) {
+      u[k] = 0.5f * r.edge_u[k];
+      v[k] = 0.5f * r.edge_v[k];
+      c[k] = r.corner[k] + u[k] + v[k];
+    }
+    const double cx = (double)u[1] * v[2] - (double)u[2] * v[1], cy = (double)u[2] * v[0] - (double)u[0] * v[2],
+                 cz = (double)u[0] * v[1] - (double)u[1] * v[0];
+    const double area = 4.0 * std::sqrt(cx * cx + cy * cy + cz * cz);
+    if (!(area > 0.0) || !std::isfinite(area)) fail(VT_ERR_INVALID_ARGUMENT, who + " has no area");
+    areas.push_back(make_float4(c[0], c[1], c[2], 0.0f));
+    areas.push_back(make_float4(u[0], u[1], u[2], (float)area));
+    areas.push_back(make_float4(v[0], v[1], v[2], 0.0f));
+    areas.push_back(make_float4(r.radiance[0], r.radiance[1], r.radiance[2], 0.0f));
+  }
+  if (sc->disc_light_count && !sc->disc_lights) fail(VT_ERR_INVALID_ARGUMENT, "disc_lights is null");
+  for (size_t i = 0; i < sc->disc_light_count; ++i) {
+    const vt_disc_light_desc& d = sc->disc_lights[i];
+    const std::string who = "disc light " + std::to_string(i);
+    if (!finite3(d.center) || !finite3(d.normal) || !finite3(d.radiance) || !std::isfinite(d.radius))
+      fail(VT_ERR_RANGE, who + " is not finite");
+    if (!(d.radius > 0.0f)) fail(VT_ERR_RANGE, who + ": radius must be > 0");
+    const double nl = std::sqrt((double)d.normal[0] * d.normal[0] + (double)d.normal[1] * d.normal[1] +
+                                (double)d.normal[2] * d.normal[2]);
+    if (!(nl > 0.0)) fail(VT_ERR_INVALID_ARGUMENT, who + ": normal is zero");
+    const double n[3] = {d.normal[0] / nl, d.normal[1] / nl, d.normal[2] / nl};
+    // tangent frame (t, b) with t x b = n, scaled by the radius
+    double t[3];
+    if (std::fabs(n[0]) > 0.9) { t[0] = -n[2]; t[1] = 0.0; t[2] = n[0]; }
+    else { t[0] = 0.0; t[1] = n[2]; t[2] = -n[1]; }
+    const double tl = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    for (double& x : t) x /= tl;
+    const double b[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
+    const double rr = d.radius;
+    areas.push_back(make_float4(d.center[0], d.center[1], d.center[2], 1.0f));
+    areas.push_back(make_float4((float)(t[0] * rr), (float)(t[1] * rr), (float)(t[2] * rr), (float)(M_PI * rr * rr)));
+    areas.push_back(make_float4((float)(b[0] * rr), (float)(b[1] * rr), (float)(b[2] * rr), 0.0f));
+    areas.push_back(make_float4(d.radiance[0], d.radiance[1], d.radiance[2], 0.0f));
   }
   // directional lights
   std::vector<float4> dirs;
@@ -377,6 +410,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   p.cdf = std::move(cdf);
   p.emit_total = total;
   p.points = std::move(pts);
+  p.area_lights = std::move(areas);
   p.dirs = std::move(dirs);
   p.env = std::move(envt);
   p.marg = std::move(marg);

@@ -26,7 +26,8 @@ struct PackedScene {
   std::vector<float4> emitters;      // 3 float4 per emissive triangle (world space)
   std::vector<float> cdf;            // inclusive area CDF
   double emit_total = 0.0;
-  std::vector<float4> points;        // 2 float4 per point light
+  std::vector<float4> points;        // kPositionalF4 float4 per point or spot light
+  std::vector<float4> area_lights;   // kAreaLightF4 float4 per rectangle or disc light
   std::vector<float4> dirs;          // 2 float4 per directional light
   std::vector<float4> env;
   std::vector<float> marg, cond;

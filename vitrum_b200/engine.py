@@ -55,6 +55,17 @@ class _RectDesc(ctypes.Structure):
                 ("radiance", ctypes.c_float * 3)]
 
 
+class _SpotDesc(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float * 3), ("direction", ctypes.c_float * 3), ("intensity", ctypes.c_float * 3),
+                ("angle", ctypes.c_float), ("penumbra", ctypes.c_float), ("distance", ctypes.c_float),
+                ("decay", ctypes.c_float)]
+
+
+class _DiscDesc(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_float * 3), ("normal", ctypes.c_float * 3), ("radius", ctypes.c_float),
+                ("radiance", ctypes.c_float * 3)]
+
+
 class _SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_size_t), ("instances", ctypes.c_void_p),
                 ("instance_count", ctypes.c_size_t), ("materials", ctypes.c_void_p),
@@ -63,7 +74,9 @@ class _SceneDesc(ctypes.Structure):
                 ("environment_width", ctypes.c_int32), ("environment_height", ctypes.c_int32),
                 ("environment_intensity", ctypes.c_float), ("directional_lights", ctypes.c_void_p),
                 ("directional_light_count", ctypes.c_size_t), ("rect_lights", ctypes.c_void_p),
-                ("rect_light_count", ctypes.c_size_t)]
+                ("rect_light_count", ctypes.c_size_t), ("spot_lights", ctypes.c_void_p),
+                ("spot_light_count", ctypes.c_size_t), ("disc_lights", ctypes.c_void_p),
+                ("disc_light_count", ctypes.c_size_t)]
 
 
 class _FrameInput(ctypes.Structure):
@@ -156,8 +169,32 @@ class DirectionalLight:
 
 
 @dataclass
+class SpotLight:
+    """core SpotEmitter: delta light at `position` emitting `intensity` into the cone of
+    half-angle `angle` (radians) around `direction`, with a smooth edge from
+    angle * (1 - penumbra), falloff 1 / d^decay and an optional range `distance` (0: none)."""
+    position: Sequence[float]
+    direction: Sequence[float]
+    intensity: Sequence[float]
+    angle: float
+    penumbra: float = 0.0
+    distance: float = 0.0
+    decay: float = 2.0
+
+
+@dataclass
+class DiscLight:
+    """core DiscAreaEmitter: disc of `radius` at `center` emitting `radiance` towards `normal`."""
+    center: Sequence[float]
+    normal: Sequence[float]
+    radius: float
+    radiance: Sequence[float]
+
+
+@dataclass
 class RectLight:
-    """corner + [0,1] edge_u + [0,1] edge_v emitting `radiance` towards edge_u x edge_v."""
+    """corner + [0,1] edge_u + [0,1] edge_v emitting `radiance` towards edge_u x edge_v
+    (an analytic emitter: never an occluder)."""
     corner: Sequence[float]
     edge_u: Sequence[float]
     edge_v: Sequence[float]
@@ -179,6 +216,8 @@ class Scene:
     environment: Optional[Environment] = None
     directional_lights: List[DirectionalLight] = field(default_factory=list)
     rect_lights: List[RectLight] = field(default_factory=list)
+    spot_lights: List[SpotLight] = field(default_factory=list)
+    disc_lights: List[DiscLight] = field(default_factory=list)
 
     @property
     def triangle_count(self) -> int:
@@ -271,13 +310,23 @@ def _marshal_scene(scene: "Scene"):
     for i, r in enumerate(scene.rect_lights):
         rls[i] = _RectDesc((ctypes.c_float * 3)(*r.corner), (ctypes.c_float * 3)(*r.edge_u),
                            (ctypes.c_float * 3)(*r.edge_v), (ctypes.c_float * 3)(*r.radiance))
+    sls = (_SpotDesc * max(1, len(scene.spot_lights)))()
+    for i, l in enumerate(scene.spot_lights):
+        sls[i] = _SpotDesc((ctypes.c_float * 3)(*l.position), (ctypes.c_float * 3)(*l.direction),
+                           (ctypes.c_float * 3)(*l.intensity), l.angle, l.penumbra, l.distance, l.decay)
+    dcs = (_DiscDesc * max(1, len(scene.disc_lights)))()
+    for i, l in enumerate(scene.disc_lights):
+        dcs[i] = _DiscDesc((ctypes.c_float * 3)(*l.center), (ctypes.c_float * 3)(*l.normal), l.radius,
+                           (ctypes.c_float * 3)(*l.radiance))
     desc = _SceneDesc(ctypes.cast(meshes, ctypes.c_void_p), len(scene.meshes),
                       ctypes.cast(insts, ctypes.c_void_p) if scene.instances else None, len(scene.instances),
                       ctypes.cast(mats, ctypes.c_void_p),
                       len(scene.materials), ctypes.cast(pls, ctypes.c_void_p), len(scene.point_lights), env_ptr,
                       ew, eh, ei, ctypes.cast(dls, ctypes.c_void_p), len(scene.directional_lights),
-                      ctypes.cast(rls, ctypes.c_void_p), len(scene.rect_lights))
-    return desc, (keep, meshes, insts, mats, pls, dls, rls)
+                      ctypes.cast(rls, ctypes.c_void_p), len(scene.rect_lights),
+                      ctypes.cast(sls, ctypes.c_void_p), len(scene.spot_lights),
+                      ctypes.cast(dcs, ctypes.c_void_p), len(scene.disc_lights))
+    return desc, (keep, meshes, insts, mats, pls, dls, rls, sls, dcs)
 
 
 # ---------------------------------------------------------------- engine
