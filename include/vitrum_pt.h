@@ -349,6 +349,18 @@ vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
 /* FP64 per-pixel mean and per-sample variance (requires oracle_accumulation);
  * 3 doubles per pixel each. */
 vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
+
+/* captureFrame({colorSpace: 'output'}) (pt-webgpu/src/index.ts:2004-2033): the
+ * present pass (pt-webgpu/src/wgsl/present.wgsl.ts; operators of
+ * shared-samplers/src/wgsl/tonemap.wgsl.ts) applied to the accumulated mean:
+ * exposure, tonemap, then the sRGB OETF.  The reference's defaults are ACES,
+ * exposure 1, sRGB. */
+typedef struct vt_present_options {
+  int32_t tonemap;          /* 0 ACES filmic, 1 AgX, 2 Reinhard, 3 clamp to [0, 1], 4 none */
+  float exposure;           /* linear multiplier, > 0 */
+  int32_t srgb;             /* 1 apply the sRGB OETF (outputColorSpace 'srgb'), 0 keep linear */
+} vt_present_options;
+vt_status vt_capture_output(vt_engine* engine, const vt_present_options* options, float* rgba, size_t float_capacity);
 /* Engine.debug.pickPrimitive (engine/debug.ts:33-35; pickPrimitiveCpu.ts:674):
  * under pixel (x, y) of the last frame's camera: the instance index in a
  * scene with instances, else the source triangle index; -1 on a miss. */

@@ -335,6 +335,34 @@ def area_lights(scene):
     return np.array(rows, np.float32).reshape(-1, 16)
 
 
+def present(rgb, tonemap=0, exposure=1.0, srgb=True):
+    """The present pass on mean radiance `rgb` (..., 3), float64: exposure, then
+    tonemap 0 ACES filmic (Narkowicz: x(2.51x + 0.03) / (x(2.43x + 0.59) + 0.14)),
+    1 AgX (log2 range [-12.47393, 4.026069], sixth-order curve), 2 Reinhard
+    x / (1 + x), 3 clamp to [0, 1], 4 none; then the sRGB OETF when `srgb`
+    (shared-samplers/src/wgsl/tonemap.wgsl.ts:8-60, pt-webgpu/src/wgsl/present.wgsl.ts:59-80)."""
+    x = np.asarray(rgb, np.float64)
+    x = np.where(np.isnan(x) | (exposure <= 0), 0.0, np.sign(x) * np.minimum(np.abs(x) * exposure, 3.402823466e38))
+    if tonemap == 1:
+        lx = np.clip((np.log2(np.maximum(x, 1e-6)) + 12.47393) / (12.47393 + 4.026069), 0.0, 1.0)
+        y = np.clip(15.5 * lx ** 6 - 40.14 * lx ** 5 + 31.96 * lx ** 4 - 6.868 * lx ** 3 + 0.4298 * lx ** 2
+                    + 0.1191 * lx - 0.00232, 0.0, 1.0)
+    elif tonemap == 2:
+        v = np.maximum(x, 0.0)
+        y = v / (1.0 + v)
+    elif tonemap == 3:
+        y = np.clip(x, 0.0, 1.0)
+    elif tonemap == 4:
+        y = x
+    else:
+        v = np.minimum(np.maximum(x, 0.0), 1e18)
+        y = np.clip(v * (2.51 * v + 0.03) / (v * (2.43 * v + 0.59) + 0.14), 0.0, 1.0)
+    if srgb:
+        v = np.maximum(y, 0.0)
+        y = np.where(v <= 0.0031308, v * 12.92, 1.055 * np.power(v, 1.0 / 2.4) - 0.055)
+    return y
+
+
 def directional_lights(scene):
     """(n, 8) float32: direction towards the light, cos(angular radius) (1 for a
     delta light), rgb (irradiance of a delta light, disc radiance otherwise), delta flag."""

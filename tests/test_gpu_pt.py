@@ -229,3 +229,23 @@ def test_autotune_keeps_the_image(cuda):
     e.render_frame(cam, 32, 32, samples=8, frame_seed=4)
     assert np.allclose(e.capture_frame(), before, rtol=1e-5, atol=1e-6)
     e.dispose()
+
+
+@pytest.mark.parametrize("tonemap,exposure,space", [("aces", 1.0, "srgb"), ("agx", 0.5, "srgb"),
+                                                    ("reinhard", 2.0, "linear"), ("linear", 1.0, "srgb"),
+                                                    ("none", 3.0, "linear")])
+def test_capture_output_is_the_present_pass(cuda, tonemap, exposure, space):
+    # captureFrame({colorSpace: 'output'}): exposure, tonemap, sRGB OETF on the
+    # accumulated mean, checked against the oracle's present pass on the linear capture
+    sc, cam = small_room()
+    e = Engine(max_bounces=3)
+    e.set_scene(sc)
+    e.render_frame(cam, 24, 16, samples=16)
+    lin = e.capture_frame()
+    out = e.capture_frame("output", tonemap=tonemap, exposure=exposure, output_color_space=space)
+    want = oracle.present(lin[..., :3], Engine.TONEMAPS[tonemap], exposure, srgb=space == "srgb")
+    assert out.shape == lin.shape and (out[..., 3] == 1).all()
+    assert np.allclose(out[..., :3], want, rtol=2e-5, atol=2e-6), np.abs(out[..., :3] - want).max()
+    with pytest.raises(N.VtError):
+        N.call("vt_capture_output", e.handle, None, N.ctypes.c_void_p(out.ctypes.data), out.size)
+    e.dispose()

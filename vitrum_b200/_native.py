@@ -67,6 +67,7 @@ SIGNATURES = {
     "vt_render_frame": [P, P, P],
     "vt_profile_frame": [P, P, P, P],
     "vt_capture": [P, P, SZ],
+    "vt_capture_output": [P, P, P, SZ],
     "vt_capture_moments": [P, P, P, SZ],
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
     "vt_trace_rays": [P, P, SZ, P, P],

@@ -73,6 +73,7 @@ struct vt_engine {
   // accumulation
   int width = 0, height = 0;
   DeviceBuffer<float4> accum;
+  DeviceBuffer<float4> present;     // present-pass output of vt_capture_output
   DeviceBuffer<double> sum64, sq64;
   int samples = 0;
   float inv_vp[16] = {};
@@ -681,6 +682,24 @@ vt_status vt_profile_frame(vt_engine* e, const vt_frame_input* input, vt_frame_o
     times->nrc_train_ms = ms[StageTimer::kNrcTrain];
     times->nrc_query_ms = ms[StageTimer::kNrcQuery];
     times->frame_ms = e->last_ms;
+  });
+}
+
+vt_status vt_capture_output(vt_engine* e, const vt_present_options* o, float* rgba, size_t cap) {
+  return vt::guard([&] {
+    if (!e || !o || !rgba) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (o->tonemap < 0 || o->tonemap > 4) fail(VT_ERR_RANGE, "tonemap must be in [0, 4]");
+    if (!(o->exposure > 0.0f) || !std::isfinite(o->exposure)) fail(VT_ERR_RANGE, "exposure must be finite and > 0");
+    if (o->srgb != 0 && o->srgb != 1) fail(VT_ERR_RANGE, "srgb must be 0 or 1");
+    if (!e->accum.ptr) fail(VT_ERR_STATE, "captureFrame before renderFrame");
+    const size_t px = (size_t)e->width * e->height;
+    if (cap < 4 * px) fail(VT_ERR_RANGE, "capture buffer too small");
+    vt::DeviceScope ds(e->device);
+    e->present.resize(px);
+    vt::pt::launch_present(e->accum.ptr, px, o->tonemap, o->exposure, o->srgb, e->present.ptr, e->stream);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaMemcpyAsync(rgba, e->present.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    VT_CUDA(cudaStreamSynchronize(e->stream));
   });
 }
 

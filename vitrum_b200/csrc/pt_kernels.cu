@@ -807,6 +807,65 @@ unsigned grid_for(uint32_t n, unsigned block) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- present
+// Tonemap operators of shared-samplers/src/wgsl/tonemap.wgsl.ts:8-60, restated:
+// exposure scales each channel (NaN and non-positive exposure give 0, results
+// stay finite); ACES filmic is Narkowicz's fit x(2.51x + 0.03) / (x(2.43x + 0.59)
+// + 0.14) clamped to [0, 1]; AgX maps log2 exposure over [-12.47393, 4.026069]
+// to [0, 1] and applies its sixth-order polynomial; Reinhard is x / (1 + x).
+__device__ __forceinline__ float exposed(float c, float exposure) {
+  if (c != c || !(exposure > 0.0f)) return 0.0f;
+  const float m = fminf(fabsf(c) * fminf(exposure, 3.402823466e38f), 3.402823466e38f);
+  return c < 0.0f ? -m : m;
+}
+__device__ __forceinline__ float tonemap_aces(float x) {
+  const float v = fminf(fmaxf(x, 0.0f), 1e18f);  // the curve is 1 (clamped) long before v^2 overflows
+  return clamp01(v * (2.51f * v + 0.03f) / (v * (2.43f * v + 0.59f) + 0.14f));
+}
+__device__ __forceinline__ float tonemap_agx(float c) {
+  const float x = clamp01((log2f(fmaxf(c, 1e-6f)) + 12.47393f) / (12.47393f + 4.026069f));
+  const float x2 = x * x, x4 = x2 * x2;
+  return clamp01(15.5f * x4 * x2 - 40.14f * x4 * x + 31.96f * x4 - 6.868f * x2 * x + 0.4298f * x2 + 0.1191f * x -
+                 0.00232f);
+}
+__device__ __forceinline__ float tonemap(float c, int mode, float exposure) {
+  const float x = exposed(c, exposure);
+  switch (mode) {
+    case 1: return tonemap_agx(x);
+    case 2: { const float v = fmaxf(x, 0.0f); return v / (1.0f + v); }
+    case 3: return clamp01(x);
+    case 4: return x;
+    default: return tonemap_aces(x);
+  }
+}
+// IEC 61966-2-1 sRGB encoding
+__device__ __forceinline__ float srgb_oetf(float c) {
+  const float v = fmaxf(c, 0.0f);
+  return v <= 0.0031308f ? v * 12.92f : 1.055f * powf(v, 1.0f / 2.4f) - 0.055f;
+}
+__global__ void k_present(const float4* __restrict__ accum, size_t pixels, int mode, float exposure, int srgb,
+                          float4* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pixels) return;
+  const float4 a = accum[i];
+  const float inv = a.w > 0.0f ? 1.0f / a.w : 0.0f;
+  float r = tonemap(fmaxf(a.x * inv, 0.0f), mode, exposure);
+  float g = tonemap(fmaxf(a.y * inv, 0.0f), mode, exposure);
+  float b = tonemap(fmaxf(a.z * inv, 0.0f), mode, exposure);
+  if (srgb) {
+    r = srgb_oetf(r);
+    g = srgb_oetf(g);
+    b = srgb_oetf(b);
+  }
+  out[i] = make_float4(r, g, b, 1.0f);
+}
+
+void launch_present(const float4* accum, size_t pixels, int tonemap, float exposure, int srgb, float4* out,
+                    cudaStream_t s) {
+  if (pixels == 0) return;
+  k_present<<<(unsigned)((pixels + 255) / 256), 256, 0, s>>>(accum, pixels, tonemap, exposure, srgb, out);
+}
+
 void launch_count_rays(const WaveBuffers& w, int cur, unsigned long long* totals, cudaStream_t s) {
   k_count_rays<<<1, 1, 0, s>>>(w, cur, totals);
 }

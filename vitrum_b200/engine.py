@@ -66,6 +66,10 @@ class _DiscDesc(ctypes.Structure):
                 ("radiance", ctypes.c_float * 3)]
 
 
+class _PresentOptions(ctypes.Structure):
+    _fields_ = [("tonemap", ctypes.c_int32), ("exposure", ctypes.c_float), ("srgb", ctypes.c_int32)]
+
+
 class _SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_size_t), ("instances", ctypes.c_void_p),
                 ("instance_count", ctypes.c_size_t), ("materials", ctypes.c_void_p),
@@ -392,10 +396,25 @@ class Engine:
         self.width, self.height = out.width, out.height
         return {f: getattr(tm, f) for f, _ in _StageTimes._fields_}
 
-    def capture_frame(self) -> np.ndarray:
-        """Mean radiance (H, W, 4) float32, alpha 1 (Engine.captureFrame)."""
+    TONEMAPS = {"aces": 0, "agx": 1, "reinhard": 2, "linear": 3, "none": 4}
+
+    def capture_frame(self, color_space: str = "linear", tonemap: str = "aces", exposure: float = 1.0,
+                      output_color_space: str = "srgb") -> np.ndarray:
+        """(H, W, 4) float32, alpha 1 (Engine.captureFrame).  color_space 'linear':
+        the mean radiance; 'output': the present pass (exposure, `tonemap` of
+        aces / agx / reinhard / linear / none, sRGB encoding unless
+        output_color_space is 'linear')."""
         out = np.empty((self.height, self.width, 4), np.float32)
-        N.call("vt_capture", self.handle, ctypes.c_void_p(out.ctypes.data), out.size)
+        if color_space == "linear":
+            N.call("vt_capture", self.handle, ctypes.c_void_p(out.ctypes.data), out.size)
+        elif color_space == "output":
+            if tonemap not in self.TONEMAPS or output_color_space not in ("srgb", "linear"):
+                raise ValueError("tonemap must be one of %s and output_color_space srgb or linear"
+                                 % sorted(self.TONEMAPS))
+            o = _PresentOptions(self.TONEMAPS[tonemap], exposure, 1 if output_color_space == "srgb" else 0)
+            N.call("vt_capture_output", self.handle, ctypes.byref(o), ctypes.c_void_p(out.ctypes.data), out.size)
+        else:
+            raise ValueError("color_space must be 'linear' or 'output'")
         return out
 
     def capture_moments(self):
