@@ -350,6 +350,16 @@ vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
  * 3 doubles per pixel each. */
 vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
 
+/* New placements for the instances of the current two-level scene (moving
+ * instances, changing their mesh or material), without rebuilding any
+ * bottom-level tree: refitTlasTransforms (shared-bvh/src/scenePack.ts:1310,
+ * refitTlas tlas.ts:990-1012) with rebuild 0 -- the top level keeps its
+ * topology and takes the new bounds -- or rebuildTlasReuseBlas
+ * (scenePack.ts:1635) with rebuild 1 -- a new binned-SAH top level.  The
+ * instance count must equal the scene's (VT_ERR_INVALID_ARGUMENT otherwise;
+ * VT_ERR_STATE without an instanced scene).  Clears the accumulation. */
+vt_status vt_update_instances(vt_engine* engine, const vt_instance_desc* instances, size_t count, int32_t rebuild);
+
 /* captureFrame({colorSpace: 'output'}) (pt-webgpu/src/index.ts:2004-2033): the
  * present pass (pt-webgpu/src/wgsl/present.wgsl.ts; operators of
  * shared-samplers/src/wgsl/tonemap.wgsl.ts) applied to the accumulated mean:

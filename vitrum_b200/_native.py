@@ -68,6 +68,7 @@ SIGNATURES = {
     "vt_profile_frame": [P, P, P, P],
     "vt_capture": [P, P, SZ],
     "vt_capture_output": [P, P, P, SZ],
+    "vt_update_instances": [P, P, SZ, I32],
     "vt_capture_moments": [P, P, P, SZ],
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],
     "vt_trace_rays": [P, P, SZ, P, P],

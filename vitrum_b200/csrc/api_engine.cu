@@ -57,6 +57,13 @@ struct vt_engine {
   DeviceBuffer<float4> inst_table; // instance records by instance index
   DeviceBuffer<float4> inst_l2w;   // local-to-world rows by instance index (hit refinement)
   int64_t n_instances = 0;
+  // two-level scenes, for instance updates: bottom-level roots / local bounds per
+  // mesh, the deepest bottom level, the top level's first node, host materials
+  std::vector<uint32_t> blas_root;
+  std::vector<std::array<double, 6>> local_box;
+  int blas_depth = 0;
+  uint32_t tlas_root = 0;
+  std::vector<vt::pt::Material> mats_host;
   // vt_trace_rays staging
   DeviceBuffer<float4> q_rays;
   DeviceBuffer<int4> q_hits;
@@ -124,6 +131,7 @@ struct vt_engine {
 namespace {
 
 void nrc_rebuild(vt_engine* e);
+void reset_accumulation(vt_engine* e);
 
 template <class T>
 void upload(DeviceBuffer<T>& dst, const std::vector<T>& src, cudaStream_t s) {
@@ -193,14 +201,67 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_area + v.n_dirs + (p.env_sampleable ? 1u : 0u);
   e->view = v;
   e->binary = std::move(p.binary);
+  e->blas_root = std::move(p.blas_root);
+  e->local_box = std::move(p.local_box);
+  e->blas_depth = p.blas_depth;
+  e->tlas_root = p.root;
+  e->mats_host = p.mats;
   e->ntri = (int64_t)p.ntri;
   e->n_emitters = (int64_t)v.n_emitters;
   e->has_scene = true;
   if (e->nrc) nrc_rebuild(e);
-  e->samples = 0;
-  if (e->accum.ptr) VT_CUDA(cudaMemset(e->accum.ptr, 0, e->accum.bytes()));
-  if (e->sum64.ptr) VT_CUDA(cudaMemset(e->sum64.ptr, 0, e->sum64.bytes()));
-  if (e->sq64.ptr) VT_CUDA(cudaMemset(e->sq64.ptr, 0, e->sq64.bytes()));
+  reset_accumulation(e);
+  VT_CUDA(cudaStreamSynchronize(e->stream));
+}
+
+// New placements for the instances of a two-level scene (refitTlasTransforms /
+// rebuildTlasReuseBlas, shared-bvh/src/scenePack.ts:1310, 1635): the bottom
+// levels stay; the top level is refitted (same topology, new bounds) or rebuilt
+// (binned SAH over the new instance bounds), re-encoded and uploaded.
+void update_instances(vt_engine* e, const vt_instance_desc* insts, size_t n, bool rebuild) {
+  if (!e->has_scene || e->n_instances == 0) fail(VT_ERR_STATE, "instance updates need a scene with instances");
+  if (n != (size_t)e->n_instances)
+    fail(VT_ERR_INVALID_ARGUMENT, "expected " + std::to_string(e->n_instances) + " instances, got " +
+                                      std::to_string(n) + " (set a new scene to change the membership)");
+  if (!insts) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
+  vt::InstanceSet placed = vt::place_instances(insts, n, e->mats_host, e->blas_root, e->local_box);
+  vt::BinaryBvhHost tl;
+  if (rebuild) {
+    tl = vt::build_tlas_host(placed.aabbs.data(), n);
+  } else {
+    tl = e->binary;
+    vt::refit_tlas_host(tl, placed.aabbs.data(), n);
+  }
+  vt::WideBvhHost tw = vt::encode_wide_tlas(tl, placed.recs.data(), e->tlas_root);
+  cudaStream_t s = e->stream;
+  VT_CUDA(cudaStreamSynchronize(s));
+  e->drop_graphs();
+  const size_t blas_u4 = (size_t)e->tlas_root * 5, tlas_u4 = tw.nodes.size() / 4;
+  if (blas_u4 + tlas_u4 != e->nodes.count) {
+    DeviceBuffer<uint4> grown(blas_u4 + tlas_u4);
+    if (blas_u4)
+      VT_CUDA(cudaMemcpyAsync(grown.ptr, e->nodes.ptr, blas_u4 * sizeof(uint4), cudaMemcpyDeviceToDevice, s));
+    VT_CUDA(cudaStreamSynchronize(s));
+    e->nodes = std::move(grown);
+  }
+  VT_CUDA(cudaMemcpyAsync(e->nodes.ptr + blas_u4, tw.nodes.data(), tw.nodes.size() * 4, cudaMemcpyHostToDevice, s));
+  std::vector<float4> il(tw.tris.size() / 4), it(n * 4), ir(placed.rows.size() / 4);
+  if (!il.empty()) std::memcpy(il.data(), tw.tris.data(), tw.tris.size() * 4);
+  std::memcpy(it.data(), placed.recs.data(), n * sizeof(vt::InstanceRecord));
+  if (!ir.empty()) std::memcpy(ir.data(), placed.rows.data(), placed.rows.size() * 4);
+  upload(e->insts, il, s);
+  upload(e->inst_table, it, s);
+  upload(e->inst_l2w, ir, s);
+  VT_CUDA(cudaStreamSynchronize(s));
+  e->binary = std::move(tl);
+  e->wide_depth = tw.depth + e->blas_depth;
+  e->stack_depth = 2 * e->wide_depth + 6;
+  e->view.nodes = e->nodes.ptr;
+  e->view.stack_depth = e->stack_depth;
+  e->view.insts = e->insts.ptr;
+  e->view.inst_table = e->inst_table.ptr;
+  reset_accumulation(e);
+  VT_CUDA(cudaStreamSynchronize(e->stream));
 }
 
 // ---------------------------------------------------------------- waves
@@ -651,6 +712,15 @@ vt_status vt_set_scene(vt_engine* e, const vt_scene_desc* scene) {
     if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
     vt::DeviceScope ds(e->device);
     set_scene(e, scene);
+  });
+}
+
+vt_status vt_update_instances(vt_engine* e, const vt_instance_desc* instances, size_t count, int32_t rebuild) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    if (rebuild != 0 && rebuild != 1) fail(VT_ERR_RANGE, "rebuild must be 0 or 1");
+    vt::DeviceScope ds(e->device);
+    update_instances(e, instances, count, rebuild != 0);
   });
 }
 

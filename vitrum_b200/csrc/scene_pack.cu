@@ -73,6 +73,83 @@ void inverse_view_proj(const float* view, const float* proj, float* out_rm) {
 
 
 
+InstanceSet place_instances(const vt_instance_desc* insts, size_t ni, const std::vector<pt::Material>& mats,
+                            const std::vector<uint32_t>& blas_root,
+                            const std::vector<std::array<double, 6>>& local_box) {
+  // world-to-local rows and world AABBs (transformAabb, scenePack.ts:197-223)
+  InstanceSet out;
+  out.recs.resize(ni);
+  out.aabbs.resize(6 * ni);
+  out.rows.reserve(12 * ni);
+  for (size_t i = 0; i < ni; ++i) {
+    const vt_instance_desc& id = insts[i];
+    if (id.mesh >= blas_root.size())
+      fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references mesh " + std::to_string(id.mesh));
+    if (id.material >= mats.size())
+      fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references material " + std::to_string(id.material));
+    if (mats[id.material].emissive) fail(VT_ERR_INVALID_ARGUMENT, "emissive materials are not supported on instances");
+    double rm[16], inv[16];
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) rm[r * 4 + c] = id.local_to_world[c * 4 + r];
+    for (double x : rm)
+      if (!std::isfinite(x)) fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " transform is not finite");
+    if (!invert4(rm, inv)) fail(VT_ERR_INVALID_ARGUMENT, "instance " + std::to_string(i) + " is not invertible");
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 4; ++c) out.rows.push_back(id.local_to_world[c * 4 + r]);
+    InstanceRecord& rec = out.recs[i];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 4; ++c) rec.w2l[4 * r + c] = (float)inv[r * 4 + c];
+    rec.blas_root = blas_root[id.mesh];
+    rec.instance_id = (uint32_t)i;
+    rec.material = id.material;
+    rec.pad = mats[id.material].flags;
+    const auto& lb = local_box[id.mesh];
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int c = 0; c < 8; ++c) {
+      const double q[3] = {(c & 1) ? lb[3] : lb[0], (c & 2) ? lb[4] : lb[1], (c & 4) ? lb[5] : lb[2]};
+      for (int k = 0; k < 3; ++k) {
+        const double v = rm[k * 4] * q[0] + rm[k * 4 + 1] * q[1] + rm[k * 4 + 2] * q[2] + rm[k * 4 + 3];
+        mn[k] = std::min(mn[k], v);
+        mx[k] = std::max(mx[k], v);
+      }
+    }
+    for (int k = 0; k < 3; ++k) { out.aabbs[6 * i + k] = mn[k]; out.aabbs[6 * i + 3 + k] = mx[k]; }
+  }
+  return out;
+}
+
+void refit_tlas_host(BinaryBvhHost& tl, const double* aabbs, size_t n) {
+  // refitTlas (shared-bvh/src/tlas.ts:990-1012): same topology and leaf
+  // assignment; leaves take the union of their instances' AABBs (stored as f32
+  // like a build), interior nodes the union of their children, bottom-up
+  // (preorder: children come after their parent)
+  for (size_t i = tl.nodes.size(); i-- > 0;) {
+    BinaryNode& nd = tl.nodes[i];
+    if (is_leaf_word(nd.w7)) {
+      double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      const uint32_t first = nd.w6, count = nd.w7 & 0xFFFFu;
+      for (uint32_t j = 0; j < count; ++j) {
+        const uint32_t inst = tl.reordered_to_source[first + j];
+        if (inst >= n) fail(VT_ERR_BUILD, "top-level leaf references instance " + std::to_string(inst));
+        for (int k = 0; k < 3; ++k) {
+          mn[k] = std::min(mn[k], aabbs[6 * inst + k]);
+          mx[k] = std::max(mx[k], aabbs[6 * inst + 3 + k]);
+        }
+      }
+      for (int k = 0; k < 3; ++k) {
+        nd.mn[k] = (float)mn[k];
+        nd.mx[k] = (float)mx[k];
+      }
+    } else {
+      const BinaryNode &l = tl.nodes[i + 1], &r = tl.nodes[i + nd.w6];
+      for (int k = 0; k < 3; ++k) {
+        nd.mn[k] = std::min(l.mn[k], r.mn[k]);
+        nd.mx[k] = std::max(l.mx[k], r.mx[k]);
+      }
+    }
+  }
+}
+
 PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base) {
   if (!sc) fail(VT_ERR_INVALID_ARGUMENT, "scene is null");
   if (sc->mesh_count && !sc->meshes) fail(VT_ERR_INVALID_ARGUMENT, "meshes is null");
@@ -183,42 +260,12 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
       vbase += md.vertex_count;
       tbase += md.triangle_count;
     }
-    // instances: world-to-local rows and world AABBs (transformAabb, scenePack.ts:197-223)
+    if (sc->instance_count && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
     const size_t ni = sc->instance_count;
-    std::vector<InstanceRecord> recs(ni);
-    std::vector<double> aabbs(6 * ni);
-    for (size_t i = 0; i < ni; ++i) {
-      const vt_instance_desc& id = sc->instances[i];
-      if (id.mesh >= sc->mesh_count) fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references mesh " +
-                                                            std::to_string(id.mesh));
-      if (id.material >= sc->material_count)
-        fail(VT_ERR_RANGE, "instance " + std::to_string(i) + " references material " + std::to_string(id.material));
-      if (mats[id.material].emissive) fail(VT_ERR_INVALID_ARGUMENT, "emissive materials are not supported on instances");
-      double rm[16], inv[16];
-      for (int r = 0; r < 4; ++r)
-        for (int c = 0; c < 4; ++c) rm[r * 4 + c] = id.local_to_world[c * 4 + r];
-      if (!invert4(rm, inv)) fail(VT_ERR_INVALID_ARGUMENT, "instance " + std::to_string(i) + " is not invertible");
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 4; ++c) inst_rows.push_back(id.local_to_world[c * 4 + r]);
-      InstanceRecord& rec = recs[i];
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 4; ++c) rec.w2l[4 * r + c] = (float)inv[r * 4 + c];
-      rec.blas_root = blas_root[id.mesh];
-      rec.instance_id = (uint32_t)i;
-      rec.material = id.material;
-      rec.pad = mats[id.material].flags;
-      const auto& lb = local_box[id.mesh];
-      double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-      for (int c = 0; c < 8; ++c) {
-        const double q[3] = {(c & 1) ? lb[3] : lb[0], (c & 2) ? lb[4] : lb[1], (c & 4) ? lb[5] : lb[2]};
-        for (int k = 0; k < 3; ++k) {
-          const double v = rm[k * 4] * q[0] + rm[k * 4 + 1] * q[1] + rm[k * 4 + 2] * q[2] + rm[k * 4 + 3];
-          mn[k] = std::min(mn[k], v);
-          mx[k] = std::max(mx[k], v);
-        }
-      }
-      for (int k = 0; k < 3; ++k) { aabbs[6 * i + k] = mn[k]; aabbs[6 * i + 3 + k] = mx[k]; }
-    }
+    InstanceSet placed = place_instances(sc->instances, ni, mats, blas_root, local_box);
+    std::vector<InstanceRecord>& recs = placed.recs;
+    std::vector<double>& aabbs = placed.aabbs;
+    inst_rows = std::move(placed.rows);
     BinaryBvhHost tl = build_tlas_host(aabbs.data(), ni);
     root = (uint32_t)(node_words.size() / 20);
     WideBvhHost tw = encode_wide_tlas(tl, recs.data(), root);
@@ -228,6 +275,9 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     std::memcpy(inst_tab.data(), recs.data(), ni * sizeof(InstanceRecord));
     depth = tw.depth + blas_depth;
     p.binary = std::move(tl);
+    p.blas_root = std::move(blas_root);
+    p.local_box = std::move(local_box);
+    p.blas_depth = blas_depth;
   }
   WideBvhHost w;
   w.nodes = std::move(node_words);

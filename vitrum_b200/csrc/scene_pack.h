@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <vector>
 
@@ -35,7 +36,25 @@ struct PackedScene {
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
   size_t ntri = 0;
+  // two-level: per mesh its bottom-level root node and local bounds; the deepest bottom level
+  std::vector<uint32_t> blas_root;
+  std::vector<std::array<double, 6>> local_box;
+  int blas_depth = 0;
 };
+
+// Instances placed over bottom-level trees: records (world-to-local rows, BLAS
+// root, id, material, material flags), world AABBs (6 doubles each) and
+// local-to-world rows (12 floats each).
+struct InstanceSet {
+  std::vector<InstanceRecord> recs;
+  std::vector<double> aabbs;
+  std::vector<float> rows;
+};
+InstanceSet place_instances(const vt_instance_desc* insts, size_t n, const std::vector<pt::Material>& mats,
+                            const std::vector<uint32_t>& blas_root,
+                            const std::vector<std::array<double, 6>>& local_box);
+// New instance AABBs into an existing top level: same topology, bounds recomputed bottom-up.
+void refit_tlas_host(BinaryBvhHost& tl, const double* aabbs, size_t n);
 
 // Validates and packs; single-level trees are offset by node_base / rec_base
 // (scenes concatenated into shared arrays); instanced scenes need both zero.

@@ -371,6 +371,18 @@ class Engine:
         desc, keep = _marshal_scene(scene)
         N.call("vt_set_scene", self.handle, ctypes.byref(desc))
 
+    def update_instances(self, instances: Sequence[Instance], rebuild: bool = False) -> None:
+        """New placements (mesh, material, transform) for the current scene's
+        instances, same count (vt_update_instances): the top level is refitted
+        (refitTlasTransforms) or, with rebuild, rebuilt over the new bounds
+        (rebuildTlasReuseBlas); bottom levels are kept.  Clears the accumulation."""
+        arr = (_InstanceDesc * max(1, len(instances)))()
+        for i, inst in enumerate(instances):
+            M = np.asarray(inst.local_to_world, np.float32).reshape(4, 4)
+            arr[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
+        N.call("vt_update_instances", self.handle, ctypes.cast(arr, ctypes.c_void_p), len(instances),
+               1 if rebuild else 0)
+
     def render_frame(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,
                      frame_seed: int = 0) -> dict:
         view, proj = camera.matrices(width / height)
