@@ -174,3 +174,16 @@ def test_watertight_kernel_bit_exact(cuda):
             assert gf[0].tobytes() == np.float32(ref["t"]).tobytes(), i
             assert np.array_equal(gf[1:4], ref["bary"]), i
             assert got[i, 5] == ref["side"] and got[i, 6] == ref["zero_edge_mask"], i
+
+
+def test_differential_gate_leaf1(cuda):
+    """The reference's CWBVH differential gate (compressedWideBvhDifferential.test.ts:239-279):
+    128-triangle random mesh, leaf size 1, 512 aimed and random rays with
+    random tMin / tMax; device closest and any hit equal the oracle's, with
+    more than 100 hits and 100 misses."""
+    from differential_cases import differential_rays, random_mesh
+    soup, centers, normals = random_mesh()
+    rays = differential_rays(centers, normals)
+    g, w = _build_both(soup, maxLeafTriangles=1)
+    rep = _assert_parity(soup, rays, g, w, "differential")
+    assert rep["hits"] > 100 and rep["n"] - rep["hits"] > 100, rep

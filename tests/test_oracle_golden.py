@@ -297,3 +297,18 @@ def test_wt_agrees_with_fp64_on_random_pairs():
         if w["hit"] and h:
             assert abs(w["t"] - t) <= 1e-4 * t
     assert hits > 500 and agree == 3000
+
+
+def test_differential_gate_leaf1_wide_equals_brute_force():
+    # compressedWideBvhDifferential.test.ts:239-279 on the oracle: the leaf-1
+    # 8-wide traversal answers exactly what brute force answers
+    from differential_cases import differential_rays, random_mesh
+    soup, centers, normals = random_mesh()
+    rays = differential_rays(centers, normals)
+    w = oracle.build_compressed_wide_bvh(soup.positions, soup.indices, max_leaf=1)
+    prim, t, _ = oracle.first_hit(w, soup.positions, rays)[:3]
+    bprim, bt = oracle.brute_first_hit(soup.positions, soup.indices, rays)[:2]
+    assert np.array_equal(prim, bprim)
+    assert np.allclose(t[prim >= 0], bt[prim >= 0], rtol=1e-12)
+    hits = int((prim >= 0).sum())
+    assert hits > 100 and len(rays) - hits > 100, hits
