@@ -195,6 +195,18 @@ vt_status vt_bvh_trace_any_device(vt_bvh* b, const vt_ray* d_rays, size_t n, uin
   });
 }
 
+// Host-buffer queries above this size run in chunks on two streams, so that the
+// copies of one chunk overlap the traversal of the other (with page-locked host
+// buffers the copies are asynchronous; with pageable ones they serialise, as
+// any copy from pageable memory does).
+constexpr size_t kQueryChunk = 1u << 19;
+
+static void ensure_copy_streams(vt_bvh* b) {
+  for (cudaStream_t& s : b->copy_streams)
+    if (!s) VT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  b->chunk_counters.resize(2);
+}
+
 vt_status vt_bvh_trace_closest(vt_bvh* b, const vt_ray* rays, size_t n, vt_hit* hits) {
   return guard([&] {
     check_trace_args(b, rays, n, hits);
@@ -202,12 +214,30 @@ vt_status vt_bvh_trace_closest(vt_bvh* b, const vt_ray* rays, size_t n, vt_hit* 
     DeviceScope ds(b->device);
     b->rays_scratch.resize(2 * n);
     b->hits_scratch.resize(n);
-    VT_CUDA(cudaMemcpy(b->rays_scratch.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice));
-    TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr), n);
-    a.hits = b->hits_scratch.ptr;
-    launch_trace_closest(a, 0);
-    VT_CUDA(cudaGetLastError());
-    VT_CUDA(cudaMemcpy(hits, b->hits_scratch.ptr, n * sizeof(vt_hit), cudaMemcpyDeviceToHost));
+    if (n <= kQueryChunk) {
+      VT_CUDA(cudaMemcpy(b->rays_scratch.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice));
+      TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr), n);
+      a.hits = b->hits_scratch.ptr;
+      launch_trace_closest(a, 0);
+      VT_CUDA(cudaGetLastError());
+      VT_CUDA(cudaMemcpy(hits, b->hits_scratch.ptr, n * sizeof(vt_hit), cudaMemcpyDeviceToHost));
+    } else {
+      ensure_copy_streams(b);
+      VT_CUDA(cudaStreamSynchronize(0));  // earlier work on the legacy stream (builds, status resets) is done
+      size_t k = 0;
+      for (size_t c = 0; c < n; c += kQueryChunk, ++k) {
+        cudaStream_t s = b->copy_streams[k & 1];
+        const size_t m = std::min(kQueryChunk, n - c);
+        VT_CUDA(cudaMemcpyAsync(b->rays_scratch.ptr + 2 * c, rays + c, m * sizeof(vt_ray), cudaMemcpyHostToDevice, s));
+        TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr + 2 * c), m);
+        a.hits = b->hits_scratch.ptr + c;
+        a.counter = b->chunk_counters.ptr + (k & 1);
+        launch_trace_closest(a, s);
+        VT_CUDA(cudaGetLastError());
+        VT_CUDA(cudaMemcpyAsync(hits + c, b->hits_scratch.ptr + c, m * sizeof(vt_hit), cudaMemcpyDeviceToHost, s));
+      }
+      for (cudaStream_t s : b->copy_streams) VT_CUDA(cudaStreamSynchronize(s));
+    }
     check_status(b);
   });
 }

@@ -24,4 +24,11 @@ struct vt_bvh {
   vt::DeviceBuffer<float4> rays_scratch;
   vt::DeviceBuffer<int4> hits_scratch;
   vt::DeviceBuffer<uint8_t> occ_scratch;
+  // two streams and ray counters for the chunked host-buffer queries (created on first use)
+  cudaStream_t copy_streams[2] = {nullptr, nullptr};
+  vt::DeviceBuffer<unsigned long long> chunk_counters;
+  ~vt_bvh() {
+    for (cudaStream_t& s : copy_streams)
+      if (s) cudaStreamDestroy(s);
+  }
 };
