@@ -350,6 +350,38 @@ vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
  * 3 doubles per pixel each. */
 vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
 
+/* What this engine renders (Engine.capabilities, core/src/engine/capabilities.ts;
+ * pt-webgpu/src/capabilities.ts): limits and the supported scene features, for
+ * the binding's capability / support-manifest object. */
+#define VT_EMITTER_POINT 1u
+#define VT_EMITTER_SPOT 2u
+#define VT_EMITTER_DIRECTIONAL 4u
+#define VT_EMITTER_RECT_AREA 8u
+#define VT_EMITTER_DISC_AREA 16u
+#define VT_EMITTER_MESH_AREA 32u        /* emissive materials on meshes (single-level scenes) */
+#define VT_EMITTER_ENVIRONMENT 64u      /* equirectangular RGB image */
+#define VT_MATERIAL_FEATURE_BASE 1u     /* base colour, roughness, metallic, emission */
+#define VT_MATERIAL_FEATURE_TRANSMISSION 2u  /* transmission, ior (smooth and rough) */
+#define VT_MATERIAL_FEATURE_SPECULAR 4u      /* KHR specular factor */
+#define VT_MATERIAL_FEATURE_DOUBLE_SIDED 8u
+#define VT_MATERIAL_FEATURE_CAST_SHADOW 16u
+#define VT_FEATURE_INSTANCES 1u         /* two-level scenes */
+#define VT_FEATURE_INSTANCE_UPDATES 2u  /* vt_update_instances */
+#define VT_FEATURE_RADIANCE_CACHE 4u    /* vt_set_nrc */
+#define VT_FEATURE_BATCH 8u             /* vt_batch_* */
+#define VT_FEATURE_PICK 16u             /* vt_pick (engines created with debug) */
+#define VT_FEATURE_OUTPUT_CAPTURE 32u   /* vt_capture_output */
+#define VT_FEATURE_FP64_MOMENTS 64u     /* vt_capture_moments (oracle_accumulation) */
+typedef struct vt_capabilities {
+  int32_t max_bounces_limit;        /* largest max_bounces */
+  int32_t max_samples_per_pixel;    /* this engine's accumulation cap */
+  int32_t max_viewport;             /* pixels per side */
+  uint32_t emitter_kinds;           /* VT_EMITTER_* bits */
+  uint32_t material_features;       /* VT_MATERIAL_FEATURE_* bits */
+  uint32_t features;                /* VT_FEATURE_* bits available on this engine */
+} vt_capabilities;
+vt_status vt_get_capabilities(const vt_engine* engine, vt_capabilities* capabilities);
+
 /* New placements for the instances of the current two-level scene (moving
  * instances, changing their mesh or material), without rebuilding any
  * bottom-level tree: refitTlasTransforms (shared-bvh/src/scenePack.ts:1310,

@@ -249,3 +249,13 @@ def test_capture_output_is_the_present_pass(cuda, tonemap, exposure, space):
     with pytest.raises(N.VtError):
         N.call("vt_capture_output", e.handle, None, N.ctypes.c_void_p(out.ctypes.data), out.size)
     e.dispose()
+
+
+def test_capabilities(cuda):
+    e = Engine(max_bounces=3, max_samples_per_pixel=77, debug=True)
+    c = e.capabilities
+    assert c["maxBouncesLimit"] == 8 and c["maxSamplesPerPixel"] == 77 and c["maxViewport"] == 16384
+    assert set(c["emitterKinds"]) == {"point", "spot", "directional", "rect-area", "disc-area", "mesh-area",
+                                      "environment"}
+    assert "pick" in c["features"] and "fp64-moments" not in c["features"]
+    e.dispose()

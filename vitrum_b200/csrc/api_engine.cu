@@ -715,6 +715,23 @@ vt_status vt_set_scene(vt_engine* e, const vt_scene_desc* scene) {
   });
 }
 
+vt_status vt_get_capabilities(const vt_engine* e, vt_capabilities* c) {
+  return vt::guard([&] {
+    if (!e || !c) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    c->max_bounces_limit = 8;
+    c->max_samples_per_pixel = e->opts.max_samples_per_pixel;
+    c->max_viewport = 16384;
+    c->emitter_kinds = VT_EMITTER_POINT | VT_EMITTER_SPOT | VT_EMITTER_DIRECTIONAL | VT_EMITTER_RECT_AREA |
+                       VT_EMITTER_DISC_AREA | VT_EMITTER_MESH_AREA | VT_EMITTER_ENVIRONMENT;
+    c->material_features = VT_MATERIAL_FEATURE_BASE | VT_MATERIAL_FEATURE_TRANSMISSION |
+                           VT_MATERIAL_FEATURE_SPECULAR | VT_MATERIAL_FEATURE_DOUBLE_SIDED |
+                           VT_MATERIAL_FEATURE_CAST_SHADOW;
+    c->features = VT_FEATURE_INSTANCES | VT_FEATURE_INSTANCE_UPDATES | VT_FEATURE_RADIANCE_CACHE | VT_FEATURE_BATCH |
+                  VT_FEATURE_OUTPUT_CAPTURE | (e->opts.debug ? VT_FEATURE_PICK : 0u) |
+                  (e->opts.oracle_accumulation ? VT_FEATURE_FP64_MOMENTS : 0u);
+  });
+}
+
 vt_status vt_update_instances(vt_engine* e, const vt_instance_desc* instances, size_t count, int32_t rebuild) {
   return vt::guard([&] {
     if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");

@@ -66,6 +66,12 @@ class _DiscDesc(ctypes.Structure):
                 ("radiance", ctypes.c_float * 3)]
 
 
+class _Capabilities(ctypes.Structure):
+    _fields_ = [("max_bounces_limit", ctypes.c_int32), ("max_samples_per_pixel", ctypes.c_int32),
+                ("max_viewport", ctypes.c_int32), ("emitter_kinds", ctypes.c_uint32),
+                ("material_features", ctypes.c_uint32), ("features", ctypes.c_uint32)]
+
+
 class _PresentOptions(ctypes.Structure):
     _fields_ = [("tonemap", ctypes.c_int32), ("exposure", ctypes.c_float), ("srgb", ctypes.c_int32)]
 
@@ -370,6 +376,22 @@ class Engine:
     def set_scene(self, scene: Scene) -> None:
         desc, keep = _marshal_scene(scene)
         N.call("vt_set_scene", self.handle, ctypes.byref(desc))
+
+    EMITTER_KINDS = {1: "point", 2: "spot", 4: "directional", 8: "rect-area", 16: "disc-area", 32: "mesh-area",
+                     64: "environment"}
+    FEATURES = {1: "instances", 2: "instance-updates", 4: "radiance-cache", 8: "batch", 16: "pick",
+                32: "output-capture", 64: "fp64-moments"}
+
+    @property
+    def capabilities(self) -> dict:
+        """Engine.capabilities (vt_get_capabilities): limits, emitter kinds, features."""
+        c = _Capabilities()
+        N.call("vt_get_capabilities", self.handle, ctypes.byref(c))
+        return {"maxBouncesLimit": c.max_bounces_limit, "maxSamplesPerPixel": c.max_samples_per_pixel,
+                "maxViewport": c.max_viewport,
+                "emitterKinds": sorted(v for k, v in self.EMITTER_KINDS.items() if c.emitter_kinds & k),
+                "features": sorted(v for k, v in self.FEATURES.items() if c.features & k),
+                "materialFeatures": c.material_features}
 
     def update_instances(self, instances: Sequence[Instance], rebuild: bool = False) -> None:
         """New placements (mesh, material, transform) for the current scene's
