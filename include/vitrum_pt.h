@@ -261,7 +261,10 @@ typedef struct vt_instance_desc {
 } vt_instance_desc;
 
 /* Scene (core Scene, core/src/scene/index.ts:42-46): primitives, emitters,
- * environment.  The environment is an equirectangular RGB image (row 0 at +y). */
+ * environment.  The environment is an equirectangular RGB image: row 0 at +y
+ * (theta = acos(y)), column u = atan2(z, x) / 2pi + 0.5, so +x is the middle
+ * column (the reference's environmentLookup, pt-webgpu/src/wgsl/pathTrace/
+ * connect.wgsl.ts:139-142). */
 typedef struct vt_scene_desc {
   const vt_mesh_desc* meshes;
   size_t mesh_count;
@@ -284,6 +287,21 @@ typedef struct vt_scene_desc {
   const vt_disc_light_desc* disc_lights;
   size_t disc_light_count;
 } vt_scene_desc;
+
+/* Procedural sky (core ProceduralSkyEnvironment, core/src/scene/environment.ts:59-71):
+ * the Preetham 1999 daylight model baked into an equirectangular RGB map that
+ * is then given as the scene's environment (the reference bakes 256 x 128:
+ * pt-webgpu/src/scene/environmentPacking.ts:221-270).  Host only. */
+typedef struct vt_sky_desc {
+  float sun_direction[3];   /* towards the sun (zero: +y) */
+  float turbidity;          /* clamped to [1.5, 30]; the reference's default 2 */
+  float rayleigh;           /* >= 0, default 1 (scales the sky) */
+  float mie_coefficient;    /* >= 0, default 0.005 (haze) */
+  float mie_directional_g;  /* Henyey-Greenstein g of the haze, default 0.8 */
+  float intensity;          /* >= 0, default 1 */
+} vt_sky_desc;
+vt_status vt_bake_preetham_sky(const vt_sky_desc* sky, int32_t width, int32_t height, float* rgb,
+                               size_t float_capacity);
 
 /* Per-frame input (core FrameInput, core/src/frame.ts:91): camera matrices
  * column-major, viewport, sampling. */

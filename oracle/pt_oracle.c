@@ -505,9 +505,11 @@ static int cdf_search(const float* cdf, int n, float u) {
   return lo;
 }
 static void env_texel(const orc_pt_t* S, v3 d, int* col, int* row, float* st) {
-  float y = fminf(fmaxf(d.y, -1.0f), 1.0f), theta = acosf(y), phi = atan2f(d.z, d.x);
-  if (phi < 0.0f) phi += 2.0f * PI_F;
-  *col = (int)(phi * (0.5f / PI_F) * S->env_w);
+  /* u = phi / 2pi + 0.5 (wrapped), row 0 at +y (environmentLookup, connect.wgsl.ts:139-142) */
+  float y = fminf(fmaxf(d.y, -1.0f), 1.0f), theta = acosf(y);
+  float u = atan2f(d.z, d.x) * (0.5f / PI_F) + 0.5f;
+  if (u >= 1.0f) u -= 1.0f;
+  *col = (int)(u * S->env_w);
   if (*col > S->env_w - 1) *col = S->env_w - 1;
   *row = (int)(theta * (1.0f / PI_F) * S->env_h);
   if (*row > S->env_h - 1) *row = S->env_h - 1;
@@ -686,7 +688,7 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
   float fv = m1 > m0 ? (u1 - m0) / (m1 - m0) : 0.5f, fu = c1 > c0 ? (u2 - c0) / (c1 - c0) : 0.5f;
   float v = ((float)row + fminf(fmaxf(fv, 0.0f), 0.999999f)) / (float)S->env_h;
   float u = ((float)col + fminf(fmaxf(fu, 0.0f), 0.999999f)) / (float)S->env_w;
-  float theta = v * PI_F, phi = u * 2.0f * PI_F, st = sinf(theta);
+  float theta = v * PI_F, phi = (u - 0.5f) * 2.0f * PI_F, st = sinf(theta);
   ls.wi = V(st * cosf(phi), cosf(theta), st * sinf(phi));
   ls.dist = INFINITY;
   ls.Le = env_le(S, col, row);

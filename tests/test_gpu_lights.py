@@ -191,3 +191,24 @@ def test_spot_and_disc_validation(cuda):
         with pytest.raises(Exception):
             e.set_scene(plane_scene(**kw))
         e.dispose()
+
+
+def test_procedural_sky_matches_cpu_oracle(cuda):
+    # Preetham daylight baked into the environment (vt_bake_preetham_sky), importance
+    # sampled with its sun disc: device vs CPU oracle over a box room without a ceiling
+    sc, cam = scenes.box_room(wall_cells=8, box_cells=4)
+    sc.meshes = [m for i, m in enumerate(sc.meshes[:-1]) if i != 1]
+    sc.environment = scenes.preetham_sky((0.3, 0.8, -0.4), turbidity=3.0, intensity=0.05)
+    W = H = 20
+    n, B = 256, 3
+    e = Engine(max_bounces=B, oracle_accumulation=True)
+    e.set_scene(sc)
+    e.render_frame(cam, W, H, samples=n)
+    gm, gv = e.capture_moments()
+    e.dispose()
+    s, q = oracle.pt_render(sc, cam, W, H, n, B)
+    cm = s / n
+    cv = np.maximum(q / n - cm * cm, 0) * n / (n - 1)
+    z = np.abs(gm - cm) / (np.sqrt((gv + cv) / n) + 1e-9)
+    assert gm.mean() > 0 and (z > 4).sum() <= 3
+    assert abs(gm.mean() / cm.mean() - 1) < 1e-2

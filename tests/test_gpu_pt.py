@@ -259,3 +259,24 @@ def test_capabilities(cuda):
                                       "environment"}
     assert "pick" in c["features"] and "fp64-moments" not in c["features"]
     e.dispose()
+
+
+def test_environment_equirect_convention(cuda):
+    # row 0 at +y, u = atan2(z, x) / 2pi + 0.5: the +x horizon is the middle column
+    # (environmentLookup, connect.wgsl.ts:139-142)
+    from vitrum_b200.engine import Environment
+    env = np.zeros((8, 16, 3), np.float32)
+    env[4, 8] = 5.0                     # theta in [pi/2, 5pi/8), phi in [0, pi/8)
+    sc = Scene(meshes=[Mesh(np.zeros((3, 3), np.float32), np.array([[0, 1, 2]], np.uint32), 0)],
+               materials=[Material()], environment=Environment(env))
+    look = Camera(eye=(0.0, 0.0, 0.0), target=(1.0, -0.15, 0.15), fov_y_deg=1.0, near=0.01, far=10.0)
+    e = Engine(max_bounces=1)
+    e.set_scene(sc)
+    e.render_frame(look, 4, 4, samples=4)
+    assert np.allclose(e.capture_frame()[..., :3], 5.0)
+    back = Camera(eye=(0.0, 0.0, 0.0), target=(-1.0, -0.15, 0.15), fov_y_deg=1.0, near=0.01, far=10.0)
+    e.render_frame(back, 4, 4, samples=4)
+    assert np.allclose(e.capture_frame()[..., :3], 0.0)
+    s, _ = oracle.pt_render(sc, look, 4, 4, 4, 1)
+    assert np.allclose(s / 4, 5.0)
+    e.dispose()

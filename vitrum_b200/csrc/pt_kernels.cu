@@ -59,9 +59,11 @@ __device__ __forceinline__ uint32_t cdf_search(const float* cdf, uint32_t n, flo
 __device__ __forceinline__ void env_texel(const SceneView& sc, float3 d, int& col, int& row, float& sin_t) {
   const float y = fminf(fmaxf(d.y, -1.0f), 1.0f);
   const float theta = acosf(y);
-  float phi = atan2f(d.z, d.x);
-  if (phi < 0.0f) phi += 2.0f * CUDART_PI_F;
-  col = min(sc.env_w - 1, (int)(phi * (0.5f / CUDART_PI_F) * sc.env_w));
+  // equirectangular convention u = phi / 2pi + 0.5 (wrapped), +x at the middle
+  // column, row 0 at +y (environmentLookup, connect.wgsl.ts:139-142)
+  float u = atan2f(d.z, d.x) * (0.5f / CUDART_PI_F) + 0.5f;
+  if (u >= 1.0f) u -= 1.0f;
+  col = min(sc.env_w - 1, (int)(u * sc.env_w));
   row = min(sc.env_h - 1, (int)(theta * (1.0f / CUDART_PI_F) * sc.env_h));
   sin_t = sinf(theta);
 }
@@ -275,7 +277,7 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
   const float fu = c1 > c0 ? (u2 - c0) / (c1 - c0) : 0.5f;
   const float v = ((float)row + fminf(fmaxf(fv, 0.0f), 0.999999f)) / (float)sc.env_h;
   const float u = ((float)col + fminf(fmaxf(fu, 0.0f), 0.999999f)) / (float)sc.env_w;
-  const float theta = v * CUDART_PI_F, phi = u * 2.0f * CUDART_PI_F;
+  const float theta = v * CUDART_PI_F, phi = (u - 0.5f) * 2.0f * CUDART_PI_F;
   const float st = sinf(theta);
   ls.wi = f3(st * cosf(phi), cosf(theta), st * sinf(phi));
   ls.dist = CUDART_INF_F;

@@ -213,7 +213,7 @@ class RectLight:
 
 @dataclass
 class Environment:
-    rgb: np.ndarray        # (H, W, 3) float32 equirectangular, row 0 at +y
+    rgb: np.ndarray        # (H, W, 3) float32 equirectangular: row 0 at +y, u = atan2(z, x)/2pi + 0.5
     intensity: float = 1.0
 
 

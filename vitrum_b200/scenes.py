@@ -243,6 +243,27 @@ def gradient_sky(width: int = 256, height: int = 128, horizon=(0.9, 0.9, 1.0), z
     return np.ascontiguousarray(np.broadcast_to(rows[:, None, :], (height, width, 3)), np.float32)
 
 
+def preetham_sky(sun_direction=(0.3, 0.8, 0.2), turbidity: float = 2.0, rayleigh: float = 1.0,
+                 mie_coefficient: float = 0.005, mie_directional_g: float = 0.8, intensity: float = 1.0,
+                 width: int = 256, height: int = 128):
+    """Procedural daylight (core ProceduralSkyEnvironment): the Preetham 1999 sky
+    baked by vt_bake_preetham_sky into a width x height equirectangular map,
+    returned as an engine Environment (the reference bakes 256 x 128)."""
+    import ctypes
+    from . import _native as N
+    from .engine import Environment
+
+    class _Sky(ctypes.Structure):
+        _fields_ = [("sun_direction", ctypes.c_float * 3), ("turbidity", ctypes.c_float),
+                    ("rayleigh", ctypes.c_float), ("mie_coefficient", ctypes.c_float),
+                    ("mie_directional_g", ctypes.c_float), ("intensity", ctypes.c_float)]
+
+    d = _Sky((ctypes.c_float * 3)(*sun_direction), turbidity, rayleigh, mie_coefficient, mie_directional_g, intensity)
+    rgb = np.empty((height, width, 3), np.float32)
+    N.call("vt_bake_preetham_sky", ctypes.byref(d), width, height, ctypes.c_void_p(rgb.ctypes.data), rgb.size)
+    return Environment(rgb)
+
+
 def instanced_cloud(n_instances: int = 1024, seed: int = 3, n_points: int = 32, sphere_levels=(3, 4, 5, 6),
                     torus_segments=(256, 64), cube_cells=(32, 64, 128), extent: float = 20.0):
     """Two-level instanced workload: 8 prototype meshes (icospheres at levels
