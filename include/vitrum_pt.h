@@ -286,6 +286,7 @@ typedef struct vt_scene_desc {
   size_t spot_light_count;
   const vt_disc_light_desc* disc_lights;
   size_t disc_light_count;
+  float environment_rotation_y;  /* CCW rotation of the environment about +y, radians (HdriEnvironment.rotationY) */
 } vt_scene_desc;
 
 /* Procedural sky (core ProceduralSkyEnvironment, core/src/scene/environment.ts:59-71):

@@ -263,7 +263,8 @@ def _pt_lib():
         L.orc_pt_render.restype = ctypes.c_int
         L.orc_pt_render.argtypes = [P, ctypes.c_long, P, ctypes.c_long, P, P, ctypes.c_int, P, ctypes.c_long, P,
                                     ctypes.c_long, P, ctypes.c_long, P,
-                                    ctypes.c_int, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, P, ctypes.c_int,
+                                    ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                     ctypes.c_int, P, P, P, P, ctypes.c_long, P]
         L._pt_ready = True
@@ -404,11 +405,12 @@ def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_bas
     totals = np.zeros(2, np.int64)
     dls = directional_lights(scene)
     als = area_lights(scene)
+    er = 0.0 if scene.environment is None else float(getattr(scene.environment, "rotation_y", 0.0))
     r = _pt_lib().orc_pt_render(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
                                 _p(pts) if pts.size else None, pts.shape[0], _p(als) if als.size else None,
                                 als.shape[0], _p(dls) if dls.size else None,
                                 dls.shape[0], _p(env) if env is not None else None,
-                                ew, eh, ei, _p(ivp), width, height, spp, max_bounces, seed, sample_base, bias,
+                                ew, eh, ei, er, _p(ivp), width, height, spp, max_bounces, seed, sample_base, bias,
                                 nthreads, _p(s), _p(q), _p(lc) if log_rays else None, _p(ls) if log_rays else None,
                                 max(log_rays, 0), _p(totals))
     if r != 0:

@@ -126,6 +126,7 @@ typedef struct {
   const float* env_cond;  /* H*(W+1) */
   int env_w, env_h, env_sampleable;
   float env_scale;
+  float env_cos, env_sin; /* environment rotation about +y */
   int n_entries;
   float bias;
   /* camera / frame */
@@ -504,7 +505,9 @@ static int cdf_search(const float* cdf, int n, float u) {
   }
   return lo;
 }
-static void env_texel(const orc_pt_t* S, v3 d, int* col, int* row, float* st) {
+static void env_texel(const orc_pt_t* S, v3 dw, int* col, int* row, float* st) {
+  /* into the unrotated map (rotateYNeg, connectCore.wgsl.ts:27-30) */
+  v3 d = V(S->env_cos * dw.x - S->env_sin * dw.z, dw.y, S->env_sin * dw.x + S->env_cos * dw.z);
   /* u = phi / 2pi + 0.5 (wrapped), row 0 at +y (environmentLookup, connect.wgsl.ts:139-142) */
   float y = fminf(fmaxf(d.y, -1.0f), 1.0f), theta = acosf(y);
   float u = atan2f(d.z, d.x) * (0.5f / PI_F) + 0.5f;
@@ -689,7 +692,8 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
   float v = ((float)row + fminf(fmaxf(fv, 0.0f), 0.999999f)) / (float)S->env_h;
   float u = ((float)col + fminf(fmaxf(fu, 0.0f), 0.999999f)) / (float)S->env_w;
   float theta = v * PI_F, phi = (u - 0.5f) * 2.0f * PI_F, st = sinf(theta);
-  ls.wi = V(st * cosf(phi), cosf(theta), st * sinf(phi));
+  v3 md = V(st * cosf(phi), cosf(theta), st * sinf(phi));
+  ls.wi = V(S->env_cos * md.x + S->env_sin * md.z, md.y, -S->env_sin * md.x + S->env_cos * md.z);
   ls.dist = INFINITY;
   ls.Le = env_le(S, col, row);
   ls.pdf = psel * env_pdf(S, col, row, st);
@@ -847,11 +851,14 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
                   const float* materials, int n_mat, const float* points, long n_points, const float* areas,
                   long n_areas, const float* dirs,
                   long n_dirs, const float* env,
-                  int env_w, int env_h, float env_scale, const float* inv_vp, int width, int height, int spp,
+                  int env_w, int env_h, float env_scale, float env_rotation, const float* inv_vp, int width,
+                  int height, int spp,
                   int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
                   double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals) {
   orc_pt_t S;
   memset(&S, 0, sizeof S);
+  S.env_cos = (float)cos((double)env_rotation);
+  S.env_sin = (float)sin((double)env_rotation);
   S.pos = pos;
   S.idx = idx;
   S.tmat = tri_mat;

@@ -4,6 +4,7 @@ and disc, with MIS for escaped BSDF rays), spot lights (cone with penumbra,
 decay and range), and analytic rectangle and disc lights (area sampling plus
 analytic hits of BSDF rays, never occluders), against known answers and the
 CPU oracle."""
+import dataclasses
 import math
 
 import numpy as np
@@ -212,3 +213,28 @@ def test_procedural_sky_matches_cpu_oracle(cuda):
     z = np.abs(gm - cm) / (np.sqrt((gv + cv) / n) + 1e-9)
     assert gm.mean() > 0 and (z > 4).sum() <= 3
     assert abs(gm.mean() / cm.mean() - 1) < 1e-2
+
+
+def test_environment_rotation_equals_shifted_map(cuda):
+    # rotationY = 2 pi k / W looks the map up k columns further (rotateYNeg,
+    # connectCore.wgsl.ts:27-30): the same image as the map with its columns shifted
+    from vitrum_b200.engine import Environment
+    sc, cam = scenes.box_room(wall_cells=8, box_cells=4)
+    sc.meshes = [m for i, m in enumerate(sc.meshes[:-1]) if i != 1]   # no ceiling, no emitter
+    rng = np.random.default_rng(4)
+    env = (rng.uniform(0.0, 1.0, (8, 16, 3)) ** 4 * 6).astype(np.float32)
+    k = 3
+    rot = dataclasses.replace(sc, environment=Environment(env, rotation_y=2 * math.pi * k / 16))
+    shift = dataclasses.replace(sc, environment=Environment(np.roll(env, -k, axis=1)))
+    out = []
+    for s in (rot, shift):
+        e = Engine(max_bounces=3, oracle_accumulation=True)
+        e.set_scene(s)
+        e.render_frame(cam, 20, 20, samples=2048)
+        out.append(e.capture_moments())
+        e.dispose()
+    (ma, va), (mb, vb) = out
+    z = np.abs(ma - mb) / (np.sqrt((va + vb) / 2048) + 1e-9)
+    assert ma.mean() > 0 and (z > 4).sum() <= 3 and abs(ma.mean() / mb.mean() - 1) < 1.5e-2
+    s, _ = oracle.pt_render(rot, cam, 20, 20, 512, 3)
+    assert abs((s / 512).mean() / ma.mean() - 1) < 4e-2

@@ -362,6 +362,8 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       B.view.env_w = p.env_w;
       B.view.env_h = p.env_h;
       B.view.env_scale = p.env_scale;
+      B.view.env_cos = (float)std::cos((double)p.env_rotation);
+      B.view.env_sin = (float)std::sin((double)p.env_rotation);
       B.view.n_light_entries =
           (B.view.n_emitters ? 1u : 0u) + B.view.n_points + B.view.n_area + B.view.n_dirs + (p.env_sampleable ? 1u : 0u);
     }

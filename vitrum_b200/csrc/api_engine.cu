@@ -198,6 +198,8 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.env_w = p.env_w;
   v.env_h = p.env_h;
   v.env_scale = p.env_scale;
+  v.env_cos = (float)std::cos((double)p.env_rotation);
+  v.env_sin = (float)std::sin((double)p.env_rotation);
   v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_area + v.n_dirs + (p.env_sampleable ? 1u : 0u);
   e->view = v;
   e->binary = std::move(p.binary);

@@ -56,7 +56,9 @@ __device__ __forceinline__ uint32_t cdf_search(const float* cdf, uint32_t n, flo
 }
 
 // ---------------------------------------------------------------- environment
-__device__ __forceinline__ void env_texel(const SceneView& sc, float3 d, int& col, int& row, float& sin_t) {
+__device__ __forceinline__ void env_texel(const SceneView& sc, float3 dw, int& col, int& row, float& sin_t) {
+  // world direction into the unrotated map: rotation about +y by -rotationY (rotateYNeg, connectCore.wgsl.ts:27-30)
+  const float3 d = f3(sc.env_cos * dw.x - sc.env_sin * dw.z, dw.y, sc.env_sin * dw.x + sc.env_cos * dw.z);
   const float y = fminf(fmaxf(d.y, -1.0f), 1.0f);
   const float theta = acosf(y);
   // equirectangular convention u = phi / 2pi + 0.5 (wrapped), +x at the middle
@@ -279,7 +281,8 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
   const float u = ((float)col + fminf(fmaxf(fu, 0.0f), 0.999999f)) / (float)sc.env_w;
   const float theta = v * CUDART_PI_F, phi = (u - 0.5f) * 2.0f * CUDART_PI_F;
   const float st = sinf(theta);
-  ls.wi = f3(st * cosf(phi), cosf(theta), st * sinf(phi));
+  const float3 md = f3(st * cosf(phi), cosf(theta), st * sinf(phi));  // map space; to world by +rotationY
+  ls.wi = f3(sc.env_cos * md.x + sc.env_sin * md.z, md.y, -sc.env_sin * md.x + sc.env_cos * md.z);
   ls.dist = CUDART_INF_F;
   ls.Le = env_radiance(sc, (int)col, (int)row);
   ls.pdf = psel * env_pdf_texel(sc, (int)col, (int)row, st);

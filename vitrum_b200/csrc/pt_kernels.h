@@ -47,6 +47,7 @@ struct SceneView {
   const float* env_conditional = nullptr;  // env_h rows of env_w + 1 entries
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
+  float env_cos = 1.0f, env_sin = 0.0f;  // environment rotation about +y (rotationY)
   // light entries, chosen uniformly by NEE: the emissive-mesh group (if any),
   // positional lights, analytic area lights, directional lights, environment (if any)
   uint32_t n_light_entries = 0;

@@ -470,6 +470,8 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   p.env_w = has_env ? sc->environment_width : 0;
   p.env_h = has_env ? sc->environment_height : 0;
   p.env_scale = sc->environment_intensity > 0.0f ? sc->environment_intensity : 1.0f;
+  if (!std::isfinite(sc->environment_rotation_y)) fail(VT_ERR_RANGE, "environment_rotation_y is not finite");
+  p.env_rotation = sc->environment_rotation_y;
   p.ntri = ntri;
   return p;
 }

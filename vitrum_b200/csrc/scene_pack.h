@@ -35,6 +35,7 @@ struct PackedScene {
   bool has_env = false, env_sampleable = false;
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
+  float env_rotation = 0.0f;
   size_t ntri = 0;
   // two-level: per mesh its bottom-level root node and local bounds; the deepest bottom level
   std::vector<uint32_t> blas_root;

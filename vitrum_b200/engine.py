@@ -86,7 +86,7 @@ class _SceneDesc(ctypes.Structure):
                 ("directional_light_count", ctypes.c_size_t), ("rect_lights", ctypes.c_void_p),
                 ("rect_light_count", ctypes.c_size_t), ("spot_lights", ctypes.c_void_p),
                 ("spot_light_count", ctypes.c_size_t), ("disc_lights", ctypes.c_void_p),
-                ("disc_light_count", ctypes.c_size_t)]
+                ("disc_light_count", ctypes.c_size_t), ("environment_rotation_y", ctypes.c_float)]
 
 
 class _FrameInput(ctypes.Structure):
@@ -215,6 +215,7 @@ class RectLight:
 class Environment:
     rgb: np.ndarray        # (H, W, 3) float32 equirectangular: row 0 at +y, u = atan2(z, x)/2pi + 0.5
     intensity: float = 1.0
+    rotation_y: float = 0.0  # CCW rotation of the dome about +y, radians (HdriEnvironment.rotationY)
 
 
 @dataclass
@@ -335,7 +336,8 @@ def _marshal_scene(scene: "Scene"):
                       ew, eh, ei, ctypes.cast(dls, ctypes.c_void_p), len(scene.directional_lights),
                       ctypes.cast(rls, ctypes.c_void_p), len(scene.rect_lights),
                       ctypes.cast(sls, ctypes.c_void_p), len(scene.spot_lights),
-                      ctypes.cast(dcs, ctypes.c_void_p), len(scene.disc_lights))
+                      ctypes.cast(dcs, ctypes.c_void_p), len(scene.disc_lights),
+                      0.0 if scene.environment is None else float(scene.environment.rotation_y))
     return desc, (keep, meshes, insts, mats, pls, dls, rls, sls, dcs)
 
 
