@@ -45,7 +45,7 @@ class BatchItem:
 
 class Batch:
     def __init__(self, items: Sequence[BatchItem], device: int = 0, max_bounces: int = 8):
-        opts = _EngineOptions(max_bounces, 1 << 20, 0, 0, 0, 0)
+        opts = _EngineOptions(max_bounces, 1 << 20, 0, 0, 0, 0, 0)
         h = ctypes.c_void_p()
         N.call("vt_batch_create", device, ctypes.byref(opts), ctypes.byref(h))
         self._h = h

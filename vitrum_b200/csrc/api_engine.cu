@@ -141,7 +141,7 @@ void upload(DeviceBuffer<T>& dst, const std::vector<T>& src, cudaStream_t s) {
 
 // ---------------------------------------------------------------- scene
 void set_scene(vt_engine* e, const vt_scene_desc* sc) {
-  vt::PackedScene p = vt::pack_scene(sc, 0, 0);
+  vt::PackedScene p = vt::pack_scene(sc, 0, 0, e->opts.bvh_max_leaf);
   cudaStream_t s = e->stream;
   VT_CUDA(cudaStreamSynchronize(s));
   e->drop_graphs();
@@ -694,6 +694,8 @@ vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine*
     if (e->opts.max_samples_per_pixel == 0) e->opts.max_samples_per_pixel = 4096;
     if (e->opts.max_samples_per_pixel < 1) fail(VT_ERR_RANGE, "max_samples_per_pixel must be >= 1");
     if (e->opts.wave_paths < 0) fail(VT_ERR_RANGE, "wave_paths must be >= 0");
+    if (e->opts.bvh_max_leaf == 0) e->opts.bvh_max_leaf = vt::kEngineLeafDefault;
+    if (e->opts.bvh_max_leaf < 1 || e->opts.bvh_max_leaf > 4) fail(VT_ERR_RANGE, "bvh_max_leaf must be in [0, 4]");
     vt::DeviceScope ds(device);
     VT_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     VT_CUDA(cudaEventCreate(&e->ev0));

@@ -150,7 +150,7 @@ void refit_tlas_host(BinaryBvhHost& tl, const double* aabbs, size_t n) {
   }
 }
 
-PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base) {
+PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf) {
   if (!sc) fail(VT_ERR_INVALID_ARGUMENT, "scene is null");
   if (sc->mesh_count && !sc->meshes) fail(VT_ERR_INVALID_ARGUMENT, "meshes is null");
   if (sc->material_count && !sc->materials) fail(VT_ERR_INVALID_ARGUMENT, "materials is null");
@@ -214,6 +214,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   const size_t ntri = tri_mat.size();
   // geometry
   BuildOptions bo;
+  bo.max_leaf = max_leaf;
   const bool two_level = sc->instance_count > 0;
   if (two_level && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
   std::vector<uint32_t> node_words;

@@ -59,7 +59,13 @@ void refit_tlas_host(BinaryBvhHost& tl, const double* aabbs, size_t n);
 
 // Validates and packs; single-level trees are offset by node_base / rec_base
 // (scenes concatenated into shared arrays); instanced scenes need both zero.
-PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base);
+PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf = 4);
+
+// Triangles per leaf of the path tracer's own trees when the options leave it
+// open: two per leaf traced the box room 4 % and the instanced cloud 7 % faster
+// than the reference build's default of four (fewer watertight tests per ray
+// for a few more node visits).
+constexpr int kEngineLeafDefault = 2;
 
 // 4x4 inverse (Gauss-Jordan, partial pivoting); false when singular.
 bool invert4(const double* m, double* inv);
