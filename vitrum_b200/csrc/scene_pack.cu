@@ -215,6 +215,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   // geometry
   BuildOptions bo;
   bo.max_leaf = max_leaf;
+  bo.bins = kEngineBins;
   const bool two_level = sc->instance_count > 0;
   if (two_level && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
   std::vector<uint32_t> node_words;

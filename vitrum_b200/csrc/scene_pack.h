@@ -66,6 +66,9 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
 // than the reference build's default of four (fewer watertight tests per ray
 // for a few more node visits).
 constexpr int kEngineLeafDefault = 2;
+// SAH bins of the path tracer's trees: 32 instead of the reference's 16 traced
+// the box room 1.4 % faster for a 0.05 s longer build.
+constexpr int kEngineBins = 32;
 
 // 4x4 inverse (Gauss-Jordan, partial pivoting); false when singular.
 bool invert4(const double* m, double* inv);
