@@ -58,10 +58,13 @@ def test_nrc_options_validation(cuda):
 
 
 def test_trained_cache_lowers_equal_time_error(cuda):
-    """Four frames after a warm-up of the cache (its training is online, every
+    """Eight frames after a warm-up of the cache (its training is online, every
     frame): the NRC frames against plain path tracing given the same device
     time, both against a 65,536-spp FP64-accumulated plain oracle, on the box
-    room (indirect light and caustics through the glass box dominate)."""
+    room (indirect light and caustics through the glass box dominate).  The
+    cache keeps training during the measured frames, so its output drifts a
+    little from frame to frame (a mean bias of up to ~4 % over four frames);
+    eight frames average that drift down so the factor below holds run to run."""
     sc, cam = scenes.box_room(wall_cells=32, box_cells=16)
     W, H, B = 192, 192, 5
     o = Engine(max_bounces=B, oracle_accumulation=True, max_samples_per_pixel=1 << 17)
@@ -78,7 +81,7 @@ def test_trained_cache_lowers_equal_time_error(cuda):
         n.render_frame(cam, W, H, samples=16, frame_seed=5)
     n.reset()
     t_nrc = 0.0
-    for _ in range(4):
+    for _ in range(8):
         n.render_frame(cam, W, H, samples=16, frame_seed=5)
         t_nrc += n.stats()["last_frame_ms"]
     e_nrc = relmse(n.capture_frame()[..., :3], ref)
@@ -93,7 +96,7 @@ def test_trained_cache_lowers_equal_time_error(cuda):
     p.render_frame(cam, W, H, samples=spp, frame_seed=7)
     e_plain = relmse(p.capture_frame()[..., :3], ref)
     p.dispose()
-    print(f"equal time ({t_nrc:.2f} ms): NRC 4 x 16 spp relMSE {e_nrc:.4f} vs plain {spp} spp {e_plain:.4f} "
+    print(f"equal time ({t_nrc:.2f} ms): NRC 8 x 16 spp relMSE {e_nrc:.4f} vs plain {spp} spp {e_plain:.4f} "
           f"({e_plain / e_nrc:.2f}x)")
     assert e_nrc < 0.5 * e_plain
 

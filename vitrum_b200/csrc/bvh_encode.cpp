@@ -1,10 +1,20 @@
 // bvh_encode.cpp -- 8-wide collapse and compressed-node encoding.
 //
-// Collapse: the reference's greedy rule (collectWideChildren,
-// packages/shared-bvh/src/compressedWideBvh.ts:215-242): starting from the
-// two children of a binary interior node, repeatedly replace the interior
-// child of largest surface area by its two children until 8 slots are used
-// or only leaves remain.  The resulting wide topology is the reference's.
+// Collapse, two rules:
+//  - the reference's greedy rule (collectWideChildren,
+//    packages/shared-bvh/src/compressedWideBvh.ts:215-242): starting from the
+//    two children of a binary interior node, repeatedly replace the interior
+//    child of largest surface area by its two children until 8 slots are used
+//    or only leaves remain.  The resulting wide topology is the reference's;
+//    every reference-facing tree uses it.
+//  - the SAH-optimal rule of Ylitie, Karras & Laine 2017 ("Efficient
+//    incoherent ray traversal on GPUs through compressed wide BVHs", sec. 3.1)
+//    for the renderer's own trees: a dynamic programme over the binary tree
+//    picks, per wide node, the frontier of at most 8 descendants, and per
+//    frontier subtree of at most 4 triangles whether it becomes one leaf slot,
+//    minimising the surface-area cost sum(A(node)) * c_node +
+//    sum(A(leaf) * triangles) * c_tri.  It only regroups the binary tree's
+//    nodes, so the triangle set, the boxes and every hit are unchanged.
 //
 // Encoding (ours, for the GPU): breadth-first node numbering so the hottest
 // nodes form a prefix, slot assignment for octant-ordered traversal, u8
@@ -53,6 +63,101 @@ int collect_wide_children(const BinaryNode* nodes, uint32_t root, uint32_t out[8
   }
   return n;
 }
+
+namespace {
+
+// Ylitie et al. 2017, sec. 3.1, restated on this binary layout (left child
+// at i + 1, right child at i + w6, so children follow their parent).
+//   C(n)    cost of n as one slot of its parent:
+//           min(leaf: c_tri * A(n) * count(n)   [count <= 4, contiguous],
+//               node: c_node * A(n) + G(n, 8))
+//   G(n, k) cost of spreading n's subtree over k slots:
+//           min over a in [1, k-1] of F(left, a) + F(right, k - a)
+//   F(x, a) = C(x) for a = 1 or x a binary leaf, else min(C(x), G(x, a))
+struct SahCollapse {
+  const BinaryNode* nodes;
+  size_t n;
+  std::vector<double> c;        // C(n)
+  std::vector<double> g;        // G(n, k) at 8 * n + k, k in [2, 8]
+  std::vector<uint8_t> split;   // slots given to the left child at 8 * n + k
+  std::vector<uint32_t> first, count;
+  std::vector<uint8_t> as_leaf; // C(n) taken by the leaf branch
+  std::vector<BinaryNode> ext;  // the binary nodes, then one leaf node per mergeable subtree
+  std::vector<uint32_t> merged; // index in ext of n's merged leaf (n itself for binary leaves)
+
+  double f(uint32_t x, int a) const {
+    if (a < 2 || is_leaf_word(nodes[x].w7)) return c[x];
+    return std::min(c[x], g[8 * (size_t)x + a]);
+  }
+
+  SahCollapse(const BinaryBvhHost& bin, double c_node, double c_tri)
+      : nodes(bin.nodes.data()), n(bin.nodes.size()), c(n), g(8 * n, 0.0), split(8 * n, 0), first(n), count(n),
+        as_leaf(n, 0), ext(bin.nodes), merged(n) {
+    for (size_t i = n; i-- > 0;) {
+      const BinaryNode& b = nodes[i];
+      const double area = half_area(b);
+      if (is_leaf_word(b.w7)) {
+        first[i] = b.w6;
+        count[i] = b.w7 & 0xFFFFu;
+        c[i] = c_tri * area * count[i];
+        as_leaf[i] = 1;
+        merged[i] = (uint32_t)i;
+        continue;
+      }
+      const uint32_t l = (uint32_t)i + 1, r = (uint32_t)i + b.w6;
+      first[i] = first[l];
+      count[i] = count[l] + count[r];
+      const bool contiguous = first[r] == first[l] + count[l];
+      for (int k = 2; k <= 8; ++k) {
+        double best = INFINITY;
+        int at = 1;
+        for (int a = 1; a < k; ++a) {
+          const double v = f(l, a) + f(r, k - a);
+          if (v < best) { best = v; at = a; }
+        }
+        g[8 * i + k] = best;
+        split[8 * i + k] = (uint8_t)at;
+      }
+      c[i] = c_node * area + g[8 * i + 8];
+      merged[i] = 0;
+      if (count[i] <= 4 && contiguous) {
+        const double leaf = c_tri * area * count[i];
+        if (leaf < c[i]) {
+          c[i] = leaf;
+          as_leaf[i] = 1;
+        }
+        BinaryNode m = b;
+        m.w6 = first[i];
+        m.w7 = 0xFFFF0000u | count[i];
+        merged[i] = (uint32_t)ext.size();
+        ext.push_back(m);
+      }
+    }
+  }
+
+  // frontier of x over a slots, appended to out (indices into ext)
+  void frontier(uint32_t x, int a, uint32_t* out, int& m) const {
+    if (a >= 2 && !is_leaf_word(nodes[x].w7) && g[8 * (size_t)x + a] < c[x]) {
+      const int s = split[8 * (size_t)x + a];
+      frontier(x + 1, s, out, m);
+      frontier(x + nodes[x].w6, a - s, out, m);
+      return;
+    }
+    out[m++] = as_leaf[x] ? merged[x] : x;
+  }
+
+  // children of the wide node rooted at binary node x (never a merged leaf)
+  int children(uint32_t x, uint32_t out[8]) const {
+    if (is_leaf_word(ext[x].w7)) { out[0] = x; return 1; }
+    const int s = split[8 * (size_t)x + 8];
+    int m = 0;
+    frontier(x + 1, s, out, m);
+    frontier(x + nodes[x].w6, 8 - s, out, m);
+    return m;
+  }
+};
+
+}  // namespace
 
 // Greedy slot assignment: slot s is visited first by rays whose direction
 // sign bits (x:4, y:2, z:1; bit set = negative) equal s, so it should hold
@@ -126,10 +231,10 @@ static int grid_exponent(double extent) {
 // node_base and record indices by rec_base (trees concatenated into shared
 // arrays); emit(leaf, slot_records) writes a leaf's payload records (16
 // floats each) for the leaf's binary node.
-template <class EmitLeaf>
-static WideBvhHost encode_core(const BinaryBvhHost& bin, uint32_t node_base, uint32_t rec_base, EmitLeaf emit) {
+template <class Children, class EmitLeaf>
+static WideBvhHost encode_core(const BinaryBvhHost& bin, const BinaryNode* nodes, uint32_t node_base,
+                               uint32_t rec_base, Children children_of, EmitLeaf emit) {
   WideBvhHost out;
-  const BinaryNode* nodes = bin.nodes.data();
   const size_t nleaf_items = bin.reordered_to_source.size();
   std::vector<uint32_t> wide_bin;   // binary node behind each wide node (BFS order)
   std::vector<int> level;
@@ -150,7 +255,7 @@ static WideBvhHost encode_core(const BinaryBvhHost& bin, uint32_t node_base, uin
   for (size_t wi = 0; wi < wide_bin.size(); ++wi) {
     const BinaryNode& parent = nodes[wide_bin[wi]];
     uint32_t ch[8];
-    int n = collect_wide_children(nodes, wide_bin[wi], ch);
+    int n = children_of(wide_bin[wi], ch);
     int slot_of[8];
     assign_slots(nodes, parent, ch, n, slot_of);
     int child_at_slot[8];
@@ -219,8 +324,9 @@ static WideBvhHost encode_core(const BinaryBvhHost& bin, uint32_t node_base, uin
 }
 
 WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
-                        int idx_stride, const uint32_t* tri_materials, uint32_t node_base, uint32_t rec_base) {
-  return encode_core(bin, node_base, rec_base, [&](const BinaryNode& leaf, float* recs) {
+                        int idx_stride, const uint32_t* tri_materials, uint32_t node_base, uint32_t rec_base,
+                        const WideCollapse* sah) {
+  auto emit = [&](const BinaryNode& leaf, float* recs) {
     const uint32_t cnt = leaf.w7 & 0xFFFFu, first = leaf.w6;
     for (uint32_t t = 0; t < cnt; ++t) {
       const uint32_t src = bin.reordered_to_source[first + t];
@@ -240,11 +346,22 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
       rec[14] = nn[2];
       rec[15] = valid ? 1.0f : 0.0f;
     }
-  });
+  };
+  if (sah && !bin.nodes.empty()) {
+    const SahCollapse plan(bin, sah->c_node, sah->c_tri);
+    return encode_core(bin, plan.ext.data(), node_base, rec_base,
+                       [&](uint32_t x, uint32_t* out) { return plan.children(x, out); }, emit);
+  }
+  const BinaryNode* nodes = bin.nodes.data();
+  return encode_core(bin, nodes, node_base, rec_base,
+                     [&](uint32_t x, uint32_t* out) { return collect_wide_children(nodes, x, out); }, emit);
 }
 
 WideBvhHost encode_wide_tlas(const BinaryBvhHost& tlas, const InstanceRecord* instances, uint32_t node_base) {
-  return encode_core(tlas, node_base, 0, [&](const BinaryNode& leaf, float* recs) {
+  const BinaryNode* nodes = tlas.nodes.data();
+  return encode_core(tlas, nodes, node_base, 0,
+                     [&](uint32_t x, uint32_t* out) { return collect_wide_children(nodes, x, out); },
+                     [&](const BinaryNode& leaf, float* recs) {
     const uint32_t cnt = leaf.w7 & 0xFFFFu, first = leaf.w6;
     for (uint32_t i = 0; i < cnt; ++i) {
       const uint32_t inst = tlas.reordered_to_source[first + i];

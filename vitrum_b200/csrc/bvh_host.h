@@ -43,11 +43,19 @@ BinaryBvhHost build_binary_host(const float* positions, size_t position_words, c
 // 8-wide collapse of one binary interior node (reference greedy rule).
 int collect_wide_children(const BinaryNode* nodes, uint32_t root, uint32_t out[8]);
 
+// Surface-area cost weights of the SAH-optimal collapse: c_node per wide node
+// entered, c_tri per triangle tested, both per unit of box half-area.
+struct WideCollapse {
+  double c_node = 1.0;
+  double c_tri = 0.5;
+};
+
 // tri_materials (optional, one per source triangle) is stored in each record's v1.w.
 // node_base / rec_base offset the encoded indices for trees concatenated into shared arrays.
+// sah == nullptr: the reference's greedy collapse; else the SAH-optimal one with those weights.
 WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int pos_stride, const uint32_t* indices,
                         int idx_stride, const uint32_t* tri_materials = nullptr, uint32_t node_base = 0,
-                        uint32_t rec_base = 0);
+                        uint32_t rec_base = 0, const WideCollapse* sah = nullptr);
 
 // Top-level instance record (64 bytes): world-to-local affine rows, then
 // (BLAS root node, instance id, material, 0) as u32 bits.

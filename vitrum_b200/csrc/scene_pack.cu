@@ -224,7 +224,8 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   uint32_t root = 0;
   if (!two_level) {
     p.binary = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
-    WideBvhHost w = encode_wide(p.binary, pos.data(), 4, idx.data(), 4, tri_mat.data(), node_base, rec_base);
+    WideBvhHost w = encode_wide(p.binary, pos.data(), 4, idx.data(), 4, tri_mat.data(), node_base, rec_base,
+                                &kEngineCollapse);
     node_words = std::move(w.nodes);
     rec_floats = std::move(w.tris);
     depth = w.depth;
@@ -250,8 +251,8 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
         for (int k = 0; k < 3; ++k) mi[4 * t + k] -= (uint32_t)vbase;
       std::vector<uint32_t> mm(md.triangle_count, md.material);
       BinaryBvhHost b = build_binary_host(mp.data(), mp.size(), mi.data(), mi.size(), bo);
-      WideBvhHost w = encode_wide(b, mp.data(), 4, mi.data(), 4, mm.data(),
-                                          (uint32_t)(node_words.size() / 20), (uint32_t)(rec_floats.size() / 16));
+      WideBvhHost w = encode_wide(b, mp.data(), 4, mi.data(), 4, mm.data(), (uint32_t)(node_words.size() / 20),
+                                  (uint32_t)(rec_floats.size() / 16), &kEngineCollapse);
       blas_root[m] = (uint32_t)(node_words.size() / 20);
       node_words.insert(node_words.end(), w.nodes.begin(), w.nodes.end());
       rec_floats.insert(rec_floats.end(), w.tris.begin(), w.tris.end());
