@@ -371,6 +371,34 @@ vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
  * 3 doubles per pixel each. */
 vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
 
+/* Auxiliary frame outputs, the textures the reference's kernel writes beside
+ * the radiance (pt-webgpu/src/wgsl/pathTrace/kernel.wgsl.ts:936-960), as RGBA
+ * float32, row-major, top-left, one float4 per pixel:
+ *   VT_AUX_NORMAL_DEPTH  first-hit normal (facing the camera ray) * 0.5 + 0.5,
+ *                        distance from the camera ray's origin; a miss
+ *                        (0.5, 1, 0.5, 0)
+ *   VT_AUX_ALBEDO        first-hit base colour, 1; a miss 0
+ *   VT_AUX_MOTION        screen motion of the first-hit point in pixels,
+ *                        (ndc(viewProj) - ndc(prevViewProj)) * 0.5 * (width, height),
+ *                        0, 1 (kernelCore.wgsl.ts:28-42 projection); a miss (0, 0, 0, 1)
+ *   VT_AUX_VARIANCE      per-pixel variance of the sample luminance (Rec. 709
+ *                        weights) over every sample accumulated since the last
+ *                        reset, max(0, E[L^2] - E[L]^2), 0, 0, 0
+ * The first three hold the first hit of the last sample of the latest
+ * rendered frame (the reference stores them per sample, so the last one
+ * stays); before any frame all four are zero. */
+#define VT_AUX_NORMAL_DEPTH 0
+#define VT_AUX_ALBEDO 1
+#define VT_AUX_MOTION 2
+#define VT_AUX_VARIANCE 3
+vt_status vt_capture_aux(vt_engine* engine, int32_t kind, float* rgba, size_t float_capacity);
+/* FrameInput.prevViewMatrix / prevProjMatrix (frameParamsPacker.ts:225-229):
+ * the camera of the previous frame, column-major like vt_frame_input, for the
+ * motion output of the NEXT vt_render_frame / vt_profile_frame only; that
+ * frame uses its own matrices where none were set (zero motion).  NULL
+ * clears a pending pair. */
+vt_status vt_set_previous_camera(vt_engine* engine, const float* prev_view, const float* prev_projection);
+
 /* What this engine renders (Engine.capabilities, core/src/engine/capabilities.ts;
  * pt-webgpu/src/capabilities.ts): limits and the supported scene features, for
  * the binding's capability / support-manifest object. */
@@ -393,6 +421,7 @@ vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* varian
 #define VT_FEATURE_PICK 16u             /* vt_pick (engines created with debug) */
 #define VT_FEATURE_OUTPUT_CAPTURE 32u   /* vt_capture_output */
 #define VT_FEATURE_FP64_MOMENTS 64u     /* vt_capture_moments (oracle_accumulation) */
+#define VT_FEATURE_AUX_OUTPUTS 128u     /* vt_capture_aux, vt_set_previous_camera */
 typedef struct vt_capabilities {
   int32_t max_bounces_limit;        /* largest max_bounces */
   int32_t max_samples_per_pixel;    /* this engine's accumulation cap */

@@ -82,6 +82,13 @@ struct vt_engine {
   DeviceBuffer<float4> accum;
   DeviceBuffer<float4> present;     // present-pass output of vt_capture_output
   DeviceBuffer<double> sum64, sq64;
+  // auxiliary outputs (first-hit normal / depth, albedo, motion; luminance
+  // moments) and their per-frame constants (view-projections, recorded sample)
+  DeviceBuffer<float4> aux_nd, aux_albedo, aux_motion, aux_moments;
+  DeviceBuffer<float> aux_consts;
+  float aux_host[vt::pt::kAuxConsts] = {};
+  bool have_prev_camera = false;   // set by vt_set_previous_camera for the next frame only
+  float prev_view[16] = {}, prev_proj[16] = {};
   int samples = 0;
   float inv_vp[16] = {};
   float view_m[16] = {}, proj_m[16] = {};
@@ -438,6 +445,8 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
       f.nrc_tiles_x = n.tiles_x;
     }
   }
+  if (mode != kNrcTrain && e->aux_nd.ptr)
+    f.aux = {e->aux_nd.ptr, e->aux_albedo.ptr, e->aux_motion.ptr, e->aux_moments.ptr, e->aux_consts.ptr};
   VT_CUDA(cudaMemsetAsync(e->counters.ptr + vt::pt::kCntQuery, 0, 2 * sizeof(uint32_t), s));
   const vt::pt::WaveBuffers w = wave_buffers(e);
   vt::pt::AccumView a;
@@ -468,6 +477,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     B(StageTimer::kTraceClosest);
     vt::launch_trace_closest_records(t, s);
     E();
+    if (b == 0) vt::pt::launch_aux_first_hit(e->view, f, w, s);
     if (f.sort_by_material) {
       B(StageTimer::kSort);
       vt::pt::launch_sort_by_material(e->view, f, w, cur, cap, s);
@@ -548,6 +558,8 @@ void reset_accumulation(vt_engine* e) {
   if (e->accum.ptr) VT_CUDA(cudaMemsetAsync(e->accum.ptr, 0, e->accum.bytes(), e->stream));
   if (e->sum64.ptr) VT_CUDA(cudaMemsetAsync(e->sum64.ptr, 0, e->sum64.bytes(), e->stream));
   if (e->sq64.ptr) VT_CUDA(cudaMemsetAsync(e->sq64.ptr, 0, e->sq64.bytes(), e->stream));
+  for (DeviceBuffer<float4>* b : {&e->aux_nd, &e->aux_albedo, &e->aux_motion, &e->aux_moments})
+    if (b->ptr) VT_CUDA(cudaMemsetAsync(b->ptr, 0, b->bytes(), e->stream));
   VT_CUDA(cudaMemsetAsync(e->counters.ptr, 0, e->counters.bytes(), e->stream));
 }
 
@@ -570,6 +582,8 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     e->height = in->height;
     const size_t px = (size_t)in->width * in->height;
     e->accum.resize(px);
+    for (DeviceBuffer<float4>* b : {&e->aux_nd, &e->aux_albedo, &e->aux_motion, &e->aux_moments}) b->resize(px);
+    if (!e->aux_consts.ptr) e->aux_consts.resize(vt::pt::kAuxConsts);
     if (e->opts.oracle_accumulation) {
       e->sum64.resize(3 * px);
       e->sq64.resize(3 * px);
@@ -584,6 +598,8 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     e->drop_graphs();
     reset_accumulation(e);
   }
+  const bool prev_camera = e->have_prev_camera;
+  e->have_prev_camera = false;  // the pair applies to this frame only
   const int room = e->opts.max_samples_per_pixel - e->samples;
   out->width = e->width;
   out->height = e->height;
@@ -601,6 +617,13 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   spp_wave = std::min(spp_wave, spp);
   while (spp % spp_wave) --spp_wave;  // equal waves: one graph per frame shape
   ensure_capacity(e, wh * spp_wave);
+  // auxiliary-output constants of this frame: view-projections and the last sample
+  vt::view_proj(in->view, in->projection, e->aux_host);
+  if (prev_camera) vt::view_proj(e->prev_view, e->prev_proj, e->aux_host + 16);
+  else std::memcpy(e->aux_host + 16, e->aux_host, 16 * sizeof(float));
+  const uint32_t last_sample = (uint32_t)e->samples + spp - 1u;
+  std::memcpy(e->aux_host + 32, &last_sample, sizeof last_sample);
+  VT_CUDA(cudaMemcpyAsync(e->aux_consts.ptr, e->aux_host, sizeof e->aux_host, cudaMemcpyHostToDevice, e->stream));
   // with the cache: train, then render waves that end in cache queries
   int mode = kPlain;
   uint32_t wave_bounces = bounces;
@@ -732,7 +755,7 @@ vt_status vt_get_capabilities(const vt_engine* e, vt_capabilities* c) {
                            VT_MATERIAL_FEATURE_CAST_SHADOW;
     c->features = VT_FEATURE_INSTANCES | VT_FEATURE_INSTANCE_UPDATES | VT_FEATURE_RADIANCE_CACHE | VT_FEATURE_BATCH |
                   VT_FEATURE_OUTPUT_CAPTURE | (e->opts.debug ? VT_FEATURE_PICK : 0u) |
-                  (e->opts.oracle_accumulation ? VT_FEATURE_FP64_MOMENTS : 0u);
+                  (e->opts.oracle_accumulation ? VT_FEATURE_FP64_MOMENTS : 0u) | VT_FEATURE_AUX_OUTPUTS;
   });
 }
 
@@ -831,6 +854,50 @@ vt_status vt_capture_moments(vt_engine* e, double* mean_rgb, double* var_rgb, si
       mean_rgb[i] = m;
       var_rgb[i] = n > 1 ? std::max(0.0, (q - m * m) * n / (n - 1)) : 0.0;
     }
+  });
+}
+
+vt_status vt_capture_aux(vt_engine* e, int32_t kind, float* rgba, size_t cap) {
+  return vt::guard([&] {
+    if (!e || !rgba) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (kind < VT_AUX_NORMAL_DEPTH || kind > VT_AUX_VARIANCE) fail(VT_ERR_RANGE, "unknown auxiliary output");
+    if (!e->aux_nd.ptr) fail(VT_ERR_STATE, "captureFrame before renderFrame");
+    const size_t px = (size_t)e->width * e->height;
+    if (cap < 4 * px) fail(VT_ERR_RANGE, "capture buffer too small");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    const DeviceBuffer<float4>& src = kind == VT_AUX_NORMAL_DEPTH ? e->aux_nd
+                                      : kind == VT_AUX_ALBEDO     ? e->aux_albedo
+                                      : kind == VT_AUX_MOTION     ? e->aux_motion
+                                                                  : e->aux_moments;
+    VT_CUDA(cudaMemcpy(rgba, src.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (kind == VT_AUX_VARIANCE) {
+      // kernel.wgsl.ts:942-945: count = max(n, 1), varL = max(0, E[L^2] - E[L]^2)
+      for (size_t i = 0; i < px; ++i) {
+        float* m = rgba + 4 * i;
+        const float n = std::max(m[2], 1.0f);
+        const float mean = m[0] / n;
+        m[0] = std::max(0.0f, m[1] / n - mean * mean);
+        m[1] = m[2] = m[3] = 0.0f;
+      }
+    }
+  });
+}
+
+vt_status vt_set_previous_camera(vt_engine* e, const float* prev_view, const float* prev_projection) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "null engine");
+    if (!prev_view != !prev_projection) fail(VT_ERR_INVALID_ARGUMENT, "give both previous matrices or neither");
+    if (!prev_view) {
+      e->have_prev_camera = false;
+      return;
+    }
+    for (int i = 0; i < 16; ++i)
+      if (!std::isfinite(prev_view[i]) || !std::isfinite(prev_projection[i]))
+        fail(VT_ERR_RANGE, "previous camera matrices must be finite");
+    std::memcpy(e->prev_view, prev_view, sizeof e->prev_view);
+    std::memcpy(e->prev_proj, prev_projection, sizeof e->prev_proj);
+    e->have_prev_camera = true;
   });
 }
 

@@ -406,6 +406,59 @@ __device__ __forceinline__ void nrc_features(const Material& m, float3 P, float3
 // ---------------------------------------------------------------- shade
 // 8 resident blocks per SM (64 registers, some spilled to L1): the kernel is
 // load-latency bound, and occupancy beats spill-free code here.
+// ---------------------------------------------------------------- auxiliary outputs
+// projectToNdc (kernelCore.wgsl.ts:28-42): clip = M (p, 1) scaled by its
+// largest magnitude, (2, 2) when that is zero or not finite or w <= 0.
+__device__ __forceinline__ float2 project_ndc(const float* M, float3 p) {
+  float c[4];
+  for (int r = 0; r < 4; ++r) c[r] = M[4 * r] * p.x + M[4 * r + 1] * p.y + M[4 * r + 2] * p.z + M[4 * r + 3];
+  const float sc = fmaxf(fmaxf(fabsf(c[0]), fabsf(c[1])), fmaxf(fabsf(c[2]), fabsf(c[3])));
+  if (!(sc > 0.0f) || sc > 3.402823e38f) return make_float2(2.0f, 2.0f);
+  const float w = c[3] / sc;
+  if (!(w > 0.0f)) return make_float2(2.0f, 2.0f);
+  return make_float2((c[0] / sc) / w, (c[1] / sc) / w);
+}
+
+// First hit of the recorded sample (kernel.wgsl.ts:947-958), one thread per
+// pixel after the wave's bounce-0 closest-hit trace: the normal facing the
+// camera ray, the hit's distance from the ray origin, the base colour and the
+// screen motion; misses write the reference's defaults.  Queue slot == path
+// id at bounce 0, and the recorded sample's paths are one pixel-major block of
+// the wave; waves that do not hold the sample return at once.
+__global__ void k_aux_first_hit(SceneView sc, FrameView f, WaveBuffers w) {
+  const uint32_t wh = f.width * f.height;
+  const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= wh) return;
+  const uint32_t first = w.counters[kCntWaveSample], want = __float_as_uint(f.aux.consts[32]);
+  if (want < first || want - first >= f.spp_wave) return;
+  const uint32_t p = (want - first) * wh + pix;
+  const AuxView& a = f.aux;
+  const int4 h = w.hits[p];
+  if (h.x < 0) {
+    a.normal_depth[pix] = make_float4(0.5f, 1.0f, 0.5f, 0.0f);
+    a.albedo[pix] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.motion[pix] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    return;
+  }
+  const float4 r0 = w.rays[0][2 * p], r1 = w.rays[0][2 * p + 1];
+  const float3 o = f3(r0.x, r0.y, r0.z), d = f3(r1.x, r1.y, r1.z);
+  const float4 nr = __ldg(sc.tris + 4 * (size_t)(uint32_t)h.x + 3);
+  float3 ng = f3(nr.x, nr.y, nr.z);
+  if (h.z >= 0) {
+    const float4* ir = sc.inst_table + 4 * (size_t)h.z;
+    const float4 m0 = __ldg(ir), m1 = __ldg(ir + 1), m2 = __ldg(ir + 2);
+    ng = normalize(f3(m0.x * ng.x + m1.x * ng.y + m2.x * ng.z, m0.y * ng.x + m1.y * ng.y + m2.y * ng.z,
+                      m0.z * ng.x + m1.z * ng.y + m2.z * ng.z));
+  }
+  const float3 n = dot(d, ng) < 0.0f ? ng : -ng;
+  const float3 P = o + d * __int_as_float(h.y);
+  const float3 base = sc.materials[hit_material(sc, h)].base_color;
+  a.normal_depth[pix] = make_float4(n.x * 0.5f + 0.5f, n.y * 0.5f + 0.5f, n.z * 0.5f + 0.5f, sqrtf(dot(P - o, P - o)));
+  a.albedo[pix] = make_float4(base.x, base.y, base.z, 1.0f);
+  const float2 c = project_ndc(a.consts, P), q = project_ndc(a.consts + 16, P);
+  a.motion[pix] = make_float4((c.x - q.x) * 0.5f * (float)f.width, (c.y - q.y) * 0.5f * (float)f.height, 0.0f, 1.0f);
+}
+
 __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, WaveBuffers w, int cur, uint32_t bounce) {
   const int nxt = cur ^ 1;
   const uint32_t n = w.counters[cur];
@@ -648,10 +701,14 @@ __global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
   const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= wh) return;
   float3 s = f3(0.0f, 0.0f, 0.0f);
+  float l1 = 0.0f, l2 = 0.0f;  // luminance moments (varianceMomentsBuffer, kernel.wgsl.ts:936-940)
   double s64[3] = {0, 0, 0}, q64[3] = {0, 0, 0};
   for (uint32_t k = 0; k < f.spp_wave; ++k) {
     const float4 r = w.radiance[(size_t)k * wh + pix];
     s = s + f3(r.x, r.y, r.z);
+    const float lum = 0.2126f * r.x + 0.7152f * r.y + 0.0722f * r.z;
+    l1 += lum;
+    l2 += lum * lum;
     if (a.sum64) {
       const double v[3] = {r.x, r.y, r.z};
       for (int c = 0; c < 3; ++c) { s64[c] += v[c]; q64[c] += v[c] * v[c]; }
@@ -659,6 +716,10 @@ __global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
   }
   float4 acc = a.accum[pix];
   a.accum[pix] = make_float4(acc.x + s.x, acc.y + s.y, acc.z + s.z, acc.w + (float)f.spp_wave);
+  if (f.aux.moments) {
+    const float4 mo = f.aux.moments[pix];
+    f.aux.moments[pix] = make_float4(mo.x + l1, mo.y + l2, mo.z + (float)f.spp_wave, 0.0f);
+  }
   if (a.sum64) {
     for (int c = 0; c < 3; ++c) {
       a.sum64[3 * (size_t)pix + c] += s64[c];
@@ -921,6 +982,11 @@ void launch_accumulate_batch(const WaveBuffers& w, float4* accum, uint32_t capac
 
 void launch_nrc_tile_update(float* tile_stats, float* tile_error, uint32_t tiles, float alpha, cudaStream_t s) {
   k_nrc_tile_update<<<grid_for(tiles, 256), 256, 0, s>>>(tile_stats, tile_error, tiles, alpha);
+}
+
+void launch_aux_first_hit(const SceneView& sc, const FrameView& f, const WaveBuffers& w, cudaStream_t s) {
+  if (!f.aux.normal_depth) return;
+  k_aux_first_hit<<<grid_for(f.width * f.height, 256), 256, 0, s>>>(sc, f, w);
 }
 
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s) {

@@ -69,6 +69,19 @@ struct BatchScene {
   unsigned long long path_begin = 0;    // first path of this scene in the batch's path space
 };
 
+// Auxiliary outputs (kernel.wgsl.ts:936-960): one float4 per pixel each.
+// consts (device): view-projection (16 floats, row-major), the previous
+// frame's view-projection (16), then as u32 bits the accumulated sample index
+// whose first hit the normal / albedo / motion buffers record.
+struct AuxView {
+  float4* normal_depth = nullptr;  // (n * 0.5 + 0.5, distance) of the recorded sample's first hit
+  float4* albedo = nullptr;        // (base colour, 1)
+  float4* motion = nullptr;        // (pixels x, y, 0, 1)
+  float4* moments = nullptr;       // (sum L, sum L^2, samples, 0), L = Rec. 709 luminance of a sample
+  const float* consts = nullptr;
+};
+constexpr int kAuxConsts = 36;
+
 struct FrameView {
   float inv_vp[16];         // row-major inverse view-projection
   uint32_t width = 0, height = 0;
@@ -86,6 +99,7 @@ struct FrameView {
   uint32_t nrc_tile = 16, nrc_tiles_x = 0;
   float nrc_spread_c = 0.0f;           // > 0: spread termination (nrc_prefix unused): query at the first
                                        // vertex k >= 2 with a(x_k) > c * a0 (spreadTermination.ts:70-184)
+  AuxView aux;              // null buffers: no auxiliary outputs (training waves, batches)
   // batch: paths of many scenes in one wave (scene id in bits 8-15 of the path flags)
   const BatchScene* batch = nullptr;
   uint32_t n_scenes = 0;
@@ -137,6 +151,9 @@ void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w,
                   uint32_t capacity, cudaStream_t s);
 void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t s);
 void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView& a, cudaStream_t s);
+// Auxiliary outputs of the recorded sample, after the bounce-0 closest-hit trace
+// (no-op without aux buffers or when this wave does not hold that sample).
+void launch_aux_first_hit(const SceneView& sc, const FrameView& f, const WaveBuffers& w, cudaStream_t s);
 // Batch: the next `capacity` paths of the batch's path space (device cursor),
 // and their accumulation (atomic per pixel) followed by the cursor advance.
 void launch_raygen_batch(const FrameView& f, const WaveBuffers& w, uint32_t capacity, cudaStream_t s);

@@ -71,6 +71,14 @@ void inverse_view_proj(const float* view, const float* proj, float* out_rm) {
   for (int i = 0; i < 16; ++i) out_rm[i] = (float)inv[i];
 }
 
+void view_proj(const float* view, const float* proj, float* out_rm) {
+  double v[16], p[16], vp[16];
+  for (int i = 0; i < 16; ++i) { v[i] = view[i]; p[i] = proj[i]; }
+  mat_mul_cm(p, v, vp);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) out_rm[r * 4 + c] = (float)vp[c * 4 + r];
+}
+
 
 
 InstanceSet place_instances(const vt_instance_desc* insts, size_t ni, const std::vector<pt::Material>& mats,

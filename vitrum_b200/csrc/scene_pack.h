@@ -79,5 +79,7 @@ constexpr WideCollapse kEngineCollapse{1.0, 0.5};
 bool invert4(const double* m, double* inv);
 // inverse(P * V) of column-major view / projection as a row-major float matrix.
 void inverse_view_proj(const float* view, const float* proj, float* out_rm);
+// P * V of column-major view / projection as a row-major float matrix.
+void view_proj(const float* view, const float* proj, float* out_rm);
 
 }  // namespace vt

@@ -383,7 +383,7 @@ class Engine:
     EMITTER_KINDS = {1: "point", 2: "spot", 4: "directional", 8: "rect-area", 16: "disc-area", 32: "mesh-area",
                      64: "environment"}
     FEATURES = {1: "instances", 2: "instance-updates", 4: "radiance-cache", 8: "batch", 16: "pick",
-                32: "output-capture", 64: "fp64-moments"}
+                32: "output-capture", 64: "fp64-moments", 128: "aux-outputs"}
 
     @property
     def capabilities(self) -> dict:
@@ -408,8 +408,21 @@ class Engine:
         N.call("vt_update_instances", self.handle, ctypes.cast(arr, ctypes.c_void_p), len(instances),
                1 if rebuild else 0)
 
+    def set_previous_camera(self, camera: "Camera | None", aspect: "float | None" = None) -> None:
+        """FrameInput.prevViewMatrix / prevProjMatrix for the next frame's motion
+        output (that frame only), the camera at `aspect` (width / height); None clears."""
+        if camera is None:
+            N.call("vt_set_previous_camera", self.handle, None, None)
+            return
+        if not aspect or aspect <= 0:
+            raise ValueError("aspect (width / height) must be positive")
+        view, proj = camera.matrices(aspect)
+        N.call("vt_set_previous_camera", self.handle, (ctypes.c_float * 16)(*view), (ctypes.c_float * 16)(*proj))
+
     def render_frame(self, camera: Camera, width: int, height: int, samples: int = 1, bounces: int = 0,
-                     frame_seed: int = 0) -> dict:
+                     frame_seed: int = 0, prev_camera: "Camera | None" = None) -> dict:
+        if prev_camera is not None:
+            self.set_previous_camera(prev_camera, width / height)
         view, proj = camera.matrices(width / height)
         fin = _FrameInput((ctypes.c_float * 16)(*view), (ctypes.c_float * 16)(*proj), width, height, frame_seed,
                           samples, bounces)
@@ -461,6 +474,18 @@ class Engine:
         N.call("vt_capture_moments", self.handle, ctypes.c_void_p(m.ctypes.data), ctypes.c_void_p(v.ctypes.data),
                m.size)
         return m, v
+
+    AUX = {"normal_depth": 0, "albedo": 1, "motion": 2, "variance": 3}
+
+    def capture_aux(self, kind: str) -> np.ndarray:
+        """Auxiliary output (H, W, 4) float32: 'normal_depth' (n * 0.5 + 0.5,
+        distance), 'albedo', 'motion' (pixels) of the first hit of the latest
+        frame's last sample, or 'variance' (luminance variance in channel 0)."""
+        if kind not in self.AUX:
+            raise ValueError("kind must be one of %s" % sorted(self.AUX))
+        out = np.empty((self.height, self.width, 4), np.float32)
+        N.call("vt_capture_aux", self.handle, self.AUX[kind], ctypes.c_void_p(out.ctypes.data), out.size)
+        return out
 
     def trace_rays(self, rays: np.ndarray):
         """Closest hits of (n, 8) float32 rays [ox oy oz tmin dx dy dz tmax] against the scene.
