@@ -422,6 +422,7 @@ vt_status vt_set_previous_camera(vt_engine* engine, const float* prev_view, cons
 #define VT_FEATURE_OUTPUT_CAPTURE 32u   /* vt_capture_output */
 #define VT_FEATURE_FP64_MOMENTS 64u     /* vt_capture_moments (oracle_accumulation) */
 #define VT_FEATURE_AUX_OUTPUTS 128u     /* vt_capture_aux, vt_set_previous_camera */
+#define VT_FEATURE_MESH_UPDATES 256u    /* vt_update_mesh */
 typedef struct vt_capabilities {
   int32_t max_bounces_limit;        /* largest max_bounces */
   int32_t max_samples_per_pixel;    /* this engine's accumulation cap */
@@ -441,6 +442,14 @@ vt_status vt_get_capabilities(const vt_engine* engine, vt_capabilities* capabili
  * instance count must equal the scene's (VT_ERR_INVALID_ARGUMENT otherwise;
  * VT_ERR_STATE without an instanced scene).  Clears the accumulation. */
 vt_status vt_update_instances(vt_engine* engine, const vt_instance_desc* instances, size_t count, int32_t rebuild);
+/* rebuildPrimitiveBlas (shared-bvh/src/scenePack.ts:1763; splices :1006-1100):
+ * new vertices / triangles / material for mesh `mesh_index` of a scene with
+ * instances.  Its bottom-level tree is rebuilt and spliced in place (later
+ * meshes rebased when its size changed), then the top level is refitted over
+ * the instances' new bounds, or rebuilt when `rebuild` is 1.  The other meshes'
+ * trees are untouched; accumulation restarts.  A scene without instances has
+ * one flat tree: VT_ERR_STATE (set the scene again). */
+vt_status vt_update_mesh(vt_engine* engine, size_t mesh_index, const vt_mesh_desc* mesh, int32_t rebuild);
 
 /* captureFrame({colorSpace: 'output'}) (pt-webgpu/src/index.ts:2004-2033): the
  * present pass (pt-webgpu/src/wgsl/present.wgsl.ts; operators of

@@ -69,6 +69,7 @@ SIGNATURES = {
     "vt_capture": [P, P, SZ],
     "vt_capture_output": [P, P, P, SZ],
     "vt_update_instances": [P, P, SZ, I32],
+    "vt_update_mesh": [P, SZ, P, I32],
     "vt_get_capabilities": [P, P],
     "vt_bake_preetham_sky": [P, I32, I32, P, SZ],
     "vt_capture_moments": [P, P, P, SZ],

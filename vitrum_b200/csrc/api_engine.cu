@@ -64,6 +64,15 @@ struct vt_engine {
   int blas_depth = 0;
   uint32_t tlas_root = 0;
   std::vector<vt::pt::Material> mats_host;
+  // two-level scenes, for mesh updates: host copies of the bottom-level node
+  // words (tlas_root wide nodes) and of the triangle records, each mesh's first
+  // record and wide depth, and the current placements
+  std::vector<uint32_t> blas_words;
+  std::vector<float> rec_host;
+  std::vector<uint32_t> blas_rec_start;
+  std::vector<int> blas_depths;
+  std::vector<size_t> mesh_tris;   // source triangles per mesh
+  std::vector<vt_instance_desc> inst_descs;
   // vt_trace_rays staging
   DeviceBuffer<float4> q_rays;
   DeviceBuffer<int4> q_hits;
@@ -215,6 +224,20 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   e->blas_depth = p.blas_depth;
   e->tlas_root = p.root;
   e->mats_host = p.mats;
+  e->blas_rec_start = std::move(p.blas_rec_start);
+  e->blas_depths = std::move(p.blas_depths);
+  if (two_level) {
+    e->blas_words.assign(p.node_words.begin(), p.node_words.begin() + (size_t)p.root * 20);
+    e->rec_host = std::move(p.rec_floats);
+    e->inst_descs.assign(sc->instances, sc->instances + sc->instance_count);
+    e->mesh_tris.resize(sc->mesh_count);
+    for (size_t m = 0; m < sc->mesh_count; ++m) e->mesh_tris[m] = sc->meshes[m].triangle_count;
+  } else {
+    e->mesh_tris.clear();
+    e->blas_words.clear();
+    e->rec_host.clear();
+    e->inst_descs.clear();
+  }
   e->ntri = (int64_t)p.ntri;
   e->n_emitters = (int64_t)v.n_emitters;
   e->has_scene = true;
@@ -234,6 +257,7 @@ void update_instances(vt_engine* e, const vt_instance_desc* insts, size_t n, boo
                                       std::to_string(n) + " (set a new scene to change the membership)");
   if (!insts) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
   vt::InstanceSet placed = vt::place_instances(insts, n, e->mats_host, e->blas_root, e->local_box);
+  if (insts != e->inst_descs.data()) e->inst_descs.assign(insts, insts + n);
   vt::BinaryBvhHost tl;
   if (rebuild) {
     tl = vt::build_tlas_host(placed.aabbs.data(), n);
@@ -271,6 +295,69 @@ void update_instances(vt_engine* e, const vt_instance_desc* insts, size_t n, boo
   e->view.inst_table = e->inst_table.ptr;
   reset_accumulation(e);
   VT_CUDA(cudaStreamSynchronize(e->stream));
+}
+
+// New geometry for one mesh of a two-level scene (rebuildPrimitiveBlas,
+// shared-bvh/src/scenePack.ts:1763, and its in-place / resized splices
+// :1006-1100): the mesh's bottom level is rebuilt and spliced into the
+// concatenated node and record arrays; when its size changed, the later
+// meshes' node and record indices and roots are rebased.  The top level is
+// then refitted (or rebuilt) over the instances' new bounds.
+void update_mesh(vt_engine* e, size_t m, const vt_mesh_desc* md, bool rebuild) {
+  if (!e->has_scene || e->n_instances == 0)
+    fail(VT_ERR_STATE, "mesh updates need a scene with instances (set the scene again to change a flat scene)");
+  if (!md) fail(VT_ERR_INVALID_ARGUMENT, "mesh is null");
+  const size_t nm = e->blas_root.size();
+  if (m >= nm) fail(VT_ERR_RANGE, "mesh index " + std::to_string(m) + " out of range");
+  std::vector<float> pos;
+  std::vector<uint32_t> idx, tri_mat;
+  vt::append_mesh(*md, m, e->mats_host.size(), pos, idx, tri_mat);
+  const uint32_t node0 = e->blas_root[m], rec0 = e->blas_rec_start[m];
+  const uint32_t node1 = m + 1 < nm ? e->blas_root[m + 1] : e->tlas_root;
+  const uint32_t rec1 = m + 1 < nm ? e->blas_rec_start[m + 1] : (uint32_t)(e->rec_host.size() / 16);
+  const uint32_t old_tlas_root = e->tlas_root;
+  vt::BlasPack bp = vt::pack_blas(pos, idx, md->material, node0, rec0, e->opts.bvh_max_leaf);
+  const int64_t dn = (int64_t)(bp.wide.nodes.size() / 20) - (int64_t)(node1 - node0);
+  const int64_t dr = (int64_t)(bp.wide.tris.size() / 16) - (int64_t)(rec1 - rec0);
+  if ((int64_t)e->rec_host.size() / 16 + dr + 32 >= (int64_t)0x40000000)
+    fail(VT_ERR_RANGE, "triangle records exceed 2^30");
+  // splice, then rebase the later bottom levels (child base at word 4, triangle base at word 5)
+  e->blas_words.erase(e->blas_words.begin() + (size_t)node0 * 20, e->blas_words.begin() + (size_t)node1 * 20);
+  e->blas_words.insert(e->blas_words.begin() + (size_t)node0 * 20, bp.wide.nodes.begin(), bp.wide.nodes.end());
+  e->rec_host.erase(e->rec_host.begin() + (size_t)rec0 * 16, e->rec_host.begin() + (size_t)rec1 * 16);
+  e->rec_host.insert(e->rec_host.begin() + (size_t)rec0 * 16, bp.wide.tris.begin(), bp.wide.tris.end());
+  const size_t later = (size_t)node0 + bp.wide.nodes.size() / 20;
+  if (dn != 0 || dr != 0) {
+    for (size_t w = later; w < e->blas_words.size() / 20; ++w) {
+      e->blas_words[20 * w + 4] = (uint32_t)((int64_t)e->blas_words[20 * w + 4] + dn);
+      e->blas_words[20 * w + 5] = (uint32_t)((int64_t)e->blas_words[20 * w + 5] + dr);
+    }
+    for (size_t k = m + 1; k < nm; ++k) {
+      e->blas_root[k] = (uint32_t)((int64_t)e->blas_root[k] + dn);
+      e->blas_rec_start[k] = (uint32_t)((int64_t)e->blas_rec_start[k] + dr);
+    }
+  }
+  e->tlas_root = (uint32_t)((int64_t)e->tlas_root + dn);
+  e->local_box[m] = bp.local_box;
+  e->blas_depths[m] = bp.wide.depth;
+  e->blas_depth = *std::max_element(e->blas_depths.begin(), e->blas_depths.end());
+  e->ntri += (int64_t)md->triangle_count - (int64_t)e->mesh_tris[m];
+  e->mesh_tris[m] = md->triangle_count;
+  const size_t tlas_u4 = e->nodes.count - (size_t)old_tlas_root * 5;
+  // upload the bottom levels and records; the top level follows in update_instances
+  cudaStream_t s = e->stream;
+  VT_CUDA(cudaStreamSynchronize(s));
+  e->drop_graphs();
+  const size_t blas_u4 = e->blas_words.size() / 4;
+  e->nodes.resize(blas_u4 + tlas_u4);  // the top level's part is written by update_instances
+  VT_CUDA(cudaMemcpyAsync(e->nodes.ptr, e->blas_words.data(), e->blas_words.size() * 4, cudaMemcpyHostToDevice, s));
+  e->tris.resize(std::max<size_t>(e->rec_host.size() / 4, 1));
+  VT_CUDA(cudaMemcpyAsync(e->tris.ptr, e->rec_host.data(), e->rec_host.size() * 4, cudaMemcpyHostToDevice, s));
+  VT_CUDA(cudaStreamSynchronize(s));
+  e->view.tris = e->tris.ptr;
+  e->view.root = e->tlas_root;
+  const std::vector<vt_instance_desc> insts = e->inst_descs;
+  update_instances(e, insts.data(), insts.size(), rebuild);
 }
 
 // ---------------------------------------------------------------- waves
@@ -755,7 +842,17 @@ vt_status vt_get_capabilities(const vt_engine* e, vt_capabilities* c) {
                            VT_MATERIAL_FEATURE_CAST_SHADOW;
     c->features = VT_FEATURE_INSTANCES | VT_FEATURE_INSTANCE_UPDATES | VT_FEATURE_RADIANCE_CACHE | VT_FEATURE_BATCH |
                   VT_FEATURE_OUTPUT_CAPTURE | (e->opts.debug ? VT_FEATURE_PICK : 0u) |
-                  (e->opts.oracle_accumulation ? VT_FEATURE_FP64_MOMENTS : 0u) | VT_FEATURE_AUX_OUTPUTS;
+                  (e->opts.oracle_accumulation ? VT_FEATURE_FP64_MOMENTS : 0u) | VT_FEATURE_AUX_OUTPUTS |
+                  VT_FEATURE_MESH_UPDATES;
+  });
+}
+
+vt_status vt_update_mesh(vt_engine* e, size_t mesh_index, const vt_mesh_desc* mesh, int32_t rebuild) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    if (rebuild != 0 && rebuild != 1) fail(VT_ERR_RANGE, "rebuild must be 0 or 1");
+    vt::DeviceScope ds(e->device);
+    update_mesh(e, mesh_index, mesh, rebuild != 0);
   });
 }
 

@@ -158,6 +158,48 @@ void refit_tlas_host(BinaryBvhHost& tl, const double* aabbs, size_t n) {
   }
 }
 
+void append_mesh(const vt_mesh_desc& md, size_t m, size_t material_count, std::vector<float>& pos,
+                 std::vector<uint32_t>& idx, std::vector<uint32_t>& tri_mat) {
+  if (md.material >= material_count)
+    fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " references material " + std::to_string(md.material));
+  if ((md.vertex_count && !md.positions) || (md.triangle_count && !md.indices))
+    fail(VT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(m) + " has null arrays");
+  const uint32_t base = (uint32_t)(pos.size() / 4);
+  for (size_t v = 0; v < md.vertex_count; ++v) {
+    for (int k = 0; k < 3; ++k) {
+      const float x = md.positions[3 * v + k];
+      if (!std::isfinite(x)) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " has a non-finite position");
+      pos.push_back(x);
+    }
+    pos.push_back(0.0f);
+  }
+  for (size_t t = 0; t < md.triangle_count; ++t) {
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t i = md.indices[3 * t + k];
+      if (i >= md.vertex_count) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " index out of range");
+      idx.push_back(base + i);
+    }
+    idx.push_back(0u);
+    tri_mat.push_back(md.material);
+  }
+}
+
+BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& idx, uint32_t material,
+                   uint32_t node_base, uint32_t rec_base, int max_leaf) {
+  BuildOptions bo;
+  bo.max_leaf = max_leaf;
+  bo.bins = kEngineBins;
+  const size_t ntri = idx.size() / 4;
+  std::vector<uint32_t> mm(ntri, material);
+  BinaryBvhHost b = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
+  BlasPack out;
+  out.wide = encode_wide(b, pos.data(), 4, idx.data(), 4, mm.data(), node_base, rec_base, &kEngineCollapse);
+  const BinaryNode& rn = b.nodes[0];
+  out.local_box = {rn.mn[0], rn.mn[1], rn.mn[2], rn.mx[0], rn.mx[1], rn.mx[2]};
+  if (ntri == 0) out.local_box = {0, 0, 0, 0, 0, 0};
+  return out;
+}
+
 PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf) {
   if (!sc) fail(VT_ERR_INVALID_ARGUMENT, "scene is null");
   if (sc->mesh_count && !sc->meshes) fail(VT_ERR_INVALID_ARGUMENT, "meshes is null");
@@ -166,31 +208,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   PackedScene p;
   std::vector<float> pos;
   std::vector<uint32_t> idx, tri_mat;
-  for (size_t m = 0; m < sc->mesh_count; ++m) {
-    const vt_mesh_desc& md = sc->meshes[m];
-    if (md.material >= sc->material_count)
-      fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " references material " + std::to_string(md.material));
-    if ((md.vertex_count && !md.positions) || (md.triangle_count && !md.indices))
-      fail(VT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(m) + " has null arrays");
-    const uint32_t base = (uint32_t)(pos.size() / 4);
-    for (size_t v = 0; v < md.vertex_count; ++v) {
-      for (int k = 0; k < 3; ++k) {
-        const float x = md.positions[3 * v + k];
-        if (!std::isfinite(x)) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " has a non-finite position");
-        pos.push_back(x);
-      }
-      pos.push_back(0.0f);
-    }
-    for (size_t t = 0; t < md.triangle_count; ++t) {
-      for (int k = 0; k < 3; ++k) {
-        const uint32_t i = md.indices[3 * t + k];
-        if (i >= md.vertex_count) fail(VT_ERR_RANGE, "mesh " + std::to_string(m) + " index out of range");
-        idx.push_back(base + i);
-      }
-      idx.push_back(0u);
-      tri_mat.push_back(md.material);
-    }
-  }
+  for (size_t m = 0; m < sc->mesh_count; ++m) append_mesh(sc->meshes[m], m, sc->material_count, pos, idx, tri_mat);
   // materials
   std::vector<pt::Material> mats(sc->material_count);
   for (size_t i = 0; i < sc->material_count; ++i) {
@@ -247,8 +265,9 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     }
   } else {
     // one bottom-level tree per mesh, in the mesh's own space, concatenated
-    std::vector<uint32_t> blas_root(sc->mesh_count);
+    std::vector<uint32_t> blas_root(sc->mesh_count), rec_start(sc->mesh_count);
     std::vector<std::array<double, 6>> local_box(sc->mesh_count);
+    std::vector<int> depths(sc->mesh_count);
     int blas_depth = 1;
     size_t vbase = 0, tbase = 0;
     for (size_t m = 0; m < sc->mesh_count; ++m) {
@@ -257,20 +276,19 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
       std::vector<uint32_t> mi(idx.begin() + 4 * tbase, idx.begin() + 4 * (tbase + md.triangle_count));
       for (size_t t = 0; t < md.triangle_count; ++t)
         for (int k = 0; k < 3; ++k) mi[4 * t + k] -= (uint32_t)vbase;
-      std::vector<uint32_t> mm(md.triangle_count, md.material);
-      BinaryBvhHost b = build_binary_host(mp.data(), mp.size(), mi.data(), mi.size(), bo);
-      WideBvhHost w = encode_wide(b, mp.data(), 4, mi.data(), 4, mm.data(), (uint32_t)(node_words.size() / 20),
-                                  (uint32_t)(rec_floats.size() / 16), &kEngineCollapse);
       blas_root[m] = (uint32_t)(node_words.size() / 20);
-      node_words.insert(node_words.end(), w.nodes.begin(), w.nodes.end());
-      rec_floats.insert(rec_floats.end(), w.tris.begin(), w.tris.end());
-      blas_depth = std::max(blas_depth, w.depth);
-      const BinaryNode& rn = b.nodes[0];
-      local_box[m] = {rn.mn[0], rn.mn[1], rn.mn[2], rn.mx[0], rn.mx[1], rn.mx[2]};
-      if (md.triangle_count == 0) local_box[m] = {0, 0, 0, 0, 0, 0};
+      rec_start[m] = (uint32_t)(rec_floats.size() / 16);
+      BlasPack bp = pack_blas(mp, mi, md.material, blas_root[m], rec_start[m], max_leaf);
+      node_words.insert(node_words.end(), bp.wide.nodes.begin(), bp.wide.nodes.end());
+      rec_floats.insert(rec_floats.end(), bp.wide.tris.begin(), bp.wide.tris.end());
+      depths[m] = bp.wide.depth;
+      blas_depth = std::max(blas_depth, bp.wide.depth);
+      local_box[m] = bp.local_box;
       vbase += md.vertex_count;
       tbase += md.triangle_count;
     }
+    p.blas_rec_start = std::move(rec_start);
+    p.blas_depths = std::move(depths);
     if (sc->instance_count && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
     const size_t ni = sc->instance_count;
     InstanceSet placed = place_instances(sc->instances, ni, mats, blas_root, local_box);

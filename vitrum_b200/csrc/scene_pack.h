@@ -40,8 +40,23 @@ struct PackedScene {
   // two-level: per mesh its bottom-level root node and local bounds; the deepest bottom level
   std::vector<uint32_t> blas_root;
   std::vector<std::array<double, 6>> local_box;
+  std::vector<uint32_t> blas_rec_start;  // first triangle record of each mesh's block
+  std::vector<int> blas_depths;          // wide depth of each bottom level
   int blas_depth = 0;
 };
+
+// Validates mesh m and appends its vertices (4 floats each), triangles (4 u32
+// each, indices rebased) and triangle materials.
+void append_mesh(const vt_mesh_desc& md, size_t m, size_t material_count, std::vector<float>& pos,
+                 std::vector<uint32_t>& idx, std::vector<uint32_t>& tri_mat);
+// One mesh's bottom-level tree (the engine's builder options and collapse),
+// its node and record indices offset by node_base / rec_base.
+struct BlasPack {
+  WideBvhHost wide;
+  std::array<double, 6> local_box;
+};
+BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& idx, uint32_t material,
+                   uint32_t node_base, uint32_t rec_base, int max_leaf);
 
 // Instances placed over bottom-level trees: records (world-to-local rows, BLAS
 // root, id, material, material flags), world AABBs (6 doubles each) and

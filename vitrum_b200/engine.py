@@ -383,7 +383,7 @@ class Engine:
     EMITTER_KINDS = {1: "point", 2: "spot", 4: "directional", 8: "rect-area", 16: "disc-area", 32: "mesh-area",
                      64: "environment"}
     FEATURES = {1: "instances", 2: "instance-updates", 4: "radiance-cache", 8: "batch", 16: "pick",
-                32: "output-capture", 64: "fp64-moments", 128: "aux-outputs"}
+                32: "output-capture", 64: "fp64-moments", 128: "aux-outputs", 256: "mesh-updates"}
 
     @property
     def capabilities(self) -> dict:
@@ -407,6 +407,16 @@ class Engine:
             arr[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
         N.call("vt_update_instances", self.handle, ctypes.cast(arr, ctypes.c_void_p), len(instances),
                1 if rebuild else 0)
+
+    def update_mesh(self, index: int, mesh: "Mesh", rebuild: bool = False) -> None:
+        """New geometry and material for mesh `index` of a scene with instances
+        (vt_update_mesh, the reference's rebuildPrimitiveBlas): its bottom level
+        is rebuilt and spliced in, the top level refitted (or rebuilt).  Clears
+        the accumulation."""
+        p = np.ascontiguousarray(mesh.positions, np.float32).reshape(-1, 3)
+        ix = np.ascontiguousarray(mesh.indices, np.uint32).reshape(-1, 3)
+        d = _MeshDesc(p.ctypes.data, p.shape[0], ix.ctypes.data, ix.shape[0], int(mesh.material))
+        N.call("vt_update_mesh", self.handle, int(index), ctypes.byref(d), 1 if rebuild else 0)
 
     def set_previous_camera(self, camera: "Camera | None", aspect: "float | None" = None) -> None:
         """FrameInput.prevViewMatrix / prevProjMatrix for the next frame's motion
