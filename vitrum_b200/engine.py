@@ -11,6 +11,7 @@ All work happens in libvitrum_pt.so (vt_create ... vt_destroy).
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import math
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
@@ -243,7 +244,9 @@ class Scene:
         return int(sum(self.meshes[i.mesh].indices.shape[0] for i in self.instances))
 
     def flattened(self) -> "Scene":
-        """The same scene with every instance baked into a world-space mesh."""
+        """The same scene with every instance baked into a world-space mesh (a
+        mirroring placement reverses the winding, so front faces stay front
+        faces, as the two-level traversal's transformed normals keep them)."""
         if not self.instances:
             return self
         out = []
@@ -251,9 +254,11 @@ class Scene:
             m = self.meshes[inst.mesh]
             M = np.asarray(inst.local_to_world, np.float64).reshape(4, 4)
             p = np.asarray(m.positions, np.float64).reshape(-1, 3) @ M[:3, :3].T + M[:3, 3]
-            out.append(Mesh(p.astype(np.float32), np.asarray(m.indices, np.uint32).reshape(-1, 3), inst.material))
-        return Scene(meshes=out, materials=self.materials, point_lights=self.point_lights,
-                     environment=self.environment, directional_lights=self.directional_lights)
+            t = np.asarray(m.indices, np.uint32).reshape(-1, 3)
+            if np.linalg.det(M[:3, :3]) < 0:
+                t = t[:, [0, 2, 1]]
+            out.append(Mesh(p.astype(np.float32), np.ascontiguousarray(t), inst.material))
+        return dataclasses.replace(self, meshes=out, instances=[])
 
 
 @dataclass
