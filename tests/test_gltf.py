@@ -78,7 +78,7 @@ def asset(as_glb=False):
     return struct.pack("<4sII", b"glTF", 2, 12 + len(body)) + body
 
 
-def check(sc, cam):
+def check(sc, cam, emission=(2, 1, 0)):
     assert len(sc.meshes) == 2  # one prototype per triangle primitive
     q, st = sc.meshes
     assert np.array_equal(q.positions[:, 2], np.zeros(4)) and q.indices.tolist() == [[0, 1, 2], [0, 2, 3]]
@@ -91,7 +91,7 @@ def check(sc, cam):
     assert np.allclose(M[3][:3, :3], np.diag([-1, 1, 1]))
     m0 = sc.materials[0]
     assert np.allclose(m0.base_color, (0.2, 0.4, 0.6)) and m0.metallic == 0 and m0.roughness == 0.5
-    assert np.allclose(m0.emission, (2, 1, 0)) and m0.transmission == pytest.approx(0.3)
+    assert np.allclose(m0.emission, emission) and m0.transmission == pytest.approx(0.3)
     assert m0.ior == pytest.approx(1.4) and m0.specular_intensity == pytest.approx(0.7) and m0.double_sided
     m1 = sc.materials[1]  # glTF defaults: metallic 1, roughness 1, single-sided
     assert m1.metallic == 1 and m1.roughness == 1 and not m1.double_sided and m1.base_color == (1.0, 1.0, 1.0)
@@ -111,10 +111,18 @@ def check(sc, cam):
 
 
 def test_gltf_dict_and_glb_import():
-    sc, cam = gltf_to_scene(asset())
-    check(sc, cam)
+    doc = asset()
+    doc["materials"][0]["emissiveFactor"] = [0, 0, 0]  # instancing needs non-emissive placements
+    sc, cam = gltf_to_scene(doc)
+    check(sc, cam, emission=(0, 0, 0))
+    # the same asset packed as .glb, emissive: imported flattened by default, refused instanced
     sc2, cam2 = gltf_to_scene(asset(as_glb=True))
-    check(sc2, cam2)
+    assert not sc2.instances and len(sc2.meshes) == 4 and np.allclose(sc2.materials[0].emission, (2, 1, 0))
+    with pytest.raises(GltfImportError):
+        gltf_to_scene(asset(as_glb=True), instanced=True)
+    glb = asset(as_glb=True)
+    sc3, cam3 = gltf_to_scene(glb, instanced=None)
+    assert np.allclose(sc3.meshes[0].positions, sc2.meshes[0].positions)
 
 
 def test_flattened_import():
@@ -147,8 +155,10 @@ def test_import_errors():
 def test_imported_scene_renders_the_same_instanced_and_flattened(cuda):
     from vitrum_b200.engine import Engine
     imgs = []
+    doc = asset()
+    doc["materials"][0]["emissiveFactor"] = [0, 0, 0]
     for instanced in (True, False):
-        sc, cam = gltf_to_scene(asset(as_glb=True), instanced=instanced)
+        sc, cam = gltf_to_scene(doc, instanced=instanced)
         e = Engine(max_bounces=3)
         e.set_scene(sc)
         e.render_frame(cam, 40, 30, samples=16, frame_seed=7)

@@ -4,7 +4,7 @@
 // eight quantised child slabs tested against [tmin, closest] in the ray's
 // octant order, internal-child hits kept as an 8-bit group mask and leaf
 // hits as a 32-bit triangle mask (Ylitie et al. 2017 node groups).  The
-// group stack lives in shared memory, one column per thread.  Triangles use
+// group stack is a per-thread local array (L1-cached where touched).  Triangles use
 // the reference's watertight f32 test (tri_intersect.cuh); the accepted hit
 // is then re-evaluated once in float-float arithmetic for the reported t
 // and barycentrics.
@@ -29,6 +29,12 @@ namespace vt {
 namespace {
 
 constexpr int kBlock = 128;
+// Group-stack entries a ray can use: the launcher passes the tree's bound
+// (two per wide level plus a few; 18 for an 8-level tree), capped here; a tree
+// that needs more reports kTraceStackOverflow.  A shared-memory stack sized to
+// that bound traced 1.9 % slower on the box room and 4 % slower on the
+// instanced cloud than this local-memory one (shared memory taken from L1).
+constexpr int kMaxStack = 64;
 // Breadth-first prefix of the tree below `root` that every CTA copies into
 // shared memory at start when staging is on: the root and its children and
 // grandchildren of a full 8-wide tree (1 + 8 + 64), 5840 bytes.
@@ -138,12 +144,16 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
   // triangle work therefore proceed in lock-step phases with most lanes
   // busy in each, and a lane whose ray finished takes the next unclaimed
   // ray from its warp's pool (one atomicAdd per 16 rays).
-  // dynamic shared memory: the stack [stk][kBlock] (one column per thread),
-  // then hot_count staged nodes (80 bytes each) starting at nodes[root]
-  extern __shared__ __align__(16) uint2 stack_mem[];
+  // The group stack is a per-thread local array: the hardware interleaves it
+  // across the warp, it is cached in L1 only where it is touched (rays rarely
+  // go deep), and no shared memory is reserved for it, so the SM keeps its
+  // largest L1 for nodes and triangle records.  `stk` <= kMaxStack entries are
+  // used.  Dynamic shared memory holds only the hot_count staged nodes (80
+  // bytes each) starting at nodes[root].
+  extern __shared__ __align__(16) uint4 hot_mem[];
   __shared__ uint64_t hot_bar;
-  uint2* const stack = stack_mem + threadIdx.x;
-  const uint4* const hot = reinterpret_cast<const uint4*>(stack_mem + stk * kBlock);
+  uint2 stack[kMaxStack];
+  const uint4* const hot = hot_mem;
   if (HOT && hot_count) {
     // one bulk copy (TMA engine, no multicast) into shared memory, completed
     // on an mbarrier by transaction bytes
@@ -274,7 +284,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
         // before this node's internal children (which wait below them)
         if (ghits) {
           if (sp < stk) {
-            stack[sp * kBlock] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
+            stack[sp] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
             ++sp;
           } else {
             atomicOr(status, kTraceStackOverflow);
@@ -282,7 +292,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
           ghits = 0;
         }
         if (sp < stk) {
-          stack[sp * kBlock] = make_uint2(w1.y | kInstGroup, th);
+          stack[sp] = make_uint2(w1.y | kInstGroup, th);
           ++sp;
         } else {
           atomicOr(status, kTraceStackOverflow);
@@ -292,7 +302,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
       if (th) {
         if (q0m == 0) { q0b = w1.y; q0m = th; }
         else if (q1m == 0) { q1b = w1.y; q1m = th; }
-        else if (sp < stk) { stack[sp * kBlock] = make_uint2(w1.y, th); ++sp; }
+        else if (sp < stk) { stack[sp] = make_uint2(w1.y, th); ++sp; }
         else {
           // no room anywhere: test the group now (correct, only slower)
           while (th) {
@@ -345,7 +355,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
           expand = true;
           if (ghits) {
             if (sp < stk) {
-              stack[sp * kBlock] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
+              stack[sp] = make_uint2(gbase | kNodeGroup, ghits | (gimask << 8));
               ++sp;
             } else {
               atomicOr(status, kTraceStackOverflow);  // stack capacity exceeded: result incomplete, reported to the host
@@ -355,7 +365,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
           break;
         }
         if (sp == 0) break;
-        const uint2 g = stack[(sp - 1) * kBlock];
+        const uint2 g = stack[sp - 1];
         const uint32_t tag = g.x & kTagMask;
         if (TWO && tag == kTagMask) {
           // return marker: leave the instance once its queued triangles are tested
@@ -369,9 +379,9 @@ __global__ void __launch_bounds__(kBlock, 6) k_trace(const uint4* __restrict__ n
           --sp;
           const uint32_t k = (uint32_t)(__ffs(g.y) - 1);
           const uint32_t rest = g.y & (g.y - 1);
-          if (rest) { stack[sp * kBlock] = make_uint2(g.x, rest); ++sp; }
+          if (rest) { stack[sp] = make_uint2(g.x, rest); ++sp; }
           if (sp < stk) {
-            stack[sp * kBlock] = make_uint2(kTagMask, 0u);
+            stack[sp] = make_uint2(kTagMask, 0u);
             ++sp;
             const float4* ir = insts + 4 * (size_t)((g.x & ~kTagMask) + k);
             const float4 m0 = __ldg(ir), m1 = __ldg(ir + 1), m2 = __ldg(ir + 2);
@@ -509,18 +519,12 @@ int resident_per_sm(K kern, size_t smem) {
   return per_sm;
 }
 
-// The stack holds exactly the entries the tree can need (a.stack_depth, at
-// most kMaxStack): its shared memory is carved out of the SM's L1, so every
-// entry not allocated stays L1 cache for nodes and triangle records (a
-// 24-entry stack traced the box room 1.8 % faster than a 32-entry one).
-constexpr int kMaxStack = 128;
-
 template <bool ANY, bool TWO>
 void launch_trace_k(const TraceArgs& a, cudaStream_t s) {
   auto plain = k_trace<ANY, TWO, false>;
   auto staged = k_trace<ANY, TWO, true>;
   const int stk = std::min(std::max(a.stack_depth, 4), kMaxStack);
-  const size_t stack_bytes = sizeof(uint2) * stk * kBlock;
+  const size_t stack_bytes = 0;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -173,12 +173,14 @@ def _light(light: dict, world: np.ndarray, where: str):
     raise GltfImportError(f"{where}: unknown light type {kind!r}")
 
 
-def gltf_to_scene(source, instanced: bool = True, scene_index: Optional[int] = None
+def gltf_to_scene(source, instanced: Optional[bool] = None, scene_index: Optional[int] = None
                   ) -> Tuple[Scene, Optional[Camera]]:
     """Scene (and the first camera, or None) from a .gltf / .glb path, raw .glb
     bytes or an already parsed glTF dict (buffers as data URIs).  instanced:
     every mesh primitive is one prototype mesh placed by Instances (a two-level
-    scene); else the placed triangles are flattened into one mesh per placement."""
+    scene); False: the placed triangles are flattened into one mesh per
+    placement; None (default): instanced unless a placement is emissive (the
+    engine samples emitters from flat scenes only)."""
     base_dir, glb_bin = ".", None
     if isinstance(source, dict):
         doc = source
@@ -264,6 +266,9 @@ def gltf_to_scene(source, instanced: bool = True, scene_index: Optional[int] = N
         for c in reversed(node.get("children", [])):
             stack.append((c, world, depth + 1))
     sc.instances = instances
-    if not instanced:
+    emissive = any(any(c > 0 for c in materials[i.material].emission) for i in instances)
+    if instanced and emissive:
+        raise GltfImportError("emissive materials are placed: import flattened (instanced=False or None)")
+    if instanced is False or (instanced is None and emissive):
         sc = sc.flattened()
     return sc, camera
