@@ -46,6 +46,10 @@ struct vt_engine {
   vt_engine_options opts{};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // shadow stream: bounce b's shadow trace and resolve run beside bounce b+1's
+  // closest-hit trace (fork after shade b, join before shade b+1)
+  cudaStream_t shadow_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // scene
   bool has_scene = false;
   vt::BinaryBvhHost binary;
@@ -112,7 +116,7 @@ struct vt_engine {
   DeviceBuffer<float4> shadow_rays, shadow_contrib, radiance;
   DeviceBuffer<uint32_t> path_pixel;  // training paths: their pixel
   DeviceBuffer<uint8_t> occluded;
-  DeviceBuffer<unsigned long long> trace_counter, totals;
+  DeviceBuffer<unsigned long long> trace_counter, shadow_counter, totals;
   DeviceBuffer<int> trace_status;
   std::unique_ptr<NrcEngine> nrc;
   int trace_blocks_per_sm = 0;      // traversal CTAs per SM (0: occupancy limit), from the autotuner
@@ -140,6 +144,9 @@ struct vt_engine {
     drop_graphs();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (shadow_stream) cudaStreamDestroy(shadow_stream);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -545,6 +552,10 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
   vt::pt::launch_raygen(f, w, s);
   E();
   int cur = 0;
+  // bounce b's shadow rays are traced on the shadow stream while bounce b+1's
+  // closest hits are traced here; shade b+1 (which reuses the shadow buffers
+  // and counters) waits for them.  Timed stage breakdowns run serially.
+  const bool overlap = tm == nullptr;
   for (uint32_t b = 0; b < bounces; ++b) {
     vt::TraceArgs t;
     t.nodes = e->nodes.ptr;
@@ -570,6 +581,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
       vt::pt::launch_sort_by_material(e->view, f, w, cur, cap, s);
       E();
     }
+    if (overlap && b > 0) VT_CUDA(cudaStreamWaitEvent(s, e->ev_join, 0));
     B(StageTimer::kShade);
     vt::pt::launch_shade(e->view, f, w, cur, b, cap, s);
     E();
@@ -578,15 +590,24 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     sh.hits = nullptr;
     sh.occluded = w.occluded;
     sh.n_dev = w.counters + vt::pt::kCntShadow;
+    cudaStream_t ss = s;
+    if (overlap) {
+      VT_CUDA(cudaEventRecord(e->ev_fork, s));
+      VT_CUDA(cudaStreamWaitEvent(e->shadow_stream, e->ev_fork, 0));
+      ss = e->shadow_stream;
+      sh.counter = e->shadow_counter.ptr;
+    }
     B(StageTimer::kTraceShadow);
-    vt::launch_trace_any(sh, s);
+    vt::launch_trace_any(sh, ss);
     E();
     B(StageTimer::kResolve);
-    vt::pt::launch_shadow_resolve(w, cap, s);
-    vt::pt::launch_count_rays(w, cur, e->totals.ptr, s);
+    vt::pt::launch_shadow_resolve(w, cap, ss);
+    vt::pt::launch_count_rays(w, cur, e->totals.ptr, ss);
     E();
+    if (overlap) VT_CUDA(cudaEventRecord(e->ev_join, ss));
     cur ^= 1;
   }
+  if (overlap && bounces > 0) VT_CUDA(cudaStreamWaitEvent(s, e->ev_join, 0));
   if (mode == kNrcTrain) {
     B(StageTimer::kNrcTrain);
     const NrcEngine& n = *e->nrc;
@@ -810,6 +831,10 @@ vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine*
     VT_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     VT_CUDA(cudaEventCreate(&e->ev0));
     VT_CUDA(cudaEventCreate(&e->ev1));
+    VT_CUDA(cudaStreamCreateWithFlags(&e->shadow_stream, cudaStreamNonBlocking));
+    VT_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    VT_CUDA(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+    e->shadow_counter.resize(1);
     e->counters.resize(vt::pt::kCntWords);
     VT_CUDA(cudaMemset(e->counters.ptr, 0, e->counters.bytes()));
     e->trace_counter.resize(1);
