@@ -27,6 +27,9 @@ struct vt_batch {
   vt_tuning tuning{1 << 22, 0, 0, 0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // shadow stream: bounce b's shadow trace and resolve beside bounce b+1's closest-hit trace
+  cudaStream_t shadow_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // scenes
   size_t count = 0;
   DeviceBuffer<uint4> nodes;
@@ -49,7 +52,7 @@ struct vt_batch {
   DeviceBuffer<uint32_t> order, keys, counters, ray_root[2], shadow_root, path_pixel;
   DeviceBuffer<float4> shadow_rays, shadow_contrib, radiance;
   DeviceBuffer<uint8_t> occluded;
-  DeviceBuffer<unsigned long long> trace_counter, totals, cursor;
+  DeviceBuffer<unsigned long long> trace_counter, shadow_counter, totals, cursor;
   DeviceBuffer<int> trace_status;
   cudaGraphExec_t graph = nullptr;
   int graph_launches = 0;
@@ -63,6 +66,9 @@ struct vt_batch {
     drop_graph();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (shadow_stream) cudaStreamDestroy(shadow_stream);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -156,6 +162,8 @@ int record_wave(vt_batch* b, cudaStream_t s) {
       vt::pt::launch_sort_by_material(unused, f, w, cur, cap, s);
       k += 2;
     }
+    // the previous bounce's shadow work (second stream) before this shade reuses its buffers
+    if (bo > 0) VT_CUDA(cudaStreamWaitEvent(s, b->ev_join, 0));
     vt::pt::launch_shade(unused, f, w, cur, bo, cap, s);
     vt::TraceArgs sh = t;
     sh.rays = w.shadow_rays;
@@ -163,12 +171,17 @@ int record_wave(vt_batch* b, cudaStream_t s) {
     sh.occluded = w.occluded;
     sh.roots = w.shadow_root;
     sh.n_dev = w.counters + vt::pt::kCntShadow;
-    vt::launch_trace_any(sh, s);
-    vt::pt::launch_shadow_resolve(w, cap, s);
-    vt::pt::launch_count_rays(w, cur, b->totals.ptr, s);
+    sh.counter = b->shadow_counter.ptr;
+    VT_CUDA(cudaEventRecord(b->ev_fork, s));
+    VT_CUDA(cudaStreamWaitEvent(b->shadow_stream, b->ev_fork, 0));
+    vt::launch_trace_any(sh, b->shadow_stream);
+    vt::pt::launch_shadow_resolve(w, cap, b->shadow_stream);
+    vt::pt::launch_count_rays(w, cur, b->totals.ptr, b->shadow_stream);
+    VT_CUDA(cudaEventRecord(b->ev_join, b->shadow_stream));
     k += 4;
     cur ^= 1;
   }
+  if (b->max_bounces > 0) VT_CUDA(cudaStreamWaitEvent(s, b->ev_join, 0));
   vt::pt::launch_accumulate_batch(w, b->accum.ptr, cap, s);
   return k + 2;
 }
@@ -256,6 +269,10 @@ vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_b
     b->counters.resize(vt::pt::kCntWords);
     VT_CUDA(cudaMemset(b->counters.ptr, 0, b->counters.bytes()));
     b->trace_counter.resize(1);
+    b->shadow_counter.resize(1);
+    VT_CUDA(cudaStreamCreateWithFlags(&b->shadow_stream, cudaStreamNonBlocking));
+    VT_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    VT_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
     b->trace_status.resize(1);
     VT_CUDA(cudaMemset(b->trace_status.ptr, 0, sizeof(int)));
     b->totals.resize(2);
