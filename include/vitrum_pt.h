@@ -156,7 +156,7 @@ typedef struct vt_engine_options {
   int32_t debug;                  /* 1 enables vt_pick (EngineOptions.debug, engine/factory.ts) */
   int32_t oracle_accumulation;    /* 1 keeps FP64 per-pixel sums and sums of squares */
   int32_t sort_by_material;       /* 1 = sort shading work by BSDF family; 0 (default) = queue order */
-  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^22 */
+  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^24 */
   int32_t bvh_max_leaf;           /* triangles per leaf of the engine's own trees, 1..4; 0 = 2 (the reference's
                                      builder with 2 instead of its default 4: the same hits, faster traversal) */
 } vt_engine_options;

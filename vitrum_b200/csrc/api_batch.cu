@@ -24,7 +24,7 @@ using vt::fail;
 struct vt_batch {
   int device = 0;
   vt_engine_options opts{};
-  vt_tuning tuning{1 << 22, 0, 0, 0};
+  vt_tuning tuning{vt::pt::kDefaultWavePaths, 0, 0, 0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // shadow stream: bounce b's shadow trace and resolve beside bounce b+1's closest-hit trace
@@ -500,7 +500,7 @@ vt_status vt_batch_autotune(vt_batch* b, vt_tuning_trial* report, size_t cap, si
     };
     vt_tuning best = start;
     double best_ms = time_it(best);
-    for (int wp : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
+    for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
       if (wp == best.wave_paths) continue;
       vt_tuning t = best;
       t.wave_paths = wp;

@@ -720,7 +720,7 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   }
   const uint32_t spp = (uint32_t)std::min(in->samples, room);
   const uint32_t wh = (uint32_t)(e->width * e->height);
-  const uint32_t wave_paths = e->opts.wave_paths > 0 ? (uint32_t)e->opts.wave_paths : (1u << 22);
+  const uint32_t wave_paths = e->opts.wave_paths > 0 ? (uint32_t)e->opts.wave_paths : (uint32_t)vt::pt::kDefaultWavePaths;
   uint32_t spp_wave = std::max<uint32_t>(1u, wave_paths / wh);
   spp_wave = std::min(spp_wave, spp);
   while (spp % spp_wave) --spp_wave;  // equal waves: one graph per frame shape
@@ -1173,10 +1173,10 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       trials.push_back({t, best});
       return best;
     };
-    vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 22), e->opts.sort_by_material > 0 ? 1 : 0,
+    vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : vt::pt::kDefaultWavePaths, e->opts.sort_by_material > 0 ? 1 : 0,
                    e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0};
     double best_ms = time_it(best);
-    for (int wp : {1 << 19, 1 << 20, 1 << 21, 1 << 22}) {
+    for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
       if (wp == best.wave_paths) continue;
       vt_tuning t = best;
       t.wave_paths = wp;
@@ -1213,7 +1213,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
 vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
   return vt::guard([&] {
     if (!e || !t) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
-    t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : (1 << 22);
+    t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : vt::pt::kDefaultWavePaths;
     t->sort_by_material = e->opts.sort_by_material > 0 ? 1 : 0;
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
     t->stage_hot_nodes = e->trace_stage_nodes ? 1 : 0;

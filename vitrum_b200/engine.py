@@ -553,7 +553,7 @@ class Engine:
         N.call("vt_engine_get_tuning", self.handle, ctypes.byref(t))
         return {f: getattr(t, f) for f, _ in _Tuning._fields_}
 
-    def set_tuning(self, wave_paths: int = 1 << 22, sort_by_material: bool = False, trace_blocks_per_sm: int = 0,
+    def set_tuning(self, wave_paths: int = 1 << 24, sort_by_material: bool = False, trace_blocks_per_sm: int = 0,
                    stage_hot_nodes: bool = False) -> None:
         """Launch shape for later frames (vt_engine_set_tuning); `tuning` of
         another engine or an autotune trial can be passed back as keywords."""
