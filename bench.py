@@ -29,9 +29,11 @@ step = one frame rendered from a cleared accumulation.  Metric: Mrays/s
   shape, one CUDA graph per batch frame) against the same frames one scene at
   a time: aggregate Mrays/s of both.
 * cpu_baseline / --impl reference: the C restatement (oracle) of the same
-  estimator on all host cores on a bounded crop (no reference CPU integrator
+  estimator on all host cores, full 512x512 frame at a few spp per step, the
+  scene and BVH built before the clock starts (no reference CPU integrator
   exists at this scale; the reference's own CPU tracer is a Lambert-only
-  brute-force test helper).
+  brute-force test helper); the query line carries the config-1 build time
+  and query rate of the C restatement of shared-bvh at 1 thread and all cores.
 * N > 1: independent replicas (pixels/frames are independent, the scene is
   replicated, no data-path collective): weak scaling.
 """
@@ -148,46 +150,96 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_pt_baseline(target_s=8.0):
-    """The path-tracing estimator restated in C (oracle) on all host cores, on a
-    bounded centre crop of the same frame: returns (Mrays/s, cores, sample text)."""
+REF_SPP = 2  # samples per pixel of each reference-arm step (full 512x512 frame)
+
+
+def _cpu_pt_scene():
     import oracle
     from vitrum_b200 import scenes
     sc, cam = scenes.box_room()
+    t0 = time.perf_counter()
+    S = oracle.PtScene(sc)
+    return S, cam, time.perf_counter() - t0
+
+
+def cpu_pt_baseline(S, cam, spp=REF_SPP):
+    """The path-tracing estimator restated in C (oracle) on the full 512x512
+    frame of the same scene and camera at `spp` samples per pixel, on all host
+    cores, plus the single-thread rate on a 64x64 frame of the same
+    camera (the scene and its BVH are built before either clock starts)."""
+    import oracle
     threads = oracle.hw_threads()
-    nc, ns, dt = oracle.pt_ray_totals(sc, cam, 64, 64, 1, BOUNCES, nthreads=threads)
-    rate = (nc + ns) / dt
-    spp = int(max(1, min(64, target_s * rate / ((nc + ns) / 1.0))))
-    nc, ns, dt = oracle.pt_ray_totals(sc, cam, 64, 64, spp, BOUNCES, nthreads=threads)
-    return (nc + ns) / dt / 1e6, threads, (f"64x64-pixel frame of the same scene and camera, {spp} spp, "
-                                           f"{BOUNCES} bounces ({nc + ns} rays); C restatement of the estimator")
+    nc, ns, dt = oracle.pt_ray_totals(S, cam, W, H, spp, BOUNCES, seed=31, nthreads=threads)
+    nc1, ns1, dt1 = oracle.pt_ray_totals(S, cam, 64, 64, 4, BOUNCES, seed=32, nthreads=1)
+    return {"value": (nc + ns) / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"full {W}x{H} frame of the same scene and camera, {spp} spp, {BOUNCES} bounces "
+                      f"({nc + ns} rays, {dt:.2f} s); C restatement of the estimator (FP64 visibility through the "
+                      f"reference binned-SAH BVH), scene and BVH built before the clock starts",
+            "single_thread": {"value": (nc1 + ns1) / dt1 / 1e6, "unit": "Mrays/s", "cores": 1,
+                              "sample": f"64x64 frame of the same camera, 4 spp ({nc1 + ns1} rays)"}}
+
+
+def cpu_query_baseline():
+    """Config-1 closest-hit workload through the C restatement of shared-bvh
+    (buildArrayBvh + 8-wide collapse, then the reference's FP64 LIFO first-hit
+    query): build ms, and query Mrays/s on 1 thread and on all host cores, each
+    on a bounded slice of the 1,048,576 bench rays."""
+    import oracle
+    from vitrum_b200 import scenes
+    soup, _ = scenes.config1(Q_TRIS, 16, seed=Q_SEED)
+    t0 = time.perf_counter()
+    b = oracle.build_array_bvh(soup.positions, soup.indices)
+    t1 = time.perf_counter()
+    w = oracle.collapse_wide(b)
+    t2 = time.perf_counter()
+    rays = scenes.sphere_rays(Q_RAYS, seed=Q_SEED + 1)
+    threads = oracle.hw_threads()
+    n1, nall = 16384, 131072
+    t3 = time.perf_counter()
+    oracle.first_hit(w, soup.positions, rays[:n1], nthreads=1)
+    t4 = time.perf_counter()
+    oracle.first_hit(w, soup.positions, rays[:nall], nthreads=threads)
+    t5 = time.perf_counter()
+    return {"value": nall / (t5 - t4) / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"first {nall} of the 1,048,576 bench rays on all cores; C restatement of shared-bvh "
+                      "(binned SAH, greedy 8-wide collapse, FP64 LIFO first-hit query)",
+            "single_thread": {"value": n1 / (t4 - t3) / 1e6, "unit": "Mrays/s", "cores": 1,
+                              "sample": f"first {n1} bench rays"},
+            "build_ms": {"binary_sah": round((t1 - t0) * 1e3, 1), "wide_collapse": round((t2 - t1) * 1e3, 1),
+                         "cores": 1}}
 
 
 def run_reference(args, rank, world):
+    """The reference's estimator on the host cores (C restatement; the
+    reference ships no production CPU integrator and no JS runtime exists on
+    this image): every step renders the full 512x512 frame of the headline
+    scene and camera at REF_SPP samples per pixel with all host threads.  The
+    scene set-up and BVH build happen once, before the warm-up."""
     if rank != 0:
         return
     import oracle
-    from vitrum_b200 import scenes
-    sc, cam = scenes.box_room()
+    S, cam, build_s = _cpu_pt_scene()
     threads = oracle.hw_threads()
-    spp = 4
-    for _ in range(args.warmup):
-        oracle.pt_ray_totals(sc, cam, 64, 64, spp, BOUNCES, nthreads=threads)
+    for i in range(args.warmup):
+        oracle.pt_ray_totals(S, cam, W, H, REF_SPP, BOUNCES, seed=1000 + i, nthreads=threads)
     rays, secs = 0, 0.0
-    for _ in range(args.steps):
-        nc, ns, dt = oracle.pt_ray_totals(sc, cam, 64, 64, spp, BOUNCES, nthreads=threads)
+    for i in range(args.steps):
+        nc, ns, dt = oracle.pt_ray_totals(S, cam, W, H, REF_SPP, BOUNCES, seed=i, nthreads=threads)
         rays += nc + ns
         secs += dt
+    S.close()
     value = rays / secs / 1e6
+    sample = (f"each step the full {W}x{H} frame of the same scene and camera at {REF_SPP} spp, {BOUNCES} bounces, "
+              f"all {threads} host threads; C restatement of the path-tracing estimator (the reference ships no "
+              f"production CPU integrator); scene + BVH built once before the warm-up ({build_s:.2f} s)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (procedural box room)", "config": {"workload": WORKLOAD},
-        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                         "sample": f"each step a 64x64-pixel frame of the same scene and camera at {spp} spp; "
-                                   "C restatement of the path-tracing estimator (the reference ships no "
-                                   "production CPU integrator)"},
+        "data": "synthetic (procedural box room)",
+        "config": {"workload": WORKLOAD, "resolution": [W, H], "spp_per_step": REF_SPP, "max_bounces": BOUNCES,
+                   "scene_build_s": round(build_s, 3)},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -539,8 +591,12 @@ def run_ours(args, rank, world, local):
         kernels_per_frame = waves * (1 + BOUNCES * (5 + (2 if tuning["sort_by_material"] else 0)) + 2)
         cpu = None
         if not args.no_cpu_baseline:
-            v, cores, sample = cpu_pt_baseline()
-            cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "port", "sample": sample}
+            S, cpu_cam, cpu_build_s = _cpu_pt_scene()
+            cpu = cpu_pt_baseline(S, cpu_cam)
+            cpu["scene_build_s"] = round(cpu_build_s, 3)
+            S.close()
+            if query is not None:
+                query["cpu_baseline"] = cpu_query_baseline()
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,

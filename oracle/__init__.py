@@ -267,6 +267,16 @@ def _pt_lib():
                                     ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
                                     ctypes.c_int, P, P, P, P, ctypes.c_long, P]
+        L.orc_pt_scene_create.restype = ctypes.c_void_p
+        L.orc_pt_scene_create.argtypes = [P, ctypes.c_long, P, ctypes.c_long, P, P, ctypes.c_int, P, ctypes.c_long,
+                                          P, ctypes.c_long, P, ctypes.c_long, P, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        L.orc_pt_scene_render.restype = ctypes.c_int
+        L.orc_pt_scene_render.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, P, P, P, P, ctypes.c_long,
+                                          P]
+        L.orc_pt_scene_free.restype = None
+        L.orc_pt_scene_free.argtypes = [P]
         L._pt_ready = True
     return L
 
@@ -388,6 +398,56 @@ def inverse_view_proj(camera, width, height):
     return np.linalg.inv(Pm @ V).astype(np.float32)
 
 
+class PtScene:
+    """The CPU path tracer's scene, set up once (BVH build, material table,
+    emitter and environment CDFs) and rendered any number of times."""
+
+    def __init__(self, scene, bias=2e-5):
+        pos, idx, tm, mats, pts, env, ei = flatten_scene(scene)
+        dls = directional_lights(scene)
+        als = area_lights(scene)
+        er = 0.0 if scene.environment is None else float(getattr(scene.environment, "rotation_y", 0.0))
+        ew, eh = (0, 0) if env is None else (env.shape[1], env.shape[0])
+        # the C side borrows these arrays: keep them alive with the handle
+        self._keep = (pos, idx, tm, mats, pts, env, dls, als)
+        self.triangles = int(idx.shape[0])
+        self.handle = _pt_lib().orc_pt_scene_create(
+            _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
+            _p(pts) if pts.size else None, pts.shape[0], _p(als) if als.size else None, als.shape[0],
+            _p(dls) if dls.size else None, dls.shape[0], _p(env) if env is not None else None, ew, eh, ei, er, bias)
+        if not self.handle:
+            raise RuntimeError("oracle path tracer: scene build failed")
+
+    def render(self, camera, width, height, spp, max_bounces, seed=0, sample_base=0, nthreads=0, log_rays=0):
+        """(sum, sum_sq) FP64 per pixel, shapes (H, W, 3); with log_rays > 0 also
+        (closest_rays, shadow_rays, (n_closest, n_shadow)) as pt_render."""
+        ivp = np.ascontiguousarray(inverse_view_proj(camera, width, height))
+        s = np.zeros((height, width, 3), np.float64)
+        q = np.zeros_like(s)
+        lc = np.zeros((max(log_rays, 0), 8), np.float32)
+        ls = np.zeros((max(log_rays, 0), 8), np.float32)
+        totals = np.zeros(2, np.int64)
+        _pt_lib().orc_pt_scene_render(self.handle, _p(ivp), width, height, spp, max_bounces, seed, sample_base,
+                                      nthreads, _p(s), _p(q), _p(lc) if log_rays else None,
+                                      _p(ls) if log_rays else None, max(log_rays, 0), _p(totals))
+        self.last_totals = (int(totals[0]), int(totals[1]))
+        if log_rays:
+            nc, ns = self.last_totals
+            return s, q, lc[:min(nc, log_rays)], ls[:min(ns, log_rays)], (nc, ns)
+        return s, q
+
+    def close(self):
+        if self.handle:
+            _pt_lib().orc_pt_scene_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_base=0, bias=2e-5, nthreads=0,
               log_rays=0):
     """CPU path tracer: (sum, sum_sq) FP64 per pixel, shapes (H, W, 3).
@@ -395,35 +455,20 @@ def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_bas
     With log_rays > 0 also returns (closest_rays, shadow_rays, totals): the
     first log_rays extension and shadow rays as (n, 8) float32 rows and the
     total number of each traced."""
-    pos, idx, tm, mats, pts, env, ei = flatten_scene(scene)
-    ivp = np.ascontiguousarray(inverse_view_proj(camera, width, height))
-    s = np.zeros((height, width, 3), np.float64)
-    q = np.zeros_like(s)
-    ew, eh = (0, 0) if env is None else (env.shape[1], env.shape[0])
-    lc = np.zeros((max(log_rays, 0), 8), np.float32)
-    ls = np.zeros((max(log_rays, 0), 8), np.float32)
-    totals = np.zeros(2, np.int64)
-    dls = directional_lights(scene)
-    als = area_lights(scene)
-    er = 0.0 if scene.environment is None else float(getattr(scene.environment, "rotation_y", 0.0))
-    r = _pt_lib().orc_pt_render(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
-                                _p(pts) if pts.size else None, pts.shape[0], _p(als) if als.size else None,
-                                als.shape[0], _p(dls) if dls.size else None,
-                                dls.shape[0], _p(env) if env is not None else None,
-                                ew, eh, ei, er, _p(ivp), width, height, spp, max_bounces, seed, sample_base, bias,
-                                nthreads, _p(s), _p(q), _p(lc) if log_rays else None, _p(ls) if log_rays else None,
-                                max(log_rays, 0), _p(totals))
-    if r != 0:
-        raise RuntimeError("oracle path tracer failed")
-    if log_rays:
-        nc, ns = int(totals[0]), int(totals[1])
-        return s, q, lc[:min(nc, log_rays)], ls[:min(ns, log_rays)], (nc, ns)
-    return s, q
+    S = PtScene(scene, bias=bias)
+    try:
+        return S.render(camera, width, height, spp, max_bounces, seed=seed, sample_base=sample_base,
+                        nthreads=nthreads, log_rays=log_rays)
+    finally:
+        S.close()
 
 
-def pt_ray_totals(scene, camera, width, height, spp, max_bounces, seed=0, nthreads=0):
-    """Rays traced by the CPU path tracer: (closest, shadow, seconds)."""
+def pt_ray_totals(pt_scene, camera, width, height, spp, max_bounces, seed=0, nthreads=0):
+    """Rays traced by one CPU render of a prepared PtScene, and its wall time:
+    (closest, shadow, seconds).  The scene's BVH build is not in the time."""
     import time
     t0 = time.perf_counter()
-    out = pt_render(scene, camera, width, height, spp, max_bounces, seed=seed, nthreads=nthreads, log_rays=1)
-    return out[4][0], out[4][1], time.perf_counter() - t0
+    pt_scene.render(camera, width, height, spp, max_bounces, seed=seed, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    nc, ns = pt_scene.last_totals
+    return nc, ns, dt

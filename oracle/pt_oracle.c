@@ -840,34 +840,32 @@ static void* pt_worker(void* arg) {
 }
 
 /*
- * Render width x height pixels x spp samples.  materials: 12 floats each
- * (base rgb 0-2, roughness 3, metallic 4, transmission 5, ior 6, emission rgb 7-9, flags 10,
- * specular intensity 11);
- * env: W*H*3 floats (NULL for none); points: 16 floats each (points then spots);
- * areas: 16 floats each (rectangles then discs).  Writes FP64
- * sum and sum of squares (3 per pixel).  Returns 0, or -1 on a build error.
+ * Scene set-up, done once per scene: the binned-SAH BVH over all triangles
+ * (orc_build_array_bvh), the material table, the emissive-triangle area CDF
+ * and the environment's luminance CDFs.  materials: 12 floats each (base rgb
+ * 0-2, roughness 3, metallic 4, transmission 5, ior 6, emission rgb 7-9,
+ * flags 10, specular intensity 11); env: W*H*3 floats (NULL for none);
+ * points: 16 floats each (points then spots); areas: 16 floats each
+ * (rectangles then discs).  The caller keeps every input array alive until
+ * orc_pt_scene_free.  Returns NULL on a build error.
  */
-int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
-                  const float* materials, int n_mat, const float* points, long n_points, const float* areas,
-                  long n_areas, const float* dirs,
-                  long n_dirs, const float* env,
-                  int env_w, int env_h, float env_scale, float env_rotation, const float* inv_vp, int width,
-                  int height, int spp,
-                  int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
-                  double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals) {
-  orc_pt_t S;
-  memset(&S, 0, sizeof S);
-  S.env_cos = (float)cos((double)env_rotation);
-  S.env_sin = (float)sin((double)env_rotation);
-  S.pos = pos;
-  S.idx = idx;
-  S.tmat = tri_mat;
-  S.ntri = ntri;
-  S.nodes = (uint32_t*)malloc(sizeof(uint32_t) * 8 * (size_t)(2 * ntri + 1));
-  S.r2s = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));
-  long nn = orc_build_array_bvh(pos, nvert * 4, 4, idx, ntri, 4, 4, 16, 58, S.nodes, S.r2s);
-  if (nn < 0) { free(S.nodes); free(S.r2s); return -1; }
-  orc_mat_t* mats = (orc_mat_t*)calloc((size_t)n_mat, sizeof(orc_mat_t));
+void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
+                          const float* materials, int n_mat, const float* points, long n_points, const float* areas,
+                          long n_areas, const float* dirs, long n_dirs, const float* env, int env_w, int env_h,
+                          float env_scale, float env_rotation, float bias) {
+  orc_pt_t* S = (orc_pt_t*)calloc(1, sizeof(orc_pt_t));
+  if (!S) return NULL;
+  S->env_cos = (float)cos((double)env_rotation);
+  S->env_sin = (float)sin((double)env_rotation);
+  S->pos = pos;
+  S->idx = idx;
+  S->tmat = tri_mat;
+  S->ntri = ntri;
+  S->nodes = (uint32_t*)malloc(sizeof(uint32_t) * 8 * (size_t)(2 * ntri + 1));
+  S->r2s = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));
+  long nn = orc_build_array_bvh(pos, nvert * 4, 4, idx, ntri, 4, 4, 16, 58, S->nodes, S->r2s);
+  if (nn < 0) { free(S->nodes); free(S->r2s); free(S); return NULL; }
+  orc_mat_t* mats = (orc_mat_t*)calloc((size_t)(n_mat > 0 ? n_mat : 1), sizeof(orc_mat_t));
   for (int i = 0; i < n_mat; ++i) {
     const float* m = materials + 12 * i;
     for (int k = 0; k < 3; ++k) { mats[i].base[k] = m[k]; mats[i].emission[k] = m[7 + k]; }
@@ -883,7 +881,7 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
     mats[i].emissive = m[7] > 0 || m[8] > 0 || m[9] > 0;
     mats[i].flags = (unsigned)m[10];
   }
-  S.mats = mats;
+  S->mats = mats;
   uint32_t* em = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));
   float* cdf = (float*)malloc(sizeof(float) * (size_t)(ntri + 1));
   double total = 0.0;
@@ -891,7 +889,7 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
   for (long t = 0; t < ntri; ++t) {
     if (!mats[tri_mat[t]].emissive) continue;
     double a[3], b[3], c[3];
-    tri_vertices(&S, t, a, b, c);
+    tri_vertices(S, t, a, b, c);
     double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
     double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
     double area = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
@@ -903,24 +901,23 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
   }
   for (long i = 0; i < ne; ++i) cdf[i] = (float)(cdf[i] / total);
   if (ne) cdf[ne - 1] = 1.0f;
-  S.em_tri = em;
-  S.em_cdf = cdf;
-  S.n_em = ne;
-  S.em_area = (float)total;
-  S.points = points;
-  S.n_points = n_points;
-  S.areas = areas;
-  S.n_areas = n_areas;
-  S.dirs = dirs;
-  S.n_dirs = n_dirs;
-  float *marg = NULL, *cond = NULL;
+  S->em_tri = em;
+  S->em_cdf = cdf;
+  S->n_em = ne;
+  S->em_area = (float)total;
+  S->points = points;
+  S->n_points = n_points;
+  S->areas = areas;
+  S->n_areas = n_areas;
+  S->dirs = dirs;
+  S->n_dirs = n_dirs;
   if (env) {
-    S.env = env;
-    S.env_w = env_w;
-    S.env_h = env_h;
-    S.env_scale = env_scale > 0 ? env_scale : 1.0f;
-    marg = (float*)malloc(sizeof(float) * (size_t)(env_h + 1));
-    cond = (float*)malloc(sizeof(float) * (size_t)env_h * (env_w + 1));
+    S->env = env;
+    S->env_w = env_w;
+    S->env_h = env_h;
+    S->env_scale = env_scale > 0 ? env_scale : 1.0f;
+    float* marg = (float*)malloc(sizeof(float) * (size_t)(env_h + 1));
+    float* cond = (float*)malloc(sizeof(float) * (size_t)env_h * (env_w + 1));
     double tot = 0.0;
     double* rows = (double*)malloc(sizeof(double) * (size_t)env_h);
     double* cum = (double*)malloc(sizeof(double) * (size_t)env_w);
@@ -930,7 +927,7 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
       for (int c = 0; c < env_w; ++c) {
         const float* px = env + 3 * ((size_t)r * env_w + c);
         double lum = 0.2126 * px[0] + 0.7152 * px[1] + 0.0722 * px[2];
-        acc += fmax(0.0, lum * S.env_scale) * st;
+        acc += fmax(0.0, lum * S->env_scale) * st;
         cum[c] = acc;
       }
       for (int c = 0; c < env_w; ++c)
@@ -946,28 +943,56 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
       marg[r + 1] = tot > 0 ? (float)(run / tot) : (float)(r + 1) / env_h;
     }
     marg[env_h] = 1.0f;
-    S.env_marg = marg;
-    S.env_cond = cond;
-    S.env_sampleable = tot > 0.0;
+    S->env_marg = marg;
+    S->env_cond = cond;
+    S->env_sampleable = tot > 0.0;
     free(rows);
     free(cum);
   }
-  S.n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_areas + (int)n_dirs + (S.env_sampleable ? 1 : 0);
-  S.bias = bias;
-  S.inv_vp = inv_vp;
-  S.width = width;
-  S.height = height;
-  S.max_bounces = max_bounces;
-  S.seed = seed;
-  S.sample_base = sample_base;
-  S.spp = spp;
-  S.sum = sum;
-  S.sq = sq;
-  S.log_closest = log_closest;
-  S.log_shadow = log_shadow;
-  S.log_cap = log_cap;
+  S->n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_areas + (int)n_dirs + (S->env_sampleable ? 1 : 0);
+  S->bias = bias;
+  return S;
+}
+
+void orc_pt_scene_free(void* h) {
+  orc_pt_t* S = (orc_pt_t*)h;
+  if (!S) return;
+  free(S->nodes);
+  free(S->r2s);
+  free((void*)S->mats);
+  free((void*)S->em_tri);
+  free((void*)S->em_cdf);
+  free((void*)S->env_marg);
+  free((void*)S->env_cond);
+  free(S);
+}
+
+/*
+ * Render width x height pixels x spp samples of a scene made by
+ * orc_pt_scene_create: FP64 sum and sum of squares (3 per pixel).  The
+ * optional ray log keeps the first log_cap rays of each kind; ray_totals gets
+ * the closest-hit and shadow rays traced by this call.  Returns 0.
+ */
+int orc_pt_scene_render(void* h, const float* inv_vp, int width, int height, int spp, int max_bounces, uint32_t seed,
+                        uint32_t sample_base, int nthreads, double* sum, double* sq, float* log_closest,
+                        float* log_shadow, long log_cap, long* ray_totals) {
+  orc_pt_t* S = (orc_pt_t*)h;
+  S->inv_vp = inv_vp;
+  S->width = width;
+  S->height = height;
+  S->max_bounces = max_bounces;
+  S->seed = seed;
+  S->sample_base = sample_base;
+  S->spp = spp;
+  S->sum = sum;
+  S->sq = sq;
+  S->log_closest = log_closest;
+  S->log_shadow = log_shadow;
+  S->log_cap = log_cap;
+  S->n_closest = 0;
+  S->n_shadow = 0;
   pt_job_t job;
-  job.S = &S;
+  job.S = S;
   job.next = 0;
   pthread_mutex_init(&job.mu, NULL);
   if (nthreads <= 0) nthreads = orc_hw_threads();
@@ -976,13 +1001,24 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
   for (int i = 0; i < nthreads; ++i) pthread_create(&th[i], NULL, pt_worker, &job);
   for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
   pthread_mutex_destroy(&job.mu);
-  if (ray_totals) { ray_totals[0] = S.n_closest; ray_totals[1] = S.n_shadow; }
-  free(S.nodes);
-  free(S.r2s);
-  free(mats);
-  free(em);
-  free(cdf);
-  free(marg);
-  free(cond);
+  if (ray_totals) { ray_totals[0] = S->n_closest; ray_totals[1] = S->n_shadow; }
+  return 0;
+}
+
+/* One-shot form: scene set-up, render, free.  Returns 0, or -1 on a build error. */
+int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
+                  const float* materials, int n_mat, const float* points, long n_points, const float* areas,
+                  long n_areas, const float* dirs,
+                  long n_dirs, const float* env,
+                  int env_w, int env_h, float env_scale, float env_rotation, const float* inv_vp, int width,
+                  int height, int spp,
+                  int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
+                  double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals) {
+  void* h = orc_pt_scene_create(pos, nvert, idx, ntri, tri_mat, materials, n_mat, points, n_points, areas, n_areas,
+                                dirs, n_dirs, env, env_w, env_h, env_scale, env_rotation, bias);
+  if (!h) return -1;
+  orc_pt_scene_render(h, inv_vp, width, height, spp, max_bounces, seed, sample_base, nthreads, sum, sq, log_closest,
+                      log_shadow, log_cap, ray_totals);
+  orc_pt_scene_free(h);
   return 0;
 }
