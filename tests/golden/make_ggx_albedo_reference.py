@@ -3,7 +3,7 @@ GGX_EAVG_LUT in pt-webgpu/src/wgsl/pathTrace/material.wgsl.ts:2852-2869) as
 text into ggx_albedo_reference.json, the fixture the generated
 vitrum_b200/csrc/ggx_albedo_lut.h is checked against.
 
-    python tests/golden/make_ggx_albedo_reference.py [reference checkout root]
+    python tests/golden/make_ggx_albedo_reference.py <reference checkout root>
 """
 import json
 import os
@@ -14,7 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_ggx_albedo_reference.py <reference checkout root>")
+    root = sys.argv[1]
     src = open(os.path.join(root, "packages/pt-webgpu/src/wgsl/pathTrace/material.wgsl.ts")).read()
 
     def grab(name):

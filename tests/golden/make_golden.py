@@ -8,7 +8,7 @@ The fixture keeps, for the `multiMesh` and `resizeSplice` packs, exactly the
 buffers the BVH tests need: packed positions, BVH-order indices, BLAS node
 words, per-primitive bindings and the TLAS buffers.  Run:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout root>
 """
 import json
 import os
@@ -31,4 +31,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout root>")
+    main(sys.argv[1])
