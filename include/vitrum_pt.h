@@ -128,6 +128,21 @@ vt_status vt_bvh_trace_any(vt_bvh* bvh, const vt_ray* rays, size_t n, uint8_t* o
 vt_status vt_bvh_destroy(vt_bvh* bvh);
 
 /*
+ * Top-level build over instance world AABBs (replaces buildTlas,
+ * shared-bvh/src/tlas.ts:859-989): binned SAH over the boxes' centroids, the
+ * balanced median fallback for degenerate, non-improving or depth-unsafe
+ * splits.  aabbs: n x 6 doubles (min xyz, max xyz) in instance order.  0 for
+ * an option takes the reference's default (maxLeafSize 1, binCount 16,
+ * maxDepth 58).  Writes the 32-byte reference node layout (8 u32 words per
+ * node, buildArrayBvh.ts:13-27; leaves index the instance permutation) and the
+ * instanceIndices permutation.  *node_count (optional) receives the node count;
+ * pass NULL buffers to query it.  Host only: no device is touched.
+ */
+vt_status vt_tlas_build(const double* aabbs, size_t n, int32_t max_leaf, int32_t bin_count, int32_t max_depth,
+                        uint32_t* nodes, size_t node_word_capacity, uint32_t* instance_indices,
+                        size_t instance_capacity, size_t* node_count);
+
+/*
  * Closest hit for host rays without allocating any device memory.  No
  * counterpart in the reference: its query is a CPU function.  For callers
  * that cannot allocate -- hosts with a fixed, pre-reserved device memory
@@ -466,6 +481,12 @@ vt_status vt_capture_output(vt_engine* engine, const vt_present_options* options
  * under pixel (x, y) of the last frame's camera: the instance index in a
  * scene with instances, else the source triangle index; -1 on a miss. */
 vt_status vt_pick(vt_engine* engine, float x, float y, int32_t* out_triangle);
+
+/* The current scene's top-level tree (scenes with instances; VT_ERR_STATE
+ * otherwise) in the reference layout of vt_tlas_build -- the tlasNodes and
+ * tlasInstanceIndices buffers of packSceneFromCore (scenePack.ts:1104-1310). */
+vt_status vt_engine_export_tlas(const vt_engine* engine, uint32_t* nodes, size_t node_word_capacity,
+                                uint32_t* instance_indices, size_t instance_capacity, size_t* node_count);
 /* Closest hit of host rays against the engine's scene (vt_bvh_trace_closest
  * on a whole scene, two-level when it has instances).  hits[i].prim is the
  * triangle index within its mesh in a scene with instances, else the index over

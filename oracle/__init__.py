@@ -472,3 +472,76 @@ def pt_ray_totals(pt_scene, camera, width, height, spp, max_bounces, seed=0, nth
     dt = time.perf_counter() - t0
     nc, ns = pt_scene.last_totals
     return nc, ns, dt
+
+
+# ---------------------------------------------------------------- pick
+def screen_to_world_ray(camera, px, py, width, height):
+    """screenToWorldRay (shared-bvh/src/pickPrimitiveCpu.ts:68-108) in FP64 on
+    the camera's float32 matrices: origin on the near plane, unit direction."""
+    view, proj = camera.matrices(width / height)
+    V = np.asarray(view, np.float64).reshape(4, 4).T
+    Pm = np.asarray(proj, np.float64).reshape(4, 4).T
+    inv = np.linalg.inv(Pm @ V)
+    nx, ny = px / width * 2 - 1, 1 - py / height * 2
+    far = inv @ np.array([nx, ny, 1.0, 1.0])
+    near = inv @ np.array([nx, ny, -1.0, 1.0])
+    far = far / np.abs(far).max()
+    near = near / np.abs(near).max()
+    o = near[:3] / near[3]
+    orient = 1.0 if far[3] == 0 else np.sign(far[3] * near[3])
+    d = (far[:3] * near[3] - near[:3] * far[3]) * orient
+    return o, d / np.sqrt(d @ d)
+
+
+def _ray_triangles(o, d, v0, v1, v2):
+    """rayTriangle (pickPrimitiveCpu.ts:151-232) over arrays of triangles:
+    hit distance (inf on a miss) and the signed barycentric margin min(u, v, w)."""
+    e1r, e2r = v1 - v0, v2 - v0
+    es = np.maximum(np.abs(e1r).max(1), np.abs(e2r).max(1))
+    ds = np.abs(d).max()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        e1, e2 = e1r / es[:, None], e2r / es[:, None]
+        dr = d / ds
+        ao = (o - v0) / es[:, None]
+        n = np.cross(e1, e2)
+        p = np.cross(dr, e2)
+        det = np.einsum("ij,ij->i", e1, p)
+        ok = (es > 0) & np.isfinite(es) & (np.abs(det) / (np.linalg.norm(n, axis=1) * np.linalg.norm(dr)) > 1e-7)
+        inv = 1.0 / det
+        u = np.einsum("ij,ij->i", ao, p) * inv
+        q = np.cross(ao, e1)
+        v = (q @ dr) * inv
+        w = 1 - u - v
+        t = np.einsum("ij,ij->i", e2, q) * inv * es / ds
+        margin = np.minimum(np.minimum(u, v), w)
+        ok &= np.isfinite(u) & np.isfinite(v) & np.isfinite(t) & (margin >= -1e-6) & (t > 0)
+    return np.where(ok, t, np.inf), np.where(np.isfinite(margin), margin, -np.inf)
+
+
+def pick_primitive(scene, camera, px, py, width, height):
+    """pickPrimitiveCpu (pickPrimitiveCpu.ts:674-695) on an engine Scene:
+    brute force over every triangle (placed in world space in FP64 for
+    instances).  Returns None on a miss, else a dict with `mesh` (the scene
+    primitive), `instance` (or -1), `triangle` (the source triangle index
+    counted over all meshes in order, single-level scenes), `t` and `margin`
+    (the barycentric distance of the hit to its triangle's nearest edge)."""
+    if width <= 0 or height <= 0:
+        return None
+    o, d = screen_to_world_ray(camera, px, py, width, height)
+    best = None
+    items = ([(k, i.mesh, np.asarray(i.local_to_world, np.float64).reshape(4, 4)) for k, i in
+              enumerate(scene.instances)] if scene.instances else
+             [(-1, m, None) for m in range(len(scene.meshes))])
+    tri_base = np.cumsum([0] + [m.indices.shape[0] for m in scene.meshes])
+    for inst, mi, M in items:
+        m = scene.meshes[mi]
+        P = np.asarray(m.positions, np.float32).astype(np.float64).reshape(-1, 3)
+        if M is not None:
+            P = P @ M[:3, :3].T + M[:3, 3]
+        I = np.asarray(m.indices, np.int64).reshape(-1, 3)
+        t, margin = _ray_triangles(o, d, P[I[:, 0]], P[I[:, 1]], P[I[:, 2]])
+        k = int(np.argmin(t))
+        if np.isfinite(t[k]) and (best is None or t[k] < best["t"]):
+            best = dict(mesh=int(mi), instance=int(inst), triangle=int(tri_base[mi] + k) if inst < 0 else -1,
+                        t=float(t[k]), margin=float(margin[k]))
+    return best

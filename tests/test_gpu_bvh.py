@@ -6,7 +6,10 @@ Everything goes through the C ABI (libvitrum_pt.so).  Bars:
   * hit ids: identical to the oracle's f32 watertight query (the device
     semantic) on every ray, and to the FP64 reference query except rays whose
     two nearest hits are within 1e-6 relative t ("tie") or that pass within
-    1e-3 barycentric of an edge ("edge", counted separately); "error" == 0;
+    the derived edge bound 1e-6 + 8 * 2^-24 / g of an edge, g the ray/normal
+    conditioning (the reference's signed 1e-6 plus f32 rounding of the
+    watertight edge functions; "edge", counted and bounded: at most
+    EDGE_MAX_PER_MILLION per 1,048,576 rays); "error" == 0;
   * t within 1e-5 relative, barycentrics within 1e-5 absolute of FP64.
 """
 import numpy as np
@@ -18,6 +21,10 @@ from vitrum_b200 import bvh as vb
 from vitrum_b200 import scenes
 
 pytestmark = pytest.mark.gpu
+
+# observed on the config-1 workload: 2 edge rays of 1,048,576 (FP64 margins
+# 2.1e-7 and 5.7e-7, both inside the reference's own signed 1e-6)
+EDGE_MAX_PER_MILLION = 8
 
 
 def _build_both(soup, **opts):
@@ -38,6 +45,7 @@ def _assert_parity(soup, rays, g, w, label):
     ref = oracle.first_hit(w, soup.positions, rays)
     rep = parity.classify(soup.positions, soup.indices, rays, hits, ref[:3])
     assert rep["error"] == 0, (label, rep)
+    assert rep["edge"] <= max(1, EDGE_MAX_PER_MILLION * rep["n"] // (1 << 20)), (label, rep)
     assert rep["t_bad"] == 0 and rep["bary_bad"] == 0, (label, rep)
     occ = g.intersect_any_hit(rays)
     assert np.array_equal(occ, hits["prim"] >= 0), label

@@ -88,10 +88,11 @@ def test_instanced_trace_matches_flattened_oracle(cuda):
     g["prim"] = np.where(inst >= 0, offs[np.maximum(inst, 0)] + hits["prim"], -1)
     wide = oracle.build_compressed_wide_bvh(pos, idx)
     ref = oracle.first_hit(wide, pos, rays)
-    res = parity.classify(pos, idx, rays, g, ref)
+    res = parity.classify(pos, idx, rays, g, ref, placed=True)
     print({k: v for k, v in res.items() if k != "error_rays"})
     assert res["hits"] > 10000
     assert res["error"] == 0, res["error_rays"][:5]
+    assert res["edge"] <= 8, res
     # t and barycentrics against the placed triangle in FP64 (the flattened f32
     # soup above is only an approximation of the placed geometry)
     hit = np.nonzero(inst >= 0)[0]
@@ -191,3 +192,71 @@ def test_full_instanced_cloud_renders(cuda):
     hits, inst = e.trace_rays(rays)
     assert (inst >= 0).sum() > 1000 and ((hits["prim"] < 0) == (inst < 0)).all()
     e.dispose()
+
+
+def _golden_engine_scene(name):
+    from test_oracle_golden import GOLDEN, SCENES
+    import json
+    from vitrum_b200.engine import Instance, Material, Mesh, Scene
+    pk = json.load(open(GOLDEN))[name]
+    prims = SCENES[name]
+    roots = [bd["blasRoot"] for bd in pk["primitiveTlasBindings"]]
+    meshes = []
+    for P in prims:
+        from test_oracle_golden import pack
+        pos, idx = pack(P)
+        meshes.append(Mesh(pos[:, :3].copy(), idx[:, :3].copy(), 0))
+    l2w = np.array(pk["tlasInstanceLocalToWorld"], np.float32).reshape(-1, 4, 4)
+    insts = [Instance(roots.index(r), l2w[i].T.copy(), 0) for i, r in enumerate(pk["tlasBlasRoots"])]
+    return Scene(meshes=meshes, materials=[Material()], instances=insts), pk
+
+
+@pytest.mark.parametrize("name", ["multiMesh", "resizeSplice"])
+def test_engine_tlas_matches_reference_golden(cuda, name):
+    """The engine's own top level (packSceneFromCore, scenePack.ts:1104-1310):
+    node words and instance order byte-equal to the reference's golden pack."""
+    sc, pk = _golden_engine_scene(name)
+    e = Engine()
+    e.set_scene(sc)
+    nodes, perm = e.export_tlas()
+    e.dispose()
+    assert nodes.shape[0] == pk["tlasNodeCount"]
+    assert np.array_equal(nodes, np.array(pk["tlasNodes"], np.uint32).reshape(-1, 8))
+    assert np.array_equal(perm, np.array(pk["tlasInstanceIndices"], np.uint32))
+
+
+def _world_aabbs(sc):
+    """transformAabb (scenePack.ts:197-223) of each placed mesh's local box, in FP64."""
+    out = []
+    for inst in sc.instances:
+        P = np.asarray(sc.meshes[inst.mesh].positions, np.float32).reshape(-1, 3).astype(np.float64)
+        lo, hi = P.min(0), P.max(0)
+        M = np.asarray(inst.local_to_world, np.float32).astype(np.float64).reshape(4, 4)
+        mn, mx = np.full(3, np.inf), np.full(3, -np.inf)
+        for c in range(8):
+            q = [(hi if c & 1 else lo)[0], (hi if c & 2 else lo)[1], (hi if c & 4 else lo)[2]]
+            for k in range(3):
+                v = M[k, 0] * q[0] + M[k, 1] * q[1] + M[k, 2] * q[2] + M[k, 3]
+                mn[k], mx[k] = min(mn[k], v), max(mx[k], v)
+        out.append(np.r_[mn, mx])
+    return np.array(out)
+
+
+def test_engine_tlas_matches_oracle_on_cloud(cuda):
+    """48- and 1024-instance clouds: the engine's top level byte-equal to the
+    oracle's buildTlas over the same world boxes, before and after a rebuild
+    over moved instances."""
+    for sc in (small_cloud()[0], scenes.instanced_cloud()[0]):
+        e = Engine()
+        e.set_scene(sc)
+        nodes, perm = e.export_tlas()
+        on, op = oracle.build_tlas(_world_aabbs(sc))
+        assert np.array_equal(nodes, on) and np.array_equal(perm, op)
+        from test_gpu_instance_update import moved
+        mv = moved(sc.instances, 3)
+        e.update_instances(mv, rebuild=True)
+        nodes, perm = e.export_tlas()
+        e.dispose()
+        import dataclasses
+        on, op = oracle.build_tlas(_world_aabbs(dataclasses.replace(sc, instances=mv)))
+        assert np.array_equal(nodes, on) and np.array_equal(perm, op)

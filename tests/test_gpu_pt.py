@@ -203,9 +203,10 @@ def test_pick_primitive(cuda):
     e = Engine(max_bounces=2, debug=True)
     e.set_scene(sc)
     e.render_frame(cam, 64, 64, samples=1)
-    tri = e.debug.pick_primitive(32.0, 32.0)
+    tri = e.debug.pick_triangle(32.37, 32.41)
     # back wall (third mesh: 2 x 8 x 8 triangles after the floor and ceiling)
     assert tri is not None and 256 <= tri < 384
+    assert e.debug.pick_primitive(32.37, 32.41) == 2
     plain = Engine(max_bounces=2)
     plain.set_scene(sc)
     plain.render_frame(cam, 8, 8, samples=1)
@@ -280,3 +281,44 @@ def test_environment_equirect_convention(cuda):
     s, _ = oracle.pt_render(sc, look, 4, 4, 4, 1)
     assert np.allclose(s / 4, 5.0)
     e.dispose()
+
+
+PICK_EDGE = 1e-4  # barycentric margin within which the f32 camera ray may pick the neighbour
+
+
+def _pick_grid(e, sc, cam, w, h, step):
+    bad, edge, hits = [], 0, 0
+    for py in np.arange(0.37, h, step):
+        for px in np.arange(0.61, w, step):
+            want = oracle.pick_primitive(sc, cam, px, py, w, h)
+            got_prim = e.debug.pick_primitive(px, py)
+            got_raw = e.debug.pick_triangle(px, py)
+            if want is None:
+                ok = got_prim is None
+            elif sc.instances:
+                ok = got_prim == want["mesh"] and got_raw == want["instance"]
+            else:
+                ok = got_prim == want["mesh"] and got_raw == want["triangle"]
+            hits += want is not None
+            if not ok:
+                if want is not None and want["margin"] < PICK_EDGE:
+                    edge += 1
+                else:
+                    bad.append((px, py, want, got_prim, got_raw))
+    return bad, edge, hits
+
+
+def test_pick_matches_bruteforce_oracle(cuda):
+    """debug.pickPrimitive against pickPrimitiveCpu's brute-force FP64 pick
+    (pickPrimitiveCpu.ts:674-695: screenToWorldRay, two-sided rayTriangle over
+    every triangle) on a grid of pixels, single-level and instanced scenes."""
+    from test_gpu_instances import small_cloud
+    for sc, cam in (small_room(), small_cloud()):
+        e = Engine(max_bounces=1, debug=True)
+        e.set_scene(sc)
+        e.render_frame(cam, 96, 72, samples=1)
+        bad, edge, hits = _pick_grid(e, sc, cam, 96, 72, 5.0)
+        e.dispose()
+        print(f"pick: {hits} hits, {edge} edge, {len(bad)} errors")
+        assert not bad, bad[:5]
+        assert hits > 50 and edge <= 2

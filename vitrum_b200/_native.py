@@ -60,6 +60,8 @@ SIGNATURES = {
     "vt_bvh_trace_closest": [P, P, SZ, P],
     "vt_bvh_trace_any": [P, P, SZ, P],
     "vt_bvh_destroy": [P],
+    "vt_tlas_build": [P, SZ, I32, I32, I32, P, SZ, P, SZ, P],
+    "vt_engine_export_tlas": [P, P, SZ, P, SZ, P],
     "vt_bvh_trace_closest_noalloc": [P, P, SZ, P],
     "vt_watertight_eval_device": [I32, P, SZ, P, P],
     "vt_create": [I32, P, P],

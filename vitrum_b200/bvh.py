@@ -5,6 +5,7 @@ Mirrors the reference's shared-bvh entry points (packages/shared-bvh/src):
     buildArrayBvh / buildCompressedWideBvh   -> build_compressed_wide_bvh()
     intersectCompressedWideBvhFirstHit       -> Bvh.intersect_first_hit()
     intersectCompressedWideBvhAnyHit         -> Bvh.intersect_any_hit()
+    buildTlas (tlas.ts:859)                  -> build_tlas()
 
 Options keep the reference names and defaults (BuildArrayBvhOpts,
 buildArrayBvh.ts:277-318).  Invalid options raise ValueError (RangeError /
@@ -132,3 +133,25 @@ def build_compressed_wide_bvh_device(positions_ptr: int, position_words: int, in
 def watertight_eval_device(cases_ptr: int, n: int, out_ptr: int, device: int = 0, stream: int = 0) -> None:
     N.call("vt_watertight_eval_device", device, ctypes.c_void_p(cases_ptr), n, ctypes.c_void_p(out_ptr),
            ctypes.c_void_p(stream))
+
+
+_TLAS_KEYS = ("maxLeafSize", "binCount", "maxDepth")
+
+
+def build_tlas(aabbs, **opts):
+    """buildTlas (shared-bvh/src/tlas.ts:859) over (n, 6) instance world AABBs
+    (min xyz, max xyz; doubles).  Options keep the reference names
+    (maxLeafSize 1, binCount 16, maxDepth 58).  Returns (nodes (m, 8) uint32 in
+    the reference's 32-byte layout, instanceIndices uint32)."""
+    for k in opts:
+        if k not in _TLAS_KEYS:
+            raise ValueError(f"unknown option {k!r}")
+    a = np.ascontiguousarray(aabbs, dtype=np.float64).reshape(-1, 6)
+    n = a.shape[0]
+    count = ctypes.c_size_t(0)
+    args = (int(opts.get("maxLeafSize", 1)), int(opts.get("binCount", 16)), int(opts.get("maxDepth", 58)))
+    N.call("vt_tlas_build", _ptr(a), n, *args, None, 0, None, 0, ctypes.byref(count))
+    nodes = np.zeros((count.value, 8), np.uint32)
+    perm = np.zeros(n, np.uint32)
+    N.call("vt_tlas_build", _ptr(a), n, *args, _ptr(nodes), nodes.size, _ptr(perm), n, ctypes.byref(count))
+    return nodes, perm

@@ -259,6 +259,27 @@ vt_status vt_bvh_trace_any(vt_bvh* b, const vt_ray* rays, size_t n, uint8_t* occ
   });
 }
 
+vt_status vt_tlas_build(const double* aabbs, size_t n, int32_t max_leaf, int32_t bin_count, int32_t max_depth,
+                        uint32_t* nodes, size_t node_word_capacity, uint32_t* instance_indices,
+                        size_t instance_capacity, size_t* node_count) {
+  return guard([&] {
+    if (n && !aabbs) fail(VT_ERR_INVALID_ARGUMENT, "aabbs is null");
+    if (max_leaf < 0 || bin_count < 0 || max_depth < 0) fail(VT_ERR_INVALID_ARGUMENT, "negative option");
+    if (bin_count == 1) fail(VT_ERR_INVALID_ARGUMENT, "binCount must be at least 2");
+    BinaryBvhHost t = build_tlas_host(aabbs, n, max_leaf ? max_leaf : 1, bin_count ? bin_count : 16,
+                                      max_depth ? max_depth : kMaxBinaryDepth);
+    if (node_count) *node_count = t.nodes.size();
+    if (nodes) {
+      if (node_word_capacity < t.nodes.size() * 8) fail(VT_ERR_RANGE, "node buffer too small");
+      std::memcpy(nodes, t.nodes.data(), t.nodes.size() * 32);
+    }
+    if (instance_indices) {
+      if (instance_capacity < t.reordered_to_source.size()) fail(VT_ERR_RANGE, "instance buffer too small");
+      std::memcpy(instance_indices, t.reordered_to_source.data(), t.reordered_to_source.size() * 4);
+    }
+  });
+}
+
 vt_status vt_bvh_destroy(vt_bvh* b) {
   return guard([&] {
     if (!b) return;

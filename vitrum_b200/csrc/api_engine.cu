@@ -1070,6 +1070,24 @@ vt_status vt_pick(vt_engine* e, float x, float y, int32_t* out_triangle) {
   });
 }
 
+vt_status vt_engine_export_tlas(const vt_engine* e, uint32_t* nodes, size_t node_word_capacity,
+                                uint32_t* instance_indices, size_t instance_capacity, size_t* node_count) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    if (!e->has_scene || e->n_instances == 0) fail(VT_ERR_STATE, "the scene has no top level (no instances)");
+    const vt::BinaryBvhHost& t = e->binary;
+    if (node_count) *node_count = t.nodes.size();
+    if (nodes) {
+      if (node_word_capacity < t.nodes.size() * 8) fail(VT_ERR_RANGE, "node buffer too small");
+      std::memcpy(nodes, t.nodes.data(), t.nodes.size() * 32);
+    }
+    if (instance_indices) {
+      if (instance_capacity < t.reordered_to_source.size()) fail(VT_ERR_RANGE, "instance buffer too small");
+      std::memcpy(instance_indices, t.reordered_to_source.data(), t.reordered_to_source.size() * 4);
+    }
+  });
+}
+
 vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits, int32_t* instances) {
   return vt::guard([&] {
     if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");

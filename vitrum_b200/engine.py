@@ -352,11 +352,26 @@ class _Debug:
     def __init__(self, engine: "Engine"):
         self._e = engine
 
-    def pick_primitive(self, x: float, y: float) -> Optional[int]:
-        """Engine.debug.pickPrimitive: source triangle index under pixel (x, y), or None."""
+    def pick_triangle(self, x: float, y: float) -> Optional[int]:
+        """vt_pick as it is: under pixel (x, y) of the last frame's camera, the
+        source triangle index (single-level scene) or the instance index (scene
+        with instances); None on a miss."""
         out = ctypes.c_int32(-1)
         N.call("vt_pick", self._e.handle, float(x), float(y), ctypes.byref(out))
         return None if out.value < 0 else int(out.value)
+
+    def pick_primitive(self, x: float, y: float) -> Optional[int]:
+        """Engine.debug.pickPrimitive (engine/debug.ts:33-35, pickPrimitiveCpu.ts:674):
+        the scene primitive under pixel (x, y) -- the index of the mesh hit (the
+        placed mesh for an instance) -- or None on a miss."""
+        hit = self.pick_triangle(x, y)
+        sc = self._e._scene
+        if hit is None or sc is None:
+            return None
+        if sc.instances:
+            return int(sc.instances[hit].mesh)
+        ends = np.cumsum([m.indices.shape[0] for m in sc.meshes])
+        return int(np.searchsorted(ends, hit, side="right"))
 
 
 class Engine:
@@ -372,6 +387,7 @@ class Engine:
         self._h = h
         self.device = device
         self.debug = _Debug(self) if debug else None
+        self._scene = None
         self._keep = []
         self.width = self.height = 0
 
@@ -384,6 +400,7 @@ class Engine:
     def set_scene(self, scene: Scene) -> None:
         desc, keep = _marshal_scene(scene)
         N.call("vt_set_scene", self.handle, ctypes.byref(desc))
+        self._scene = scene
 
     EMITTER_KINDS = {1: "point", 2: "spot", 4: "directional", 8: "rect-area", 16: "disc-area", 32: "mesh-area",
                      64: "environment"}
@@ -412,6 +429,8 @@ class Engine:
             arr[i] = _InstanceDesc(int(inst.mesh), int(inst.material), (ctypes.c_float * 16)(*M.T.reshape(-1)))
         N.call("vt_update_instances", self.handle, ctypes.cast(arr, ctypes.c_void_p), len(instances),
                1 if rebuild else 0)
+        if self._scene is not None:
+            self._scene = dataclasses.replace(self._scene, instances=list(instances))
 
     def update_mesh(self, index: int, mesh: "Mesh", rebuild: bool = False) -> None:
         """New geometry and material for mesh `index` of a scene with instances
@@ -422,6 +441,10 @@ class Engine:
         ix = np.ascontiguousarray(mesh.indices, np.uint32).reshape(-1, 3)
         d = _MeshDesc(p.ctypes.data, p.shape[0], ix.ctypes.data, ix.shape[0], int(mesh.material))
         N.call("vt_update_mesh", self.handle, int(index), ctypes.byref(d), 1 if rebuild else 0)
+        if self._scene is not None:
+            meshes = list(self._scene.meshes)
+            meshes[index] = mesh
+            self._scene = dataclasses.replace(self._scene, meshes=meshes)
 
     def set_previous_camera(self, camera: "Camera | None", aspect: "float | None" = None) -> None:
         """FrameInput.prevViewMatrix / prevProjMatrix for the next frame's motion
@@ -561,6 +584,19 @@ class Engine:
         t = _Tuning(int(wave_paths), 1 if sort_by_material else 0, int(trace_blocks_per_sm),
                     1 if stage_hot_nodes else 0)
         N.call("vt_engine_set_tuning", self.handle, ctypes.byref(t))
+
+    def export_tlas(self):
+        """The scene's top-level tree in the reference layout (tlasNodes,
+        tlasInstanceIndices of packSceneFromCore, scenePack.ts:1104-1310)."""
+        count = ctypes.c_size_t(0)
+        N.call("vt_engine_export_tlas", self.handle, None, 0, None, 0, ctypes.byref(count))
+        nodes = np.zeros((count.value, 8), np.uint32)
+        perm = np.zeros(max(count.value, 1), np.uint32)
+        N.call("vt_engine_export_tlas", self.handle, ctypes.c_void_p(nodes.ctypes.data), nodes.size,
+               ctypes.c_void_p(perm.ctypes.data), perm.size, ctypes.byref(count))
+        leaf = (nodes[:, 7] >> 16) == 0xFFFF
+        n_inst = int((nodes[leaf, 7] & 0xFFFF).sum())
+        return nodes, perm[:n_inst].copy()
 
     def stats(self) -> dict:
         s = _EngineStats()
