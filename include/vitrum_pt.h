@@ -150,10 +150,12 @@ vt_status vt_tlas_build(const double* aabbs, size_t n, int32_t max_leaf, int32_t
  * cudaMalloc may happen; vt_bvh_trace_closest grows per-object staging
  * instead.  Scratch is a library-wide device array of 3 MiB + 256 B, held by
  * every GPU that loads the library until exit; n is at most 65,536 rays per
- * call (VT_ERR_RANGE beyond).  The first call on a device looks up that
- * array's address and must precede any stream capture.  Calls that overlap
- * on the GPU race on the shared array.  Synchronous; same results as
- * vt_bvh_trace_closest.
+ * call (VT_ERR_RANGE beyond).  The first call on a device loads the module
+ * that holds the array (lazy loading may allocate in the driver that once):
+ * make it during set-up, before any stream capture -- a call with n == 0
+ * does only that.  Calls that overlap on the GPU race on the shared array.
+ * Runs on the legacy default stream and blocks until the hits are in host
+ * memory; same results as vt_bvh_trace_closest.
  */
 vt_status vt_bvh_trace_closest_noalloc(const vt_bvh* bvh, const vt_ray* rays, size_t n, vt_hit* hits);
 
@@ -171,7 +173,8 @@ typedef struct vt_engine_options {
   int32_t debug;                  /* 1 enables vt_pick (EngineOptions.debug, engine/factory.ts) */
   int32_t oracle_accumulation;    /* 1 keeps FP64 per-pixel sums and sums of squares */
   int32_t sort_by_material;       /* 1 = sort shading work by BSDF family; 0 (default) = queue order */
-  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^24 */
+  int32_t wave_paths;             /* paths in flight per wave; 0 = 2^24 (~300 B of device state per path,
+                                     about 4.7 GB), halved down to 2^20 until it fits half the free memory */
   int32_t bvh_max_leaf;           /* triangles per leaf of the engine's own trees, 1..4; 0 = 2 (the reference's
                                      builder with 2 instead of its default 4: the same hits, faster traversal) */
 } vt_engine_options;
@@ -495,6 +498,28 @@ vt_status vt_engine_export_tlas(const vt_engine* engine, uint32_t* nodes, size_t
  * No reference counterpart: the WebGPU engine exposes no ray query. */
 vt_status vt_trace_rays(vt_engine* engine, const vt_ray* rays, size_t n, vt_hit* hits, int32_t* instances);
 /* Engine.reset (pt-webgpu index.ts:2052): clears the accumulation. */
+/*
+ * Failure-detection hook (engines created with debug = 1; no reference
+ * counterpart).  Bounds the first wait of each bounded device wait -- the
+ * radiance-cache kernels' waits for their tensor-core products and the
+ * traversal's wait for its shared-memory staging copy -- to `cycles` clocks;
+ * 0 restores the default of about a second.  An expired wait makes the kernel
+ * record it, wait for its own copies or products in flight under the full
+ * limit, free its tensor memory and return, so vt_render_frame reports
+ * VT_ERR_TIMEOUT (cache) or VT_ERR_BUILD (staging) and the engine stays usable.
+ */
+vt_status vt_engine_set_wait_limit(vt_engine* engine, int64_t cycles);
+
+/*
+ * Failure-injection hook (tests; the reference's FailureDevice of
+ * pt-webgpu/src/__tests__/transactionalResourceReplacement.test.ts).  The nth
+ * device allocation the library makes on the calling thread from now on fails
+ * as an out-of-memory cudaMalloc would (VT_ERR_OUT_OF_MEMORY, "injected device
+ * allocation failure"); 0 disarms.  vt_set_scene is transactional: a failure at
+ * any stage leaves the engine's previous scene in place.
+ */
+vt_status vt_debug_fail_device_allocation(int64_t nth);
+
 vt_status vt_reset(vt_engine* engine);
 vt_status vt_engine_get_stats(const vt_engine* engine, vt_engine_stats* out_stats);
 /* Engine.dispose */

@@ -6,7 +6,9 @@ such as the Node addon on a path where no cudaMalloc may happen).  Its scratch
 is one library-wide device array, so this test makes two calls in a row on
 different ray batches -- the second sees whatever the first left in the array
 -- and each must equal what vt_bvh_trace_closest returns for the same rays.
-Runs last (file name) and passes alone or after the other tests.
+A further test checks the property the call exists for: after the set-up
+call, full-size calls leave the device's free memory unchanged.  Runs last
+(file name) and passes alone or after the other tests.
 """
 import ctypes
 
@@ -57,4 +59,23 @@ def test_noalloc_rejects_batches_beyond_its_scratch(cuda):
         _noalloc(g, rays)
     assert e.value.status == 2 and "65536" in str(e.value)
     assert _noalloc(g, rays[:0]).size == 0
+    g.close()
+
+
+def test_noalloc_calls_leave_free_device_memory_unchanged(cuda):
+    import torch
+    soup = scenes.random_triangles(5000, seed=82)
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices)
+    rays = scenes.sphere_rays(MAX_RAYS, seed=83)
+    _noalloc(g, rays[:0])          # set-up call: loads the module, resolves the scratch address
+    want = _noalloc(g, rays)       # and one full call, so every kernel it launches is loaded
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        got = _noalloc(g, rays)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert np.array_equal(got["prim"], want["prim"])
+    # an allocation the size of the staging (3 MiB) would show here
+    assert free1 == free0, (free0, free1)
     g.close()

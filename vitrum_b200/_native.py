@@ -100,6 +100,8 @@ SIGNATURES = {
     "vt_nrc_set_params": [P, P, P],
     "vt_nrc_query_device": [P, P, SZ, P, P],
     "vt_nrc_train_device": [P, P, SZ, P],
+    "vt_engine_set_wait_limit": [P, ctypes.c_int64],
+    "vt_debug_fail_device_allocation": [ctypes.c_int64],
     "vt_reset": [P],
     "vt_engine_get_stats": [P, P],
     "vt_destroy": [P],

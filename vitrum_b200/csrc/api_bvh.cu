@@ -25,6 +25,13 @@ thread_local std::string t_last_error;
 void set_last_error(const std::string& msg) { t_last_error = msg; }
 void clear_last_error() { t_last_error.clear(); }
 
+thread_local long long t_alloc_fail_countdown = 0;  // 0: disarmed
+void arm_allocation_failure(long long nth) { t_alloc_fail_countdown = nth > 0 ? nth : 0; }
+bool injected_allocation_failure() {
+  if (t_alloc_fail_countdown <= 0) return false;
+  return --t_alloc_fail_countdown == 0;
+}
+
 static BuildOptions resolve(const vt_bvh_build_options* o) {
   BuildOptions r;
   if (!o) return r;
@@ -99,6 +106,13 @@ extern "C" {
 
 const char* vt_last_error(void) { return t_last_error.c_str(); }
 const char* vt_version(void) { return "vitrum_b200 0.1 (sm_100a)"; }
+
+vt_status vt_debug_fail_device_allocation(int64_t nth) {
+  return guard([&] {
+    if (nth < 0) fail(VT_ERR_RANGE, "nth must be >= 0");
+    arm_allocation_failure(nth);
+  });
+}
 
 vt_status vt_bvh_build(int32_t device, const float* positions, size_t position_words, const uint32_t* indices,
                        size_t index_words, const vt_bvh_build_options* options, vt_bvh** out_bvh) {

@@ -107,6 +107,7 @@ struct vt_engine {
   float view_m[16] = {}, proj_m[16] = {};
   bool have_camera = false;
   uint32_t frame_seed = 0;
+  mutable uint32_t auto_wave_paths = 0;  // default wave size, fitted to free memory once (wave_paths_of)
   // wave buffers
   uint32_t capacity = 0;
   DeviceBuffer<float4> rays[2], through[2];
@@ -121,6 +122,7 @@ struct vt_engine {
   std::unique_ptr<NrcEngine> nrc;
   int trace_blocks_per_sm = 0;      // traversal CTAs per SM (0: occupancy limit), from the autotuner
   bool trace_stage_nodes = false;   // traversal CTAs stage the top of the tree in shared memory
+  long long debug_wait_cycles = 0;  // failure-detection hook: first-wait limit of bounded waits (0: default)
   // graph cache: one executable per wave shape and mode
   struct Graph {
     uint32_t spp_wave = 0, bounces = 0;
@@ -164,38 +166,62 @@ void upload(DeviceBuffer<T>& dst, const std::vector<T>& src, cudaStream_t s) {
 
 // ---------------------------------------------------------------- scene
 void set_scene(vt_engine* e, const vt_scene_desc* sc) {
+  // Transactional replacement (the reference's staged upload with rollback,
+  // pt-webgpu/src/scene/uploadSceneBuffers.ts, transactionalResourceReplacement.test.ts):
+  // every device buffer of the new scene is allocated and filled first; only
+  // when all of them succeeded do they replace the engine's, so a failure at
+  // any stage leaves the previous scene and its image untouched.
   vt::PackedScene p = vt::pack_scene(sc, 0, 0, e->opts.bvh_max_leaf);
   cudaStream_t s = e->stream;
-  VT_CUDA(cudaStreamSynchronize(s));
-  e->drop_graphs();
-  e->nodes.resize(p.node_words.size() / 4);
-  VT_CUDA(cudaMemcpyAsync(e->nodes.ptr, p.node_words.data(), p.node_words.size() * 4, cudaMemcpyHostToDevice, s));
-  e->tris.resize(std::max<size_t>(p.rec_floats.size() / 4, 1));
+  struct Staged {
+    DeviceBuffer<uint4> nodes;
+    DeviceBuffer<float4> tris, insts, inst_table, inst_l2w;
+    DeviceBuffer<vt::pt::Material> materials;
+    DeviceBuffer<float4> emitters, points, area_lights, dirs, env;
+    DeviceBuffer<float> emitter_cdf, env_marginal, env_conditional;
+  } n;
+  n.nodes.resize(p.node_words.size() / 4);
+  VT_CUDA(cudaMemcpyAsync(n.nodes.ptr, p.node_words.data(), p.node_words.size() * 4, cudaMemcpyHostToDevice, s));
+  n.tris.resize(std::max<size_t>(p.rec_floats.size() / 4, 1));
   if (!p.rec_floats.empty())
-    VT_CUDA(cudaMemcpyAsync(e->tris.ptr, p.rec_floats.data(), p.rec_floats.size() * 4, cudaMemcpyHostToDevice, s));
+    VT_CUDA(cudaMemcpyAsync(n.tris.ptr, p.rec_floats.data(), p.rec_floats.size() * 4, cudaMemcpyHostToDevice, s));
+  const bool two_level = p.two_level;
+  std::vector<float4> il(p.inst_lanes.size() / 4), it(p.inst_tab.size() / 4), ir(p.inst_rows.size() / 4);
+  if (!il.empty()) std::memcpy(il.data(), p.inst_lanes.data(), p.inst_lanes.size() * 4);
+  if (!it.empty()) std::memcpy(it.data(), p.inst_tab.data(), p.inst_tab.size() * 4);
+  if (!ir.empty()) std::memcpy(ir.data(), p.inst_rows.data(), p.inst_rows.size() * 4);
+  upload(n.insts, il, s);
+  upload(n.inst_table, it, s);
+  upload(n.inst_l2w, ir, s);
+  upload(n.materials, p.mats, s);
+  upload(n.emitters, p.emitters, s);
+  upload(n.emitter_cdf, p.cdf, s);
+  upload(n.points, p.points, s);
+  upload(n.area_lights, p.area_lights, s);
+  upload(n.dirs, p.dirs, s);
+  upload(n.env, p.env, s);
+  upload(n.env_marginal, p.marg, s);
+  upload(n.env_conditional, p.cond, s);
+  VT_CUDA(cudaStreamSynchronize(s));
+  // commit
+  e->drop_graphs();
+  e->nodes = std::move(n.nodes);
+  e->tris = std::move(n.tris);
+  e->insts = std::move(n.insts);
+  e->inst_table = std::move(n.inst_table);
+  e->inst_l2w = std::move(n.inst_l2w);
+  e->materials = std::move(n.materials);
+  e->emitters = std::move(n.emitters);
+  e->emitter_cdf = std::move(n.emitter_cdf);
+  e->points = std::move(n.points);
+  e->area_lights = std::move(n.area_lights);
+  e->dirs = std::move(n.dirs);
+  e->env = std::move(n.env);
+  e->env_marginal = std::move(n.env_marginal);
+  e->env_conditional = std::move(n.env_conditional);
   e->wide_depth = p.depth;
   e->stack_depth = p.stack_depth;
-  const bool two_level = p.two_level;
-  {
-    std::vector<float4> il(p.inst_lanes.size() / 4), it(p.inst_tab.size() / 4), ir(p.inst_rows.size() / 4);
-    if (!il.empty()) std::memcpy(il.data(), p.inst_lanes.data(), p.inst_lanes.size() * 4);
-    if (!it.empty()) std::memcpy(it.data(), p.inst_tab.data(), p.inst_tab.size() * 4);
-    if (!ir.empty()) std::memcpy(ir.data(), p.inst_rows.data(), p.inst_rows.size() * 4);
-    upload(e->insts, il, s);
-    upload(e->inst_table, it, s);
-    upload(e->inst_l2w, ir, s);
-  }
   e->n_instances = (int64_t)p.n_instances;
-  upload(e->materials, p.mats, s);
-  upload(e->emitters, p.emitters, s);
-  upload(e->emitter_cdf, p.cdf, s);
-  upload(e->points, p.points, s);
-  upload(e->area_lights, p.area_lights, s);
-  upload(e->dirs, p.dirs, s);
-  upload(e->env, p.env, s);
-  upload(e->env_marginal, p.marg, s);
-  upload(e->env_conditional, p.cond, s);
-  VT_CUDA(cudaStreamSynchronize(s));
   vt::pt::SceneView v;
   v.nodes = e->nodes.ptr;
   v.tris = e->tris.ptr;
@@ -368,6 +394,33 @@ void update_mesh(vt_engine* e, size_t m, const vt_mesh_desc* md, bool rebuild) {
 }
 
 // ---------------------------------------------------------------- waves
+// Device bytes of wave state per path (ray queues, path state, hits, sort keys,
+// shadow queue, radiance, pixel ids) -- about 300.
+size_t wave_bytes_per_path(const vt_engine* e) {
+  return 2 * (2 * sizeof(*e->rays[0].ptr) + sizeof(*e->through[0].ptr) + sizeof(*e->state[0].ptr)) +
+         sizeof(*e->hits.ptr) + sizeof(*e->order.ptr) + sizeof(*e->keys.ptr) + 2 * sizeof(*e->shadow_rays.ptr) +
+         sizeof(*e->shadow_contrib.ptr) + sizeof(*e->occluded.ptr) + sizeof(*e->radiance.ptr) +
+         sizeof(*e->path_pixel.ptr);
+}
+
+// Paths per wave: the option, or kDefaultWavePaths halved (down to 1 M) until
+// the wave state fits in half of the device memory that is free (counting the
+// engine's own wave buffers as free), so that several engines on one GPU do
+// not each claim ~4.7 GB.  Decided once per engine.
+uint32_t wave_paths_of(const vt_engine* e) {
+  if (e->opts.wave_paths > 0) return (uint32_t)e->opts.wave_paths;
+  if (!e->auto_wave_paths) {
+    size_t free_b = 0, total_b = 0;
+    VT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per = wave_bytes_per_path(e);
+    const size_t budget = (free_b + (size_t)e->capacity * per) / 2;
+    uint32_t w = (uint32_t)vt::pt::kDefaultWavePaths;
+    while (w > (1u << 20) && (size_t)w * per > budget) w >>= 1;
+    e->auto_wave_paths = w;
+  }
+  return e->auto_wave_paths;
+}
+
 void ensure_capacity(vt_engine* e, uint32_t cap) {
   if (e->capacity >= cap) return;
   e->drop_graphs();
@@ -466,6 +519,7 @@ void nrc_rebuild(vt_engine* e) {
   }
   for (int i = 0; i < 3; ++i) { c.aabb_min[i] = mn[i]; c.aabb_max[i] = mx[i]; }
   n.cache = std::make_unique<vt::nrc::Cache>(c, k.seed);
+  n.cache->set_wait_cycles(e->debug_wait_cycles);
   n.frames = 0;
   e->drop_graphs();
 }
@@ -568,6 +622,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.stack_depth = e->stack_depth;
     t.node_count = e->nodes.count / 5;
     t.stage_nodes = e->trace_stage_nodes;
+    t.stage_wait_cycles = e->debug_wait_cycles;
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.n_dev = w.counters + cur;
@@ -720,7 +775,7 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   }
   const uint32_t spp = (uint32_t)std::min(in->samples, room);
   const uint32_t wh = (uint32_t)(e->width * e->height);
-  const uint32_t wave_paths = e->opts.wave_paths > 0 ? (uint32_t)e->opts.wave_paths : (uint32_t)vt::pt::kDefaultWavePaths;
+  const uint32_t wave_paths = wave_paths_of(e);
   uint32_t spp_wave = std::max<uint32_t>(1u, wave_paths / wh);
   spp_wave = std::min(spp_wave, spp);
   while (spp % spp_wave) --spp_wave;  // equal waves: one graph per frame shape
@@ -773,7 +828,10 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     int d[2] = {0, 0};
     VT_CUDA(cudaMemcpy(d, e->nrc->cache->d_diag(), sizeof d, cudaMemcpyDeviceToHost));
     if (d[0]) {
+      // the frame's cache queries may be missing: drop its samples with the
+      // accumulation, so the next frame starts clean
       VT_CUDA(cudaMemset(e->nrc->cache->d_diag(), 0, sizeof(int)));
+      reset_accumulation(e);
       fail(VT_ERR_TIMEOUT, "tensor-core wait expired in an NRC kernel");
     }
   }
@@ -782,7 +840,12 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   e->last_ms = ms;
   int st = 0;
   VT_CUDA(cudaMemcpy(&st, e->trace_status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) fail(VT_ERR_BUILD, vt::trace_status_message(st));
+  if (st) {
+    // reported once; the frame's samples leave with the accumulation
+    VT_CUDA(cudaMemset(e->trace_status.ptr, 0, sizeof(int)));
+    reset_accumulation(e);
+    fail(VT_ERR_BUILD, vt::trace_status_message(st));
+  }
   e->samples += (int)spp;
   out->kind = 0;
   out->samples_accumulated = e->samples;
@@ -1048,6 +1111,7 @@ vt_status vt_pick(vt_engine* e, float x, float y, int32_t* out_triangle) {
     t.stack_depth = e->stack_depth;
     t.node_count = e->nodes.count / 5;
     t.stage_nodes = e->trace_stage_nodes;
+    t.stage_wait_cycles = e->debug_wait_cycles;
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.inst_table = e->view.inst_table;
@@ -1114,6 +1178,7 @@ vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits
     t.stack_depth = e->stack_depth;
     t.node_count = e->nodes.count / 5;
     t.stage_nodes = e->trace_stage_nodes;
+    t.stage_wait_cycles = e->debug_wait_cycles;
     t.insts = e->view.insts;
     t.root = e->view.root;
     t.inst_table = e->view.inst_table;
@@ -1127,7 +1192,10 @@ vt_status vt_trace_rays(vt_engine* e, const vt_ray* rays, size_t n, vt_hit* hits
     int st = 0;
     VT_CUDA(cudaMemcpyAsync(&st, e->q_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     VT_CUDA(cudaStreamSynchronize(e->stream));
-    if (st) fail(VT_ERR_BUILD, vt::trace_status_message(st));
+    if (st) {
+      VT_CUDA(cudaMemset(e->q_status.ptr, 0, sizeof(int)));
+      fail(VT_ERR_BUILD, vt::trace_status_message(st));
+    }
   });
 }
 
@@ -1191,7 +1259,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       trials.push_back({t, best});
       return best;
     };
-    vt_tuning best{e->opts.wave_paths > 0 ? e->opts.wave_paths : vt::pt::kDefaultWavePaths, e->opts.sort_by_material > 0 ? 1 : 0,
+    vt_tuning best{(int32_t)wave_paths_of(e), e->opts.sort_by_material > 0 ? 1 : 0,
                    e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0};
     double best_ms = time_it(best);
     for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
@@ -1231,7 +1299,8 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
 vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
   return vt::guard([&] {
     if (!e || !t) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
-    t->wave_paths = e->opts.wave_paths > 0 ? e->opts.wave_paths : vt::pt::kDefaultWavePaths;
+    vt::DeviceScope ds(e->device);
+    t->wave_paths = (int32_t)wave_paths_of(e);
     t->sort_by_material = e->opts.sort_by_material > 0 ? 1 : 0;
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
     t->stage_hot_nodes = e->trace_stage_nodes ? 1 : 0;
@@ -1253,6 +1322,19 @@ vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
     e->trace_blocks_per_sm = t->trace_blocks_per_sm;
     e->trace_stage_nodes = t->stage_hot_nodes != 0;
     e->drop_graphs();
+  });
+}
+
+vt_status vt_engine_set_wait_limit(vt_engine* e, int64_t cycles) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    if (!e->opts.debug) fail(VT_ERR_STATE, "the wait-limit hook requires the debug option");
+    if (cycles < 0) fail(VT_ERR_RANGE, "cycles must be >= 0");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    e->debug_wait_cycles = cycles;
+    if (e->nrc) e->nrc->cache->set_wait_cycles(cycles);
+    e->drop_graphs();  // captured launches hold the old limits
   });
 }
 

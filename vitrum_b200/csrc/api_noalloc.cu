@@ -12,16 +12,20 @@
 // traversal kernel needs, plus device staging for the rays and hit records --
 // is one file-scope __device__ array of kNoAllocScratchBytes (3 MiB + 256 B),
 // which every GPU that loads the library holds until the process exits.
-// Host code cannot use the array's name as a device address; the first call
-// on each device looks the address up with cudaGetSymbolAddress while that
-// device is current and caches it.  That first call must therefore come
-// before any CUDA stream capture begins.  All calls share the one array and
-// it keeps the last call's contents: the status word is cleared here and the
-// counter by the kernel launcher, and calls that overlap on the GPU (other
-// threads, other streams) race on the array.
+// Host code cannot use the array's name as a device address; every call looks
+// the address up with cudaGetSymbolAddress while the BVH's device is current
+// (a lookup, once the module is loaded), so nothing goes stale after a
+// cudaDeviceReset.  The first call on each device is different: with lazy
+// module loading (the CUDA 12 default) it loads this file's module, which may
+// allocate in the driver once.  Make that first call during set-up -- a call
+// with n == 0 does only this and traces nothing -- and before any CUDA stream
+// capture begins.  All calls share the one array and it keeps the last
+// call's contents: the status word is cleared here and the counter by the
+// kernel launcher, and calls that overlap on the GPU (other threads, other
+// streams) race on the array.  Each call runs on the legacy default stream
+// and blocks until the hit records are in host memory.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "bvh_object.h"
@@ -36,22 +40,13 @@ constexpr size_t kNoAllocScratchBytes = kHeaderBytes + kNoAllocMaxRays * (sizeof
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 128;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on `device` (which must be current).
-unsigned char* scratch_for(int device) {
-  if (device < 0 || device >= kMaxDevices) vt::fail(VT_ERR_RANGE, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      vt::fail(VT_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-    g_scratch_addr[device] = p;
-  }
-  return static_cast<unsigned char*>(g_scratch_addr[device]);
+// Device address of g_noalloc_scratch on the current device.
+unsigned char* scratch_address() {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr)
+    vt::fail(VT_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+  return static_cast<unsigned char*>(p);
 }
 
 }  // namespace
@@ -63,9 +58,9 @@ extern "C" vt_status vt_bvh_trace_closest_noalloc(const vt_bvh* bvh, const vt_ra
     if (n > kNoAllocMaxRays)
       vt::fail(VT_ERR_RANGE, "vt_bvh_trace_closest_noalloc takes at most " + std::to_string(kNoAllocMaxRays) +
                                  " rays per call, got " + std::to_string(n) + "; split the batch");
-    if (n == 0) return;
     vt::DeviceScope ds(bvh->device);
-    unsigned char* base = scratch_for(bvh->device);
+    unsigned char* base = scratch_address();
+    if (n == 0) return;  // set-up call: the module is loaded and the address resolved
     auto* counter = reinterpret_cast<unsigned long long*>(base);
     auto* status = reinterpret_cast<int*>(base + 8);
     auto* d_rays = reinterpret_cast<float4*>(base + kHeaderBytes);

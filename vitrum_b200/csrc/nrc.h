@@ -48,6 +48,8 @@ struct Config {
 };
 
 // Device-side view used by the kernels.
+constexpr long long kDefaultWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
+
 struct View {
   const __half* w16 = nullptr;       // [6][64 out][64 in] fp16 weights
   const __half2* table16 = nullptr;  // [levels][T] fp16 feature pairs
@@ -59,6 +61,9 @@ struct View {
   float aabb_min[3] = {0, 0, 0};
   float aabb_inv[3] = {1, 1, 1};     // 1 / extent (0 for a flat axis)
   int* error = nullptr;              // non-zero: a bounded wait expired (kernel returned early)
+  // clocks a kernel waits for its MMAs before it gives up (sets *error, drains
+  // under the full limit, frees TMEM, returns); shortened only to test that path
+  long long wait_cycles = kDefaultWaitCycles;
   float* loss = nullptr;             // sum of per-sample losses of a training step
   // error estimate per screen tile: samples whose target.w holds (pixel + 1) add
   // (prediction luminance, target luminance, 1) to tile_stats[3 * tile]

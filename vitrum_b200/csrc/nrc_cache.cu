@@ -88,6 +88,7 @@ View Cache::view() const {
     v.aabb_inv[k] = ext > 1e-20f ? 1.0f / ext : 0.0f;
   }
   v.error = diag_.ptr;
+  v.wait_cycles = wait_cycles_;
   v.loss = loss_.ptr;
   v.tile_stats = tile_stats_;
   v.tile_width = tile_width_;

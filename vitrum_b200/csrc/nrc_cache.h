@@ -42,6 +42,8 @@ class Cache {
     tiles_x_ = tiles_x;
   }
   void clear_gradients(cudaStream_t s);
+  // Clocks the kernels wait for their MMAs before giving up (0: kDefaultWaitCycles).
+  void set_wait_cycles(long long c) { wait_cycles_ = c > 0 ? c : kDefaultWaitCycles; }
 
   const Config& config() const { return cfg_; }
   uint64_t steps() const { return step_; }
@@ -53,6 +55,7 @@ class Cache {
  private:
   void adam(cudaStream_t s);
   Config cfg_;
+  long long wait_cycles_ = kDefaultWaitCycles;
   float res_[kMaxLevels] = {};
   uint64_t step_ = 0;
   DeviceBuffer<float> w_, w_m_, w_v_, grad_w_;

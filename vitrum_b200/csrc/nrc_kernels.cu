@@ -31,7 +31,7 @@ namespace nrc {
 
 namespace {
 
-constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
+constexpr long long kWaitCycles = kDefaultWaitCycles;  // drains after an expired wait
 constexpr uint32_t kTileBytes = kTile * kWidth * 2;   // 16 KB activation tile
 constexpr uint32_t kWBytes = kWidth * kWidth * 2;      // 8 KB weight tile
 constexpr uint32_t kIdesc = tc::idesc_f16(128, 64, false, false);     // X * W^T
@@ -190,8 +190,8 @@ __device__ __forceinline__ void issue_fwd(uint32_t tmem_d, uint32_t a_tile, uint
 
 // Thread-uniform bounded wait on the barrier's current phase.
 // On failure `phase` keeps the parity of the phase still pending.
-__device__ __forceinline__ bool wait_all(uint64_t* bar, uint32_t& phase) {
-  const bool ok = __syncthreads_and(tc::mbar_wait(bar, phase, kWaitCycles)) != 0;
+__device__ __forceinline__ bool wait_all(const View& v, uint64_t* bar, uint32_t& phase) {
+  const bool ok = __syncthreads_and(tc::mbar_wait(bar, phase, v.wait_cycles)) != 0;
   if (ok) phase ^= 1u;
   return ok;
 }
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128, 1)
         issue_fwd(tmem, a_s, w_s + l * kWBytes);
         tc::mma_commit(bar);
       }
-      if (!wait_all(bar, phase)) { failed = true; break; }
+      if (!wait_all(v, bar, phase)) { failed = true; break; }
       tc::fence_after_sync();
       if (l + 1 < kLayers) {
         uint32_t acc[64];
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(128, 1)
         issue_fwd(tmem, x_s + l * kTileBytes, w_s + l * kWBytes);
         tc::mma_commit(bar);
       }
-      if (!wait_all(bar, phase)) { failed = true; break; }
+      if (!wait_all(v, bar, phase)) { failed = true; break; }
       tc::fence_after_sync();
       if (l + 1 < kLayers) {
         uint32_t acc[64];
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(128, 1)
           tc::mma_f16(tmem, tc::desc_k(g_s, kk), tc::desc_mn(w_s + l * kWBytes, kk, kWBytes), kIdescBwd, kk);
         tc::mma_commit(bar);
       }
-      if (!wait_all(bar, phase)) { failed = true; break; }
+      if (!wait_all(v, bar, phase)) { failed = true; break; }
       tc::fence_after_sync();
       uint32_t acc[64];
       load_acc64(lane_addr, acc);  // dX_l

@@ -46,9 +46,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Non-blocking probe of phase `parity` (mbarrier.test_wait: returns at once).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Limits below this many clocks poll with test_wait, whose return is immediate
+// (try_wait may suspend the thread for a while before it gives up).
+constexpr long long kShortWaitCycles = 1000000ll;
 // Bounded wait for phase `parity`: false after ~`max_cycles` clocks.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long max_cycles) {
   const long long t0 = clock64();
+  if (max_cycles < kShortWaitCycles) {
+    while (!mbar_test_wait(bar, parity)) {
+      if (clock64() - t0 > max_cycles) return false;
+    }
+    return true;
+  }
   while (!mbar_try_wait(bar, parity)) {
     if (clock64() - t0 > max_cycles) return false;
   }

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
                                                   const uint32_t* __restrict__ n_dev,
                                                   const float4* __restrict__ insts, uint32_t root,
                                                   const uint32_t* __restrict__ roots, uint32_t hot_count,
-                                                  int stk) {
+                                                  int stk, long long stage_wait) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -162,6 +162,7 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
   __shared__ uint64_t hot_bar;
   uint2 stack[kMaxStack];
   const uint4* const hot = hot_mem;
+  uint32_t hot_n = hot_count;  // staged nodes this CTA reads from shared memory
   if (HOT && hot_count) {
     // one bulk copy (TMA engine, no multicast) into shared memory, completed
     // on an mbarrier by transaction bytes
@@ -175,12 +176,13 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
                    : "memory");
     }
     __syncthreads();
-    if (!tc::mbar_wait(&hot_bar, 0, kStagingWaitCycles)) {
-      // report, let a late copy land before the shared memory is released,
-      // and leave the rays to the other CTAs
+    if (!tc::mbar_wait(&hot_bar, 0, stage_wait)) {
+      // report, let a late copy land (full limit) so nothing writes this
+      // CTA's shared memory after it, and traverse from global memory: the
+      // results stay complete, the host reads the status bit
       atomicOr(status, kTraceStagingWait);
       tc::mbar_wait(&hot_bar, 0, kStagingWaitCycles);
-      return;
+      hot_n = 0;
     }
   }
   const uint32_t lane = threadIdx.x & 31u;
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
       if (HOT) {
         // staged prefix from shared memory, the rest from global (one generic load path)
         const uint32_t hrel = node - root;
-        if (hrel < hot_count) np = hot + hrel * 5;
+        if (hrel < hot_n) np = hot + hrel * 5;
         w0 = np[0]; w1 = np[1]; w2 = np[2]; w3 = np[3]; w4 = np[4];
       } else {
         w0 = __ldg(np); w1 = __ldg(np + 1); w2 = __ldg(np + 2); w3 = __ldg(np + 3); w4 = __ldg(np + 4);
@@ -554,7 +556,7 @@ void launch_trace_k(const TraceArgs& a, cudaStream_t s) {
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
   (hot ? staged : plain)<<<(unsigned)grid, kBlock, stack_bytes + 80 * (size_t)hot, s>>>(
       a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded, a.status, a.counter, a.n_dev, a.insts, a.root, a.roots, hot,
-      stk);
+      stk, a.stage_wait_cycles > 0 ? a.stage_wait_cycles : kStagingWaitCycles);
 }
 
 template <bool ANY>

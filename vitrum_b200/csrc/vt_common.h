@@ -55,6 +55,12 @@ vt_status guard(F&& fn) {
   }
 }
 
+// Failure-injection hook for tests (vt_debug_fail_device_allocation): the
+// nth DeviceBuffer allocation on this thread from the arming on fails as if
+// cudaMalloc had run out of memory.  Returns true for the allocation that must fail.
+void arm_allocation_failure(long long nth);
+bool injected_allocation_failure();
+
 // Owning device allocation (cudaMalloc / cudaFree), move-only.
 template <class T>
 struct DeviceBuffer {
@@ -78,7 +84,10 @@ struct DeviceBuffer {
   void resize(size_t n) {
     if (n == count) return;
     release();
-    if (n) VT_CUDA(cudaMalloc(&ptr, n * sizeof(T)));
+    if (n) {
+      if (injected_allocation_failure()) fail(VT_ERR_OUT_OF_MEMORY, "injected device allocation failure");
+      VT_CUDA(cudaMalloc(&ptr, n * sizeof(T)));
+    }
     count = n;
   }
   size_t bytes() const { return count * sizeof(T); }

@@ -348,9 +348,22 @@ def _marshal_scene(scene: "Scene"):
 
 
 # ---------------------------------------------------------------- engine
+def debug_fail_device_allocation(nth: int) -> None:
+    """Failure-injection hook (vt_debug_fail_device_allocation): the nth device
+    allocation the library makes on this thread from now on fails as an
+    out-of-memory cudaMalloc would; 0 disarms."""
+    N.call("vt_debug_fail_device_allocation", int(nth))
+
+
 class _Debug:
     def __init__(self, engine: "Engine"):
         self._e = engine
+
+    def set_wait_limit(self, cycles: int) -> None:
+        """Failure-detection hook (vt_engine_set_wait_limit): bound the first
+        wait of the cache kernels' and the staging copy's bounded waits to
+        `cycles` clocks (0: the default of about a second)."""
+        N.call("vt_engine_set_wait_limit", self._e.handle, int(cycles))
 
     def pick_triangle(self, x: float, y: float) -> Optional[int]:
         """vt_pick as it is: under pixel (x, y) of the last frame's camera, the
