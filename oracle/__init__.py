@@ -545,3 +545,93 @@ def pick_primitive(scene, camera, px, py, width, height):
             best = dict(mesh=int(mi), instance=int(inst), triangle=int(tri_base[mi] + k) if inst < 0 else -1,
                         t=float(t[k]), margin=float(margin[k]))
     return best
+
+
+# ---------------------------------------------------------------- BSDF probes
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, np.float32)
+    return a if shape is None else a.reshape(shape)
+
+
+def _bsdf_lib():
+    L = _pt_lib()
+    if not getattr(L, "_bsdf_ready", False):
+        P = ctypes.c_void_p
+        F = ctypes.c_float
+        L.orc_smith_g1.restype = F
+        L.orc_smith_g1.argtypes = [F, F]
+        L.orc_ggx_d.restype = F
+        L.orc_ggx_d.argtypes = [F, F]
+        L.orc_ggx_vndf_batch.restype = None
+        L.orc_ggx_vndf_batch.argtypes = [P, F, P, ctypes.c_long, P]
+        L.orc_vndf_pdf_batch.restype = None
+        L.orc_vndf_pdf_batch.argtypes = [P, P, P, ctypes.c_long, P]
+        L.orc_diel_fresnel.restype = F
+        L.orc_diel_fresnel.argtypes = [P, F, F]
+        L.orc_diel_event_probs.restype = None
+        L.orc_diel_event_probs.argtypes = [P, F, F, F, P]
+        L.orc_bsdf_eval_batch.restype = None
+        L.orc_bsdf_eval_batch.argtypes = [P, F, P, P, ctypes.c_long, P, P]
+        L.orc_bsdf_sample_batch.restype = None
+        L.orc_bsdf_sample_batch.argtypes = [P, F, P, ctypes.c_long, ctypes.c_uint32, P, P, P, P]
+        L._bsdf_ready = True
+    return L
+
+
+def material12(base=(1, 1, 1), roughness=0.5, metallic=0.0, transmission=0.0, ior=1.5, specular=1.0):
+    """The oracle's 12-float material record (layout at orc_pt_scene_create)."""
+    return _f32([*base, roughness, metallic, transmission, ior, 0, 0, 0, 0, specular])
+
+
+def smith_g1(c, alpha):
+    return float(_bsdf_lib().orc_smith_g1(c, alpha))
+
+
+def ggx_d(nh, alpha):
+    return float(_bsdf_lib().orc_ggx_d(nh, alpha))
+
+
+def ggx_vndf(wo, alpha, u):
+    """Visible-normal samples (n, 3) for uniforms u (n, 2)."""
+    u = _f32(u, (-1, 2))
+    out = np.empty((u.shape[0], 3), np.float32)
+    _bsdf_lib().orc_ggx_vndf_batch(_p(_f32(wo)), alpha, _p(u), u.shape[0], _p(out))
+    return out
+
+
+def vndf_pdf(mat, wo, wm):
+    """Half-vector density D(wm) G1(wo) (wo.wm) / (n.wo) for directions wm (n, 3)."""
+    wm = _f32(wm, (-1, 3))
+    out = np.empty(wm.shape[0], np.float32)
+    _bsdf_lib().orc_vndf_pdf_batch(_p(mat), _p(_f32(wo)), _p(wm), wm.shape[0], _p(out))
+    return out
+
+
+def diel_fresnel(mat, c, eta):
+    return float(_bsdf_lib().orc_diel_fresnel(_p(mat), c, eta))
+
+
+def diel_event_probs(mat, eta, cos_o, wo_wm):
+    """(joint reflection, diffuse, transmission, P(reflection | not diffuse))."""
+    out = np.empty(4, np.float32)
+    _bsdf_lib().orc_diel_event_probs(_p(mat), eta, cos_o, wo_wm, _p(out))
+    return out
+
+
+def bsdf_eval(mat, eta, wo, wi):
+    """(f |cos wi| rgb (n, 3), sampling density (n,)) for directions wi (n, 3)."""
+    wi = _f32(wi, (-1, 3))
+    fc = np.empty((wi.shape[0], 3), np.float32)
+    pdf = np.empty(wi.shape[0], np.float32)
+    _bsdf_lib().orc_bsdf_eval_batch(_p(mat), eta, _p(_f32(wo)), _p(wi), wi.shape[0], _p(fc), _p(pdf))
+    return fc, pdf
+
+
+def bsdf_sample(mat, eta, wo, n, seed=1):
+    """n BSDF samples: (wi (n, 3), weight (n, 3), pdf (n,), flags (n,): bit 0 valid, bit 1 delta)."""
+    wi = np.empty((n, 3), np.float32)
+    w = np.empty((n, 3), np.float32)
+    pdf = np.empty(n, np.float32)
+    fl = np.empty(n, np.int32)
+    _bsdf_lib().orc_bsdf_sample_batch(_p(mat), eta, _p(_f32(wo)), n, seed, _p(wi), _p(w), _p(pdf), _p(fl))
+    return wi, w, pdf, fl

@@ -839,6 +839,77 @@ static void* pt_worker(void* arg) {
   return NULL;
 }
 
+/* material record of 12 floats (layout at orc_pt_scene_create) */
+static orc_mat_t make_mat(const float* m) {
+  orc_mat_t r;
+  memset(&r, 0, sizeof r);
+  for (int k = 0; k < 3; ++k) { r.base[k] = m[k]; r.emission[k] = m[7 + k]; }
+  r.roughness = m[3];
+  r.ior = m[6] > 0 ? fmaxf(m[6], 1.0f) : 1.5f;
+  r.metallic = m[4];
+  r.transmission = clamp01f(m[5]);
+  r.specular = m[11];
+  float ratio = (r.ior - 1.0f) / (r.ior + 1.0f);
+  r.f0_ior = ratio * ratio * r.specular;
+  r.kind = (m[5] > 0 && m[4] == 0.0f) ? 2 : (m[4] > 0.0f ? 1 : 0);
+  r.alpha = fmaxf(m[3] * m[3], 1e-3f);
+  r.emissive = m[7] > 0 || m[8] > 0 || m[9] > 0;
+  r.flags = (unsigned)m[10];
+  return r;
+}
+
+/*
+ * BSDF probes for the known-answer tests, in the shading frame (normal +z).
+ * eta = n_t / n_i for light arriving along wo (dielectrics).
+ */
+float orc_smith_g1(float c, float alpha) { return smith_g1(c, alpha); }
+float orc_ggx_d(float nh, float alpha) { return ggx_d(nh, alpha); }
+void orc_ggx_vndf_batch(const float* wo, float alpha, const float* u, long n, float* wm) {
+  v3 o = V(wo[0], wo[1], wo[2]);
+  for (long i = 0; i < n; ++i) {
+    v3 h = ggx_vndf(o, alpha, u[2 * i], u[2 * i + 1]);
+    wm[3 * i] = h.x; wm[3 * i + 1] = h.y; wm[3 * i + 2] = h.z;
+  }
+}
+void orc_vndf_pdf_batch(const float* mat12, const float* wo, const float* wm, long n, float* out) {
+  orc_mat_t m = make_mat(mat12);
+  v3 o = V(wo[0], wo[1], wo[2]);
+  for (long i = 0; i < n; ++i) out[i] = vndf_pdf(&m, o, V(wm[3 * i], wm[3 * i + 1], wm[3 * i + 2]));
+}
+float orc_diel_fresnel(const float* mat12, float c, float eta) {
+  orc_mat_t m = make_mat(mat12);
+  return diel_fresnel(&m, c, eta);
+}
+void orc_diel_event_probs(const float* mat12, float eta, float cos_o, float wo_wm, float* out4) {
+  orc_mat_t m = make_mat(mat12);
+  diel_event_probs(&m, eta, cos_o, wo_wm, out4);
+}
+/* f * |cos wi| (rgb) and the sampling density of wi, for n directions wi */
+void orc_bsdf_eval_batch(const float* mat12, float eta, const float* wo, const float* wi, long n, float* fc,
+                         float* pdf) {
+  orc_mat_t m = make_mat(mat12);
+  v3 o = V(wo[0], wo[1], wo[2]);
+  for (long i = 0; i < n; ++i) {
+    v3 f;
+    bsdf_eval(&m, eta, o, V(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), &f, &pdf[i]);
+    fc[3 * i] = f.x; fc[3 * i + 1] = f.y; fc[3 * i + 2] = f.z;
+  }
+}
+/* n samples of the BSDF from one PCG stream; flags bit 0 valid, bit 1 delta */
+void orc_bsdf_sample_batch(const float* mat12, float eta, const float* wo, long n, uint32_t seed, float* wi,
+                           float* weight, float* pdf, int* flags) {
+  orc_mat_t m = make_mat(mat12);
+  v3 o = V(wo[0], wo[1], wo[2]);
+  uint32_t rng = pcg_init(seed, seed * 7u + 1u, 0x9E3779B9u);
+  for (long i = 0; i < n; ++i) {
+    bsample_t b = sample_bsdf(&m, eta, o, &rng);
+    wi[3 * i] = b.wi.x; wi[3 * i + 1] = b.wi.y; wi[3 * i + 2] = b.wi.z;
+    weight[3 * i] = b.weight.x; weight[3 * i + 1] = b.weight.y; weight[3 * i + 2] = b.weight.z;
+    pdf[i] = b.pdf;
+    flags[i] = (b.valid ? 1 : 0) | (b.delta ? 2 : 0);
+  }
+}
+
 /*
  * Scene set-up, done once per scene: the binned-SAH BVH over all triangles
  * (orc_build_array_bvh), the material table, the emissive-triangle area CDF
@@ -866,21 +937,7 @@ void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, lon
   long nn = orc_build_array_bvh(pos, nvert * 4, 4, idx, ntri, 4, 4, 16, 58, S->nodes, S->r2s);
   if (nn < 0) { free(S->nodes); free(S->r2s); free(S); return NULL; }
   orc_mat_t* mats = (orc_mat_t*)calloc((size_t)(n_mat > 0 ? n_mat : 1), sizeof(orc_mat_t));
-  for (int i = 0; i < n_mat; ++i) {
-    const float* m = materials + 12 * i;
-    for (int k = 0; k < 3; ++k) { mats[i].base[k] = m[k]; mats[i].emission[k] = m[7 + k]; }
-    mats[i].roughness = m[3];
-    mats[i].ior = m[6] > 0 ? fmaxf(m[6], 1.0f) : 1.5f;
-    mats[i].metallic = m[4];
-    mats[i].transmission = clamp01f(m[5]);
-    mats[i].specular = m[11];
-    float ratio = (mats[i].ior - 1.0f) / (mats[i].ior + 1.0f);
-    mats[i].f0_ior = ratio * ratio * mats[i].specular;
-    mats[i].kind = (m[5] > 0 && m[4] == 0.0f) ? 2 : (m[4] > 0.0f ? 1 : 0);
-    mats[i].alpha = fmaxf(m[3] * m[3], 1e-3f);
-    mats[i].emissive = m[7] > 0 || m[8] > 0 || m[9] > 0;
-    mats[i].flags = (unsigned)m[10];
-  }
+  for (int i = 0; i < n_mat; ++i) mats[i] = make_mat(materials + 12 * i);
   S->mats = mats;
   uint32_t* em = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(ntri + 1));
   float* cdf = (float*)malloc(sizeof(float) * (size_t)(ntri + 1));
