@@ -127,6 +127,48 @@ vt_status vt_bvh_trace_any(vt_bvh* bvh, const vt_ray* rays, size_t n, uint8_t* o
 
 vt_status vt_bvh_destroy(vt_bvh* bvh);
 
+/* Structural proof of a packed binary BVH (validateBvhEncoding,
+ * shared-bvh/src/validateBvhEncoding.ts:55, BvhEncodingProof). */
+typedef struct vt_bvh_proof {
+  int64_t node_count;
+  int64_t root_count;
+  int64_t interior_node_count;
+  int64_t leaf_node_count;
+  int64_t max_depth;
+  int64_t max_traversal_stack_entries;   /* depth + 1: the deepest path plus one pending sibling per ancestor */
+  int64_t traversal_stack_capacity;
+  int64_t triangle_count;                /* -1 when not checked */
+} vt_bvh_proof;
+
+/*
+ * Replaces validateBvhEncoding (validateBvhEncoding.ts:55): proves a packed
+ * binary BVH (node_words = 8 u32 per node, buildArrayBvh.ts:13-27) safe for a
+ * fixed-stack traversal -- buffer extent, declared roots, reachability with
+ * exclusive ownership, split axes, finite ordered bounds enclosing both
+ * children, leaf ranges tiling [0, triangle_count) exactly (triangle_count
+ * < 0: not checked), and depth + 1 <= traversal_stack_capacity (0: 60).
+ * roots == NULL: root 0.  A violation returns VT_ERR_BUILD with the
+ * reference's message; host only.
+ */
+vt_status vt_validate_bvh_encoding(const uint32_t* node_words, size_t word_count, size_t total_nodes,
+                                   const uint32_t* roots, size_t root_count, int64_t triangle_count,
+                                   int32_t traversal_stack_capacity, vt_bvh_proof* out_proof);
+
+/* Proof of this library's 8-wide tree as it lies on the device (read back):
+ * every node reached once, record masks contiguous, every triangle named by
+ * exactly one leaf record, every vertex inside its slot's and all ancestor
+ * slots' dequantised boxes, stack bound within capacity.  The same proof runs
+ * on every tree before it is published (vt_bvh_build*, vt_set_scene). */
+typedef struct vt_wide_proof {
+  int64_t node_count;
+  int64_t internal_slots;
+  int64_t leaf_slots;
+  int64_t triangle_count;
+  int64_t depth;
+  int64_t stack_entries;
+} vt_wide_proof;
+vt_status vt_bvh_validate(const vt_bvh* bvh, vt_wide_proof* out_proof);
+
 /*
  * Top-level build over instance world AABBs (replaces buildTlas,
  * shared-bvh/src/tlas.ts:859-989): binned SAH over the boxes' centroids, the

@@ -195,3 +195,16 @@ def test_differential_gate_leaf1(cuda):
     g, w = _build_both(soup, maxLeafTriangles=1)
     rep = _assert_parity(soup, rays, g, w, "differential")
     assert rep["hits"] > 100 and rep["n"] - rep["hits"] > 100, rep
+
+
+@pytest.mark.parametrize("n,leaf", [(65536, 4), (5000, 1), (20000, 3), (1, 4)])
+def test_device_tree_passes_structural_proof(cuda, n, leaf):
+    """The 8-wide tree read back from the device: every node once, every
+    triangle named by one leaf record, vertices inside all culling boxes."""
+    soup = scenes.random_triangles(n, seed=100 + leaf)
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices, maxLeafTriangles=leaf)
+    p = g.validate()
+    info = g.info()
+    assert p["triangle_count"] == n and p["node_count"] == info["wide_node_count"]
+    assert p["depth"] == info["wide_depth"] and p["stack_entries"] <= 64
+    g.close()

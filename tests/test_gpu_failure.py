@@ -97,7 +97,7 @@ def test_set_scene_rolls_back_at_every_allocation_stage(cuda):
         try:
             e.set_scene(other)
         except N.VtError as err:
-            assert err.value.status == VT_ERR_OUT_OF_MEMORY and "injected" in str(err)
+            assert err.status == VT_ERR_OUT_OF_MEMORY and "injected" in str(err)
             stages += 1
             # the previous scene is intact: the same image, bit for bit
             assert _frame(e, cam).tobytes() == want.tobytes(), k

@@ -158,8 +158,9 @@ def test_pick_returns_instance_index(cuda):
     e = Engine(max_bounces=1, debug=True)
     e.set_scene(sc)
     e.render_frame(cam, 64, 64, samples=1)
-    assert e.debug.pick_primitive(32.0, 32.0) == 1
-    assert e.debug.pick_primitive(2.0, 2.0) is None
+    assert e.debug.pick_triangle(32.0, 32.0) == 1      # the middle instance
+    assert e.debug.pick_primitive(32.0, 32.0) == 0     # ... of the scene's one mesh primitive
+    assert e.debug.pick_triangle(2.0, 2.0) is None and e.debug.pick_primitive(2.0, 2.0) is None
     e.dispose()
 
 

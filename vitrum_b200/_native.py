@@ -36,6 +36,17 @@ class BvhInfo(ctypes.Structure):
                 ("binary_depth", ctypes.c_int32), ("build_ms", ctypes.c_double)]
 
 
+class BvhProof(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("node_count", "root_count", "interior_node_count", "leaf_node_count",
+                                               "max_depth", "max_traversal_stack_entries",
+                                               "traversal_stack_capacity", "triangle_count")]
+
+
+class WideProof(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("node_count", "internal_slots", "leaf_slots", "triangle_count",
+                                               "depth", "stack_entries")]
+
+
 class WatertightResult(ctypes.Structure):
     _fields_ = [("hit", ctypes.c_int32), ("t", ctypes.c_float), ("bary", ctypes.c_float * 3),
                 ("side", ctypes.c_int32), ("zero_edge_mask", ctypes.c_int32)]
@@ -61,6 +72,8 @@ SIGNATURES = {
     "vt_bvh_trace_any": [P, P, SZ, P],
     "vt_bvh_destroy": [P],
     "vt_tlas_build": [P, SZ, I32, I32, I32, P, SZ, P, SZ, P],
+    "vt_validate_bvh_encoding": [P, SZ, SZ, P, SZ, ctypes.c_int64, I32, P],
+    "vt_bvh_validate": [P, P],
     "vt_engine_export_tlas": [P, P, SZ, P, SZ, P],
     "vt_bvh_trace_closest_noalloc": [P, P, SZ, P],
     "vt_watertight_eval_device": [I32, P, SZ, P, P],

@@ -6,6 +6,7 @@ Mirrors the reference's shared-bvh entry points (packages/shared-bvh/src):
     intersectCompressedWideBvhFirstHit       -> Bvh.intersect_first_hit()
     intersectCompressedWideBvhAnyHit         -> Bvh.intersect_any_hit()
     buildTlas (tlas.ts:859)                  -> build_tlas()
+    validateBvhEncoding                      -> validate_bvh_encoding()
 
 Options keep the reference names and defaults (BuildArrayBvhOpts,
 buildArrayBvh.ts:277-318).  Invalid options raise ValueError (RangeError /
@@ -71,6 +72,13 @@ class Bvh:
         i = N.BvhInfo()
         N.call("vt_bvh_get_info", self.handle, ctypes.byref(i))
         return {f: getattr(i, f) for f, _ in N.BvhInfo._fields_}
+
+    def validate(self) -> dict:
+        """Structural proof of the device-resident 8-wide tree (vt_bvh_validate);
+        raises VtError(VT_ERR_BUILD) on a violation."""
+        p = N.WideProof()
+        N.call("vt_bvh_validate", self.handle, ctypes.byref(p))
+        return {f: getattr(p, f) for f, _ in N.WideProof._fields_}
 
     def export_binary(self):
         """(nodes (n, 8) uint32 in the reference layout, reordered_to_source uint32)."""
@@ -155,3 +163,25 @@ def build_tlas(aabbs, **opts):
     perm = np.zeros(n, np.uint32)
     N.call("vt_tlas_build", _ptr(a), n, *args, _ptr(nodes), nodes.size, _ptr(perm), n, ctypes.byref(count))
     return nodes, perm
+
+
+def validate_bvh_encoding(node_words, total_nodes, roots=None, triangle_count=None, traversal_stack_capacity=None):
+    """validateBvhEncoding (shared-bvh/src/validateBvhEncoding.ts:55): structural
+    proof of a packed binary BVH (8 u32 words per node).  Returns the proof as
+    a dict with the reference's keys; raises VtError(VT_ERR_BUILD) carrying the
+    reference's message on a violation."""
+    w = np.ascontiguousarray(np.asarray(node_words).view(np.uint32) if np.asarray(node_words).dtype == np.float32
+                             else np.asarray(node_words, np.uint32)).reshape(-1)
+    r = None if roots is None else np.ascontiguousarray(roots, np.uint32)
+    p = N.BvhProof()
+    N.call("vt_validate_bvh_encoding", _ptr(w) if w.size else None, w.size, int(total_nodes),
+           _ptr(r) if r is not None and r.size else (ctypes.c_void_p(1) if r is not None else None),
+           0 if r is None else r.size, -1 if triangle_count is None else int(triangle_count),
+           0 if traversal_stack_capacity is None else int(traversal_stack_capacity), ctypes.byref(p))
+    out = {"nodeCount": p.node_count, "rootCount": p.root_count, "interiorNodeCount": p.interior_node_count,
+           "leafNodeCount": p.leaf_node_count, "maxDepth": p.max_depth,
+           "maxTraversalStackEntries": p.max_traversal_stack_entries,
+           "traversalStackCapacity": p.traversal_stack_capacity}
+    if triangle_count is not None:
+        out["triangleCount"] = p.triangle_count
+    return out

@@ -45,6 +45,10 @@ static BuildOptions resolve(const vt_bvh_build_options* o) {
 
 static void upload(vt_bvh* b, const float* positions, const uint32_t* indices) {
   WideBvhHost w = encode_wide(b->binary, positions, b->opts.position_stride, indices, b->opts.index_stride);
+  // publication proofs (the reference validates every tree it publishes)
+  validate_binary(b->binary, b->ntri);
+  validate_wide(w.nodes.data(), w.nodes.size() / 20, w.tris.data(), w.tris.size() / 16, 0, (size_t)b->ntri, false,
+                kTraversalStack);
   DeviceScope ds(b->device);
   b->nodes.resize(w.nodes.size() / 4);
   b->tris.resize(std::max<size_t>(w.tris.size() / 4, 1));
@@ -270,6 +274,46 @@ vt_status vt_bvh_trace_any(vt_bvh* b, const vt_ray* rays, size_t n, uint8_t* occ
     VT_CUDA(cudaGetLastError());
     VT_CUDA(cudaMemcpy(occluded, b->occ_scratch.ptr, n, cudaMemcpyDeviceToHost));
     check_status(b);
+  });
+}
+
+vt_status vt_validate_bvh_encoding(const uint32_t* node_words, size_t word_count, size_t total_nodes,
+                                   const uint32_t* roots, size_t root_count, int64_t triangle_count,
+                                   int32_t traversal_stack_capacity, vt_bvh_proof* out) {
+  return guard([&] {
+    if (word_count && !node_words) fail(VT_ERR_INVALID_ARGUMENT, "node_words is null");
+    if (traversal_stack_capacity < 0) fail(VT_ERR_RANGE, "traversal_stack_capacity must be >= 0");
+    BinaryProof p = validate_binary_encoding(node_words, word_count, total_nodes, roots, roots ? root_count : 0,
+                                             triangle_count, traversal_stack_capacity ? traversal_stack_capacity : 60);
+    if (out) {
+      out->node_count = p.node_count;
+      out->root_count = p.root_count;
+      out->interior_node_count = p.interior_node_count;
+      out->leaf_node_count = p.leaf_node_count;
+      out->max_depth = p.max_depth;
+      out->max_traversal_stack_entries = p.max_stack_entries;
+      out->traversal_stack_capacity = p.stack_capacity;
+      out->triangle_count = p.triangle_count;
+    }
+  });
+}
+
+vt_status vt_bvh_validate(const vt_bvh* b, vt_wide_proof* out) {
+  return guard([&] {
+    if (!b || !out) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    DeviceScope ds(b->device);
+    std::vector<uint32_t> nodes(b->nodes.count * 4);
+    std::vector<float> recs(b->tris.count * 4);
+    VT_CUDA(cudaMemcpy(nodes.data(), b->nodes.ptr, nodes.size() * 4, cudaMemcpyDeviceToHost));
+    VT_CUDA(cudaMemcpy(recs.data(), b->tris.ptr, recs.size() * 4, cudaMemcpyDeviceToHost));
+    WideProof p = validate_wide(nodes.data(), nodes.size() / 20, recs.data(), recs.size() / 16, 0, (size_t)b->ntri,
+                                false, kTraversalStack);
+    out->node_count = p.node_count;
+    out->internal_slots = p.internal_slots;
+    out->leaf_slots = p.leaf_slots;
+    out->triangle_count = p.items;
+    out->depth = p.depth;
+    out->stack_entries = p.stack_entries;
   });
 }
 

@@ -32,6 +32,30 @@ struct WideBvhHost {
 };
 
 void validate_options(const BuildOptions& o);
+
+// Structural proof of a packed binary BVH (the reference's validateBvhEncoding,
+// shared-bvh/src/validateBvhEncoding.ts:55); throws vt::Error(VT_ERR_BUILD).
+// roots == nullptr: root 0; tri_count < 0: leaf ranges are not checked.
+struct BinaryProof {
+  int64_t node_count = 0, root_count = 0, interior_node_count = 0, leaf_node_count = 0, max_depth = 0,
+          max_stack_entries = 0, stack_capacity = 0, triangle_count = -1;
+};
+BinaryProof validate_binary_encoding(const uint32_t* words, size_t word_count, size_t total_nodes,
+                                     const uint32_t* roots, size_t n_roots, int64_t tri_count, int stack_cap);
+inline BinaryProof validate_binary(const BinaryBvhHost& b, int64_t tri_count, int stack_cap = 60) {
+  return validate_binary_encoding(reinterpret_cast<const uint32_t*>(b.nodes.data()), b.nodes.size() * 8,
+                                  b.nodes.size(), nullptr, 0, tri_count, stack_cap);
+}
+
+// Structural proof of one 8-wide tree (bvh_validate.cpp): node indices are
+// absolute, the arrays start at node node_base / record rec_base; items are
+// triangles (source id in v0.w) or, for a top level, instances (instance id).
+struct WideProof {
+  int64_t node_count = 0, internal_slots = 0, leaf_slots = 0, items = 0, depth = 0, stack_entries = 0;
+};
+WideProof validate_wide(const uint32_t* nodes, size_t n_nodes, const float* recs, size_t n_recs, uint32_t root,
+                        size_t n_items, bool instance_records, int stack_cap, uint32_t node_base = 0,
+                        uint32_t rec_base = 0);
 // The same tree built on the GPU from device positions / indices (binCount <= 16).
 BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const uint32_t* d_idx, size_t index_words,
                                const BuildOptions& o, cudaStream_t s);

@@ -194,6 +194,9 @@ BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& i
   BinaryBvhHost b = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
   BlasPack out;
   out.wide = encode_wide(b, pos.data(), 4, idx.data(), 4, mm.data(), node_base, rec_base, &kEngineCollapse);
+  validate_binary(b, (int64_t)ntri);
+  validate_wide(out.wide.nodes.data(), out.wide.nodes.size() / 20, out.wide.tris.data(), out.wide.tris.size() / 16,
+                node_base, ntri, false, kTraversalStack, node_base, rec_base);
   const BinaryNode& rn = b.nodes[0];
   out.local_box = {rn.mn[0], rn.mn[1], rn.mn[2], rn.mx[0], rn.mx[1], rn.mx[2]};
   if (ntri == 0) out.local_box = {0, 0, 0, 0, 0, 0};
@@ -252,6 +255,9 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     p.binary = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
     WideBvhHost w = encode_wide(p.binary, pos.data(), 4, idx.data(), 4, tri_mat.data(), node_base, rec_base,
                                 &kEngineCollapse);
+    validate_binary(p.binary, (int64_t)ntri);
+    validate_wide(w.nodes.data(), w.nodes.size() / 20, w.tris.data(), w.tris.size() / 16, node_base, ntri, false,
+                  kTraversalStack, node_base, rec_base);
     node_words = std::move(w.nodes);
     rec_floats = std::move(w.tris);
     depth = w.depth;
@@ -298,6 +304,9 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     BinaryBvhHost tl = build_tlas_host(aabbs.data(), ni);
     root = (uint32_t)(node_words.size() / 20);
     WideBvhHost tw = encode_wide_tlas(tl, recs.data(), root);
+    validate_binary(tl, (int64_t)ni);
+    validate_wide(tw.nodes.data(), tw.nodes.size() / 20, tw.tris.data(), tw.tris.size() / 16, root, ni, true,
+                  kTraversalStack, root, 0);
     node_words.insert(node_words.end(), tw.nodes.begin(), tw.nodes.end());
     inst_lanes = std::move(tw.tris);
     inst_tab.resize(16 * ni);
@@ -479,6 +488,9 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   p.rec_floats = std::move(w.tris);
   p.depth = w.depth;
   p.stack_depth = two_level ? 2 * w.depth + 6 : 2 * w.depth + 2;
+  if (p.stack_depth > kTraversalStack)
+    fail(VT_ERR_BUILD, "8-wide encoding proof: traversal needs " + std::to_string(p.stack_depth) +
+                           " stack entries (top and bottom levels), capacity " + std::to_string(kTraversalStack));
   p.root = two_level ? root : node_base;
   p.inst_lanes = std::move(inst_lanes);
   p.inst_tab = std::move(inst_tab);
