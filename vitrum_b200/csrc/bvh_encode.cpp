@@ -217,13 +217,22 @@ static bool reference_normal(const float a[3], const float b[3], const float c[3
   return true;
 }
 
-// Smallest e with 255 * 2^e >= extent (extent > 0), clamped to the normal range.
-static int grid_exponent(double extent) {
+// Grid corners origin + q * 2^e compared exactly: in 113-bit arithmetic the sum
+// of an f32 origin (24 bits) and q * 2^e (8 bits) is exact unless the two are
+// more than 2^88 apart in magnitude (a box whose extent is below 2^-88 of its
+// coordinates), where the traversal's slab slack of 8 f32 ulps covers it.
+static inline __float128 corner(float origin, int q, int e) {
+  return (__float128)origin + (__float128)std::ldexp((double)q, e);
+}
+
+// Smallest e with origin + 255 * 2^e >= hi (exactly), clamped to the normal range.
+static int grid_exponent(float origin, float hi) {
+  const double extent = (double)hi - (double)origin;
   if (!(extent > 0)) return -126;
   int e;
   std::frexp(extent / 255.0, &e);  // extent/255 = m * 2^e, m in [0.5, 1)
   while (e > -126 && std::ldexp(255.0, e - 1) >= extent) --e;
-  while (std::ldexp(255.0, e) < extent) ++e;
+  while (e < 127 && corner(origin, 255, e) < (__float128)hi) ++e;
   return std::min(127, std::max(-126, e));
 }
 
@@ -268,7 +277,7 @@ static WideBvhHost encode_core(const BinaryBvhHost& bin, const BinaryNode* nodes
     std::memcpy(bytes, p, 12);
     int ex[3];
     for (int k = 0; k < 3; ++k) {
-      ex[k] = grid_exponent((double)parent.mx[k] - (double)parent.mn[k]);
+      ex[k] = grid_exponent(parent.mn[k], parent.mx[k]);
       bytes[12 + k] = (uint8_t)(ex[k] + 127);
     }
     uint8_t imask = 0;
@@ -297,10 +306,13 @@ static WideBvhHost encode_core(const BinaryBvhHost& bin, const BinaryNode* nodes
         double step = std::ldexp(1.0, ex[k]);
         double lo = std::floor(((double)c.mn[k] - (double)p[k]) / step);
         double hi = std::ceil(((double)c.mx[k] - (double)p[k]) / step);
-        lo = std::min(255.0, std::max(0.0, lo));
-        hi = std::min(255.0, std::max(0.0, hi));
-        qlo[k * 8 + s] = (uint8_t)lo;
-        qhi[k * 8 + s] = (uint8_t)hi;
+        int ql = (int)std::min(255.0, std::max(0.0, lo));
+        int qh = (int)std::min(255.0, std::max(0.0, hi));
+        // outward exactly: (c - p) / step rounds when c is tiny next to p
+        while (ql > 0 && corner(p[k], ql, ex[k]) > (__float128)c.mn[k]) --ql;
+        while (qh < 255 && corner(p[k], qh, ex[k]) < (__float128)c.mx[k]) ++qh;
+        qlo[k * 8 + s] = (uint8_t)ql;
+        qhi[k * 8 + s] = (uint8_t)qh;
       }
       if (is_leaf_word(c.w7)) {
         const uint32_t cnt = c.w7 & 0xFFFFu;

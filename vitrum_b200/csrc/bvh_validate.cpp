@@ -17,7 +17,7 @@
 //   * the leaf records lie inside the record array and name every item
 //     (triangle source id, or instance id for a top level) exactly once;
 //   * conservative culling: every vertex of a leaf's triangles lies inside
-//     the dequantised box (origin + q * 2^e, exact in double) of its own slot
+//     the dequantised box (origin + q * 2^e, exact in 113-bit arithmetic) of its own slot
 //     and of every ancestor slot a ray must pass to reach it (instance leaves
 //     of a top level: skipped, their world boxes are not stored);
 //   * the traversal's stack bound (two entries per level plus two) fits.
@@ -165,11 +165,13 @@ WideProof validate_wide(const uint32_t* nodes_in, size_t n_local, const float* r
   std::vector<uint8_t> item_seen(n_items, 0);
   // breadth-first walk; each entry carries the intersection of its ancestors'
   // slot boxes -- what a ray must pass to reach it
-  struct Item { uint32_t node; int depth; double cull[6]; };
+  // boxes in 113-bit arithmetic: origin + q * 2^e is exact there (bvh_encode.cpp)
+  using Q = __float128;
+  struct Item { uint32_t node; int depth; Q cull[6]; };
   std::vector<Item> queue(1);
   queue[0].node = root;
   queue[0].depth = 1;
-  for (int k = 0; k < 3; ++k) { queue[0].cull[k] = -INFINITY; queue[0].cull[3 + k] = INFINITY; }
+  for (int k = 0; k < 3; ++k) { queue[0].cull[k] = (Q)-INFINITY; queue[0].cull[3 + k] = (Q)INFINITY; }
   std::vector<uint8_t> visited(n_nodes - root, 0);  // this tree's nodes follow its root
   for (size_t qi = 0; qi < queue.size(); ++qi) {
     const Item it = queue[qi];
@@ -181,7 +183,7 @@ WideProof validate_wide(const uint32_t* nodes_in, size_t n_local, const float* r
     p.depth = std::max<int64_t>(p.depth, it.depth);
     const uint32_t* w = nodes + 20 * (size_t)node;
     const uint8_t* bytes = reinterpret_cast<const uint8_t*>(w);
-    const double org[3] = {f32_of(w[0]), f32_of(w[1]), f32_of(w[2])};
+    const Q org[3] = {(Q)f32_of(w[0]), (Q)f32_of(w[1]), (Q)f32_of(w[2])};
     int ex[3];
     for (int k = 0; k < 3; ++k) ex[k] = (int)bytes[12 + k] - 127;
     const uint8_t imask = bytes[15];
@@ -198,12 +200,14 @@ WideProof validate_wide(const uint32_t* nodes_in, size_t n_local, const float* r
           if (qlo[k * 8 + s] != 255 || qhi[k * 8 + s] != 0) bad(W, at + " is empty but its box is not inverted");
         continue;
       }
-      double box[6];
+      Q box[6];
       for (int k = 0; k < 3; ++k) {
         if (qlo[k * 8 + s] > qhi[k * 8 + s]) bad(W, at + " has an inverted box");
-        // slot box in double (exact), intersected with the ancestors' boxes
-        box[k] = std::max(it.cull[k], org[k] + std::ldexp((double)qlo[k * 8 + s], ex[k]));
-        box[3 + k] = std::min(it.cull[3 + k], org[k] + std::ldexp((double)qhi[k * 8 + s], ex[k]));
+        // the slot box, intersected with the ancestors' boxes
+        const Q lo = org[k] + (Q)std::ldexp((double)qlo[k * 8 + s], ex[k]);
+        const Q hi = org[k] + (Q)std::ldexp((double)qhi[k * 8 + s], ex[k]);
+        box[k] = it.cull[k] > lo ? it.cull[k] : lo;
+        box[3 + k] = it.cull[3 + k] < hi ? it.cull[3 + k] : hi;
       }
       if (internal) {
         if (nib) bad(W, at + " is internal and owns records");
@@ -238,7 +242,7 @@ WideProof validate_wide(const uint32_t* nodes_in, size_t n_local, const float* r
         if (instance_records || rec[15] == 0.0f) continue;
         for (int v = 0; v < 3; ++v)
           for (int k = 0; k < 3; ++k) {
-            const double x = rec[4 * v + k];
+            const Q x = (Q)rec[4 * v + k];
             if (!(x >= box[k] && x <= box[3 + k]))
               bad(W, at + ": a vertex of record " + std::to_string(r) + " lies outside the boxes that cull it");
           }
