@@ -169,6 +169,38 @@ typedef struct vt_wide_proof {
 } vt_wide_proof;
 vt_status vt_bvh_validate(const vt_bvh* bvh, vt_wide_proof* out_proof);
 
+/* One emitter of a light tree (LightTreeBuildInput, shared-samplers/src/lightTree.ts:114-144). */
+typedef struct vt_light_tree_emitter {
+  double power;            /* luminance (x area for area emitters), >= 0 */
+  double centroid[3];
+  double aabb_min[3];
+  double aabb_max[3];
+  double cone_axis[3];     /* orientation cone (oriented = 1): emission axis, */
+  double cone_theta_o;     /* spread of the axes and */
+  double cone_theta_e;     /* emission half-angle beyond the axis (radians) */
+  int32_t oriented;        /* 0: full-sphere emitter */
+} vt_light_tree_emitter;
+
+/*
+ * Replaces buildLightTree + packLightTreeForGPU (lightTree.ts:492, 611): the
+ * pre-order binary light tree over n emitters, packed as 16 floats per node
+ * (emitter index, represented power, children, AABB, unit cone axis,
+ * outward-rounded cosines of thetaO and thetaO + thetaE, subtree leaf count).
+ * *node_count receives the node count (2n - 1); pass NULL to query it.  Host only.
+ */
+vt_status vt_light_tree_build(const vt_light_tree_emitter* emitters, size_t n, float* nodes, size_t float_capacity,
+                              size_t* node_count);
+
+/*
+ * The device selection the path tracer's next-event estimation uses
+ * (samplePackedLightTreeCPU, lightTree.ts:1237): for each point (3 floats) and
+ * 24-bit draw, the selected emitter and its probability (bucket count / 2^24).
+ * DEVICE pointers; enqueued on cuda_stream.
+ */
+vt_status vt_light_tree_select_device(const float* d_tree, size_t node_count, const float* d_points,
+                                      const uint32_t* d_buckets, size_t n, uint32_t* d_emitter, float* d_pmf,
+                                      void* cuda_stream);
+
 /*
  * Top-level build over instance world AABBs (replaces buildTlas,
  * shared-bvh/src/tlas.ts:859-989): binned SAH over the boxes' centroids, the
@@ -219,6 +251,9 @@ typedef struct vt_engine_options {
                                      about 4.7 GB), halved down to 2^20 until it fits half the free memory */
   int32_t bvh_max_leaf;           /* triangles per leaf of the engine's own trees, 1..4; 0 = 2 (the reference's
                                      builder with 2 instead of its default 4: the same hits, faster traversal) */
+  int32_t light_selection;        /* next-event light selection: 0 = the light tree when the scene has two or more
+                                     light entries (the reference's full tier: power x proximity x orientation,
+                                     shared-samplers/src/lightTree.ts), 1 = uniform over the entries */
 } vt_engine_options;
 
 /* Material (core MaterialSpec subset, core/src/scene/material.ts), the

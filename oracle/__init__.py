@@ -266,11 +266,11 @@ def _pt_lib():
                                     ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, P, ctypes.c_int,
                                     ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
-                                    ctypes.c_int, P, P, P, P, ctypes.c_long, P]
+                                    ctypes.c_int, P, P, P, P, ctypes.c_long, P, ctypes.c_int]
         L.orc_pt_scene_create.restype = ctypes.c_void_p
         L.orc_pt_scene_create.argtypes = [P, ctypes.c_long, P, ctypes.c_long, P, P, ctypes.c_int, P, ctypes.c_long,
                                           P, ctypes.c_long, P, ctypes.c_long, P, ctypes.c_int, ctypes.c_int,
-                                          ctypes.c_float, ctypes.c_float, ctypes.c_float]
+                                          ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int]
         L.orc_pt_scene_render.restype = ctypes.c_int
         L.orc_pt_scene_render.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, P, P, P, P, ctypes.c_long,
@@ -402,7 +402,7 @@ class PtScene:
     """The CPU path tracer's scene, set up once (BVH build, material table,
     emitter and environment CDFs) and rendered any number of times."""
 
-    def __init__(self, scene, bias=2e-5):
+    def __init__(self, scene, bias=2e-5, light_selection="tree"):
         pos, idx, tm, mats, pts, env, ei = flatten_scene(scene)
         dls = directional_lights(scene)
         als = area_lights(scene)
@@ -414,7 +414,8 @@ class PtScene:
         self.handle = _pt_lib().orc_pt_scene_create(
             _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(tm), _p(mats), mats.shape[0],
             _p(pts) if pts.size else None, pts.shape[0], _p(als) if als.size else None, als.shape[0],
-            _p(dls) if dls.size else None, dls.shape[0], _p(env) if env is not None else None, ew, eh, ei, er, bias)
+            _p(dls) if dls.size else None, dls.shape[0], _p(env) if env is not None else None, ew, eh, ei, er, bias,
+            {"tree": 0, "uniform": 1}[light_selection])
         if not self.handle:
             raise RuntimeError("oracle path tracer: scene build failed")
 
@@ -449,13 +450,13 @@ class PtScene:
 
 
 def pt_render(scene, camera, width, height, spp, max_bounces, seed=0, sample_base=0, bias=2e-5, nthreads=0,
-              log_rays=0):
+              log_rays=0, light_selection="tree"):
     """CPU path tracer: (sum, sum_sq) FP64 per pixel, shapes (H, W, 3).
 
     With log_rays > 0 also returns (closest_rays, shadow_rays, totals): the
     first log_rays extension and shadow rays as (n, 8) float32 rows and the
     total number of each traced."""
-    S = PtScene(scene, bias=bias)
+    S = PtScene(scene, bias=bias, light_selection=light_selection)
     try:
         return S.render(camera, width, height, spp, max_bounces, seed=seed, sample_base=sample_base,
                         nthreads=nthreads, log_rays=log_rays)
@@ -635,3 +636,59 @@ def bsdf_sample(mat, eta, wo, n, seed=1):
     fl = np.empty(n, np.int32)
     _bsdf_lib().orc_bsdf_sample_batch(_p(mat), eta, _p(_f32(wo)), n, seed, _p(wi), _p(w), _p(pdf), _p(fl))
     return wi, w, pdf, fl
+
+
+# ---------------------------------------------------------------- light tree
+def _lt_lib():
+    L = lib()
+    if not getattr(L, "_lt_ready", False):
+        P = ctypes.c_void_p
+        L.orc_lt_build.restype = ctypes.c_long
+        L.orc_lt_build.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_long]
+        L.orc_lt_sample.restype = ctypes.c_float
+        L.orc_lt_sample.argtypes = [P, ctypes.c_long, P, ctypes.c_float, ctypes.c_uint32, P]
+        L.orc_lt_pdf.restype = ctypes.c_float
+        L.orc_lt_pdf.argtypes = [P, ctypes.c_long, P, ctypes.c_float, ctypes.c_int]
+        L.orc_lt_importance.restype = ctypes.c_float
+        L.orc_lt_importance.argtypes = [P, ctypes.c_long, P, ctypes.c_float]
+        L._lt_ready = True
+    return L
+
+
+LT_BUCKETS = 1 << 24
+LT_FLOOR = 1e-3
+
+
+def light_tree_build(powers, centroids, aabbs, cones=None):
+    """buildLightTree + packLightTreeForGPU (shared-samplers/src/lightTree.ts:492, 611):
+    (nodes, 16) float32.  aabbs (n, 6) min|max; cones (n, 6) axis, thetaO, thetaE,
+    oriented flag (None: every emitter full-sphere)."""
+    pw = np.ascontiguousarray(powers, np.float64)
+    n = pw.size
+    c = np.ascontiguousarray(centroids, np.float64).reshape(n, 3)
+    b = np.ascontiguousarray(aabbs, np.float64).reshape(n, 6)
+    k = np.zeros((n, 6)) if cones is None else np.ascontiguousarray(cones, np.float64).reshape(n, 6)
+    out = np.zeros((2 * n, 16), np.float32)
+    m = _lt_lib().orc_lt_build(_p(pw), _p(c), _p(b), _p(k), n, _p(out), 2 * n)
+    if m < 0:
+        raise RuntimeError("light tree build failed")
+    return out[:m].copy()
+
+
+def light_tree_sample(tree, p, bucket, floor=LT_FLOOR):
+    """samplePackedLightTreeCPU with the 24-bit draw `bucket`: (emitter, pmf)."""
+    t = np.ascontiguousarray(tree, np.float32)
+    e = ctypes.c_int(-1)
+    pmf = _lt_lib().orc_lt_sample(_p(t), t.shape[0], _p(_f32(p)), floor, int(bucket), ctypes.byref(e))
+    return e.value, float(pmf)
+
+
+def light_tree_pdf(tree, p, emitter, floor=LT_FLOOR):
+    """packedLightTreePdfCPU: the PMF of `emitter` at point p."""
+    t = np.ascontiguousarray(tree, np.float32)
+    return float(_lt_lib().orc_lt_pdf(_p(t), t.shape[0], _p(_f32(p)), floor, int(emitter)))
+
+
+def light_tree_importance(tree, node, p, floor=LT_FLOOR):
+    t = np.ascontiguousarray(tree, np.float32)
+    return float(_lt_lib().orc_lt_importance(_p(t), int(node), _p(_f32(p)), floor))

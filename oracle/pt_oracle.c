@@ -34,6 +34,10 @@ long orc_build_array_bvh(const float* positions, long n_pos_words, int pos_strid
 int orc_tri_hit_d(const double o[3], const double d[3], const double a[3], const double b[3], const double c[3],
                   double tmin, double* t);
 int orc_hw_threads(void);
+long orc_lt_build(const double* power, const double* centroid, const double* aabb, const double* cone, long n,
+                  float* out, long cap);
+void orc_lt_merge_cones(const double* cones, long n, double* out6);
+float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d2, uint32_t bucket, int* emitter);
 
 #define PI_F 3.14159265358979323846f
 
@@ -128,6 +132,8 @@ typedef struct {
   float env_scale;
   float env_cos, env_sin; /* environment rotation about +y */
   int n_entries;
+  float* lt;              /* light tree over the entries (16 floats per node) or NULL: uniform selection */
+  long lt_nodes;
   float bias;
   /* camera / frame */
   const float* inv_vp;    /* row-major */
@@ -530,7 +536,8 @@ static v3 env_le(const orc_pt_t* S, int col, int row) {
   return scl(V(e[0], e[1], e[2]), S->env_scale);
 }
 
-typedef struct { v3 wi, Le; float dist, pdf; int delta, valid; } lsample_t;
+/* pdf includes the entry selection; pdf_light is the same without it (the MIS density) */
+typedef struct { v3 wi, Le; float dist, pdf, pdf_light; int delta, valid; } lsample_t;
 
 /* point / spot falloff: 1 / d^decay and the range window (material.wgsl.ts:2176-2204) */
 static float positional_falloff(float dist, float d2, float range, float decay) {
@@ -591,8 +598,21 @@ static int area_light_hit(const orc_pt_t* S, v3 o, v3 d, float t_max, v3* Le, fl
 static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
   lsample_t ls;
   memset(&ls, 0, sizeof ls);
-  float psel = 1.0f / (float)S->n_entries;
-  uint32_t e = rand_bounded(rng, (uint32_t)S->n_entries);
+  /* entry selection: the light tree (one 24-bit draw) or uniform; the
+   * selection probability is divided out of the estimate, not part of the MIS
+   * weights (pt-webgpu mediumNee.wgsl.ts:14-37, connect.wgsl.ts:598) */
+  float psel;
+  uint32_t e;
+  if (S->lt) {
+    float p3[3] = {P.x, P.y, P.z};
+    int em = -1;
+    psel = orc_lt_sample(S->lt, S->lt_nodes, p3, 1e-3f, pcg_next(rng) >> 8, &em);
+    if (em < 0 || em >= S->n_entries || !(psel > 0.0f)) return ls;
+    e = (uint32_t)em;
+  } else {
+    psel = 1.0f / (float)S->n_entries;
+    e = rand_bounded(rng, (uint32_t)S->n_entries);
+  }
   if (S->n_em > 0) {
     if (e == 0) {
       float u = rand01(rng);
@@ -613,7 +633,8 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
       const orc_mat_t* m = &S->mats[S->tmat[S->em_tri[k]]];
       ls.Le = V(m->emission[0], m->emission[1], m->emission[2]);
       ls.dist = dist;
-      ls.pdf = psel * d2 / (S->em_area * cosl);
+      ls.pdf_light = d2 / (S->em_area * cosl);
+      ls.pdf = psel * ls.pdf_light;
       ls.valid = 1;
       return ls;
     }
@@ -637,6 +658,7 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
     ls.dist = dist;
     ls.Le = scl(V(p[4], p[5], p[6]), cone * positional_falloff(dist, d2, p[13], p[14]));
     ls.pdf = psel;
+    ls.pdf_light = 1.0f;
     ls.delta = 1;
     ls.valid = 1;
     return ls;
@@ -658,7 +680,8 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
     if (!(cosl > 0.0f)) return ls;
     ls.Le = V(q[12], q[13], q[14]);
     ls.dist = dist;
-    ls.pdf = psel * d2 / (q[7] * cosl);
+    ls.pdf_light = d2 / (q[7] * cosl);
+    ls.pdf = psel * ls.pdf_light;
     ls.valid = 1;
     return ls;
   }
@@ -671,6 +694,7 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
     if (q[7] != 0.0f) {
       ls.wi = w;
       ls.pdf = psel;
+      ls.pdf_light = 1.0f;
       ls.delta = 1;
     } else {
       float u1 = rand01(rng), u2 = rand01(rng);
@@ -678,7 +702,8 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
       v3 tu, tv;
       onb(w, &tu, &tv);
       ls.wi = add(add(scl(tu, st * cosf(ph)), scl(tv, st * sinf(ph))), scl(w, ct));
-      ls.pdf = psel / (2.0f * PI_F * (1.0f - q[3]));
+      ls.pdf_light = 1.0f / (2.0f * PI_F * (1.0f - q[3]));
+      ls.pdf = psel * ls.pdf_light;
     }
     ls.valid = 1;
     return ls;
@@ -696,7 +721,8 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
   ls.wi = V(S->env_cos * md.x + S->env_sin * md.z, md.y, -S->env_sin * md.x + S->env_cos * md.z);
   ls.dist = INFINITY;
   ls.Le = env_le(S, col, row);
-  ls.pdf = psel * env_pdf(S, col, row, st);
+  ls.pdf_light = env_pdf(S, col, row, st);
+  ls.pdf = psel * ls.pdf_light;
   ls.valid = ls.pdf > 0.0f;
   return ls;
 }
@@ -727,7 +753,7 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
       v3 le = V(0, 0, 0);
       float pa;
       if (area_light_hit(S, o, d, tri < 0 ? INFINITY : (float)t, &le, &pa)) {
-        float w = prev_delta ? 1.0f : power_h(prev_pdf, pa / (float)S->n_entries);
+        float w = prev_delta ? 1.0f : power_h(prev_pdf, pa);
         L = add(L, scl(mul(T, le), w));
       }
     }
@@ -736,7 +762,7 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
         const float* q = S->dirs + 8 * k;
         if (q[7] != 0.0f || dot3(d, V(q[0], q[1], q[2])) < q[3]) continue;
         float w = 1.0f;
-        if (!prev_delta) w = power_h(prev_pdf, 1.0f / ((float)S->n_entries * 2.0f * PI_F * (1.0f - q[3])));
+        if (!prev_delta) w = power_h(prev_pdf, 1.0f / (2.0f * PI_F * (1.0f - q[3])));
         L = add(L, scl(mul(T, V(q[4], q[5], q[6])), w));
       }
       if (S->env) {
@@ -744,7 +770,7 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
         float st;
         env_texel(S, d, &col, &row, &st);
         float w = 1.0f;
-        if (!prev_delta && S->env_sampleable) w = power_h(prev_pdf, env_pdf(S, col, row, st) / (float)S->n_entries);
+        if (!prev_delta && S->env_sampleable) w = power_h(prev_pdf, env_pdf(S, col, row, st));
         L = add(L, scl(mul(T, env_le(S, col, row)), w));
       }
       break;
@@ -763,7 +789,7 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
       float w = 1.0f;
       if (!prev_delta) {
         float cosl = -dn;
-        float pl = cosl > 0.0f ? (1.0f / (float)S->n_entries) * tf * tf / (S->em_area * cosl) : 0.0f;
+        float pl = cosl > 0.0f ? tf * tf / (S->em_area * cosl) : 0.0f;
         w = power_h(prev_pdf, pl);
       }
       L = add(L, scl(mul(T, V(m->emission[0], m->emission[1], m->emission[2])), w));
@@ -782,7 +808,7 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
         float pb;
         bsdf_eval(m, eta, wol, wil, &fc, &pb);
         if (maxc(fc) > 0.0f) {
-          float w = (ls.delta || last) ? 1.0f : power_h(ls.pdf, pb);
+          float w = (ls.delta || last) ? 1.0f : power_h(ls.pdf_light, pb);
           v3 cc = scl(mul(mul(T, fc), ls.Le), w / ls.pdf);
           if (maxc(cc) > 0.0f) {
             v3 so = add(P, scl(n, wil.z > 0.0f ? off : -off));
@@ -911,6 +937,117 @@ void orc_bsdf_sample_batch(const float* mat12, float eta, const float* wo, long 
 }
 
 /*
+ * The light tree over the light entries in sample_light's order: the
+ * emissive-mesh group (one entry: power = sum of luminance x area, union AABB,
+ * the triangles' one-sided cones merged), points, spots (cone along the beam,
+ * half angle acos(cos outer)), rectangles and discs (one-sided cones), then the
+ * directionals and the environment with the union AABB of the positional
+ * lights (the reference's buildLightTreeInputForScene,
+ * pt-webgpu/src/scene/emitterPacking.ts:1005-1232).
+ */
+static double lum_f(double r, double g, double b) { return (double)(float)(0.2126 * r + 0.7152 * g + 0.0722 * b); }
+static void unit3(const double* v, double* o) {
+  double l = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  for (int k = 0; k < 3; ++k) o[k] = l > 1e-12 ? v[k] / l : 0.0;
+}
+static void build_light_tree(orc_pt_t* S, double env_tot) {
+  long n = S->n_entries, k = 0;
+  double* pw = (double*)calloc((size_t)n, sizeof(double));
+  double* cen = (double*)calloc((size_t)(3 * n), sizeof(double));
+  double* box = (double*)calloc((size_t)(6 * n), sizeof(double));
+  double* cone = (double*)calloc((size_t)(6 * n), sizeof(double));
+  double umn[3] = {INFINITY, INFINITY, INFINITY}, umx[3] = {-INFINITY, -INFINITY, -INFINITY};
+#define EXTEND(i) for (int q_ = 0; q_ < 3; ++q_) { umn[q_] = fmin(umn[q_], box[6 * (i) + q_]); umx[q_] = fmax(umx[q_], box[6 * (i) + 3 + q_]); }
+  if (S->n_em > 0) {
+    double* tc = (double*)calloc((size_t)(6 * S->n_em), sizeof(double));
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, p = 0.0;
+    for (long t = 0; t < S->n_em; ++t) {
+      double A[3], B[3], C[3];
+      tri_vertices(S, S->em_tri[t], A, B, C);
+      const orc_mat_t* m = &S->mats[S->tmat[S->em_tri[t]]];
+      double e1[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]}, e2[3] = {C[0] - A[0], C[1] - A[1], C[2] - A[2]};
+      double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+      float area = (float)(0.5 * sqrt(cx * cx + cy * cy + cz * cz));
+      p += (double)(float)(lum_f(m->emission[0], m->emission[1], m->emission[2]) * (double)area);
+      for (int q = 0; q < 3; ++q) {
+        mn[q] = fmin(mn[q], fmin(A[q], fmin(B[q], C[q])));
+        mx[q] = fmax(mx[q], fmax(A[q], fmax(B[q], C[q])));
+      }
+      double nn[3] = {cx, cy, cz};
+      unit3(nn, tc + 6 * t);
+      tc[6 * t + 3] = 0.0;
+      tc[6 * t + 4] = M_PI / 2;
+      tc[6 * t + 5] = 1.0;
+    }
+    pw[k] = p;
+    for (int q = 0; q < 3; ++q) {
+      box[6 * k + q] = mn[q];
+      box[6 * k + 3 + q] = mx[q];
+      cen[3 * k + q] = 0.5 * mn[q] + 0.5 * mx[q];
+    }
+    orc_lt_merge_cones(tc, S->n_em, cone + 6 * k);
+    free(tc);
+    EXTEND(k);
+    ++k;
+  }
+  for (long i = 0; i < S->n_points; ++i, ++k) {
+    const float* q = S->points + 16 * i;
+    pw[k] = lum_f(q[4], q[5], q[6]);
+    for (int c = 0; c < 3; ++c) cen[3 * k + c] = box[6 * k + c] = box[6 * k + 3 + c] = q[c];
+    if (q[15] != 0.0f) {
+      double ax[3] = {q[8], q[9], q[10]};
+      unit3(ax, cone + 6 * k);
+      cone[6 * k + 3] = 0.0;
+      cone[6 * k + 4] = acos(fmax(-1.0, fmin(1.0, (double)q[11])));
+      cone[6 * k + 5] = 1.0;
+    }
+    EXTEND(k);
+  }
+  for (long i = 0; i < S->n_areas; ++i, ++k) {
+    const float* q = S->areas + 16 * i;
+    pw[k] = (double)(float)(lum_f(q[12], q[13], q[14]) * (double)q[7]);
+    double U[3] = {q[4], q[5], q[6]}, W[3] = {q[8], q[9], q[10]};
+    double r = sqrt(U[0] * U[0] + U[1] * U[1] + U[2] * U[2]);
+    for (int c = 0; c < 3; ++c) {
+      double h = q[3] != 0.0f ? r : fabs(U[c]) + fabs(W[c]);
+      cen[3 * k + c] = q[c];
+      box[6 * k + c] = (double)q[c] - h;
+      box[6 * k + 3 + c] = (double)q[c] + h;
+    }
+    double nn[3] = {U[1] * W[2] - U[2] * W[1], U[2] * W[0] - U[0] * W[2], U[0] * W[1] - U[1] * W[0]};
+    unit3(nn, cone + 6 * k);
+    cone[6 * k + 3] = 0.0;
+    cone[6 * k + 4] = M_PI / 2;
+    cone[6 * k + 5] = 1.0;
+    EXTEND(k);
+  }
+#undef EXTEND
+  if (!isfinite(umn[0])) for (int q = 0; q < 3; ++q) umn[q] = umx[q] = 0.0;
+  long distant = S->n_dirs + (S->env_sampleable ? 1 : 0);
+  for (long i = 0; i < distant; ++i, ++k) {
+    if (i < S->n_dirs) {
+      const float* q = S->dirs + 8 * i;
+      double c = q[3];
+      pw[k] = lum_f(q[4], q[5], q[6]) * (q[7] != 0.0f ? 1.0 : M_PI * (1.0 - c * c));
+    } else {
+      pw[k] = (double)(float)(env_tot * (2.0 * M_PI * M_PI / ((double)S->env_w * S->env_h)));
+    }
+    for (int q = 0; q < 3; ++q) {
+      box[6 * k + q] = umn[q];
+      box[6 * k + 3 + q] = umx[q];
+      cen[3 * k + q] = (umn[q] + umx[q]) / 2;
+    }
+  }
+  S->lt = (float*)calloc((size_t)(16 * (2 * n)), sizeof(float));
+  S->lt_nodes = orc_lt_build(pw, cen, box, cone, n, S->lt, 2 * n);
+  if (S->lt_nodes <= 0) { free(S->lt); S->lt = NULL; S->lt_nodes = 0; }
+  free(pw);
+  free(cen);
+  free(box);
+  free(cone);
+}
+
+/*
  * Scene set-up, done once per scene: the binned-SAH BVH over all triangles
  * (orc_build_array_bvh), the material table, the emissive-triangle area CDF
  * and the environment's luminance CDFs.  materials: 12 floats each (base rgb
@@ -923,7 +1060,7 @@ void orc_bsdf_sample_batch(const float* mat12, float eta, const float* wo, long 
 void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, long ntri, const uint32_t* tri_mat,
                           const float* materials, int n_mat, const float* points, long n_points, const float* areas,
                           long n_areas, const float* dirs, long n_dirs, const float* env, int env_w, int env_h,
-                          float env_scale, float env_rotation, float bias) {
+                          float env_scale, float env_rotation, float bias, int light_selection) {
   orc_pt_t* S = (orc_pt_t*)calloc(1, sizeof(orc_pt_t));
   if (!S) return NULL;
   S->env_cos = (float)cos((double)env_rotation);
@@ -968,6 +1105,7 @@ void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, lon
   S->n_areas = n_areas;
   S->dirs = dirs;
   S->n_dirs = n_dirs;
+  double env_tot = 0.0;
   if (env) {
     S->env = env;
     S->env_w = env_w;
@@ -1003,11 +1141,13 @@ void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, lon
     S->env_marg = marg;
     S->env_cond = cond;
     S->env_sampleable = tot > 0.0;
+    env_tot = tot;
     free(rows);
     free(cum);
   }
   S->n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_areas + (int)n_dirs + (S->env_sampleable ? 1 : 0);
   S->bias = bias;
+  if (light_selection == 0 && S->n_entries >= 2) build_light_tree(S, env_tot);
   return S;
 }
 
@@ -1021,6 +1161,7 @@ void orc_pt_scene_free(void* h) {
   free((void*)S->em_cdf);
   free((void*)S->env_marg);
   free((void*)S->env_cond);
+  free(S->lt);
   free(S);
 }
 
@@ -1070,9 +1211,10 @@ int orc_pt_render(const float* pos, long nvert, const uint32_t* idx, long ntri, 
                   int env_w, int env_h, float env_scale, float env_rotation, const float* inv_vp, int width,
                   int height, int spp,
                   int max_bounces, uint32_t seed, uint32_t sample_base, float bias, int nthreads, double* sum,
-                  double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals) {
+                  double* sq, float* log_closest, float* log_shadow, long log_cap, long* ray_totals,
+                  int light_selection) {
   void* h = orc_pt_scene_create(pos, nvert, idx, ntri, tri_mat, materials, n_mat, points, n_points, areas, n_areas,
-                                dirs, n_dirs, env, env_w, env_h, env_scale, env_rotation, bias);
+                                dirs, n_dirs, env, env_w, env_h, env_scale, env_rotation, bias, light_selection);
   if (!h) return -1;
   orc_pt_scene_render(h, inv_vp, width, height, spp, max_bounces, seed, sample_base, nthreads, sum, sq, log_closest,
                       log_shadow, log_cap, ray_totals);

@@ -36,6 +36,12 @@ class BvhInfo(ctypes.Structure):
                 ("binary_depth", ctypes.c_int32), ("build_ms", ctypes.c_double)]
 
 
+class LightTreeEmitter(ctypes.Structure):
+    _fields_ = [("power", ctypes.c_double), ("centroid", ctypes.c_double * 3), ("aabb_min", ctypes.c_double * 3),
+                ("aabb_max", ctypes.c_double * 3), ("cone_axis", ctypes.c_double * 3), ("cone_theta_o", ctypes.c_double),
+                ("cone_theta_e", ctypes.c_double), ("oriented", ctypes.c_int32)]
+
+
 class BvhProof(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("node_count", "root_count", "interior_node_count", "leaf_node_count",
                                                "max_depth", "max_traversal_stack_entries",
@@ -73,6 +79,8 @@ SIGNATURES = {
     "vt_bvh_destroy": [P],
     "vt_tlas_build": [P, SZ, I32, I32, I32, P, SZ, P, SZ, P],
     "vt_validate_bvh_encoding": [P, SZ, SZ, P, SZ, ctypes.c_int64, I32, P],
+    "vt_light_tree_build": [P, SZ, P, SZ, P],
+    "vt_light_tree_select_device": [P, SZ, P, P, SZ, P, P, P],
     "vt_bvh_validate": [P, P],
     "vt_engine_export_tlas": [P, P, SZ, P, SZ, P],
     "vt_bvh_trace_closest_noalloc": [P, P, SZ, P],

@@ -36,7 +36,7 @@ struct vt_batch {
   DeviceBuffer<float4> tris;
   DeviceBuffer<vt::pt::Material> mats;
   DeviceBuffer<float4> emitters, points, dirs, env, areas;
-  DeviceBuffer<float> cdf, marg, cond;
+  DeviceBuffer<float> cdf, marg, cond, ltree;
   DeviceBuffer<vt::pt::BatchScene> scenes;
   std::vector<vt::pt::BatchScene> host;
   unsigned long long total_paths = 0;
@@ -326,8 +326,8 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
     std::vector<float> recs;
     std::vector<vt::pt::Material> mats;
     std::vector<float4> ems, pts, dls, env, arl;
-    std::vector<float> cdf, marg, cond;
-    struct Off { size_t mat, em, cdf, pt, dl, env, marg, cond, arl; };
+    std::vector<float> cdf, marg, cond, ltree;
+    struct Off { size_t mat, em, cdf, pt, dl, env, marg, cond, arl, lt; };
     std::vector<Off> off(count);
     b->host.assign(count, vt::pt::BatchScene{});
     unsigned long long path = 0;
@@ -345,7 +345,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
         if (w[6]) w[5] += rb;
       }
       off[i] = {mats.size(), ems.size(), cdf.size(), pts.size(), dls.size(), env.size(), marg.size(), cond.size(),
-                arl.size()};
+                arl.size(), ltree.size()};
       nodes.insert(nodes.end(), p.node_words.begin(), p.node_words.end());
       recs.insert(recs.end(), p.rec_floats.begin(), p.rec_floats.end());
       mats.insert(mats.end(), p.mats.begin(), p.mats.end());
@@ -357,6 +357,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       env.insert(env.end(), p.env.begin(), p.env.end());
       marg.insert(marg.end(), p.marg.begin(), p.marg.end());
       cond.insert(cond.end(), p.cond.begin(), p.cond.end());
+      ltree.insert(ltree.end(), p.light_tree.begin(), p.light_tree.end());
       vt::pt::BatchScene& B = b->host[i];
       const vt_frame_input& f = frames[i];
       vt::inverse_view_proj(f.view, f.projection, B.inv_vp);
@@ -408,6 +409,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
     upload(b->env, env, s);
     upload(b->marg, marg, s);
     upload(b->cond, cond, s);
+    upload(b->ltree, ltree, s);
     for (size_t i = 0; i < count; ++i) {
       vt::pt::SceneView& v = b->host[i].view;
       const vt::PackedScene& p = packed[i];
@@ -423,6 +425,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       v.env = p.has_env ? b->env.ptr + off[i].env : nullptr;
       v.env_marginal = p.env_sampleable ? b->marg.ptr + off[i].marg : nullptr;
       v.env_conditional = p.env_sampleable ? b->cond.ptr + off[i].cond : nullptr;
+      v.light_tree = p.light_tree.empty() ? nullptr : b->ltree.ptr + off[i].lt;
     }
     upload(b->scenes, b->host, s);
     b->accum.resize(std::max<size_t>(pixels, 1));

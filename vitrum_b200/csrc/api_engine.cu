@@ -88,6 +88,7 @@ struct vt_engine {
   DeviceBuffer<float4> points, dirs, area_lights;
   DeviceBuffer<float4> env;
   DeviceBuffer<float> env_marginal, env_conditional;
+  DeviceBuffer<float> light_tree;  // packed light tree (light_tree.h), empty below two light entries
   vt::pt::SceneView view;
   int64_t ntri = 0, n_emitters = 0;
   // accumulation
@@ -178,7 +179,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
     DeviceBuffer<float4> tris, insts, inst_table, inst_l2w;
     DeviceBuffer<vt::pt::Material> materials;
     DeviceBuffer<float4> emitters, points, area_lights, dirs, env;
-    DeviceBuffer<float> emitter_cdf, env_marginal, env_conditional;
+    DeviceBuffer<float> emitter_cdf, env_marginal, env_conditional, light_tree;
   } n;
   n.nodes.resize(p.node_words.size() / 4);
   VT_CUDA(cudaMemcpyAsync(n.nodes.ptr, p.node_words.data(), p.node_words.size() * 4, cudaMemcpyHostToDevice, s));
@@ -202,6 +203,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   upload(n.env, p.env, s);
   upload(n.env_marginal, p.marg, s);
   upload(n.env_conditional, p.cond, s);
+  upload(n.light_tree, p.light_tree, s);
   VT_CUDA(cudaStreamSynchronize(s));
   // commit
   e->drop_graphs();
@@ -219,6 +221,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   e->env = std::move(n.env);
   e->env_marginal = std::move(n.env_marginal);
   e->env_conditional = std::move(n.env_conditional);
+  e->light_tree = std::move(n.light_tree);
   e->wide_depth = p.depth;
   e->stack_depth = p.stack_depth;
   e->n_instances = (int64_t)p.n_instances;
@@ -250,6 +253,7 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.env_cos = (float)std::cos((double)p.env_rotation);
   v.env_sin = (float)std::sin((double)p.env_rotation);
   v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_area + v.n_dirs + (p.env_sampleable ? 1u : 0u);
+  v.light_tree = (!p.light_tree.empty() && e->opts.light_selection == 0) ? e->light_tree.ptr : nullptr;
   e->view = v;
   e->binary = std::move(p.binary);
   e->blas_root = std::move(p.blas_root);
@@ -890,6 +894,7 @@ vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine*
     if (e->opts.wave_paths < 0) fail(VT_ERR_RANGE, "wave_paths must be >= 0");
     if (e->opts.bvh_max_leaf == 0) e->opts.bvh_max_leaf = vt::kEngineLeafDefault;
     if (e->opts.bvh_max_leaf < 1 || e->opts.bvh_max_leaf > 4) fail(VT_ERR_RANGE, "bvh_max_leaf must be in [0, 4]");
+    if (e->opts.light_selection < 0 || e->opts.light_selection > 1) fail(VT_ERR_RANGE, "light_selection must be 0 or 1");
     vt::DeviceScope ds(device);
     VT_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     VT_CUDA(cudaEventCreate(&e->ev0));

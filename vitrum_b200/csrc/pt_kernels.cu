@@ -26,8 +26,10 @@
 
 #include <cstdint>
 
+#include "light_tree.cuh"
 #include "pt_common.cuh"
 #include "pt_kernels.h"
+#include "vt_common.h"
 
 namespace vt {
 namespace pt {
@@ -89,6 +91,7 @@ struct LightSample {
   float dist;       // distance to the light point (inf for the environment)
   float3 Le;        // emitted radiance (area/env) or intensity / dist^2 (point)
   float pdf;        // solid-angle pdf including the entry selection (delta: selection only)
+  float pdf_light;  // the same without the selection: the density the MIS weights compare
   bool delta;
   bool valid;
 };
@@ -166,8 +169,19 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
   ls.valid = false;
   ls.delta = false;
   const uint32_t n = sc.n_light_entries;
-  const float psel = 1.0f / (float)n;
-  uint32_t e = rand_bounded(rng, n);
+  // entry selection: the light tree (one 24-bit draw, power x proximity x
+  // orientation, lightTree.ts:1237-1319) or uniform; its probability is divided
+  // out of the estimate but kept out of the MIS weights, as the reference does
+  // (pt-webgpu mediumNee.wgsl.ts:14-37, connect.wgsl.ts:598)
+  float psel;
+  uint32_t e;
+  if (sc.light_tree) {
+    psel = lt::select(sc.light_tree, P.x, P.y, P.z, pcg_next(rng) >> 8, e);
+    if (e >= n || !(psel > 0.0f)) return ls;
+  } else {
+    psel = 1.0f / (float)n;
+    e = rand_bounded(rng, n);
+  }
   const bool has_area = sc.n_emitters > 0;
   if (has_area) {
     if (e == 0) {
@@ -189,7 +203,8 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
       const Material m = sc.materials[__float_as_uint(a.w)];
       ls.Le = m.emission;
       ls.dist = dist;
-      ls.pdf = psel * d2 / (sc.emit_area_total * cosl);
+      ls.pdf_light = d2 / (sc.emit_area_total * cosl);
+      ls.pdf = psel * ls.pdf_light;
       ls.valid = true;
       return ls;
     }
@@ -214,6 +229,7 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
     ls.dist = dist;
     ls.Le = f3(I.x, I.y, I.z) * (cone * positional_falloff(dist, d2, ex.y, ex.z));
     ls.pdf = psel;
+    ls.pdf_light = 1.0f;
     ls.delta = true;
     ls.valid = true;
     return ls;
@@ -242,7 +258,8 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
     if (!(cosl > 0.0f)) return ls;
     ls.Le = f3(a3.x, a3.y, a3.z);
     ls.dist = dist;
-    ls.pdf = psel * d2 / (a1.w * cosl);
+    ls.pdf_light = d2 / (a1.w * cosl);
+    ls.pdf = psel * ls.pdf_light;
     ls.valid = true;
     return ls;
   }
@@ -255,6 +272,7 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
     if (dl.w != 0.0f) {  // delta: irradiance along w
       ls.wi = w;
       ls.pdf = psel;
+      ls.pdf_light = 1.0f;
       ls.delta = true;
     } else {  // disc of angular radius acos(dw.w): uniform in the cone
       const float u1 = rand01(rng), u2 = rand01(rng);
@@ -263,7 +281,8 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
       float3 tu, tv;
       onb(w, tu, tv);
       ls.wi = tu * (st * cosf(ph)) + tv * (st * sinf(ph)) + w * ct;
-      ls.pdf = psel / (2.0f * CUDART_PI_F * (1.0f - dw.w));
+      ls.pdf_light = 1.0f / (2.0f * CUDART_PI_F * (1.0f - dw.w));
+      ls.pdf = psel * ls.pdf_light;
     }
     ls.valid = true;
     return ls;
@@ -285,15 +304,27 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
   ls.wi = f3(sc.env_cos * md.x + sc.env_sin * md.z, md.y, -sc.env_sin * md.x + sc.env_cos * md.z);
   ls.dist = CUDART_INF_F;
   ls.Le = env_radiance(sc, (int)col, (int)row);
-  ls.pdf = psel * env_pdf_texel(sc, (int)col, (int)row, st);
+  ls.pdf_light = env_pdf_texel(sc, (int)col, (int)row, st);
+  ls.pdf = psel * ls.pdf_light;
   ls.valid = ls.pdf > 0.0f;
   return ls;
 }
 
-// pdf (solid angle, with selection) of reaching an emissive triangle point by light sampling
+// solid-angle pdf of reaching an emissive triangle point by sampling the
+// emissive-mesh entry (given that entry: the MIS density)
 __device__ __forceinline__ float area_light_pdf(const SceneView& sc, float dist, float cosl) {
   if (!(cosl > 0.0f)) return 0.0f;
-  return (1.0f / (float)sc.n_light_entries) * dist * dist / (sc.emit_area_total * cosl);
+  return dist * dist / (sc.emit_area_total * cosl);
+}
+
+// ---------------------------------------------------------------- light-tree probe
+__global__ void k_light_tree_select(const float* tree, const float* points, const uint32_t* buckets, size_t n,
+                                    uint32_t* entry, float* pmf) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t e = 0xFFFFFFFFu;
+  pmf[i] = lt::select(tree, points[3 * i], points[3 * i + 1], points[3 * i + 2], buckets[i] & (lt::kBuckets - 1u), e);
+  entry[i] = e;
 }
 
 // ---------------------------------------------------------------- raygen
@@ -497,7 +528,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
         float3 Le;
         float pa;
         if (area_light_hit(sc, o, d, h.x < 0 ? CUDART_INF_F : __int_as_float(h.y), Le, pa)) {
-          const float wgt = prev_delta ? 1.0f : power_heuristic(prev_pdf, pa / (float)sc.n_light_entries);
+          const float wgt = prev_delta ? 1.0f : power_heuristic(prev_pdf, pa);
           rad = rad + T * Le * wgt;
         }
       }
@@ -508,7 +539,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
           if (dl.w != 0.0f || dot(d, f3(dw.x, dw.y, dw.z)) < dw.w) continue;
           float wgt = 1.0f;
           if (!prev_delta)
-            wgt = power_heuristic(prev_pdf, 1.0f / ((float)sc.n_light_entries * 2.0f * CUDART_PI_F * (1.0f - dw.w)));
+            wgt = power_heuristic(prev_pdf, 1.0f / (2.0f * CUDART_PI_F * (1.0f - dw.w)));
           rad = rad + T * f3(dl.x, dl.y, dl.z) * wgt;
         }
         if (sc.env) {
@@ -517,7 +548,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
           env_texel(sc, d, col, row, sin_t);
           float wgt = 1.0f;
           if (!prev_delta && sc.env_marginal)
-            wgt = power_heuristic(prev_pdf, env_pdf_texel(sc, col, row, sin_t) / (float)sc.n_light_entries);
+            wgt = power_heuristic(prev_pdf, env_pdf_texel(sc, col, row, sin_t));
           rad = rad + T * env_radiance(sc, col, row) * wgt;
         }
       } else {
@@ -599,7 +630,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
               const float3 wil = to_local(ls.wi, tb, bb, n);
               bsdf_eval(m, os, eta, wol, wil, fc, pb);
               if (maxc(fc) > 0.0f) {
-                const float wgt = (ls.delta || last) ? 1.0f : power_heuristic(ls.pdf, pb);
+                const float wgt = (ls.delta || last) ? 1.0f : power_heuristic(ls.pdf_light, pb);
                 const float3 c = T * fc * ls.Le * (wgt / ls.pdf);
                 if (maxc(c) > 0.0f) {
                   const float3 so = P + n * (wil.z > 0.0f ? off : -off);
@@ -996,3 +1027,17 @@ void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView
 
 }  // namespace pt
 }  // namespace vt
+
+extern "C" vt_status vt_light_tree_select_device(const float* d_tree, size_t node_count, const float* d_points,
+                                                 const uint32_t* d_buckets, size_t n, uint32_t* d_emitter,
+                                                 float* d_pmf, void* cuda_stream) {
+  return vt::guard([&] {
+    if (n && (!d_tree || !d_points || !d_buckets || !d_emitter || !d_pmf))
+      vt::fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (n && node_count == 0) vt::fail(VT_ERR_INVALID_ARGUMENT, "empty tree");
+    if (!n) return;
+    vt::pt::k_light_tree_select<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)cuda_stream>>>(
+        d_tree, d_points, d_buckets, n, d_emitter, d_pmf);
+    VT_CUDA(cudaGetLastError());
+  });
+}

@@ -56,6 +56,8 @@ struct SceneView {
   // light entries, chosen uniformly by NEE: the emissive-mesh group (if any),
   // positional lights, analytic area lights, directional lights, environment (if any)
   uint32_t n_light_entries = 0;
+  // light tree over the light entries (light_tree.h layout) or nullptr: uniform selection
+  const float* light_tree = nullptr;
   // two-level scenes: instance records (4 float4: world-to-local rows, (blas root, id, material, 0))
   const float4* insts = nullptr;       // in top-level leaf order (traversal)
   const float4* inst_table = nullptr;  // by instance index (shading)

@@ -13,6 +13,8 @@
 #include <vector>
 
 #include "scene_pack.h"
+#include "light_tree.h"
+#include "pt_kernels.h"
 
 namespace vt {
 
@@ -449,6 +451,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   std::vector<float> marg, cond;
   const bool has_env = sc->environment_rgb && sc->environment_width > 0 && sc->environment_height > 0;
   bool env_sampleable = false;
+  double env_total = 0.0;  // sum of luminance * intensity * sin(theta) over the texels
   if (has_env) {
     const int W = sc->environment_width, H = sc->environment_height;
     const float scale = sc->environment_intensity > 0.0f ? sc->environment_intensity : 1.0f;
@@ -481,6 +484,104 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     }
     marg[H] = 1.0f;
     env_sampleable = tot > 0.0;
+    env_total = tot;
+  }
+  // light tree over the light entries, in sample_light's order: the emissive-mesh
+  // group, points, spots, rectangles, discs, directionals, the environment
+  // (the reference's buildLightTreeInputForScene, emitterPacking.ts:1005-1232,
+  // with the emissive triangles as one entry sampled by area)
+  {
+    std::vector<lt::Emitter> le;
+    double umn[3] = {INFINITY, INFINITY, INFINITY}, umx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    auto extend = [&](const double* mn, const double* mx) {
+      for (int k = 0; k < 3; ++k) { umn[k] = std::min(umn[k], mn[k]); umx[k] = std::max(umx[k], mx[k]); }
+    };
+    auto lum_f = [](double r, double g, double b) { return (double)(float)(0.2126 * r + 0.7152 * g + 0.0722 * b); };
+    auto unit = [](const double* v, double* o) {
+      const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      for (int k = 0; k < 3; ++k) o[k] = l > 1e-12 ? v[k] / l : 0.0;
+    };
+    if (!em.empty()) {
+      lt::Emitter g;
+      for (int k = 0; k < 3; ++k) { g.mn[k] = INFINITY; g.mx[k] = -INFINITY; }
+      std::vector<lt::Emitter> tris(em.size() / 3);
+      for (size_t k = 0; k < tris.size(); ++k) {
+        const float4 a = em[3 * k], b = em[3 * k + 1], c = em[3 * k + 2];
+        uint32_t mb;
+        std::memcpy(&mb, &a.w, 4);
+        const float3 L = mats[mb].emission;
+        g.power += (double)(float)(lum_f(L.x, L.y, L.z) * (double)b.w);
+        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z}, C[3] = {c.x, c.y, c.z};
+        for (int q = 0; q < 3; ++q) {
+          g.mn[q] = std::min(g.mn[q], std::min(A[q], std::min(B[q], C[q])));
+          g.mx[q] = std::max(g.mx[q], std::max(A[q], std::max(B[q], C[q])));
+        }
+        const double e1[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]}, e2[3] = {C[0] - A[0], C[1] - A[1], C[2] - A[2]};
+        const double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        tris[k].oriented = true;
+        unit(n, tris[k].axis);
+      }
+      for (int k = 0; k < 3; ++k) g.centroid[k] = 0.5 * g.mn[k] + 0.5 * g.mx[k];
+      // one-sided emitters: the group's cone bounds every triangle's outward hemisphere
+      lt::merge_into(g, tris);
+      extend(g.mn, g.mx);
+      le.push_back(g);
+    }
+    for (size_t i = 0; i < pts.size() / pt::kPositionalF4; ++i) {
+      const float4* q = &pts[pt::kPositionalF4 * i];
+      const float4 P = q[0], I = q[1], ax = q[2];
+      lt::Emitter e;
+      e.power = lum_f(I.x, I.y, I.z);
+      const double c[3] = {P.x, P.y, P.z};
+      for (int k = 0; k < 3; ++k) e.centroid[k] = e.mn[k] = e.mx[k] = c[k];
+      if (q[3].w != 0.0f) {  // spot: its beam
+        e.oriented = true;
+        const double a[3] = {ax.x, ax.y, ax.z};
+        unit(a, e.axis);
+        e.theta_o = 0.0;
+        e.theta_e = std::acos(std::max(-1.0, std::min(1.0, (double)ax.w)));
+      }
+      extend(e.mn, e.mx);
+      le.push_back(e);
+    }
+    for (size_t i = 0; i < areas.size() / pt::kAreaLightF4; ++i) {
+      const float4* q = &areas[pt::kAreaLightF4 * i];
+      const float4 c = q[0], u = q[1], v = q[2], L = q[3];
+      lt::Emitter e;
+      e.power = (double)(float)(lum_f(L.x, L.y, L.z) * (double)u.w);
+      const double C[3] = {c.x, c.y, c.z}, U[3] = {u.x, u.y, u.z}, W[3] = {v.x, v.y, v.z};
+      const double r = std::sqrt(U[0] * U[0] + U[1] * U[1] + U[2] * U[2]);
+      for (int k = 0; k < 3; ++k) {
+        const double h = c.w != 0.0f ? r : std::fabs(U[k]) + std::fabs(W[k]);
+        e.centroid[k] = C[k];
+        e.mn[k] = C[k] - h;
+        e.mx[k] = C[k] + h;
+      }
+      const double n[3] = {U[1] * W[2] - U[2] * W[1], U[2] * W[0] - U[0] * W[2], U[0] * W[1] - U[1] * W[0]};
+      e.oriented = true;
+      unit(n, e.axis);
+      extend(e.mn, e.mx);
+      le.push_back(e);
+    }
+    if (!std::isfinite(umn[0])) for (int k = 0; k < 3; ++k) umn[k] = umx[k] = 0.0;
+    auto distant = [&](double power) {
+      lt::Emitter e;
+      e.power = power;
+      for (int k = 0; k < 3; ++k) {
+        e.mn[k] = umn[k];
+        e.mx[k] = umx[k];
+        e.centroid[k] = (umn[k] + umx[k]) / 2;
+      }
+      le.push_back(e);
+    };
+    for (size_t i = 0; i < dirs.size() / 2; ++i) {
+      const float4 w4 = dirs[2 * i], L = dirs[2 * i + 1];
+      const double c = w4.w;
+      distant(lum_f(L.x, L.y, L.z) * (L.w != 0.0f ? 1.0 : M_PI * (1.0 - c * c)));
+    }
+    if (env_sampleable)
+      distant((double)(float)(env_total * (2.0 * M_PI * M_PI / ((double)sc->environment_width * sc->environment_height))));
+    if (le.size() >= 2) p.light_tree = lt::build_packed(le);
   }
   if (two_level && (node_base || rec_base)) fail(VT_ERR_INVALID_ARGUMENT, "instanced scenes cannot be offset");
   p.two_level = two_level;

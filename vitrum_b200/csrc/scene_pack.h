@@ -36,6 +36,7 @@ struct PackedScene {
   int env_w = 0, env_h = 0;
   float env_scale = 1.0f;
   float env_rotation = 0.0f;
+  std::vector<float> light_tree;     // packed light tree over the light entries (two or more entries)
   size_t ntri = 0;
   // two-level: per mesh its bottom-level root node and local bounds; the deepest bottom level
   std::vector<uint32_t> blas_root;

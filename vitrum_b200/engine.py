@@ -26,7 +26,7 @@ class _EngineOptions(ctypes.Structure):
     _fields_ = [("max_bounces", ctypes.c_int32), ("max_samples_per_pixel", ctypes.c_int32),
                 ("debug", ctypes.c_int32), ("oracle_accumulation", ctypes.c_int32),
                 ("sort_by_material", ctypes.c_int32), ("wave_paths", ctypes.c_int32),
-                ("bvh_max_leaf", ctypes.c_int32)]
+                ("bvh_max_leaf", ctypes.c_int32), ("light_selection", ctypes.c_int32)]
 
 
 class _MaterialDesc(ctypes.Structure):
@@ -392,9 +392,10 @@ class Engine:
 
     def __init__(self, device: int = 0, max_bounces: int = 8, max_samples_per_pixel: int = 4096,
                  debug: bool = False, oracle_accumulation: bool = False, sort_by_material: bool = False,
-                 wave_paths: int = 0, bvh_max_leaf: int = 0):
+                 wave_paths: int = 0, bvh_max_leaf: int = 0, light_selection: str = "tree"):
         opts = _EngineOptions(max_bounces, max_samples_per_pixel, 1 if debug else 0, 1 if oracle_accumulation else 0,
-                              1 if sort_by_material else 0, wave_paths, bvh_max_leaf)
+                              1 if sort_by_material else 0, wave_paths, bvh_max_leaf,
+                              {"tree": 0, "uniform": 1}[light_selection])
         h = ctypes.c_void_p()
         N.call("vt_create", device, ctypes.byref(opts), ctypes.byref(h))
         self._h = h
