@@ -392,7 +392,8 @@ def run_batch(args, dev, local, barrier):
     t0 = time.perf_counter()
     b = Batch(items, device=local)
     build_s = time.perf_counter() - t0
-    b.set_tuning(tuned["wave_paths"], bool(tuned["sort_by_material"]), tuned["trace_blocks_per_sm"])
+    b.set_tuning(tuned["wave_paths"], bool(tuned["sort_by_material"]), tuned["trace_blocks_per_sm"],
+                 sort_rays=bool(tuned["sort_rays"]))
     b.render()  # warm-up (graph capture)
     steps = max(1, min(args.steps, 3))
     ms, rays = 0.0, 0
@@ -432,10 +433,95 @@ def run_batch(args, dev, local, barrier):
 
 # ------------------------------------------------------------------ radiance cache workload
 NRC_W, NRC_H, NRC_SPP, NRC_WARM, NRC_FRAMES = 480, 270, 16, 32, 8
+# RNG keys are frame seed ^ sample index: the oracle's keys [2^20, 2^20 + 2^16)
+# share none with the curves' frames (seed 7, small sample indices)
+ORACLE_SEED = (1 << 20) | 4242
 
 
 def _relmse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+_CLOUD_ORACLE = {}
+
+
+def _cloud_oracle(args, local):
+    """The 1024-instance cloud at NRC_W x NRC_H, 8 bounces, args.oracle_spp
+    samples accumulated in FP64 (rendered once per run): (mean, per-sample
+    variance, seconds)."""
+    if "ref" not in _CLOUD_ORACLE:
+        from vitrum_b200 import scenes
+        from vitrum_b200.engine import Engine
+        sc, cam = scenes.instanced_cloud()
+        t0 = time.perf_counter()
+        o = Engine(device=local, max_bounces=I_BOUNCES, oracle_accumulation=True, max_samples_per_pixel=1 << 20)
+        o.set_scene(sc)
+        done = 0
+        while done < args.oracle_spp:
+            k = min(2048, args.oracle_spp - done)
+            o.render_frame(cam, NRC_W, NRC_H, samples=k, frame_seed=ORACLE_SEED)
+            done += k
+        ref, var = o.capture_moments()
+        o.dispose()
+        _CLOUD_ORACLE["ref"] = (ref, var, time.perf_counter() - t0)
+    return _CLOUD_ORACLE["ref"]
+
+
+LT_SPP, LT_SEEDS = 64, 5
+
+
+def run_light_tree(args, dev, local, barrier):
+    """Next-event light selection on the 1024-instance cloud with 32 point
+    lights: the light tree (power x proximity x orientation x receiver
+    cosine bound, half the buckets spread evenly) against uniform selection.
+    Per selection: the device time of a 1920x1080 x 16 spp frame and of a
+    480x270 x 64 spp frame, and the relMSE of the latter against the FP64
+    oracle over LT_SEEDS seeds (median; also with the 0.1 % worst pixels
+    dropped, the error being heavy-tailed through the metal and glass
+    instances).  Equal time: relMSE x frame time, lower is better."""
+    from vitrum_b200 import scenes
+    from vitrum_b200.engine import Engine
+    sc, cam = scenes.instanced_cloud()
+    ref, _, _ = _cloud_oracle(args, local)
+
+    def trimmed(img):
+        e = np.sort(((img - ref) ** 2 / (ref ** 2 + 1e-2)).ravel())
+        return float(e[:int(e.size * 0.999)].mean())
+
+    out = {}
+    for sel in ("uniform", "tree"):
+        e = Engine(device=local, max_bounces=I_BOUNCES, max_samples_per_pixel=1 << 20, light_selection=sel)
+        e.set_scene(sc)
+        for i in range(2):
+            e.render_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=900 + i)
+        full = []
+        for i in range(3):
+            e.render_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=910 + i)
+            full.append(e.stats()["last_frame_ms"])
+        e.reset()
+        e.render_frame(cam, NRC_W, NRC_H, samples=LT_SPP, frame_seed=920)  # warm the small frame's graph
+        small, rel, rel_t = [], [], []
+        for k in range(1, LT_SEEDS + 1):
+            e.reset()
+            e.render_frame(cam, NRC_W, NRC_H, samples=LT_SPP, frame_seed=k << 16)
+            small.append(e.stats()["last_frame_ms"])
+            img = e.capture_frame()[..., :3].astype(np.float64)
+            rel.append(_relmse(img, ref))
+            rel_t.append(trimmed(img))
+        e.dispose()
+        out[sel] = {"frame_ms_1920x1080_16spp": round(float(np.median(full)), 3),
+                    "frame_ms_480x270_64spp": round(float(np.median(small)), 3),
+                    "relmse": round(float(np.median(rel)), 6), "relmse_trimmed": round(float(np.median(rel_t)), 6),
+                    "relmse_per_seed": [round(r, 6) for r in rel]}
+    u, t = out["uniform"], out["tree"]
+    cost = t["frame_ms_480x270_64spp"] / u["frame_ms_480x270_64spp"]
+    out["tree_cost_per_sample"] = round(cost, 3)
+    out["equal_time_gain"] = round(u["relmse"] / (t["relmse"] * cost), 3)
+    out["equal_time_gain_trimmed"] = round(u["relmse_trimmed"] / (t["relmse_trimmed"] * cost), 3)
+    out["workload"] = ("1024-instance cloud, 32 point lights + gradient sky, 8 bounces; relMSE at 480x270 x %d spp "
+                       "vs the %d-spp FP64 oracle, %d seeds (median)" % (LT_SPP, args.oracle_spp, LT_SEEDS))
+    out["metric"] = "equal_time_gain = (relMSE x frame ms) uniform / tree; > 1: the tree wins"
+    return out
 
 
 def run_nrc(args, dev, local, barrier):
@@ -449,17 +535,7 @@ def run_nrc(args, dev, local, barrier):
     from vitrum_b200.engine import Engine
     sc, cam = scenes.instanced_cloud()
     B = I_BOUNCES
-    t0 = time.perf_counter()
-    o = Engine(device=local, max_bounces=B, oracle_accumulation=True, max_samples_per_pixel=1 << 20)
-    o.set_scene(sc)
-    done = 0
-    while done < args.oracle_spp:
-        k = min(2048, args.oracle_spp - done)
-        o.render_frame(cam, NRC_W, NRC_H, samples=k, frame_seed=4242)
-        done += k
-    ref, _ = o.capture_moments()
-    o.dispose()
-    oracle_s = time.perf_counter() - t0
+    ref, _, oracle_s = _cloud_oracle(args, local)
 
     def curve(nrc):
         e = Engine(device=local, max_bounces=B, max_samples_per_pixel=1 << 20)
@@ -576,6 +652,7 @@ def run_ours(args, rank, world, local):
     query = run_query(args, dev, local, rank, world, barrier) if solo and not args.no_query else None
     instanced = run_instanced(args, dev, local, barrier) if solo and not args.no_instanced else None
     nrc = run_nrc(args, dev, local, barrier) if solo and not args.no_nrc else None
+    light_tree = run_light_tree(args, dev, local, barrier) if solo and not args.no_light_tree else None
     batch = run_batch(args, dev, local, barrier) if solo and not args.no_batch else None
 
     if rank == 0:
@@ -625,6 +702,7 @@ def run_ours(args, rank, world, local):
             "query": query,
             "instanced": instanced,
             "nrc": nrc,
+            "light_tree": light_tree,
             "batch": batch,
         }
         print(json.dumps(line), flush=True)
@@ -643,6 +721,7 @@ def main():
     ap.add_argument("--no-instanced", action="store_true")
     ap.add_argument("--no-nrc", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-light-tree", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--oracle-spp", type=int, default=65536)
     args = ap.parse_args()

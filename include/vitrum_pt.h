@@ -192,14 +192,23 @@ vt_status vt_light_tree_build(const vt_light_tree_emitter* emitters, size_t n, f
                               size_t* node_count);
 
 /*
- * The device selection the path tracer's next-event estimation uses
- * (samplePackedLightTreeCPU, lightTree.ts:1237): for each point (3 floats) and
- * 24-bit draw, the selected emitter and its probability (bucket count / 2^24).
- * DEVICE pointers; enqueued on cuda_stream.
+ * The device selection the path tracer's next-event estimation uses: for each
+ * point (3 floats) and 24-bit draw, the selected entry and its probability
+ * (bucket count / 2^24).  Entries 0 .. P-1 are the tree's leaves (P = (node_count
+ * + 1) / 2, selected by samplePackedLightTreeCPU's descent, lightTree.ts:1237);
+ * entries P .. P + n_distant - 1 are distant lights (directionals, an
+ * environment), which take n_distant / (n_distant + 1) of the buckets (all of
+ * them without a tree) shared evenly.  d_normals (3 floats per point, or null
+ * for none) are unit receiver normals: the descent's importance is multiplied
+ * by cos(max(0, theta_i - theta_u)) of each child seen from the point (Conty
+ * Estevez & Kulla 2018), which the reference's importance leaves out; a zero
+ * normal (transmissive surface) keeps the reference's importance.  Half of the
+ * tree's buckets are split evenly over its leaves (the reference keeps one per
+ * leaf).  DEVICE pointers; enqueued on cuda_stream.
  */
-vt_status vt_light_tree_select_device(const float* d_tree, size_t node_count, const float* d_points,
-                                      const uint32_t* d_buckets, size_t n, uint32_t* d_emitter, float* d_pmf,
-                                      void* cuda_stream);
+vt_status vt_light_tree_select_device(const float* d_tree, size_t node_count, uint32_t n_distant,
+                                      const float* d_points, const float* d_normals, const uint32_t* d_buckets,
+                                      size_t n, uint32_t* d_emitter, float* d_pmf, void* cuda_stream);
 
 /*
  * Top-level build over instance world AABBs (replaces buildTlas,
@@ -251,9 +260,10 @@ typedef struct vt_engine_options {
                                      about 4.7 GB), halved down to 2^20 until it fits half the free memory */
   int32_t bvh_max_leaf;           /* triangles per leaf of the engine's own trees, 1..4; 0 = 2 (the reference's
                                      builder with 2 instead of its default 4: the same hits, faster traversal) */
-  int32_t light_selection;        /* next-event light selection: 0 = the light tree when the scene has two or more
-                                     light entries (the reference's full tier: power x proximity x orientation,
-                                     shared-samplers/src/lightTree.ts), 1 = uniform over the entries */
+  int32_t light_selection;        /* next-event light selection: 0 = with two or more light entries, the light tree
+                                     (shared-samplers/src/lightTree.ts: power x proximity x orientation) over the
+                                     positional entries and the distant ones (directionals, environment) sharing
+                                     n / (n + 1) of the selection evenly; 1 = uniform over the entries */
 } vt_engine_options;
 
 /* Material (core MaterialSpec subset, core/src/scene/material.ts), the
@@ -730,6 +740,8 @@ typedef struct vt_tuning {
                                  children, grandchildren) into shared memory with one bulk copy;
                                  0: every node read goes through L1/L2.  A batch takes 0 only
                                  (its launches carry one root per ray). */
+  int32_t sort_rays;          /* 1: from bounce 1 on, each closest-hit queue is traced in direction-octant
+                                 order (a counting sort by the signs of the direction); 0: queue order */
 } vt_tuning;
 
 vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_batch** out);

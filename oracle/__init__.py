@@ -647,6 +647,9 @@ def _lt_lib():
         L.orc_lt_build.argtypes = [P, P, P, P, ctypes.c_long, P, ctypes.c_long]
         L.orc_lt_sample.restype = ctypes.c_float
         L.orc_lt_sample.argtypes = [P, ctypes.c_long, P, ctypes.c_float, ctypes.c_uint32, P]
+        L.orc_lt_select.restype = ctypes.c_float
+        L.orc_lt_select.argtypes = [P, ctypes.c_long, ctypes.c_uint32, ctypes.c_uint32, P, P, ctypes.c_float,
+                                    ctypes.c_uint32, P]
         L.orc_lt_pdf.restype = ctypes.c_float
         L.orc_lt_pdf.argtypes = [P, ctypes.c_long, P, ctypes.c_float, ctypes.c_int]
         L.orc_lt_importance.restype = ctypes.c_float
@@ -692,3 +695,15 @@ def light_tree_pdf(tree, p, emitter, floor=LT_FLOOR):
 def light_tree_importance(tree, node, p, floor=LT_FLOOR):
     t = np.ascontiguousarray(tree, np.float32)
     return float(_lt_lib().orc_lt_importance(_p(t), int(node), _p(_f32(p)), floor))
+
+
+def light_select(tree, n_pos, n_dist, p, bucket, normal=None, floor=LT_FLOOR):
+    """The integrator's selection: tree over n_pos positional entries (tree None
+    for one), n_dist distant entries evenly within n_dist / (n_dist + 1), the
+    receiver term for `normal` (None: none): (entry, pmf)."""
+    t = np.zeros((0, 16), np.float32) if tree is None else np.ascontiguousarray(tree, np.float32)
+    e = ctypes.c_int(-1)
+    nrm = None if normal is None else _p(_f32(normal))
+    pmf = _lt_lib().orc_lt_select(_p(t) if t.size else None, t.shape[0], int(n_pos), int(n_dist), _p(_f32(p)), nrm,
+                                  floor, int(bucket), ctypes.byref(e))
+    return e.value, float(pmf)

@@ -13,6 +13,8 @@
  *   packedNodeImportanceUnchecked (every stage rounded to f32)         :938-1151
  *   allocateLeftBuckets / samplePackedLightTreeCPU /
  *   packedLightTreePdfCPU (24-bit bucket descent, exact PMF)           :1177-1408
+ * (orc_lt_sample / orc_lt_pdf exactly so; orc_lt_select, the integrator's
+ * selection, reserves more buckets per leaf and keeps distant lights outside).
  * The JS Math.fround(Math.log2(x)) and 2 ** x stages are (float)log2((double)x)
  * and (float)exp2((double)x) here.
  */
@@ -291,6 +293,60 @@ static float lt_cone_factor(const float* n, float px, float py, float pz) {
   return fmaxf(F32_MIN_NORMAL, fminf(1.0f, (ca - n[14]) / span));
 }
 
+/*
+ * Receiver term of the integrator's selection (Conty Estevez & Kulla 2018's
+ * bound on the shading point's cosine): cos(max(0, theta_i - theta_u)) of
+ * the node seen from p above the plane of the unit normal nrm, theta_u the
+ * node's angular radius; 0 when the node lies wholly below that plane, 1 for
+ * nrm == 0 (transmissive surfaces) or p inside the node's bounding sphere.
+ */
+static float lt_receiver_factor(const float* n, const float* p, const float* nrm) {
+  if (!nrm || (nrm[0] == 0.0f && nrm[1] == 0.0f && nrm[2] == 0.0f)) return 1.0f;
+  const float *mn = n + 4, *mx = n + 7;
+  float dvx = (0.25f * mn[0] + 0.25f * mx[0]) - 0.5f * p[0];
+  float dvy = (0.25f * mn[1] + 0.25f * mx[1]) - 0.5f * p[1];
+  float dvz = (0.25f * mn[2] + 0.25f * mx[2]) - 0.5f * p[2];
+  float rx = 0.25f * mx[0] - 0.25f * mn[0], ry = 0.25f * mx[1] - 0.25f * mn[1], rz = 0.25f * mx[2] - 0.25f * mn[2];
+  float ds = fmax3a(dvx, dvy, dvz);
+  if (!(ds >= F32_MIN_NORMAL) || ds > F32_MAX) return 1.0f;
+  float sdx = dvx / ds, sdy = dvy / ds, sdz = dvz / ds;
+  float sdl = sqrtf(fdot(sdx, sdy, sdz, sdx, sdy, sdz));
+  float rs = fmax3a(rx, ry, rz), rod = 0.0f;
+  if (rs >= F32_MIN_NORMAL) {
+    float srx = rx / rs, sry = ry / rs, srz = rz / rs;
+    float srl = sqrtf(fdot(srx, sry, srz, srx, sry, srz));
+    float lr = ((flog2(rs) + flog2(srl)) - flog2(ds)) - flog2(sdl);
+    if (lr >= 0.0f) return 1.0f;
+    rod = fexp2(fmaxf(lr, -126.0f));
+  }
+  float dx = sdx / sdl, dy = sdy / sdl, dz = sdz / sdl;
+  float ct = fmaxf(-1.0f, fminf(1.0f, fdot(nrm[0], nrm[1], nrm[2], dx, dy, dz)));
+  float stu = fmaxf(0.0f, fminf(1.0f, rod));
+  float ctu = sqrtf(fmaxf(0.0f, 1.0f - stu * stu));
+  float ca = 1.0f;
+  if (ct < ctu) {
+    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    float a = ct * ctu, b = st * stu;
+    ca = fmaxf(-1.0f, fminf(1.0f, a + b));
+  }
+  return ca > 0.0f ? ca : 0.0f;
+}
+
+static float lt_importance_n(const float* tree, long idx, const float* p, const float* nrm, float floor_d2) {
+  const float* n = tree + LT_FLOATS * idx;
+  float power = n[1];
+  if (!(power > 0.0f)) return 0.0f;
+  float d2 = fmaxf(fmaxf(lt_dist2(p[0], p[1], p[2], n + 4), floor_d2), F32_MIN_NORMAL);
+  float cone = lt_cone_factor(n, p[0], p[1], p[2]);
+  if (!(cone > 0.0f)) return 0.0f;
+  float recv = lt_receiver_factor(n, p, nrm);
+  if (!(recv > 0.0f)) return 0.0f;
+  float li = (flog2(power) - flog2(d2)) + flog2(fmaxf(cone * recv, F32_MIN_NORMAL));
+  if (li >= 127.99999f) return F32_MAX;
+  if (li <= -126.0f) return F32_MIN_NORMAL;
+  return fmaxf(F32_MIN_NORMAL, fminf(F32_MAX, fexp2(li)));
+}
+
 float orc_lt_importance(const float* tree, long idx, const float* p, float floor_d2) {
   const float* n = tree + LT_FLOATS * idx;
   float power = n[1];
@@ -304,7 +360,9 @@ float orc_lt_importance(const float* tree, long idx, const float* p, float floor
   return fmaxf(F32_MIN_NORMAL, fminf(F32_MAX, fexp2(li)));
 }
 
-static uint32_t lt_left_buckets(uint32_t cur, uint32_t ll, uint32_t rl, float a, float b) {
+static uint32_t lt_left_buckets(uint32_t cur, uint32_t ll, uint32_t rl, float a, float b, uint32_t reserve) {
+  ll *= reserve;
+  rl *= reserve;
   uint32_t remaining = cur - (ll + rl);
   float pl = 0.5f;
   if (!(a == 0.0f && b == 0.0f)) {
@@ -317,12 +375,10 @@ static uint32_t lt_left_buckets(uint32_t cur, uint32_t ll, uint32_t rl, float a,
   return ll + (e > remaining ? remaining : e);
 }
 
-/* Entry for point p from the 24-bit draw `bucket`; returns its PMF (0: none). */
-float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d2, uint32_t bucket, int* emitter) {
-  *emitter = -1;
-  if (nodes <= 0) return 0.0f;
+static float lt_descend(const float* tree, long nodes, const float* p, const float* nrm, float floor_d2, uint32_t cur,
+                        uint32_t bucket, uint32_t reserve, int* emitter) {
   long node = 0;
-  uint32_t cur = LT_BUCKETS;
+  *emitter = -1;
   for (long guard = 0; guard <= nodes; ++guard) {
     const float* n = tree + LT_FLOATS * node;
     if (n[2] < 0.0f) {
@@ -331,11 +387,46 @@ float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d
     }
     long l = (long)n[2], r = (long)n[3];
     uint32_t lb = lt_left_buckets(cur, (uint32_t)tree[LT_FLOATS * l + 15], (uint32_t)tree[LT_FLOATS * r + 15],
-                                  orc_lt_importance(tree, l, p, floor_d2), orc_lt_importance(tree, r, p, floor_d2));
+                                  lt_importance_n(tree, l, p, nrm, floor_d2), lt_importance_n(tree, r, p, nrm, floor_d2),
+                                  reserve);
     if (bucket < lb) { cur = lb; node = l; }
     else { bucket -= lb; cur -= lb; node = r; }
   }
   return 0.0f;
+}
+
+/* Entry for point p from the 24-bit draw `bucket`; returns its PMF (0: none). */
+float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d2, uint32_t bucket, int* emitter) {
+  *emitter = -1;
+  if (nodes <= 0) return 0.0f;
+  return lt_descend(tree, nodes, p, NULL, floor_d2, LT_BUCKETS, bucket, 1u, emitter);
+}
+
+/*
+ * The integrator's selection: entries 0 .. n_pos-1 by the tree over the
+ * positional entries (tree NULL: a single one), entries n_pos .. n_pos+n_dist-1
+ * (distant lights) evenly within n_dist / (n_dist + 1) of the 2^24 buckets.
+ * In the tree's descent every leaf keeps a defensive reserve of half the
+ * tree's buckets split evenly (the reference keeps one bucket per leaf); the
+ * other half follows the importance, times the receiver term for the unit
+ * normal nrm (NULL or zero: none).
+ */
+float orc_lt_select(const float* tree, long nodes, uint32_t n_pos, uint32_t n_dist, const float* p, const float* nrm,
+                    float floor_d2, uint32_t bucket, int* emitter) {
+  uint32_t D = n_dist == 0 ? 0u : (n_pos == 0 ? LT_BUCKETS : (uint32_t)(((uint64_t)LT_BUCKETS * n_dist) / (n_dist + 1u)));
+  *emitter = -1;
+  if (bucket < D) {
+    uint32_t j = (uint32_t)(((uint64_t)bucket * n_dist) / D);
+    uint64_t lo = ((uint64_t)j * D + n_dist - 1u) / n_dist, hi = ((uint64_t)(j + 1u) * D + n_dist - 1u) / n_dist;
+    *emitter = (int)(n_pos + j);
+    return (float)(hi - lo) / (float)LT_BUCKETS;
+  }
+  if (n_pos == 0) return 0.0f;
+  if (!tree || nodes <= 1) { *emitter = 0; return (float)(LT_BUCKETS - D) / (float)LT_BUCKETS; }
+  /* defensive half: each leaf keeps (buckets / 2) / leaves of the tree's buckets */
+  uint32_t reserve = (LT_BUCKETS - D) / (2u * (uint32_t)tree[15]);
+  if (reserve < 1u) reserve = 1u;
+  return lt_descend(tree, nodes, p, nrm, floor_d2, LT_BUCKETS - D, bucket - D, reserve, emitter);
 }
 
 /* PMF of one emitter at point p (the deterministic inverse of orc_lt_sample). */
@@ -355,7 +446,8 @@ float orc_lt_pdf(const float* tree, long nodes, const float* p, float floor_d2, 
       if (n[2] < 0.0f) { out = n[0] == (float)emitter ? (float)cur / (float)LT_BUCKETS : 0.0f; break; }
       long l = (long)n[2], r = (long)n[3];
       uint32_t lb = lt_left_buckets(cur, (uint32_t)tree[LT_FLOATS * l + 15], (uint32_t)tree[LT_FLOATS * r + 15],
-                                    orc_lt_importance(tree, l, p, floor_d2), orc_lt_importance(tree, r, p, floor_d2));
+                                    orc_lt_importance(tree, l, p, floor_d2), orc_lt_importance(tree, r, p, floor_d2),
+                                    1u);
       if (contains[l]) { cur = lb; node = l; }
       else { cur -= lb; node = r; }
     }

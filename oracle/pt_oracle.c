@@ -37,7 +37,8 @@ int orc_hw_threads(void);
 long orc_lt_build(const double* power, const double* centroid, const double* aabb, const double* cone, long n,
                   float* out, long cap);
 void orc_lt_merge_cones(const double* cones, long n, double* out6);
-float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d2, uint32_t bucket, int* emitter);
+float orc_lt_select(const float* tree, long nodes, uint32_t n_pos, uint32_t n_dist, const float* p, const float* nrm,
+                    float floor_d2, uint32_t bucket, int* emitter);
 
 #define PI_F 3.14159265358979323846f
 
@@ -132,7 +133,8 @@ typedef struct {
   float env_scale;
   float env_cos, env_sin; /* environment rotation about +y */
   int n_entries;
-  float* lt;              /* light tree over the entries (16 floats per node) or NULL: uniform selection */
+  int lt_mode;            /* 1: tree selection (light tree over the positional entries, distant ones outside) */
+  float* lt;              /* the tree (16 floats per node), NULL below two positional entries */
   long lt_nodes;
   float bias;
   /* camera / frame */
@@ -595,7 +597,8 @@ static int area_light_hit(const orc_pt_t* S, v3 o, v3 d, float t_max, v3* Le, fl
   return found;
 }
 
-static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
+/* N: the unit normal on the incoming side for surfaces that reflect only, else zero */
+static lsample_t sample_light(const orc_pt_t* S, v3 P, v3 N, uint32_t* rng) {
   lsample_t ls;
   memset(&ls, 0, sizeof ls);
   /* entry selection: the light tree (one 24-bit draw) or uniform; the
@@ -603,10 +606,13 @@ static lsample_t sample_light(const orc_pt_t* S, v3 P, uint32_t* rng) {
    * weights (pt-webgpu mediumNee.wgsl.ts:14-37, connect.wgsl.ts:598) */
   float psel;
   uint32_t e;
-  if (S->lt) {
+  if (S->lt_mode) {
     float p3[3] = {P.x, P.y, P.z};
     int em = -1;
-    psel = orc_lt_sample(S->lt, S->lt_nodes, p3, 1e-3f, pcg_next(rng) >> 8, &em);
+    uint32_t n_dist = (uint32_t)S->n_dirs + (S->env_sampleable ? 1u : 0u);
+    float n3[3] = {N.x, N.y, N.z};
+    psel = orc_lt_select(S->lt, S->lt_nodes, (uint32_t)S->n_entries - n_dist, n_dist, p3, n3, 1e-3f,
+                         pcg_next(rng) >> 8, &em);
     if (em < 0 || em >= S->n_entries || !(psel > 0.0f)) return ls;
     e = (uint32_t)em;
   } else {
@@ -802,7 +808,7 @@ static v3 radiance_sample(orc_pt_t* S, int x, int y, uint32_t sample) {
     int alive = 0;
     float eta = front ? m->ior : 1.0f / m->ior;
     if (S->n_entries > 0 && has_finite_support(m)) {
-      lsample_t ls = sample_light(S, P, &rng);
+      lsample_t ls = sample_light(S, P, m->kind == 2 && m->transmission > 0.0f ? V(0, 0, 0) : n, &rng);
       if (ls.valid) {
         v3 wil = V(dot3(ls.wi, tb), dot3(ls.wi, bb), dot3(ls.wi, n)), fc;
         float pb;
@@ -937,27 +943,26 @@ void orc_bsdf_sample_batch(const float* mat12, float eta, const float* wo, long 
 }
 
 /*
- * The light tree over the light entries in sample_light's order: the
- * emissive-mesh group (one entry: power = sum of luminance x area, union AABB,
- * the triangles' one-sided cones merged), points, spots (cone along the beam,
- * half angle acos(cos outer)), rectangles and discs (one-sided cones), then the
- * directionals and the environment with the union AABB of the positional
- * lights (the reference's buildLightTreeInputForScene,
- * pt-webgpu/src/scene/emitterPacking.ts:1005-1232).
+ * The light tree over the positional light entries in sample_light's order:
+ * the emissive-mesh group (one entry: power = sum of luminance x area, union
+ * AABB, the triangles' one-sided cones merged), points, spots (cone along the
+ * beam, half angle acos(cos outer)), rectangles and discs (one-sided cones)
+ * (the reference's buildLightTreeInputForScene,
+ * pt-webgpu/src/scene/emitterPacking.ts:1005-1232).  The distant entries
+ * (directionals, the environment) are chosen outside the tree (orc_lt_select).
  */
 static double lum_f(double r, double g, double b) { return (double)(float)(0.2126 * r + 0.7152 * g + 0.0722 * b); }
 static void unit3(const double* v, double* o) {
   double l = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   for (int k = 0; k < 3; ++k) o[k] = l > 1e-12 ? v[k] / l : 0.0;
 }
-static void build_light_tree(orc_pt_t* S, double env_tot) {
-  long n = S->n_entries, k = 0;
+static void build_light_tree(orc_pt_t* S) {
+  long n = (long)(S->n_em > 0 ? 1 : 0) + S->n_points + S->n_areas, k = 0;
+  if (n < 2) return;
   double* pw = (double*)calloc((size_t)n, sizeof(double));
   double* cen = (double*)calloc((size_t)(3 * n), sizeof(double));
   double* box = (double*)calloc((size_t)(6 * n), sizeof(double));
   double* cone = (double*)calloc((size_t)(6 * n), sizeof(double));
-  double umn[3] = {INFINITY, INFINITY, INFINITY}, umx[3] = {-INFINITY, -INFINITY, -INFINITY};
-#define EXTEND(i) for (int q_ = 0; q_ < 3; ++q_) { umn[q_] = fmin(umn[q_], box[6 * (i) + q_]); umx[q_] = fmax(umx[q_], box[6 * (i) + 3 + q_]); }
   if (S->n_em > 0) {
     double* tc = (double*)calloc((size_t)(6 * S->n_em), sizeof(double));
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, p = 0.0;
@@ -987,7 +992,6 @@ static void build_light_tree(orc_pt_t* S, double env_tot) {
     }
     orc_lt_merge_cones(tc, S->n_em, cone + 6 * k);
     free(tc);
-    EXTEND(k);
     ++k;
   }
   for (long i = 0; i < S->n_points; ++i, ++k) {
@@ -1001,7 +1005,6 @@ static void build_light_tree(orc_pt_t* S, double env_tot) {
       cone[6 * k + 4] = acos(fmax(-1.0, fmin(1.0, (double)q[11])));
       cone[6 * k + 5] = 1.0;
     }
-    EXTEND(k);
   }
   for (long i = 0; i < S->n_areas; ++i, ++k) {
     const float* q = S->areas + 16 * i;
@@ -1019,24 +1022,6 @@ static void build_light_tree(orc_pt_t* S, double env_tot) {
     cone[6 * k + 3] = 0.0;
     cone[6 * k + 4] = M_PI / 2;
     cone[6 * k + 5] = 1.0;
-    EXTEND(k);
-  }
-#undef EXTEND
-  if (!isfinite(umn[0])) for (int q = 0; q < 3; ++q) umn[q] = umx[q] = 0.0;
-  long distant = S->n_dirs + (S->env_sampleable ? 1 : 0);
-  for (long i = 0; i < distant; ++i, ++k) {
-    if (i < S->n_dirs) {
-      const float* q = S->dirs + 8 * i;
-      double c = q[3];
-      pw[k] = lum_f(q[4], q[5], q[6]) * (q[7] != 0.0f ? 1.0 : M_PI * (1.0 - c * c));
-    } else {
-      pw[k] = (double)(float)(env_tot * (2.0 * M_PI * M_PI / ((double)S->env_w * S->env_h)));
-    }
-    for (int q = 0; q < 3; ++q) {
-      box[6 * k + q] = umn[q];
-      box[6 * k + 3 + q] = umx[q];
-      cen[3 * k + q] = (umn[q] + umx[q]) / 2;
-    }
   }
   S->lt = (float*)calloc((size_t)(16 * (2 * n)), sizeof(float));
   S->lt_nodes = orc_lt_build(pw, cen, box, cone, n, S->lt, 2 * n);
@@ -1105,7 +1090,6 @@ void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, lon
   S->n_areas = n_areas;
   S->dirs = dirs;
   S->n_dirs = n_dirs;
-  double env_tot = 0.0;
   if (env) {
     S->env = env;
     S->env_w = env_w;
@@ -1141,13 +1125,15 @@ void* orc_pt_scene_create(const float* pos, long nvert, const uint32_t* idx, lon
     S->env_marg = marg;
     S->env_cond = cond;
     S->env_sampleable = tot > 0.0;
-    env_tot = tot;
     free(rows);
     free(cum);
   }
   S->n_entries = (ne ? 1 : 0) + (int)n_points + (int)n_areas + (int)n_dirs + (S->env_sampleable ? 1 : 0);
   S->bias = bias;
-  if (light_selection == 0 && S->n_entries >= 2) build_light_tree(S, env_tot);
+  if (light_selection == 0 && S->n_entries >= 2) {
+    S->lt_mode = 1;
+    build_light_tree(S);
+  }
   return S;
 }
 

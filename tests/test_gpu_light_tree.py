@@ -3,7 +3,12 @@ mediumNee.wgsl.ts:14-37 selection with the selection probability outside the
 MIS weights): the device selection against the oracle draw for draw, the
 path-traced image with tree selection against the CPU oracle's, and the
 tree-selected estimator against a uniform-selection FP64 oracle of the same
-scene (unbiased, lower error at equal samples on a 32-point-light cloud)."""
+scene (unbiased, lower error at equal samples on a 32-point-light cloud).
+Distant entries (directionals, the environment) are selected outside the
+tree, evenly within n / (n + 1) of the draws: inside the reference's single
+tree they receive the positional lights' union box, which gives them ~1000
+times the importance of a light a few units away (power over the 1e-3 distance
+floor) and starves the point lights of samples."""
 import math
 
 import numpy as np
@@ -16,6 +21,8 @@ from vitrum_b200.light_tree import BUCKETS, build_light_tree, select_device
 
 pytestmark = pytest.mark.gpu
 
+ORACLE_SEED = (1 << 20) | 12345
+
 
 def test_device_selection_matches_oracle(cuda):
     rng = np.random.default_rng(11)
@@ -27,16 +34,23 @@ def test_device_selection_matches_oracle(cuda):
     tree = build_light_tree(rng.uniform(0.1, 50, n), c, np.concatenate([c - h, c + h], 1), k)
     pts = rng.uniform(-25, 25, (20000, 3)).astype(np.float32)
     buckets = rng.integers(0, BUCKETS, 20000).astype(np.uint32)
-    de, dp = select_device(tree, pts, buckets)
-    want = [oracle.light_tree_sample(tree, p, int(b)) for p, b in zip(pts, buckets)]
-    we = np.array([w[0] for w in want])
-    wp = np.array([w[1] for w in want], np.float32)
-    same = (de == we)
-    # log2 / exp2 may differ by an ulp between the device and the host library,
-    # which can move a bucket boundary by one: a handful of draws may differ
-    assert same.mean() > 0.999, same.mean()
-    assert np.array_equal(dp[same], wp[same]) or np.abs(dp[same] - wp[same]).max() <= 2.0 / BUCKETS
-    assert (dp >= 1.0 / BUCKETS).all() and np.all(np.round(dp * BUCKETS) == dp * BUCKETS)
+    nrm = rng.normal(size=(20000, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    nrm[::7] = 0.0  # transmissive receivers: no receiver term
+    nrm = nrm.astype(np.float32)
+    for n_dist, normals in ((0, None), (2, None), (0, nrm), (1, nrm)):
+        de, dp = select_device(tree, pts, buckets, n_distant=n_dist, normals=normals)
+        want = [oracle.light_select(tree, n, n_dist, p, int(b), None if normals is None else normals[i])
+                for i, (p, b) in enumerate(zip(pts, buckets))]
+        we = np.array([w[0] for w in want])
+        wp = np.array([w[1] for w in want], np.float32)
+        same = (de == we)
+        # log2f / exp2f on the device and the host library's log2 / exp2 can differ in
+        # the last place; the bucket split then moves by a few buckets at some levels
+        assert same.mean() > 0.999, same.mean()
+        assert (np.abs(dp[same] - wp[same]) <= 1e-4 * wp[same] + 64.0 / BUCKETS).all()
+        assert (dp >= 1.0 / BUCKETS).all() and np.all(np.round(dp * BUCKETS) == dp * BUCKETS)
+        assert ((de >= n) == (buckets < (BUCKETS * n_dist) // (n_dist + 1))).all()
 
 
 def many_light_room():
@@ -78,23 +92,51 @@ def render(sc, cam, W, H, spp, seed, selection, B=6):
         e.render_frame(cam, W, H, samples=k, frame_seed=seed)
         done += k
     m, v = e.capture_moments()
-    ms = e.stats()["last_frame_ms"]
     e.dispose()
     return m, v
 
 
 def test_tree_is_unbiased_and_beats_uniform_on_32_point_lights(cuda):
+    """Eight 1024-sample renders per selection, each against a 65,536-sample
+    uniform-selection render.  The error is heavy-tailed in both (paths
+    through the metal and glass instances): each render's relMSE drops its
+    0.1% worst pixels before the two selections are compared, and the pixels
+    below -4 sigma (a heavy-tailed pixel's mean and variance both come out
+    low while its rare bright paths are missing) are judged against the
+    uniform selection's own count on the same draws (the CPU oracle gives
+    tree 1, uniform 3 such pixels here)."""
     sc, cam = scenes.instanced_cloud(n_instances=48, seed=5, n_points=32, sphere_levels=(1, 2), torus_segments=(24, 8),
                                      cube_cells=(3, 5), extent=4.0)
     W, H = 96, 54
-    om, ov = render(sc, cam, W, H, 65536, 12345, "uniform")          # reference: uniform selection
-    tm, tv = render(sc, cam, W, H, 1024, 777, "tree")
-    um, uv = render(sc, cam, W, H, 1024, 777, "uniform")
-    z = (tm - om) / (np.sqrt(tv / 1024 + ov / 65536) + 1e-12)
-    rel = lambda x: float(np.mean((x - om) ** 2 / (om ** 2 + 1e-2)))
-    pos, neg = int((z > 4).sum()), int((z < -4).sum())
-    print(f"tree vs uniform-selection oracle: +4sigma {pos}, -4sigma {neg} of {z.size}; relMSE tree "
-          f"{rel(tm):.3e} uniform {rel(um):.3e}; mean ratio {tm.mean() / om.mean():.4f}")
+    # RNG keys are seed ^ sample index: the oracle's keys [2^20, 2^20 + 65536)
+    # share none with the renders' [k 2^16, k 2^16 + 1024), k = 1 .. 8
+    om, ov = render(sc, cam, W, H, 65536, ORACLE_SEED, "uniform")    # reference: uniform selection
+
+    def trimmed_rel(x):
+        e = np.sort(((x - om) ** 2 / (om ** 2 + 1e-2)).ravel())
+        return float(e[:int(e.size * 0.999)].mean())
+
+    runs = {"tree": [], "uniform": []}
+    rel = {"tree": [], "uniform": []}
+    for k in range(1, 9):
+        for sel in runs:
+            m, v = render(sc, cam, W, H, 1024, k << 16, sel)
+            runs[sel].append((m, v))
+            rel[sel].append(trimmed_rel(m))
+    n = 1024 * 8
+    z = {}
+    for sel, r in runs.items():
+        m, v = np.mean([a for a, _ in r], axis=0), np.mean([b for _, b in r], axis=0)  # n-sample mean, variance
+        z[sel] = (m - om) / (np.sqrt(v / n + ov / 65536) + 1e-12)
+        if sel == "tree":
+            tm = m
+    zt = z["tree"]
+    pos = int((zt > 4).any(axis=-1).sum())
+    neg, neg_u = (int((z[s_] < -4).any(axis=-1).sum()) for s_ in ("tree", "uniform"))
+    rel_t, rel_u = rel["tree"], rel["uniform"]
+    print(f"tree vs uniform-selection oracle: pixels +4sigma {pos}, -4sigma {neg} (uniform {neg_u}) of "
+          f"{W * H}; trimmed relMSE tree {np.mean(rel_t):.3e} uniform {np.mean(rel_u):.3e}; mean ratio "
+          f"{tm.mean() / om.mean():.4f}")
     assert abs(tm.mean() / om.mean() - 1) < 5e-3
-    assert neg <= 3 and abs(np.median(z)) < 0.2
-    assert rel(tm) < rel(um)
+    assert pos <= 2 and neg <= max(3, neg_u + 2) and abs(np.median(zt)) < 0.2
+    assert np.mean(rel_t) < 0.95 * np.mean(rel_u) and sum(a < b for a, b in zip(rel_t, rel_u)) >= 6

@@ -63,16 +63,27 @@ def with_lights(sc, *kinds, scale=1.0, keep_mesh_light=False):
 
 @pytest.mark.parametrize("a,b", [("rect", "disc"), ("disc", "spot"), ("rect", "spot")])
 def test_two_lights_sum(cuda, a, b):
+    """Eight renders of each image.  Light reaching the camera through the
+    metal surfaces makes the image mean heavy-tailed (one 4096-sample render
+    of disc + spot lands anywhere within about 5 % of the sum), so the
+    difference of the image means is judged against its standard error over
+    the renders, which then resolves a bias of about 3 % of the sum."""
     sc, cam = room()
-    ma, va = render(with_lights(sc, a), cam, seed=3)
-    mb, vb = render(with_lights(sc, b), cam, seed=4)
-    mab, vab = render(with_lights(sc, a, b), cam, seed=5)
-    n = 4096
-    z = (mab - ma - mb) / (np.sqrt((va + vb + vab) / n) + 1e-9)
-    print(f"{a}+{b}: mean {mab.mean():.4f} vs {ma.mean() + mb.mean():.4f}, |z|>4: {(np.abs(z) > 4).sum()}")
-    # neighbouring pixels' sample streams are not independent, so the image
-    # mean's error exceeds the per-pixel estimate; 2.5 % is several of its sigma
-    assert abs(mab.mean() / (ma.mean() + mb.mean()) - 1) < 0.025
+    scenes_ = [with_lights(sc, a), with_lights(sc, b), with_lights(sc, a, b)]
+    reps, n = 8, 16384
+    means = np.zeros((reps, 3))
+    for i in range(reps):
+        out = [render(s, cam, spp=n, seed=3 * i + k + 3) for k, s in enumerate(scenes_)]
+        means[i] = [m.mean() for m, _ in out]
+        if i == 0:
+            (ma, va), (mb, vb), (mab, vab) = out
+            z = (mab - ma - mb) / (np.sqrt((va + vb + vab) / n) + 1e-9)
+    d = means[:, 2] - means[:, 0] - means[:, 1]
+    tot = (means[:, 0] + means[:, 1]).mean()
+    se = d.std(ddof=1) / np.sqrt(reps)
+    print(f"{a}+{b}: difference {d.mean() / tot:+.4f} +- {se / tot:.4f} of the sum; first render |z|>4: "
+          f"{(np.abs(z) > 4).sum()}")
+    assert abs(d.mean()) < 4 * se + 1e-3 * tot and se < 0.0075 * tot
     assert (z < -4).sum() <= 3
 
 

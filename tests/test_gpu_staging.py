@@ -67,6 +67,7 @@ def test_set_tuning_validation(cuda):
         with pytest.raises(N.VtError):
             e.set_tuning(**bad)
     e.set_tuning(wave_paths=1 << 18, sort_by_material=True, trace_blocks_per_sm=6, stage_hot_nodes=True)
-    assert e.tuning == {"wave_paths": 1 << 18, "sort_by_material": 1, "trace_blocks_per_sm": 6, "stage_hot_nodes": 1}
+    assert e.tuning == {"wave_paths": 1 << 18, "sort_by_material": 1, "trace_blocks_per_sm": 6, "stage_hot_nodes": 1,
+                        "sort_rays": 0}
     e.render_frame(cam, 16, 16, samples=2)
     e.dispose()

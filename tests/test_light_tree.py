@@ -127,3 +127,35 @@ def test_near_light_dominates_and_cones_cull():
     assert behind[0] < 1e-3 and in_front[0] > 0.2
     # full-sphere packing: axis 0 and both cosines -1
     assert (t[0, 10:13] == 0).all() and t[0, 13] == -1 and t[0, 14] == -1
+
+
+def test_distant_entries_share_their_buckets_evenly():
+    p, c, b, k = random_input(5, seed=2)
+    t = oracle.light_tree_build(p, c, b, k)
+    for n_dist in (1, 2, 3):
+        d = (BUCKETS * n_dist) // (n_dist + 1)
+        tot = {}
+        for bucket in np.linspace(0, BUCKETS - 1, 4001).astype(np.int64):
+            e, pmf = oracle.light_select(t, 5, n_dist, [0.5, 0.5, 0.5], int(bucket))
+            assert (e >= 5) == (bucket < d)
+            tot[e] = pmf
+        dist = [tot[5 + j] for j in range(n_dist)]
+        assert abs(sum(dist) - d / BUCKETS) < 1e-12 and max(dist) - min(dist) <= 1.0 / BUCKETS
+    # one positional entry: it takes the rest; none: the distant ones take all
+    assert oracle.light_select(None, 1, 1, [0, 0, 0], BUCKETS - 1) == (0, 0.5)
+    assert oracle.light_select(None, 0, 2, [0, 0, 0], BUCKETS - 1) == (1, 0.5)
+
+
+def test_receiver_term_favours_lights_above_the_surface():
+    """Two equal point lights above and below a receiver: with the normal up,
+    the one below the horizon keeps only its defensive share (half the
+    buckets over two leaves), the one above takes the rest; without a normal,
+    or with a zero one (transmissive surfaces), they split evenly."""
+    k = np.zeros((2, 6))
+    k[:, 3], k[:, 4] = 0.0, math.pi
+    c = np.array([[0.0, 1.0, 0.0], [0.0, -1.0, 0.0]])
+    t = oracle.light_tree_build(np.array([1.0, 1.0]), c, np.concatenate([c, c], 1), k)
+    up = dict(oracle.light_select(t, 2, 0, [0, 0, 0], b, [0, 1, 0]) for b in (0, BUCKETS - 1))
+    assert up == {0: 0.75, 1: 0.25}  # entry 0 is the light above
+    for nrm in (None, [0, 0, 0]):
+        assert oracle.light_select(t, 2, 0, [0, 0, 0], 0, nrm)[1] == 0.5

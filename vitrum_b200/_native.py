@@ -80,7 +80,7 @@ SIGNATURES = {
     "vt_tlas_build": [P, SZ, I32, I32, I32, P, SZ, P, SZ, P],
     "vt_validate_bvh_encoding": [P, SZ, SZ, P, SZ, ctypes.c_int64, I32, P],
     "vt_light_tree_build": [P, SZ, P, SZ, P],
-    "vt_light_tree_select_device": [P, SZ, P, P, SZ, P, P, P],
+    "vt_light_tree_select_device": [P, SZ, ctypes.c_uint32, P, P, P, SZ, P, P, P],
     "vt_bvh_validate": [P, P],
     "vt_engine_export_tlas": [P, P, SZ, P, SZ, P],
     "vt_bvh_trace_closest_noalloc": [P, P, SZ, P],

@@ -24,7 +24,7 @@ using vt::fail;
 struct vt_batch {
   int device = 0;
   vt_engine_options opts{};
-  vt_tuning tuning{vt::pt::kDefaultWavePaths, 0, 0, 0};
+  vt_tuning tuning{vt::pt::kDefaultWavePaths, 0, 0, 0, 0};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // shadow stream: bounce b's shadow trace and resolve beside bounce b+1's closest-hit trace
@@ -156,6 +156,11 @@ int record_wave(vt_batch* b, cudaStream_t s) {
     t.roots = w.ray_root[cur];
     t.n_dev = w.counters + cur;
     t.blocks_per_sm = b->tuning.trace_blocks_per_sm;
+    if (b->tuning.sort_rays && bo > 0) {
+      vt::pt::launch_sort_rays(w, cur, cap, s);
+      t.order = w.order;
+      k += 2;
+    }
     vt::launch_trace_closest_records(t, s);
     k += 1;
     if (f.sort_by_material) {
@@ -166,6 +171,7 @@ int record_wave(vt_batch* b, cudaStream_t s) {
     if (bo > 0) VT_CUDA(cudaStreamWaitEvent(s, b->ev_join, 0));
     vt::pt::launch_shade(unused, f, w, cur, bo, cap, s);
     vt::TraceArgs sh = t;
+    sh.order = nullptr;
     sh.rays = w.shadow_rays;
     sh.hits = nullptr;
     sh.occluded = w.occluded;
@@ -241,6 +247,7 @@ void validate_tuning(const vt_tuning& t) {
   if (t.trace_blocks_per_sm < 0 || t.trace_blocks_per_sm > 16) fail(VT_ERR_RANGE, "trace_blocks_per_sm in [0, 16]");
   if (t.stage_hot_nodes != 0)
     fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 for a batch (its launches carry one root node per ray)");
+  if (t.sort_rays != 0 && t.sort_rays != 1) fail(VT_ERR_RANGE, "sort_rays must be 0 or 1");
 }
 
 }  // namespace
@@ -425,6 +432,7 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       v.env = p.has_env ? b->env.ptr + off[i].env : nullptr;
       v.env_marginal = p.env_sampleable ? b->marg.ptr + off[i].marg : nullptr;
       v.env_conditional = p.env_sampleable ? b->cond.ptr + off[i].cond : nullptr;
+      v.light_tree_mode = v.n_light_entries >= 2;
       v.light_tree = p.light_tree.empty() ? nullptr : b->ltree.ptr + off[i].lt;
     }
     upload(b->scenes, b->host, s);
@@ -520,6 +528,12 @@ vt_status vt_batch_autotune(vt_batch* b, vt_tuning_trial* report, size_t cap, si
       if (bp == best.trace_blocks_per_sm) continue;
       vt_tuning t = best;
       t.trace_blocks_per_sm = bp;
+      const double ms = time_it(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    {
+      vt_tuning t = best;
+      t.sort_rays = best.sort_rays ? 0 : 1;
       const double ms = time_it(t);
       if (ms < best_ms) { best_ms = ms; best = t; }
     }

@@ -123,6 +123,7 @@ struct vt_engine {
   std::unique_ptr<NrcEngine> nrc;
   int trace_blocks_per_sm = 0;      // traversal CTAs per SM (0: occupancy limit), from the autotuner
   bool trace_stage_nodes = false;   // traversal CTAs stage the top of the tree in shared memory
+  bool sort_rays = false;           // closest-hit queues of bounces >= 1 traced in direction-octant order
   long long debug_wait_cycles = 0;  // failure-detection hook: first-wait limit of bounded waits (0: default)
   // graph cache: one executable per wave shape and mode
   struct Graph {
@@ -253,7 +254,8 @@ void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   v.env_cos = (float)std::cos((double)p.env_rotation);
   v.env_sin = (float)std::sin((double)p.env_rotation);
   v.n_light_entries = (v.n_emitters ? 1u : 0u) + v.n_points + v.n_area + v.n_dirs + (p.env_sampleable ? 1u : 0u);
-  v.light_tree = (!p.light_tree.empty() && e->opts.light_selection == 0) ? e->light_tree.ptr : nullptr;
+  v.light_tree_mode = e->opts.light_selection == 0 && v.n_light_entries >= 2;
+  v.light_tree = (v.light_tree_mode && !p.light_tree.empty()) ? e->light_tree.ptr : nullptr;
   e->view = v;
   e->binary = std::move(p.binary);
   e->blas_root = std::move(p.blas_root);
@@ -631,6 +633,13 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.root = e->view.root;
     t.n_dev = w.counters + cur;
     t.blocks_per_sm = e->trace_blocks_per_sm;
+    if (e->sort_rays && b > 0) {
+      // scattered directions from bounce 1 on: trace the queue octant by octant
+      B(StageTimer::kSort);
+      vt::pt::launch_sort_rays(w, cur, cap, s);
+      E();
+      t.order = w.order;
+    }
     B(StageTimer::kTraceClosest);
     vt::launch_trace_closest_records(t, s);
     E();
@@ -645,6 +654,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     vt::pt::launch_shade(e->view, f, w, cur, b, cap, s);
     E();
     vt::TraceArgs sh = t;
+    sh.order = nullptr;
     sh.rays = w.shadow_rays;
     sh.hits = nullptr;
     sh.occluded = w.occluded;
@@ -1250,6 +1260,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       e->opts.sort_by_material = t.sort_by_material ? 1 : 0;
       e->trace_blocks_per_sm = t.trace_blocks_per_sm;
       e->trace_stage_nodes = t.stage_hot_nodes != 0;
+      e->sort_rays = t.sort_rays != 0;
       e->drop_graphs();
     };
     auto time_it = [&](const vt_tuning& t) {
@@ -1265,7 +1276,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       return best;
     };
     vt_tuning best{(int32_t)wave_paths_of(e), e->opts.sort_by_material > 0 ? 1 : 0,
-                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0};
+                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0, e->sort_rays ? 1 : 0};
     double best_ms = time_it(best);
     for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
       if (wp == best.wave_paths) continue;
@@ -1293,6 +1304,12 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       const double ms = time_it(t);
       if (ms < best_ms) { best_ms = ms; best = t; }
     }
+    {
+      vt_tuning t = best;
+      t.sort_rays = best.sort_rays ? 0 : 1;
+      const double ms = time_it(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
     apply(best);
     reset_accumulation(e);
     if (count) *count = trials.size();
@@ -1309,6 +1326,7 @@ vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
     t->sort_by_material = e->opts.sort_by_material > 0 ? 1 : 0;
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
     t->stage_hot_nodes = e->trace_stage_nodes ? 1 : 0;
+    t->sort_rays = e->sort_rays ? 1 : 0;
   });
 }
 
@@ -1320,12 +1338,14 @@ vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
     if (t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 16)
       fail(VT_ERR_RANGE, "trace_blocks_per_sm must be in [0, 16]");
     if (t->stage_hot_nodes != 0 && t->stage_hot_nodes != 1) fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 or 1");
+    if (t->sort_rays != 0 && t->sort_rays != 1) fail(VT_ERR_RANGE, "sort_rays must be 0 or 1");
     vt::DeviceScope ds(e->device);
     VT_CUDA(cudaStreamSynchronize(e->stream));
     e->opts.wave_paths = t->wave_paths;
     e->opts.sort_by_material = t->sort_by_material;
     e->trace_blocks_per_sm = t->trace_blocks_per_sm;
     e->trace_stage_nodes = t->stage_hot_nodes != 0;
+    e->sort_rays = t->sort_rays != 0;
     e->drop_graphs();
   });
 }

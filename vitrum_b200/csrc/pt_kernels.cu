@@ -164,7 +164,9 @@ __device__ __forceinline__ bool area_light_hit(const SceneView& sc, float3 o, fl
   return found;
 }
 
-__device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng) {
+// N: the unit normal on the incoming side for surfaces that only reflect,
+// zero for transmissive ones (the light tree's receiver term)
+__device__ LightSample sample_light(const SceneView& sc, float3 P, float3 N, uint32_t& rng) {
   LightSample ls;
   ls.valid = false;
   ls.delta = false;
@@ -175,8 +177,9 @@ __device__ LightSample sample_light(const SceneView& sc, float3 P, uint32_t& rng
   // (pt-webgpu mediumNee.wgsl.ts:14-37, connect.wgsl.ts:598)
   float psel;
   uint32_t e;
-  if (sc.light_tree) {
-    psel = lt::select(sc.light_tree, P.x, P.y, P.z, pcg_next(rng) >> 8, e);
+  if (sc.light_tree_mode) {
+    const uint32_t n_dist = sc.n_dirs + (sc.env_marginal ? 1u : 0u);
+    psel = lt::select(sc.light_tree, n - n_dist, n_dist, P.x, P.y, P.z, N.x, N.y, N.z, pcg_next(rng) >> 8, e);
     if (e >= n || !(psel > 0.0f)) return ls;
   } else {
     psel = 1.0f / (float)n;
@@ -318,12 +321,16 @@ __device__ __forceinline__ float area_light_pdf(const SceneView& sc, float dist,
 }
 
 // ---------------------------------------------------------------- light-tree probe
-__global__ void k_light_tree_select(const float* tree, const float* points, const uint32_t* buckets, size_t n,
-                                    uint32_t* entry, float* pmf) {
+__global__ void k_light_tree_select(const float* tree, uint32_t n_pos, uint32_t n_dist, const float* points,
+                                    const float* normals, const uint32_t* buckets, size_t n, uint32_t* entry,
+                                    float* pmf) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t e = 0xFFFFFFFFu;
-  pmf[i] = lt::select(tree, points[3 * i], points[3 * i + 1], points[3 * i + 2], buckets[i] & (lt::kBuckets - 1u), e);
+  const float nx = normals ? normals[3 * i] : 0.0f, ny = normals ? normals[3 * i + 1] : 0.0f,
+              nz = normals ? normals[3 * i + 2] : 0.0f;
+  pmf[i] = lt::select(tree, n_pos, n_dist, points[3 * i], points[3 * i + 1], points[3 * i + 2], nx, ny, nz,
+                      buckets[i] & (lt::kBuckets - 1u), e);
   entry[i] = e;
 }
 
@@ -410,6 +417,53 @@ __global__ void k_scatter(WaveBuffers w, int cur) {
     const uint32_t key = valid ? w.keys[i] : 0xFFu;
 #pragma unroll
     for (uint32_t k = 0; k < 4; ++k) {
+      const uint32_t m = __ballot_sync(kFull, key == k);
+      if (!m) continue;
+      const int leader = __ffs(m) - 1;
+      uint32_t b = 0;
+      if ((int)lane == leader) b = atomicAdd(&w.counters[kCntCursor + k], (uint32_t)__popc(m));
+      b = __shfl_sync(kFull, b, leader);
+      if (key == k) w.order[off[k] + b + __popc(m & ((1u << lane) - 1u))] = i;
+    }
+  }
+}
+
+// Trace order of the closest-hit queue: a counting sort of the queued rays by
+// direction octant, stable up to warp scheduling, so rays that entered the queue
+// in pixel order (nearby origins) stay together within an octant and a warp's
+// rays share the near-to-far child order of the 8-wide nodes.
+__global__ void k_ray_octant(WaveBuffers w, int cur) {
+  const uint32_t n = w.counters[cur];
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    uint32_t key = 0xFFu;
+    if (valid) {
+      const float4 d = w.rays[cur][2 * (size_t)i + 1];
+      key = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+      w.keys[i] = key;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
+      const uint32_t m = __ballot_sync(kFull, key == k);
+      if (m && lane == (uint32_t)(__ffs(m) - 1)) atomicAdd(&w.counters[kCntHist + k], (uint32_t)__popc(m));
+    }
+  }
+}
+
+__global__ void k_ray_octant_scatter(WaveBuffers w, int cur) {
+  const uint32_t n = w.counters[cur];
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t off[8];
+  off[0] = 0;
+#pragma unroll
+  for (int k = 1; k < 8; ++k) off[k] = off[k - 1] + w.counters[kCntHist + k - 1];
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const uint32_t key = i < n ? w.keys[i] : 0xFFu;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
       const uint32_t m = __ballot_sync(kFull, key == k);
       if (!m) continue;
       const int leader = __ffs(m) - 1;
@@ -623,7 +677,8 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
           const OpaqueSide os = surface_side(m, wol);
           // ---- next-event estimation (surfaces with a finite BSDF lobe)
           if (sc.n_light_entries > 0 && has_finite_support(m)) {
-            const LightSample ls = sample_light(sc, P, rng);
+            const LightSample ls =
+                sample_light(sc, P, (m.kind == kDielectric && m.transmission > 0.0f) ? f3(0.0f, 0.0f, 0.0f) : n, rng);
             if (ls.valid) {
               float3 fc;
               float pb;
@@ -979,6 +1034,13 @@ void launch_sort_by_material(const SceneView& sc, const FrameView& f, const Wave
   k_scatter<<<g, 256, 0, s>>>(w, cur);
 }
 
+void launch_sort_rays(const WaveBuffers& w, int cur, uint32_t capacity, cudaStream_t s) {
+  cudaMemsetAsync(w.counters + kCntHist, 0, sizeof(uint32_t) * 16, s);
+  const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
+  k_ray_octant<<<g, 256, 0, s>>>(w, cur);
+  k_ray_octant_scatter<<<g, 256, 0, s>>>(w, cur);
+}
+
 void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur, uint32_t bounce,
                   uint32_t capacity, cudaStream_t s) {
   cudaMemsetAsync(w.counters + (cur ^ 1), 0, sizeof(uint32_t), s);
@@ -1028,16 +1090,19 @@ void launch_accumulate(const FrameView& f, const WaveBuffers& w, const AccumView
 }  // namespace pt
 }  // namespace vt
 
-extern "C" vt_status vt_light_tree_select_device(const float* d_tree, size_t node_count, const float* d_points,
+extern "C" vt_status vt_light_tree_select_device(const float* d_tree, size_t node_count, uint32_t n_distant,
+                                                 const float* d_points, const float* d_normals,
                                                  const uint32_t* d_buckets, size_t n, uint32_t* d_emitter,
                                                  float* d_pmf, void* cuda_stream) {
   return vt::guard([&] {
-    if (n && (!d_tree || !d_points || !d_buckets || !d_emitter || !d_pmf))
-      vt::fail(VT_ERR_INVALID_ARGUMENT, "null argument");
-    if (n && node_count == 0) vt::fail(VT_ERR_INVALID_ARGUMENT, "empty tree");
+    if (n && (!d_points || !d_buckets || !d_emitter || !d_pmf)) vt::fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (node_count && !d_tree) vt::fail(VT_ERR_INVALID_ARGUMENT, "tree is null");
+    if (node_count == 0 && n_distant == 0) vt::fail(VT_ERR_INVALID_ARGUMENT, "no entries");
     if (!n) return;
+    // the positional entries are the tree's leaves ((node_count + 1) / 2); one without a tree
+    const uint32_t n_pos = node_count ? (uint32_t)((node_count + 1) / 2) : 0u;
     vt::pt::k_light_tree_select<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)cuda_stream>>>(
-        d_tree, d_points, d_buckets, n, d_emitter, d_pmf);
+        node_count > 1 ? d_tree : nullptr, n_pos, n_distant, d_points, d_normals, d_buckets, n, d_emitter, d_pmf);
     VT_CUDA(cudaGetLastError());
   });
 }

@@ -56,7 +56,10 @@ struct SceneView {
   // light entries, chosen uniformly by NEE: the emissive-mesh group (if any),
   // positional lights, analytic area lights, directional lights, environment (if any)
   uint32_t n_light_entries = 0;
-  // light tree over the light entries (light_tree.h layout) or nullptr: uniform selection
+  // next-event selection: uniform over the entries, or (light_tree_mode) the
+  // light tree over the positional entries (light_tree.h layout; nullptr when
+  // there is one) with the distant entries (directionals, environment) outside it
+  bool light_tree_mode = false;
   const float* light_tree = nullptr;
   // two-level scenes: instance records (4 float4: world-to-local rows, (blas root, id, material, 0))
   const float4* insts = nullptr;       // in top-level leaf order (traversal)
@@ -154,6 +157,8 @@ struct AccumView {
 void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s);
 void launch_sort_by_material(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur,
                              uint32_t capacity, cudaStream_t s);
+// w.order = the closest-hit queue `cur` partitioned by ray direction octant (trace order)
+void launch_sort_rays(const WaveBuffers& w, int cur, uint32_t capacity, cudaStream_t s);
 void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur, uint32_t bounce,
                   uint32_t capacity, cudaStream_t s);
 void launch_shadow_resolve(const WaveBuffers& w, uint32_t capacity, cudaStream_t s);

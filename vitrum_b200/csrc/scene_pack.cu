@@ -486,16 +486,12 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     env_sampleable = tot > 0.0;
     env_total = tot;
   }
-  // light tree over the light entries, in sample_light's order: the emissive-mesh
-  // group, points, spots, rectangles, discs, directionals, the environment
-  // (the reference's buildLightTreeInputForScene, emitterPacking.ts:1005-1232,
-  // with the emissive triangles as one entry sampled by area)
+  // light tree over the positional light entries, in sample_light's order: the
+  // emissive-mesh group, points, spots, rectangles, discs (the reference's
+  // buildLightTreeInputForScene, emitterPacking.ts:1005-1232, with the emissive
+  // triangles as one entry sampled by area)
   {
     std::vector<lt::Emitter> le;
-    double umn[3] = {INFINITY, INFINITY, INFINITY}, umx[3] = {-INFINITY, -INFINITY, -INFINITY};
-    auto extend = [&](const double* mn, const double* mx) {
-      for (int k = 0; k < 3; ++k) { umn[k] = std::min(umn[k], mn[k]); umx[k] = std::max(umx[k], mx[k]); }
-    };
     auto lum_f = [](double r, double g, double b) { return (double)(float)(0.2126 * r + 0.7152 * g + 0.0722 * b); };
     auto unit = [](const double* v, double* o) {
       const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
@@ -524,7 +520,6 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
       for (int k = 0; k < 3; ++k) g.centroid[k] = 0.5 * g.mn[k] + 0.5 * g.mx[k];
       // one-sided emitters: the group's cone bounds every triangle's outward hemisphere
       lt::merge_into(g, tris);
-      extend(g.mn, g.mx);
       le.push_back(g);
     }
     for (size_t i = 0; i < pts.size() / pt::kPositionalF4; ++i) {
@@ -541,7 +536,6 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
         e.theta_o = 0.0;
         e.theta_e = std::acos(std::max(-1.0, std::min(1.0, (double)ax.w)));
       }
-      extend(e.mn, e.mx);
       le.push_back(e);
     }
     for (size_t i = 0; i < areas.size() / pt::kAreaLightF4; ++i) {
@@ -560,27 +554,10 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
       const double n[3] = {U[1] * W[2] - U[2] * W[1], U[2] * W[0] - U[0] * W[2], U[0] * W[1] - U[1] * W[0]};
       e.oriented = true;
       unit(n, e.axis);
-      extend(e.mn, e.mx);
       le.push_back(e);
     }
-    if (!std::isfinite(umn[0])) for (int k = 0; k < 3; ++k) umn[k] = umx[k] = 0.0;
-    auto distant = [&](double power) {
-      lt::Emitter e;
-      e.power = power;
-      for (int k = 0; k < 3; ++k) {
-        e.mn[k] = umn[k];
-        e.mx[k] = umx[k];
-        e.centroid[k] = (umn[k] + umx[k]) / 2;
-      }
-      le.push_back(e);
-    };
-    for (size_t i = 0; i < dirs.size() / 2; ++i) {
-      const float4 w4 = dirs[2 * i], L = dirs[2 * i + 1];
-      const double c = w4.w;
-      distant(lum_f(L.x, L.y, L.z) * (L.w != 0.0f ? 1.0 : M_PI * (1.0 - c * c)));
-    }
-    if (env_sampleable)
-      distant((double)(float)(env_total * (2.0 * M_PI * M_PI / ((double)sc->environment_width * sc->environment_height))));
+    // the distant entries (directionals, the environment) are chosen outside the
+    // tree, evenly within n_dist / (n_dist + 1) of the selection (light_tree.cuh)
     if (le.size() >= 2) p.light_tree = lt::build_packed(le);
   }
   if (two_level && (node_base || rec_base)) fail(VT_ERR_INVALID_ARGUMENT, "instanced scenes cannot be offset");

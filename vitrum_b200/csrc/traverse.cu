@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
                                                   const uint32_t* __restrict__ n_dev,
                                                   const float4* __restrict__ insts, uint32_t root,
                                                   const uint32_t* __restrict__ roots, uint32_t hot_count,
-                                                  int stk, long long stage_wait) {
+                                                  int stk, long long stage_wait,
+                                                  const uint32_t* __restrict__ order) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -225,6 +226,7 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
       const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
       if (!live && rank < avail) {
         ray = pool_next + rank;
+        if (order) ray = __ldg(order + ray);  // trace order differs from queue order
         const float4 r0 = __ldg(rays + 2 * (size_t)ray), r1 = __ldg(rays + 2 * (size_t)ray + 1);
         R.tmin = r0.w;
         R.closest = r1.w;
@@ -556,7 +558,7 @@ void launch_trace_k(const TraceArgs& a, cudaStream_t s) {
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
   (hot ? staged : plain)<<<(unsigned)grid, kBlock, stack_bytes + 80 * (size_t)hot, s>>>(
       a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded, a.status, a.counter, a.n_dev, a.insts, a.root, a.roots, hot,
-      stk, a.stage_wait_cycles > 0 ? a.stage_wait_cycles : kStagingWaitCycles);
+      stk, a.stage_wait_cycles > 0 ? a.stage_wait_cycles : kStagingWaitCycles, a.order);
 }
 
 template <bool ANY>

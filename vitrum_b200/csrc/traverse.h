@@ -31,6 +31,7 @@ struct TraceArgs {
   size_t node_count = 0;            // nodes in `nodes` (0: unknown, no shared-memory staging)
   bool stage_nodes = false;         // each CTA copies the top of the tree below `root` into shared memory
   long long stage_wait_cycles = 0;  // clocks a CTA waits for that copy before it gives up (0: about a second)
+  const uint32_t* order = nullptr;  // optional trace order: slot i traces ray order[i] (results stay at that ray)
 };
 
 // Bits of the device status word a traversal launch sets.

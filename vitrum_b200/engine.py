@@ -591,12 +591,12 @@ class Engine:
         return {f: getattr(t, f) for f, _ in _Tuning._fields_}
 
     def set_tuning(self, wave_paths: int = 1 << 24, sort_by_material: bool = False, trace_blocks_per_sm: int = 0,
-                   stage_hot_nodes: bool = False) -> None:
+                   stage_hot_nodes: bool = False, sort_rays: bool = False) -> None:
         """Launch shape for later frames (vt_engine_set_tuning); `tuning` of
         another engine or an autotune trial can be passed back as keywords."""
         from .batch import _Tuning
         t = _Tuning(int(wave_paths), 1 if sort_by_material else 0, int(trace_blocks_per_sm),
-                    1 if stage_hot_nodes else 0)
+                    1 if stage_hot_nodes else 0, 1 if sort_rays else 0)
         N.call("vt_engine_set_tuning", self.handle, ctypes.byref(t))
 
     def export_tlas(self):

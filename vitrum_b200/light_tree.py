@@ -44,19 +44,28 @@ def build_light_tree(powers, centroids, aabbs, cones=None) -> np.ndarray:
     return out
 
 
-def select_device(tree, points, buckets, device=0):
-    """Device selection for each point (n, 3) and 24-bit draw: (emitter uint32, pmf float32) numpy arrays."""
+def select_device(tree, points, buckets, n_distant=0, normals=None, device=0):
+    """Device selection for each point (n, 3), receiver normal (n, 3; None:
+    none) and 24-bit draw over the tree's leaves plus `n_distant` distant
+    entries: (entry uint32, pmf float32) arrays."""
     import torch
     dev = torch.device("cuda", device)
-    t = torch.from_numpy(np.ascontiguousarray(tree, np.float32)).to(dev)
+    tree = np.zeros((0, FLOATS_PER_NODE), np.float32) if tree is None else tree
+    t = torch.from_numpy(np.ascontiguousarray(tree, np.float32).reshape(-1, FLOATS_PER_NODE)).to(dev)
     p = torch.from_numpy(np.ascontiguousarray(points, np.float32).reshape(-1, 3)).to(dev)
     b = torch.from_numpy(np.ascontiguousarray(buckets, np.uint32).view(np.int32)).to(dev)
     n = p.shape[0]
+    nr = None
+    if normals is not None:
+        nr = torch.from_numpy(np.ascontiguousarray(normals, np.float32).reshape(-1, 3)).to(dev)
+        if nr.shape[0] != n:
+            raise ValueError("normals and points differ in length")
     e = torch.empty(n, dtype=torch.int32, device=dev)
     pmf = torch.empty(n, dtype=torch.float32, device=dev)
     s = torch.cuda.current_stream(dev)
-    N.call("vt_light_tree_select_device", ctypes.c_void_p(t.data_ptr()), t.shape[0], ctypes.c_void_p(p.data_ptr()),
-           ctypes.c_void_p(b.data_ptr()), n, ctypes.c_void_p(e.data_ptr()), ctypes.c_void_p(pmf.data_ptr()),
+    N.call("vt_light_tree_select_device", ctypes.c_void_p(t.data_ptr()) if t.shape[0] else None, t.shape[0],
+           int(n_distant), ctypes.c_void_p(p.data_ptr()),
+           ctypes.c_void_p(nr.data_ptr()) if nr is not None else None, ctypes.c_void_p(b.data_ptr()), n, ctypes.c_void_p(e.data_ptr()), ctypes.c_void_p(pmf.data_ptr()),
            ctypes.c_void_p(s.cuda_stream))
     torch.cuda.synchronize(dev)
     return e.cpu().numpy().view(np.uint32), pmf.cpu().numpy()
