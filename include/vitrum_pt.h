@@ -475,6 +475,13 @@ vt_status vt_capture(vt_engine* engine, float* rgba, size_t float_capacity);
 /* FP64 per-pixel mean and per-sample variance (requires oracle_accumulation);
  * 3 doubles per pixel each. */
 vt_status vt_capture_moments(vt_engine* engine, double* mean_rgb, double* variance_rgb, size_t double_capacity);
+/* Per-pixel shape of the sample distribution of luminance L = 0.2126 R +
+ * 0.7152 G + 0.0722 B (requires oracle_accumulation; FP64 sums of L .. L^4):
+ * 4 doubles per pixel -- mean, per-sample variance (n - 1), skewness
+ * m3 / m2^1.5 and excess kurtosis m4 / m2^2 - 3 (central moments; 0 for a
+ * constant pixel).  No reference counterpart: the unbiasedness tests judge
+ * +-4 sigma exceedances by these. */
+vt_status vt_capture_luminance_moments(vt_engine* engine, double* out, size_t double_capacity);
 
 /* Auxiliary frame outputs, the textures the reference's kernel writes beside
  * the radiance (pt-webgpu/src/wgsl/pathTrace/kernel.wgsl.ts:936-960), as RGBA

@@ -654,6 +654,8 @@ def _lt_lib():
         L.orc_lt_pdf.argtypes = [P, ctypes.c_long, P, ctypes.c_float, ctypes.c_int]
         L.orc_lt_importance.restype = ctypes.c_float
         L.orc_lt_importance.argtypes = [P, ctypes.c_long, P, ctypes.c_float]
+        L.orc_lt_importance_direct.restype = ctypes.c_float
+        L.orc_lt_importance_direct.argtypes = [P, ctypes.c_long, P, P, ctypes.c_float]
         L._lt_ready = True
     return L
 
@@ -695,6 +697,14 @@ def light_tree_pdf(tree, p, emitter, floor=LT_FLOOR):
 def light_tree_importance(tree, node, p, floor=LT_FLOOR):
     t = np.ascontiguousarray(tree, np.float32)
     return float(_lt_lib().orc_lt_importance(_p(t), int(node), _p(_f32(p)), floor))
+
+
+def light_tree_importance_direct(tree, node, p, normal=None, floor=LT_FLOOR):
+    """The integrator's importance of `node` at p (receiver term for `normal`,
+    None: none), evaluated directly rather than in the reference's log form."""
+    t = np.ascontiguousarray(tree, np.float32)
+    nrm = None if normal is None else _p(_f32(normal))
+    return float(_lt_lib().orc_lt_importance_direct(_p(t), int(node), _p(_f32(p)), nrm, floor))
 
 
 def light_select(tree, n_pos, n_dist, p, bucket, normal=None, floor=LT_FLOOR):

@@ -294,57 +294,56 @@ static float lt_cone_factor(const float* n, float px, float py, float pz) {
 }
 
 /*
- * Receiver term of the integrator's selection (Conty Estevez & Kulla 2018's
- * bound on the shading point's cosine): cos(max(0, theta_i - theta_u)) of
- * the node seen from p above the plane of the unit normal nrm, theta_u the
- * node's angular radius; 0 when the node lies wholly below that plane, 1 for
- * nrm == 0 (transmissive surfaces) or p inside the node's bounding sphere.
+ * The integrator's importance (device light_tree.cuh importance()): the same
+ * quantity as orc_lt_importance -- power / max(dist^2 to the box, floor) times
+ * the orientation cone's bound -- times the receiver term for the unit normal
+ * nrm (Conty Estevez & Kulla 2018's bound cos(max(0, theta_i - theta_u)) on
+ * the shading cosine; NULL or zero: none), evaluated directly in f32 rather
+ * than in the reference's scale-safe log form: one reciprocal square root
+ * serves both bounds, and the packed cone axis is unit (the build normalises
+ * it).  Each operation is rounded on its own, as on the device.
  */
-static float lt_receiver_factor(const float* n, const float* p, const float* nrm) {
-  if (!nrm || (nrm[0] == 0.0f && nrm[1] == 0.0f && nrm[2] == 0.0f)) return 1.0f;
-  const float *mn = n + 4, *mx = n + 7;
-  float dvx = (0.25f * mn[0] + 0.25f * mx[0]) - 0.5f * p[0];
-  float dvy = (0.25f * mn[1] + 0.25f * mx[1]) - 0.5f * p[1];
-  float dvz = (0.25f * mn[2] + 0.25f * mx[2]) - 0.5f * p[2];
-  float rx = 0.25f * mx[0] - 0.25f * mn[0], ry = 0.25f * mx[1] - 0.25f * mn[1], rz = 0.25f * mx[2] - 0.25f * mn[2];
-  float ds = fmax3a(dvx, dvy, dvz);
-  if (!(ds >= F32_MIN_NORMAL) || ds > F32_MAX) return 1.0f;
-  float sdx = dvx / ds, sdy = dvy / ds, sdz = dvz / ds;
-  float sdl = sqrtf(fdot(sdx, sdy, sdz, sdx, sdy, sdz));
-  float rs = fmax3a(rx, ry, rz), rod = 0.0f;
-  if (rs >= F32_MIN_NORMAL) {
-    float srx = rx / rs, sry = ry / rs, srz = rz / rs;
-    float srl = sqrtf(fdot(srx, sry, srz, srx, sry, srz));
-    float lr = ((flog2(rs) + flog2(srl)) - flog2(ds)) - flog2(sdl);
-    if (lr >= 0.0f) return 1.0f;
-    rod = fexp2(fmaxf(lr, -126.0f));
-  }
-  float dx = sdx / sdl, dy = sdy / sdl, dz = sdz / sdl;
-  float ct = fmaxf(-1.0f, fminf(1.0f, fdot(nrm[0], nrm[1], nrm[2], dx, dy, dz)));
-  float stu = fmaxf(0.0f, fminf(1.0f, rod));
-  float ctu = sqrtf(fmaxf(0.0f, 1.0f - stu * stu));
-  float ca = 1.0f;
-  if (ct < ctu) {
-    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-    float a = ct * ctu, b = st * stu;
-    ca = fmaxf(-1.0f, fminf(1.0f, a + b));
-  }
-  return ca > 0.0f ? ca : 0.0f;
+static float lt_bound_cos(float c, float cu, float su) {
+  if (c >= cu) return 1.0f;
+  float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+  float a = c * cu, b = s * su;
+  return fmaxf(-1.0f, fminf(1.0f, a + b));
 }
 
-static float lt_importance_n(const float* tree, long idx, const float* p, const float* nrm, float floor_d2) {
+float orc_lt_importance_direct(const float* tree, long idx, const float* p, const float* nrm, float floor_d2) {
   const float* n = tree + LT_FLOATS * idx;
   float power = n[1];
   if (!(power > 0.0f)) return 0.0f;
-  float d2 = fmaxf(fmaxf(lt_dist2(p[0], p[1], p[2], n + 4), floor_d2), F32_MIN_NORMAL);
-  float cone = lt_cone_factor(n, p[0], p[1], p[2]);
-  if (!(cone > 0.0f)) return 0.0f;
-  float recv = lt_receiver_factor(n, p, nrm);
-  if (!(recv > 0.0f)) return 0.0f;
-  float li = (flog2(power) - flog2(d2)) + flog2(fmaxf(cone * recv, F32_MIN_NORMAL));
-  if (li >= 127.99999f) return F32_MAX;
-  if (li <= -126.0f) return F32_MIN_NORMAL;
-  return fmaxf(F32_MIN_NORMAL, fminf(F32_MAX, fexp2(li)));
+  const float *mn = n + 4, *mx = n + 7;
+  float ex = fmaxf(fmaxf(mn[0] - p[0], 0.0f), p[0] - mx[0]);
+  float ey = fmaxf(fmaxf(mn[1] - p[1], 0.0f), p[1] - mx[1]);
+  float ez = fmaxf(fmaxf(mn[2] - p[2], 0.0f), p[2] - mx[2]);
+  float d2 = fmaxf(fdot(ex, ey, ez, ex, ey, ez), floor_d2);
+  float vx = p[0] - 0.5f * (mn[0] + mx[0]), vy = p[1] - 0.5f * (mn[1] + mx[1]), vz = p[2] - 0.5f * (mn[2] + mx[2]);
+  float hx = 0.5f * (mx[0] - mn[0]), hy = 0.5f * (mx[1] - mn[1]), hz = 0.5f * (mx[2] - mn[2]);
+  float r2 = fdot(hx, hy, hz, hx, hy, hz), l2 = fdot(vx, vy, vz, vx, vy, vz);
+  float w = 1.0f;
+  if (l2 > r2 && l2 <= F32_MAX) { /* p outside the bounding sphere */
+    float inv = (float)(1.0 / sqrt((double)l2));
+    float su = fminf(1.0f, sqrtf(r2) * inv);
+    float cu = sqrtf(fmaxf(0.0f, 1.0f - su * su));
+    if (n[10] != 0.0f || n[11] != 0.0f || n[12] != 0.0f) {
+      float ca = lt_bound_cos(fmaxf(-1.0f, fminf(1.0f, fdot(n[10], n[11], n[12], vx, vy, vz) * inv)), cu, su);
+      if (ca < n[14]) return 0.0f;
+      if (ca < n[13]) {
+        float span = n[13] - n[14];
+        if (span > 0.0f) w = fmaxf(F32_MIN_NORMAL, (ca - n[14]) / span);
+      }
+    }
+    if (nrm && (nrm[0] != 0.0f || nrm[1] != 0.0f || nrm[2] != 0.0f)) {
+      float ci = lt_bound_cos(fmaxf(-1.0f, fminf(1.0f, -(fdot(nrm[0], nrm[1], nrm[2], vx, vy, vz) * inv))), cu, su);
+      if (!(ci > 0.0f)) return 0.0f;
+      w = w * ci;
+    }
+  }
+  float imp = (power * w) / d2;
+  if (!(imp <= F32_MAX)) return F32_MAX;
+  return fmaxf(F32_MIN_NORMAL, imp);
 }
 
 float orc_lt_importance(const float* tree, long idx, const float* p, float floor_d2) {
@@ -375,8 +374,9 @@ static uint32_t lt_left_buckets(uint32_t cur, uint32_t ll, uint32_t rl, float a,
   return ll + (e > remaining ? remaining : e);
 }
 
-static float lt_descend(const float* tree, long nodes, const float* p, const float* nrm, float floor_d2, uint32_t cur,
-                        uint32_t bucket, uint32_t reserve, int* emitter) {
+/* direct: the integrator's importance (orc_lt_importance_direct with nrm), else the reference's */
+static float lt_descend(const float* tree, long nodes, const float* p, const float* nrm, int direct, float floor_d2,
+                        uint32_t cur, uint32_t bucket, uint32_t reserve, int* emitter) {
   long node = 0;
   *emitter = -1;
   for (long guard = 0; guard <= nodes; ++guard) {
@@ -386,8 +386,9 @@ static float lt_descend(const float* tree, long nodes, const float* p, const flo
       return (float)cur / (float)LT_BUCKETS;
     }
     long l = (long)n[2], r = (long)n[3];
-    uint32_t lb = lt_left_buckets(cur, (uint32_t)tree[LT_FLOATS * l + 15], (uint32_t)tree[LT_FLOATS * r + 15],
-                                  lt_importance_n(tree, l, p, nrm, floor_d2), lt_importance_n(tree, r, p, nrm, floor_d2),
+    float il = direct ? orc_lt_importance_direct(tree, l, p, nrm, floor_d2) : orc_lt_importance(tree, l, p, floor_d2);
+    float ir = direct ? orc_lt_importance_direct(tree, r, p, nrm, floor_d2) : orc_lt_importance(tree, r, p, floor_d2);
+    uint32_t lb = lt_left_buckets(cur, (uint32_t)tree[LT_FLOATS * l + 15], (uint32_t)tree[LT_FLOATS * r + 15], il, ir,
                                   reserve);
     if (bucket < lb) { cur = lb; node = l; }
     else { bucket -= lb; cur -= lb; node = r; }
@@ -399,7 +400,7 @@ static float lt_descend(const float* tree, long nodes, const float* p, const flo
 float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d2, uint32_t bucket, int* emitter) {
   *emitter = -1;
   if (nodes <= 0) return 0.0f;
-  return lt_descend(tree, nodes, p, NULL, floor_d2, LT_BUCKETS, bucket, 1u, emitter);
+  return lt_descend(tree, nodes, p, NULL, 0, floor_d2, LT_BUCKETS, bucket, 1u, emitter);
 }
 
 /*
@@ -408,8 +409,8 @@ float orc_lt_sample(const float* tree, long nodes, const float* p, float floor_d
  * (distant lights) evenly within n_dist / (n_dist + 1) of the 2^24 buckets.
  * In the tree's descent every leaf keeps a defensive reserve of half the
  * tree's buckets split evenly (the reference keeps one bucket per leaf); the
- * other half follows the importance, times the receiver term for the unit
- * normal nrm (NULL or zero: none).
+ * other half follows orc_lt_importance_direct for the unit normal nrm (NULL
+ * or zero: no receiver term).
  */
 float orc_lt_select(const float* tree, long nodes, uint32_t n_pos, uint32_t n_dist, const float* p, const float* nrm,
                     float floor_d2, uint32_t bucket, int* emitter) {
@@ -426,7 +427,7 @@ float orc_lt_select(const float* tree, long nodes, uint32_t n_pos, uint32_t n_di
   /* defensive half: each leaf keeps (buckets / 2) / leaves of the tree's buckets */
   uint32_t reserve = (LT_BUCKETS - D) / (2u * (uint32_t)tree[15]);
   if (reserve < 1u) reserve = 1u;
-  return lt_descend(tree, nodes, p, nrm, floor_d2, LT_BUCKETS - D, bucket - D, reserve, emitter);
+  return lt_descend(tree, nodes, p, nrm, 1, floor_d2, LT_BUCKETS - D, bucket - D, reserve, emitter);
 }
 
 /* PMF of one emitter at point p (the deterministic inverse of orc_lt_sample). */

@@ -96,6 +96,7 @@ SIGNATURES = {
     "vt_get_capabilities": [P, P],
     "vt_bake_preetham_sky": [P, I32, I32, P, SZ],
     "vt_capture_moments": [P, P, P, SZ],
+    "vt_capture_luminance_moments": [P, P, SZ],
     "vt_capture_aux": [P, I32, P, SZ],
     "vt_set_previous_camera": [P, P, P],
     "vt_pick": [P, ctypes.c_float, ctypes.c_float, P],

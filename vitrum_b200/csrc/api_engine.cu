@@ -95,7 +95,7 @@ struct vt_engine {
   int width = 0, height = 0;
   DeviceBuffer<float4> accum;
   DeviceBuffer<float4> present;     // present-pass output of vt_capture_output
-  DeviceBuffer<double> sum64, sq64;
+  DeviceBuffer<double> sum64, sq64, lum64;
   // auxiliary outputs (first-hit normal / depth, albedo, motion; luminance
   // moments) and their per-frame constants (view-projections, recorded sample)
   DeviceBuffer<float4> aux_nd, aux_albedo, aux_motion, aux_moments;
@@ -607,6 +607,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
   a.accum = e->accum.ptr;
   a.sum64 = e->sum64.ptr;
   a.sq64 = e->sq64.ptr;
+  a.lum64 = e->lum64.ptr;
   const uint32_t cap = f.paths;
   B(StageTimer::kRaygen);
   vt::pt::launch_raygen(f, w, s);
@@ -735,6 +736,7 @@ void reset_accumulation(vt_engine* e) {
   if (e->accum.ptr) VT_CUDA(cudaMemsetAsync(e->accum.ptr, 0, e->accum.bytes(), e->stream));
   if (e->sum64.ptr) VT_CUDA(cudaMemsetAsync(e->sum64.ptr, 0, e->sum64.bytes(), e->stream));
   if (e->sq64.ptr) VT_CUDA(cudaMemsetAsync(e->sq64.ptr, 0, e->sq64.bytes(), e->stream));
+  if (e->lum64.ptr) VT_CUDA(cudaMemsetAsync(e->lum64.ptr, 0, e->lum64.bytes(), e->stream));
   for (DeviceBuffer<float4>* b : {&e->aux_nd, &e->aux_albedo, &e->aux_motion, &e->aux_moments})
     if (b->ptr) VT_CUDA(cudaMemsetAsync(b->ptr, 0, b->bytes(), e->stream));
   VT_CUDA(cudaMemsetAsync(e->counters.ptr, 0, e->counters.bytes(), e->stream));
@@ -764,6 +766,7 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     if (e->opts.oracle_accumulation) {
       e->sum64.resize(3 * px);
       e->sq64.resize(3 * px);
+      e->lum64.resize(4 * px);
     }
   }
   if (size_changed || cam_changed) {
@@ -1053,6 +1056,36 @@ vt_status vt_capture_moments(vt_engine* e, double* mean_rgb, double* var_rgb, si
       const double q = n > 0 ? var_rgb[i] / n : 0.0;
       mean_rgb[i] = m;
       var_rgb[i] = n > 1 ? std::max(0.0, (q - m * m) * n / (n - 1)) : 0.0;
+    }
+  });
+}
+
+vt_status vt_capture_luminance_moments(vt_engine* e, double* out, size_t cap) {
+  return vt::guard([&] {
+    if (!e || !out) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->opts.oracle_accumulation || !e->lum64.ptr) fail(VT_ERR_STATE, "engine has no FP64 accumulation");
+    const size_t px = (size_t)e->width * e->height;
+    if (cap < 4 * px) fail(VT_ERR_RANGE, "moment buffer too small");
+    vt::DeviceScope ds(e->device);
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    VT_CUDA(cudaMemcpy(out, e->lum64.ptr, 4 * px * sizeof(double), cudaMemcpyDeviceToHost));
+    const double n = (double)e->samples;
+    for (size_t i = 0; i < px; ++i) {
+      double* o = out + 4 * i;
+      if (!(n > 1)) {
+        o[0] = n > 0 ? o[0] / n : 0.0;
+        o[1] = o[2] = o[3] = 0.0;
+        continue;
+      }
+      // central moments from the raw ones
+      const double m = o[0] / n, r2 = o[1] / n, r3 = o[2] / n, r4 = o[3] / n, mm = m * m;
+      const double c2 = std::max(0.0, r2 - mm);
+      const double c3 = r3 - 3.0 * m * r2 + 2.0 * mm * m;
+      const double c4 = r4 - 4.0 * m * r3 + 6.0 * mm * r2 - 3.0 * mm * mm;
+      o[0] = m;
+      o[1] = c2 * n / (n - 1);
+      o[2] = c2 > 0 ? c3 / (c2 * std::sqrt(c2)) : 0.0;
+      o[3] = c2 > 0 ? std::max(-2.0, c4 / (c2 * c2) - 3.0) : 0.0;
     }
   });
 }

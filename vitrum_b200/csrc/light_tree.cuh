@@ -1,8 +1,9 @@
 // light_tree.cuh -- device selection of one light entry from the packed light
-// tree (layout in light_tree.h), the reference's samplePackedLightTreeCPU /
-// packedNodeImportanceUnchecked (packages/shared-samplers/src/lightTree.ts:938-1319)
-// in f32 with every operation rounded on its own (no contraction), so the
-// bucket split follows the same arithmetic as the CPU oracle.
+// tree (layout in light_tree.h): the reference's samplePackedLightTreeCPU bucket
+// descent (packages/shared-samplers/src/lightTree.ts:938-1319) over an importance
+// of the same quantity plus a receiver bound, in f32 with every operation
+// rounded on its own (no contraction), so the bucket split follows the same
+// arithmetic as the CPU oracle's restatement.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,128 +25,64 @@ __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b)
 __device__ __forceinline__ float dot3r(float ax, float ay, float az, float bx, float by, float bz) {
   return fadd(fadd(fmul(ax, bx), fmul(ay, by)), fmul(az, bz));
 }
-__device__ __forceinline__ float max3abs(float a, float b, float c) {
-  return fmaxf(fabsf(a), fmaxf(fabsf(b), fabsf(c)));
+
+// cos(max(0, theta - theta_u)) for cos theta = c and the half-angle theta_u (cu, su)
+__device__ __forceinline__ float bound_cos(float c, float cu, float su) {
+  if (c >= cu) return 1.0f;
+  const float s = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(c, c))));
+  return fmaxf(-1.0f, fminf(1.0f, fadd(fmul(c, cu), fmul(s, su))));
 }
 
-// squared distance from p to the box, scale-safe (packedDist2ToAabbCPU)
-__device__ __forceinline__ float dist2_box(float px, float py, float pz, const float* b) {
-  const float hx = fmaxf(fmaxf(fsub(fmul(0.5f, b[0]), fmul(0.5f, px)), 0.0f), fsub(fmul(0.5f, px), fmul(0.5f, b[3])));
-  const float hy = fmaxf(fmaxf(fsub(fmul(0.5f, b[1]), fmul(0.5f, py)), 0.0f), fsub(fmul(0.5f, py), fmul(0.5f, b[4])));
-  const float hz = fmaxf(fmaxf(fsub(fmul(0.5f, b[2]), fmul(0.5f, pz)), 0.0f), fsub(fmul(0.5f, pz), fmul(0.5f, b[5])));
-  const float hs = max3abs(hx, hy, hz);
-  if (!(hs >= kF32MinNormal)) return 0.0f;
-  if (hs > fmul(0.5f, kF32Max)) return kF32Max;
-  const float sx = fdiv(hx, hs), sy = fdiv(hy, hs), sz = fdiv(hz, hs);
-  const float ss = dot3r(sx, sy, sz, sx, sy, sz);
-  const float s = fmul(2.0f, hs);
-  const float lim = __fsqrt_rn(fdiv(kF32Max, ss));
-  if (s >= lim) return kF32Max;
-  return fminf(kF32Max, fmul(fmul(s, s), ss));
-}
-
-// orientation-cone factor (packedConeFactorCPU): 1 inside the normal cone, a
-// cosine-space taper to the emission bound, 0 beyond it
-__device__ __forceinline__ float cone_factor(const float* n, float px, float py, float pz) {
-  const float axs = max3abs(n[10], n[11], n[12]);
-  if (!(axs > 0.0f) || axs > kF32Max) return 1.0f;
-  const float ax = fdiv(n[10], axs), ay = fdiv(n[11], axs), az = fdiv(n[12], axs);
-  const float al = __fsqrt_rn(dot3r(ax, ay, az, ax, ay, az));
-  const float* mn = n + 4;
-  const float* mx = n + 7;
-  const float dvx = fsub(fsub(fmul(0.5f, px), fmul(0.25f, mn[0])), fmul(0.25f, mx[0]));
-  const float dvy = fsub(fsub(fmul(0.5f, py), fmul(0.25f, mn[1])), fmul(0.25f, mx[1]));
-  const float dvz = fsub(fsub(fmul(0.5f, pz), fmul(0.25f, mn[2])), fmul(0.25f, mx[2]));
-  const float rx = fsub(fmul(0.25f, mx[0]), fmul(0.25f, mn[0]));
-  const float ry = fsub(fmul(0.25f, mx[1]), fmul(0.25f, mn[1]));
-  const float rz = fsub(fmul(0.25f, mx[2]), fmul(0.25f, mn[2]));
-  const float ds = max3abs(dvx, dvy, dvz);
-  if (!(ds >= kF32MinNormal) || ds > kF32Max) return 1.0f;
-  const float sdx = fdiv(dvx, ds), sdy = fdiv(dvy, ds), sdz = fdiv(dvz, ds);
-  const float sdl = __fsqrt_rn(dot3r(sdx, sdy, sdz, sdx, sdy, sdz));
-  const float rs = max3abs(rx, ry, rz);
-  float r_over_d = 0.0f;
-  if (rs >= kF32MinNormal) {
-    const float srx = fdiv(rx, rs), sry = fdiv(ry, rs), srz = fdiv(rz, rs);
-    const float srl = __fsqrt_rn(dot3r(srx, sry, srz, srx, sry, srz));
-    const float lr = fsub(fsub(fadd(log2f(rs), log2f(srl)), log2f(ds)), log2f(sdl));
-    if (lr >= 0.0f) return 1.0f;
-    r_over_d = exp2f(fmaxf(lr, -126.0f));
-  }
-  const float dx = fdiv(sdx, sdl), dy = fdiv(sdy, sdl), dz = fdiv(sdz, sdl);
-  const float nx = fdiv(ax, al), ny = fdiv(ay, al), nz = fdiv(az, al);
-  const float ct = fmaxf(-1.0f, fminf(1.0f, dot3r(nx, ny, nz, dx, dy, dz)));
-  const float stu = fmaxf(0.0f, fminf(1.0f, r_over_d));
-  const float ctu = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(stu, stu))));
-  float ca = 1.0f;
-  if (ct < ctu) {
-    const float st = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(ct, ct))));
-    ca = fmaxf(-1.0f, fminf(1.0f, fadd(fmul(ct, ctu), fmul(st, stu))));
-  }
-  if (ca < n[14]) return 0.0f;
-  if (ca >= n[13]) return 1.0f;
-  const float span = fsub(n[13], n[14]);
-  if (!(span > 0.0f)) return 1.0f;
-  return fmaxf(kF32MinNormal, fminf(1.0f, fdiv(fsub(ca, n[14]), span)));
-}
-
-// Receiver term (Conty Estevez & Kulla 2018's bound on the shading point's
-// cosine): cos(max(0, theta_i - theta_u)) of the node seen from p above the
-// plane of the unit normal (nx, ny, nz), theta_u the node's angular radius; 0
-// when the node lies wholly below that plane, 1 for a zero normal
-// (transmissive surfaces) or p inside the node's bounding sphere.
-__device__ __forceinline__ float receiver_factor(const float* n, float px, float py, float pz, float nx, float ny,
-                                                 float nz) {
-  if (nx == 0.0f && ny == 0.0f && nz == 0.0f) return 1.0f;
-  const float* mn = n + 4;
-  const float* mx = n + 7;
-  const float dvx = fsub(fadd(fmul(0.25f, mn[0]), fmul(0.25f, mx[0])), fmul(0.5f, px));
-  const float dvy = fsub(fadd(fmul(0.25f, mn[1]), fmul(0.25f, mx[1])), fmul(0.5f, py));
-  const float dvz = fsub(fadd(fmul(0.25f, mn[2]), fmul(0.25f, mx[2])), fmul(0.5f, pz));
-  const float rx = fsub(fmul(0.25f, mx[0]), fmul(0.25f, mn[0]));
-  const float ry = fsub(fmul(0.25f, mx[1]), fmul(0.25f, mn[1]));
-  const float rz = fsub(fmul(0.25f, mx[2]), fmul(0.25f, mn[2]));
-  const float ds = max3abs(dvx, dvy, dvz);
-  if (!(ds >= kF32MinNormal) || ds > kF32Max) return 1.0f;
-  const float sdx = fdiv(dvx, ds), sdy = fdiv(dvy, ds), sdz = fdiv(dvz, ds);
-  const float sdl = __fsqrt_rn(dot3r(sdx, sdy, sdz, sdx, sdy, sdz));
-  const float rs = max3abs(rx, ry, rz);
-  float r_over_d = 0.0f;
-  if (rs >= kF32MinNormal) {
-    const float srx = fdiv(rx, rs), sry = fdiv(ry, rs), srz = fdiv(rz, rs);
-    const float srl = __fsqrt_rn(dot3r(srx, sry, srz, srx, sry, srz));
-    const float lr = fsub(fsub(fadd(log2f(rs), log2f(srl)), log2f(ds)), log2f(sdl));
-    if (lr >= 0.0f) return 1.0f;
-    r_over_d = exp2f(fmaxf(lr, -126.0f));
-  }
-  const float dx = fdiv(sdx, sdl), dy = fdiv(sdy, sdl), dz = fdiv(sdz, sdl);
-  const float ct = fmaxf(-1.0f, fminf(1.0f, dot3r(nx, ny, nz, dx, dy, dz)));
-  const float stu = fmaxf(0.0f, fminf(1.0f, r_over_d));
-  const float ctu = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(stu, stu))));
-  float ca = 1.0f;
-  if (ct < ctu) {
-    const float st = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(ct, ct))));
-    ca = fmaxf(-1.0f, fminf(1.0f, fadd(fmul(ct, ctu), fmul(st, stu))));
-  }
-  return ca > 0.0f ? ca : 0.0f;
-}
-
-// importance of packed node `idx` for the point p (packedNodeImportanceUnchecked),
-// times the receiver term for the normal n
+// Importance of packed node `idx` for the point p with unit normal n (zero:
+// none): the quantity of the reference's packedNodeImportanceUnchecked
+// (lightTree.ts:1237-1319) -- power / max(dist^2 to the box, floor) times the
+// orientation cone's taper at cos(max(0, theta - theta_u)) -- times the
+// receiver bound cos(max(0, theta_i - theta_u)) on the shading cosine (Conty
+// Estevez & Kulla 2018), theta_u the node's bounding-sphere half-angle.  It is
+// evaluated directly, not in the reference's scale-safe log form: one
+// reciprocal square root serves both bounds and the packed axis is unit (the
+// build normalises it), about a fifth of the instructions.  Every operation
+// is rounded on its own, as in the CPU oracle's restatement.
 __device__ __forceinline__ float importance(const float* tree, uint32_t idx, float px, float py, float pz, float nx,
                                             float ny, float nz) {
   const float* n = tree + (size_t)idx * kFloatsPerNode;
-  const float power = n[1];
+  const float power = __ldg(n + 1);
   if (!(power > 0.0f)) return 0.0f;
-  const float d2 = fmaxf(fmaxf(dist2_box(px, py, pz, n + 4), kDist2Floor), kF32MinNormal);
-  const float cone = cone_factor(n, px, py, pz);
-  if (!(cone > 0.0f)) return 0.0f;
-  const float recv = receiver_factor(n, px, py, pz, nx, ny, nz);
-  if (!(recv > 0.0f)) return 0.0f;
-  const float li = fadd(fsub(log2f(power), log2f(d2)), log2f(fmaxf(fmul(cone, recv), kF32MinNormal)));
-  if (li >= 127.99999f) return kF32Max;
-  if (li <= -126.0f) return kF32MinNormal;
-  return fmaxf(kF32MinNormal, fminf(kF32Max, exp2f(li)));
+  const float mnx = __ldg(n + 4), mny = __ldg(n + 5), mnz = __ldg(n + 6);
+  const float mxx = __ldg(n + 7), mxy = __ldg(n + 8), mxz = __ldg(n + 9);
+  const float ex = fmaxf(fmaxf(fsub(mnx, px), 0.0f), fsub(px, mxx));
+  const float ey = fmaxf(fmaxf(fsub(mny, py), 0.0f), fsub(py, mxy));
+  const float ez = fmaxf(fmaxf(fsub(mnz, pz), 0.0f), fsub(pz, mxz));
+  const float d2 = fmaxf(dot3r(ex, ey, ez, ex, ey, ez), kDist2Floor);
+  const float vx = fsub(px, fmul(0.5f, fadd(mnx, mxx)));
+  const float vy = fsub(py, fmul(0.5f, fadd(mny, mxy)));
+  const float vz = fsub(pz, fmul(0.5f, fadd(mnz, mxz)));
+  const float hx = fmul(0.5f, fsub(mxx, mnx)), hy = fmul(0.5f, fsub(mxy, mny)), hz = fmul(0.5f, fsub(mxz, mnz));
+  const float r2 = dot3r(hx, hy, hz, hx, hy, hz), l2 = dot3r(vx, vy, vz, vx, vy, vz);
+  float w = 1.0f;
+  if (l2 > r2 && l2 <= kF32Max) {  // p outside the bounding sphere
+    const float inv = __frsqrt_rn(l2);
+    const float su = fminf(1.0f, fmul(__fsqrt_rn(r2), inv));
+    const float cu = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(su, su))));
+    const float ax = __ldg(n + 10), ay = __ldg(n + 11), az = __ldg(n + 12);
+    if (ax != 0.0f || ay != 0.0f || az != 0.0f) {
+      const float ca = bound_cos(fmaxf(-1.0f, fminf(1.0f, fmul(dot3r(ax, ay, az, vx, vy, vz), inv))), cu, su);
+      const float cos_o = __ldg(n + 13), cos_e = __ldg(n + 14);
+      if (ca < cos_e) return 0.0f;
+      if (ca < cos_o) {
+        const float span = fsub(cos_o, cos_e);
+        if (span > 0.0f) w = fmaxf(kF32MinNormal, fdiv(fsub(ca, cos_e), span));
+      }
+    }
+    if (nx != 0.0f || ny != 0.0f || nz != 0.0f) {
+      const float ci = bound_cos(fmaxf(-1.0f, fminf(1.0f, -fmul(dot3r(nx, ny, nz, vx, vy, vz), inv))), cu, su);
+      if (!(ci > 0.0f)) return 0.0f;
+      w = fmul(w, ci);
+    }
+  }
+  const float imp = fdiv(fmul(power, w), d2);
+  if (!(imp <= kF32Max)) return kF32Max;
+  return fmaxf(kF32MinNormal, imp);
 }
 
 // buckets of the current interval that go to the left child (allocateLeftBuckets)

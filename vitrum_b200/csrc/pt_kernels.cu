@@ -788,7 +788,7 @@ __global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
   if (pix >= wh) return;
   float3 s = f3(0.0f, 0.0f, 0.0f);
   float l1 = 0.0f, l2 = 0.0f;  // luminance moments (varianceMomentsBuffer, kernel.wgsl.ts:936-940)
-  double s64[3] = {0, 0, 0}, q64[3] = {0, 0, 0};
+  double s64[3] = {0, 0, 0}, q64[3] = {0, 0, 0}, m64[4] = {0, 0, 0, 0};
   for (uint32_t k = 0; k < f.spp_wave; ++k) {
     const float4 r = w.radiance[(size_t)k * wh + pix];
     s = s + f3(r.x, r.y, r.z);
@@ -798,6 +798,13 @@ __global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
     if (a.sum64) {
       const double v[3] = {r.x, r.y, r.z};
       for (int c = 0; c < 3; ++c) { s64[c] += v[c]; q64[c] += v[c] * v[c]; }
+    }
+    if (a.lum64) {
+      const double L = 0.2126 * r.x + 0.7152 * r.y + 0.0722 * r.z, L2 = L * L;
+      m64[0] += L;
+      m64[1] += L2;
+      m64[2] += L2 * L;
+      m64[3] += L2 * L2;
     }
   }
   float4 acc = a.accum[pix];
@@ -812,6 +819,8 @@ __global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
       a.sq64[3 * (size_t)pix + c] += q64[c];
     }
   }
+  if (a.lum64)
+    for (int k = 0; k < 4; ++k) a.lum64[4 * (size_t)pix + k] += m64[k];
 }
 
 // next wave's samples start after this wave's (read by k_raygen)

@@ -152,6 +152,7 @@ struct AccumView {
   float4* accum = nullptr;    // rgb sum, sample count (FP32, the displayed estimate)
   double* sum64 = nullptr;    // 3 per pixel, FP64 sum (oracle accumulation)
   double* sq64 = nullptr;     // 3 per pixel, FP64 sum of squares
+  double* lum64 = nullptr;    // 4 per pixel, FP64 sums of L, L^2, L^3, L^4 (L: a sample's Rec. 709 luminance)
 };
 
 void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s);

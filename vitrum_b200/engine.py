@@ -527,6 +527,13 @@ class Engine:
                m.size)
         return m, v
 
+    def capture_luminance_moments(self):
+        """Per-pixel FP64 shape of the luminance samples, (H, W, 4): mean,
+        per-sample variance, skewness, excess kurtosis (oracle_accumulation)."""
+        out = np.empty((self.height, self.width, 4), np.float64)
+        N.call("vt_capture_luminance_moments", self.handle, ctypes.c_void_p(out.ctypes.data), out.size)
+        return out
+
     AUX = {"normal_depth": 0, "albedo": 1, "motion": 2, "variance": 3}
 
     def capture_aux(self, kind: str) -> np.ndarray:
