@@ -432,23 +432,30 @@ def run_batch(args, dev, local, barrier):
 
 
 # ------------------------------------------------------------------ radiance cache workload
-NRC_W, NRC_H, NRC_SPP, NRC_WARM, NRC_FRAMES = 480, 270, 16, 32, 8
-# RNG keys are frame seed ^ sample index: the oracle's keys [2^20, 2^20 + 2^16)
-# share none with the curves' frames (seed 7, small sample indices)
-ORACLE_SEED = (1 << 20) | 4242
+NRC_SPP, NRC_WARM, NRC_FRAMES, NRC_SEEDS = 16, 8, 64, 5
 
 
-def _relmse(img, ref):
-    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+# RNG keys are frame seed ^ sample index: the oracle's keys [2^20, 2^20 + 2^14)
+# share none with the measured sequences' ((s + 1) 2^12 ^ [0, 1024))
+ORACLE_SEED = 1 << 20
+
+
+def _relmse(img, ref, ref_var=None):
+    """mean((x - ref)^2 / (ref^2 + 1e-2)); with ref_var (the oracle mean's own
+    variance per pixel) its noise is taken out: E(x - ref)^2 = E(x - mu)^2 + ref_var."""
+    d2 = (img - ref) ** 2
+    if ref_var is not None:
+        d2 = d2 - ref_var
+    return float(np.mean(d2 / (ref ** 2 + 1e-2)))
 
 
 _CLOUD_ORACLE = {}
 
 
 def _cloud_oracle(args, local):
-    """The 1024-instance cloud at NRC_W x NRC_H, 8 bounces, args.oracle_spp
-    samples accumulated in FP64 (rendered once per run): (mean, per-sample
-    variance, seconds)."""
+    """The 1024-instance cloud at 1920x1080, 8 bounces, args.oracle_spp samples
+    accumulated in FP64, rendered once per run: (mean, variance of the mean,
+    seconds)."""
     if "ref" not in _CLOUD_ORACLE:
         from vitrum_b200 import scenes
         from vitrum_b200.engine import Engine
@@ -458,12 +465,13 @@ def _cloud_oracle(args, local):
         o.set_scene(sc)
         done = 0
         while done < args.oracle_spp:
-            k = min(2048, args.oracle_spp - done)
-            o.render_frame(cam, NRC_W, NRC_H, samples=k, frame_seed=ORACLE_SEED)
+            k = min(1024, args.oracle_spp - done)
+            o.render_frame(cam, I_W, I_H, samples=k, frame_seed=ORACLE_SEED)
             done += k
         ref, var = o.capture_moments()
         o.dispose()
-        _CLOUD_ORACLE["ref"] = (ref, var, time.perf_counter() - t0)
+        _CLOUD_ORACLE["ref"] = (ref.astype(np.float32), (var / args.oracle_spp).astype(np.float32),
+                                time.perf_counter() - t0)
     return _CLOUD_ORACLE["ref"]
 
 
@@ -472,20 +480,20 @@ LT_SPP, LT_SEEDS = 64, 5
 
 def run_light_tree(args, dev, local, barrier):
     """Next-event light selection on the 1024-instance cloud with 32 point
-    lights: the light tree (power x proximity x orientation x receiver
-    cosine bound, half the buckets spread evenly) against uniform selection.
-    Per selection: the device time of a 1920x1080 x 16 spp frame and of a
-    480x270 x 64 spp frame, and the relMSE of the latter against the FP64
-    oracle over LT_SEEDS seeds (median; also with the 0.1 % worst pixels
-    dropped, the error being heavy-tailed through the metal and glass
-    instances).  Equal time: relMSE x frame time, lower is better."""
+    lights at 1920x1080: the light tree (power x proximity x orientation x
+    receiver cosine bound, half the buckets spread evenly) against uniform
+    selection.  Per selection: the device time of a 16-spp and a 64-spp frame,
+    and the relMSE of the 64-spp frame against the FP64 oracle over LT_SEEDS
+    seeds (median; also with the 0.1 % worst pixels dropped, the error being
+    heavy-tailed through the metal and glass instances).  Equal time: relMSE x
+    frame time, lower is better."""
     from vitrum_b200 import scenes
     from vitrum_b200.engine import Engine
     sc, cam = scenes.instanced_cloud()
-    ref, _, _ = _cloud_oracle(args, local)
+    ref, rvar, _ = _cloud_oracle(args, local)
 
     def trimmed(img):
-        e = np.sort(((img - ref) ** 2 / (ref ** 2 + 1e-2)).ravel())
+        e = np.sort((((img - ref) ** 2 - rvar) / (ref ** 2 + 1e-2)).ravel())
         return float(e[:int(e.size * 0.999)].mean())
 
     out = {}
@@ -499,90 +507,126 @@ def run_light_tree(args, dev, local, barrier):
             e.render_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=910 + i)
             full.append(e.stats()["last_frame_ms"])
         e.reset()
-        e.render_frame(cam, NRC_W, NRC_H, samples=LT_SPP, frame_seed=920)  # warm the small frame's graph
-        small, rel, rel_t = [], [], []
+        e.render_frame(cam, I_W, I_H, samples=LT_SPP, frame_seed=920)  # the 64-spp frame's graph
+        ms, rel, rel_t = [], [], []
         for k in range(1, LT_SEEDS + 1):
             e.reset()
-            e.render_frame(cam, NRC_W, NRC_H, samples=LT_SPP, frame_seed=k << 16)
-            small.append(e.stats()["last_frame_ms"])
-            img = e.capture_frame()[..., :3].astype(np.float64)
-            rel.append(_relmse(img, ref))
+            e.render_frame(cam, I_W, I_H, samples=LT_SPP, frame_seed=k << 16)
+            ms.append(e.stats()["last_frame_ms"])
+            img = e.capture_frame()[..., :3]
+            rel.append(_relmse(img, ref, rvar))
             rel_t.append(trimmed(img))
         e.dispose()
-        out[sel] = {"frame_ms_1920x1080_16spp": round(float(np.median(full)), 3),
-                    "frame_ms_480x270_64spp": round(float(np.median(small)), 3),
+        out[sel] = {"frame_ms_16spp": round(float(np.median(full)), 3),
+                    "frame_ms_64spp": round(float(np.median(ms)), 3),
                     "relmse": round(float(np.median(rel)), 6), "relmse_trimmed": round(float(np.median(rel_t)), 6),
                     "relmse_per_seed": [round(r, 6) for r in rel]}
     u, t = out["uniform"], out["tree"]
-    cost = t["frame_ms_480x270_64spp"] / u["frame_ms_480x270_64spp"]
+    cost = t["frame_ms_64spp"] / u["frame_ms_64spp"]
     out["tree_cost_per_sample"] = round(cost, 3)
     out["equal_time_gain"] = round(u["relmse"] / (t["relmse"] * cost), 3)
     out["equal_time_gain_trimmed"] = round(u["relmse_trimmed"] / (t["relmse_trimmed"] * cost), 3)
-    out["workload"] = ("1024-instance cloud, 32 point lights + gradient sky, 8 bounces; relMSE at 480x270 x %d spp "
-                       "vs the %d-spp FP64 oracle, %d seeds (median)" % (LT_SPP, args.oracle_spp, LT_SEEDS))
+    out["workload"] = ("1024-instance cloud, 32 point lights + gradient sky, 1920x1080, 8 bounces; relMSE of a "
+                       "%d-spp frame vs the %d-spp FP64 oracle (its own variance taken out), %d seeds (median)"
+                       % (LT_SPP, args.oracle_spp, LT_SEEDS))
     out["metric"] = "equal_time_gain = (relMSE x frame ms) uniform / tree; > 1: the tree wins"
     return out
 
 
 def run_nrc(args, dev, local, barrier):
-    """Equal-time relMSE, neural radiance cache vs plain path tracing, on the
-    1024-instance scene at 480x270 (a quarter of 1920x1080 per side, so that
-    the 65,536-spp FP64-accumulated oracle fits the run), 8 bounces, 16 spp per
-    frame, cache warmed by NRC_WARM frames of online training first; plus the
-    per-frame costs of both at 1920x1080 x 16 spp."""
-    import torch
+    """Neural radiance cache against plain path tracing on the 1024-instance
+    cloud at 1920x1080, 8 bounces, 16 spp per frame, from a cold start: each
+    arm is a fresh engine rendering NRC_FRAMES progressive frames, the NRC
+    arm's cache freshly initialised, training online every frame (4 Adam steps
+    x 65,536 samples), its first NRC_WARM frames plain path tracing while it
+    learns -- all of it charged to its device time.  NRC_SEEDS seeds (frame
+    seeds and cache initialisations); per budget (the NRC arm's device time
+    after 1, 2, 4, ... frames) the median over seeds of the accumulated image's
+    relMSE, plain interpolated to the same time; plus the steady-state
+    single-frame relMSE and frame costs."""
     from vitrum_b200 import scenes
     from vitrum_b200.engine import Engine
+    from vitrum_b200.nrc import NrcConfig
     sc, cam = scenes.instanced_cloud()
-    B = I_BOUNCES
-    ref, _, oracle_s = _cloud_oracle(args, local)
+    ref, rvar, oracle_s = _cloud_oracle(args, local)
 
-    def curve(nrc):
-        e = Engine(device=local, max_bounces=B, max_samples_per_pixel=1 << 20)
+    def arm(nrc, s):
+        e = Engine(device=local, max_bounces=I_BOUNCES, max_samples_per_pixel=1 << 20)
         e.set_scene(sc)
         if nrc:
-            e.set_nrc(prefix_bounces=1, train_steps=4, train_batch=65536)
-            for _ in range(NRC_WARM):
-                e.render_frame(cam, NRC_W, NRC_H, samples=NRC_SPP, frame_seed=7)
-            e.reset()
-        t, pts = 0.0, []
+            e.set_nrc(prefix_bounces=1, train_steps=4, train_batch=65536, warmup_frames=NRC_WARM,
+                      cache=NrcConfig(seed=s + 1))
+        t, curve, restart, frame_rel, frame_ms = 0.0, [], [], [], []
+        prev = np.zeros_like(ref)
+        since = np.zeros_like(ref)  # the frames since the cache took over (all frames for plain)
         for f in range(NRC_FRAMES):
-            e.render_frame(cam, NRC_W, NRC_H, samples=NRC_SPP, frame_seed=7)
-            t += e.stats()["last_frame_ms"]
-            pts.append((t, _relmse(e.capture_frame()[..., :3].astype(np.float64), ref)))
-        e.reset()
-        full = e.profile_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=8)
+            e.render_frame(cam, I_W, I_H, samples=NRC_SPP, frame_seed=(s + 1) << 12)
+            ms = e.stats()["last_frame_ms"]
+            t += ms
+            acc = e.capture_frame()[..., :3]
+            cur = acc * (f + 1) - prev  # this frame's own image
+            prev = acc * (f + 1)
+            first = NRC_WARM if nrc else 0
+            if f >= first:
+                since += cur
+                restart.append((t, _relmse(since / (f + 1 - first), ref, rvar)))
+            curve.append((t, _relmse(acc, ref, rvar)))
+            frame_rel.append(_relmse(cur, ref, rvar))
+            frame_ms.append(ms)
+        stages = e.profile_frame(cam, I_W, I_H, samples=NRC_SPP, frame_seed=(s + 1) << 12) if s == 0 else None
         e.dispose()
-        return pts, full
-
-    plain, plain_full = curve(False)
-    nrc, nrc_full = curve(True)
+        return curve, frame_rel, frame_ms, stages, restart
 
     def at(pts, t):  # relMSE of the accumulated image at device time t (log-linear interpolation)
         ts = [p[0] for p in pts]
         if t <= ts[0]:
-            return pts[0][1] * ts[0] / t  # fewer samples than one frame: variance ~ 1/time
+            return pts[0][1] * ts[0] / t  # less than one frame: variance ~ 1 / time
         for (ta, ra), (tb, rb) in zip(pts, pts[1:]):
             if t <= tb:
                 w = (t - ta) / (tb - ta)
-                return float(np.exp((1 - w) * np.log(ra) + w * np.log(rb)))
+                return float(np.exp((1 - w) * np.log(max(ra, 1e-12)) + w * np.log(max(rb, 1e-12))))
         return pts[-1][1] * ts[-1] / t
-    budgets = [nrc[k][0] for k in (0, 1, 3, 7)]
-    table = [{"ms": round(b, 2), "nrc": round(at(nrc, b), 5), "plain": round(at(plain, b), 5),
-              "ratio": round(at(plain, b) / at(nrc, b), 2)} for b in budgets]
+
+    runs = [(arm(False, s), arm(True, s)) for s in range(NRC_SEEDS)]
+    marks = [f for f in (1, 2, 4, 8, 16, 32, 64) if f <= NRC_FRAMES]
+    table, table_restart = [], []
+    for f in marks:
+        b = [nrc[0][f - 1][0] for _, nrc in runs]
+        rn = [nrc[0][f - 1][1] for _, nrc in runs]
+        rp = [at(plain[0], nrc[0][f - 1][0]) for plain, nrc in runs]
+        table.append({"frames": f, "ms": round(float(np.median(b)), 1), "nrc": round(float(np.median(rn)), 5),
+                      "plain": round(float(np.median(rp)), 5),
+                      "ratio": round(float(np.median([p / n for p, n in zip(rp, rn)])), 2)})
+        if f > NRC_WARM:
+            rn = [nrc[4][f - 1 - NRC_WARM][1] for _, nrc in runs]
+            table_restart.append({"frames": f, "ms": round(float(np.median(b)), 1),
+                                  "nrc": round(float(np.median(rn)), 5), "plain": round(float(np.median(rp)), 5),
+                                  "ratio": round(float(np.median([p / n for p, n in zip(rp, rn)])), 2)})
+    steady = slice(NRC_WARM + 16, NRC_FRAMES)
+    pf = {k: float(np.median([np.median(r[i][1][steady]) for r in runs])) for i, k in ((0, "plain"), (1, "nrc"))}
+    pm = {k: float(np.median([np.median(r[i][2][steady]) for r in runs])) for i, k in ((0, "plain"), (1, "nrc"))}
+    st_plain, st_nrc = runs[0][0][3], runs[0][1][3]
     return {
-        "workload": "1024-instance cloud, 480x270, 8 bounces, 16 spp per frame; NRC: hash grid 16 x 2^19 x 2 fp16 "
-                    "(base 16, growth 1.5), 64-input MLP 5 x 64 ReLU + 3, fp16/fp32-accumulate on tcgen05, 4 Adam "
-                    "steps x 65,536 samples per frame, 1-bounce prefix; cache warmed by %d frames" % NRC_WARM,
-        "oracle": {"spp": args.oracle_spp, "accumulation": "fp64", "seconds": round(oracle_s, 1)},
-        "metric": "relMSE = mean((x - ref)^2 / (ref^2 + 1e-2)) at equal device time",
+        "workload": "1024-instance cloud, 1920x1080, 8 bounces, 16 spp per frame, %d frames from a cold start, %d "
+                    "seeds; NRC: hash grid 16 x 2^19 x 2 fp16 (base 16, growth 1.5), 64-input MLP 5 x 64 ReLU + 3, "
+                    "fp16/fp32-accumulate on tcgen05, 4 Adam steps x 65,536 samples per frame, 1-bounce prefix, "
+                    "first %d frames plain while the cache trains (charged)" % (NRC_FRAMES, NRC_SEEDS, NRC_WARM),
+        "oracle": {"spp": args.oracle_spp, "accumulation": "fp64", "seconds": round(oracle_s, 1),
+                   "note": "its per-pixel variance of the mean is subtracted from every squared error"},
+        "metric": "relMSE = mean((x - ref)^2 / (ref^2 + 1e-2)) of the accumulated image at equal device time "
+                  "(median over seeds)",
         "equal_time": table,
-        "nrc_curve": [(round(t, 2), round(r, 5)) for t, r in nrc],
-        "plain_curve": [(round(t, 2), round(r, 5)) for t, r in plain],
-        "full_frame_1920x1080_16spp_ms": {"plain": round(plain_full["frame_ms"], 2),
-                                          "nrc": round(nrc_full["frame_ms"], 2),
-                                          "nrc_train_ms": round(nrc_full["nrc_train_ms"], 2),
-                                          "nrc_query_ms": round(nrc_full["nrc_query_ms"], 2)},
+        "equal_time_restart": table_restart,
+        "restart_note": "the NRC arm's image accumulated from the first cache frame on (the warm-up frames shown "
+                        "while the cache learns, their time still charged)",
+        "steady_frame": {"relmse_plain": round(pf["plain"], 5), "relmse_nrc": round(pf["nrc"], 5),
+                         "ms_plain": round(pm["plain"], 2), "ms_nrc": round(pm["nrc"], 2),
+                         "equal_time_gain": round(pf["plain"] * pm["plain"] / (pf["nrc"] * pm["nrc"]), 2),
+                         "frames": [steady.start, NRC_FRAMES]},
+        "full_frame_1920x1080_16spp_ms": {"plain": round(st_plain["frame_ms"], 2),
+                                          "nrc": round(st_nrc["frame_ms"], 2),
+                                          "nrc_train_ms": round(st_nrc["nrc_train_ms"], 2),
+                                          "nrc_query_ms": round(st_nrc["nrc_query_ms"], 2)},
     }
 
 
@@ -723,7 +767,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-light-tree", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--oracle-spp", type=int, default=65536)
+    ap.add_argument("--oracle-spp", type=int, default=16384)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = _env_rank()

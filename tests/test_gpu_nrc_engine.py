@@ -1,6 +1,7 @@
 """Path tracing with the neural radiance cache through the Engine: the cache
-changes nothing while it warms up, and a trained cache lowers the error of an
-equal-time frame against the 65,536-spp FP64-accumulated oracle."""
+changes nothing while it warms up, and from a cold start the cache's frames
+have at least 2x lower error than equal-time plain frames against the
+65,536-spp FP64-accumulated oracle."""
 import numpy as np
 import pytest
 
@@ -58,48 +59,54 @@ def test_nrc_options_validation(cuda):
 
 
 def test_trained_cache_lowers_equal_time_error(cuda):
-    """Eight frames after a warm-up of the cache (its training is online, every
-    frame): the NRC frames against plain path tracing given the same device
-    time, both against a 65,536-spp FP64-accumulated plain oracle, on the box
-    room (indirect light and caustics through the glass box dominate).  The
-    cache keeps training during the measured frames, so its output drifts a
-    little from frame to frame (a mean bias of up to ~4 % over four frames);
-    eight frames average that drift down.  Measured gains over eight frames:
-    1.7x to 2.4x lower relMSE; the bar below (1.33x) holds run to run."""
-    sc, cam = scenes.box_room(wall_cells=32, box_cells=16)
-    W, H, B = 192, 192, 5
+    """From a cold start (fresh cache, 8 plain warm-up frames while it trains,
+    online training every frame after that), the cache's frames against plain
+    path tracing given each frame's device time (training included), on the
+    cloud with 8 point lights, sky, metal and glass instances; both against a
+    65,536-spp FP64-accumulated oracle (whose own variance is taken out of the
+    squared error).  The steady-state frames (24 to 39) have at least 2x lower
+    relMSE than equal-time plain frames (median over the frames)."""
+    sc, cam = cloud()
+    W, H, B = 320, 180, 8
     o = Engine(max_bounces=B, oracle_accumulation=True, max_samples_per_pixel=1 << 17)
     o.set_scene(sc)
     for _ in range(16):
-        o.render_frame(cam, W, H, samples=4096, frame_seed=99)
-    ref, _ = o.capture_moments()
+        o.render_frame(cam, W, H, samples=4096, frame_seed=1 << 20)
+    ref, var = o.capture_moments()
     o.dispose()
+    ref_var = var / 65536
+
+    def rel(img):
+        return float(np.mean(((img - ref) ** 2 - ref_var) / (ref ** 2 + 1e-2)))
 
     n = Engine(max_bounces=B, max_samples_per_pixel=1 << 20)
     n.set_scene(sc)
-    n.set_nrc(prefix_bounces=1, cache=NrcConfig(levels=12, log2_table_size=16), **SMALL)
-    for _ in range(48):
-        n.render_frame(cam, W, H, samples=16, frame_seed=5)
-    n.reset()
-    t_nrc = 0.0
-    for _ in range(8):
-        n.render_frame(cam, W, H, samples=16, frame_seed=5)
-        t_nrc += n.stats()["last_frame_ms"]
-    e_nrc = relmse(n.capture_frame()[..., :3], ref)
+    n.set_nrc(prefix_bounces=1, warmup_frames=8, **SMALL)
+    e_nrc, t_nrc = [], []
+    for f in range(40):
+        n.reset()
+        n.render_frame(cam, W, H, samples=16, frame_seed=(1 << 12) + 16 * f)
+        if f >= 24:
+            t_nrc.append(n.stats()["last_frame_ms"])
+            e_nrc.append(rel(n.capture_frame()[..., :3]))
     n.dispose()
 
     p = Engine(max_bounces=B, max_samples_per_pixel=1 << 20)
     p.set_scene(sc)
-    p.render_frame(cam, W, H, samples=64, frame_seed=6)
-    t64 = p.stats()["last_frame_ms"]
-    spp = max(64, int(64 * t_nrc / t64))  # plain samples in the NRC frames' time
-    p.reset()
-    p.render_frame(cam, W, H, samples=spp, frame_seed=7)
-    e_plain = relmse(p.capture_frame()[..., :3], ref)
+    p.render_frame(cam, W, H, samples=16, frame_seed=2 << 12)
+    p.render_frame(cam, W, H, samples=16, frame_seed=2 << 12)
+    t16 = p.stats()["last_frame_ms"]
+    spp = max(1, int(round(16 * np.median(t_nrc) / t16)))  # plain samples in one cache frame's time
+    e_plain = []
+    for f in range(16):
+        p.reset()
+        p.render_frame(cam, W, H, samples=spp, frame_seed=(3 << 12) + 64 * f)
+        e_plain.append(rel(p.capture_frame()[..., :3]))
     p.dispose()
-    print(f"equal time ({t_nrc:.2f} ms): NRC 8 x 16 spp relMSE {e_nrc:.4f} vs plain {spp} spp {e_plain:.4f} "
-          f"({e_plain / e_nrc:.2f}x)")
-    assert e_nrc < 0.75 * e_plain
+    gain = np.median(e_plain) / np.median(e_nrc)
+    print(f"equal time ({np.median(t_nrc):.2f} ms per frame, plain {spp} spp vs 16 spp into the cache): relMSE "
+          f"NRC {np.median(e_nrc):.4f} plain {np.median(e_plain):.4f} ({gain:.2f}x)")
+    assert gain >= 2.0
 
 
 def test_error_fallback_tiles_keep_path_tracing(cuda):
