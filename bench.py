@@ -179,12 +179,18 @@ def cpu_pt_baseline(S, cam, spp=REF_SPP):
                               "sample": f"64x64 frame of the same camera, 4 spp ({nc1 + ns1} rays)"}}
 
 
+_QUERY_HITS = {}
+
+
 def cpu_query_baseline():
     """Config-1 closest-hit workload through the C restatement of shared-bvh
     (buildArrayBvh + 8-wide collapse, then the reference's FP64 LIFO first-hit
     query): build ms, and query Mrays/s on 1 thread and on all host cores, each
-    on a bounded slice of the 1,048,576 bench rays."""
+    on a bounded slice of the 1,048,576 bench rays.  The FP64 hits of that
+    slice also check the device's hits of the same rays (tie / edge / error
+    counts, as the parity tests classify them)."""
     import oracle
+    from oracle import parity
     from vitrum_b200 import scenes
     soup, _ = scenes.config1(Q_TRIS, 16, seed=Q_SEED)
     t0 = time.perf_counter()
@@ -198,9 +204,17 @@ def cpu_query_baseline():
     t3 = time.perf_counter()
     oracle.first_hit(w, soup.positions, rays[:n1], nthreads=1)
     t4 = time.perf_counter()
-    oracle.first_hit(w, soup.positions, rays[:nall], nthreads=threads)
+    ref = oracle.first_hit(w, soup.positions, rays[:nall], nthreads=threads)
     t5 = time.perf_counter()
+    check = None
+    if "hits" in _QUERY_HITS:
+        from vitrum_b200.bvh import HIT_DTYPE
+        dev_hits = _QUERY_HITS["hits"][:nall].view(HIT_DTYPE).reshape(-1)
+        rep = parity.classify(soup.positions, soup.indices, rays[:nall], dev_hits, ref[:3])
+        check = {k: rep[k] for k in ("n", "hits", "mismatches", "tie", "edge", "error")}
+        check["edge_margin_max"] = rep["edge_margin_max"]
     return {"value": nall / (t5 - t4) / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "parity_vs_fp64": check,
             "sample": f"first {nall} of the 1,048,576 bench rays on all cores; C restatement of shared-bvh "
                       "(binned SAH, greedy 8-wide collapse, FP64 LIFO first-hit query)",
             "single_thread": {"value": n1 / (t4 - t3) / 1e6, "unit": "Mrays/s", "cores": 1,
@@ -275,6 +289,8 @@ def run_query(args, dev, local, rank, world, barrier):
     barrier()
     per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
+    if rank == 0:
+        _QUERY_HITS["hits"] = d_hits[0].cpu().numpy()  # batch 0: the rays the CPU baseline re-traces
     pin = [torch.from_numpy(r).pin_memory() for r in host]
     pin_hits = torch.empty((Q_RAYS, 4), dtype=torch.int32).pin_memory()
     N.call("vt_bvh_trace_closest", g.handle, ctypes.c_void_p(pin[0].data_ptr()), Q_RAYS,
