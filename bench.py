@@ -646,6 +646,55 @@ def run_nrc(args, dev, local, barrier):
     }
 
 
+def run_build(args, dev, local):
+    """Scene builds (host wall clock, the second of two calls so that module
+    loading is not counted): the engine's set_scene with the trees built on the
+    GPU (binned-SAH binary tree, SAH-optimal 8-wide encoding, top level)
+    against the same words built on the host, for the box room and a
+    2,097,152-triangle room; and the reference-facing BVH build of the
+    65,536-triangle query soup (vt_bvh_build_device vs vt_bvh_build)."""
+    import torch
+    from vitrum_b200 import bvh as vb
+    from vitrum_b200 import scenes
+    from vitrum_b200.engine import Engine
+    out = {}
+
+    def scene_ms(sc, build):
+        e = Engine(device=local, max_bounces=2, scene_build=build)
+        ts = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            e.set_scene(sc)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        e.dispose()
+        return round(ts[-1], 1)
+
+    for name, sc in (("box_room_262146_tris", scenes.box_room()[0]),
+                     ("room_2097152_tris", scenes.box_room_sized(1 << 21)[0])):
+        out[name] = {"gpu_ms": scene_ms(sc, "gpu"), "host_ms": scene_ms(sc, "host"),
+                     "triangles": int(sc.triangle_count)}
+    soup, _ = scenes.config1(Q_TRIS, 16, seed=Q_SEED)
+    pos = np.ascontiguousarray(soup.positions, np.float32)
+    idx = np.ascontiguousarray(soup.indices, np.uint32)
+    dp = torch.from_numpy(pos.reshape(-1)).to(dev)
+    di = torch.from_numpy(idx.reshape(-1).view(np.int32)).to(dev)
+    g_ms, h_ms = [], []
+    for _ in range(2):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        g = vb.build_compressed_wide_bvh_device(dp.data_ptr(), dp.numel(), di.data_ptr(), di.numel(), device=local)
+        g_ms.append((time.perf_counter() - t0) * 1e3)
+        g.close()
+        t0 = time.perf_counter()
+        h = vb.build_compressed_wide_bvh(pos, idx, device=local)
+        h_ms.append((time.perf_counter() - t0) * 1e3)
+        h.close()
+    out["query_soup_65536_tris"] = {"gpu_ms": round(g_ms[-1], 1), "host_ms": round(h_ms[-1], 1),
+                                    "note": "reference options (4 per leaf, 16 bins, greedy collapse), incl. the "
+                                            "publication proofs on the host copy"}
+    return out
+
+
 # ------------------------------------------------------------------ path tracing workload
 def run_ours(args, rank, world, local):
     import torch
@@ -713,6 +762,7 @@ def run_ours(args, rank, world, local):
     instanced = run_instanced(args, dev, local, barrier) if solo and not args.no_instanced else None
     nrc = run_nrc(args, dev, local, barrier) if solo and not args.no_nrc else None
     light_tree = run_light_tree(args, dev, local, barrier) if solo and not args.no_light_tree else None
+    builds = run_build(args, dev, local) if solo and not args.no_build else None
     batch = run_batch(args, dev, local, barrier) if solo and not args.no_batch else None
 
     if rank == 0:
@@ -763,6 +813,7 @@ def run_ours(args, rank, world, local):
             "instanced": instanced,
             "nrc": nrc,
             "light_tree": light_tree,
+            "build": builds,
             "batch": batch,
         }
         print(json.dumps(line), flush=True)
@@ -782,6 +833,7 @@ def main():
     ap.add_argument("--no-nrc", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-light-tree", action="store_true")
+    ap.add_argument("--no-build", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--oracle-spp", type=int, default=16384)
     args = ap.parse_args()

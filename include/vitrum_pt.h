@@ -89,7 +89,10 @@ typedef struct vt_hit {
 vt_status vt_bvh_build(int32_t device, const float* positions, size_t position_words, const uint32_t* indices,
                        size_t index_words, const vt_bvh_build_options* options, vt_bvh** out_bvh);
 
-/* Same build from DEVICE arrays (no host round trip for the geometry). */
+/* Same build from DEVICE arrays, on the GPU: the binned-SAH binary tree (one
+ * CTA per node per level, every binCount the options allow) and its 8-wide
+ * encoding, word for word those of vt_bvh_build; the host receives copies for
+ * the publication proofs and the exports. */
 vt_status vt_bvh_build_device(int32_t device, const float* d_positions, size_t position_words,
                               const uint32_t* d_indices, size_t index_words, const vt_bvh_build_options* options,
                               void* cuda_stream, vt_bvh** out_bvh);
@@ -104,6 +107,13 @@ vt_status vt_bvh_get_info(const vt_bvh* bvh, vt_bvh_info* out_info);
  */
 vt_status vt_bvh_export_binary(const vt_bvh* bvh, uint32_t* nodes, size_t node_word_capacity,
                                uint32_t* reordered_to_source, size_t triangle_capacity);
+
+/* The published 8-wide nodes (20 words each) and triangle records (16 floats
+ * each) of this backend's own encoding (no reference counterpart; the
+ * reference's compressed nodes are a different layout).  Null buffers: only
+ * the sizes are written to out_words / out_floats. */
+vt_status vt_bvh_export_wide(const vt_bvh* bvh, uint32_t* node_words, size_t word_capacity, float* records,
+                             size_t float_capacity, size_t* out_words, size_t* out_floats);
 
 /*
  * Closest hit for n rays (replaces intersectCompressedWideBvhFirstHit,
@@ -264,6 +274,10 @@ typedef struct vt_engine_options {
                                      (shared-samplers/src/lightTree.ts: power x proximity x orientation) over the
                                      positional entries and the distant ones (directionals, environment) sharing
                                      n / (n + 1) of the selection evenly; 1 = uniform over the entries */
+  int32_t scene_build;            /* where setScene builds the trees: 0 = on the GPU (binned-SAH binary tree, SAH-
+                                     optimal 8-wide encoding and the instance top level); 1 = on the host (the same
+                                     words, the reference pipeline the GPU build is checked against).  Debug
+                                     engines also run the structural proofs on every tree they publish. */
 } vt_engine_options;
 
 /* Material (core MaterialSpec subset, core/src/scene/material.ts), the
@@ -582,6 +596,13 @@ vt_status vt_pick(vt_engine* engine, float x, float y, int32_t* out_triangle);
 /* The current scene's top-level tree (scenes with instances; VT_ERR_STATE
  * otherwise) in the reference layout of vt_tlas_build -- the tlasNodes and
  * tlasInstanceIndices buffers of packSceneFromCore (scenePack.ts:1104-1310). */
+/* The engine's device node array (20 words per wide node: bottom levels, then
+ * the top level) and triangle records (16 floats each) as they are on the GPU,
+ * copied back (no reference counterpart; for comparing the GPU and host scene
+ * builds).  Null buffers: only the sizes are written. */
+vt_status vt_engine_export_scene(const vt_engine* engine, uint32_t* node_words, size_t word_capacity, float* records,
+                                 size_t float_capacity, size_t* out_words, size_t* out_floats);
+
 vt_status vt_engine_export_tlas(const vt_engine* engine, uint32_t* nodes, size_t node_word_capacity,
                                 uint32_t* instance_indices, size_t instance_capacity, size_t* node_count);
 /* Closest hit of host rays against the engine's scene (vt_bvh_trace_closest

@@ -122,18 +122,25 @@ def test_adam_step_matches_oracle(cuda):
 
 
 def test_training_reduces_loss_and_generalises(cuda):
+    """300 Adam steps at learning rate 1e-2 on a smooth target.  The held-out
+    error is typically 1e-3 to 2e-3; an occasional late loss spike (Adam's
+    step at a high learning rate) lifts a single checkpoint about tenfold, so
+    the bar is on the median of the last three checkpoints."""
     cfg = NrcConfig(levels=8, log2_table_size=14, base_resolution=4, growth=1.5)
     c = RadianceCache(cfg)
-    first = None
+    held = training_samples(8192, 77)
+    first, rels, losses = None, [], []
     for step in range(300):
         loss = c.train_step(training_samples(4096, 1000 + step))
         first = loss if first is None else first
-    held = training_samples(8192, 77)
-    pred = c.query(held[:, :16])
-    rel = float(np.mean((pred - held[:, 16:19]) ** 2) / np.mean(held[:, 16:19] ** 2))
-    print(f"loss {first:.4f} -> {loss:.5f}; held-out relative MSE {rel:.4f}")
-    assert loss < 0.1 * first
-    assert rel < 0.02
+        if step in (279, 289, 299):
+            pred = c.query(held[:, :16])
+            rels.append(float(np.mean((pred - held[:, 16:19]) ** 2) / np.mean(held[:, 16:19] ** 2)))
+            losses.append(loss)
+    rel = float(np.median(rels))
+    print(f"loss {first:.4f} -> {losses}; held-out relative MSE at steps 280/290/300 {rels}")
+    assert np.median(losses) < 0.1 * first
+    assert rel < 0.01
     c.close()
 
 

@@ -96,6 +96,8 @@ SIGNATURES = {
     "vt_get_capabilities": [P, P],
     "vt_bake_preetham_sky": [P, I32, I32, P, SZ],
     "vt_capture_moments": [P, P, P, SZ],
+    "vt_engine_export_scene": [P, P, SZ, P, SZ, P, P],
+    "vt_bvh_export_wide": [P, P, SZ, P, SZ, P, P],
     "vt_capture_luminance_moments": [P, P, SZ],
     "vt_capture_aux": [P, I32, P, SZ],
     "vt_set_previous_camera": [P, P, P],

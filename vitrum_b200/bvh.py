@@ -88,6 +88,17 @@ class Bvh:
         N.call("vt_bvh_export_binary", self.handle, _ptr(nodes), nodes.size, _ptr(r2s), r2s.size)
         return nodes, r2s[: inf["triangle_count"]]
 
+    def export_wide(self):
+        """(node words uint32, 20 per 8-wide node; records float32, 16 per
+        triangle record) of this backend's published encoding."""
+        nw, nf = ctypes.c_size_t(), ctypes.c_size_t()
+        N.call("vt_bvh_export_wide", self.handle, None, 0, None, 0, ctypes.byref(nw), ctypes.byref(nf))
+        words = np.empty(nw.value, np.uint32)
+        recs = np.empty(nf.value, np.float32)
+        N.call("vt_bvh_export_wide", self.handle, _ptr(words), words.size, _ptr(recs), recs.size, ctypes.byref(nw),
+               ctypes.byref(nf))
+        return words, recs
+
     # ------------------------------------------------------------- queries
     def intersect_first_hit(self, rays: np.ndarray) -> np.ndarray:
         """Closest hit for host rays (n, 8) float32 -> structured (prim, t, u, v)."""

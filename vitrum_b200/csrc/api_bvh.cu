@@ -43,8 +43,9 @@ static BuildOptions resolve(const vt_bvh_build_options* o) {
   return r;
 }
 
-static void upload(vt_bvh* b, const float* positions, const uint32_t* indices) {
-  WideBvhHost w = encode_wide(b->binary, positions, b->opts.position_stride, indices, b->opts.index_stride);
+// Proves and publishes an encoded tree: the device arrays come from the GPU
+// encoder's output when there is one (dev), else from the host arrays.
+static void publish(vt_bvh* b, const WideBvhHost& w, const WideBvhDevice* dev) {
   // publication proofs (the reference validates every tree it publishes)
   validate_binary(b->binary, b->ntri);
   validate_wide(w.nodes.data(), w.nodes.size() / 20, w.tris.data(), w.tris.size() / 16, 0, (size_t)b->ntri, false,
@@ -52,8 +53,13 @@ static void upload(vt_bvh* b, const float* positions, const uint32_t* indices) {
   DeviceScope ds(b->device);
   b->nodes.resize(w.nodes.size() / 4);
   b->tris.resize(std::max<size_t>(w.tris.size() / 4, 1));
-  VT_CUDA(cudaMemcpy(b->nodes.ptr, w.nodes.data(), w.nodes.size() * 4, cudaMemcpyHostToDevice));
-  if (!w.tris.empty()) VT_CUDA(cudaMemcpy(b->tris.ptr, w.tris.data(), w.tris.size() * 4, cudaMemcpyHostToDevice));
+  const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  VT_CUDA(cudaMemcpy(b->nodes.ptr, dev ? (const void*)dev->nodes.ptr : w.nodes.data(), w.nodes.size() * 4, kind));
+  if (!w.tris.empty())
+    VT_CUDA(cudaMemcpy(b->tris.ptr, dev ? (const void*)dev->recs.ptr : w.tris.data(), w.tris.size() * 4, kind));
+  VT_CUDA(cudaDeviceSynchronize());  // the copies are complete before any stream of the caller's uses the tree
+  b->wide_host_nodes = w.nodes;
+  b->wide_host_recs = w.tris;
   b->status.resize(1);
   VT_CUDA(cudaMemset(b->status.ptr, 0, sizeof(int)));
   b->counter.resize(1);
@@ -69,7 +75,8 @@ static vt_bvh* build_host(int device, const float* positions, size_t pw, const u
   b->opts = resolve(options);
   b->binary = build_binary_host(positions, pw, indices, iw, b->opts);
   b->ntri = (int64_t)(iw / b->opts.index_stride);
-  upload(b.get(), positions, indices);
+  const WideBvhHost w = encode_wide(b->binary, positions, b->opts.position_stride, indices, b->opts.index_stride);
+  publish(b.get(), w, nullptr);
   b->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return b.release();
 }
@@ -143,21 +150,34 @@ vt_status vt_bvh_build_device(int32_t device, const float* d_positions, size_t p
     auto b = std::make_unique<vt_bvh>();
     b->device = device;
     b->opts = resolve(options);
-    // the binary tree is built on the GPU (binCount <= 16), the wide encoding on the host
-    if (b->opts.bins <= 16) {
-      b->binary = build_binary_gpu(d_positions, position_words, d_indices, index_words, b->opts, s);
-    }
-    std::vector<float> p(position_words);
-    std::vector<uint32_t> i(index_words);
-    if (position_words)
-      VT_CUDA(cudaMemcpyAsync(p.data(), d_positions, position_words * 4, cudaMemcpyDeviceToHost, s));
-    if (index_words) VT_CUDA(cudaMemcpyAsync(i.data(), d_indices, index_words * 4, cudaMemcpyDeviceToHost, s));
-    VT_CUDA(cudaStreamSynchronize(s));
-    if (b->opts.bins > 16) b->binary = build_binary_host(p.data(), position_words, i.data(), index_words, b->opts);
+    // the binary tree and its 8-wide encoding are built on the GPU (every binCount
+    // the options allow); the host receives copies for the publication proofs
+    BinaryBvhDevice bd;
+    b->binary = build_binary_gpu(d_positions, position_words, d_indices, index_words, b->opts, s, &bd);
     b->ntri = (int64_t)(index_words / b->opts.index_stride);
-    upload(b.get(), p.data(), i.data());
+    WideBvhDevice wd;
+    const WideBvhHost w = encode_wide_gpu(bd, d_positions, b->opts.position_stride, d_indices, b->opts.index_stride,
+                                          nullptr, 0, 0, nullptr, nullptr, s, &wd);
+    publish(b.get(), w, &wd);
     b->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     *out_bvh = b.release();
+  });
+}
+
+vt_status vt_bvh_export_wide(const vt_bvh* b, uint32_t* node_words, size_t word_capacity, float* records,
+                             size_t float_capacity, size_t* out_words, size_t* out_floats) {
+  return guard([&] {
+    if (!b) fail(VT_ERR_INVALID_ARGUMENT, "bvh is null");
+    if (out_words) *out_words = b->wide_host_nodes.size();
+    if (out_floats) *out_floats = b->wide_host_recs.size();
+    if (node_words) {
+      if (word_capacity < b->wide_host_nodes.size()) fail(VT_ERR_RANGE, "node buffer too small");
+      std::memcpy(node_words, b->wide_host_nodes.data(), b->wide_host_nodes.size() * 4);
+    }
+    if (records) {
+      if (float_capacity < b->wide_host_recs.size()) fail(VT_ERR_RANGE, "record buffer too small");
+      std::memcpy(records, b->wide_host_recs.data(), b->wide_host_recs.size() * 4);
+    }
   });
 }
 

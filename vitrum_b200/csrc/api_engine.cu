@@ -167,13 +167,22 @@ void upload(DeviceBuffer<T>& dst, const std::vector<T>& src, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------- scene
+static vt::SceneBuild scene_build_of(const vt_engine* e) {
+  vt::SceneBuild sb;
+  sb.gpu = e->opts.scene_build == 0;
+  sb.device = e->device;
+  sb.stream = e->stream;
+  sb.validate = e->opts.debug != 0;
+  return sb;
+}
+
 void set_scene(vt_engine* e, const vt_scene_desc* sc) {
   // Transactional replacement (the reference's staged upload with rollback,
   // pt-webgpu/src/scene/uploadSceneBuffers.ts, transactionalResourceReplacement.test.ts):
   // every device buffer of the new scene is allocated and filled first; only
   // when all of them succeeded do they replace the engine's, so a failure at
   // any stage leaves the previous scene and its image untouched.
-  vt::PackedScene p = vt::pack_scene(sc, 0, 0, e->opts.bvh_max_leaf);
+  vt::PackedScene p = vt::pack_scene(sc, 0, 0, e->opts.bvh_max_leaf, scene_build_of(e));
   cudaStream_t s = e->stream;
   struct Staged {
     DeviceBuffer<uint4> nodes;
@@ -298,13 +307,14 @@ void update_instances(vt_engine* e, const vt_instance_desc* insts, size_t n, boo
   vt::InstanceSet placed = vt::place_instances(insts, n, e->mats_host, e->blas_root, e->local_box);
   if (insts != e->inst_descs.data()) e->inst_descs.assign(insts, insts + n);
   vt::BinaryBvhHost tl;
+  const vt::SceneBuild sb = scene_build_of(e);
   if (rebuild) {
-    tl = vt::build_tlas_host(placed.aabbs.data(), n);
+    tl = vt::build_top_level(sb, placed.aabbs.data(), n);
   } else {
     tl = e->binary;
     vt::refit_tlas_host(tl, placed.aabbs.data(), n);
   }
-  vt::WideBvhHost tw = vt::encode_wide_tlas(tl, placed.recs.data(), e->tlas_root);
+  vt::WideBvhHost tw = vt::encode_top_level(sb, tl, placed.recs, e->tlas_root);
   cudaStream_t s = e->stream;
   VT_CUDA(cudaStreamSynchronize(s));
   e->drop_graphs();
@@ -355,7 +365,7 @@ void update_mesh(vt_engine* e, size_t m, const vt_mesh_desc* md, bool rebuild) {
   const uint32_t node1 = m + 1 < nm ? e->blas_root[m + 1] : e->tlas_root;
   const uint32_t rec1 = m + 1 < nm ? e->blas_rec_start[m + 1] : (uint32_t)(e->rec_host.size() / 16);
   const uint32_t old_tlas_root = e->tlas_root;
-  vt::BlasPack bp = vt::pack_blas(pos, idx, md->material, node0, rec0, e->opts.bvh_max_leaf);
+  vt::BlasPack bp = vt::pack_blas(pos, idx, md->material, node0, rec0, e->opts.bvh_max_leaf, scene_build_of(e));
   const int64_t dn = (int64_t)(bp.wide.nodes.size() / 20) - (int64_t)(node1 - node0);
   const int64_t dr = (int64_t)(bp.wide.tris.size() / 16) - (int64_t)(rec1 - rec0);
   if ((int64_t)e->rec_host.size() / 16 + dr + 32 >= (int64_t)0x40000000)
@@ -908,6 +918,7 @@ vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine*
     if (e->opts.bvh_max_leaf == 0) e->opts.bvh_max_leaf = vt::kEngineLeafDefault;
     if (e->opts.bvh_max_leaf < 1 || e->opts.bvh_max_leaf > 4) fail(VT_ERR_RANGE, "bvh_max_leaf must be in [0, 4]");
     if (e->opts.light_selection < 0 || e->opts.light_selection > 1) fail(VT_ERR_RANGE, "light_selection must be 0 or 1");
+    if (e->opts.scene_build < 0 || e->opts.scene_build > 1) fail(VT_ERR_RANGE, "scene_build must be 0 or 1");
     vt::DeviceScope ds(device);
     VT_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     VT_CUDA(cudaEventCreate(&e->ev0));
@@ -1178,6 +1189,27 @@ vt_status vt_pick(vt_engine* e, float x, float y, int32_t* out_triangle) {
       uint32_t id;
       std::memcpy(&id, &v0.w, 4);
       *out_triangle = (int32_t)id;
+    }
+  });
+}
+
+vt_status vt_engine_export_scene(const vt_engine* e, uint32_t* node_words, size_t word_capacity, float* records,
+                                 size_t float_capacity, size_t* out_words, size_t* out_floats) {
+  return vt::guard([&] {
+    if (!e) fail(VT_ERR_INVALID_ARGUMENT, "engine is null");
+    if (!e->has_scene) fail(VT_ERR_STATE, "export before setScene");
+    vt::DeviceScope ds(e->device);
+    const size_t nw = e->nodes.count * 4, nf = e->tris.count * 4;
+    if (out_words) *out_words = nw;
+    if (out_floats) *out_floats = nf;
+    VT_CUDA(cudaStreamSynchronize(e->stream));
+    if (node_words) {
+      if (word_capacity < nw) fail(VT_ERR_RANGE, "node buffer too small");
+      VT_CUDA(cudaMemcpy(node_words, e->nodes.ptr, nw * 4, cudaMemcpyDeviceToHost));
+    }
+    if (records) {
+      if (float_capacity < nf) fail(VT_ERR_RANGE, "record buffer too small");
+      VT_CUDA(cudaMemcpy(records, e->tris.ptr, nf * 4, cudaMemcpyDeviceToHost));
     }
   });
 }

@@ -4,14 +4,15 @@
 //
 // Top down, one level of the tree per launch, one CTA per node of the level:
 //   1. node bounds and centroid bounds (CTA reduction);
-//   2. per axis with centroid span > 1e-9: 16 bins (count + bounds) in per-warp
-//      shared-memory copies merged by the CTA, prefix / suffix sweeps with the
-//      prefix bounds rounded to f32 as the reference stores them, SAH cost;
+//   2. per axis with centroid span > 1e-9: up to 256 bins (count + bounds) in
+//      shared memory, bounds kept as order-preserving 64-bit keys updated with
+//      atomic min / max (exact and order-free), prefix / suffix sweeps with the
+//      bounds rounded to f32 as the reference stores them, SAH cost;
 //   3. stable partition of the node's index range by bin <= split (CTA scan,
 //      chunk by chunk, through a scratch range), or the balanced fallback:
 //      sort by (centroid on the widest axis, triangle index) -- bitonic in
-//      shared memory up to 4096 triangles, on the host beyond -- and split at
-//      count / 2;
+//      shared memory up to 4096 triangles, two stable device radix passes
+//      (index, then centroid) beyond -- and split at count / 2;
 //   4. children appended to the next level's list.
 // Bounds are minima / maxima (exact, order-free: -0 wins a min tie, +0 a max
 // tie, as in JS Math.min / Math.max), every other operation is a single
@@ -28,6 +29,8 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "bvh_host.h"
 #include "vt_common.h"
 
@@ -37,7 +40,7 @@ namespace {
 
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxBins = 16;        // the GPU path builds with binCount <= 16
+constexpr int kMaxBins = 256;       // binCount in [2, 256], as the options allow
 constexpr int kSortMax = 4096;      // fallback sorts up to this many in shared memory
 
 struct GNode {
@@ -46,7 +49,7 @@ struct GNode {
   int32_t axis;                     // split axis, -1 leaf
   uint32_t size, pre;               // subtree node count, preorder index
   float mn[3], mx[3];
-  int32_t host_sort;                // 1: the fallback sort of this node is done by the host
+  int32_t big_sort;                 // 1: the fallback sort of this node runs as device radix passes
   int32_t pad;
 };
 
@@ -69,30 +72,15 @@ __device__ __forceinline__ int bin_of(double c, double cmin, double span, int bi
   return f < (double)(bins - 1) ? (int)f : bins - 1;
 }
 
-// shared-memory min / max of doubles through 64-bit CAS (JS tie rules)
-__device__ __forceinline__ void smin(double* p, double v) {
-  unsigned long long* a = reinterpret_cast<unsigned long long*>(p);
-  unsigned long long old = *a;
-  while (true) {
-    const double o = __longlong_as_double((long long)old);
-    const double n = jmin(o, v);
-    if (__double_as_longlong(n) == (long long)old) return;
-    const unsigned long long got = atomicCAS(a, old, (unsigned long long)__double_as_longlong(n));
-    if (got == old) return;
-    old = got;
-  }
+// Order-preserving 64-bit key of a double: key(a) < key(b) iff a < b, and
+// key(-0) < key(+0), so an integer min / max follows the JS tie rules (-0
+// wins a min tie, +0 a max tie).
+__device__ __forceinline__ unsigned long long okey(double d) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
-__device__ __forceinline__ void smax(double* p, double v) {
-  unsigned long long* a = reinterpret_cast<unsigned long long*>(p);
-  unsigned long long old = *a;
-  while (true) {
-    const double o = __longlong_as_double((long long)old);
-    const double n = jmax(o, v);
-    if (__double_as_longlong(n) == (long long)old) return;
-    const unsigned long long got = atomicCAS(a, old, (unsigned long long)__double_as_longlong(n));
-    if (got == old) return;
-    old = got;
-  }
+__device__ __forceinline__ double okey_value(unsigned long long k) {
+  return __longlong_as_double((long long)((k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k));
 }
 
 // Triangle bounds and centroids in double from the f32 vertices.
@@ -119,11 +107,13 @@ __global__ void k_prep(const float* __restrict__ pos, int ps, size_t nvert, cons
 
 struct Shared {
   double red[kWarps][12];                        // CTA reduction of node / centroid bounds
-  double bmn[kWarps][kMaxBins][3], bmx[kWarps][kMaxBins][3];
-  unsigned int bc[kWarps][kMaxBins];
+  unsigned long long bmn[kMaxBins][3], bmx[kMaxBins][3];  // bin bounds as okey()s
+  unsigned int bc[kMaxBins];
+  float smn[kMaxBins][3], smx[kMaxBins][3];      // suffix bounds (f32, as stored)
+  int sc[kMaxBins];
   double nb[12];                                 // node bounds (6) + centroid bounds (6)
   double best_cost;
-  int best_axis, best_split, nl, decision;       // decision: 0 leaf, 1 SAH split, 2 fallback, 3 host fallback
+  int best_axis, best_split, nl, decision;       // decision: 0 leaf, 1 SAH split, 2 fallback, 3 large fallback
   unsigned int scan[kWarps + 1];
 };
 
@@ -162,73 +152,57 @@ __device__ void cta_bounds(const double* tb, const double* cen, const uint32_t* 
   __syncthreads();
 }
 
-// Bins of one axis into S (per-warp copies, merged into warp slot 0).
+// Bins of one axis into S.
 __device__ void cta_bins(const double* tb, const double* cen, const uint32_t* A, uint32_t b, uint32_t c, int axis,
                          double cmin, double span, int bins, Shared& S) {
-  const int w = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < kWarps * kMaxBins; i += blockDim.x) {
-    const int q = i / kMaxBins, j = i % kMaxBins;
-    S.bc[q][j] = 0;
-    for (int k = 0; k < 3; ++k) { S.bmn[q][j][k] = INFINITY; S.bmx[q][j][k] = -INFINITY; }
+  for (int j = threadIdx.x; j < bins; j += blockDim.x) {
+    S.bc[j] = 0;
+    for (int k = 0; k < 3; ++k) { S.bmn[j][k] = okey(INFINITY); S.bmx[j][k] = okey(-INFINITY); }
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
     const uint32_t t = A[b + i];
     const int j = bin_of(cen[3 * (size_t)t + axis], cmin, span, bins);
-    atomicAdd(&S.bc[w][j], 1u);
+    atomicAdd(&S.bc[j], 1u);
     for (int k = 0; k < 3; ++k) {
-      smin(&S.bmn[w][j][k], tb[6 * (size_t)t + k]);
-      smax(&S.bmx[w][j][k], tb[6 * (size_t)t + 3 + k]);
+      atomicMin(&S.bmn[j][k], okey(tb[6 * (size_t)t + k]));
+      atomicMax(&S.bmx[j][k], okey(tb[6 * (size_t)t + 3 + k]));
     }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < bins; i += blockDim.x) {
-    unsigned int cnt = S.bc[0][i];
-    double lo[3] = {S.bmn[0][i][0], S.bmn[0][i][1], S.bmn[0][i][2]};
-    double hi[3] = {S.bmx[0][i][0], S.bmx[0][i][1], S.bmx[0][i][2]};
-    for (int q = 1; q < kWarps; ++q) {
-      cnt += S.bc[q][i];
-      for (int k = 0; k < 3; ++k) { lo[k] = jmin(lo[k], S.bmn[q][i][k]); hi[k] = jmax(hi[k], S.bmx[q][i][k]); }
-    }
-    S.bc[0][i] = cnt;
-    for (int k = 0; k < 3; ++k) { S.bmn[0][i][k] = lo[k]; S.bmx[0][i][k] = hi[k]; }
   }
   __syncthreads();
 }
 
-// Sweeps and costs of one axis (thread 0), updating the best split.
+// Sweeps and costs of one axis (thread 0), updating the best split: the
+// suffix sweep into shared memory, then the prefix sweep beside the costs.
 __device__ void choose(int axis, int bins, double parent_sa, Shared& S) {
-  float pmn[kMaxBins][3], pmx[kMaxBins][3], smn[kMaxBins][3], smx[kMaxBins][3];
-  int pc[kMaxBins], sc[kMaxBins];
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   int c = 0;
-  for (int i = 0; i < bins; ++i) {
+  for (int i = bins - 1; i >= 0; --i) {
     for (int k = 0; k < 3; ++k) {
-      lo[k] = jmin(lo[k], S.bmn[0][i][k]);
-      hi[k] = jmax(hi[k], S.bmx[0][i][k]);
-      pmn[i][k] = (float)lo[k];
-      pmx[i][k] = (float)hi[k];
+      lo[k] = jmin(lo[k], okey_value(S.bmn[i][k]));
+      hi[k] = jmax(hi[k], okey_value(S.bmx[i][k]));
+      S.smn[i][k] = (float)lo[k];
+      S.smx[i][k] = (float)hi[k];
     }
-    c += (int)S.bc[0][i];
-    pc[i] = c;
+    c += (int)S.bc[i];
+    S.sc[i] = c;
   }
   for (int k = 0; k < 3; ++k) { lo[k] = INFINITY; hi[k] = -INFINITY; }
   c = 0;
-  for (int i = bins - 1; i >= 0; --i) {
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = jmin(lo[k], S.bmn[0][i][k]);
-      hi[k] = jmax(hi[k], S.bmx[0][i][k]);
-      smn[i][k] = (float)lo[k];
-      smx[i][k] = (float)hi[k];
-    }
-    c += (int)S.bc[0][i];
-    sc[i] = c;
-  }
   for (int s = 0; s < bins - 1; ++s) {
-    const int lc = pc[s], rc = sc[s + 1];
+    float pmn[3], pmx[3];
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = jmin(lo[k], okey_value(S.bmn[s][k]));
+      hi[k] = jmax(hi[k], okey_value(S.bmx[s][k]));
+      pmn[k] = (float)lo[k];
+      pmx[k] = (float)hi[k];
+    }
+    c += (int)S.bc[s];
+    const int lc = c, rc = S.sc[s + 1];
     if (lc == 0 || rc == 0) continue;
-    const double lsa = half_sa(pmn[s][0], pmn[s][1], pmn[s][2], pmx[s][0], pmx[s][1], pmx[s][2]);
-    const double rsa = half_sa(smn[s + 1][0], smn[s + 1][1], smn[s + 1][2], smx[s + 1][0], smx[s + 1][1], smx[s + 1][2]);
+    const double lsa = half_sa(pmn[0], pmn[1], pmn[2], pmx[0], pmx[1], pmx[2]);
+    const double rsa = half_sa(S.smn[s + 1][0], S.smn[s + 1][1], S.smn[s + 1][2], S.smx[s + 1][0], S.smx[s + 1][1],
+                               S.smx[s + 1][2]);
     const double num = __dadd_rn(__dmul_rn(lsa, (double)lc), __dmul_rn(rsa, (double)rc));
     const double cost = parent_sa > 0 ? __ddiv_rn(num, parent_sa) : num;
     if (cost < S.best_cost) {
@@ -343,7 +317,7 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
     }
     N.left = N.right = -1;
     N.axis = -1;
-    N.host_sort = 0;
+    N.big_sort = 0;
     S.best_cost = INFINITY;
     S.best_axis = 0;
     S.best_split = 0;
@@ -389,7 +363,7 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
   if (threadIdx.x == 0) {
     N.axis = ax;
     if (S.decision == 3) {
-      N.host_sort = 1;
+      N.big_sort = 1;
       atomicOr(&counters[3], 1);
     }
     const int l = atomicAdd(&counters[0], 2);
@@ -425,6 +399,18 @@ __global__ void k_preorder(GNode* nodes, const int32_t* level, int n) {
   nodes[N.right].pre = N.pre + 1 + nodes[N.left].size;
 }
 
+// Keys of the large fallback sort: -0 canonicalised to +0 (the reference's
+// comparator subtracts, so equal centroids tie and fall to the index), then
+// mapped to order-preserving integers.
+__global__ void k_sort_keys(const double* __restrict__ cen, const uint32_t* __restrict__ A, uint32_t c, int axis,
+                            unsigned long long* __restrict__ keys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c) return;
+  double v = cen[3 * (size_t)A[i] + axis];
+  if (v == 0.0) v = 0.0;
+  keys[i] = okey(v);
+}
+
 __global__ void k_emit(const GNode* nodes, int n, BinaryNode* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -443,10 +429,26 @@ __global__ void k_emit(const GNode* nodes, int n, BinaryNode* out) {
 
 }  // namespace
 
+// Sorts A[0, c) by (cen[axis], index) with two stable device radix passes.
+static void sort_segment_device(const double* cen, uint32_t* A, uint32_t c, int axis, cudaStream_t s) {
+  DeviceBuffer<uint32_t> a2(c);
+  DeviceBuffer<unsigned long long> k1(c), k2(c);
+  size_t t1 = 0, t2 = 0;
+  VT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, t1, A, a2.ptr, (int)c, 0, 32, s));
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, k1.ptr, k2.ptr, a2.ptr, A, (int)c, 0, 64, s));
+  DeviceBuffer<unsigned char> tmp(std::max(t1, t2));
+  size_t tb = tmp.count;
+  VT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.ptr, tb, A, a2.ptr, (int)c, 0, 32, s));  // by index
+  k_sort_keys<<<(c + 255) / 256, 256, 0, s>>>(cen, a2.ptr, c, axis, k1.ptr);
+  VT_CUDA(cudaGetLastError());
+  tb = tmp.count;
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, k1.ptr, k2.ptr, a2.ptr, A, (int)c, 0, 64, s));  // stable
+  VT_CUDA(cudaStreamSynchronize(s));
+}
+
 BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const uint32_t* d_idx, size_t index_words,
-                               const BuildOptions& o, cudaStream_t s) {
+                               const BuildOptions& o, cudaStream_t s, BinaryBvhDevice* keep) {
   validate_options(o);
-  if (o.bins > kMaxBins) fail(VT_ERR_RANGE, "the GPU build supports binCount <= 16");
   if (position_words % o.position_stride) fail(VT_ERR_RANGE, "positions.length must be divisible by positionStride");
   if (index_words % o.index_stride) fail(VT_ERR_RANGE, "indices.length must be divisible by indexStride");
   const size_t ntri = index_words / o.index_stride;
@@ -511,43 +513,41 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
                              std::to_string(o.max_leaf));
     }
     if (cnt[3]) {
-      // fallback sorts of nodes too large for the shared-memory sort, on the host (rare)
-      std::vector<GNode> hn(cnt[0]);
-      VT_CUDA(cudaMemcpy(hn.data(), nodes.ptr, sizeof(GNode) * cnt[0], cudaMemcpyDeviceToHost));
-      std::vector<double> hc(3 * ntri);
-      VT_CUDA(cudaMemcpy(hc.data(), cen.ptr, hc.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      // fallback sorts of nodes too large for the shared-memory sort (rare): device radix passes
       for (int32_t idn : cur) {
-        const GNode& N = hn[idn];
-        if (!N.host_sort) continue;
-        std::vector<uint32_t> seg(N.count);
-        VT_CUDA(cudaMemcpy(seg.data(), A.ptr + N.begin, N.count * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        const int ax = N.axis;
-        std::sort(seg.begin(), seg.end(), [&](uint32_t a, uint32_t b) {
-          const double d = hc[3 * (size_t)a + ax] - hc[3 * (size_t)b + ax];
-          return d != 0 ? d < 0 : a < b;
-        });
-        VT_CUDA(cudaMemcpy(A.ptr + N.begin, seg.data(), N.count * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        GNode N;
+        VT_CUDA(cudaMemcpyAsync(&N, nodes.ptr + idn, sizeof N, cudaMemcpyDeviceToHost, s));
+        VT_CUDA(cudaStreamSynchronize(s));
+        if (N.big_sort) sort_segment_device(cen.ptr, A.ptr + N.begin, N.count, N.axis, s);
       }
       VT_CUDA(cudaMemsetAsync(counters.ptr + 3, 0, sizeof(int), s));
     }
     std::vector<int32_t> next(cnt[1]);
-    if (cnt[1]) VT_CUDA(cudaMemcpy(next.data(), nx->ptr, cnt[1] * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (cnt[1]) {
+      VT_CUDA(cudaMemcpyAsync(next.data(), nx->ptr, cnt[1] * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      VT_CUDA(cudaStreamSynchronize(s));
+    }
     std::swap(in, nx);
     cur = std::move(next);
   }
   int total = 0;
-  VT_CUDA(cudaMemcpy(&total, counters.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+  VT_CUDA(cudaMemcpyAsync(&total, counters.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VT_CUDA(cudaStreamSynchronize(s));
   // subtree sizes bottom-up, preorder indices top-down
   DeviceBuffer<int32_t> ids;
   for (int L = (int)levels.size() - 1; L >= 0; --L) {
     ids.resize(levels[L].size());
-    VT_CUDA(cudaMemcpy(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    // on the build's stream: a plain copy from pageable memory can return before
+    // it lands, and a kernel on a non-blocking stream would not wait for it
+    VT_CUDA(cudaMemcpyAsync(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     k_sizes<<<(unsigned)((levels[L].size() + 255) / 256), 256, 0, s>>>(nodes.ptr, ids.ptr, (int)levels[L].size());
     VT_CUDA(cudaStreamSynchronize(s));
   }
   for (size_t L = 0; L < levels.size(); ++L) {
     ids.resize(levels[L].size());
-    VT_CUDA(cudaMemcpy(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    // on the build's stream: a plain copy from pageable memory can return before
+    // it lands, and a kernel on a non-blocking stream would not wait for it
+    VT_CUDA(cudaMemcpyAsync(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     k_preorder<<<(unsigned)((levels[L].size() + 255) / 256), 256, 0, s>>>(nodes.ptr, ids.ptr, (int)levels[L].size());
     VT_CUDA(cudaStreamSynchronize(s));
   }
@@ -561,6 +561,12 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
   VT_CUDA(cudaStreamSynchronize(s));
   // deepest internal node: the last level holds only leaves
   out.depth = levels.size() >= 2 ? (int)levels.size() - 2 : 0;
+  if (keep) {
+    keep->nodes = std::move(dout);
+    keep->order = std::move(A);
+    keep->n_nodes = (size_t)total;
+    keep->ntri = ntri;
+  }
   return out;
 }
 

@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "bvh_exact.h"
 #include "bvh_host.h"
 
 namespace vt {
@@ -217,22 +218,14 @@ static bool reference_normal(const float a[3], const float b[3], const float c[3
   return true;
 }
 
-// Grid corners origin + q * 2^e compared exactly: in 113-bit arithmetic the sum
-// of an f32 origin (24 bits) and q * 2^e (8 bits) is exact unless the two are
-// more than 2^88 apart in magnitude (a box whose extent is below 2^-88 of its
-// coordinates), where the traversal's slab slack of 8 f32 ulps covers it.
-static inline __float128 corner(float origin, int q, int e) {
-  return (__float128)origin + (__float128)std::ldexp((double)q, e);
-}
-
-// Smallest e with origin + 255 * 2^e >= hi (exactly), clamped to the normal range.
+// Smallest e with origin + 255 * 2^e >= hi (exactly, corner_sign), clamped to the normal range.
 static int grid_exponent(float origin, float hi) {
   const double extent = (double)hi - (double)origin;
   if (!(extent > 0)) return -126;
   int e;
   std::frexp(extent / 255.0, &e);  // extent/255 = m * 2^e, m in [0.5, 1)
   while (e > -126 && std::ldexp(255.0, e - 1) >= extent) --e;
-  while (e < 127 && corner(origin, 255, e) < (__float128)hi) ++e;
+  while (e < 127 && corner_sign(origin, 255, e, hi) < 0) ++e;
   return std::min(127, std::max(-126, e));
 }
 
@@ -309,8 +302,8 @@ static WideBvhHost encode_core(const BinaryBvhHost& bin, const BinaryNode* nodes
         int ql = (int)std::min(255.0, std::max(0.0, lo));
         int qh = (int)std::min(255.0, std::max(0.0, hi));
         // outward exactly: (c - p) / step rounds when c is tiny next to p
-        while (ql > 0 && corner(p[k], ql, ex[k]) > (__float128)c.mn[k]) --ql;
-        while (qh < 255 && corner(p[k], qh, ex[k]) < (__float128)c.mx[k]) ++qh;
+        while (ql > 0 && corner_sign(p[k], ql, ex[k], c.mn[k]) > 0) --ql;
+        while (qh < 255 && corner_sign(p[k], qh, ex[k], c.mx[k]) < 0) ++qh;
         qlo[k * 8 + s] = (uint8_t)ql;
         qhi[k * 8 + s] = (uint8_t)qh;
       }

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "bvh_types.h"
+#include "vt_common.h"
 
 namespace vt {
 
@@ -56,9 +57,17 @@ struct WideProof {
 WideProof validate_wide(const uint32_t* nodes, size_t n_nodes, const float* recs, size_t n_recs, uint32_t root,
                         size_t n_items, bool instance_records, int stack_cap, uint32_t node_base = 0,
                         uint32_t rec_base = 0);
-// The same tree built on the GPU from device positions / indices (binCount <= 16).
+// Device copies of a binary tree: nodes in preorder and the BVH-order
+// triangle permutation (reordered_to_source).
+struct BinaryBvhDevice {
+  DeviceBuffer<BinaryNode> nodes;
+  DeviceBuffer<uint32_t> order;
+  size_t n_nodes = 0, ntri = 0;
+};
+// The same tree built on the GPU from device positions / indices; with keep,
+// its device arrays are handed over for a device encoding.
 BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const uint32_t* d_idx, size_t index_words,
-                               const BuildOptions& o, cudaStream_t s);
+                               const BuildOptions& o, cudaStream_t s, BinaryBvhDevice* keep = nullptr);
 
 // Binned-SAH binary build on host arrays (throws vt::Error).
 BinaryBvhHost build_binary_host(const float* positions, size_t position_words, const uint32_t* indices,
@@ -73,6 +82,22 @@ struct WideCollapse {
   double c_node = 1.0;
   double c_tri = 0.5;
 };
+
+// Device copies of an encoded tree: 20 words per wide node, 16 floats per record.
+struct WideBvhDevice {
+  DeviceBuffer<uint32_t> nodes;
+  DeviceBuffer<float> recs;
+  size_t n_nodes = 0, n_recs = 0;
+};
+// encode_wide on the GPU from a device binary tree (bvh_encode_gpu.cu): the
+// same node words and records.  Triangle records from d_pos / d_idx (and
+// d_tri_mat), or, with d_inst_recs (16 floats per instance), a top level's
+// instance records; sah == nullptr: the reference's greedy collapse.  The
+// result is returned on the host; with keep also kept on the device.
+WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int pos_stride, const uint32_t* d_idx,
+                            int idx_stride, const uint32_t* d_tri_mat, uint32_t node_base, uint32_t rec_base,
+                            const WideCollapse* sah, const float* d_inst_recs, cudaStream_t s,
+                            WideBvhDevice* keep = nullptr);
 
 // tri_materials (optional, one per source triangle) is stored in each record's v1.w.
 // node_base / rec_base offset the encoded indices for trees concatenated into shared arrays.
@@ -96,6 +121,11 @@ static_assert(sizeof(InstanceRecord) == 64, "instance record is 64 bytes");
 // (shared-bvh/src/tlas.ts:859-989): aabbs = 6 doubles per instance.
 BinaryBvhHost build_tlas_host(const double* aabbs, size_t n, int max_leaf = 1, int bins = 16,
                               int max_depth = kMaxBinaryDepth);
+
+// The same top level built on the GPU (tlas_build_gpu.cu), word for word; with
+// keep, its device arrays are handed over for a device encoding.
+BinaryBvhHost build_tlas_gpu(const double* aabbs, size_t n, int max_leaf, int bins, int max_depth, cudaStream_t s,
+                             BinaryBvhDevice* keep = nullptr);
 
 // Wide encoding of a TLAS: leaf payload records are InstanceRecords.
 WideBvhHost encode_wide_tlas(const BinaryBvhHost& tlas, const InstanceRecord* instances, uint32_t node_base);

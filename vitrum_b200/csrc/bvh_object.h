@@ -1,6 +1,8 @@
 // bvh_object.h -- the vt_bvh object behind the C ABI handle.
 #pragma once
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -16,6 +18,8 @@ struct vt_bvh {
   vt::DeviceBuffer<float4> tris;         // triangle records
   vt::DeviceBuffer<int> status;          // traversal status word
   vt::DeviceBuffer<unsigned long long> counter;  // persistent-kernel ray counter (calls on one bvh are serialised)
+  std::vector<uint32_t> wide_host_nodes;  // the published 8-wide nodes and records (host copies, for export)
+  std::vector<float> wide_host_recs;
   int64_t ntri = 0;
   int64_t wide_count = 0;
   int wide_depth = 0;

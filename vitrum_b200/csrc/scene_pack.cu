@@ -186,26 +186,81 @@ void append_mesh(const vt_mesh_desc& md, size_t m, size_t material_count, std::v
   }
 }
 
-BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& idx, uint32_t material,
-                   uint32_t node_base, uint32_t rec_base, int max_leaf) {
+// The engine's tree over vertices pos (4 floats each) and triangles idx (4
+// u32 each): the binned-SAH build and the SAH-optimal 8-wide encoding, on the
+// GPU or on the host (the same words either way).
+static void build_tree(const SceneBuild& sb, const std::vector<float>& pos, const std::vector<uint32_t>& idx,
+                       const uint32_t* tri_mat, uint32_t node_base, uint32_t rec_base, int max_leaf,
+                       BinaryBvhHost& bin, WideBvhHost& wide) {
   BuildOptions bo;
   bo.max_leaf = max_leaf;
   bo.bins = kEngineBins;
   const size_t ntri = idx.size() / 4;
+  if (sb.gpu) {
+    DeviceScope ds(sb.device);
+    DeviceBuffer<float> dpos(std::max<size_t>(pos.size(), 1));
+    DeviceBuffer<uint32_t> didx(std::max<size_t>(idx.size(), 1)), dmat(std::max<size_t>(ntri, 1));
+    if (!pos.empty()) VT_CUDA(cudaMemcpyAsync(dpos.ptr, pos.data(), pos.size() * 4, cudaMemcpyHostToDevice, sb.stream));
+    if (!idx.empty()) VT_CUDA(cudaMemcpyAsync(didx.ptr, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, sb.stream));
+    if (ntri && tri_mat) VT_CUDA(cudaMemcpyAsync(dmat.ptr, tri_mat, ntri * 4, cudaMemcpyHostToDevice, sb.stream));
+    BinaryBvhDevice bd;
+    bin = build_binary_gpu(dpos.ptr, pos.size(), didx.ptr, idx.size(), bo, sb.stream, &bd);
+    wide = encode_wide_gpu(bd, dpos.ptr, 4, didx.ptr, 4, tri_mat ? dmat.ptr : nullptr, node_base, rec_base,
+                           &kEngineCollapse, nullptr, sb.stream);
+  } else {
+    bin = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
+    wide = encode_wide(bin, pos.data(), 4, idx.data(), 4, tri_mat, node_base, rec_base, &kEngineCollapse);
+  }
+  if (sb.validate) {
+    validate_binary(bin, (int64_t)ntri);
+    validate_wide(wide.nodes.data(), wide.nodes.size() / 20, wide.tris.data(), wide.tris.size() / 16, node_base, ntri,
+                  false, kTraversalStack, node_base, rec_base);
+  }
+}
+
+BinaryBvhHost build_top_level(const SceneBuild& sb, const double* aabbs, size_t n) {
+  if (!sb.gpu) return build_tlas_host(aabbs, n);
+  DeviceScope ds(sb.device);
+  return build_tlas_gpu(aabbs, n, 1, 16, kMaxBinaryDepth, sb.stream);
+}
+
+WideBvhHost encode_top_level(const SceneBuild& sb, const BinaryBvhHost& tl, const std::vector<InstanceRecord>& recs,
+                             uint32_t root) {
+  if (!sb.gpu) return encode_wide_tlas(tl, recs.data(), root);
+  DeviceScope ds(sb.device);
+  BinaryBvhDevice bd;
+  bd.n_nodes = tl.nodes.size();
+  bd.ntri = tl.reordered_to_source.size();
+  bd.nodes.resize(std::max<size_t>(bd.n_nodes, 1));
+  bd.order.resize(std::max<size_t>(bd.ntri, 1));
+  DeviceBuffer<float> drecs(std::max<size_t>(16 * recs.size(), 1));
+  if (bd.n_nodes)
+    VT_CUDA(cudaMemcpyAsync(bd.nodes.ptr, tl.nodes.data(), bd.n_nodes * sizeof(BinaryNode), cudaMemcpyHostToDevice,
+                            sb.stream));
+  if (bd.ntri)
+    VT_CUDA(cudaMemcpyAsync(bd.order.ptr, tl.reordered_to_source.data(), bd.ntri * 4, cudaMemcpyHostToDevice,
+                            sb.stream));
+  if (!recs.empty())
+    VT_CUDA(cudaMemcpyAsync(drecs.ptr, recs.data(), recs.size() * sizeof(InstanceRecord), cudaMemcpyHostToDevice,
+                            sb.stream));
+  return encode_wide_gpu(bd, nullptr, 4, nullptr, 4, nullptr, root, 0, nullptr, drecs.ptr, sb.stream);
+}
+
+BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& idx, uint32_t material,
+                   uint32_t node_base, uint32_t rec_base, int max_leaf, const SceneBuild& sb) {
+  const size_t ntri = idx.size() / 4;
   std::vector<uint32_t> mm(ntri, material);
-  BinaryBvhHost b = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
+  BinaryBvhHost b;
   BlasPack out;
-  out.wide = encode_wide(b, pos.data(), 4, idx.data(), 4, mm.data(), node_base, rec_base, &kEngineCollapse);
-  validate_binary(b, (int64_t)ntri);
-  validate_wide(out.wide.nodes.data(), out.wide.nodes.size() / 20, out.wide.tris.data(), out.wide.tris.size() / 16,
-                node_base, ntri, false, kTraversalStack, node_base, rec_base);
+  build_tree(sb, pos, idx, mm.data(), node_base, rec_base, max_leaf, b, out.wide);
   const BinaryNode& rn = b.nodes[0];
   out.local_box = {rn.mn[0], rn.mn[1], rn.mn[2], rn.mx[0], rn.mx[1], rn.mx[2]};
   if (ntri == 0) out.local_box = {0, 0, 0, 0, 0, 0};
   return out;
 }
 
-PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf) {
+PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf,
+                       const SceneBuild& sb) {
   if (!sc) fail(VT_ERR_INVALID_ARGUMENT, "scene is null");
   if (sc->mesh_count && !sc->meshes) fail(VT_ERR_INVALID_ARGUMENT, "meshes is null");
   if (sc->material_count && !sc->materials) fail(VT_ERR_INVALID_ARGUMENT, "materials is null");
@@ -244,9 +299,6 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   }
   const size_t ntri = tri_mat.size();
   // geometry
-  BuildOptions bo;
-  bo.max_leaf = max_leaf;
-  bo.bins = kEngineBins;
   const bool two_level = sc->instance_count > 0;
   if (two_level && !sc->instances) fail(VT_ERR_INVALID_ARGUMENT, "instances is null");
   std::vector<uint32_t> node_words;
@@ -254,12 +306,8 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
   int depth = 1;
   uint32_t root = 0;
   if (!two_level) {
-    p.binary = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
-    WideBvhHost w = encode_wide(p.binary, pos.data(), 4, idx.data(), 4, tri_mat.data(), node_base, rec_base,
-                                &kEngineCollapse);
-    validate_binary(p.binary, (int64_t)ntri);
-    validate_wide(w.nodes.data(), w.nodes.size() / 20, w.tris.data(), w.tris.size() / 16, node_base, ntri, false,
-                  kTraversalStack, node_base, rec_base);
+    WideBvhHost w;
+    build_tree(sb, pos, idx, tri_mat.data(), node_base, rec_base, max_leaf, p.binary, w);
     node_words = std::move(w.nodes);
     rec_floats = std::move(w.tris);
     depth = w.depth;
@@ -286,7 +334,7 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
         for (int k = 0; k < 3; ++k) mi[4 * t + k] -= (uint32_t)vbase;
       blas_root[m] = (uint32_t)(node_words.size() / 20);
       rec_start[m] = (uint32_t)(rec_floats.size() / 16);
-      BlasPack bp = pack_blas(mp, mi, md.material, blas_root[m], rec_start[m], max_leaf);
+      BlasPack bp = pack_blas(mp, mi, md.material, blas_root[m], rec_start[m], max_leaf, sb);
       node_words.insert(node_words.end(), bp.wide.nodes.begin(), bp.wide.nodes.end());
       rec_floats.insert(rec_floats.end(), bp.wide.tris.begin(), bp.wide.tris.end());
       depths[m] = bp.wide.depth;
@@ -303,12 +351,14 @@ PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec
     std::vector<InstanceRecord>& recs = placed.recs;
     std::vector<double>& aabbs = placed.aabbs;
     inst_rows = std::move(placed.rows);
-    BinaryBvhHost tl = build_tlas_host(aabbs.data(), ni);
+    BinaryBvhHost tl = build_top_level(sb, aabbs.data(), ni);
     root = (uint32_t)(node_words.size() / 20);
-    WideBvhHost tw = encode_wide_tlas(tl, recs.data(), root);
-    validate_binary(tl, (int64_t)ni);
-    validate_wide(tw.nodes.data(), tw.nodes.size() / 20, tw.tris.data(), tw.tris.size() / 16, root, ni, true,
-                  kTraversalStack, root, 0);
+    WideBvhHost tw = encode_top_level(sb, tl, recs, root);
+    if (sb.validate) {
+      validate_binary(tl, (int64_t)ni);
+      validate_wide(tw.nodes.data(), tw.nodes.size() / 20, tw.tris.data(), tw.tris.size() / 16, root, ni, true,
+                    kTraversalStack, root, 0);
+    }
     node_words.insert(node_words.end(), tw.nodes.begin(), tw.nodes.end());
     inst_lanes = std::move(tw.tris);
     inst_tab.resize(16 * ni);

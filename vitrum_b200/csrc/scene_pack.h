@@ -56,8 +56,16 @@ struct BlasPack {
   WideBvhHost wide;
   std::array<double, 6> local_box;
 };
+// Where a scene's trees are built: on the GPU (device, stream) or on the host;
+// validate runs the publication proofs on the result.
+struct SceneBuild {
+  bool gpu = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool validate = true;
+};
 BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& idx, uint32_t material,
-                   uint32_t node_base, uint32_t rec_base, int max_leaf);
+                   uint32_t node_base, uint32_t rec_base, int max_leaf, const SceneBuild& sb = SceneBuild());
 
 // Instances placed over bottom-level trees: records (world-to-local rows, BLAS
 // root, id, material, material flags), world AABBs (6 doubles each) and
@@ -70,12 +78,18 @@ struct InstanceSet {
 InstanceSet place_instances(const vt_instance_desc* insts, size_t n, const std::vector<pt::Material>& mats,
                             const std::vector<uint32_t>& blas_root,
                             const std::vector<std::array<double, 6>>& local_box);
+// The top level over instance AABBs (6 doubles each) and its 8-wide encoding
+// with instance records, on the GPU or on the host as sb says (the same words).
+BinaryBvhHost build_top_level(const SceneBuild& sb, const double* aabbs, size_t n);
+WideBvhHost encode_top_level(const SceneBuild& sb, const BinaryBvhHost& tl, const std::vector<InstanceRecord>& recs,
+                             uint32_t root);
 // New instance AABBs into an existing top level: same topology, bounds recomputed bottom-up.
 void refit_tlas_host(BinaryBvhHost& tl, const double* aabbs, size_t n);
 
 // Validates and packs; single-level trees are offset by node_base / rec_base
 // (scenes concatenated into shared arrays); instanced scenes need both zero.
-PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf = 4);
+PackedScene pack_scene(const vt_scene_desc* sc, uint32_t node_base, uint32_t rec_base, int max_leaf = 4,
+                       const SceneBuild& sb = SceneBuild());
 
 // Triangles per leaf of the path tracer's own trees when the options leave it
 // open: two per leaf traced the box room 4 % and the instanced cloud 7 % faster

@@ -26,7 +26,8 @@ class _EngineOptions(ctypes.Structure):
     _fields_ = [("max_bounces", ctypes.c_int32), ("max_samples_per_pixel", ctypes.c_int32),
                 ("debug", ctypes.c_int32), ("oracle_accumulation", ctypes.c_int32),
                 ("sort_by_material", ctypes.c_int32), ("wave_paths", ctypes.c_int32),
-                ("bvh_max_leaf", ctypes.c_int32), ("light_selection", ctypes.c_int32)]
+                ("bvh_max_leaf", ctypes.c_int32), ("light_selection", ctypes.c_int32),
+                ("scene_build", ctypes.c_int32)]
 
 
 class _MaterialDesc(ctypes.Structure):
@@ -392,10 +393,11 @@ class Engine:
 
     def __init__(self, device: int = 0, max_bounces: int = 8, max_samples_per_pixel: int = 4096,
                  debug: bool = False, oracle_accumulation: bool = False, sort_by_material: bool = False,
-                 wave_paths: int = 0, bvh_max_leaf: int = 0, light_selection: str = "tree"):
+                 wave_paths: int = 0, bvh_max_leaf: int = 0, light_selection: str = "tree",
+                 scene_build: str = "gpu"):
         opts = _EngineOptions(max_bounces, max_samples_per_pixel, 1 if debug else 0, 1 if oracle_accumulation else 0,
                               1 if sort_by_material else 0, wave_paths, bvh_max_leaf,
-                              {"tree": 0, "uniform": 1}[light_selection])
+                              {"tree": 0, "uniform": 1}[light_selection], {"gpu": 0, "host": 1}[scene_build])
         h = ctypes.c_void_p()
         N.call("vt_create", device, ctypes.byref(opts), ctypes.byref(h))
         self._h = h
@@ -526,6 +528,17 @@ class Engine:
         N.call("vt_capture_moments", self.handle, ctypes.c_void_p(m.ctypes.data), ctypes.c_void_p(v.ctypes.data),
                m.size)
         return m, v
+
+    def export_scene(self):
+        """The device node words (uint32, 20 per wide node) and triangle records
+        (float32, 16 per record) of the current scene (vt_engine_export_scene)."""
+        nw, nf = ctypes.c_size_t(), ctypes.c_size_t()
+        N.call("vt_engine_export_scene", self.handle, None, 0, None, 0, ctypes.byref(nw), ctypes.byref(nf))
+        words = np.empty(nw.value, np.uint32)
+        recs = np.empty(nf.value, np.float32)
+        N.call("vt_engine_export_scene", self.handle, ctypes.c_void_p(words.ctypes.data), words.size,
+               ctypes.c_void_p(recs.ctypes.data), recs.size, ctypes.byref(nw), ctypes.byref(nf))
+        return words, recs
 
     def capture_luminance_moments(self):
         """Per-pixel FP64 shape of the luminance samples, (H, W, 4): mean,
