@@ -25,6 +25,19 @@ thread_local std::string t_last_error;
 void set_last_error(const std::string& msg) { t_last_error = msg; }
 void clear_last_error() { t_last_error.clear(); }
 
+void configure_scratch_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  static bool done[64] = {};
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long keep = 1ull << 30;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[dev] = true;
+}
+
 thread_local long long t_alloc_fail_countdown = 0;  // 0: disarmed
 void arm_allocation_failure(long long nth) { t_alloc_fail_countdown = nth > 0 ? nth : 0; }
 bool injected_allocation_failure() {

@@ -431,12 +431,12 @@ __global__ void k_emit(const GNode* nodes, int n, BinaryNode* out) {
 
 // Sorts A[0, c) by (cen[axis], index) with two stable device radix passes.
 static void sort_segment_device(const double* cen, uint32_t* A, uint32_t c, int axis, cudaStream_t s) {
-  DeviceBuffer<uint32_t> a2(c);
-  DeviceBuffer<unsigned long long> k1(c), k2(c);
+  ScratchBuffer<uint32_t> a2(c, s);
+  ScratchBuffer<unsigned long long> k1(c, s), k2(c, s);
   size_t t1 = 0, t2 = 0;
   VT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, t1, A, a2.ptr, (int)c, 0, 32, s));
   VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, k1.ptr, k2.ptr, a2.ptr, A, (int)c, 0, 64, s));
-  DeviceBuffer<unsigned char> tmp(std::max(t1, t2));
+  ScratchBuffer<unsigned char> tmp(std::max(t1, t2), s);
   size_t tb = tmp.count;
   VT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.ptr, tb, A, a2.ptr, (int)c, 0, 32, s));  // by index
   k_sort_keys<<<(c + 255) / 256, 256, 0, s>>>(cen, a2.ptr, c, axis, k1.ptr);
@@ -460,11 +460,12 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
     return out;
   }
   if (ntri >= (1u << 30)) fail(VT_ERR_RANGE, "too many triangles for one tree");
-  DeviceBuffer<double> tb(6 * ntri), cen(3 * ntri);
-  DeviceBuffer<uint32_t> A(ntri), tmp(ntri);
-  DeviceBuffer<GNode> nodes(2 * ntri);
-  DeviceBuffer<int32_t> lvl_a(ntri + 2), lvl_b(ntri + 2);
-  DeviceBuffer<int> counters(4);
+  ScratchBuffer<double> tb(6 * ntri, s), cen(3 * ntri, s);
+  DeviceBuffer<uint32_t> A(ntri);
+  ScratchBuffer<uint32_t> tmp(ntri, s);
+  ScratchBuffer<GNode> nodes(2 * ntri, s);
+  ScratchBuffer<int32_t> lvl_a(ntri + 2, s), lvl_b(ntri + 2, s), ids(ntri + 2, s);
+  ScratchBuffer<int> counters(4, s);
   VT_CUDA(cudaMemsetAsync(counters.ptr, 0, 4 * sizeof(int), s));
   k_prep<<<(unsigned)((ntri + 255) / 256), 256, 0, s>>>(d_pos, o.position_stride, position_words / o.position_stride,
                                                         d_idx, o.index_stride, (uint32_t)ntri, tb.ptr, cen.ptr, A.ptr,
@@ -497,8 +498,8 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
   // levels: node ids of each level kept for the size / preorder passes
   std::vector<std::vector<int32_t>> levels;
   std::vector<int32_t> cur = {0};
-  DeviceBuffer<int32_t>* in = &lvl_a;
-  DeviceBuffer<int32_t>* nx = &lvl_b;
+  ScratchBuffer<int32_t>* in = &lvl_a;
+  ScratchBuffer<int32_t>* nx = &lvl_b;
   while (!cur.empty()) {
     levels.push_back(cur);
     VT_CUDA(cudaMemsetAsync(counters.ptr + 1, 0, sizeof(int), s));
@@ -534,9 +535,7 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
   VT_CUDA(cudaMemcpyAsync(&total, counters.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
   VT_CUDA(cudaStreamSynchronize(s));
   // subtree sizes bottom-up, preorder indices top-down
-  DeviceBuffer<int32_t> ids;
   for (int L = (int)levels.size() - 1; L >= 0; --L) {
-    ids.resize(levels[L].size());
     // on the build's stream: a plain copy from pageable memory can return before
     // it lands, and a kernel on a non-blocking stream would not wait for it
     VT_CUDA(cudaMemcpyAsync(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
@@ -544,7 +543,6 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
     VT_CUDA(cudaStreamSynchronize(s));
   }
   for (size_t L = 0; L < levels.size(); ++L) {
-    ids.resize(levels[L].size());
     // on the build's stream: a plain copy from pageable memory can return before
     // it lands, and a kernel on a non-blocking stream would not wait for it
     VT_CUDA(cudaMemcpyAsync(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));

@@ -493,11 +493,11 @@ WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int 
     }
     return out;
   }
-  DeviceBuffer<DpNode> dp;
+  ScratchBuffer<DpNode> dp;
   if (sah) {
-    DeviceBuffer<uint32_t> parent(n);
-    DeviceBuffer<unsigned int> visits(n);
-    dp.resize(n);
+    ScratchBuffer<uint32_t> parent(n, s);
+    ScratchBuffer<unsigned int> visits(n, s);
+    dp.resize(n, s);
     VT_CUDA(cudaMemsetAsync(parent.ptr, 0xFF, n * sizeof(uint32_t), s));
     VT_CUDA(cudaMemsetAsync(visits.ptr, 0, n * sizeof(unsigned int), s));
     k_parents<<<(n + 255) / 256, 256, 0, s>>>(bin.nodes.ptr, n, parent.ptr);
@@ -512,10 +512,10 @@ WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int 
   size_t rec_cap = 28 + 4 * (size_t)bin.ntri + 64;
   DeviceBuffer<float> recs(16 * rec_cap);
   VT_CUDA(cudaMemsetAsync(recs.ptr, 0, recs.bytes(), s));
-  DeviceBuffer<uint32_t> lvl_a(max_wide), lvl_b(max_wide), n_int(max_wide), span(max_wide);
-  DeviceBuffer<LevelPlan> plan(max_wide);
-  DeviceBuffer<unsigned long long> totals(2);
-  DeviceBuffer<int> err(1);
+  ScratchBuffer<uint32_t> lvl_a(max_wide, s), lvl_b(max_wide, s), n_int(max_wide, s), span(max_wide, s);
+  ScratchBuffer<LevelPlan> plan(max_wide, s);
+  ScratchBuffer<unsigned long long> totals(2, s);
+  ScratchBuffer<int> err(1, s);
   VT_CUDA(cudaMemsetAsync(err.ptr, 0, sizeof(int), s));
   const uint32_t root = 0;
   VT_CUDA(cudaMemcpyAsync(lvl_a.ptr, &root, sizeof root, cudaMemcpyHostToDevice, s));
@@ -523,8 +523,8 @@ WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int 
              d_inst_recs, node_base, rec_base};
   uint32_t level_n = 1, level_start = 0, rec_used = 28;
   int depth = 0;
-  DeviceBuffer<uint32_t>* cur = &lvl_a;
-  DeviceBuffer<uint32_t>* nxt = &lvl_b;
+  ScratchBuffer<uint32_t>* cur = &lvl_a;
+  ScratchBuffer<uint32_t>* nxt = &lvl_b;
   while (level_n) {
     ++depth;
     const unsigned blocks = (level_n + 127) / 128;

@@ -198,8 +198,8 @@ static void build_tree(const SceneBuild& sb, const std::vector<float>& pos, cons
   const size_t ntri = idx.size() / 4;
   if (sb.gpu) {
     DeviceScope ds(sb.device);
-    DeviceBuffer<float> dpos(std::max<size_t>(pos.size(), 1));
-    DeviceBuffer<uint32_t> didx(std::max<size_t>(idx.size(), 1)), dmat(std::max<size_t>(ntri, 1));
+    ScratchBuffer<float> dpos(std::max<size_t>(pos.size(), 1), sb.stream);
+    ScratchBuffer<uint32_t> didx(std::max<size_t>(idx.size(), 1), sb.stream), dmat(std::max<size_t>(ntri, 1), sb.stream);
     if (!pos.empty()) VT_CUDA(cudaMemcpyAsync(dpos.ptr, pos.data(), pos.size() * 4, cudaMemcpyHostToDevice, sb.stream));
     if (!idx.empty()) VT_CUDA(cudaMemcpyAsync(didx.ptr, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, sb.stream));
     if (ntri && tri_mat) VT_CUDA(cudaMemcpyAsync(dmat.ptr, tri_mat, ntri * 4, cudaMemcpyHostToDevice, sb.stream));
@@ -233,7 +233,7 @@ WideBvhHost encode_top_level(const SceneBuild& sb, const BinaryBvhHost& tl, cons
   bd.ntri = tl.reordered_to_source.size();
   bd.nodes.resize(std::max<size_t>(bd.n_nodes, 1));
   bd.order.resize(std::max<size_t>(bd.ntri, 1));
-  DeviceBuffer<float> drecs(std::max<size_t>(16 * recs.size(), 1));
+  ScratchBuffer<float> drecs(std::max<size_t>(16 * recs.size(), 1), sb.stream);
   if (bd.n_nodes)
     VT_CUDA(cudaMemcpyAsync(bd.nodes.ptr, tl.nodes.data(), bd.n_nodes * sizeof(BinaryNode), cudaMemcpyHostToDevice,
                             sb.stream));

@@ -464,11 +464,13 @@ BinaryBvhHost build_tlas_gpu(const double* aabbs, size_t n, int max_leaf, int bi
     const int need = leaves <= 1 ? 0 : (int)std::ceil(std::log2((double)leaves));
     if (need > max_depth) fail(VT_ERR_RANGE, "instances cannot fit the traversal-safe depth");
   }
-  DeviceBuffer<double> d_aabbs(6 * n), mn(3 * n), mx(3 * n), cen(3 * n), skey(2 * n), nmn(3 * 2 * n), nmx(3 * 2 * n);
-  DeviceBuffer<uint32_t> W(n), tmp(n), sval(2 * n);
-  DeviceBuffer<TNode> tn(2 * n);
-  DeviceBuffer<int32_t> lvl_a(n + 2), lvl_b(n + 2), ids;
-  DeviceBuffer<int> counters(3);
+  ScratchBuffer<double> d_aabbs(6 * n, s), mn(3 * n, s), mx(3 * n, s), cen(3 * n, s), skey(2 * n, s),
+      nmn(3 * 2 * n, s), nmx(3 * 2 * n, s);
+  DeviceBuffer<uint32_t> W(n);
+  ScratchBuffer<uint32_t> tmp(n, s), sval(2 * n, s);
+  ScratchBuffer<TNode> tn(2 * n, s);
+  ScratchBuffer<int32_t> lvl_a(n + 2, s), lvl_b(n + 2, s), ids(n + 2, s);
+  ScratchBuffer<int> counters(3, s);
   VT_CUDA(cudaMemcpyAsync(d_aabbs.ptr, aabbs, 6 * n * sizeof(double), cudaMemcpyHostToDevice, s));
   k_tlas_prep<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_aabbs.ptr, (uint32_t)n, mn.ptr, mx.ptr, cen.ptr, W.ptr);
   VT_CUDA(cudaGetLastError());
@@ -483,8 +485,8 @@ BinaryBvhHost build_tlas_gpu(const double* aabbs, size_t n, int max_leaf, int bi
   VT_CUDA(cudaMemcpyAsync(lvl_a.ptr, &root_id, sizeof root_id, cudaMemcpyHostToDevice, s));
   std::vector<std::vector<int32_t>> levels;
   std::vector<int32_t> cur = {0};
-  DeviceBuffer<int32_t>* in = &lvl_a;
-  DeviceBuffer<int32_t>* nx = &lvl_b;
+  ScratchBuffer<int32_t>* in = &lvl_a;
+  ScratchBuffer<int32_t>* nx = &lvl_b;
   while (!cur.empty()) {
     levels.push_back(cur);
     VT_CUDA(cudaMemsetAsync(counters.ptr + 1, 0, sizeof(int), s));
@@ -509,7 +511,6 @@ BinaryBvhHost build_tlas_gpu(const double* aabbs, size_t n, int max_leaf, int bi
   VT_CUDA(cudaStreamSynchronize(s));
   // subtree sizes and interior bounds bottom up, preorder numbers top down
   for (int L = (int)levels.size() - 1; L >= 0; --L) {
-    ids.resize(levels[L].size());
     VT_CUDA(cudaMemcpyAsync(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     k_tlas_sizes_bounds<<<(unsigned)((levels[L].size() + 255) / 256), 256, 0, s>>>(tn.ptr, ids.ptr,
                                                                                    (int)levels[L].size(), nmn.ptr,
@@ -517,7 +518,6 @@ BinaryBvhHost build_tlas_gpu(const double* aabbs, size_t n, int max_leaf, int bi
     VT_CUDA(cudaStreamSynchronize(s));
   }
   for (size_t L = 0; L < levels.size(); ++L) {
-    ids.resize(levels[L].size());
     VT_CUDA(cudaMemcpyAsync(ids.ptr, levels[L].data(), levels[L].size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     k_tlas_preorder<<<(unsigned)((levels[L].size() + 255) / 256), 256, 0, s>>>(tn.ptr, ids.ptr, (int)levels[L].size());
     VT_CUDA(cudaStreamSynchronize(s));

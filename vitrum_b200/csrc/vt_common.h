@@ -93,6 +93,54 @@ struct DeviceBuffer {
   size_t bytes() const { return count * sizeof(T); }
 };
 
+// Scratch device memory from the stream-ordered pool: allocation and release
+// are enqueued on the stream (no device-wide synchronisation), and released
+// blocks stay in the current device's pool (up to 1 GiB kept) for the next
+// build's scratch.
+void configure_scratch_pool();
+template <class T>
+struct ScratchBuffer {
+  T* ptr = nullptr;
+  size_t count = 0;
+  cudaStream_t stream = nullptr;
+  ScratchBuffer() = default;
+  ScratchBuffer(size_t n, cudaStream_t s) { resize(n, s); }
+  ScratchBuffer(const ScratchBuffer&) = delete;
+  ScratchBuffer& operator=(const ScratchBuffer&) = delete;
+  ScratchBuffer(ScratchBuffer&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) {
+    o.ptr = nullptr;
+    o.count = 0;
+  }
+  ScratchBuffer& operator=(ScratchBuffer&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      count = o.count;
+      stream = o.stream;
+      o.ptr = nullptr;
+      o.count = 0;
+    }
+    return *this;
+  }
+  ~ScratchBuffer() { release(); }
+  void release() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    count = 0;
+  }
+  void resize(size_t n, cudaStream_t s) {
+    release();
+    stream = s;
+    if (n) {
+      if (injected_allocation_failure()) fail(VT_ERR_OUT_OF_MEMORY, "injected device allocation failure");
+      configure_scratch_pool();
+      VT_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s));
+    }
+    count = n;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
 // Sets the current device for the lifetime of the scope and restores it.
 struct DeviceScope {
   int prev = -1;
