@@ -582,10 +582,9 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
   auto B = [&](int st) { if (tm) tm->begin(st, s); };
   auto E = [&]() { if (tm) tm->end(s); };
   vt::pt::FrameView f;
-  std::memcpy(f.inv_vp, e->inv_vp, sizeof f.inv_vp);
+  f.cam = e->aux_consts.ptr + vt::pt::kCamConsts;
   f.width = (uint32_t)e->width;
   f.height = (uint32_t)e->height;
-  f.frame_seed = e->frame_seed;
   f.spp_wave = spp_wave;
   f.max_bounces = bounces;
   f.paths = f.width * f.height * spp_wave;
@@ -785,7 +784,9 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
     std::memcpy(e->proj_m, in->projection, sizeof e->proj_m);
     e->frame_seed = in->frame_seed;
     e->have_camera = true;
-    e->drop_graphs();
+    // the camera and the seed reach the kernels through the per-frame constants:
+    // the captured graphs stay; a new size needs new ones
+    if (size_changed) e->drop_graphs();
     reset_accumulation(e);
   }
   const bool prev_camera = e->have_prev_camera;
@@ -813,6 +814,8 @@ void render_frame(vt_engine* e, const vt_frame_input* in, vt_frame_output* out, 
   else std::memcpy(e->aux_host + 16, e->aux_host, 16 * sizeof(float));
   const uint32_t last_sample = (uint32_t)e->samples + spp - 1u;
   std::memcpy(e->aux_host + 32, &last_sample, sizeof last_sample);
+  std::memcpy(e->aux_host + vt::pt::kCamConsts, e->inv_vp, sizeof e->inv_vp);
+  std::memcpy(e->aux_host + vt::pt::kCamConsts + 16, &e->frame_seed, sizeof e->frame_seed);
   VT_CUDA(cudaMemcpyAsync(e->aux_consts.ptr, e->aux_host, sizeof e->aux_host, cudaMemcpyHostToDevice, e->stream));
   // with the cache: train, then render waves that end in cache queries
   int mode = kPlain;

@@ -341,21 +341,22 @@ __global__ void k_raygen(FrameView f, WaveBuffers w) {
   if (i >= f.paths) return;
   const uint32_t wh = f.width * f.height;
   uint32_t pix = i % wh, s = i / wh;
+  const float* M = f.cam;
+  const uint32_t frame_seed = __float_as_uint(__ldg(M + 16));
   uint32_t key;
   if (f.train) {
     // training paths: uniformly random pixels, a key stream of their own
-    uint32_t h = pcg_init(i, *w.nrc_seed, 0x7A3D9E1Bu ^ f.frame_seed);
+    uint32_t h = pcg_init(i, *w.nrc_seed, 0x7A3D9E1Bu ^ frame_seed);
     pix = pcg_next(h) % wh;
     key = pcg_next(h) | 1u;
   } else {
-    key = f.frame_seed ^ (w.counters[kCntWaveSample] + s);
+    key = frame_seed ^ (w.counters[kCntWaveSample] + s);
   }
   const uint32_t x = pix % f.width, y = pix / f.width;
   uint32_t rng = pcg_init(x, y, key);
   const float jx = rand01(rng), jy = rand01(rng);
   const float u = ((float)x + jx) / (float)f.width, v = ((float)y + jy) / (float)f.height;
   const float nx = u * 2.0f - 1.0f, ny = 1.0f - v * 2.0f;
-  const float* M = f.inv_vp;
   float nf[4], fr[4];
   for (int r = 0; r < 4; ++r) {
     nf[r] = M[4 * r] * nx + M[4 * r + 1] * ny - M[4 * r + 2] + M[4 * r + 3];

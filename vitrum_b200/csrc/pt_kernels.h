@@ -90,12 +90,15 @@ struct AuxView {
   float4* moments = nullptr;       // (sum L, sum L^2, samples, 0), L = Rec. 709 luminance of a sample
   const float* consts = nullptr;
 };
-constexpr int kAuxConsts = 36;
+// then the camera block at kCamConsts: the inverse view-projection (16 floats,
+// row-major) and the frame seed (u32 bits), written every frame so that a
+// new camera or seed needs no new graph
+constexpr int kCamConsts = 36;
+constexpr int kAuxConsts = kCamConsts + 17;
 
 struct FrameView {
-  float inv_vp[16];         // row-major inverse view-projection
+  const float* cam = nullptr;  // device: inverse view-projection (16 floats, row-major), frame seed (u32 bits)
   uint32_t width = 0, height = 0;
-  uint32_t frame_seed = 0;
   uint32_t spp_wave = 1;    // samples per pixel in one wave
   uint32_t max_bounces = 5;
   uint32_t paths = 0;       // width * height * spp_wave

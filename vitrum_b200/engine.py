@@ -503,12 +503,16 @@ class Engine:
     TONEMAPS = {"aces": 0, "agx": 1, "reinhard": 2, "linear": 3, "none": 4}
 
     def capture_frame(self, color_space: str = "linear", tonemap: str = "aces", exposure: float = 1.0,
-                      output_color_space: str = "srgb") -> np.ndarray:
+                      output_color_space: str = "srgb", out: "np.ndarray | None" = None) -> np.ndarray:
         """(H, W, 4) float32, alpha 1 (Engine.captureFrame).  color_space 'linear':
         the mean radiance; 'output': the present pass (exposure, `tonemap` of
         aces / agx / reinhard / linear / none, sRGB encoding unless
-        output_color_space is 'linear')."""
-        out = np.empty((self.height, self.width, 4), np.float32)
+        output_color_space is 'linear').  out: an (H, W, 4) float32 C-contiguous
+        array to fill (page-locked memory makes the copy a direct DMA)."""
+        if out is None:
+            out = np.empty((self.height, self.width, 4), np.float32)
+        elif out.shape != (self.height, self.width, 4) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous (height, width, 4) float32 array")
         if color_space == "linear":
             N.call("vt_capture", self.handle, ctypes.c_void_p(out.ctypes.data), out.size)
         elif color_space == "output":
