@@ -45,10 +45,11 @@ def test_device_selection_matches_oracle(cuda):
         we = np.array([w[0] for w in want])
         wp = np.array([w[1] for w in want], np.float32)
         same = (de == we)
-        # log2f / exp2f on the device and the host library's log2 / exp2 can differ in
-        # the last place; the bucket split then moves by a few buckets at some levels
+        # the device's importance uses the hardware's approximate square roots and
+        # divisions, the oracle correctly rounded ones: a split moves by a few buckets,
+        # more where the cone taper subtracts nearly equal cosines
         assert same.mean() > 0.999, same.mean()
-        assert (np.abs(dp[same] - wp[same]) <= 1e-4 * wp[same] + 64.0 / BUCKETS).all()
+        assert (np.abs(dp[same] - wp[same]) <= 1e-3 * wp[same] + 64.0 / BUCKETS).all()
         assert (dp >= 1.0 / BUCKETS).all() and np.all(np.round(dp * BUCKETS) == dp * BUCKETS)
         assert ((de >= n) == (buckets < (BUCKETS * n_dist) // (n_dist + 1))).all()
 

@@ -1,9 +1,7 @@
 // light_tree.cuh -- device selection of one light entry from the packed light
 // tree (layout in light_tree.h): the reference's samplePackedLightTreeCPU bucket
 // descent (packages/shared-samplers/src/lightTree.ts:938-1319) over an importance
-// of the same quantity plus a receiver bound, in f32 with every operation
-// rounded on its own (no contraction), so the bucket split follows the same
-// arithmetic as the CPU oracle's restatement.
+// of the same quantity plus a receiver bound.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,19 +16,15 @@ namespace lt {
 constexpr float kF32Max = 3.40282346638528859812e38f;
 constexpr float kF32MinNormal = 1.17549435082228750797e-38f;
 
-__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
-__device__ __forceinline__ float dot3r(float ax, float ay, float az, float bx, float by, float bz) {
-  return fadd(fadd(fmul(ax, bx), fmul(ay, by)), fmul(az, bz));
-}
+
+// sqrt(x) for x >= 0 through the hardware reciprocal square root (0 at 0)
+__device__ __forceinline__ float fast_sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 
 // cos(max(0, theta - theta_u)) for cos theta = c and the half-angle theta_u (cu, su)
 __device__ __forceinline__ float bound_cos(float c, float cu, float su) {
   if (c >= cu) return 1.0f;
-  const float s = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(c, c))));
-  return fmaxf(-1.0f, fminf(1.0f, fadd(fmul(c, cu), fmul(s, su))));
+  const float s = fast_sqrt(fmaxf(0.0f, 1.0f - c * c));
+  return fmaxf(-1.0f, fminf(1.0f, c * cu + s * su));
 }
 
 // Importance of packed node `idx` for the point p with unit normal n (zero:
@@ -39,10 +33,12 @@ __device__ __forceinline__ float bound_cos(float c, float cu, float su) {
 // orientation cone's taper at cos(max(0, theta - theta_u)) -- times the
 // receiver bound cos(max(0, theta_i - theta_u)) on the shading cosine (Conty
 // Estevez & Kulla 2018), theta_u the node's bounding-sphere half-angle.  It is
-// evaluated directly, not in the reference's scale-safe log form: one
-// reciprocal square root serves both bounds and the packed axis is unit (the
-// build normalises it), about a fifth of the instructions.  Every operation
-// is rounded on its own, as in the CPU oracle's restatement.
+// evaluated directly (one reciprocal square root serves both bounds, the
+// packed axis is unit) with the hardware's approximate square roots and
+// divisions: the selection and the probability it returns come from this one
+// function, so the estimator is exact whatever the rounding; against the CPU
+// oracle's correctly rounded restatement a split moves by a few of the 2^24
+// buckets at most.
 __device__ __forceinline__ float importance(const float* tree, uint32_t idx, float px, float py, float pz, float nx,
                                             float ny, float nz) {
   const float* n = tree + (size_t)idx * kFloatsPerNode;
@@ -50,37 +46,36 @@ __device__ __forceinline__ float importance(const float* tree, uint32_t idx, flo
   if (!(power > 0.0f)) return 0.0f;
   const float mnx = __ldg(n + 4), mny = __ldg(n + 5), mnz = __ldg(n + 6);
   const float mxx = __ldg(n + 7), mxy = __ldg(n + 8), mxz = __ldg(n + 9);
-  const float ex = fmaxf(fmaxf(fsub(mnx, px), 0.0f), fsub(px, mxx));
-  const float ey = fmaxf(fmaxf(fsub(mny, py), 0.0f), fsub(py, mxy));
-  const float ez = fmaxf(fmaxf(fsub(mnz, pz), 0.0f), fsub(pz, mxz));
-  const float d2 = fmaxf(dot3r(ex, ey, ez, ex, ey, ez), kDist2Floor);
-  const float vx = fsub(px, fmul(0.5f, fadd(mnx, mxx)));
-  const float vy = fsub(py, fmul(0.5f, fadd(mny, mxy)));
-  const float vz = fsub(pz, fmul(0.5f, fadd(mnz, mxz)));
-  const float hx = fmul(0.5f, fsub(mxx, mnx)), hy = fmul(0.5f, fsub(mxy, mny)), hz = fmul(0.5f, fsub(mxz, mnz));
-  const float r2 = dot3r(hx, hy, hz, hx, hy, hz), l2 = dot3r(vx, vy, vz, vx, vy, vz);
+  const float ex = fmaxf(fmaxf(mnx - px, 0.0f), px - mxx);
+  const float ey = fmaxf(fmaxf(mny - py, 0.0f), py - mxy);
+  const float ez = fmaxf(fmaxf(mnz - pz, 0.0f), pz - mxz);
+  const float d2 = fmaxf(ex * ex + ey * ey + ez * ez, kDist2Floor);
+  const float vx = px - 0.5f * (mnx + mxx), vy = py - 0.5f * (mny + mxy), vz = pz - 0.5f * (mnz + mxz);
+  const float hx = 0.5f * (mxx - mnx), hy = 0.5f * (mxy - mny), hz = 0.5f * (mxz - mnz);
+  const float r2 = hx * hx + hy * hy + hz * hz, l2 = vx * vx + vy * vy + vz * vz;
   float w = 1.0f;
   if (l2 > r2 && l2 <= kF32Max) {  // p outside the bounding sphere
-    const float inv = __frsqrt_rn(l2);
-    const float su = fminf(1.0f, fmul(__fsqrt_rn(r2), inv));
-    const float cu = __fsqrt_rn(fmaxf(0.0f, fsub(1.0f, fmul(su, su))));
+    const float inv = rsqrtf(l2);
+    const float su = fminf(1.0f, fast_sqrt(r2) * inv);
+    const float cu = fast_sqrt(fmaxf(0.0f, 1.0f - su * su));
     const float ax = __ldg(n + 10), ay = __ldg(n + 11), az = __ldg(n + 12);
     if (ax != 0.0f || ay != 0.0f || az != 0.0f) {
-      const float ca = bound_cos(fmaxf(-1.0f, fminf(1.0f, fmul(dot3r(ax, ay, az, vx, vy, vz), inv))), cu, su);
+      const float ca = bound_cos(fmaxf(-1.0f, fminf(1.0f, (ax * vx + ay * vy + az * vz) * inv)), cu, su);
       const float cos_o = __ldg(n + 13), cos_e = __ldg(n + 14);
       if (ca < cos_e) return 0.0f;
       if (ca < cos_o) {
-        const float span = fsub(cos_o, cos_e);
-        if (span > 0.0f) w = fmaxf(kF32MinNormal, fdiv(fsub(ca, cos_e), span));
+        const float span = cos_o - cos_e;
+        if (span > 0.0f) w = fmaxf(kF32MinNormal, __fdividef(ca - cos_e, span));
       }
     }
     if (nx != 0.0f || ny != 0.0f || nz != 0.0f) {
-      const float ci = bound_cos(fmaxf(-1.0f, fminf(1.0f, -fmul(dot3r(nx, ny, nz, vx, vy, vz), inv))), cu, su);
+      const float ci = bound_cos(fmaxf(-1.0f, fminf(1.0f, -(nx * vx + ny * vy + nz * vz) * inv)), cu, su);
       if (!(ci > 0.0f)) return 0.0f;
-      w = fmul(w, ci);
+      w *= ci;
     }
   }
-  const float imp = fdiv(fmul(power, w), d2);
+  // power * w / d2 (d2 >= the floor; __fdividef is exact enough below 2^126)
+  const float imp = d2 < 1e37f ? __fdividef(power * w, d2) : (power * w) / d2;
   if (!(imp <= kF32Max)) return kF32Max;
   return fmaxf(kF32MinNormal, imp);
 }
@@ -93,12 +88,14 @@ __device__ __forceinline__ uint32_t left_buckets(uint32_t cur, uint32_t ll, uint
   const uint32_t remaining = cur - (ll + rl);
   float p_left = 0.5f;
   if (!(a == 0.0f && b == 0.0f)) {
-    const float s = fmaxf(a, b);
-    const float l = fdiv(a, s), r = fdiv(b, s);
-    p_left = fdiv(l, fadd(l, r));
+    if (fmaxf(a, b) > 1e37f) {  // keep a + b and the approximate division in range
+      a *= 0x1p-64f;
+      b *= 0x1p-64f;
+    }
+    p_left = __fdividef(a, a + b);
   }
-  const float ideal = fmul((float)remaining, p_left);
-  const float extra = floorf(fadd(ideal, 0.5f));
+  const float ideal = (float)remaining * p_left;
+  const float extra = floorf(ideal + 0.5f);
   const uint32_t e = extra <= 0.0f ? 0u : (uint32_t)fminf(extra, (float)remaining);
   return ll + (e > remaining ? remaining : e);
 }
