@@ -105,12 +105,27 @@ __global__ void k_prep(const float* __restrict__ pos, int ps, size_t nvert, cons
   }
 }
 
+// Per-bin arrays in dynamic shared memory (80 bytes per bin), laid out by bin_arrays().
+struct Bins {
+  unsigned long long (*mn)[3], (*mx)[3];  // bin bounds as okey()s
+  float (*smn)[3], (*smx)[3];             // suffix bounds (f32, as stored)
+  unsigned int* c;
+  int* sc;
+};
+__host__ __device__ constexpr size_t bin_bytes(int bins) { return (size_t)bins * 80; }
+__device__ __forceinline__ Bins bin_arrays(unsigned char* dyn, int bins) {
+  Bins B;
+  B.mn = reinterpret_cast<unsigned long long(*)[3]>(dyn);
+  B.mx = reinterpret_cast<unsigned long long(*)[3]>(dyn + (size_t)bins * 24);
+  B.smn = reinterpret_cast<float(*)[3]>(dyn + (size_t)bins * 48);
+  B.smx = reinterpret_cast<float(*)[3]>(dyn + (size_t)bins * 60);
+  B.c = reinterpret_cast<unsigned int*>(dyn + (size_t)bins * 72);
+  B.sc = reinterpret_cast<int*>(dyn + (size_t)bins * 76);
+  return B;
+}
+
 struct Shared {
-  double red[kWarps][12];                        // CTA reduction of node / centroid bounds
-  unsigned long long bmn[kMaxBins][3], bmx[kMaxBins][3];  // bin bounds as okey()s
-  unsigned int bc[kMaxBins];
-  float smn[kMaxBins][3], smx[kMaxBins][3];      // suffix bounds (f32, as stored)
-  int sc[kMaxBins];
+  double red[kWarps][12];                        // CTA reduction of node / centroid bounds (up to 16 warps)
   double nb[12];                                 // node bounds (6) + centroid bounds (6)
   double best_cost;
   int best_axis, best_split, nl, decision;       // decision: 0 leaf, 1 SAH split, 2 fallback, 3 large fallback
@@ -146,7 +161,7 @@ __device__ void cta_bounds(const double* tb, const double* cen, const uint32_t* 
     const int k = threadIdx.x;
     const bool is_min = (k < 3) || (k >= 6 && k < 9);
     double r = S.red[0][k];
-    for (int q = 1; q < kWarps; ++q) r = is_min ? jmin(r, S.red[q][k]) : jmax(r, S.red[q][k]);
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) r = is_min ? jmin(r, S.red[q][k]) : jmax(r, S.red[q][k]);
     S.nb[k] = r;
   }
   __syncthreads();
@@ -154,19 +169,19 @@ __device__ void cta_bounds(const double* tb, const double* cen, const uint32_t* 
 
 // Bins of one axis into S.
 __device__ void cta_bins(const double* tb, const double* cen, const uint32_t* A, uint32_t b, uint32_t c, int axis,
-                         double cmin, double span, int bins, Shared& S) {
+                         double cmin, double span, int bins, const Bins& B) {
   for (int j = threadIdx.x; j < bins; j += blockDim.x) {
-    S.bc[j] = 0;
-    for (int k = 0; k < 3; ++k) { S.bmn[j][k] = okey(INFINITY); S.bmx[j][k] = okey(-INFINITY); }
+    B.c[j] = 0;
+    for (int k = 0; k < 3; ++k) { B.mn[j][k] = okey(INFINITY); B.mx[j][k] = okey(-INFINITY); }
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
     const uint32_t t = A[b + i];
     const int j = bin_of(cen[3 * (size_t)t + axis], cmin, span, bins);
-    atomicAdd(&S.bc[j], 1u);
+    atomicAdd(&B.c[j], 1u);
     for (int k = 0; k < 3; ++k) {
-      atomicMin(&S.bmn[j][k], okey(tb[6 * (size_t)t + k]));
-      atomicMax(&S.bmx[j][k], okey(tb[6 * (size_t)t + 3 + k]));
+      atomicMin(&B.mn[j][k], okey(tb[6 * (size_t)t + k]));
+      atomicMax(&B.mx[j][k], okey(tb[6 * (size_t)t + 3 + k]));
     }
   }
   __syncthreads();
@@ -174,35 +189,35 @@ __device__ void cta_bins(const double* tb, const double* cen, const uint32_t* A,
 
 // Sweeps and costs of one axis (thread 0), updating the best split: the
 // suffix sweep into shared memory, then the prefix sweep beside the costs.
-__device__ void choose(int axis, int bins, double parent_sa, Shared& S) {
+__device__ void choose(int axis, int bins, double parent_sa, const Bins& B, Shared& S) {
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   int c = 0;
   for (int i = bins - 1; i >= 0; --i) {
     for (int k = 0; k < 3; ++k) {
-      lo[k] = jmin(lo[k], okey_value(S.bmn[i][k]));
-      hi[k] = jmax(hi[k], okey_value(S.bmx[i][k]));
-      S.smn[i][k] = (float)lo[k];
-      S.smx[i][k] = (float)hi[k];
+      lo[k] = jmin(lo[k], okey_value(B.mn[i][k]));
+      hi[k] = jmax(hi[k], okey_value(B.mx[i][k]));
+      B.smn[i][k] = (float)lo[k];
+      B.smx[i][k] = (float)hi[k];
     }
-    c += (int)S.bc[i];
-    S.sc[i] = c;
+    c += (int)B.c[i];
+    B.sc[i] = c;
   }
   for (int k = 0; k < 3; ++k) { lo[k] = INFINITY; hi[k] = -INFINITY; }
   c = 0;
   for (int s = 0; s < bins - 1; ++s) {
     float pmn[3], pmx[3];
     for (int k = 0; k < 3; ++k) {
-      lo[k] = jmin(lo[k], okey_value(S.bmn[s][k]));
-      hi[k] = jmax(hi[k], okey_value(S.bmx[s][k]));
+      lo[k] = jmin(lo[k], okey_value(B.mn[s][k]));
+      hi[k] = jmax(hi[k], okey_value(B.mx[s][k]));
       pmn[k] = (float)lo[k];
       pmx[k] = (float)hi[k];
     }
-    c += (int)S.bc[s];
-    const int lc = c, rc = S.sc[s + 1];
+    c += (int)B.c[s];
+    const int lc = c, rc = B.sc[s + 1];
     if (lc == 0 || rc == 0) continue;
     const double lsa = half_sa(pmn[0], pmn[1], pmn[2], pmx[0], pmx[1], pmx[2]);
-    const double rsa = half_sa(S.smn[s + 1][0], S.smn[s + 1][1], S.smn[s + 1][2], S.smx[s + 1][0], S.smx[s + 1][1],
-                               S.smx[s + 1][2]);
+    const double rsa = half_sa(B.smn[s + 1][0], B.smn[s + 1][1], B.smn[s + 1][2], B.smx[s + 1][0], B.smx[s + 1][1],
+                               B.smx[s + 1][2]);
     const double num = __dadd_rn(__dmul_rn(lsa, (double)lc), __dmul_rn(rsa, (double)rc));
     const double cost = parent_sa > 0 ? __ddiv_rn(num, parent_sa) : num;
     if (cost < S.best_cost) {
@@ -234,7 +249,7 @@ __device__ void cta_partition(const double* cen, uint32_t* A, uint32_t* tmp, uin
     __syncthreads();
     if (threadIdx.x == 0) {
       unsigned int run = 0;
-      for (int q = 0; q < kWarps; ++q) {
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
         const unsigned int x = S.scan[q];
         S.scan[q] = run;
         run += x;
@@ -297,6 +312,7 @@ __device__ void cta_sort(const double* cen, uint32_t* A, uint32_t b, uint32_t c,
 
 struct Params {
   int max_leaf, bins, max_depth;
+  int sort_cap;  // the shared-memory fallback sort's capacity at this level (a power of two <= kSortMax)
 };
 
 __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, const int32_t* __restrict__ level,
@@ -304,8 +320,9 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
                                                     const double* __restrict__ cen, uint32_t* __restrict__ A,
                                                     uint32_t* __restrict__ tmp, int32_t* __restrict__ next,
                                                     int* __restrict__ counters, Params p) {
-  extern __shared__ unsigned char dyn[];
+  extern __shared__ __align__(16) unsigned char dyn[];
   __shared__ Shared S;
+  const Bins B = bin_arrays(dyn, p.bins);
   const int id = level[blockIdx.x];
   GNode& N = nodes[id];
   const uint32_t b = N.begin, c = N.count;
@@ -331,8 +348,8 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
   for (int axis = 0; axis < 3; ++axis) {
     const double span = __dsub_rn(S.nb[9 + axis], S.nb[6 + axis]);
     if (span <= 1e-9) continue;
-    cta_bins(tb, cen, A, b, c, axis, S.nb[6 + axis], span, p.bins, S);
-    if (threadIdx.x == 0) choose(axis, p.bins, parent_sa, S);
+    cta_bins(tb, cen, A, b, c, axis, S.nb[6 + axis], span, p.bins, B);
+    if (threadIdx.x == 0) choose(axis, p.bins, parent_sa, B, S);
     __syncthreads();
   }
   if (threadIdx.x == 0) {
@@ -347,7 +364,7 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
       }
       S.best_axis = ax;
       S.nl = (int)(c / 2);
-      S.decision = c <= (uint32_t)kSortMax ? 2 : 3;
+      S.decision = c <= (uint32_t)p.sort_cap ? 2 : 3;
     }
   }
   __syncthreads();
@@ -356,8 +373,8 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
     const double span = __dsub_rn(S.nb[9 + ax], S.nb[6 + ax]);
     cta_partition(cen, A, tmp, b, c, ax, S.nb[6 + ax], span, p.bins, S.best_split, (uint32_t)S.nl, S);
   } else if (S.decision == 2) {
-    double* keys = reinterpret_cast<double*>(dyn);
-    uint32_t* vals = reinterpret_cast<uint32_t*>(keys + kSortMax);
+    double* keys = reinterpret_cast<double*>(dyn + bin_bytes(p.bins));
+    uint32_t* vals = reinterpret_cast<uint32_t*>(keys + p.sort_cap);
     cta_sort(cen, A, b, c, ax, keys, vals);
   }
   if (threadIdx.x == 0) {
@@ -377,6 +394,7 @@ __global__ void __launch_bounds__(kThreads) k_level(GNode* __restrict__ nodes, c
     R.begin = b + (uint32_t)S.nl;
     R.count = c - (uint32_t)S.nl;
     R.depth = N.depth + 1;
+    atomicMax(&counters[4], max(S.nl, (int)(c - (uint32_t)S.nl)));  // the next level's largest node
     const int q = atomicAdd(&counters[1], 2);
     next[q] = l;
     next[q + 1] = l + 1;
@@ -465,8 +483,8 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
   ScratchBuffer<uint32_t> tmp(ntri, s);
   ScratchBuffer<GNode> nodes(2 * ntri, s);
   ScratchBuffer<int32_t> lvl_a(ntri + 2, s), lvl_b(ntri + 2, s), ids(ntri + 2, s);
-  ScratchBuffer<int> counters(4, s);
-  VT_CUDA(cudaMemsetAsync(counters.ptr, 0, 4 * sizeof(int), s));
+  ScratchBuffer<int> counters(5, s);  // nodes, next-level size, depth error, large sorts, largest next node
+  VT_CUDA(cudaMemsetAsync(counters.ptr, 0, 5 * sizeof(int), s));
   k_prep<<<(unsigned)((ntri + 255) / 256), 256, 0, s>>>(d_pos, o.position_stride, position_words / o.position_stride,
                                                         d_idx, o.index_stride, (uint32_t)ntri, tb.ptr, cen.ptr, A.ptr,
                                                         counters.ptr + 3);
@@ -484,17 +502,18 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
   root.depth = 0;
   root.pre = 0;
   VT_CUDA(cudaMemcpyAsync(nodes.ptr, &root, sizeof root, cudaMemcpyHostToDevice, s));
-  const int zero_one[4] = {1, 0, 0, 0};
+  const int zero_one[5] = {1, 0, 0, 0, 0};
   VT_CUDA(cudaMemcpyAsync(counters.ptr, zero_one, sizeof zero_one, cudaMemcpyHostToDevice, s));
   int32_t root_id = 0;
   VT_CUDA(cudaMemcpyAsync(lvl_a.ptr, &root_id, sizeof root_id, cudaMemcpyHostToDevice, s));
-  const size_t dyn = kSortMax * (sizeof(double) + sizeof(uint32_t));
   static bool attr = false;
   if (!attr) {
-    VT_CUDA(cudaFuncSetAttribute(k_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    const size_t most = bin_bytes(kMaxBins) + (size_t)kSortMax * (sizeof(double) + sizeof(uint32_t));
+    VT_CUDA(cudaFuncSetAttribute(k_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
     attr = true;
   }
-  Params p{o.max_leaf, o.bins, o.max_depth};
+  Params p{o.max_leaf, o.bins, o.max_depth, kSortMax};
+  uint32_t level_max = (uint32_t)ntri;  // the largest node of the current level
   // levels: node ids of each level kept for the size / preorder passes
   std::vector<std::vector<int32_t>> levels;
   std::vector<int32_t> cur = {0};
@@ -503,10 +522,18 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
   while (!cur.empty()) {
     levels.push_back(cur);
     VT_CUDA(cudaMemsetAsync(counters.ptr + 1, 0, sizeof(int), s));
-    k_level<<<(unsigned)cur.size(), kThreads, dyn, s>>>(nodes.ptr, in->ptr, (int)cur.size(), tb.ptr, cen.ptr, A.ptr,
+    VT_CUDA(cudaMemsetAsync(counters.ptr + 4, 0, sizeof(int), s));
+    // launch shape from the level's largest node: small nodes get small CTAs and
+    // little shared memory, so that many of them run on each SM at once
+    const int threads = level_max >= 2048 ? kThreads : level_max >= 256 ? 256 : level_max >= 64 ? 128 : 64;
+    uint32_t cap = 1;
+    while (cap < level_max && cap < (uint32_t)kSortMax) cap <<= 1;
+    p.sort_cap = (int)cap;
+    const size_t dyn = bin_bytes(o.bins) + (size_t)cap * (sizeof(double) + sizeof(uint32_t));
+    k_level<<<(unsigned)cur.size(), threads, dyn, s>>>(nodes.ptr, in->ptr, (int)cur.size(), tb.ptr, cen.ptr, A.ptr,
                                                        tmp.ptr, nx->ptr, counters.ptr, p);
     VT_CUDA(cudaGetLastError());
-    int cnt[4];
+    int cnt[5];
     VT_CUDA(cudaMemcpyAsync(cnt, counters.ptr, sizeof cnt, cudaMemcpyDeviceToHost, s));
     VT_CUDA(cudaStreamSynchronize(s));
     if (cnt[2]) {
@@ -530,6 +557,7 @@ BinaryBvhHost build_binary_gpu(const float* d_pos, size_t position_words, const 
     }
     std::swap(in, nx);
     cur = std::move(next);
+    level_max = (uint32_t)cnt[4];
   }
   int total = 0;
   VT_CUDA(cudaMemcpyAsync(&total, counters.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
