@@ -341,6 +341,11 @@ def run_instanced(args, dev, local, barrier):
         e.reset()
         e.render_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=seed)
 
+    # launch shape from the project's autotuner (outside the timed region): on this
+    # scene, with lambertian, metal and glass instances and sky misses in one queue,
+    # it turns the material sort on
+    trials = e.autotune(cam, I_W, I_H, samples=I_SPP, frame_seed=555) if not args.no_autotune else []
+    tuning = dict(e.tuning, trials=len(trials))
     frame(7)
     e.reset()
     stages = e.profile_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=8)
@@ -382,6 +387,7 @@ def run_instanced(args, dev, local, barrier):
                            "shadow": (r1["shadow_rays"] - r0["shadow_rays"]) / steps},
         "stages_ms": {k: round(v, 3) for k, v in stages.items() if k.endswith("_ms")},
         "scene_build_s": round(build_s, 3),
+        "tuning": tuning,
         "instance_update": dict(upd, note="host wall clock of vt_update_instances for 1024 moved instances, "
                                           "including the top-level upload"),
     }

@@ -640,6 +640,7 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.stage_nodes = e->trace_stage_nodes;
     t.stage_wait_cycles = e->debug_wait_cycles;
     t.insts = e->view.insts;
+    t.inst_table = e->view.inst_table;
     t.root = e->view.root;
     t.n_dev = w.counters + cur;
     t.blocks_per_sm = e->trace_blocks_per_sm;

@@ -374,105 +374,127 @@ __global__ void k_raygen(FrameView f, WaveBuffers w) {
 }
 
 // ---------------------------------------------------------------- material sort
-__device__ __forceinline__ uint32_t hit_material(const SceneView& sc, int4 h) {
-  if (h.z >= 0) return __float_as_uint(__ldg(sc.inst_table + 4 * (size_t)h.z + 3).z);
-  return __float_as_uint(__ldg(sc.tris + 4 * (size_t)(uint32_t)h.x + 1).w);
-}
+// the material id the closest-hit traversal wrote with the hit (instance
+// material, or the triangle record's)
+__device__ __forceinline__ uint32_t hit_material(const SceneView& sc, int4 h) { return (uint32_t)h.w; }
 
 __device__ __forceinline__ uint32_t hit_key(const SceneView& sc, int4 h) {
   if (h.x < 0) return 0u;
   return 1u + sc.materials[hit_material(sc, h)].kind;
 }
 
-__global__ void k_classify(SceneView sc0, FrameView f, WaveBuffers w, int cur) {
-  const uint32_t n = w.counters[cur];
-  const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
-       base += gridDim.x * blockDim.x) {
-    const uint32_t i = base + lane;
-    const bool valid = i < n;
-    uint32_t key = 0xFFu;
-    if (valid) {
-      const SceneView& sc = f.batch ? f.batch[(w.state[cur][i].z >> 8) & 0xFFu].view : sc0;
-      key = hit_key(sc, w.hits[i]);
-    }
-    if (valid) w.keys[i] = key;
-#pragma unroll
-    for (uint32_t k = 0; k < 4; ++k) {
-      const uint32_t m = __ballot_sync(kFull, key == k);
-      if (m && lane == (uint32_t)(__ffs(m) - 1)) atomicAdd(&w.counters[kCntHist + k], (uint32_t)__popc(m));
-    }
-  }
+// Counting sorts of the queue (by BSDF family for shading, by ray direction
+// octant for tracing) into w.order, stable and without global atomics: CTA b
+// of the grid owns one contiguous, warp-aligned range of the queue; it writes
+// each entry's key and its range's per-key counts, one small kernel turns the
+// counts into per-(CTA, key) offsets, and the CTA then scatters its range in
+// order (warp ballots, a per-chunk scan over its warps).
+__device__ __forceinline__ void sort_range(uint32_t n, uint32_t& lo, uint32_t& hi) {
+  const uint32_t per = (((n + gridDim.x - 1) / gridDim.x) + 31u) & ~31u;
+  lo = min(n, blockIdx.x * per);
+  hi = min(n, lo + per);
 }
 
-__global__ void k_scatter(WaveBuffers w, int cur) {
+// MODE 0: key 0 for a miss, else 1 + the hit material's BSDF kind (K = 4);
+// MODE 1: the ray's direction octant (K = 8)
+template <int K, int MODE>
+__global__ void __launch_bounds__(256) k_sort_keys(SceneView sc0, FrameView f, WaveBuffers w, int cur) {
   const uint32_t n = w.counters[cur];
+  uint32_t lo, hi;
+  sort_range(n, lo, hi);
+  __shared__ uint32_t cnt[K];
+  if (threadIdx.x < K) cnt[threadIdx.x] = 0;
+  __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
-  uint32_t off[4];
-  off[0] = 0;
-  for (int k = 1; k < 4; ++k) off[k] = off[k - 1] + w.counters[kCntHist + k - 1];
-  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
-       base += gridDim.x * blockDim.x) {
-    const uint32_t i = base + lane;
-    const bool valid = i < n;
-    const uint32_t key = valid ? w.keys[i] : 0xFFu;
+  uint32_t local[K];
 #pragma unroll
-    for (uint32_t k = 0; k < 4; ++k) {
-      const uint32_t m = __ballot_sync(kFull, key == k);
-      if (!m) continue;
-      const int leader = __ffs(m) - 1;
-      uint32_t b = 0;
-      if ((int)lane == leader) b = atomicAdd(&w.counters[kCntCursor + k], (uint32_t)__popc(m));
-      b = __shfl_sync(kFull, b, leader);
-      if (key == k) w.order[off[k] + b + __popc(m & ((1u << lane) - 1u))] = i;
-    }
-  }
-}
-
-// Trace order of the closest-hit queue: a counting sort of the queued rays by
-// direction octant, stable up to warp scheduling, so rays that entered the queue
-// in pixel order (nearby origins) stay together within an octant and a warp's
-// rays share the near-to-far child order of the 8-wide nodes.
-__global__ void k_ray_octant(WaveBuffers w, int cur) {
-  const uint32_t n = w.counters[cur];
-  const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t i = base + lane;
-    const bool valid = i < n;
+  for (int k = 0; k < K; ++k) local[k] = 0;
+  for (uint32_t base = lo; base < hi; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool valid = i < hi;
     uint32_t key = 0xFFu;
     if (valid) {
-      const float4 d = w.rays[cur][2 * (size_t)i + 1];
-      key = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+      if (MODE == 0) {
+        const SceneView& sc = f.batch ? f.batch[(w.state[cur][i].z >> 8) & 0xFFu].view : sc0;
+        key = hit_key(sc, w.hits[i]);
+      } else {
+        const float4 d = w.rays[cur][2 * (size_t)i + 1];
+        key = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+      }
       w.keys[i] = key;
     }
 #pragma unroll
-    for (uint32_t k = 0; k < 8; ++k) {
-      const uint32_t m = __ballot_sync(kFull, key == k);
-      if (m && lane == (uint32_t)(__ffs(m) - 1)) atomicAdd(&w.counters[kCntHist + k], (uint32_t)__popc(m));
+    for (int k = 0; k < K; ++k) {
+      const uint32_t m = __ballot_sync(kFull, valid && key == (uint32_t)k);
+      if (lane == 0) local[k] += (uint32_t)__popc(m);
     }
+  }
+  if (lane == 0)
+    for (int k = 0; k < K; ++k)
+      if (local[k]) atomicAdd(&cnt[k], local[k]);
+  __syncthreads();
+  if (threadIdx.x < K) w.counters[kCntSortHist + blockIdx.x * K + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// per-(CTA, key) start offsets: key-major, CTAs in order within a key
+template <int K>
+__global__ void __launch_bounds__(1024) k_sort_offsets(WaveBuffers w, uint32_t g) {
+  __shared__ uint32_t h[kSortGrid * K];
+  __shared__ uint32_t tot[K];
+  for (uint32_t i = threadIdx.x; i < g * K; i += blockDim.x) h[i] = w.counters[kCntSortHist + i];
+  __syncthreads();
+  if (threadIdx.x < K) {
+    uint32_t run = 0;
+    for (uint32_t b = 0; b < g; ++b) {
+      const uint32_t c = h[b * K + threadIdx.x];
+      h[b * K + threadIdx.x] = run;
+      run += c;
+    }
+    tot[threadIdx.x] = run;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < g * K; i += blockDim.x) {
+    uint32_t pre = 0;
+    for (uint32_t k = 0; k < i % K; ++k) pre += tot[k];
+    w.counters[kCntSortOff + i] = h[i] + pre;
   }
 }
 
-__global__ void k_ray_octant_scatter(WaveBuffers w, int cur) {
+template <int K>
+__global__ void __launch_bounds__(256) k_sort_scatter(WaveBuffers w, int cur) {
   const uint32_t n = w.counters[cur];
-  const uint32_t lane = threadIdx.x & 31u;
-  uint32_t off[8];
-  off[0] = 0;
+  uint32_t lo, hi;
+  sort_range(n, lo, hi);
+  __shared__ uint32_t base_k[K];
+  __shared__ uint32_t wcnt[8][K];
+  if (threadIdx.x < K) base_k[threadIdx.x] = w.counters[kCntSortOff + blockIdx.x * K + threadIdx.x];
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  for (uint32_t base = lo; base < hi; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool valid = i < hi;
+    const uint32_t key = valid ? w.keys[i] : 0xFFu;
+    uint32_t mine = 0;
 #pragma unroll
-  for (int k = 1; k < 8; ++k) off[k] = off[k - 1] + w.counters[kCntHist + k - 1];
-  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t i = base + lane;
-    const uint32_t key = i < n ? w.keys[i] : 0xFFu;
-#pragma unroll
-    for (uint32_t k = 0; k < 8; ++k) {
-      const uint32_t m = __ballot_sync(kFull, key == k);
-      if (!m) continue;
-      const int leader = __ffs(m) - 1;
-      uint32_t b = 0;
-      if ((int)lane == leader) b = atomicAdd(&w.counters[kCntCursor + k], (uint32_t)__popc(m));
-      b = __shfl_sync(kFull, b, leader);
-      if (key == k) w.order[off[k] + b + __popc(m & ((1u << lane) - 1u))] = i;
+    for (int k = 0; k < K; ++k) {
+      const uint32_t m = __ballot_sync(kFull, valid && key == (uint32_t)k);
+      if (lane == 0) wcnt[wid][k] = (uint32_t)__popc(m);
+      if (key == (uint32_t)k) mine = m;
     }
+    __syncthreads();
+    if (valid) {
+      uint32_t pos = base_k[key];
+      for (uint32_t q = 0; q < wid; ++q) pos += wcnt[q][key];
+      pos += (uint32_t)__popc(mine & ((1u << lane) - 1u));
+      w.order[pos] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+      uint32_t t = 0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += wcnt[q][threadIdx.x];
+      base_k[threadIdx.x] += t;
+    }
+    __syncthreads();
   }
 }
 
@@ -1038,17 +1060,17 @@ void launch_raygen(const FrameView& f, const WaveBuffers& w, cudaStream_t s) {
 
 void launch_sort_by_material(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur,
                              uint32_t capacity, cudaStream_t s) {
-  cudaMemsetAsync(w.counters + kCntHist, 0, sizeof(uint32_t) * 16, s);
-  const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
-  k_classify<<<g, 256, 0, s>>>(sc, f, w, cur);
-  k_scatter<<<g, 256, 0, s>>>(w, cur);
+  const unsigned g = grid_for(capacity, 256) < kSortGrid ? grid_for(capacity, 256) : kSortGrid;
+  k_sort_keys<4, 0><<<g, 256, 0, s>>>(sc, f, w, cur);
+  k_sort_offsets<4><<<1, 1024, 0, s>>>(w, g);
+  k_sort_scatter<4><<<g, 256, 0, s>>>(w, cur);
 }
 
 void launch_sort_rays(const WaveBuffers& w, int cur, uint32_t capacity, cudaStream_t s) {
-  cudaMemsetAsync(w.counters + kCntHist, 0, sizeof(uint32_t) * 16, s);
-  const unsigned g = grid_for(capacity, 256) < 148 * 8 ? grid_for(capacity, 256) : 148 * 8;
-  k_ray_octant<<<g, 256, 0, s>>>(w, cur);
-  k_ray_octant_scatter<<<g, 256, 0, s>>>(w, cur);
+  const unsigned g = grid_for(capacity, 256) < kSortGrid ? grid_for(capacity, 256) : kSortGrid;
+  k_sort_keys<8, 1><<<g, 256, 0, s>>>(SceneView{}, FrameView{}, w, cur);
+  k_sort_offsets<8><<<1, 1024, 0, s>>>(w, g);
+  k_sort_scatter<8><<<g, 256, 0, s>>>(w, cur);
 }
 
 void launch_shade(const SceneView& sc, const FrameView& f, const WaveBuffers& w, int cur, uint32_t bounce,

@@ -147,8 +147,11 @@ struct WaveBuffers {
 
 enum : int {
   kCntShadow = 2, kCntHist = 3, kCntCursor = 11, kCntWaveSample = 19, kCntQuery = 20, kCntSamples = 21,
-  kCntBatchPaths = 22, kCntWords = 23
+  kCntBatchPaths = 22,
+  // the counting sorts' per-(CTA, key) counts and offsets (kSortGrid CTAs, up to 8 keys)
+  kCntSortHist = 23, kCntSortOff = 23 + 148 * 8 * 8, kCntWords = 23 + 2 * 148 * 8 * 8
 };
+constexpr uint32_t kSortGrid = 148 * 8;  // CTAs of the counting sorts (one contiguous queue range each)
 
 // Accumulation targets.
 struct AccumView {

@@ -145,7 +145,8 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
                                                   const float4* __restrict__ insts, uint32_t root,
                                                   const uint32_t* __restrict__ roots, uint32_t hot_count,
                                                   int stk, long long stage_wait,
-                                                  const uint32_t* __restrict__ order) {
+                                                  const uint32_t* __restrict__ order,
+                                                  const float4* __restrict__ inst_table) {
   // Persistent warps, one ray per lane.  Every iteration each live lane
   // (1) expands at most one wide node, (2) runs at most two watertight
   // triangle tests from a two-entry queue of triangle groups, and (3) picks
@@ -437,9 +438,15 @@ __global__ void __launch_bounds__(kBlock, trace_min_blocks<TWO>())
       occluded[ray] = (uint8_t)(R.best >= 0 ? 1 : 0);
       continue;
     }
-    // closest: (triangle record, watertight t); k_refine_hits turns it into
-    // (source id, t, u, v) in a coalesced pass with every lane busy
-    hits[ray] = make_int4(R.best, __float_as_int(R.closest), best_inst, 0);
+    // closest: (triangle record, watertight t, instance, material id); the
+    // material lets shading skip the record -> material load.  k_refine_hits
+    // turns the record into (source id, t, u, v) in a coalesced pass with every
+    // lane busy
+    int mat = -1;
+    if (R.best >= 0)
+      mat = (TWO && best_inst >= 0 && inst_table) ? __float_as_int(__ldg(inst_table + 4 * (size_t)best_inst + 3).z)
+                                                  : __float_as_int(__ldg(tris + 4 * (size_t)R.best + 1).w);
+    hits[ray] = make_int4(R.best, __float_as_int(R.closest), best_inst, mat);
   }
 }
 
@@ -558,7 +565,7 @@ void launch_trace_k(const TraceArgs& a, cudaStream_t s) {
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
   (hot ? staged : plain)<<<(unsigned)grid, kBlock, stack_bytes + 80 * (size_t)hot, s>>>(
       a.nodes, a.tris, a.rays, a.n, a.hits, a.occluded, a.status, a.counter, a.n_dev, a.insts, a.root, a.roots, hot,
-      stk, a.stage_wait_cycles > 0 ? a.stage_wait_cycles : kStagingWaitCycles, a.order);
+      stk, a.stage_wait_cycles > 0 ? a.stage_wait_cycles : kStagingWaitCycles, a.order, a.inst_table);
 }
 
 template <bool ANY>

@@ -23,7 +23,8 @@ struct TraceArgs {
   const uint32_t* n_dev = nullptr;  // when set, the ray count is read from this device word (n = capacity)
   const float4* insts = nullptr;    // two-level: instance records (4 float4 each); nodes[root] is the TLAS root
   uint32_t root = 0;                // first node to expand
-  const float4* inst_table = nullptr;  // refinement of instance hits: records by instance index
+  const float4* inst_table = nullptr;  // records by instance index: refinement of instance hits, and the
+                                       // material id a closest hit of the path tracer carries
   const uint32_t* roots = nullptr;    // optional per-ray root node (rays of several scenes in one launch)
   const float4* inst_l2w = nullptr;   // refinement of instance hits: local-to-world rows (3 per instance)
   int* inst_out = nullptr;          // optional: instance index per ray (-1 miss / single level)
