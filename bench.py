@@ -150,7 +150,7 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ CPU baseline
-REF_SPP = 2  # samples per pixel of each reference-arm step (full 512x512 frame)
+REF_SPP = 32  # samples per pixel of each reference-arm step (full 512x512 frame, about 5 s on 16 host cores)
 
 
 def _cpu_pt_scene():
