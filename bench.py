@@ -291,6 +291,18 @@ def run_query(args, dev, local, rank, world, barrier):
     total_ms = ev[0].elapsed_time(ev[-1])
     if rank == 0:
         _QUERY_HITS["hits"] = d_hits[0].cpu().numpy()  # batch 0: the rays the CPU baseline re-traces
+    # the same launches in spatial trace order (entry cell and octant, 2^5 cells per axis), sort included
+    g.set_trace_order(5)
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(dev)
+    ev[0].record(stream)
+    for i in range(args.steps):
+        step(i)
+    ev[1].record(stream)
+    torch.cuda.synchronize(dev)
+    spatial_ms = ev[0].elapsed_time(ev[1]) / args.steps
+    g.set_trace_order(0)
     pin = [torch.from_numpy(r).pin_memory() for r in host]
     pin_hits = torch.empty((Q_RAYS, 4), dtype=torch.int32).pin_memory()
     N.call("vt_bvh_trace_closest", g.handle, ctypes.c_void_p(pin[0].data_ptr()), Q_RAYS,
@@ -310,6 +322,7 @@ def run_query(args, dev, local, rank, world, barrier):
                     "4 rotating ray batches (192 MB rays+hits) > 126 MB L2",
         "value": Q_RAYS * args.steps / (total_ms / 1e3) / 1e6, "unit": "Mrays/s",
         "ms_per_launch": total_ms / args.steps,
+        "spatial_order_ms_per_launch": spatial_ms,
         "e2e": {"value": Q_RAYS * args.steps / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": Q_RAYS * 32,
                 "d2h_bytes_per_step": Q_RAYS * 16},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

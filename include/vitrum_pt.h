@@ -119,10 +119,27 @@ vt_status vt_bvh_export_wide(const vt_bvh* bvh, uint32_t* node_words, size_t wor
  * Closest hit for n rays (replaces intersectCompressedWideBvhFirstHit,
  * shared-bvh/src/compressedWideBvh.ts:754).  DEVICE pointers: rays (n vt_ray),
  * hits (n vt_hit).  Enqueued on cuda_stream (NULL = default stream); returns
- * once the launch is enqueued.
+ * once the launch is enqueued.  With a spatial trace order set
+ * (vt_bvh_set_trace_order), batches of 65,536 rays or more are sorted first;
+ * the first such call at a new largest batch size allocates the sort's
+ * scratch (8 bytes per ray plus the bucket arrays), so make it before any
+ * stream capture.
  */
 vt_status vt_bvh_trace_closest_device(vt_bvh* bvh, const vt_ray* d_rays, size_t n, vt_hit* d_hits,
                                       void* cuda_stream);
+
+/*
+ * Trace order of this BVH's query batches (no reference counterpart: the
+ * reference traces one ray at a time).  cell_bits 1..6: batches of at least
+ * 65,536 rays are traced grouped by the 2^cell_bits-per-axis cell of the scene
+ * box where each ray enters it and by direction octant, so neighbouring lanes
+ * walk the same nodes; 0: input order.  Results are the same either way (each
+ * hit is written at its own ray).  Default 0: on rays spread uniformly over
+ * the scene (the closest-hit benchmark's sphere of origins) the persistent
+ * traversal, which refills each finished lane with the next ray, runs as fast
+ * unsorted, and the sort's cost is not repaid.
+ */
+vt_status vt_bvh_set_trace_order(vt_bvh* bvh, int32_t cell_bits);
 
 /*
  * Any hit for n rays (replaces intersectCompressedWideBvhAnyHit,
@@ -768,8 +785,12 @@ typedef struct vt_tuning {
                                  children, grandchildren) into shared memory with one bulk copy;
                                  0: every node read goes through L1/L2.  A batch takes 0 only
                                  (its launches carry one root per ray). */
-  int32_t sort_rays;          /* 1: from bounce 1 on, each closest-hit queue is traced in direction-octant
-                                 order (a counting sort by the signs of the direction); 0: queue order */
+  int32_t sort_rays;          /* trace order: 0 queue order; each closest-hit queue from bounce 1 on by
+                                 1 direction octant (a counting sort by the signs of the direction) or
+                                 2 the 2^6-per-axis cell of the scene box the ray starts in, then its
+                                 octant (the spatial order of vt_bvh_set_trace_order); 3 each shadow
+                                 queue by its 2^4-per-axis origin cell and octant (engines only;
+                                 batches take 0 or 1) */
 } vt_tuning;
 
 vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_batch** out);

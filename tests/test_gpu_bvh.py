@@ -81,6 +81,34 @@ def test_closest_hit_parity_config1(cuda):
     print("config1 parity:", rep)
 
 
+def test_trace_order_keeps_every_result(cuda):
+    """With a spatial trace order set, batches of >= 65,536 rays trace by entry
+    cell and octant; each result is written at its own ray, so every cell size
+    and input order give the same hits, bit for bit, through the host and the
+    device calls."""
+    import torch
+    soup = scenes.random_triangles(65536, seed=2024)
+    rays = scenes.sphere_rays(1 << 18, seed=77)
+    rays[::97, 4:7] *= -1.0  # some rays point away from the scene (miss cell)
+    g = vb.build_compressed_wide_bvh(soup.positions, soup.indices)
+    g.set_trace_order(0)
+    want = g.intersect_first_hit(rays)
+    want_any = g.intersect_any_hit(rays)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((rays.shape[0], 4), dtype=torch.int32, device="cuda")
+    for bits in (1, 3, 5, 6):
+        g.set_trace_order(bits)
+        got = g.intersect_first_hit(rays)
+        assert np.array_equal(got.view(np.int32).reshape(-1, 4), want.view(np.int32).reshape(-1, 4)), bits
+        assert np.array_equal(g.intersect_any_hit(rays), want_any), bits
+        g.trace_closest_device(d_rays.data_ptr(), rays.shape[0], d_hits.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(d_hits.cpu().numpy(), want.view(np.int32).reshape(-1, 4)), bits
+    with pytest.raises(Exception):
+        g.set_trace_order(7)
+    g.close()
+
+
 @pytest.mark.parametrize("leaf", [1, 2, 3])
 def test_closest_hit_parity_leaf_sizes(cuda, leaf):
     soup = scenes.random_triangles(5000, seed=10 + leaf)

@@ -328,17 +328,19 @@ def test_pick_matches_bruteforce_oracle(cuda):
         assert hits > 50 and edge <= 2
 
 
-def test_octant_trace_order_does_not_change_the_image(cuda):
-    """sort_rays traces each closest-hit queue in direction-octant order; every
-    ray's record is its own, so the image is bit for bit the same."""
+def test_trace_orders_do_not_change_the_image(cuda):
+    """sort_rays traces each closest-hit queue in direction-octant order (1) or
+    by origin cell and octant (2), or each shadow queue by origin cell (3); every
+    ray's record is its own, so the image is bit for bit the same as in queue order."""
     sc, cam = small_room()
     imgs = []
-    for sort in (False, True):
+    for sort in (0, 1, 2, 3):
         e = Engine(max_bounces=5)
         e.set_scene(sc)
         e.set_tuning(wave_paths=1 << 20, sort_rays=sort)
         e.render_frame(cam, 32, 32, samples=32)
         imgs.append(e.capture_frame())
-        assert e.tuning["sort_rays"] == (1 if sort else 0)
+        assert e.tuning["sort_rays"] == sort
         e.dispose()
-    assert np.array_equal(imgs[0], imgs[1])
+    for i in (1, 2, 3):
+        assert np.array_equal(imgs[0], imgs[i]), i

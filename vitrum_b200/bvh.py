@@ -113,6 +113,11 @@ class Bvh:
         N.call("vt_bvh_trace_any", self.handle, _ptr(rays), rays.shape[0], _ptr(out))
         return out.astype(bool)
 
+    def set_trace_order(self, cell_bits: int) -> None:
+        """Spatial trace order of batches of >= 65,536 rays: 2^cell_bits cells per
+        axis (1..6), 0 = input order.  Results do not depend on it."""
+        N.call("vt_bvh_set_trace_order", self.handle, int(cell_bits))
+
     def trace_closest_device(self, rays_ptr: int, n: int, hits_ptr: int, stream: int = 0) -> None:
         """Enqueue closest hit on device buffers (32-byte rays, 16-byte hits)."""
         N.call("vt_bvh_trace_closest_device", self.handle, ctypes.c_void_p(rays_ptr), n,

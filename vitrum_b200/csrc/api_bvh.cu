@@ -15,6 +15,7 @@
 
 #include "bvh_host.h"
 #include "bvh_object.h"
+#include "ray_order.h"
 #include "traverse.h"
 #include "vt_common.h"
 
@@ -111,6 +112,46 @@ static TraceArgs trace_args(vt_bvh* b, const vt_ray* rays, size_t n) {
   a.counter = b->counter.ptr;
   a.node_count = b->nodes.count / 5;
   return a;
+}
+
+// Batches below this size trace in input order: the sort's four launches cost
+// more than the coherence gains.
+constexpr size_t kOrderMinRays = 1u << 16;
+
+static bool ordered(const vt_bvh* b, size_t n) {
+  return b->order_bits > 0 && n >= kOrderMinRays && !b->binary.nodes.empty();
+}
+
+// Scratch of the spatial trace order for batches of up to n rays (grown, never shrunk).
+static void ensure_order_scratch(vt_bvh* b, size_t n) {
+  if (!ordered(b, n)) return;
+  if (b->order_keys.count < n) {
+    b->order_keys.resize(n);
+    b->order_idx.resize(n);
+  }
+  const size_t words = 2 * ray_order_count_words(b->order_bits);
+  if (b->order_counts.count < words) b->order_counts.resize(words);
+}
+
+// Enqueues the spatial sort of a.rays[0, a.n) on s and points the launch at the
+// permutation; `off` is the batch's first ray within the scratch, `k` picks the
+// bucket array (0 / 1: the two chunk streams).
+static void order_batch(vt_bvh* b, TraceArgs& a, size_t off, int k, cudaStream_t s) {
+  if (!ordered(b, a.n)) return;
+  RayOrderArgs o;
+  o.rays = a.rays;
+  o.n = a.n;
+  const BinaryNode& r = b->binary.nodes[0];
+  for (int i = 0; i < 3; ++i) {
+    o.lo[i] = r.mn[i];
+    o.hi[i] = r.mx[i];
+  }
+  o.cell_bits = b->order_bits;
+  o.keys = b->order_keys.ptr + off;
+  o.order = b->order_idx.ptr + off;
+  o.counts = b->order_counts.ptr + (size_t)k * ray_order_count_words(b->order_bits);
+  launch_ray_order(o, s);
+  a.order = o.order;
 }
 
 static void check_status(vt_bvh* b) {
@@ -227,10 +268,20 @@ vt_status vt_bvh_trace_closest_device(vt_bvh* b, const vt_ray* d_rays, size_t n,
   return guard([&] {
     check_trace_args(b, d_rays, n, d_hits);
     DeviceScope ds(b->device);
+    ensure_order_scratch(b, n);
     TraceArgs a = trace_args(b, d_rays, n);
     a.hits = reinterpret_cast<int4*>(d_hits);
+    order_batch(b, a, 0, 0, (cudaStream_t)cuda_stream);
     launch_trace_closest(a, (cudaStream_t)cuda_stream);
     VT_CUDA(cudaGetLastError());
+  });
+}
+
+vt_status vt_bvh_set_trace_order(vt_bvh* b, int32_t cell_bits) {
+  return guard([&] {
+    if (!b) fail(VT_ERR_INVALID_ARGUMENT, "bvh is null");
+    if (cell_bits < 0 || cell_bits > kRayOrderMaxCellBits) fail(VT_ERR_RANGE, "cell_bits must be in [0, 6]");
+    b->order_bits = cell_bits;
   });
 }
 
@@ -239,8 +290,10 @@ vt_status vt_bvh_trace_any_device(vt_bvh* b, const vt_ray* d_rays, size_t n, uin
   return guard([&] {
     check_trace_args(b, d_rays, n, d_occluded);
     DeviceScope ds(b->device);
+    ensure_order_scratch(b, n);
     TraceArgs a = trace_args(b, d_rays, n);
     a.occluded = d_occluded;
+    order_batch(b, a, 0, 0, (cudaStream_t)cuda_stream);
     launch_trace_any(a, (cudaStream_t)cuda_stream);
     VT_CUDA(cudaGetLastError());
   });
@@ -265,10 +318,12 @@ vt_status vt_bvh_trace_closest(vt_bvh* b, const vt_ray* rays, size_t n, vt_hit* 
     DeviceScope ds(b->device);
     b->rays_scratch.resize(2 * n);
     b->hits_scratch.resize(n);
+    ensure_order_scratch(b, n);
     if (n <= kQueryChunk) {
       VT_CUDA(cudaMemcpy(b->rays_scratch.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice));
       TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr), n);
       a.hits = b->hits_scratch.ptr;
+      order_batch(b, a, 0, 0, 0);
       launch_trace_closest(a, 0);
       VT_CUDA(cudaGetLastError());
       VT_CUDA(cudaMemcpy(hits, b->hits_scratch.ptr, n * sizeof(vt_hit), cudaMemcpyDeviceToHost));
@@ -283,6 +338,7 @@ vt_status vt_bvh_trace_closest(vt_bvh* b, const vt_ray* rays, size_t n, vt_hit* 
         TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr + 2 * c), m);
         a.hits = b->hits_scratch.ptr + c;
         a.counter = b->chunk_counters.ptr + (k & 1);
+        order_batch(b, a, c, (int)(k & 1), s);
         launch_trace_closest(a, s);
         VT_CUDA(cudaGetLastError());
         VT_CUDA(cudaMemcpyAsync(hits + c, b->hits_scratch.ptr + c, m * sizeof(vt_hit), cudaMemcpyDeviceToHost, s));
@@ -300,9 +356,11 @@ vt_status vt_bvh_trace_any(vt_bvh* b, const vt_ray* rays, size_t n, uint8_t* occ
     DeviceScope ds(b->device);
     b->rays_scratch.resize(2 * n);
     b->occ_scratch.resize(n);
+    ensure_order_scratch(b, n);
     VT_CUDA(cudaMemcpy(b->rays_scratch.ptr, rays, n * sizeof(vt_ray), cudaMemcpyHostToDevice));
     TraceArgs a = trace_args(b, reinterpret_cast<const vt_ray*>(b->rays_scratch.ptr), n);
     a.occluded = b->occ_scratch.ptr;
+    order_batch(b, a, 0, 0, 0);
     launch_trace_any(a, 0);
     VT_CUDA(cudaGetLastError());
     VT_CUDA(cudaMemcpy(occluded, b->occ_scratch.ptr, n, cudaMemcpyDeviceToHost));

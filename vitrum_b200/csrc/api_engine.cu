@@ -23,6 +23,7 @@
 #include "nrc_cache.h"
 #include "scene_pack.h"
 #include "pt_kernels.h"
+#include "ray_order.h"
 #include "traverse.h"
 #include "vt_common.h"
 
@@ -40,6 +41,14 @@ struct NrcEngine {
   uint32_t train_paths = 0;
   int frames = 0;  // frames rendered since the cache was created
 };
+
+// Morton bits per axis of the engine's spatial trace orders: closest-hit queues
+// (sort_rays 2) by 2^6 cells per axis (2^21 buckets, about a hundred rays each at
+// a 16 M-path wave on one room); shadow queues (sort_rays 3), whose rays from one
+// cell head for the same few lights, by 2^4 (2^15 buckets: lanes of a warp share
+// buckets, so the counting atomics aggregate).
+constexpr int kEngineOrderCellBits = 6;
+constexpr int kShadowOrderCellBits = 4;
 
 struct vt_engine {
   int device = 0;
@@ -123,7 +132,11 @@ struct vt_engine {
   std::unique_ptr<NrcEngine> nrc;
   int trace_blocks_per_sm = 0;      // traversal CTAs per SM (0: occupancy limit), from the autotuner
   bool trace_stage_nodes = false;   // traversal CTAs stage the top of the tree in shared memory
-  bool sort_rays = false;           // closest-hit queues of bounces >= 1 traced in direction-octant order
+  int sort_rays = 0;               // trace order: 0 queue order; closest-hit queues of bounces >= 1 by
+                                    // 1 direction octant or 2 origin cell (Morton) and octant; 3 shadow
+                                    // queues by origin cell and octant
+  DeviceBuffer<uint32_t> ray_order_counts;  // buckets of the spatial trace order (sort_rays 2)
+  DeviceBuffer<uint32_t> shadow_keys, shadow_order, shadow_order_counts;  // the shadow queues' (sort_rays 3)
   long long debug_wait_cycles = 0;  // failure-detection hook: first-wait limit of bounded waits (0: default)
   // graph cache: one executable per wave shape and mode
   struct Graph {
@@ -437,8 +450,20 @@ uint32_t wave_paths_of(const vt_engine* e) {
   return e->auto_wave_paths;
 }
 
+// Buffers of the shadow queues' spatial order, when sort_rays 3 asks for it.
+void ensure_shadow_order(vt_engine* e) {
+  if (e->sort_rays != 3 || e->shadow_order.count >= e->capacity) return;
+  e->drop_graphs();
+  e->shadow_keys.resize(e->capacity);
+  e->shadow_order.resize(e->capacity);
+  e->shadow_order_counts.resize(vt::ray_order_count_words(kShadowOrderCellBits));
+}
+
 void ensure_capacity(vt_engine* e, uint32_t cap) {
-  if (e->capacity >= cap) return;
+  if (e->capacity >= cap) {
+    ensure_shadow_order(e);
+    return;
+  }
   e->drop_graphs();
   for (int q = 0; q < 2; ++q) {
     e->rays[q].resize(2 * (size_t)cap);
@@ -448,12 +473,14 @@ void ensure_capacity(vt_engine* e, uint32_t cap) {
   e->hits.resize(cap);
   e->order.resize(cap);
   e->keys.resize(cap);
+  e->ray_order_counts.resize(vt::ray_order_count_words(kEngineOrderCellBits));
   e->shadow_rays.resize(2 * (size_t)cap);
   e->shadow_contrib.resize(cap);
   e->occluded.resize(cap);
   e->radiance.resize(cap);
   e->path_pixel.resize(cap);
   e->capacity = cap;
+  ensure_shadow_order(e);
 }
 
 vt::pt::WaveBuffers wave_buffers(vt_engine* e) {
@@ -577,6 +604,25 @@ void ensure_nrc_buffers(vt_engine* e, uint32_t render_paths) {
 // Wave modes: plain path tracing, render with cache queries, cache training.
 enum WaveMode : int { kPlain = 0, kNrcRender = 1, kNrcTrain = 2 };
 
+// Spatial trace order of one queue (vt::launch_ray_order) over the scene's bounds.
+vt::RayOrderArgs spatial_order(const vt_engine* e, const float4* rays, uint32_t cap, const uint32_t* n_dev,
+                               uint32_t* keys, uint32_t* counts, uint32_t* order, int cell_bits) {
+  vt::RayOrderArgs o;
+  o.rays = rays;
+  o.n = cap;
+  o.n_dev = n_dev;
+  const vt::BinaryNode& r = e->binary.nodes[0];
+  for (int i = 0; i < 3; ++i) {
+    o.lo[i] = r.mn[i];
+    o.hi[i] = r.mx[i];
+  }
+  o.cell_bits = cell_bits;
+  o.keys = keys;
+  o.counts = counts;
+  o.order = order;
+  return o;
+}
+
 void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t s, StageTimer* tm = nullptr,
                  int mode = kPlain) {
   auto B = [&](int st) { if (tm) tm->begin(st, s); };
@@ -644,10 +690,18 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
     t.root = e->view.root;
     t.n_dev = w.counters + cur;
     t.blocks_per_sm = e->trace_blocks_per_sm;
-    if (e->sort_rays && b > 0) {
+    if (e->sort_rays == 1 && b > 0) {
       // scattered directions from bounce 1 on: trace the queue octant by octant
       B(StageTimer::kSort);
       vt::pt::launch_sort_rays(w, cur, cap, s);
+      E();
+      t.order = w.order;
+    } else if (e->sort_rays == 2 && b > 0 && !e->binary.nodes.empty()) {
+      // ... or grouped by the cell of the scene box the ray starts in and its octant
+      B(StageTimer::kSort);
+      vt::launch_ray_order(spatial_order(e, w.rays[cur], cap, w.counters + cur, w.keys, e->ray_order_counts.ptr,
+                                         w.order, kEngineOrderCellBits),
+                           s);
       E();
       t.order = w.order;
     }
@@ -676,6 +730,14 @@ void record_wave(vt_engine* e, uint32_t spp_wave, uint32_t bounces, cudaStream_t
       VT_CUDA(cudaStreamWaitEvent(e->shadow_stream, e->ev_fork, 0));
       ss = e->shadow_stream;
       sh.counter = e->shadow_counter.ptr;
+    }
+    if (e->sort_rays == 3 && !e->binary.nodes.empty() && e->shadow_order.ptr) {
+      B(StageTimer::kSort);
+      vt::launch_ray_order(spatial_order(e, w.shadow_rays, cap, w.counters + vt::pt::kCntShadow, e->shadow_keys.ptr,
+                                         e->shadow_order_counts.ptr, e->shadow_order.ptr, kShadowOrderCellBits),
+                           ss);
+      E();
+      sh.order = e->shadow_order.ptr;
     }
     B(StageTimer::kTraceShadow);
     vt::launch_trace_any(sh, ss);
@@ -1329,7 +1391,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       e->opts.sort_by_material = t.sort_by_material ? 1 : 0;
       e->trace_blocks_per_sm = t.trace_blocks_per_sm;
       e->trace_stage_nodes = t.stage_hot_nodes != 0;
-      e->sort_rays = t.sort_rays != 0;
+      e->sort_rays = t.sort_rays;
       e->drop_graphs();
     };
     auto time_it = [&](const vt_tuning& t) {
@@ -1345,7 +1407,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       return best;
     };
     vt_tuning best{(int32_t)wave_paths_of(e), e->opts.sort_by_material > 0 ? 1 : 0,
-                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0, e->sort_rays ? 1 : 0};
+                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0, e->sort_rays};
     double best_ms = time_it(best);
     for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
       if (wp == best.wave_paths) continue;
@@ -1373,9 +1435,11 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       const double ms = time_it(t);
       if (ms < best_ms) { best_ms = ms; best = t; }
     }
-    {
+    const int sort_start = best.sort_rays;
+    for (int sr : {0, 1, 2, 3}) {
+      if (sr == sort_start) continue;
       vt_tuning t = best;
-      t.sort_rays = best.sort_rays ? 0 : 1;
+      t.sort_rays = sr;
       const double ms = time_it(t);
       if (ms < best_ms) { best_ms = ms; best = t; }
     }
@@ -1395,7 +1459,7 @@ vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
     t->sort_by_material = e->opts.sort_by_material > 0 ? 1 : 0;
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
     t->stage_hot_nodes = e->trace_stage_nodes ? 1 : 0;
-    t->sort_rays = e->sort_rays ? 1 : 0;
+    t->sort_rays = e->sort_rays;
   });
 }
 
@@ -1407,14 +1471,14 @@ vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
     if (t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 16)
       fail(VT_ERR_RANGE, "trace_blocks_per_sm must be in [0, 16]");
     if (t->stage_hot_nodes != 0 && t->stage_hot_nodes != 1) fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 or 1");
-    if (t->sort_rays != 0 && t->sort_rays != 1) fail(VT_ERR_RANGE, "sort_rays must be 0 or 1");
+    if (t->sort_rays < 0 || t->sort_rays > 3) fail(VT_ERR_RANGE, "sort_rays must be in [0, 3]");
     vt::DeviceScope ds(e->device);
     VT_CUDA(cudaStreamSynchronize(e->stream));
     e->opts.wave_paths = t->wave_paths;
     e->opts.sort_by_material = t->sort_by_material;
     e->trace_blocks_per_sm = t->trace_blocks_per_sm;
     e->trace_stage_nodes = t->stage_hot_nodes != 0;
-    e->sort_rays = t->sort_rays != 0;
+    e->sort_rays = t->sort_rays;
     e->drop_graphs();
   });
 }

@@ -31,6 +31,11 @@ struct vt_bvh {
   // two streams and ray counters for the chunked host-buffer queries (created on first use)
   cudaStream_t copy_streams[2] = {nullptr, nullptr};
   vt::DeviceBuffer<unsigned long long> chunk_counters;
+  // spatial trace order of query batches (vt_bvh_set_trace_order): Morton bits
+  // per axis (0: input order), and its scratch, grown on demand: bucket keys and
+  // the permutation (one word per ray each), two bucket arrays (one per stream)
+  int order_bits = 0;
+  vt::DeviceBuffer<uint32_t> order_keys, order_idx, order_counts;
   ~vt_bvh() {
     for (cudaStream_t& s : copy_streams)
       if (s) cudaStreamDestroy(s);
