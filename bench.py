@@ -354,11 +354,12 @@ def run_instanced(args, dev, local, barrier):
         e.reset()
         e.render_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=seed)
 
-    # launch shape from the project's autotuner (outside the timed region): on this
-    # scene, with lambertian, metal and glass instances and sky misses in one queue,
-    # it turns the material sort on
+    # tree shape and launch shape from the project's autotuners (outside the timed
+    # region): on this scene, with lambertian, metal and glass instances and sky
+    # misses in one queue, the launch-shape tuner turns the material sort on
+    shape_trials = e.autotune_bvh(sc, cam, I_W, I_H, samples=I_SPP, frame_seed=555) if not args.no_autotune else []
     trials = e.autotune(cam, I_W, I_H, samples=I_SPP, frame_seed=555) if not args.no_autotune else []
-    tuning = dict(e.tuning, trials=len(trials))
+    tuning = dict(e.tuning, trials=len(trials), bvh_shape_trials=shape_trials)
     frame(7)
     e.reset()
     stages = e.profile_frame(cam, I_W, I_H, samples=I_SPP, frame_seed=8)
@@ -741,7 +742,9 @@ def run_ours(args, rank, world, local):
         e.reset()
         e.render_frame(cam, W, H, samples=SPP, frame_seed=seed)
 
-    # launch shape from the project's autotuner (outside the timed region)
+    # tree shape (leaf size, collapse width) and launch shape from the project's
+    # autotuners (outside the timed region)
+    shape_trials = e.autotune_bvh(sc, cam, W, H, samples=SPP, frame_seed=555) if not args.no_autotune else []
     trials = e.autotune(cam, W, H, samples=SPP, frame_seed=555) if not args.no_autotune else []
     tuning = e.tuning
     for i in range(args.warmup):
@@ -814,7 +817,7 @@ def run_ours(args, rank, world, local):
             "config": {"workload": WORKLOAD, "parallelism": f"replicas{world}", "resolution": [W, H], "spp": SPP,
                        "max_bounces": BOUNCES, "triangles": sc.triangle_count,
                        "l2": "per-frame wave state ~400 MB > 126 MB L2; BVH L2-resident",
-                       "tuning": tuning, "autotune_trials": trials,
+                       "tuning": tuning, "autotune_trials": trials, "bvh_shape_trials": shape_trials,
                        "scene_build_s": round(build_s, 3)},
             "samples_per_s": samples_per_s, "ms_per_frame": dev_s * 1e3 / args.steps,
             "rays_per_frame": {"extension": per_frame_closest, "shadow": per_frame_shadow},

@@ -295,6 +295,8 @@ typedef struct vt_engine_options {
                                      optimal 8-wide encoding and the instance top level); 1 = on the host (the same
                                      words, the reference pipeline the GPU build is checked against).  Debug
                                      engines also run the structural proofs on every tree they publish. */
+  int32_t bvh_width;              /* children per wide node at most in the engine's own triangle trees, 2..8;
+                                     0 = 8 (the node format's capacity; the SAH-optimal collapse fills it) */
 } vt_engine_options;
 
 /* Material (core MaterialSpec subset, core/src/scene/material.ts), the
@@ -819,6 +821,19 @@ vt_status vt_batch_destroy(vt_batch* batch);
 vt_status vt_engine_autotune(vt_engine* engine, const vt_frame_input* frame, vt_tuning_trial* report,
                              size_t report_capacity, size_t* report_count);
 vt_status vt_engine_get_tuning(const vt_engine* engine, vt_tuning* tuning);
+/* BVH-shape autotuner of a single-scene engine (no reference counterpart):
+ * rebuilds `scene`'s trees for candidate shapes -- triangles per leaf (1..4)
+ * at the current width, then collapse width (children per wide node, 8, 6, 4)
+ * at the best leaf size -- renders `frame` with each after a warm-up and keeps
+ * the fastest (the engine ends with `scene` set in that shape and a cleared
+ * accumulation).  The scene is read as vt_set_scene reads it. */
+typedef struct vt_bvh_shape_trial {
+  int32_t bvh_width;
+  int32_t bvh_max_leaf;
+  double frame_ms;
+} vt_bvh_shape_trial;
+vt_status vt_engine_autotune_bvh(vt_engine* engine, const vt_scene_desc* scene, const vt_frame_input* frame,
+                                 vt_bvh_shape_trial* report, size_t report_capacity, size_t* report_count);
 /* Sets the launch shape directly (e.g. one found by an earlier autotune). */
 vt_status vt_engine_set_tuning(vt_engine* engine, const vt_tuning* tuning);
 

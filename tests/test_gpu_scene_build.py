@@ -18,8 +18,8 @@ from vitrum_b200.engine import Engine, Instance, Mesh
 pytestmark = pytest.mark.gpu
 
 
-def export(sc, build, debug=False):
-    e = Engine(max_bounces=2, scene_build=build, debug=debug)
+def export(sc, build, debug=False, width=0):
+    e = Engine(max_bounces=2, scene_build=build, debug=debug, bvh_width=width)
     t0 = time.perf_counter()
     e.set_scene(sc)
     dt = time.perf_counter() - t0
@@ -43,6 +43,47 @@ def test_single_level_box_room(cuda):
     print(f"box room {sc.triangle_count} triangles: set_scene GPU {g[4] * 1e3:.0f} ms, host {h[4] * 1e3:.0f} ms")
     g[0].dispose()
     h[0].dispose()
+
+
+@pytest.mark.parametrize("width", [4, 6])
+def test_collapse_widths_gpu_equals_host(cuda, width):
+    """Narrower SAH-optimal collapses (at most `width` children per wide node):
+    the GPU encoding equals the host's word for word, a debug engine's proofs
+    accept it, and the first hits are those of the full-width tree."""
+    sc, cam = scenes.box_room(wall_cells=32, box_cells=16)
+    g, h = export(sc, "gpu", debug=True, width=width), export(sc, "host", width=width)
+    same(g, h)
+    full = export(sc, "gpu")
+    assert g[1].size > full[1].size  # more, narrower nodes
+    rays = np.concatenate([scenes.sphere_rays(20000, seed=31, radius=2.0, target_half=0.4)])
+    rays[:, :3] += 0.5
+    a, _ = g[0].trace_rays(rays)
+    b, _ = full[0].trace_rays(rays)
+    assert np.array_equal(a["prim"], b["prim"]) and np.array_equal(a["t"], b["t"])
+    for x in (g, h, full):
+        x[0].dispose()
+
+
+def test_bvh_shape_autotune(cuda):
+    """vt_engine_autotune_bvh tries leaf sizes and widths, keeps the fastest and
+    leaves the scene set in that shape: a frame renders as a fresh engine
+    created with that shape renders it."""
+    sc, cam = scenes.box_room(wall_cells=16, box_cells=8)
+    e = Engine(max_bounces=3)
+    trials = e.autotune_bvh(sc, cam, 64, 64, samples=4)
+    assert len(trials) == 6
+    assert {(t["bvh_width"], t["bvh_max_leaf"]) for t in trials} >= {(8, 1), (8, 2), (8, 3), (8, 4)}
+    best = min(trials, key=lambda t: t["frame_ms"])
+    e.render_frame(cam, 32, 32, samples=8)
+    img = e.capture_frame()
+    f = Engine(max_bounces=3, bvh_width=best["bvh_width"], bvh_max_leaf=best["bvh_max_leaf"])
+    f.set_scene(sc)
+    f.render_frame(cam, 32, 32, samples=8)
+    assert np.array_equal(img, f.capture_frame())
+    with pytest.raises(Exception):
+        Engine(bvh_width=9)
+    e.dispose()
+    f.dispose()
 
 
 def planar_cloud():

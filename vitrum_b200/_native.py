@@ -78,6 +78,7 @@ SIGNATURES = {
     "vt_bvh_trace_any": [P, P, SZ, P],
     "vt_bvh_destroy": [P],
     "vt_bvh_set_trace_order": [P, I32],
+    "vt_engine_autotune_bvh": [P, P, P, P, SZ, P],
     "vt_tlas_build": [P, SZ, I32, I32, I32, P, SZ, P, SZ, P],
     "vt_validate_bvh_encoding": [P, SZ, SZ, P, SZ, ctypes.c_int64, I32, P],
     "vt_light_tree_build": [P, SZ, P, SZ, P],

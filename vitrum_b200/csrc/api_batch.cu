@@ -264,6 +264,8 @@ vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_b
     if (b->opts.max_bounces == 0) b->opts.max_bounces = 8;
     if (b->opts.max_bounces < 1 || b->opts.max_bounces > 8) fail(VT_ERR_RANGE, "max_bounces must be in [1, 8]");
     if (b->opts.bvh_max_leaf < 0 || b->opts.bvh_max_leaf > 4) fail(VT_ERR_RANGE, "bvh_max_leaf must be in [0, 4]");
+    if (b->opts.bvh_width != 0 && (b->opts.bvh_width < 2 || b->opts.bvh_width > 8))
+      fail(VT_ERR_RANGE, "bvh_width must be 0 or in [2, 8]");
     if (b->opts.wave_paths > 0) b->tuning.wave_paths = b->opts.wave_paths;
     if (b->opts.sort_by_material > 0) b->tuning.sort_by_material = 1;
     int n = 0;
@@ -314,8 +316,10 @@ vt_status vt_batch_set_scenes(vt_batch* b, const vt_scene_desc* scenes, const vt
       pool.emplace_back([&] {
         for (size_t i = next++; i < count; i = next++) {
           try {
+            vt::SceneBuild sb;
+            sb.bvh_width = b->opts.bvh_width > 0 ? b->opts.bvh_width : 8;
             packed[i] = vt::pack_scene(&scenes[i], 0, 0,
-                                       b->opts.bvh_max_leaf > 0 ? b->opts.bvh_max_leaf : vt::kEngineLeafDefault);
+                                       b->opts.bvh_max_leaf > 0 ? b->opts.bvh_max_leaf : vt::kEngineLeafDefault, sb);
           } catch (const vt::Error& e) {
             codes[i] = e.status;
             errors[i] = e.what();

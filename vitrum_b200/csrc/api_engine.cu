@@ -186,6 +186,7 @@ static vt::SceneBuild scene_build_of(const vt_engine* e) {
   sb.device = e->device;
   sb.stream = e->stream;
   sb.validate = e->opts.debug != 0;
+  sb.bvh_width = e->opts.bvh_width;
   return sb;
 }
 
@@ -983,6 +984,8 @@ vt_status vt_create(int32_t device, const vt_engine_options* options, vt_engine*
     if (e->opts.wave_paths < 0) fail(VT_ERR_RANGE, "wave_paths must be >= 0");
     if (e->opts.bvh_max_leaf == 0) e->opts.bvh_max_leaf = vt::kEngineLeafDefault;
     if (e->opts.bvh_max_leaf < 1 || e->opts.bvh_max_leaf > 4) fail(VT_ERR_RANGE, "bvh_max_leaf must be in [0, 4]");
+    if (e->opts.bvh_width == 0) e->opts.bvh_width = 8;
+    if (e->opts.bvh_width < 2 || e->opts.bvh_width > 8) fail(VT_ERR_RANGE, "bvh_width must be 0 or in [2, 8]");
     if (e->opts.light_selection < 0 || e->opts.light_selection > 1) fail(VT_ERR_RANGE, "light_selection must be 0 or 1");
     if (e->opts.scene_build < 0 || e->opts.scene_build > 1) fail(VT_ERR_RANGE, "scene_build must be 0 or 1");
     vt::DeviceScope ds(device);
@@ -1444,6 +1447,53 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       if (ms < best_ms) { best_ms = ms; best = t; }
     }
     apply(best);
+    reset_accumulation(e);
+    if (count) *count = trials.size();
+    if (report)
+      for (size_t i = 0; i < trials.size() && i < cap; ++i) report[i] = trials[i];
+  });
+}
+
+vt_status vt_engine_autotune_bvh(vt_engine* e, const vt_scene_desc* sc, const vt_frame_input* frame,
+                                 vt_bvh_shape_trial* report, size_t cap, size_t* count) {
+  return vt::guard([&] {
+    if (!e || !sc || !frame) fail(VT_ERR_INVALID_ARGUMENT, "null argument");
+    if (frame->samples < 1) fail(VT_ERR_RANGE, "autotune needs a frame with samples >= 1");
+    vt::DeviceScope ds(e->device);
+    std::vector<vt_bvh_shape_trial> trials;
+    const int width0 = e->opts.bvh_width, leaf0 = e->opts.bvh_max_leaf;
+    int built_w = 0, built_l = 0;
+    auto time_it = [&](int width, int leaf) {
+      e->opts.bvh_width = width;
+      e->opts.bvh_max_leaf = leaf;
+      set_scene(e, sc);
+      built_w = width;
+      built_l = leaf;
+      vt_frame_output out{};
+      double best = 1e30;
+      for (int rep = 0; rep < 3; ++rep) {  // first render captures the graph
+        reset_accumulation(e);
+        render_frame(e, frame, &out);
+        if (rep) best = std::min(best, e->last_ms);
+      }
+      trials.push_back({width, leaf, best});
+      return best;
+    };
+    int bw = width0, bl = leaf0;
+    double best_ms = time_it(bw, bl);
+    for (int leaf = 1; leaf <= 4; ++leaf) {
+      if (leaf == leaf0) continue;
+      const double ms = time_it(width0, leaf);
+      if (ms < best_ms) { best_ms = ms; bl = leaf; }
+    }
+    for (int width : {8, 6, 4}) {
+      if (width == width0) continue;
+      const double ms = time_it(width, bl);
+      if (ms < best_ms) { best_ms = ms; bw = width; }
+    }
+    e->opts.bvh_width = bw;
+    e->opts.bvh_max_leaf = bl;
+    if (built_w != bw || built_l != bl) set_scene(e, sc);
     reset_accumulation(e);
     if (count) *count = trials.size();
     if (report)

@@ -71,7 +71,7 @@ namespace {
 // at i + 1, right child at i + w6, so children follow their parent).
 //   C(n)    cost of n as one slot of its parent:
 //           min(leaf: c_tri * A(n) * count(n)   [count <= 4, contiguous],
-//               node: c_node * A(n) + G(n, 8))
+//               node: c_node * A(n) + G(n, W))   W = width, 8 by default
 //   G(n, k) cost of spreading n's subtree over k slots:
 //           min over a in [1, k-1] of F(left, a) + F(right, k - a)
 //   F(x, a) = C(x) for a = 1 or x a binary leaf, else min(C(x), G(x, a))
@@ -91,9 +91,11 @@ struct SahCollapse {
     return std::min(c[x], g[8 * (size_t)x + a]);
   }
 
-  SahCollapse(const BinaryBvhHost& bin, double c_node, double c_tri)
+  int width;
+
+  SahCollapse(const BinaryBvhHost& bin, double c_node, double c_tri, int w)
       : nodes(bin.nodes.data()), n(bin.nodes.size()), c(n), g(8 * n, 0.0), split(8 * n, 0), first(n), count(n),
-        as_leaf(n, 0), ext(bin.nodes), merged(n) {
+        as_leaf(n, 0), ext(bin.nodes), merged(n), width(w) {
     for (size_t i = n; i-- > 0;) {
       const BinaryNode& b = nodes[i];
       const double area = half_area(b);
@@ -119,7 +121,7 @@ struct SahCollapse {
         g[8 * i + k] = best;
         split[8 * i + k] = (uint8_t)at;
       }
-      c[i] = c_node * area + g[8 * i + 8];
+      c[i] = c_node * area + g[8 * i + width];
       merged[i] = 0;
       if (count[i] <= 4 && contiguous) {
         const double leaf = c_tri * area * count[i];
@@ -150,10 +152,10 @@ struct SahCollapse {
   // children of the wide node rooted at binary node x (never a merged leaf)
   int children(uint32_t x, uint32_t out[8]) const {
     if (is_leaf_word(ext[x].w7)) { out[0] = x; return 1; }
-    const int s = split[8 * (size_t)x + 8];
+    const int s = split[8 * (size_t)x + width];
     int m = 0;
     frontier(x + 1, s, out, m);
-    frontier(x + nodes[x].w6, 8 - s, out, m);
+    frontier(x + nodes[x].w6, width - s, out, m);
     return m;
   }
 };
@@ -353,7 +355,7 @@ WideBvhHost encode_wide(const BinaryBvhHost& bin, const float* positions, int po
     }
   };
   if (sah && !bin.nodes.empty()) {
-    const SahCollapse plan(bin, sah->c_node, sah->c_tri);
+    const SahCollapse plan(bin, sah->c_node, sah->c_tri, std::min(std::max(sah->width, 2), 8));
     return encode_core(bin, plan.ext.data(), node_base, rec_base,
                        [&](uint32_t x, uint32_t* out) { return plan.children(x, out); }, emit);
   }

@@ -77,7 +77,8 @@ __device__ __forceinline__ void load_dp(const DpNode* p, DpNode& o) {
 }
 
 __global__ void k_plan(const BinaryNode* __restrict__ nodes, uint32_t n, const uint32_t* __restrict__ parent,
-                       unsigned int* __restrict__ visits, DpNode* __restrict__ dp, double c_node, double c_tri) {
+                       unsigned int* __restrict__ visits, DpNode* __restrict__ dp, double c_node, double c_tri,
+                       int width) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const BinaryNode b = nodes[i];
@@ -118,7 +119,7 @@ __global__ void k_plan(const BinaryNode* __restrict__ nodes, uint32_t n, const u
       o.split[k - 2] = (uint8_t)at;
     }
     const double area = half_area_d(nb);
-    o.c = __dadd_rn(__dmul_rn(c_node, area), o.g[6]);
+    o.c = __dadd_rn(__dmul_rn(c_node, area), o.g[width - 2]);
     o.as_leaf = 0;
     if (o.count <= 4 && contiguous) {
       const double leaf = __dmul_rn(__dmul_rn(c_tri, area), (double)o.count);
@@ -235,6 +236,7 @@ __device__ __forceinline__ bool entry_is_leaf(const BinaryNode* nodes, uint32_t 
   return (e & kMerged) || leaf_word(nodes[e].w7);
 }
 
+// sah: 0 the reference's greedy collapse, else the SAH-optimal collapse at that width (2..8)
 __global__ void k_level_plan(const BinaryNode* __restrict__ nodes, const DpNode* __restrict__ dp, int sah,
                              const uint32_t* __restrict__ level, uint32_t n_level, LevelPlan* __restrict__ plan,
                              uint32_t* __restrict__ n_int, uint32_t* __restrict__ span) {
@@ -249,9 +251,9 @@ __global__ void k_level_plan(const BinaryNode* __restrict__ nodes, const DpNode*
       p.ch[0] = x;
       n = 1;
     } else {
-      const int s = dp[x].split[6];
+      const int s = dp[x].split[sah - 2];
       frontier(nodes, dp, x + 1, s, p.ch, n);
-      frontier(nodes, dp, x + nodes[x].w6, 8 - s, p.ch, n);
+      frontier(nodes, dp, x + nodes[x].w6, sah - s, p.ch, n);
     }
   } else {
     n = greedy_children(nodes, x, p.ch);
@@ -494,6 +496,7 @@ WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int 
     return out;
   }
   ScratchBuffer<DpNode> dp;
+  const int width = sah ? std::min(std::max(sah->width, 2), 8) : 0;
   if (sah) {
     ScratchBuffer<uint32_t> parent(n, s);
     ScratchBuffer<unsigned int> visits(n, s);
@@ -502,7 +505,8 @@ WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int 
     VT_CUDA(cudaMemsetAsync(visits.ptr, 0, n * sizeof(unsigned int), s));
     k_parents<<<(n + 255) / 256, 256, 0, s>>>(bin.nodes.ptr, n, parent.ptr);
     VT_CUDA(cudaGetLastError());
-    k_plan<<<(n + 255) / 256, 256, 0, s>>>(bin.nodes.ptr, n, parent.ptr, visits.ptr, dp.ptr, sah->c_node, sah->c_tri);
+    k_plan<<<(n + 255) / 256, 256, 0, s>>>(bin.nodes.ptr, n, parent.ptr, visits.ptr, dp.ptr, sah->c_node, sah->c_tri,
+                                           width);
     VT_CUDA(cudaGetLastError());
     VT_CUDA(cudaStreamSynchronize(s));
   }
@@ -528,7 +532,7 @@ WideBvhHost encode_wide_gpu(const BinaryBvhDevice& bin, const float* d_pos, int 
   while (level_n) {
     ++depth;
     const unsigned blocks = (level_n + 127) / 128;
-    k_level_plan<<<blocks, 128, 0, s>>>(bin.nodes.ptr, sah ? dp.ptr : nullptr, sah ? 1 : 0, cur->ptr, level_n,
+    k_level_plan<<<blocks, 128, 0, s>>>(bin.nodes.ptr, sah ? dp.ptr : nullptr, sah ? width : 0, cur->ptr, level_n,
                                         plan.ptr, n_int.ptr, span.ptr);
     VT_CUDA(cudaGetLastError());
     k_scan2<<<1, 1024, 0, s>>>(n_int.ptr, span.ptr, level_n, totals.ptr);

@@ -77,10 +77,12 @@ BinaryBvhHost build_binary_host(const float* positions, size_t position_words, c
 int collect_wide_children(const BinaryNode* nodes, uint32_t root, uint32_t out[8]);
 
 // Surface-area cost weights of the SAH-optimal collapse: c_node per wide node
-// entered, c_tri per triangle tested, both per unit of box half-area.
+// entered, c_tri per triangle tested, both per unit of box half-area; width:
+// children per wide node at most (2..8; the node format holds 8).
 struct WideCollapse {
   double c_node = 1.0;
   double c_tri = 0.5;
+  int width = 8;
 };
 
 // Device copies of an encoded tree: 20 words per wide node, 16 floats per record.

@@ -195,6 +195,8 @@ static void build_tree(const SceneBuild& sb, const std::vector<float>& pos, cons
   BuildOptions bo;
   bo.max_leaf = max_leaf;
   bo.bins = kEngineBins;
+  WideCollapse collapse = kEngineCollapse;
+  collapse.width = sb.bvh_width;
   const size_t ntri = idx.size() / 4;
   if (sb.gpu) {
     DeviceScope ds(sb.device);
@@ -206,10 +208,10 @@ static void build_tree(const SceneBuild& sb, const std::vector<float>& pos, cons
     BinaryBvhDevice bd;
     bin = build_binary_gpu(dpos.ptr, pos.size(), didx.ptr, idx.size(), bo, sb.stream, &bd);
     wide = encode_wide_gpu(bd, dpos.ptr, 4, didx.ptr, 4, tri_mat ? dmat.ptr : nullptr, node_base, rec_base,
-                           &kEngineCollapse, nullptr, sb.stream);
+                           &collapse, nullptr, sb.stream);
   } else {
     bin = build_binary_host(pos.data(), pos.size(), idx.data(), idx.size(), bo);
-    wide = encode_wide(bin, pos.data(), 4, idx.data(), 4, tri_mat, node_base, rec_base, &kEngineCollapse);
+    wide = encode_wide(bin, pos.data(), 4, idx.data(), 4, tri_mat, node_base, rec_base, &collapse);
   }
   if (sb.validate) {
     validate_binary(bin, (int64_t)ntri);

@@ -63,6 +63,7 @@ struct SceneBuild {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool validate = true;
+  int bvh_width = 8;  // children per wide node at most of the triangle trees (2..8)
 };
 BlasPack pack_blas(const std::vector<float>& pos, const std::vector<uint32_t>& idx, uint32_t material,
                    uint32_t node_base, uint32_t rec_base, int max_leaf, const SceneBuild& sb = SceneBuild());

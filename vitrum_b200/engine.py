@@ -27,7 +27,11 @@ class _EngineOptions(ctypes.Structure):
                 ("debug", ctypes.c_int32), ("oracle_accumulation", ctypes.c_int32),
                 ("sort_by_material", ctypes.c_int32), ("wave_paths", ctypes.c_int32),
                 ("bvh_max_leaf", ctypes.c_int32), ("light_selection", ctypes.c_int32),
-                ("scene_build", ctypes.c_int32)]
+                ("scene_build", ctypes.c_int32), ("bvh_width", ctypes.c_int32)]
+
+
+class _BvhShapeTrial(ctypes.Structure):
+    _fields_ = [("bvh_width", ctypes.c_int32), ("bvh_max_leaf", ctypes.c_int32), ("frame_ms", ctypes.c_double)]
 
 
 class _MaterialDesc(ctypes.Structure):
@@ -394,10 +398,11 @@ class Engine:
     def __init__(self, device: int = 0, max_bounces: int = 8, max_samples_per_pixel: int = 4096,
                  debug: bool = False, oracle_accumulation: bool = False, sort_by_material: bool = False,
                  wave_paths: int = 0, bvh_max_leaf: int = 0, light_selection: str = "tree",
-                 scene_build: str = "gpu"):
+                 scene_build: str = "gpu", bvh_width: int = 0):
         opts = _EngineOptions(max_bounces, max_samples_per_pixel, 1 if debug else 0, 1 if oracle_accumulation else 0,
                               1 if sort_by_material else 0, wave_paths, bvh_max_leaf,
-                              {"tree": 0, "uniform": 1}[light_selection], {"gpu": 0, "host": 1}[scene_build])
+                              {"tree": 0, "uniform": 1}[light_selection], {"gpu": 0, "host": 1}[scene_build],
+                              bvh_width)
         h = ctypes.c_void_p()
         N.call("vt_create", device, ctypes.byref(opts), ctypes.byref(h))
         self._h = h
@@ -606,6 +611,23 @@ class Engine:
         self.width, self.height = width, height
         return [dict({f: getattr(trials[i].tuning, f) for f, _ in _Tuning._fields_}, frame_ms=trials[i].frame_ms)
                 for i in range(min(n.value, 32))]
+
+    def autotune_bvh(self, scene: Scene, camera: Camera, width: int, height: int, samples: int = 1,
+                     bounces: int = 0, frame_seed: int = 0):
+        """The BVH-shape autotuner (vt_engine_autotune_bvh): rebuilds `scene` with
+        candidate leaf sizes and collapse widths, times this frame with each and
+        keeps the fastest (the scene stays set).  Returns the trials."""
+        desc, keep = _marshal_scene(scene)
+        view, proj = camera.matrices(width / height)
+        fin = _FrameInput((ctypes.c_float * 16)(*view), (ctypes.c_float * 16)(*proj), width, height, frame_seed,
+                          samples, bounces)
+        trials = (_BvhShapeTrial * 16)()
+        n = ctypes.c_size_t()
+        N.call("vt_engine_autotune_bvh", self.handle, ctypes.byref(desc), ctypes.byref(fin),
+               ctypes.cast(trials, ctypes.c_void_p), 16, ctypes.byref(n))
+        self._scene = scene
+        self.width, self.height = width, height
+        return [{f: getattr(trials[i], f) for f, _ in _BvhShapeTrial._fields_} for i in range(min(n.value, 16))]
 
     @property
     def tuning(self) -> dict:
