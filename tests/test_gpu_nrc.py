@@ -6,6 +6,8 @@ and accumulates in fp32; the oracle rounds at the same places and sums in
 float64.  Predictions agree to 1e-2 of their scale; gradients to 3e-2 in
 relative Frobenius norm per layer and over the table.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -60,6 +62,27 @@ def test_query_matches_oracle(cuda, n):
     print(f"n={n}: max |gpu - oracle| / scale = {err:.2e}")
     assert err < 1e-2
     c.close()
+
+
+@pytest.mark.parametrize("n", [1, 129, 385, 40000, 300000])
+def test_query_tiles_per_cta_agree(cuda, n):
+    """The MLP tile knob (query tiles of 128 in flight per inference CTA, one per
+    warpgroup, 1..3) changes only the launch shape: every query's prediction is
+    the same bit for bit, and matches the oracle, at tile counts that leave
+    warpgroups without a tile."""
+    cfg = NrcConfig(levels=8, log2_table_size=12, base_resolution=4, growth=1.6)
+    recs = random_records(n, 21)
+    outs = []
+    for tiles in (1, 2, 3):
+        c = RadianceCache(dataclasses.replace(cfg, infer_tiles=tiles))
+        W, T = randomise(c, 7)
+        outs.append(c.query(recs))
+        c.close()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    want = oracle_pred(cfg, W, T, recs[:2000])
+    assert np.abs(outs[2][:2000] - want).max() / (np.abs(want).max() + 1e-3) < 1e-2
+    with pytest.raises(Exception):
+        RadianceCache(dataclasses.replace(cfg, infer_tiles=4))
 
 
 def test_query_full_size_grid(cuda):

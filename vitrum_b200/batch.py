@@ -26,7 +26,7 @@ class _BatchStats(ctypes.Structure):
 class _Tuning(ctypes.Structure):
     _fields_ = [("wave_paths", ctypes.c_int32), ("sort_by_material", ctypes.c_int32),
                 ("trace_blocks_per_sm", ctypes.c_int32), ("stage_hot_nodes", ctypes.c_int32),
-                ("sort_rays", ctypes.c_int32)]
+                ("sort_rays", ctypes.c_int32), ("nrc_infer_tiles", ctypes.c_int32)]
 
 
 class _Trial(ctypes.Structure):
@@ -91,7 +91,7 @@ class Batch:
     def set_tuning(self, wave_paths: int, sort_by_material: bool = False, trace_blocks_per_sm: int = 0,
                    stage_hot_nodes: bool = False, sort_rays: bool = False) -> None:
         t = _Tuning(wave_paths, 1 if sort_by_material else 0, trace_blocks_per_sm, 1 if stage_hot_nodes else 0,
-                    1 if sort_rays else 0)
+                    1 if sort_rays else 0, 0)
         N.call("vt_batch_set_tuning", self.handle, ctypes.byref(t))
 
     def autotune(self) -> List[dict]:

@@ -553,6 +553,7 @@ void nrc_rebuild(vt_engine* e) {
   c.growth = k.growth;
   c.lr = k.learning_rate;
   c.table_lr = k.table_learning_rate;
+  c.infer_tiles = k.infer_tiles > 0 ? k.infer_tiles : vt::nrc::kDefaultInferTiles;
   float mn[3] = {0, 0, 0}, mx[3] = {1, 1, 1};
   if (e->has_scene && !e->binary.nodes.empty()) {
     const vt::BinaryNode& r = e->binary.nodes[0];
@@ -1381,6 +1382,15 @@ vt_status vt_set_nrc(vt_engine* e, const vt_nrc_render_options* o) {
   });
 }
 
+// The radiance cache's query tiles per inference CTA (0 without a cache), and
+// a new value for it kept across cache rebuilds (0 leaves it).
+static int nrc_tiles_of(const vt_engine* e) { return e->nrc && e->nrc->cache ? e->nrc->cache->config().infer_tiles : 0; }
+static void set_nrc_tiles(vt_engine* e, int tiles) {
+  if (!e->nrc || tiles <= 0) return;
+  e->nrc->opts.cache.infer_tiles = tiles;
+  if (e->nrc->cache) e->nrc->cache->set_infer_tiles(tiles);
+}
+
 vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tuning_trial* report, size_t cap,
                              size_t* count) {
   return vt::guard([&] {
@@ -1395,6 +1405,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       e->trace_blocks_per_sm = t.trace_blocks_per_sm;
       e->trace_stage_nodes = t.stage_hot_nodes != 0;
       e->sort_rays = t.sort_rays;
+      set_nrc_tiles(e, t.nrc_infer_tiles);
       e->drop_graphs();
     };
     auto time_it = [&](const vt_tuning& t) {
@@ -1410,7 +1421,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       return best;
     };
     vt_tuning best{(int32_t)wave_paths_of(e), e->opts.sort_by_material > 0 ? 1 : 0,
-                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0, e->sort_rays};
+                   e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0, e->sort_rays, nrc_tiles_of(e)};
     double best_ms = time_it(best);
     for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
       if (wp == best.wave_paths) continue;
@@ -1445,6 +1456,17 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
       t.sort_rays = sr;
       const double ms = time_it(t);
       if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    if (e->nrc) {
+      // the radiance cache's MLP tile: query tiles in flight per inference CTA
+      const int tiles_start = best.nrc_infer_tiles;
+      for (int nt : {1, 2, 3}) {
+        if (nt == tiles_start) continue;
+        vt_tuning t = best;
+        t.nrc_infer_tiles = nt;
+        const double ms = time_it(t);
+        if (ms < best_ms) { best_ms = ms; best = t; }
+      }
     }
     apply(best);
     reset_accumulation(e);
@@ -1510,6 +1532,7 @@ vt_status vt_engine_get_tuning(const vt_engine* e, vt_tuning* t) {
     t->trace_blocks_per_sm = e->trace_blocks_per_sm;
     t->stage_hot_nodes = e->trace_stage_nodes ? 1 : 0;
     t->sort_rays = e->sort_rays;
+    t->nrc_infer_tiles = nrc_tiles_of(e);
   });
 }
 
@@ -1522,6 +1545,7 @@ vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
       fail(VT_ERR_RANGE, "trace_blocks_per_sm must be in [0, 16]");
     if (t->stage_hot_nodes != 0 && t->stage_hot_nodes != 1) fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 or 1");
     if (t->sort_rays < 0 || t->sort_rays > 3) fail(VT_ERR_RANGE, "sort_rays must be in [0, 3]");
+    if (t->nrc_infer_tiles < 0 || t->nrc_infer_tiles > 3) fail(VT_ERR_RANGE, "nrc_infer_tiles must be in [0, 3]");
     vt::DeviceScope ds(e->device);
     VT_CUDA(cudaStreamSynchronize(e->stream));
     e->opts.wave_paths = t->wave_paths;
@@ -1529,6 +1553,7 @@ vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
     e->trace_blocks_per_sm = t->trace_blocks_per_sm;
     e->trace_stage_nodes = t->stage_hot_nodes != 0;
     e->sort_rays = t->sort_rays;
+    set_nrc_tiles(e, t->nrc_infer_tiles);
     e->drop_graphs();
   });
 }

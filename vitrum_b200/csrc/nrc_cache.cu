@@ -37,6 +37,7 @@ void validate(const Config& c) {
   for (int k = 0; k < 3; ++k)
     if (!std::isfinite(c.aabb_min[k]) || !std::isfinite(c.aabb_max[k]) || !(c.aabb_max[k] >= c.aabb_min[k]))
       fail(VT_ERR_INVALID_ARGUMENT, "aabb must be finite with max >= min");
+  if (c.infer_tiles < 1 || c.infer_tiles > 3) fail(VT_ERR_RANGE, "infer_tiles must be 0 or in 1..3");
 }
 
 }  // namespace
@@ -106,7 +107,7 @@ void Cache::set_aabb(const float* mn, const float* mx) {
 
 void Cache::query(const float4* records, uint32_t stride, const uint32_t* n_dev, uint32_t n, float* rgb,
                   float4* radiance, cudaStream_t s) const {
-  launch_infer(view(), records, stride, n_dev, n, rgb, radiance, s);
+  launch_infer(view(), records, stride, n_dev, n, rgb, radiance, cfg_.infer_tiles, s);
 }
 
 void Cache::clear_gradients(cudaStream_t s) {
@@ -199,6 +200,7 @@ vt::nrc::Config to_config(const vt_nrc_config* c) {
     k.aabb_min[i] = c->aabb_min[i];
     k.aabb_max[i] = c->aabb_max[i];
   }
+  k.infer_tiles = c->infer_tiles > 0 ? c->infer_tiles : vt::nrc::kDefaultInferTiles;
   return k;
 }
 

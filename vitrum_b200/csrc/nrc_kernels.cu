@@ -219,21 +219,45 @@ __device__ void fail_and_drain(const View& v, uint64_t* bar, uint32_t phase) {
 }
 
 // ---------------------------------------------------------------- inference
-__global__ void __launch_bounds__(128, 1)
+// Named barrier of warpgroup g (ids 1..T; 0 is __syncthreads): the 128 threads
+// of one tile synchronise without waiting for the CTA's other tiles.
+__device__ __forceinline__ void group_sync(uint32_t id) {
+  asm volatile("barrier.cta.sync %0, 128;" ::"r"(id) : "memory");
+}
+__device__ __forceinline__ bool group_and(uint32_t id, bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred a, b;\n\tsetp.ne.u32 a, %1, 0;\n\tbarrier.cta.red.and.pred b, %2, 128, a;\n\t"
+      "selp.u32 %0, 1, 0, b;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)p), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
+// T tiles of 128 queries in flight per CTA, one per warpgroup (the MLP tile
+// knob): the warpgroups share the CTA's weight tiles and TMEM allocation (64
+// columns each) and run independently -- each encodes its tile (16 levels x 8
+// table gathers per query), issues its own MMA chain from its first thread and
+// waits on its own mbarrier -- so one tile's gathers overlap another's MMAs.
+template <int T>
+__global__ void __launch_bounds__(128 * T, T == 1 ? 3 : 2)
     k_nrc_infer(View v, const float4* __restrict__ recs, uint32_t stride, const uint32_t* __restrict__ n_dev,
                 uint32_t n_host, float* __restrict__ rgb, float4* __restrict__ radiance) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
   uint8_t* wt = base;
-  uint8_t* act = base + kLayers * kWBytes;  // one tile: each layer's MMA has finished reading it before the
-                                            // epilogue writes the next layer's input over it
-  uint64_t* bar = reinterpret_cast<uint64_t*>(act + kTileBytes);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
-  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t tid = threadIdx.x & 127u, warp = tid >> 5, g = threadIdx.x >> 7, gid = g + 1;
+  // this warpgroup's tile: each layer's MMA has finished reading it before the
+  // epilogue writes the next layer's input over it
+  uint8_t* act = base + kLayers * kWBytes + g * kTileBytes;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + kLayers * kWBytes + T * kTileBytes) + g;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(reinterpret_cast<uint64_t*>(base + kLayers * kWBytes + T * kTileBytes) + T);
+  constexpr uint32_t kCols = T == 1 ? 64u : (T == 2 ? 128u : 256u);  // a power of two >= 64 T
   const uint32_t n = n_dev ? *n_dev : n_host;
-  if ((uint32_t)blockIdx.x * kTile >= n) return;  // uniform per CTA: no tile, no TMEM
-  if (warp == 0) {
-    tc::tmem_alloc(slot, 64);
+  if ((uint32_t)blockIdx.x * T * kTile >= n) return;  // uniform per CTA: no tile, no TMEM
+  if (threadIdx.x < 32) {
+    tc::tmem_alloc(slot, kCols);
     tc::tmem_relinquish();
   }
   if (tid == 0) {
@@ -245,12 +269,12 @@ __global__ void __launch_bounds__(128, 1)
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t tmem = *slot;
+  const uint32_t tmem = *slot + 64u * g;
   const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
   const uint32_t w_s = tc::smem_u32(wt), a_s = tc::smem_u32(act);
   uint32_t phase = 0;
   bool failed = false;
-  for (uint32_t tile = blockIdx.x; tile * kTile < n && !failed; tile += gridDim.x) {
+  for (uint32_t tile = blockIdx.x * T + g; tile * kTile < n && !failed; tile += gridDim.x * T) {
     const uint32_t i = tile * kTile + tid;
     const bool valid = i < n;
     uint32_t p[32];
@@ -260,13 +284,15 @@ __global__ void __launch_bounds__(128, 1)
     store_row(act, tid, p);
     tc::fence_async_smem();
     tc::fence_before_sync();
-    __syncthreads();
+    group_sync(gid);
     for (int l = 0; l < kLayers; ++l) {
       if (tid == 0) {
         issue_fwd(tmem, a_s, w_s + l * kWBytes);
         tc::mma_commit(bar);
       }
-      if (!wait_all(v, bar, phase)) { failed = true; break; }
+      // thread-uniform bounded wait (per warpgroup); on failure `phase` keeps the pending parity
+      if (!group_and(gid, tc::mbar_wait(bar, phase, v.wait_cycles))) { failed = true; break; }
+      phase ^= 1u;
       tc::fence_after_sync();
       if (l + 1 < kLayers) {
         uint32_t acc[64];
@@ -277,7 +303,7 @@ __global__ void __launch_bounds__(128, 1)
         store_row(act, tid, p);
         tc::fence_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
+        group_sync(gid);
       } else {
         uint32_t o[16];
         tc::tmem_ld16(lane_addr, o);
@@ -302,9 +328,16 @@ __global__ void __launch_bounds__(128, 1)
       }
     }
   }
-  if (failed) fail_and_drain(v, bar, phase);
+  if (failed) {
+    // flag, give the issued MMAs a bounded chance to finish
+    if (tid == 0) {
+      atomicExch(v.error, 1);
+      tc::mbar_wait(bar, phase, kWaitCycles);
+    }
+    group_sync(gid);
+  }
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+  if (threadIdx.x < 32) tc::tmem_dealloc(*slot, kCols);
 }
 
 // ---------------------------------------------------------------- training
@@ -552,7 +585,7 @@ __global__ void k_nrc_adam_table(float2* __restrict__ master, float2* __restrict
   }
 }
 
-constexpr size_t kInferSmem = kLayers * kWBytes + kTileBytes + 64 + 1024;
+constexpr size_t infer_smem(int t) { return kLayers * kWBytes + (size_t)t * kTileBytes + 64 + 1024; }
 constexpr size_t kTrainSmem = kLayers * kWBytes + (1 + kLayers) * kTileBytes + 64 + 1024;
 
 int sm_count() {
@@ -568,18 +601,33 @@ void level_resolutions(const Config& c, float* out) {
   for (int l = 0; l < kMaxLevels; ++l) out[l] = (float)std::floor((double)c.base_resolution * std::pow((double)c.growth, l));
 }
 
-void launch_infer(const View& v, const float4* records, uint32_t rec_stride_f4, const uint32_t* n_dev, uint32_t n,
-                  float* rgb_out, float4* radiance, cudaStream_t s) {
-  if (n == 0) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem);
-    attr = true;
+template <int T>
+void launch_infer_t(const View& v, const float4* records, uint32_t rec_stride_f4, const uint32_t* n_dev, uint32_t n,
+                    float* rgb_out, float4* radiance, cudaStream_t s) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaFuncSetAttribute(k_nrc_infer<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem(T));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nrc_infer<T>, 128 * T, infer_smem(T));
+    // TMEM: 512 columns per SM, 64 T (rounded up to a power of two) per CTA
+    const int cols = T == 1 ? 64 : (T == 2 ? 128 : 256);
+    per_sm = per_sm < 512 / cols ? per_sm : 512 / cols;
+    if (per_sm < 1) per_sm = 1;
   }
-  // three CTAs per SM (65 KB shared memory and 64 TMEM columns each)
   const uint32_t tiles = (n + kTile - 1) / kTile;
-  const uint32_t grid = tiles < (uint32_t)(3 * sm_count()) ? tiles : (uint32_t)(3 * sm_count());
-  k_nrc_infer<<<grid, 128, kInferSmem, s>>>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance);
+  const uint32_t ctas = (tiles + T - 1) / T;
+  const uint32_t cap = (uint32_t)(per_sm * sm_count());
+  k_nrc_infer<T><<<ctas < cap ? ctas : cap, 128 * T, infer_smem(T), s>>>(v, records, rec_stride_f4, n_dev, n, rgb_out,
+                                                                          radiance);
+}
+
+void launch_infer(const View& v, const float4* records, uint32_t rec_stride_f4, const uint32_t* n_dev, uint32_t n,
+                  float* rgb_out, float4* radiance, int tiles_per_cta, cudaStream_t s) {
+  if (n == 0) return;
+  // tiles in flight per CTA: 1 (three CTAs per SM: 65 KB shared memory each), 2 (two CTAs per
+  // SM, 81 KB), 3 (two CTAs per SM, 97 KB)
+  if (tiles_per_cta >= 3) launch_infer_t<3>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
+  else if (tiles_per_cta == 2) launch_infer_t<2>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
+  else launch_infer_t<1>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
 }
 
 void launch_train(const View& v, const float4* samples, uint32_t n, cudaStream_t s) {

@@ -637,14 +637,15 @@ class Engine:
         return {f: getattr(t, f) for f, _ in _Tuning._fields_}
 
     def set_tuning(self, wave_paths: int = 1 << 24, sort_by_material: bool = False, trace_blocks_per_sm: int = 0,
-                   stage_hot_nodes: bool = False, sort_rays: int = 0) -> None:
+                   stage_hot_nodes: bool = False, sort_rays: int = 0, nrc_infer_tiles: int = 0) -> None:
         """Launch shape for later frames (vt_engine_set_tuning); `tuning` of
         another engine or an autotune trial can be passed back as keywords.
         sort_rays: 0 queue order, 1 direction octant, 2 origin cell and octant
-        (True / False read as 1 / 0)."""
+        (True / False read as 1 / 0).  nrc_infer_tiles: query tiles per inference
+        CTA of the radiance cache (1..3; 0 leaves it)."""
         from .batch import _Tuning
         t = _Tuning(int(wave_paths), 1 if sort_by_material else 0, int(trace_blocks_per_sm),
-                    1 if stage_hot_nodes else 0, int(sort_rays))
+                    1 if stage_hot_nodes else 0, int(sort_rays), int(nrc_infer_tiles))
         N.call("vt_engine_set_tuning", self.handle, ctypes.byref(t))
 
     def export_tlas(self):

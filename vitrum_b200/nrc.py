@@ -25,7 +25,8 @@ class _Config(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_int32), ("log2_table_size", ctypes.c_int32),
                 ("base_resolution", ctypes.c_float), ("growth", ctypes.c_float),
                 ("learning_rate", ctypes.c_float), ("table_learning_rate", ctypes.c_float),
-                ("aabb_min", ctypes.c_float * 3), ("aabb_max", ctypes.c_float * 3), ("seed", ctypes.c_uint32)]
+                ("aabb_min", ctypes.c_float * 3), ("aabb_max", ctypes.c_float * 3), ("seed", ctypes.c_uint32),
+                ("infer_tiles", ctypes.c_int32)]
 
 
 @dataclass
@@ -41,11 +42,12 @@ class NrcConfig:
     aabb_min: Sequence[float] = (0.0, 0.0, 0.0)
     aabb_max: Sequence[float] = (1.0, 1.0, 1.0)
     seed: int = 1
+    infer_tiles: int = 0  # query tiles of 128 in flight per inference CTA (1..3; 0: the default)
 
     def to_c(self) -> _Config:
         return _Config(self.levels, self.log2_table_size, self.base_resolution, self.growth, self.learning_rate,
                        self.table_learning_rate, (ctypes.c_float * 3)(*self.aabb_min),
-                       (ctypes.c_float * 3)(*self.aabb_max), self.seed)
+                       (ctypes.c_float * 3)(*self.aabb_max), self.seed, self.infer_tiles)
 
     @property
     def table_floats(self) -> int:

@@ -2,7 +2,8 @@
 
     python -m vitrum_b200.workloads box_room  [--width 512 --height 512 --spp 64 --bounces 5]
     python -m vitrum_b200.workloads instanced [--width 1920 --height 1080 --spp 16 --bounces 8]
-    python -m vitrum_b200.workloads query     [--rays 1048576]
+    python -m vitrum_b200.workloads query     [--rays 1048576 --trace-order 0]
+    python -m vitrum_b200.workloads nrc       [--rays 1048576 --frames 10 --tiles 1]
     (--nrc: path tracing with the neural radiance cache, 4 x 65,536 training samples per frame)
 
 Prints the frame's stage times (or the query's hit count) as one JSON line.
@@ -13,14 +14,15 @@ import argparse
 import json
 
 
-def nrc_timing(n, reps):
+def nrc_timing(n, reps, tiles=0):
     """Cache query and training throughput on device arrays (default cache
-    config: 16 x 2^19 x 2 hash grid, 5 x 64 MLP), CUDA-event timed."""
+    config: 16 x 2^19 x 2 hash grid, 5 x 64 MLP; `tiles` query tiles per
+    inference CTA, 0 = the default), CUDA-event timed."""
     import numpy as np
     import torch
     from .nrc import NrcConfig, RadianceCache
     dev = torch.device("cuda", 0)
-    c = RadianceCache(NrcConfig(aabb_min=(-1, -1, -1), aabb_max=(1, 1, 1)))
+    c = RadianceCache(NrcConfig(aabb_min=(-1, -1, -1), aabb_max=(1, 1, 1), infer_tiles=tiles))
     g = torch.Generator(device=dev).manual_seed(1)
     rec = torch.rand((n, 16), device=dev, generator=g) * 2 - 1
     d = rec[:, 3:6] / rec[:, 3:6].norm(dim=1, keepdim=True)
@@ -45,7 +47,7 @@ def nrc_timing(n, reps):
     t_ms = ev[1].elapsed_time(ev[2]) / reps
     c.close()
     flop = 2 * 64 * 64 * 6  # padded MMA work per query (algorithmic 2 * 20,672)
-    return {"workload": "nrc", "queries": n, "query_ms": q_ms, "queries_per_s": n / q_ms * 1e3,
+    return {"workload": "nrc", "queries": n, "infer_tiles": tiles, "query_ms": q_ms, "queries_per_s": n / q_ms * 1e3,
             "mma_tflops": n * flop / q_ms / 1e9, "train_step_ms_65536": t_ms}
 
 
@@ -60,15 +62,19 @@ def main(argv=None):
     ap.add_argument("--rays", type=int, default=1 << 20)
     ap.add_argument("--instances", type=int, default=1024)
     ap.add_argument("--nrc", action="store_true", help="path tracing with the neural radiance cache")
+    ap.add_argument("--tiles", type=int, default=0, help="nrc: query tiles per inference CTA (1..3)")
+    ap.add_argument("--trace-order", type=int, default=0,
+                    help="query: spatial trace order, Morton bits per axis (0: input order)")
     a = ap.parse_args(argv)
     from . import scenes
     if a.workload == "nrc":
-        print(json.dumps(nrc_timing(a.rays, a.frames)))
+        print(json.dumps(nrc_timing(a.rays, a.frames, a.tiles)))
         return
     if a.workload == "query":
         from .bvh import build_compressed_wide_bvh
         soup, rays = scenes.config1(65536, a.rays, seed=2024)
         with build_compressed_wide_bvh(soup.positions, soup.indices) as g:
+            g.set_trace_order(a.trace_order)
             hits = g.intersect_first_hit(rays)
         print(json.dumps({"workload": "query", "rays": a.rays, "hits": int((hits["prim"] >= 0).sum())}))
         return
