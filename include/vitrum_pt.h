@@ -830,7 +830,8 @@ vt_status vt_engine_get_tuning(const vt_engine* engine, vt_tuning* tuning);
  * rebuilds `scene`'s trees for candidate shapes -- triangles per leaf (1..4)
  * at the current width, then collapse width (children per wide node, 8, 6, 4)
  * at the best leaf size -- renders `frame` with each after a warm-up and keeps
- * the fastest (the engine ends with `scene` set in that shape and a cleared
+ * the fastest, a candidate replacing the current shape only when it is 0.5 %
+ * faster (the engine ends with `scene` set in that shape and a cleared
  * accumulation).  The scene is read as vt_set_scene reads it. */
 typedef struct vt_bvh_shape_trial {
   int32_t bvh_width;

@@ -73,7 +73,15 @@ def test_bvh_shape_autotune(cuda):
     trials = e.autotune_bvh(sc, cam, 64, 64, samples=4)
     assert len(trials) == 6
     assert {(t["bvh_width"], t["bvh_max_leaf"]) for t in trials} >= {(8, 1), (8, 2), (8, 3), (8, 4)}
-    best = min(trials, key=lambda t: t["frame_ms"])
+    kept = (8, 2)  # the starting shape; a candidate replaces it only when 0.5 % faster
+    best_ms = trials[0]["frame_ms"]
+    for t in trials[1:4]:
+        if t["frame_ms"] < best_ms * 0.995:
+            kept, best_ms = (8, t["bvh_max_leaf"]), t["frame_ms"]
+    for t in trials[4:]:
+        if t["frame_ms"] < best_ms * 0.995:
+            kept, best_ms = (t["bvh_width"], kept[1]), t["frame_ms"]
+    best = {"bvh_width": kept[0], "bvh_max_leaf": kept[1]}
     e.render_frame(cam, 32, 32, samples=8)
     img = e.capture_frame()
     f = Engine(max_bounces=3, bvh_width=best["bvh_width"], bvh_max_leaf=best["bvh_max_leaf"])

@@ -63,11 +63,13 @@ def test_set_tuning_validation(cuda):
     sc, cam = scenes.box_room()
     e = Engine(max_bounces=2)
     e.set_scene(sc)
-    for bad in (dict(wave_paths=10), dict(trace_blocks_per_sm=17), dict(trace_blocks_per_sm=-1)):
+    for bad in (dict(wave_paths=10), dict(trace_blocks_per_sm=17), dict(trace_blocks_per_sm=-1), dict(sort_rays=4),
+                dict(nrc_infer_tiles=4)):
         with pytest.raises(N.VtError):
             e.set_tuning(**bad)
     e.set_tuning(wave_paths=1 << 18, sort_by_material=True, trace_blocks_per_sm=6, stage_hot_nodes=True)
+    # nrc_infer_tiles reads 0 on an engine without the radiance cache
     assert e.tuning == {"wave_paths": 1 << 18, "sort_by_material": 1, "trace_blocks_per_sm": 6, "stage_hot_nodes": 1,
-                        "sort_rays": 0}
+                        "sort_rays": 0, "nrc_infer_tiles": 0}
     e.render_frame(cam, 16, 16, samples=2)
     e.dispose()
