@@ -109,6 +109,43 @@ def test_trace_order_keeps_every_result(cuda):
     g.close()
 
 
+def test_traversal_trees_give_the_same_hits(cuda):
+    """The tree the queries traverse (traversalTree): the built tree grouped by the
+    reference's 8-wide rule or the SAH-optimal one, or a second tree with two
+    triangles per leaf (the default).  The exported binary tree is the built one
+    in every case, the hits (id, t, u, v) agree bit for bit except exact f32 t
+    ties, and host and GPU builds encode the same traversal words."""
+    import torch
+    soup = scenes.random_triangles(65536, seed=2024)
+    rays = scenes.sphere_rays(1 << 17, seed=88)
+    b = oracle.build_array_bvh(soup.positions, soup.indices)
+    out = {}
+    for tree in ("reference", "sah", "fast"):
+        g = vb.build_compressed_wide_bvh(soup.positions, soup.indices, traversalTree=tree)
+        nodes, r2s = g.export_binary()
+        assert np.array_equal(nodes, b.nodes) and np.array_equal(r2s, b.reordered_to_source), tree
+        out[tree] = (g.intersect_first_hit(rays), g.export_wide())
+        dp = torch.from_numpy(np.ascontiguousarray(soup.positions, np.float32).reshape(-1)).cuda()
+        di = torch.from_numpy(np.ascontiguousarray(soup.indices, np.uint32).reshape(-1).view(np.int32)).cuda()
+        gd = vb.build_compressed_wide_bvh_device(dp.data_ptr(), dp.numel(), di.data_ptr(), di.numel(),
+                                                 traversalTree=tree)
+        wd = gd.export_wide()
+        assert np.array_equal(wd[0], out[tree][1][0]) and np.array_equal(wd[1].view(np.uint32),
+                                                                          out[tree][1][1].view(np.uint32)), tree
+        gd.close()
+        g.close()
+    base = out["reference"][0]
+    for tree in ("sah", "fast"):
+        h = out[tree][0]
+        diff = np.nonzero(h["prim"] != base["prim"])[0]
+        assert diff.size <= 2, (tree, diff[:10])  # only exact f32 t ties may pick another triangle
+        same = h["prim"] == base["prim"]
+        assert np.array_equal(h[same].view(np.int32).reshape(-1, 4), base[same].view(np.int32).reshape(-1, 4))
+    assert out["fast"][1][0].size != out["reference"][1][0].size
+    with pytest.raises(ValueError):
+        vb.build_compressed_wide_bvh(soup.positions, soup.indices, traversalTree="binary")
+
+
 @pytest.mark.parametrize("leaf", [1, 2, 3])
 def test_closest_hit_parity_leaf_sizes(cuda, leaf):
     soup = scenes.random_triangles(5000, seed=10 + leaf)

@@ -27,7 +27,7 @@ class VtError(RuntimeError):
 class BuildOptions(ctypes.Structure):
     _fields_ = [("position_stride", ctypes.c_int32), ("index_stride", ctypes.c_int32),
                 ("max_leaf_triangles", ctypes.c_int32), ("bin_count", ctypes.c_int32),
-                ("max_depth", ctypes.c_int32)]
+                ("max_depth", ctypes.c_int32), ("traversal_tree", ctypes.c_int32)]
 
 
 class BvhInfo(ctypes.Structure):

@@ -20,16 +20,23 @@ import numpy as np
 
 from . import _native as N
 
-_OPTION_KEYS = ("positionStride", "indexStride", "maxLeafTriangles", "binCount", "maxDepth")
+# the reference's BuildArrayBvhOpts keys, plus traversalTree: the tree the queries traverse
+# ("reference": the built tree, reference 8-wide grouping; "sah": the built tree, SAH-optimal
+# grouping; "fast", the default: a second tree with <= 2 triangles per leaf, 32 bins, SAH-optimal
+# grouping).  The exported binary tree and every hit are the same whichever is chosen.
+_OPTION_KEYS = ("positionStride", "indexStride", "maxLeafTriangles", "binCount", "maxDepth", "traversalTree")
+_TRAVERSAL = {None: 0, "reference": 1, "sah": 2, "fast": 3}
 
 
 def _options(opts: dict) -> N.BuildOptions:
     for k in opts:
         if k not in _OPTION_KEYS:
             raise ValueError(f"unknown option {k!r}")
+    if opts.get("traversalTree") not in _TRAVERSAL:
+        raise ValueError("traversalTree must be 'reference', 'sah' or 'fast'")
     return N.BuildOptions(int(opts.get("positionStride", 4)), int(opts.get("indexStride", 4)),
                           int(opts.get("maxLeafTriangles", 4)), int(opts.get("binCount", 16)),
-                          int(opts.get("maxDepth", 58)))
+                          int(opts.get("maxDepth", 58)), _TRAVERSAL[opts.get("traversalTree")])
 
 
 def _ptr(a) -> ctypes.c_void_p:

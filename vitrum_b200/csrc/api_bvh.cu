@@ -54,7 +54,23 @@ static BuildOptions resolve(const vt_bvh_build_options* o) {
   if (o->max_leaf_triangles) r.max_leaf = o->max_leaf_triangles;
   if (o->bin_count) r.bins = o->bin_count;
   if (o->max_depth) r.max_depth = o->max_depth;
+  if (o->traversal_tree) r.traversal_tree = o->traversal_tree;
   return r;
+}
+
+// The 8-wide grouping the traversal tree is encoded with (nullptr: the reference's rule).
+static const WideCollapse* query_collapse(const BuildOptions& o) {
+  static const WideCollapse kSah{1.0, 0.5, 8};
+  return o.traversal_tree >= 2 ? &kSah : nullptr;
+}
+// Options of the separate traversal tree (traversal_tree 3): at most two
+// triangles per leaf and 32 bins, as the engine's own trees.
+static bool separate_tree(const BuildOptions& o) { return o.traversal_tree == 3; }
+static BuildOptions traversal_options(const BuildOptions& o) {
+  BuildOptions t = o;
+  t.max_leaf = std::min(o.max_leaf, 2);
+  t.bins = 32;
+  return t;
 }
 
 // Proves and publishes an encoded tree: the device arrays come from the GPU
@@ -89,7 +105,11 @@ static vt_bvh* build_host(int device, const float* positions, size_t pw, const u
   b->opts = resolve(options);
   b->binary = build_binary_host(positions, pw, indices, iw, b->opts);
   b->ntri = (int64_t)(iw / b->opts.index_stride);
-  const WideBvhHost w = encode_wide(b->binary, positions, b->opts.position_stride, indices, b->opts.index_stride);
+  BinaryBvhHost trav;
+  if (separate_tree(b->opts)) trav = build_binary_host(positions, pw, indices, iw, traversal_options(b->opts));
+  const BinaryBvhHost& tb = separate_tree(b->opts) ? trav : b->binary;
+  const WideBvhHost w = encode_wide(tb, positions, b->opts.position_stride, indices, b->opts.index_stride,
+                                    nullptr, 0, 0, query_collapse(b->opts));
   publish(b.get(), w, nullptr);
   b->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return b.release();
@@ -209,9 +229,13 @@ vt_status vt_bvh_build_device(int32_t device, const float* d_positions, size_t p
     BinaryBvhDevice bd;
     b->binary = build_binary_gpu(d_positions, position_words, d_indices, index_words, b->opts, s, &bd);
     b->ntri = (int64_t)(index_words / b->opts.index_stride);
+    BinaryBvhDevice td;
+    if (separate_tree(b->opts))
+      build_binary_gpu(d_positions, position_words, d_indices, index_words, traversal_options(b->opts), s, &td);
     WideBvhDevice wd;
-    const WideBvhHost w = encode_wide_gpu(bd, d_positions, b->opts.position_stride, d_indices, b->opts.index_stride,
-                                          nullptr, 0, 0, nullptr, nullptr, s, &wd);
+    const WideBvhHost w = encode_wide_gpu(separate_tree(b->opts) ? td : bd, d_positions, b->opts.position_stride,
+                                          d_indices, b->opts.index_stride, nullptr, 0, 0, query_collapse(b->opts),
+                                          nullptr, s, &wd);
     publish(b.get(), w, &wd);
     b->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     *out_bvh = b.release();

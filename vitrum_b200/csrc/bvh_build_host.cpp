@@ -192,6 +192,7 @@ void validate_options(const BuildOptions& o) {
   if (o.max_leaf < 1 || o.max_leaf > 4)
     fail(VT_ERR_RANGE, "maxLeafTriangles must be in [1, 4] for 8-wide device nodes, got " + std::to_string(o.max_leaf));
   if (o.bins < 2 || o.bins > 256) fail(VT_ERR_RANGE, "binCount must be in [2, 256], got " + std::to_string(o.bins));
+  if (o.traversal_tree < 1 || o.traversal_tree > 3) fail(VT_ERR_RANGE, "traversal_tree must be in [0, 3]");
   if (o.max_depth < 0 || o.max_depth > kMaxBinaryDepth)
     fail(VT_ERR_RANGE, "maxDepth must be in [0, 58], got " + std::to_string(o.max_depth));
 }

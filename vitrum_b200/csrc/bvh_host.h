@@ -18,6 +18,9 @@ struct BuildOptions {
   int max_leaf = 4;
   int bins = 16;
   int max_depth = kMaxBinaryDepth;
+  // tree the queries traverse: 1 this tree, reference grouping; 2 this tree, SAH-optimal
+  // grouping; 3 a second tree (<= 2 per leaf, 32 bins), SAH-optimal grouping
+  int traversal_tree = 3;
 };
 
 struct BinaryBvhHost {
