@@ -37,8 +37,8 @@ constexpr int kWeights = kLayers * kWidth * kWidth;
 enum : int { kColSh = 32, kColNormal = 48, kColRough = 51, kColDiffuse = 52, kColSpecular = 55, kColOne = 58 };
 
 // Query tiles in flight per inference CTA when the configuration leaves it open:
-// two (two CTAs of 256 threads per SM) ran 1,048,576 queries of the 16 x 2^19 grid
-// in 0.46 ms against 0.75 ms with one (three CTAs of 128) and 0.97 ms with three.
+// two (8 warps per SM) ran 1,048,576 queries of the 16 x 2^19 grid in 0.46 ms
+// against 0.75 ms with one (4 warps) and 0.97 ms with three.
 constexpr int kDefaultInferTiles = 2;
 
 struct Config {

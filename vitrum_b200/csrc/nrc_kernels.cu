@@ -623,8 +623,10 @@ void launch_infer_t(const View& v, const float4* records, uint32_t rec_stride_f4
 void launch_infer(const View& v, const float4* records, uint32_t rec_stride_f4, const uint32_t* n_dev, uint32_t n,
                   float* rgb_out, float4* radiance, int tiles_per_cta, cudaStream_t s) {
   if (n == 0) return;
-  // tiles in flight per CTA: 1 (three CTAs per SM: 65 KB shared memory each), 2 (two CTAs per
-  // SM, 81 KB), 3 (two CTAs per SM, 97 KB)
+  // tiles in flight per CTA: 1, 2 or 3 (65, 81 or 97 KB of shared memory).  Under the default
+  // carve-out one CTA runs per SM, which keeps most of the unified L1 for the hash-table gathers:
+  // asking for the largest shared-memory carve-out (three, two and two CTAs per SM) made two tiles
+  // per CTA slower (0.47 -> 0.82 ms for 1,048,576 queries)
   if (tiles_per_cta >= 3) launch_infer_t<3>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
   else if (tiles_per_cta == 2) launch_infer_t<2>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
   else launch_infer_t<1>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
