@@ -81,6 +81,15 @@ void upload(DeviceBuffer<T>& dst, const std::vector<T>& src, cudaStream_t s) {
   if (!src.empty()) VT_CUDA(cudaMemcpyAsync(dst.ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
+// Device bytes of wave state per path in flight.
+size_t batch_bytes_per_path(const vt_batch* b) {
+  return 2 * (2 * sizeof(*b->rays[0].ptr) + sizeof(*b->through[0].ptr) + sizeof(*b->state[0].ptr) +
+              sizeof(*b->ray_root[0].ptr)) +
+         sizeof(*b->hits.ptr) + sizeof(*b->order.ptr) + sizeof(*b->keys.ptr) + 2 * sizeof(*b->shadow_rays.ptr) +
+         sizeof(*b->shadow_contrib.ptr) + sizeof(*b->shadow_root.ptr) + sizeof(*b->occluded.ptr) +
+         sizeof(*b->radiance.ptr) + sizeof(*b->path_pixel.ptr);
+}
+
 void ensure_capacity(vt_batch* b, uint32_t cap) {
   if (b->capacity >= cap) return;
   b->drop_graph();
@@ -515,8 +524,16 @@ vt_status vt_batch_autotune(vt_batch* b, vt_tuning_trial* report, size_t cap, si
     };
     vt_tuning best = start;
     double best_ms = time_it(best);
-    for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
+    // wave sizes up to the batch frame's paths whose wave state fits in half of
+    // the free device memory (the batch's own wave buffers counted as free)
+    size_t free_b = 0, total_b = 0;
+    VT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = (free_b + (size_t)b->capacity * batch_bytes_per_path(b)) / 2;
+    for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26}) {
       if (wp == best.wave_paths) continue;
+      if (wp > (1 << 24) &&
+          ((unsigned long long)wp / 2 >= b->total_paths || (size_t)wp * batch_bytes_per_path(b) > budget))
+        continue;
       vt_tuning t = best;
       t.wave_paths = wp;
       const double ms = time_it(t);

@@ -1423,8 +1423,16 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
     vt_tuning best{(int32_t)wave_paths_of(e), e->opts.sort_by_material > 0 ? 1 : 0,
                    e->trace_blocks_per_sm, e->trace_stage_nodes ? 1 : 0, e->sort_rays, nrc_tiles_of(e)};
     double best_ms = time_it(best);
-    for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
+    // wave sizes up to the frame's paths (rounded up to a power of two) whose
+    // wave state fits in half of the free device memory (the engine's own wave
+    // buffers counted as free)
+    size_t free_b = 0, total_b = 0;
+    VT_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = (free_b + (size_t)e->capacity * wave_bytes_per_path(e)) / 2;
+    const size_t frame_paths = (size_t)frame->width * frame->height * (size_t)frame->samples;
+    for (int wp : {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26}) {
       if (wp == best.wave_paths) continue;
+      if (wp > (1 << 24) && ((size_t)wp / 2 >= frame_paths || (size_t)wp * wave_bytes_per_path(e) > budget)) continue;
       vt_tuning t = best;
       t.wave_paths = wp;
       const double ms = time_it(t);
