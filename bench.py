@@ -572,7 +572,7 @@ def run_light_tree(args, dev, local, barrier):
     return out
 
 
-def run_nrc(args, dev, local, barrier):
+def run_nrc(args, dev, local, barrier, shape=None):
     """Neural radiance cache against plain path tracing on the 1024-instance
     cloud at 1920x1080, 8 bounces, 16 spp per frame, from a cold start: each
     arm is a fresh engine rendering NRC_FRAMES progressive frames, the NRC
@@ -582,16 +582,21 @@ def run_nrc(args, dev, local, barrier):
     seeds and cache initialisations); per budget (the NRC arm's device time
     after 1, 2, 4, ... frames) the median over seeds of the accumulated image's
     relMSE, plain interpolated to the same time; plus the steady-state
-    single-frame relMSE and frame costs."""
+    single-frame relMSE and frame costs.  `shape`: the launch shape the
+    instanced leg's autotuner chose for this scene, given to both arms."""
     from vitrum_b200 import scenes
     from vitrum_b200.engine import Engine
     from vitrum_b200.nrc import NrcConfig
     sc, cam = scenes.instanced_cloud()
     ref, rvar, oracle_s = _cloud_oracle(args, local)
+    keys = ("wave_paths", "sort_by_material", "trace_blocks_per_sm", "stage_hot_nodes", "sort_rays")
+    launch = {k: shape[k] for k in keys} if shape else None
 
     def arm(nrc, s):
         e = Engine(device=local, max_bounces=I_BOUNCES, max_samples_per_pixel=1 << 20)
         e.set_scene(sc)
+        if launch:
+            e.set_tuning(**launch)
         if nrc:
             e.set_nrc(prefix_bounces=1, train_steps=4, train_batch=65536, warmup_frames=NRC_WARM,
                       cache=NrcConfig(seed=s + 1))
@@ -649,7 +654,9 @@ def run_nrc(args, dev, local, barrier):
         "workload": "1024-instance cloud, 1920x1080, 8 bounces, 16 spp per frame, %d frames from a cold start, %d "
                     "seeds; NRC: hash grid 16 x 2^19 x 2 fp16 (base 16, growth 1.5), 64-input MLP 5 x 64 ReLU + 3, "
                     "fp16/fp32-accumulate on tcgen05, 4 Adam steps x 65,536 samples per frame, 1-bounce prefix, "
-                    "first %d frames plain while the cache trains (charged)" % (NRC_FRAMES, NRC_SEEDS, NRC_WARM),
+                    "first %d frames plain while the cache trains (charged); both arms at the instanced leg's "
+                    "autotuned launch shape" % (NRC_FRAMES, NRC_SEEDS, NRC_WARM),
+        "launch_shape": launch,
         "oracle": {"spp": args.oracle_spp, "accumulation": "fp64", "seconds": round(oracle_s, 1),
                    "note": "its per-pixel variance of the mean is subtracted from every squared error"},
         "metric": "relMSE = mean((x - ref)^2 / (ref^2 + 1e-2)) of the accumulated image at equal device time "
@@ -787,7 +794,8 @@ def run_ours(args, rank, world, local):
     solo = world == 1
     query = run_query(args, dev, local, rank, world, barrier) if solo and not args.no_query else None
     instanced = run_instanced(args, dev, local, barrier) if solo and not args.no_instanced else None
-    nrc = run_nrc(args, dev, local, barrier) if solo and not args.no_nrc else None
+    nrc = run_nrc(args, dev, local, barrier, instanced["tuning"] if instanced else None) \
+        if solo and not args.no_nrc else None
     light_tree = run_light_tree(args, dev, local, barrier) if solo and not args.no_light_tree else None
     builds = run_build(args, dev, local) if solo and not args.no_build else None
     batch = run_batch(args, dev, local, barrier) if solo and not args.no_batch else None
