@@ -56,6 +56,33 @@ def test_unknown_build_option_raises():
         bvh.build_compressed_wide_bvh(np.zeros(12, np.float32), np.zeros(4, np.uint32), leafSize=2)
 
 
+def test_traversal_tree_option_maps_to_the_abi():
+    # the reference's option keys plus traversalTree; names map to the C enum (0 = default)
+    o = bvh._options({"maxLeafTriangles": 2, "traversalTree": "sah"})
+    assert (o.max_leaf_triangles, o.traversal_tree) == (2, 2)
+    assert bvh._options({}).traversal_tree == 0
+    assert bvh._options({"traversalTree": "fast"}).traversal_tree == 3
+    with pytest.raises(ValueError):
+        bvh._options({"traversalTree": "binary"})
+    with pytest.raises(N.VtError):  # set before any device work: a null handle is rejected
+        N.call("vt_bvh_set_trace_order", None, 5)
+
+
+def test_tuning_and_option_structs_match_the_header():
+    # every vt_tuning / vt_engine_options / vt_nrc_config field the header declares, in order
+    import re
+    from vitrum_b200.batch import _Tuning
+    from vitrum_b200.engine import _EngineOptions
+    from vitrum_b200.nrc import _Config
+    hdr = open(__import__("os").path.join(__import__("os").path.dirname(__file__), "..", "include",
+                                          "vitrum_pt.h")).read()
+    for cname, py in (("vt_tuning", _Tuning), ("vt_engine_options", _EngineOptions), ("vt_nrc_config", _Config)):
+        body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (cname, cname), hdr, re.S).group(1)
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = re.findall(r"(\w+)(?:\[\d+\])?;", body)
+        assert fields == [f for f, _ in py._fields_], cname
+
+
 def test_generators_are_deterministic():
     a, ra = scenes.config1(256, 64, seed=7)
     b, rb = scenes.config1(256, 64, seed=7)
