@@ -335,12 +335,33 @@ __global__ void k_light_tree_select(const float* tree, uint32_t n_pos, uint32_t 
 }
 
 // ---------------------------------------------------------------- raygen
+// Pixel of the j-th path of a sample plane (j < W * H): 8 x 4 pixel tiles in
+// row-major tile order, so the 32 paths of a warp look through one compact
+// tile (their rays, and the next bounce's origins, lie close together); the
+// pixels outside the full tiles follow, the right strip then the bottom rows,
+// each row-major.  A bijection of [0, W * H); the per-pixel sample streams are
+// keyed by the pixel, so the image does not depend on it.
+__device__ __forceinline__ uint32_t tile_pixel(uint32_t j, uint32_t W, uint32_t H) {
+  constexpr uint32_t kTw = 8, kTh = 4;
+  const uint32_t cols = W / kTw, rows = H / kTh;
+  const uint32_t full = cols * rows * (kTw * kTh);
+  if (j < full) {
+    const uint32_t t = j / (kTw * kTh), r = j % (kTw * kTh);
+    return ((t / cols) * kTh + r / kTw) * W + (t % cols) * kTw + r % kTw;
+  }
+  uint32_t k = j - full;
+  const uint32_t rw = W - cols * kTw, strip = rw * rows * kTh;
+  if (k < strip) return (k / rw) * W + cols * kTw + k % rw;
+  k -= strip;
+  return (rows * kTh + k / W) * W + k % W;
+}
+
 __global__ void k_raygen(FrameView f, WaveBuffers w) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) w.counters[0] = f.paths;
   if (i >= f.paths) return;
   const uint32_t wh = f.width * f.height;
-  uint32_t pix = i % wh, s = i / wh;
+  uint32_t pix = tile_pixel(i % wh, f.width, f.height), s = i / wh;
   const float* M = f.cam;
   const uint32_t frame_seed = __float_as_uint(__ldg(M + 16));
   uint32_t key;
@@ -531,15 +552,16 @@ __device__ __forceinline__ float2 project_ndc(const float* M, float3 p) {
 // pixel after the wave's bounce-0 closest-hit trace: the normal facing the
 // camera ray, the hit's distance from the ray origin, the base colour and the
 // screen motion; misses write the reference's defaults.  Queue slot == path
-// id at bounce 0, and the recorded sample's paths are one pixel-major block of
-// the wave; waves that do not hold the sample return at once.
+// id at bounce 0, and the recorded sample's paths are one block of the wave
+// (in tile_pixel order); waves that do not hold the sample return at once.
 __global__ void k_aux_first_hit(SceneView sc, FrameView f, WaveBuffers w) {
   const uint32_t wh = f.width * f.height;
-  const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= wh) return;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= wh) return;
+  const uint32_t pix = tile_pixel(j, f.width, f.height);
   const uint32_t first = w.counters[kCntWaveSample], want = __float_as_uint(f.aux.consts[32]);
   if (want < first || want - first >= f.spp_wave) return;
-  const uint32_t p = (want - first) * wh + pix;
+  const uint32_t p = (want - first) * wh + j;
   const AuxView& a = f.aux;
   const int4 h = w.hits[p];
   if (h.x < 0) {
@@ -675,7 +697,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(SceneView sc0, FrameView f, Wa
         }
         if (query && f.nrc_tile_error) {
           // tiles whose cache error estimate is above the threshold keep path tracing
-          const uint32_t pix = path % (f.width * f.height);
+          const uint32_t pix = tile_pixel(path % (f.width * f.height), f.width, f.height);
           const uint32_t tile = (pix / f.width / f.nrc_tile) * f.nrc_tiles_x + (pix % f.width) / f.nrc_tile;
           if (f.nrc_tile_error[tile] > f.nrc_fallback) query = false;
         }
@@ -807,13 +829,14 @@ __global__ void k_shadow_resolve(WaveBuffers w) {
 
 __global__ void k_accumulate(FrameView f, WaveBuffers w, AccumView a) {
   const uint32_t wh = f.width * f.height;
-  const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= wh) return;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;  // path slot within a sample plane
+  if (j >= wh) return;
+  const uint32_t pix = tile_pixel(j, f.width, f.height);
   float3 s = f3(0.0f, 0.0f, 0.0f);
   float l1 = 0.0f, l2 = 0.0f;  // luminance moments (varianceMomentsBuffer, kernel.wgsl.ts:936-940)
   double s64[3] = {0, 0, 0}, q64[3] = {0, 0, 0}, m64[4] = {0, 0, 0, 0};
   for (uint32_t k = 0; k < f.spp_wave; ++k) {
-    const float4 r = w.radiance[(size_t)k * wh + pix];
+    const float4 r = w.radiance[(size_t)k * wh + j];
     s = s + f3(r.x, r.y, r.z);
     const float lum = 0.2126f * r.x + 0.7152f * r.y + 0.0722f * r.z;
     l1 += lum;
