@@ -958,7 +958,7 @@ __global__ void k_raygen_batch(FrameView f, WaveBuffers w, uint32_t capacity) {
   const BatchScene& B = f.batch[lo];
   const unsigned long long local = g - B.path_begin;
   const uint32_t wh = B.width * B.height;
-  const uint32_t pix = (uint32_t)(local % wh), sample = (uint32_t)(local / wh);
+  const uint32_t pix = tile_pixel((uint32_t)(local % wh), B.width, B.height), sample = (uint32_t)(local / wh);
   const uint32_t x = pix % B.width, y = pix / B.width;
   uint32_t rng = pcg_init(x, y, B.frame_seed ^ sample);
   const float jx = rand01(rng), jy = rand01(rng);
