@@ -90,6 +90,10 @@ def test_trace_order_keeps_every_result(cuda):
     soup = scenes.random_triangles(65536, seed=2024)
     rays = scenes.sphere_rays(1 << 18, seed=77)
     rays[::97, 4:7] *= -1.0  # some rays point away from the scene (miss cell)
+    rays[5, 0] = np.nan       # degenerate rays: a NaN origin, a zero direction, an empty interval,
+    rays[6, 4:7] = 0.0        # an infinite origin -- each lands in some bucket and keeps its result
+    rays[7, 3], rays[7, 7] = 2.0, 1.0
+    rays[8, 0:3] = np.inf
     g = vb.build_compressed_wide_bvh(soup.positions, soup.indices)
     g.set_trace_order(0)
     want = g.intersect_first_hit(rays)
