@@ -1108,16 +1108,13 @@ vt_status vt_capture(vt_engine* e, float* rgba, size_t cap) {
     const size_t px = (size_t)e->width * e->height;
     if (cap < 4 * px) fail(VT_ERR_RANGE, "capture buffer too small");
     vt::DeviceScope ds(e->device);
+    // the mean on the device (the staging array of the present pass), then one
+    // copy into the caller's memory (a direct DMA when it is page-locked)
+    e->present.resize(px);
+    vt::pt::launch_capture_mean(e->accum.ptr, px, e->present.ptr, e->stream);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaMemcpyAsync(rgba, e->present.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
     VT_CUDA(cudaStreamSynchronize(e->stream));
-    VT_CUDA(cudaMemcpy(rgba, e->accum.ptr, px * sizeof(float4), cudaMemcpyDeviceToHost));
-    for (size_t i = 0; i < px; ++i) {
-      const float n = rgba[4 * i + 3];
-      const float inv = n > 0.0f ? 1.0f / n : 0.0f;
-      rgba[4 * i] *= inv;
-      rgba[4 * i + 1] *= inv;
-      rgba[4 * i + 2] *= inv;
-      rgba[4 * i + 3] = 1.0f;
-    }
   });
 }
 

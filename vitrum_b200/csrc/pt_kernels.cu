@@ -1070,6 +1070,21 @@ __global__ void k_present(const float4* __restrict__ accum, size_t pixels, int m
   out[i] = make_float4(r, g, b, 1.0f);
 }
 
+// Mean radiance per pixel (captureFrame 'linear'): sum / count with the
+// correctly rounded reciprocal and product, alpha 1 (0 where nothing landed).
+__global__ void k_capture_mean(const float4* __restrict__ accum, size_t pixels, float4* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pixels) return;
+  const float4 a = accum[i];
+  const float inv = a.w > 0.0f ? __frcp_rn(a.w) : 0.0f;
+  out[i] = make_float4(__fmul_rn(a.x, inv), __fmul_rn(a.y, inv), __fmul_rn(a.z, inv), 1.0f);
+}
+
+void launch_capture_mean(const float4* accum, size_t pixels, float4* out, cudaStream_t s) {
+  if (pixels == 0) return;
+  k_capture_mean<<<(unsigned)((pixels + 255) / 256), 256, 0, s>>>(accum, pixels, out);
+}
+
 void launch_present(const float4* accum, size_t pixels, int tonemap, float exposure, int srgb, float4* out,
                     cudaStream_t s) {
   if (pixels == 0) return;

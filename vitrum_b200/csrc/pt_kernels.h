@@ -180,6 +180,7 @@ void launch_accumulate_batch(const WaveBuffers& w, float4* accum, uint32_t capac
 // Present pass of an accumulation (sums with the sample count in .w): the mean
 // through exposure and a tonemap (0 ACES filmic, 1 AgX, 2 Reinhard, 3 clamp,
 // 4 none), then the sRGB OETF when `srgb` (present.wgsl.ts:59-80).
+void launch_capture_mean(const float4* accum, size_t pixels, float4* out, cudaStream_t s);
 void launch_present(const float4* accum, size_t pixels, int tonemap, float exposure, int srgb, float4* out,
                     cudaStream_t s);
 // totals[0] += queue count traced this bounce, totals[1] += shadow rays traced
