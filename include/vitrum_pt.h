@@ -710,7 +710,7 @@ typedef struct vt_nrc_config {
   uint32_t seed;             /* weight / table initialisation */
   int32_t infer_tiles;       /* query tiles of 128 in flight per inference CTA, one per warpgroup (the MLP
                                 tile: more tiles keep more table gathers in flight and overlap one tile's
-                                gathers with another's tensor-core products), 1..3; 0 = the default */
+                                gathers with another's tensor-core products), 1..4; 0 = the default (4) */
 } vt_nrc_config;
 
 /* Features of one cache query or training sample, 16 floats:
@@ -805,7 +805,7 @@ typedef struct vt_tuning {
                                  queue by its 2^4-per-axis origin cell and octant (engines only;
                                  batches take 0 or 1) */
   int32_t nrc_infer_tiles;    /* engines rendering with the radiance cache: query tiles of 128 in flight per
-                                 inference CTA (vt_nrc_config.infer_tiles, 1..3); 0 = unchanged */
+                                 inference CTA (vt_nrc_config.infer_tiles, 1..4); 0 = unchanged */
 } vt_tuning;
 
 vt_status vt_batch_create(int32_t device, const vt_engine_options* options, vt_batch** out);

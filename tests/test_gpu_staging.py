@@ -64,7 +64,7 @@ def test_set_tuning_validation(cuda):
     e = Engine(max_bounces=2)
     e.set_scene(sc)
     for bad in (dict(wave_paths=10), dict(trace_blocks_per_sm=17), dict(trace_blocks_per_sm=-1), dict(sort_rays=4),
-                dict(nrc_infer_tiles=4)):
+                dict(nrc_infer_tiles=5)):
         with pytest.raises(N.VtError):
             e.set_tuning(**bad)
     e.set_tuning(wave_paths=1 << 18, sort_by_material=True, trace_blocks_per_sm=6, stage_hot_nodes=True)

@@ -1465,7 +1465,7 @@ vt_status vt_engine_autotune(vt_engine* e, const vt_frame_input* frame, vt_tunin
     if (e->nrc) {
       // the radiance cache's MLP tile: query tiles in flight per inference CTA
       const int tiles_start = best.nrc_infer_tiles;
-      for (int nt : {1, 2, 3}) {
+      for (int nt : {1, 2, 3, 4}) {
         if (nt == tiles_start) continue;
         vt_tuning t = best;
         t.nrc_infer_tiles = nt;
@@ -1553,7 +1553,7 @@ vt_status vt_engine_set_tuning(vt_engine* e, const vt_tuning* t) {
       fail(VT_ERR_RANGE, "trace_blocks_per_sm must be in [0, 16]");
     if (t->stage_hot_nodes != 0 && t->stage_hot_nodes != 1) fail(VT_ERR_RANGE, "stage_hot_nodes must be 0 or 1");
     if (t->sort_rays < 0 || t->sort_rays > 3) fail(VT_ERR_RANGE, "sort_rays must be in [0, 3]");
-    if (t->nrc_infer_tiles < 0 || t->nrc_infer_tiles > 3) fail(VT_ERR_RANGE, "nrc_infer_tiles must be in [0, 3]");
+    if (t->nrc_infer_tiles < 0 || t->nrc_infer_tiles > 4) fail(VT_ERR_RANGE, "nrc_infer_tiles must be in [0, 4]");
     vt::DeviceScope ds(e->device);
     VT_CUDA(cudaStreamSynchronize(e->stream));
     e->opts.wave_paths = t->wave_paths;

@@ -37,9 +37,9 @@ constexpr int kWeights = kLayers * kWidth * kWidth;
 enum : int { kColSh = 32, kColNormal = 48, kColRough = 51, kColDiffuse = 52, kColSpecular = 55, kColOne = 58 };
 
 // Query tiles in flight per inference CTA when the configuration leaves it open:
-// two (8 warps per SM) ran 1,048,576 queries of the 16 x 2^19 grid in 0.46 ms
-// against 0.75 ms with one (4 warps) and 0.97 ms with three.
-constexpr int kDefaultInferTiles = 2;
+// one CTA per SM keeps 4 T warps in flight; 1,048,576 queries of the 16 x 2^19
+// grid took 0.75 / 0.46 / 0.40 / 0.39 ms with T = 1 / 2 / 3 / 4.
+constexpr int kDefaultInferTiles = 4;
 
 struct Config {
   int levels = 16;
@@ -50,7 +50,7 @@ struct Config {
   float table_lr = 1e-2f;    // hash grid
   float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
   float aabb_min[3] = {0, 0, 0}, aabb_max[3] = {1, 1, 1};
-  int infer_tiles = kDefaultInferTiles;  // query tiles of 128 in flight per inference CTA (1..3)
+  int infer_tiles = kDefaultInferTiles;  // query tiles of 128 in flight per inference CTA (1..4)
 };
 
 // Device-side view used by the kernels.
@@ -84,7 +84,7 @@ struct View {
 
 // Inference over n records -> rgb[n] (or added into radiance[path] * throughput when
 // `paths` is given: records are followed by (path id bits, T.rgb) float4 each).
-// tiles_per_cta: query tiles of 128 in flight per CTA, one per warpgroup (1..3).
+// tiles_per_cta: query tiles of 128 in flight per CTA, one per warpgroup (1..4).
 void launch_infer(const View& v, const float4* records, uint32_t rec_stride_f4, const uint32_t* n_dev, uint32_t n,
                   float* rgb_out, float4* radiance, int tiles_per_cta, cudaStream_t s);
 // One training pass over n samples (records + float4 target per sample):

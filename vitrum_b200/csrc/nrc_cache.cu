@@ -37,7 +37,7 @@ void validate(const Config& c) {
   for (int k = 0; k < 3; ++k)
     if (!std::isfinite(c.aabb_min[k]) || !std::isfinite(c.aabb_max[k]) || !(c.aabb_max[k] >= c.aabb_min[k]))
       fail(VT_ERR_INVALID_ARGUMENT, "aabb must be finite with max >= min");
-  if (c.infer_tiles < 1 || c.infer_tiles > 3) fail(VT_ERR_RANGE, "infer_tiles must be 0 or in 1..3");
+  if (c.infer_tiles < 1 || c.infer_tiles > 4) fail(VT_ERR_RANGE, "infer_tiles must be 0 or in 1..4");
 }
 
 }  // namespace

@@ -42,8 +42,8 @@ class Cache {
     tiles_x_ = tiles_x;
   }
   void clear_gradients(cudaStream_t s);
-  // Query tiles in flight per inference CTA (1..3).
-  void set_infer_tiles(int t) { cfg_.infer_tiles = t < 1 ? 1 : (t > 3 ? 3 : t); }
+  // Query tiles in flight per inference CTA (1..4).
+  void set_infer_tiles(int t) { cfg_.infer_tiles = t < 1 ? 1 : (t > 4 ? 4 : t); }
   // Clocks the kernels wait for their MMAs before giving up (0: kDefaultWaitCycles).
   void set_wait_cycles(long long c) { wait_cycles_ = c > 0 ? c : kDefaultWaitCycles; }
 

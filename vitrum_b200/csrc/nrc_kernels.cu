@@ -241,7 +241,7 @@ __device__ __forceinline__ bool group_and(uint32_t id, bool p) {
 // table gathers per query), issues its own MMA chain from its first thread and
 // waits on its own mbarrier -- so one tile's gathers overlap another's MMAs.
 template <int T>
-__global__ void __launch_bounds__(128 * T, T == 1 ? 3 : 2)
+__global__ void __launch_bounds__(128 * T, T == 1 ? 3 : (T == 2 ? 2 : 1))
     k_nrc_infer(View v, const float4* __restrict__ recs, uint32_t stride, const uint32_t* __restrict__ n_dev,
                 uint32_t n_host, float* __restrict__ rgb, float4* __restrict__ radiance) {
   extern __shared__ uint8_t smem_raw[];
@@ -623,11 +623,12 @@ void launch_infer_t(const View& v, const float4* records, uint32_t rec_stride_f4
 void launch_infer(const View& v, const float4* records, uint32_t rec_stride_f4, const uint32_t* n_dev, uint32_t n,
                   float* rgb_out, float4* radiance, int tiles_per_cta, cudaStream_t s) {
   if (n == 0) return;
-  // tiles in flight per CTA: 1, 2 or 3 (65, 81 or 97 KB of shared memory).  Under the default
+  // tiles in flight per CTA: 1 to 4 (65 to 113 KB of shared memory).  Under the default
   // carve-out one CTA runs per SM, which keeps most of the unified L1 for the hash-table gathers:
-  // asking for the largest shared-memory carve-out (three, two and two CTAs per SM) made two tiles
-  // per CTA slower (0.47 -> 0.82 ms for 1,048,576 queries)
-  if (tiles_per_cta >= 3) launch_infer_t<3>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
+  // asking for the largest shared-memory carve-out (three or two CTAs per SM) made two tiles per
+  // CTA slower (0.47 -> 0.82 ms for 1,048,576 queries)
+  if (tiles_per_cta >= 4) launch_infer_t<4>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
+  else if (tiles_per_cta == 3) launch_infer_t<3>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
   else if (tiles_per_cta == 2) launch_infer_t<2>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
   else launch_infer_t<1>(v, records, rec_stride_f4, n_dev, n, rgb_out, radiance, s);
 }

@@ -642,7 +642,7 @@ class Engine:
         another engine or an autotune trial can be passed back as keywords.
         sort_rays: 0 queue order, 1 direction octant, 2 origin cell and octant
         (True / False read as 1 / 0).  nrc_infer_tiles: query tiles per inference
-        CTA of the radiance cache (1..3; 0 leaves it)."""
+        CTA of the radiance cache (1..4; 0 leaves it)."""
         from .batch import _Tuning
         t = _Tuning(int(wave_paths), 1 if sort_by_material else 0, int(trace_blocks_per_sm),
                     1 if stage_hot_nodes else 0, int(sort_rays), int(nrc_infer_tiles))

@@ -42,7 +42,7 @@ class NrcConfig:
     aabb_min: Sequence[float] = (0.0, 0.0, 0.0)
     aabb_max: Sequence[float] = (1.0, 1.0, 1.0)
     seed: int = 1
-    infer_tiles: int = 0  # query tiles of 128 in flight per inference CTA (1..3; 0: the default)
+    infer_tiles: int = 0  # query tiles of 128 in flight per inference CTA (1..4; 0: the default)
 
     def to_c(self) -> _Config:
         return _Config(self.levels, self.log2_table_size, self.base_resolution, self.growth, self.learning_rate,

@@ -62,7 +62,7 @@ def main(argv=None):
     ap.add_argument("--rays", type=int, default=1 << 20)
     ap.add_argument("--instances", type=int, default=1024)
     ap.add_argument("--nrc", action="store_true", help="path tracing with the neural radiance cache")
-    ap.add_argument("--tiles", type=int, default=0, help="nrc: query tiles per inference CTA (1..3)")
+    ap.add_argument("--tiles", type=int, default=0, help="nrc: query tiles per inference CTA (1..4)")
     ap.add_argument("--trace-order", type=int, default=0,
                     help="query: spatial trace order, Morton bits per axis (0: input order)")
     a = ap.parse_args(argv)
