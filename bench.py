@@ -23,11 +23,16 @@ step = one frame rendered from a cleared accumulation.  Metric: Mrays/s
 * instanced: the two-level workload (1024 instances, 1920x1080, 16 spp, 8
   bounces) in the same line: Mrays/s, ms/frame, stage times.
 * nrc: equal-time relMSE of the neural-radiance-cache path tracer against
-  plain path tracing on the instanced scene (480x270, 65,536-spp FP64 oracle),
-  and both frame costs at 1920x1080 x 16 spp.
+  plain path tracing on the instanced scene at 1920x1080 x 16 spp per frame:
+  64 frames from a cold start (training and warm-up charged), five seeds,
+  against a 16,384-spp FP64 oracle; accumulated and per-frame results.
+* light_tree: light-tree against uniform NEE selection at equal time on the
+  instanced scene; build: GPU scene builds against the host pipeline.
 * batch: 64 box rooms of uneven size rendered as one batch (autotuned launch
   shape, one CUDA graph per batch frame) against the same frames one scene at
   a time: aggregate Mrays/s of both.
+* Launch shapes and tree shapes come from the project's autotuners, run
+  outside the timed regions.
 * cpu_baseline / --impl reference: the C restatement (oracle) of the same
   estimator on all host cores, full 512x512 frame at a few spp per step, the
   scene and BVH built before the clock starts (no reference CPU integrator
