@@ -530,8 +530,9 @@ __global__ void __launch_bounds__(128, 1)
 // ---------------------------------------------------------------- Adam
 __device__ __forceinline__ bool fin(float x) { return x == x && fabsf(x) <= 3.402823e38f; }
 
+// ibc1 / ibc2: 1 / (1 - beta^t), rounded once on the host (a product per value instead of two divisions)
 __device__ __forceinline__ float adam_one(float cur, float& m, float& vv, float g, float lr, float b1, float b2,
-                                          float eps, float bc1, float bc2, int* diag) {
+                                          float eps, float ibc1, float ibc2, int* diag) {
   if (!fin(cur) || !fin(m) || !fin(vv) || vv < 0.0f) {
     m = 0.0f;
     vv = 0.0f;
@@ -544,7 +545,7 @@ __device__ __forceinline__ float adam_one(float cur, float& m, float& vv, float 
   }
   const float mi = b1 * m + (1.0f - b1) * g;
   const float vi = b2 * vv + (1.0f - b2) * g * g;
-  const float mh = mi / bc1, vh = vi / bc2;
+  const float mh = mi * ibc1, vh = vi * ibc2;
   const float up = cur - lr * mh / (sqrtf(vh) + eps);
   if (!fin(up) || !fin(mi) || !fin(vi)) {
     if (diag) atomicAdd(diag, 1);
@@ -557,10 +558,10 @@ __device__ __forceinline__ float adam_one(float cur, float& m, float& vv, float 
 
 __global__ void k_nrc_adam(float* __restrict__ master, float* __restrict__ m, float* __restrict__ v,
                            float* __restrict__ grad, __half* __restrict__ out16, size_t count, float lr, float b1,
-                           float b2, float eps, float bc1, float bc2, int* diag) {
+                           float b2, float eps, float ibc1, float ibc2, int* diag) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
     float mm = m[i], vv = v[i];
-    const float up = adam_one(master[i], mm, vv, grad[i], lr, b1, b2, eps, bc1, bc2, diag);
+    const float up = adam_one(master[i], mm, vv, grad[i], lr, b1, b2, eps, ibc1, ibc2, diag);
     master[i] = up;
     m[i] = mm;
     v[i] = vv;
@@ -571,12 +572,12 @@ __global__ void k_nrc_adam(float* __restrict__ master, float* __restrict__ m, fl
 
 __global__ void k_nrc_adam_table(float2* __restrict__ master, float2* __restrict__ m, float2* __restrict__ v,
                                  float2* __restrict__ grad, __half2* __restrict__ out16, size_t pairs, float lr,
-                                 float b1, float b2, float eps, float bc1, float bc2, int* diag) {
+                                 float b1, float b2, float eps, float ibc1, float ibc2, int* diag) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += (size_t)gridDim.x * blockDim.x) {
     float2 w = master[i], mm = m[i], vv = v[i];
     const float2 g = grad[i];
-    w.x = adam_one(w.x, mm.x, vv.x, g.x, lr, b1, b2, eps, bc1, bc2, diag);
-    w.y = adam_one(w.y, mm.y, vv.y, g.y, lr, b1, b2, eps, bc1, bc2, diag);
+    w.x = adam_one(w.x, mm.x, vv.x, g.x, lr, b1, b2, eps, ibc1, ibc2, diag);
+    w.y = adam_one(w.y, mm.y, vv.y, g.y, lr, b1, b2, eps, ibc1, ibc2, diag);
     master[i] = w;
     m[i] = mm;
     v[i] = vv;
@@ -650,7 +651,7 @@ void launch_adam(float* master, float* m, float* v, float* grad, __half* out16, 
   if (!count) return;
   const size_t g = (count + 255) / 256;
   k_nrc_adam<<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, s>>>(master, m, v, grad, out16, count, lr, beta1,
-                                                                      beta2, eps, bc1, bc2, diag);
+                                                                      beta2, eps, 1.0f / bc1, 1.0f / bc2, diag);
 }
 
 void launch_adam_table(float* master, float* m, float* v, float2* grad, __half2* out16, size_t pairs, float lr,
@@ -659,7 +660,7 @@ void launch_adam_table(float* master, float* m, float* v, float2* grad, __half2*
   const size_t g = (pairs + 255) / 256;
   k_nrc_adam_table<<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, s>>>(
       reinterpret_cast<float2*>(master), reinterpret_cast<float2*>(m), reinterpret_cast<float2*>(v), grad, out16,
-      pairs, lr, beta1, beta2, eps, bc1, bc2, diag);
+      pairs, lr, beta1, beta2, eps, 1.0f / bc1, 1.0f / bc2, diag);
 }
 
 }  // namespace nrc
